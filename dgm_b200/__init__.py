@@ -1,0 +1,226 @@
+"""dgm_b200: B200-native DG residual + RK-stage engine with DGM's Domain interface.
+
+The compute path is libdgmx.so (hand-written sm_100a CUDA kernels behind the
+C ABI in include/dgmx.h).  This module is the host-side mirror of DGM's
+Domain/TimeInt interface over that ABI: ``Domain.time_derivative(U, F)``
+(src/Domain.hpp:243), ``Domain.advance(dt, nsteps)`` (TimeInt::advance,
+src/TimeInt.hpp:177-181), ``Domain.set_ic``-style state setting with
+projection, and restart-layout modal output.  There is no CPU fallback: if
+the library or a CUDA device is missing, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import meshgen  # noqa: F401
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdgmx.so")
+_lib = None
+
+EULER2D, NS2D, EULER3D, NS3D, SHALLOW = 1, 2, 8, 9, 30
+TVD3, RK4, LSRK14 = 3, 4, 14
+FLUX = {"laxfriedrichs": 0, "lf": 0, "roe": 1}
+STATUS = {0: "ok", 1: "argument", 2: "unsupported", 3: "cuda", 4: "non-physical", 5: "io", 6: "memory"}
+
+
+class DgmxError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"dgmx {STATUS.get(code, code)} error: {msg}")
+        self.code = code
+
+
+class NonPhysicalState(DgmxError):
+    pass
+
+
+class _Mesh(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("ne", ctypes.c_int), ("verts", ctypes.POINTER(ctypes.c_double)),
+                ("ncon", ctypes.c_int), ("con", ctypes.POINTER(ctypes.c_int)),
+                ("porder", ctypes.POINTER(ctypes.c_int)), ("qorder", ctypes.POINTER(ctypes.c_int))]
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("physics", ctypes.c_int), ("flux", ctypes.c_int), ("inttype", ctypes.c_int),
+                ("precision", ctypes.c_int), ("sw_balance", ctypes.c_int), ("device", ctypes.c_int),
+                ("gamma", ctypes.c_double), ("vis", ctypes.c_double), ("Pr", ctypes.c_double)]
+
+
+def lib():
+    """Load libdgmx.so (built by __graft_entry__.build / dgm_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise DgmxError(3, f"{LIB_PATH} is missing: run python -m dgm_b200.build")
+        L = ctypes.CDLL(LIB_PATH)
+        P, D, I = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int
+        L.dgmx_create.argtypes = [ctypes.POINTER(_Mesh), ctypes.POINTER(_Params), ctypes.POINTER(P)]
+        L.dgmx_create_from_files.argtypes = [ctypes.c_char_p, ctypes.POINTER(_Params), ctypes.POINTER(P)]
+        L.dgmx_destroy.argtypes = [P]
+        L.dgmx_sizes.argtypes = [P, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long),
+                                 ctypes.POINTER(ctypes.c_long)]
+        L.dgmx_coordinates.argtypes = [P, D, D, D]
+        for f in ("dgmx_set_state", "dgmx_get_state", "dgmx_get_modes", "dgmx_integrals"):
+            getattr(L, f).argtypes = [P, D]
+        for f in ("dgmx_set_state_device", "dgmx_get_state_device"):
+            getattr(L, f).argtypes = [P, ctypes.c_void_p]
+        L.dgmx_time_derivative.argtypes = [P, D, D]
+        L.dgmx_time_derivative_device.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p]
+        L.dgmx_advance.argtypes = [P, ctypes.c_double, I]
+        L.dgmx_advance_async.argtypes = [P, ctypes.c_double, I]
+        L.dgmx_sync.argtypes = [P]
+        L.dgmx_last_error.argtypes = [P]
+        L.dgmx_last_error.restype = ctypes.c_char_p
+        L.dgmx_launch_count.argtypes = [P]
+        L.dgmx_launch_count.restype = ctypes.c_long
+        L.dgmx_kernel_list.argtypes = [ctypes.POINTER(ctypes.c_int), I]
+        L.dgmx_stream.argtypes = [P]
+        L.dgmx_stream.restype = ctypes.c_void_p
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def kernel_list():
+    """Compiled instantiations: rows of (physics, L, Q, elements/CTA, threads, smem bytes)."""
+    n = 4096
+    buf = (ctypes.c_int * (6 * n))()
+    k = lib().dgmx_kernel_list(buf, n)
+    return np.frombuffer(buf, dtype=np.int32)[: 6 * k].reshape(k, 6).copy()
+
+
+class Domain:
+    """One DGM Domain on one GPU (Field layout [field][element][Q^d])."""
+
+    def __init__(self, mesh, physics: int, flux: str = "laxfriedrichs", inttype: int = LSRK14,
+                 gamma: float = 1.4, vis: float = 0.0, Pr: float = 0.72, sw_balance: bool = True,
+                 device: int = 0, precision: int = 0):
+        self._keep = []
+        verts = np.ascontiguousarray(mesh.verts, dtype=np.float64)
+        con = np.ascontiguousarray(mesh.con, dtype=np.int32)
+        por = np.ascontiguousarray(mesh.porder, dtype=np.int32)
+        qor = np.ascontiguousarray(mesh.qorder, dtype=np.int32)
+        self._keep += [verts, con, por, qor]
+        m = _Mesh(int(mesh.dim), int(verts.shape[0]), _dp(verts), int(con.shape[0]),
+                  con.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                  por.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                  qor.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        p = _Params(physics, FLUX[flux.lower()], inttype, precision, 1 if sw_balance else 0, device,
+                    gamma, vis, Pr)
+        h = ctypes.c_void_p()
+        st = lib().dgmx_create(ctypes.byref(m), ctypes.byref(p), ctypes.byref(h))
+        if st != 0:
+            raise DgmxError(st, lib().dgmx_last_error(None).decode())
+        self._init(h, mesh.dim)
+
+    @classmethod
+    def from_files(cls, root: str, inttype: int = TVD3, physics: int = EULER3D, device: int = 0):
+        """Domain from DGM input files root.inp/.msh/.con/.ord."""
+        p = _Params(physics, 0, inttype, 0, 1, device, 1.4, 0.0, 0.72)
+        h = ctypes.c_void_p()
+        st = lib().dgmx_create_from_files(root.encode(), ctypes.byref(p), ctypes.byref(h))
+        if st != 0:
+            raise DgmxError(st, lib().dgmx_last_error(None).decode())
+        self = cls.__new__(cls)
+        self._keep = []
+        nf, nq, nm = ctypes.c_long(), ctypes.c_long(), ctypes.c_long()
+        lib().dgmx_sizes(h, ctypes.byref(nf), ctypes.byref(nq), ctypes.byref(nm))
+        self._init(h, None)
+        return self
+
+    def _init(self, h, dim):
+        self.h = h
+        nf, nq, nm = ctypes.c_long(), ctypes.c_long(), ctypes.c_long()
+        lib().dgmx_sizes(h, ctypes.byref(nf), ctypes.byref(nq), ctypes.byref(nm))
+        self.nf, self.nq, self.nm = nf.value, nq.value, nm.value
+        self.dim = dim
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dgmx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != 0:
+            msg = lib().dgmx_last_error(self.h).decode()
+            raise (NonPhysicalState if st == 4 else DgmxError)(st, msg)
+
+    # --- data movement -------------------------------------------------
+    def coordinates(self):
+        x, y, z = (np.zeros(self.nq) for _ in range(3))
+        self._check(lib().dgmx_coordinates(self.h, _dp(x), _dp(y), _dp(z)))
+        return x, y, z
+
+    def set_state(self, U):
+        """Set U (GLL values, Field layout) and project it (set_ic + project)."""
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(self.nf, self.nq)
+        self._check(lib().dgmx_set_state(self.h, _dp(U)))
+
+    def state(self):
+        U = np.zeros((self.nf, self.nq))
+        self._check(lib().dgmx_get_state(self.h, _dp(U)))
+        return U
+
+    def state_into(self, U):
+        """get_state into a caller array (page-locked arrays are written by DMA)."""
+        assert U.dtype == np.float64 and U.flags.c_contiguous and U.size == self.nf * self.nq
+        self._check(lib().dgmx_get_state(self.h, _dp(U)))
+        return U
+
+    def modes(self):
+        """Restart-layout modal coefficients [field][element][L^d]."""
+        Uh = np.zeros((self.nf, self.nm))
+        self._check(lib().dgmx_get_modes(self.h, _dp(Uh)))
+        return Uh
+
+    def set_state_device(self, ptr: int):
+        self._check(lib().dgmx_set_state_device(self.h, ctypes.c_void_p(ptr)))
+
+    def state_device(self, ptr: int):
+        self._check(lib().dgmx_get_state_device(self.h, ctypes.c_void_p(ptr)))
+
+    # --- the hot path --------------------------------------------------
+    def time_derivative(self, U, F=None):
+        """Domain::time_derivative: returns F = -dU/dt (projected) at GLL points."""
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(self.nf, self.nq)
+        if F is None:
+            F = np.zeros_like(U)
+        self._check(lib().dgmx_time_derivative(self.h, _dp(U), _dp(F)))
+        return F
+
+    def time_derivative_device(self, U_ptr: int, F_ptr: int):
+        self._check(lib().dgmx_time_derivative_device(self.h, ctypes.c_void_p(U_ptr), ctypes.c_void_p(F_ptr)))
+
+    def advance(self, dt: float, nsteps: int = 1):
+        """TimeInt::advance repeated nsteps times (device resident)."""
+        self._check(lib().dgmx_advance(self.h, float(dt), int(nsteps)))
+
+    def advance_async(self, dt: float, nsteps: int = 1):
+        self._check(lib().dgmx_advance_async(self.h, float(dt), int(nsteps)))
+
+    def sync(self):
+        self._check(lib().dgmx_sync(self.h))
+
+    def integrals(self):
+        out = np.zeros(self.nf)
+        self._check(lib().dgmx_integrals(self.h, _dp(out)))
+        return out
+
+    def launch_count(self) -> int:
+        return lib().dgmx_launch_count(self.h)
+
+    def stream(self) -> int:
+        """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        return lib().dgmx_stream(self.h) or 0

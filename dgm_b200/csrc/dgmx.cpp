@@ -1,0 +1,595 @@
+// C ABI of the B200 DG engine (include/dgmx.h): handle management, device
+// buffers, and the integrator stage sequences replayed from CUDA graphs.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "dgmx_internal.hpp"
+
+using namespace dgmx;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+// TVD-RK3 (src/TimeInt.cpp:738-740), RK4 (:204-209), LSRK14 (:1870-1917)
+const double kTvdA[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0};
+const double kTvdB[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
+const double kRk4A[3] = {0.5, 0.5, 1.0};
+const double kRk4B[4] = {0.16666666666666667, 0.33333333333333333, 0.33333333333333333, 0.16666666666666667};
+const double kLsrkA[14] = {0.0, -0.7188012108672410, -0.7785331173421570, -0.0053282796654044,
+                           -0.8552979934029281, -3.9564138245774565, -1.5780575380587385,
+                           -2.0837094552574054, -0.7483334182761610, -0.7032861106563359,
+                           0.0013917096117681, -0.0932075369637460, -0.9514200470875948,
+                           -7.1151571693922548};
+const double kLsrkB[14] = {0.0367762454319673, 0.3136296607553959, 0.1531848691869027, 0.0030097086818182,
+                           0.3326293790646110, 0.2440251405350864, 0.3718879239592277, 0.6204126221582444,
+                           0.1524043173028741, 0.0760894927419266, 0.0077604214040978, 0.0024647284755382,
+                           0.0780348340049386, 5.5059777270269628};
+
+template <class T>
+cudaError_t dalloc(T **p, size_t n) {
+  return cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * (n ? n : 1));
+}
+
+// true if p is page-locked host memory the copy engines can read directly
+bool is_pinned(const void *p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) { cudaGetLastError(); return false; }
+  return at.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+struct dgmx_domain {
+  dgmx_params prm{};
+  int dim = 0, nf = 0, ne = 0, L = 0, Q = 0, G = 0, nfaces = 0, gf = 0, ld = 0, qd = 0;
+  HostMesh mesh;
+  Tables1D tab;
+  const KernelOps *ops = nullptr;
+  cudaStream_t stream = nullptr;
+  // device state
+  double *U = nullptr, *Ut = nullptr, *Acc = nullptr;   // modal registers [e][n][ld]
+  double *T[2] = {nullptr, nullptr};                     // traces [e][f][n][gf]
+  double *Rsw = nullptr;                                 // shallow-water first RHS (modal)
+  double *nod_in = nullptr, *nod_out = nullptr;          // Field-layout staging
+  double *Jdev = nullptr, *integ = nullptr;
+  int *gclass = nullptr, *perm = nullptr, *err = nullptr;
+  GeomClass *classes = nullptr;
+  FaceLink *links = nullptr;
+  double *host_pinned = nullptr;                         // pinned staging for host I/O
+  int tcur = 0;
+  bool sw_captured = false;
+  long launches = 0;
+  // graph of one whole step
+  cudaGraphExec_t graph = nullptr;
+  double graph_dt = 0.0;
+  int graph_tcur = -1;
+  std::string errmsg;
+
+  size_t nmodal() const { return (size_t)ne * nf * ld; }
+  size_t nnodal() const { return (size_t)ne * nf * qd; }
+  size_t ntrace() const { return (size_t)ne * nfaces * nf * gf; }
+
+  dgmx_status fail(dgmx_status s, const std::string &m) {
+    errmsg = m;
+    return s;
+  }
+  dgmx_status cuda(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return DGMX_OK;
+    errmsg = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? DGMX_ERR_MEMORY : DGMX_ERR_CUDA;
+  }
+
+  StageArgs base_args() const {
+    StageArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.gclass = gclass; a.classes = classes; a.links = links; a.perm = perm;
+    a.ne = ne; a.gamma = prm.gamma; a.vis = prm.vis; a.Pr = prm.Pr; a.flux = prm.flux;
+    a.err = err;
+    return a;
+  }
+
+  void release() {
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
+    void *ptrs[] = {U, Ut, Acc, T[0], T[1], Rsw, nod_in, nod_out, Jdev, integ, gclass, perm, err, classes, links};
+    for (void *p : ptrs) if (p) cudaFree(p);
+    if (host_pinned) cudaFreeHost(host_pinned);
+    if (stream) cudaStreamDestroy(stream);
+    U = Ut = Acc = Rsw = nod_in = nod_out = Jdev = integ = host_pinned = nullptr;
+    T[0] = T[1] = nullptr; gclass = perm = err = nullptr; classes = nullptr; links = nullptr; stream = nullptr;
+  }
+};
+
+namespace {
+
+// enqueue the stages of one time step on d->stream
+dgmx_status enqueue_step(dgmx_domain *d, double dt) {
+  StageArgs a = d->base_args();
+  a.dt = dt;
+  a.U = d->U; a.Ut = d->Ut; a.A = d->Acc;
+  if (d->prm.physics == DGMX_SHALLOW && d->prm.sw_balance) a.Rsub = d->Rsw;
+  auto run = [&](int kind, const double *X, double c0, double c1) -> dgmx_status {
+    a.kind = kind; a.X = X; a.c0 = c0; a.c1 = c1;
+    a.Tin = d->T[d->tcur]; a.Tout = d->T[d->tcur ^ 1];
+    cudaError_t e = d->ops->stage(a, d->stream);
+    if (e != cudaSuccess) return d->cuda(e, "stage kernel launch");
+    d->tcur ^= 1;
+    ++d->launches;
+    return DGMX_OK;
+  };
+  dgmx_status st = DGMX_OK;
+  switch (d->prm.inttype) {
+    case DGMX_LSRK14:
+      for (int s = 0; s < 14 && st == DGMX_OK; ++s) st = run(kLSRK, d->U, kLsrkA[s], kLsrkB[s]);
+      break;
+    case DGMX_TVD3:
+      st = run(kTVD0, d->U, 0.0, 0.0);
+      if (st == DGMX_OK) st = run(kTVD1, d->Ut, kTvdA[1], kTvdB[1]);
+      if (st == DGMX_OK) st = run(kTVD2, d->Ut, kTvdA[2], kTvdB[2]);
+      break;
+    case DGMX_RK4:
+      st = run(kRK40, d->U, -kRk4A[0] * dt, -kRk4B[0]);
+      if (st == DGMX_OK) st = run(kRK41, d->Ut, -kRk4A[1] * dt, -kRk4B[1]);
+      if (st == DGMX_OK) st = run(kRK41, d->Ut, -kRk4A[2] * dt, -kRk4B[2]);
+      if (st == DGMX_OK) st = run(kRK43, d->Ut, dt, -kRk4B[3]);
+      break;
+    default:
+      return d->fail(DGMX_ERR_UNSUPPORTED, "inttype must be 3, 4 or 14");
+  }
+  return st;
+}
+
+int stages_per_step(int inttype) { return inttype == DGMX_LSRK14 ? 14 : (inttype == DGMX_TVD3 ? 3 : 4); }
+
+// traces of U into T[tcur]
+dgmx_status refresh_traces(dgmx_domain *d) {
+  StageArgs a = d->base_args();
+  cudaError_t e = d->ops->traces_modal(a, d->U, d->T[d->tcur], d->stream);
+  ++d->launches;
+  return d->cuda(e, "trace kernel launch");
+}
+
+// Shallow-water balance: the first RHS ever evaluated is subtracted from all
+// later ones (src/Shallow.cpp:255-267).  Captured from the current state.
+dgmx_status capture_sw_source(dgmx_domain *d) {
+  StageArgs a = d->base_args();
+  a.kind = kRHS; a.X = d->U; a.U = d->U; a.Ut = d->Ut; a.A = d->Rsw;
+  a.Tin = d->T[d->tcur]; a.Tout = d->T[d->tcur ^ 1];
+  cudaError_t e = d->ops->stage(a, d->stream);
+  ++d->launches;
+  d->tcur ^= 1;
+  d->sw_captured = true;
+  return d->cuda(e, "shallow-water source capture");
+}
+
+dgmx_status check_error_word(dgmx_domain *d) {
+  int h[2] = {0, 0};
+  cudaError_t e = cudaMemcpyAsync(h, d->err, sizeof(h), cudaMemcpyDeviceToHost, d->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+  if (e != cudaSuccess) return d->cuda(e, "error word readback");
+  if (h[0] & 1) {
+    char buf[160];
+    std::snprintf(buf, sizeof(buf), "non-physical state (density or pressure below eps^(2/3)) on element %d", h[1]);
+    return d->fail(DGMX_ERR_NONPHYSICAL, buf);
+  }
+  return DGMX_OK;
+}
+
+dgmx_status reset_error_word(dgmx_domain *d) {
+  const int init[2] = {0, 0x7fffffff};
+  return d->cuda(cudaMemcpyAsync(d->err, init, sizeof(init), cudaMemcpyHostToDevice, d->stream), "error reset");
+}
+
+dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **out) {
+  if (!m || !p || !out) { g_create_error = "null argument"; return DGMX_ERR_ARGUMENT; }
+  *out = nullptr;
+  auto d = std::make_unique<dgmx_domain>();
+  d->prm = *p;
+  if (d->prm.gamma <= 0) d->prm.gamma = 1.4;
+  if (d->prm.Pr <= 0) d->prm.Pr = 0.72;
+  const int phys = p->physics;
+  if (phys != DGMX_EULER2D && phys != DGMX_EULER3D && phys != DGMX_SHALLOW && phys != DGMX_NS2D &&
+      phys != DGMX_NS3D) {
+    g_create_error = "unknown physics " + std::to_string(phys);
+    return DGMX_ERR_ARGUMENT;
+  }
+  if (m->dim != dim_of(phys)) { g_create_error = "mesh dimension does not match the physics"; return DGMX_ERR_ARGUMENT; }
+  if (p->inttype != DGMX_TVD3 && p->inttype != DGMX_RK4 && p->inttype != DGMX_LSRK14) {
+    g_create_error = "inttype must be 3 (TVD), 4 (RK4) or 14 (LSRK14)";
+    return DGMX_ERR_UNSUPPORTED;
+  }
+  if (p->flux != DGMX_FLUX_LF && p->flux != DGMX_FLUX_ROE) { g_create_error = "flux must be LF or Roe"; return DGMX_ERR_UNSUPPORTED; }
+  if (phys == DGMX_SHALLOW && p->flux != DGMX_FLUX_LF) { g_create_error = "shallow water supports Lax-Friedrichs only"; return DGMX_ERR_UNSUPPORTED; }
+  if (p->precision != DGMX_FP64) { g_create_error = "only the FP64 kernels are built"; return DGMX_ERR_UNSUPPORTED; }
+  if (!m->porder || m->ne <= 0) { g_create_error = "mesh needs porder"; return DGMX_ERR_ARGUMENT; }
+  const int pp = m->porder[0];
+  const int qq = (m->qorder && m->qorder[0]) ? m->qorder[0] : pp + 2;
+  for (int e = 0; e < m->ne; ++e) {
+    const int qe = (m->qorder && m->qorder[e]) ? m->qorder[e] : m->porder[e] + 2;
+    if (m->porder[e] != pp || qe != qq) {
+      g_create_error = "the GPU path needs one polynomial order for all elements";
+      return DGMX_ERR_UNSUPPORTED;
+    }
+  }
+  d->ops = find_ops(phys, pp + 1, qq);
+  if (!d->ops) {
+    g_create_error = "no kernels built for physics " + std::to_string(phys) + ", p=" + std::to_string(pp) +
+                     ", q=" + std::to_string(qq);
+    return DGMX_ERR_UNSUPPORTED;
+  }
+  d->dim = m->dim; d->nf = nfields_of(phys); d->ne = m->ne;
+  d->L = pp + 1; d->Q = qq; d->G = qq - 1;
+  d->nfaces = 2 * d->dim;
+  d->gf = d->dim == 2 ? d->G : d->G * d->G;
+  d->ld = d->dim == 2 ? d->L * d->L : d->L * d->L * d->L;
+  d->qd = d->dim == 2 ? d->Q * d->Q : d->Q * d->Q * d->Q;
+  d->tab = make_tables(d->L, d->Q, d->G);
+  std::string err;
+  if (!build_mesh(*m, d->tab, d->mesh, err)) { g_create_error = err; return DGMX_ERR_ARGUMENT; }
+
+  cudaError_t e = cudaSetDevice(p->device);
+  if (e != cudaSuccess) { g_create_error = std::string("cudaSetDevice: ") + cudaGetErrorString(e); return DGMX_ERR_CUDA; }
+  dgmx_status st;
+  auto chk = [&](cudaError_t ce, const char *what) {
+    if (ce != cudaSuccess) { st = d->cuda(ce, what); return false; }
+    return true;
+  };
+  st = DGMX_OK;
+  if (!chk(d->ops->init(d->tab), "kernel table upload")) { g_create_error = d->errmsg; d->release(); return st; }
+  if (!chk(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking), "stream")) { g_create_error = d->errmsg; d->release(); return st; }
+  bool ok = chk(dalloc(&d->U, d->nmodal()), "alloc U") && chk(dalloc(&d->Ut, d->nmodal()), "alloc Ut") &&
+            chk(dalloc(&d->Acc, d->nmodal()), "alloc Acc") && chk(dalloc(&d->T[0], d->ntrace()), "alloc T0") &&
+            chk(dalloc(&d->T[1], d->ntrace()), "alloc T1") && chk(dalloc(&d->nod_in, d->nnodal()), "alloc nodal") &&
+            chk(dalloc(&d->nod_out, d->nnodal()), "alloc nodal") && chk(dalloc(&d->Jdev, (size_t)d->ne), "alloc J") &&
+            chk(dalloc(&d->integ, (size_t)d->nf), "alloc integrals") &&
+            chk(dalloc(&d->gclass, (size_t)d->ne), "alloc gclass") &&
+            chk(dalloc(&d->classes, d->mesh.classes.size()), "alloc classes") &&
+            chk(dalloc(&d->links, d->mesh.links.size()), "alloc links") &&
+            chk(dalloc(&d->perm, d->mesh.perm.size()), "alloc perm") && chk(dalloc(&d->err, (size_t)2), "alloc err") &&
+            (phys != DGMX_SHALLOW || chk(dalloc(&d->Rsw, d->nmodal()), "alloc sw source"));
+  if (ok) {
+    ok = chk(cudaMemcpy(d->gclass, d->mesh.gclass.data(), sizeof(int) * d->ne, cudaMemcpyHostToDevice), "upload") &&
+         chk(cudaMemcpy(d->classes, d->mesh.classes.data(), sizeof(GeomClass) * d->mesh.classes.size(),
+                        cudaMemcpyHostToDevice), "upload") &&
+         chk(cudaMemcpy(d->links, d->mesh.links.data(), sizeof(FaceLink) * d->mesh.links.size(),
+                        cudaMemcpyHostToDevice), "upload") &&
+         chk(cudaMemcpy(d->perm, d->mesh.perm.data(), sizeof(int) * d->mesh.perm.size(), cudaMemcpyHostToDevice),
+             "upload") &&
+         chk(cudaMemcpy(d->Jdev, d->mesh.J.data(), sizeof(double) * d->ne, cudaMemcpyHostToDevice), "upload") &&
+         chk(cudaMemset(d->U, 0, sizeof(double) * d->nmodal()), "memset") &&
+         chk(cudaMemset(d->Ut, 0, sizeof(double) * d->nmodal()), "memset") &&
+         chk(cudaMemset(d->Acc, 0, sizeof(double) * d->nmodal()), "memset") &&
+         chk(cudaMemset(d->T[0], 0, sizeof(double) * d->ntrace()), "memset") &&
+         chk(cudaMemset(d->T[1], 0, sizeof(double) * d->ntrace()), "memset") &&
+         chk(cudaHostAlloc(reinterpret_cast<void **>(&d->host_pinned), sizeof(double) * d->nnodal() * 2,
+                           cudaHostAllocDefault), "pinned staging");
+  }
+  if (!ok) { g_create_error = d->errmsg; d->release(); return st; }
+  if ((st = reset_error_word(d.get())) != DGMX_OK) { g_create_error = d->errmsg; d->release(); return st; }
+  cudaStreamSynchronize(d->stream);
+  *out = d.release();
+  return DGMX_OK;
+}
+
+dgmx_status set_state_from_device_nodal(dgmx_domain *d, const double *Un_dev) {
+  StageArgs a = d->base_args();
+  cudaError_t e = d->ops->forward(a, Un_dev, d->U, d->stream);
+  ++d->launches;
+  if (e != cudaSuccess) return d->cuda(e, "forward kernel");
+  if ((e = cudaMemsetAsync(d->Ut, 0, sizeof(double) * d->nmodal(), d->stream))) return d->cuda(e, "memset");
+  if ((e = cudaMemsetAsync(d->Acc, 0, sizeof(double) * d->nmodal(), d->stream))) return d->cuda(e, "memset");
+  d->tcur = 0;
+  d->sw_captured = false;
+  dgmx_status st = refresh_traces(d);
+  if (st != DGMX_OK) return st;
+  return d->cuda(cudaStreamSynchronize(d->stream), "set_state");
+}
+
+}  // namespace
+
+extern "C" {
+
+dgmx_status dgmx_create(const dgmx_mesh *mesh, const dgmx_params *params, dgmx_domain **out) {
+  try {
+    return create_impl(mesh, params, out);
+  } catch (const std::exception &ex) {
+    g_create_error = ex.what();
+    return DGMX_ERR_ARGUMENT;
+  }
+}
+
+dgmx_status dgmx_create_from_files(const char *root, const dgmx_params *params, dgmx_domain **out) {
+  if (!root || !params || !out) { g_create_error = "null argument"; return DGMX_ERR_ARGUMENT; }
+  try {
+    FileCase fc;
+    std::string err;
+    if (!read_case_files(root, fc, err)) { g_create_error = err; return DGMX_ERR_IO; }
+    dgmx_params p = *params;
+    if (fc.eqntype >= 0) p.physics = fc.eqntype;
+    if (fc.inttype >= 0) p.inttype = fc.inttype;
+    if (fc.gamma > 0) p.gamma = fc.gamma;
+    if (fc.vis >= 0) p.vis = fc.vis;
+    if (fc.Pr > 0) p.Pr = fc.Pr;
+    if (!fc.flux.empty()) p.flux = fc.flux == "roe" ? DGMX_FLUX_ROE : DGMX_FLUX_LF;
+    dgmx_mesh m;
+    m.dim = fc.dim; m.ne = fc.ne; m.verts = fc.verts.data();
+    m.ncon = (int)(fc.con.size() / 4); m.con = fc.con.data();
+    m.porder = fc.porder.data(); m.qorder = fc.qorder.data();
+    return create_impl(&m, &p, out);
+  } catch (const std::exception &ex) {
+    g_create_error = ex.what();
+    return DGMX_ERR_IO;
+  }
+}
+
+dgmx_status dgmx_destroy(dgmx_domain *d) {
+  if (!d) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(d->prm.device);
+  if (d->stream) cudaStreamSynchronize(d->stream);
+  d->release();
+  delete d;
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_sizes(const dgmx_domain *d, long *nf, long *nq, long *nm) {
+  if (!d) return DGMX_ERR_ARGUMENT;
+  if (nf) *nf = d->nf;
+  if (nq) *nq = (long)d->ne * d->qd;
+  if (nm) *nm = (long)d->ne * d->ld;
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_coordinates(const dgmx_domain *d, double *x, double *y, double *z) {
+  if (!d) return DGMX_ERR_ARGUMENT;
+  const size_t n = d->mesh.cx.size();
+  if (x) std::memcpy(x, d->mesh.cx.data(), sizeof(double) * n);
+  if (y) std::memcpy(y, d->mesh.cy.data(), sizeof(double) * n);
+  if (z) std::memcpy(z, d->mesh.cz.data(), sizeof(double) * n);
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_set_state_device(dgmx_domain *d, const double *U_dev) {
+  if (!d || !U_dev) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(d->prm.device);
+  return set_state_from_device_nodal(d, U_dev);
+}
+
+dgmx_status dgmx_set_state(dgmx_domain *d, const double *U) {
+  if (!d || !U) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(d->prm.device);
+  const size_t n = d->nnodal();
+  const double *src = U;
+  if (!is_pinned(U)) { std::memcpy(d->host_pinned, U, sizeof(double) * n); src = d->host_pinned; }
+  cudaError_t e = cudaMemcpyAsync(d->nod_in, src, sizeof(double) * n, cudaMemcpyHostToDevice, d->stream);
+  if (e != cudaSuccess) return d->cuda(e, "state upload");
+  return set_state_from_device_nodal(d, d->nod_in);
+}
+
+dgmx_status dgmx_get_state_device(dgmx_domain *d, double *U_dev) {
+  if (!d || !U_dev) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(d->prm.device);
+  StageArgs a = d->base_args();
+  cudaError_t e = d->ops->backward(a, d->U, U_dev, d->stream);
+  ++d->launches;
+  if (e != cudaSuccess) return d->cuda(e, "backward kernel");
+  return d->cuda(cudaStreamSynchronize(d->stream), "get_state");
+}
+
+dgmx_status dgmx_get_state(dgmx_domain *d, double *U) {
+  if (!d || !U) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(d->prm.device);
+  StageArgs a = d->base_args();
+  cudaError_t e = d->ops->backward(a, d->U, d->nod_out, d->stream);
+  ++d->launches;
+  if (e != cudaSuccess) return d->cuda(e, "backward kernel");
+  const size_t n = d->nnodal();
+  const bool direct = is_pinned(U);
+  if ((e = cudaMemcpyAsync(direct ? U : d->host_pinned, d->nod_out, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                           d->stream)))
+    return d->cuda(e, "state download");
+  if ((e = cudaStreamSynchronize(d->stream))) return d->cuda(e, "get_state");
+  if (!direct) std::memcpy(U, d->host_pinned, sizeof(double) * n);
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_get_modes(dgmx_domain *d, double *Uh) {
+  if (!d || !Uh) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(d->prm.device);
+  std::vector<double> em(d->nmodal());
+  cudaError_t e = cudaMemcpyAsync(em.data(), d->U, sizeof(double) * em.size(), cudaMemcpyDeviceToHost, d->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+  if (e != cudaSuccess) return d->cuda(e, "modes download");
+  // element-major [e][n][m] -> restart layout [n][e][m]
+  for (int el = 0; el < d->ne; ++el)
+    for (int n = 0; n < d->nf; ++n)
+      std::memcpy(Uh + ((size_t)n * d->ne + el) * d->ld, em.data() + ((size_t)el * d->nf + n) * d->ld,
+                  sizeof(double) * d->ld);
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_time_derivative_device(dgmx_domain *d, const double *U_dev, double *F_dev) {
+  if (!d || !U_dev || !F_dev) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(d->prm.device);
+  StageArgs a = d->base_args();
+  a.Xn = U_dev; a.Fn = F_dev;
+  a.Tout = d->T[d->tcur ^ 1];
+  cudaError_t e = d->ops->traces_nodal(a, d->stream);
+  ++d->launches;
+  if (e != cudaSuccess) return d->cuda(e, "nodal trace kernel");
+  a.Tin = d->T[d->tcur ^ 1];
+  if (d->prm.physics == DGMX_SHALLOW && d->prm.sw_balance) {
+    if (!d->sw_captured) { a.Rcap = d->Rsw; d->sw_captured = true; }
+    a.Rsub = d->Rsw;
+  }
+  e = d->ops->rhs_nodal(a, d->stream);
+  ++d->launches;
+  if (e != cudaSuccess) return d->cuda(e, "nodal rhs kernel");
+  // the traces of the current modal register live in T[tcur]; T[tcur^1]
+  // was used as scratch and is rewritten by the next stage.
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_time_derivative(dgmx_domain *d, const double *U, double *F) {
+  if (!d || !U || !F) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(d->prm.device);
+  const size_t n = d->nnodal();
+  dgmx_status st = reset_error_word(d);
+  if (st != DGMX_OK) return st;
+  const bool pin_in = is_pinned(U), pin_out = is_pinned(F);
+  if (!pin_in) std::memcpy(d->host_pinned, U, sizeof(double) * n);
+  cudaError_t e = cudaMemcpyAsync(d->nod_in, pin_in ? U : d->host_pinned, sizeof(double) * n,
+                                  cudaMemcpyHostToDevice, d->stream);
+  if (e != cudaSuccess) return d->cuda(e, "upload");
+  if ((st = dgmx_time_derivative_device(d, d->nod_in, d->nod_out)) != DGMX_OK) return st;
+  if ((e = cudaMemcpyAsync(pin_out ? F : d->host_pinned + n, d->nod_out, sizeof(double) * n,
+                           cudaMemcpyDeviceToHost, d->stream)))
+    return d->cuda(e, "download");
+  if ((st = check_error_word(d)) != DGMX_OK) return st;
+  if (!pin_out) std::memcpy(F, d->host_pinned + n, sizeof(double) * n);
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_advance_async(dgmx_domain *d, double dt, int nsteps) {
+  if (!d || nsteps < 0) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(d->prm.device);
+  if (nsteps == 0) return DGMX_OK;
+  dgmx_status st;
+  if (d->prm.physics == DGMX_SHALLOW && d->prm.sw_balance && !d->sw_captured)
+    if ((st = capture_sw_source(d)) != DGMX_OK) return st;
+  // The trace buffers swap once per stage, so a graph holds two steps when a
+  // step has an odd stage count (TVD3) and the buffer parity repeats.  The
+  // graph is rebuilt when dt or the starting parity changes.
+  const int nst = stages_per_step(d->prm.inttype);
+  const int reps = (nst & 1) ? 2 : 1;
+  if (nsteps >= reps && (!d->graph || d->graph_dt != dt || d->graph_tcur != d->tcur)) {
+    if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+    const int t0 = d->tcur;
+    const long l0 = d->launches;
+    cudaGraph_t g;
+    cudaError_t e = cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return d->cuda(e, "graph capture");
+    st = DGMX_OK;
+    for (int r = 0; r < reps && st == DGMX_OK; ++r) st = enqueue_step(d, dt);
+    e = cudaStreamEndCapture(d->stream, &g);
+    d->tcur = t0;               // capture recorded the launches, ran nothing
+    d->launches = l0;
+    if (st != DGMX_OK) return st;
+    if (e != cudaSuccess) return d->cuda(e, "graph capture");
+    e = cudaGraphInstantiate(&d->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return d->cuda(e, "graph instantiate");
+    d->graph_dt = dt;
+    d->graph_tcur = t0;
+  }
+  int s = 0;
+  for (; d->graph && s + reps <= nsteps; s += reps) {
+    cudaError_t e = cudaGraphLaunch(d->graph, d->stream);
+    if (e != cudaSuccess) return d->cuda(e, "graph launch");
+    d->launches += (long)nst * reps;
+  }
+  for (; s < nsteps; ++s)
+    if ((st = enqueue_step(d, dt)) != DGMX_OK) return st;
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_sync(dgmx_domain *d) {
+  if (!d) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(d->prm.device);
+  dgmx_status st = check_error_word(d);
+  if (st != DGMX_OK) { reset_error_word(d); return st; }
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_advance(dgmx_domain *d, double dt, int nsteps) {
+  dgmx_status st = dgmx_advance_async(d, dt, nsteps);
+  if (st != DGMX_OK) return st;
+  return dgmx_sync(d);
+}
+
+dgmx_status dgmx_integrals(dgmx_domain *d, double *totals) {
+  if (!d || !totals) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(d->prm.device);
+  // integral of the orthonormal mode 0 over the reference element: 2^d/sqrt(2)^d
+  const double c = std::pow(std::sqrt(2.0), d->dim);
+  cudaError_t e = launch_integrals(d->nf, d->ne, d->ld, c, d->U, d->Jdev, d->integ, d->stream);
+  ++d->launches;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(totals, d->integ, sizeof(double) * d->nf, cudaMemcpyDeviceToHost, d->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+  return d->cuda(e, "integrals");
+}
+
+const char *dgmx_last_error(const dgmx_domain *d) {
+  return d ? d->errmsg.c_str() : g_create_error.c_str();
+}
+
+long dgmx_launch_count(const dgmx_domain *d) { return d ? d->launches : 0; }
+
+void *dgmx_stream(const dgmx_domain *d) { return d ? (void *)d->stream : nullptr; }
+
+// Kernel instantiations compiled into this library: rows of (physics, L, Q,
+// elements per CTA, threads per CTA, shared memory bytes).  Returns the row
+// count; writes at most cap rows.
+int dgmx_kernel_list(int *rows, int cap) {
+  std::vector<std::vector<int>> v;
+  list_ops(v);
+  for (int i = 0; i < (int)v.size() && i < cap; ++i)
+    for (int k = 0; k < 6; ++k) rows[i * 6 + k] = v[i][k];
+  return (int)v.size();
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------
+// Host-only inspection entry points (no CUDA calls): the 1-D tables and the
+// processed connectivity, so the setup can be checked on machines without a
+// GPU.
+extern "C" {
+
+dgmx_status dgmx_tables(int L, int Q, double *z, double *w, double *D, double *B, double *Bg, double *gl2g,
+                        double *g2gl) {
+  if (L < 1 || Q < 2 || !z || !w || !D || !B || !Bg || !gl2g || !g2gl) return DGMX_ERR_ARGUMENT;
+  const Tables1D t = make_tables(L, Q, Q - 1);
+  std::memcpy(z, t.z.data(), sizeof(double) * Q);
+  std::memcpy(w, t.w.data(), sizeof(double) * Q);
+  std::memcpy(D, t.D.data(), sizeof(double) * Q * Q);
+  std::memcpy(B, t.B.data(), sizeof(double) * L * Q);
+  std::memcpy(Bg, t.Bg.data(), sizeof(double) * L * (Q - 1));
+  std::memcpy(gl2g, t.gl2g.data(), sizeof(double) * (Q - 1) * Q);
+  std::memcpy(g2gl, t.g2gl.data(), sizeof(double) * Q * (Q - 1));
+  return DGMX_OK;
+}
+
+// links: ne*nfaces*4 ints (neighbour, neighbour face, master flag, class id);
+// perm_pairs: ne*nfaces*gf ints, the neighbour's point index for each own
+// face point.  Uses mesh->porder[0]/qorder[0].
+dgmx_status dgmx_mesh_links(const dgmx_mesh *m, int *links, int *perm_pairs) {
+  if (!m || !links || !perm_pairs || !m->porder) return DGMX_ERR_ARGUMENT;
+  try {
+    const int p = m->porder[0], q = (m->qorder && m->qorder[0]) ? m->qorder[0] : p + 2;
+    const Tables1D t = make_tables(p + 1, q, q - 1);
+    HostMesh hm;
+    std::string err;
+    if (!build_mesh(*m, t, hm, err)) { g_create_error = err; return DGMX_ERR_ARGUMENT; }
+    for (int e = 0; e < hm.ne; ++e)
+      for (int f = 0; f < hm.nfaces; ++f) {
+        const FaceLink &l = hm.links[(size_t)e * hm.nfaces + f];
+        const GeomClass &c = hm.classes[hm.gclass[e]];
+        int *o = links + ((size_t)e * hm.nfaces + f) * 4;
+        o[0] = l.elem; o[1] = l.face; o[2] = (c.master >> f) & 1; o[3] = hm.gclass[e];
+        for (int g = 0; g < hm.gf; ++g) perm_pairs[((size_t)e * hm.nfaces + f) * hm.gf + g] = hm.perm[l.perm + g];
+      }
+    return DGMX_OK;
+  } catch (const std::exception &ex) {
+    g_create_error = ex.what();
+    return DGMX_ERR_ARGUMENT;
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,140 @@
+// Internal declarations shared by the host setup (C++) and the kernels (CUDA).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/dgmx.h"
+
+namespace dgmx {
+
+// ------------------------------------------------------------------ tables
+struct Tables1D {
+  int L = 0, Q = 0, G = 0;
+  std::vector<double> z, w, zg, wg;
+  std::vector<double> D;      // Q x Q, D[i*Q+j] = l_j'(z_i)
+  std::vector<double> B;      // L x Q orthonormal Legendre on GLL, B[a*Q+i]
+  std::vector<double> Bg;     // L x G orthonormal Legendre on Gauss, Bg[a*G+g]
+  std::vector<double> gl2g;   // G x Q
+  std::vector<double> g2gl;   // Q x G
+};
+Tables1D make_tables(int L, int Q, int G);
+void gll_points(int Q, double *z, double *w);
+void gauss_points(int G, double *z, double *w);
+
+// ------------------------------------------------------------ mesh / geometry
+// Geometry shared by all elements of one class (affine elements with equal
+// metrics, face normals, Jacobian ratios and master pattern).
+struct GeomClass {
+  double metric[9];     // rx ry rz sx sy sz tx ty tz (2-D: rx ry 0 sx sy 0 ...)
+  double J;             // element Jacobian
+  double nrm[6][3];     // unit normal of face f in the frame of its master side
+  double jr[6];         // side Jacobian / element Jacobian on this element's side
+  int master;           // bit f set: this element owns (is master of) face f
+  int pad;
+};
+
+struct FaceLink {
+  int elem;             // neighbour element
+  int face;             // neighbour's face id
+  int perm;             // offset of the point permutation in the perm table
+  int pad;
+};
+
+struct HostMesh {
+  int dim = 0, ne = 0, p = 0, L = 0, Q = 0, G = 0, nfaces = 0, gf = 0;
+  std::vector<double> cx, cy, cz;    // GLL coordinates, Field layout
+  std::vector<double> J;             // per element Jacobian
+  std::vector<int> gclass;           // per element geometry class
+  std::vector<GeomClass> classes;
+  std::vector<FaceLink> links;       // ne * nfaces
+  std::vector<int> perm;             // concatenated permutations (gf each)
+};
+
+// Processes a DGM mesh: connectivity masters (src/Field.cpp:3478-3540),
+// orientation flags (src/Field.cpp:416-680), affine geometry
+// (src/Quad.cpp:1227-1285, src/Hex.cpp:1130-1280) and side geometry
+// (src/Quad.cpp:1367-1455, src/Hex.cpp:1385-1497).
+bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::string &err);
+
+// DGM input files (.inp/.msh/.con/.ord)
+struct FileCase {
+  int dim = 0, ne = 0;
+  std::vector<double> verts;
+  std::vector<int> con, porder, qorder;
+  int eqntype = -1, inttype = -1, p = -1, q = 0;
+  double gamma = -1, vis = -1, Pr = -1;
+  std::string flux;
+};
+bool read_case_files(const std::string &root, FileCase &fc, std::string &err);
+
+// ------------------------------------------------------------------ kernels
+// Integrator stage kinds.  X is the register the RHS is evaluated on.
+enum StageKind : int {
+  kLSRK = 0,      // X=U : Ut = A Ut - dt R; U = B Ut + U
+  kTVD0 = 1,      // X=U : Ut = -dt R + U
+  kTVD1 = 2,      // X=Ut: T = -dt R + Ut; Ut = b T; Ut = a U + Ut
+  kTVD2 = 3,      // X=Ut: T = -dt R + Ut; U = a U; U = b T + U
+  kRK40 = 4,      // X=U : Ut = c0 R + U; A = c1 R
+  kRK41 = 5,      // X=Ut: Ut = c0 R + U; A = c1 R + A
+  kRK43 = 6,      // X=Ut: A = c1 R + A; U = c0 A + U
+  kRHS = 7,       // X   : A = R (no update)
+};
+
+struct StageArgs {
+  // registers, element-major modal layout [e][field][L^d]
+  const double *X;        // state the RHS is evaluated on
+  double *U, *Ut, *A;     // solution, second register, RK4 accumulator
+  const double *Tin;      // traces of X, [e][face][field][gf]
+  double *Tout;           // traces of the next stage's X
+  int kind;
+  double c0, c1, c2;      // stage coefficients (see StageKind)
+  double dt;
+  // nodal I/O (Domain::time_derivative path), Field layout [field][e][Q^d]
+  const double *Xn;
+  double *Fn;
+  // mesh
+  const int *gclass;
+  const GeomClass *classes;
+  const FaceLink *links;
+  const int *perm;
+  int ne;
+  double gamma, vis, Pr;
+  int flux;
+  int *err;               // err[0] bit 0: non-physical state; err[1]: min element
+  // shallow-water balance (REO_SHALLOW_ENFORCE_BALANCE, src/Shallow.cpp:251-267)
+  double *Rcap;           // if set, the projected RHS is stored here (modal)
+  const double *Rsub;     // if set, subtracted from the projected RHS
+};
+
+// Launchers for one (physics, L, Q) instantiation; all enqueue on stream s.
+struct KernelOps {
+  int epb = 0, nt = 0;
+  size_t smem = 0;
+  cudaError_t (*init)(const Tables1D &t) = nullptr;   // tables + smem attributes, current device
+  cudaError_t (*stage)(const StageArgs &a, cudaStream_t s) = nullptr;
+  cudaError_t (*traces_modal)(const StageArgs &a, const double *Xm, double *T, cudaStream_t s) = nullptr;
+  cudaError_t (*traces_nodal)(const StageArgs &a, cudaStream_t s) = nullptr;
+  cudaError_t (*rhs_nodal)(const StageArgs &a, cudaStream_t s) = nullptr;
+  cudaError_t (*forward)(const StageArgs &a, const double *Un, double *Um, cudaStream_t s) = nullptr;
+  cudaError_t (*backward)(const StageArgs &a, const double *Um, double *Un, cudaStream_t s) = nullptr;
+};
+void register_ops(int physics, int L, int Q, const KernelOps &ops);
+const KernelOps *find_ops(int physics, int L, int Q);
+void list_ops(std::vector<std::vector<int>> &out);
+
+// Field integrals from modal register mode 0: out[n] = sum_e J_e c_d Um[e][n][0].
+cudaError_t launch_integrals(int nf, int ne, int ld, double c_d, const double *Um, const double *J,
+                             double *out, cudaStream_t s);
+
+inline int nfields_of(int physics) {
+  return physics == DGMX_SHALLOW ? 3 : (physics == DGMX_EULER3D || physics == DGMX_NS3D ? 5 : 4);
+}
+inline int dim_of(int physics) {
+  return (physics == DGMX_EULER3D || physics == DGMX_NS3D) ? 3 : 2;
+}
+
+}  // namespace dgmx

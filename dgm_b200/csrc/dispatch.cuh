@@ -1,0 +1,83 @@
+// Launchers for one kernel instantiation and the registry hook used by the
+// per-physics compilation units (k_*.cu).
+#pragma once
+
+#include "stage.cuh"
+
+namespace dgmx {
+
+template <int L, int Q>
+cudaError_t upload_tables_lq(const Tables1D &t) {
+  cudaError_t e;
+  if ((e = cudaMemcpyToSymbol(cB<L, Q>, t.B.data(), sizeof(double) * L * Q)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(cBg<L, Q>, t.Bg.data(), sizeof(double) * L * (Q - 1))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(cD<L, Q>, t.D.data(), sizeof(double) * Q * Q)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(cG2GL<L, Q>, t.g2gl.data(), sizeof(double) * Q * (Q - 1))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(cGL2G<L, Q>, t.gl2g.data(), sizeof(double) * (Q - 1) * Q)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(cW<L, Q>, t.w.data(), sizeof(double) * Q)) != cudaSuccess) return e;
+  double end[2 * L];
+  for (int a = 0; a < L; ++a) { end[a] = t.B[a * Q + 0]; end[L + a] = t.B[a * Q + Q - 1]; }
+  return cudaMemcpyToSymbol(cEnd<L, Q>, end, sizeof(end));
+}
+
+template <int PHYS, int L, int Q, int EPB>
+struct Launch {
+  using C = Cfg<PHYS, L, Q, EPB>;
+  static dim3 grid(int ne) { return dim3((unsigned)((ne + EPB - 1) / EPB)); }
+  static cudaError_t init(const Tables1D &t) {
+    cudaError_t e = upload_tables_lq<L, Q>(t);
+    if (e != cudaSuccess) return e;
+    const int sm = (int)C::SMEM;
+    if ((e = cudaFuncSetAttribute(stage_kernel<C, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+    if ((e = cudaFuncSetAttribute(traces_modal_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+    if ((e = cudaFuncSetAttribute(traces_nodal_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+    if ((e = cudaFuncSetAttribute(rhs_nodal_kernel<C, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+    if ((e = cudaFuncSetAttribute(forward_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+    return cudaFuncSetAttribute(backward_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  }
+  static cudaError_t stage(const StageArgs &a, cudaStream_t s) {
+    stage_kernel<C, PHYS><<<grid(a.ne), C::NT, C::SMEM, s>>>(a);
+    return cudaGetLastError();
+  }
+  static cudaError_t traces_modal(const StageArgs &a, const double *X, double *T, cudaStream_t s) {
+    traces_modal_kernel<C><<<grid(a.ne), C::NT, C::SMEM, s>>>(a, X, T);
+    return cudaGetLastError();
+  }
+  static cudaError_t traces_nodal(const StageArgs &a, cudaStream_t s) {
+    traces_nodal_kernel<C><<<grid(a.ne), C::NT, C::SMEM, s>>>(a);
+    return cudaGetLastError();
+  }
+  static cudaError_t rhs_nodal(const StageArgs &a, cudaStream_t s) {
+    rhs_nodal_kernel<C, PHYS><<<grid(a.ne), C::NT, C::SMEM, s>>>(a);
+    return cudaGetLastError();
+  }
+  static cudaError_t forward(const StageArgs &a, const double *Un, double *Um, cudaStream_t s) {
+    forward_kernel<C><<<grid(a.ne), C::NT, C::SMEM, s>>>(a, Un, Um);
+    return cudaGetLastError();
+  }
+  static cudaError_t backward(const StageArgs &a, const double *Um, double *Un, cudaStream_t s) {
+    backward_kernel<C><<<grid(a.ne), C::NT, C::SMEM, s>>>(a, Um, Un);
+    return cudaGetLastError();
+  }
+  static KernelOps ops() {
+    KernelOps o;
+    o.epb = EPB; o.nt = C::NT; o.smem = C::SMEM;
+    o.init = init; o.stage = stage; o.traces_modal = traces_modal; o.traces_nodal = traces_nodal;
+    o.rhs_nodal = rhs_nodal; o.forward = forward; o.backward = backward;
+    return o;
+  }
+};
+
+// Elements per CTA: pack small elements so a CTA has >= ~128 threads.
+constexpr int default_epb(int dim, int Q) {
+  return dim == 3 ? (Q * Q * Q >= 100 ? 1 : (Q * Q * Q >= 50 ? 2 : 4))
+                  : (Q * Q >= 100 ? 1 : (128 / (Q * Q) > 8 ? 8 : 128 / (Q * Q)));
+}
+
+template <int PHYS, int P, int Q>
+void reg() {
+  constexpr int EPB = default_epb(phys_dim(PHYS), Q);
+  register_ops(PHYS, P + 1, Q, Launch<PHYS, P + 1, Q, EPB>::ops());
+}
+
+}  // namespace dgmx

@@ -1,0 +1,15 @@
+// Euler 3-D kernel instantiations (Hex, FP64), p = 1..7, q = p+2 (and p+1).
+#include "dispatch.cuh"
+
+namespace dgmx {
+namespace {
+struct RegEuler3D {
+  RegEuler3D() {
+    reg<DGMX_EULER3D, 1, 3>();
+#define R(P) reg<DGMX_EULER3D, P, P + 1>(); reg<DGMX_EULER3D, P, P + 2>();
+    R(2) R(3) R(4) R(5) R(6) R(7)
+#undef R
+  }
+} reg_euler3d;
+}  // namespace
+}  // namespace dgmx

@@ -1,0 +1,290 @@
+// Device building blocks of the B200 DG engine: constant tables, the
+// sum-factorised axis contraction, and the pointwise physics (volume fluxes
+// and numerical face fluxes).  Included by the per-physics kernel units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "dgmx_internal.hpp"
+
+namespace dgmx {
+
+template <int B, int E>
+struct Pow { static constexpr int v = B * Pow<B, E - 1>::v; };
+template <int B>
+struct Pow<B, 0> { static constexpr int v = 1; };
+
+// 1-D tables for one (L, Q) pair in constant memory.  With the contraction
+// loops fully unrolled the indices are compile-time constants, so the
+// coefficients become constant-bank operands of the FMAs.
+template <int L, int Q> __constant__ double cB[L * Q];          // B[a*Q+i]
+template <int L, int Q> __constant__ double cBg[L * (Q - 1)];   // Bg[a*G+g]
+template <int L, int Q> __constant__ double cD[Q * Q];          // D[i*Q+m]
+template <int L, int Q> __constant__ double cG2GL[Q * (Q - 1)]; // [i*G+g]
+template <int L, int Q> __constant__ double cGL2G[(Q - 1) * Q]; // [g*Q+i]
+template <int L, int Q> __constant__ double cW[Q];              // GLL weights
+template <int L, int Q> __constant__ double cEnd[2 * L];        // B[a][0], B[a][Q-1]
+
+// Matrix accessors: M::get(in_index, out_index)
+template <int L, int Q> struct MatB   { static __device__ __forceinline__ double get(int a, int i) { return cB<L, Q>[a * Q + i]; } };
+template <int L, int Q> struct MatBt  { static __device__ __forceinline__ double get(int i, int a) { return cB<L, Q>[a * Q + i]; } };
+template <int L, int Q> struct MatBg  { static __device__ __forceinline__ double get(int a, int g) { return cBg<L, Q>[a * (Q - 1) + g]; } };
+template <int L, int Q> struct MatD   { static __device__ __forceinline__ double get(int m, int i) { return cD<L, Q>[i * Q + m]; } };
+template <int L, int Q> struct MatG2GL{ static __device__ __forceinline__ double get(int g, int i) { return cG2GL<L, Q>[i * (Q - 1) + g]; } };
+template <int L, int Q> struct MatGL2G{ static __device__ __forceinline__ double get(int i, int g) { return cGL2G<L, Q>[g * Q + i]; } };
+
+// Contraction along axis AX of a batch of 3-D arrays (I0, I1, I2) with
+// I_AX = K: out[...n...] = sum_k M(k, n) in[...k...], N outputs per pencil.
+// Each thread owns one pencil: K loads, K*N FMAs with uniform coefficients.
+// Batch b reads in + b*sin and writes out + b*sout.
+template <int I0, int I1, int I2, int AX, int K, int N, class M, bool ACC>
+__device__ __forceinline__ void contract(const double *__restrict__ in, double *__restrict__ out, int nbatch,
+                                         int sin, int sout, int tid, int nthr) {
+  constexpr int O1 = AX == 1 ? N : I1, O2 = AX == 2 ? N : I2;
+  constexpr int P0 = AX == 0 ? I1 : I0;
+  constexpr int P1 = AX == 2 ? I1 : I2;
+  constexpr int NP = P0 * P1;
+  constexpr int is0 = I1 * I2, is1 = I2;
+  constexpr int os0 = O1 * O2, os1 = O2;
+  constexpr int isA = AX == 0 ? is0 : (AX == 1 ? is1 : 1);
+  constexpr int osA = AX == 0 ? os0 : (AX == 1 ? os1 : 1);
+  for (int w = tid; w < nbatch * NP; w += nthr) {
+    const int b = w / NP, p = w - b * NP;
+    const int pa = p / P1, pb = p - pa * P1;
+    int io, oo;
+    if (AX == 0) { io = pa * is1 + pb; oo = pa * os1 + pb; }
+    else if (AX == 1) { io = pa * is0 + pb; oo = pa * os0 + pb; }
+    else { io = pa * is0 + pb * is1; oo = pa * os0 + pb * os1; }
+    const double *src = in + (size_t)b * sin + io;
+    double *dst = out + (size_t)b * sout + oo;
+    double v[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = src[k * isA];
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+      double acc = 0.0;
+#pragma unroll
+      for (int k = 0; k < K; ++k) acc = fma(M::get(k, n), v[k], acc);
+      if (ACC) dst[n * osA] += acc; else dst[n * osA] = acc;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ physics
+// Positivity threshold aepsM = eps^(2/3) (src/Constants.hpp:43).
+__device__ constexpr double kAeps = 4.8148248609680896e-11;
+
+// Physical flux components for one point.  Operation order follows the
+// reference volume loops (src/Euler.cpp:335-384, src/Euler3d.cpp:506-566,
+// src/Shallow.cpp:305-339).  Fills F[d][n] for d < DIM.
+template <int PHYS>
+__device__ __forceinline__ void volume_flux(const double *U, double gamma, double (*F)[5]) {
+  if constexpr (PHYS == DGMX_EULER2D || PHYS == DGMX_NS2D) {
+    const double gm1 = gamma - 1.0, m5g = -0.5 * gm1;
+    const double r = U[0], ru = U[1], rv = U[2], rE = U[3];
+    const double u = ru / r, v = rv / r;
+    double p = u * ru;
+    p = v * rv + p;
+    p = m5g * p;
+    p = fma(gm1, rE, p);
+    F[0][0] = ru;            F[1][0] = rv;
+    F[0][1] = ru * u + p;    F[1][1] = ru * v;
+    F[0][2] = rv * u;        F[1][2] = rv * v + p;
+    const double e = rE + p;
+    F[0][3] = u * e;         F[1][3] = v * e;
+  } else if constexpr (PHYS == DGMX_EULER3D || PHYS == DGMX_NS3D) {
+    const double gm1 = gamma - 1.0, m5g = -0.5 * gm1;
+    const double r = U[0], ru = U[1], rv = U[2], rw = U[3], rE = U[4];
+    const double u = ru / r, v = rv / r, w = rw / r;
+    double p = u * ru;
+    p = fma(v, rv, p);
+    p = fma(w, rw, p);
+    p = m5g * p;
+    p = fma(gm1, rE, p);
+    F[0][0] = ru; F[1][0] = rv; F[2][0] = rw;
+    F[0][1] = fma(ru, u, p); F[1][1] = ru * v;        F[2][1] = ru * w;
+    F[0][2] = rv * u;        F[1][2] = fma(rv, v, p); F[2][2] = rv * w;
+    F[0][3] = rw * u;        F[1][3] = rw * v;        F[2][3] = fma(rw, w, p);
+    const double e = rE + p;
+    F[0][4] = u * e; F[1][4] = v * e; F[2][4] = w * e;
+  } else {  // shallow water, geopotential form
+    const double phi = U[0], uphi = U[1], vphi = U[2];
+    const double u = uphi / phi, v = vphi / phi;
+    const double p = 0.5 * (phi * phi);
+    F[0][0] = uphi;            F[1][0] = vphi;
+    F[0][1] = fma(uphi, u, p); F[1][1] = uphi * v;
+    F[0][2] = vphi * u;        F[1][2] = fma(vphi, v, p);
+  }
+}
+
+// Numerical flux on one face point in the frame of the master side:
+// UL = master state, UR = slave state, n = master outward normal.
+// Outputs Fh (numerical flux), FL = F(UL).n, FR = F(UR).n.
+// Returns false if density or pressure is below aepsM.
+// Euler 2-D: src/Euler.cpp:443-741 (LF and Roe); Euler 3-D:
+// src/Euler3d.cpp:601-816 (LF) plus the rotated-frame Roe extension;
+// shallow water: src/Shallow.cpp:380-510.
+template <int PHYS>
+__device__ __forceinline__ bool face_flux(const double *UL, const double *UR, const double *n, double gamma,
+                                          int flux, double *Fh, double *FL, double *FR) {
+  bool ok = true;
+  if constexpr (PHYS == DGMX_EULER2D || PHYS == DGMX_NS2D) {
+    const double gm1 = gamma - 1.0;
+    const double nx = n[0], ny = n[1];
+    const double rl = UL[0], rul = UL[1] * nx + UL[2] * ny, rvl = UL[2] * nx - UL[1] * ny, rEl = UL[3];
+    const double irl = 1.0 / rl, ul = irl * rul, vl = irl * rvl;
+    const double pl = gm1 * (rEl - 0.5 * (rul * ul + rvl * vl));
+    const double Hl = irl * (rEl + pl);
+    ok = ok && rl >= kAeps && pl >= kAeps;
+    FL[0] = rul;
+    FL[1] = (rul * ul + pl) * nx - (rvl * ul) * ny;
+    FL[2] = (rul * ul + pl) * ny + (rvl * ul) * nx;
+    FL[3] = ul * (rEl + pl);
+    const double rr = UR[0], rur = UR[1] * nx + UR[2] * ny, rvr = UR[2] * nx - UR[1] * ny, rEr = UR[3];
+    const double irr = 1.0 / rr, ur = irr * rur, vr = irr * rvr;
+    const double pr = gm1 * (rEr - 0.5 * (rur * ur + rvr * vr));
+    const double Hr = irr * (rEr + pr);
+    ok = ok && rr >= kAeps && pr >= kAeps;
+    FR[0] = rr * ur;
+    FR[1] = (rur * ur + pr) * nx - (rvr * ur) * ny;
+    FR[2] = (rur * ur + pr) * ny + (rvr * ur) * nx;
+    FR[3] = ur * (rEr + pr);
+    if (flux == DGMX_FLUX_ROE) {
+      const double R = sqrt(rr / rl), iRp1 = 1.0 / (1.0 + R);
+      const double u = (ul + R * ur) * iRp1, v = (vl + R * vr) * iRp1, H = (Hl + R * Hr) * iRp1;
+      const double a = sqrt(gm1 * (H - 0.5 * (u * u + v * v)));
+      const double ainv = 1.0 / a, c1inv = 1.0 / (gm1 * ainv * ainv);
+      double al[4], G[4];
+      al[2] = (rvr - rvl) - v * (rr - rl);
+      al[1] = gm1 * ainv * ainv * ((rr - rl) * (H - u * u) + u * (rur - rul) -
+                                   ((rEr - rEl) - ((rvr - rvl) - v * (rr - rl)) * v));
+      al[0] = 0.5 * ainv * ((rr - rl) * (u + a) - (rur - rul) - a * al[1]);
+      al[3] = (rr - rl) - (al[0] + al[1]);
+      const double l0 = fmin(u - a, 0.0), l1 = fmin(u, 0.0), l3 = fmin(u + a, 0.0);
+      G[0] = l0 * al[0]; G[1] = l0 * (u - a) * al[0]; G[2] = l0 * v * al[0]; G[3] = l0 * (H - u * a) * al[0];
+      G[0] += l1 * al[1]; G[1] += l1 * u * al[1]; G[2] += l1 * v * al[1]; G[3] += l1 * (H - c1inv) * al[1];
+      G[2] += l1 * al[2]; G[3] += l1 * v * al[2];
+      G[0] += l3 * al[3]; G[1] += l3 * (u + a) * al[3]; G[2] += l3 * v * al[3]; G[3] += l3 * (H + u * a) * al[3];
+      Fh[0] = FL[0] + G[0];
+      Fh[1] = FL[1] + G[1] * nx - G[2] * ny;
+      Fh[2] = FL[2] + G[1] * ny + G[2] * nx;
+      Fh[3] = FL[3] + G[3];
+    } else {
+      const double al = sqrt(gm1 * (Hl - 0.5 * (ul * ul + vl * vl)));
+      const double ar = sqrt(gm1 * (Hr - 0.5 * (ur * ur + vr * vr)));
+      double lmax = fmax(fabs(ul - al), fabs(ul));
+      lmax = fmax(lmax, fabs(ul + al));
+      lmax = fmax(lmax, fmax(fabs(ur - ar), fabs(ur)));
+      lmax = fmax(lmax, fabs(ur + ar));
+#pragma unroll
+      for (int k = 0; k < 4; ++k) Fh[k] = 0.5 * (FL[k] + FR[k] + lmax * (UL[k] - UR[k]));
+    }
+  } else if constexpr (PHYS == DGMX_EULER3D || PHYS == DGMX_NS3D) {
+    const double gm1 = gamma - 1.0;
+    const double nx = n[0], ny = n[1], nz = n[2];
+    double sx = ny, sy = nz, sz = nx;
+    const double sdn = nx * sx + ny * sy + nz * sz;
+    sx -= sdn * nx; sy -= sdn * ny; sz -= sdn * nz;
+    const double sni = 1.0 / sqrt(sx * sx + sy * sy + sz * sz);
+    sx *= sni; sy *= sni; sz *= sni;
+    double tx = ny * sz - sy * nz, ty = nz * sx - sz * nx, tz = nx * sy - sx * ny;
+    const double tni = 1.0 / sqrt(tx * tx + ty * ty + tz * tz);
+    tx *= tni; ty *= tni; tz *= tni;
+    const double detA = (nx * sy * tz + sx * ty * nz + tx * sz * ny) - (nz * sy * tx + sz * ty * nx + tz * sx * ny);
+    const double id = 1.0 / detA;
+    const double xn = (sy * tz - sz * ty) * id, yn = -(sx * tz - sz * tx) * id, zn = (sx * ty - sy * tx) * id;
+    const double xs = -(ny * tz - nz * ty) * id, ys = (nx * tz - nz * tx) * id, zs = -(nx * ty - ny * tx) * id;
+    const double xt = (ny * sz - nz * sy) * id, yt = -(nx * sz - nz * sx) * id, zt = (nx * sy - ny * sx) * id;
+    const double rl = UL[0];
+    const double rul = UL[1] * nx + UL[2] * ny + UL[3] * nz;
+    const double rvl = UL[1] * sx + UL[2] * sy + UL[3] * sz;
+    const double rwl = UL[1] * tx + UL[2] * ty + UL[3] * tz;
+    const double rEl = UL[4];
+    const double irl = 1.0 / rl, ul = irl * rul, vl = irl * rvl, wl = irl * rwl;
+    const double pl = gm1 * (rEl - 0.5 * (rul * ul + rvl * vl + rwl * wl));
+    const double Hl = irl * (rEl + pl);
+    ok = ok && rl >= kAeps && pl >= kAeps;
+    FL[0] = rl * ul;
+    FL[1] = (rul * ul + pl) * xn + (rvl * ul) * xs + (rwl * ul) * xt;
+    FL[2] = (rul * ul + pl) * yn + (rvl * ul) * ys + (rwl * ul) * yt;
+    FL[3] = (rul * ul + pl) * zn + (rvl * ul) * zs + (rwl * ul) * zt;
+    FL[4] = ul * (rEl + pl);
+    const double rr = UR[0];
+    const double rur = UR[1] * nx + UR[2] * ny + UR[3] * nz;
+    const double rvr = UR[1] * sx + UR[2] * sy + UR[3] * sz;
+    const double rwr = UR[1] * tx + UR[2] * ty + UR[3] * tz;
+    const double rEr = UR[4];
+    const double irr = 1.0 / rr, ur = irr * rur, vr = irr * rvr, wr = irr * rwr;
+    const double pr = gm1 * (rEr - 0.5 * (rur * ur + rvr * vr + rwr * wr));
+    const double Hr = irr * (rEr + pr);
+    ok = ok && rr >= kAeps && pr >= kAeps;
+    FR[0] = rr * ur;
+    FR[1] = (rur * ur + pr) * xn + (rvr * ur) * xs + (rwr * ur) * xt;
+    FR[2] = (rur * ur + pr) * yn + (rvr * ur) * ys + (rwr * ur) * yt;
+    FR[3] = (rur * ur + pr) * zn + (rvr * ur) * zs + (rwr * ur) * zt;
+    FR[4] = ur * (rEr + pr);
+    if (flux == DGMX_FLUX_ROE) {
+      // Roe average in the (n, s, t) frame; the 2-D Roe of src/Euler.cpp
+      // with a second tangential velocity carried like the first.
+      const double R = sqrt(rr / rl), iRp1 = 1.0 / (1.0 + R);
+      const double u = (ul + R * ur) * iRp1, v = (vl + R * vr) * iRp1, w = (wl + R * wr) * iRp1;
+      const double H = (Hl + R * Hr) * iRp1;
+      const double a2 = gm1 * (H - 0.5 * (u * u + v * v + w * w));
+      const double a = sqrt(a2), ainv = 1.0 / a, c1inv = a2 / gm1;
+      const double dr = rr - rl, dru = rur - rul, drv = rvr - rvl, drw = rwr - rwl, drE = rEr - rEl;
+      double al[5], G[5];
+      al[2] = drv - v * dr;
+      al[3] = drw - w * dr;
+      al[1] = gm1 * ainv * ainv * (dr * (H - u * u) + u * dru - ((drE - al[2] * v - al[3] * w)));
+      al[0] = 0.5 * ainv * (dr * (u + a) - dru - a * al[1]);
+      al[4] = dr - (al[0] + al[1]);
+      const double l0 = fmin(u - a, 0.0), l1 = fmin(u, 0.0), l4 = fmin(u + a, 0.0);
+      G[0] = l0 * al[0]; G[1] = l0 * (u - a) * al[0]; G[2] = l0 * v * al[0]; G[3] = l0 * w * al[0];
+      G[4] = l0 * (H - u * a) * al[0];
+      G[0] += l1 * al[1]; G[1] += l1 * u * al[1]; G[2] += l1 * v * al[1]; G[3] += l1 * w * al[1];
+      G[4] += l1 * (H - c1inv) * al[1];
+      G[2] += l1 * al[2]; G[4] += l1 * v * al[2];
+      G[3] += l1 * al[3]; G[4] += l1 * w * al[3];
+      G[0] += l4 * al[4]; G[1] += l4 * (u + a) * al[4]; G[2] += l4 * v * al[4]; G[3] += l4 * w * al[4];
+      G[4] += l4 * (H + u * a) * al[4];
+      Fh[0] = FL[0] + G[0];
+      Fh[1] = FL[1] + G[1] * xn + G[2] * xs + G[3] * xt;
+      Fh[2] = FL[2] + G[1] * yn + G[2] * ys + G[3] * yt;
+      Fh[3] = FL[3] + G[1] * zn + G[2] * zs + G[3] * zt;
+      Fh[4] = FL[4] + G[4];
+    } else {
+      const double al = sqrt(gm1 * (Hl - 0.5 * (ul * ul + vl * vl + wl * wl)));
+      const double ar = sqrt(gm1 * (Hr - 0.5 * (ur * ur + vr * vr + wr * wr)));
+      double lmax = fmax(fabs(ul - al), fabs(ul));
+      lmax = fmax(lmax, fabs(ul + al));
+      lmax = fmax(lmax, fmax(fabs(ur - ar), fabs(ur)));
+      lmax = fmax(lmax, fabs(ur + ar));
+#pragma unroll
+      for (int k = 0; k < 5; ++k) Fh[k] = 0.5 * (FL[k] + FR[k] + lmax * (UL[k] - UR[k]));
+    }
+  } else {  // shallow water LF
+    const double nx = n[0], ny = n[1];
+    const double phil = UL[0], upl = UL[1] * nx + UL[2] * ny, vpl = UL[2] * nx - UL[1] * ny;
+    const double ul = upl / phil, pl = 0.5 * phil * phil;
+    ok = ok && phil >= kAeps && pl >= kAeps;
+    FL[0] = upl;
+    FL[1] = (upl * ul + pl) * nx - (vpl * ul) * ny;
+    FL[2] = (upl * ul + pl) * ny + (vpl * ul) * nx;
+    const double phir = UR[0], upr = UR[1] * nx + UR[2] * ny, vpr = UR[2] * nx - UR[1] * ny;
+    const double ur = upr / phir, pr = 0.5 * phir * phir;
+    ok = ok && phir >= kAeps && pr >= kAeps;
+    FR[0] = upr;
+    FR[1] = (upr * ur + pr) * nx - (vpr * ur) * ny;
+    FR[2] = (upr * ur + pr) * ny + (vpr * ur) * nx;
+    const double al = sqrt(phil), ar = sqrt(phir);
+    double lmax = fmax(fabs(ul - al), fabs(ul));
+    lmax = fmax(lmax, fabs(ul + al));
+    lmax = fmax(lmax, fmax(fabs(ur - ar), fabs(ur)));
+    lmax = fmax(lmax, fabs(ur + ar));
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Fh[k] = 0.5 * (FL[k] + FR[k] + lmax * (UL[k] - UR[k]));
+  }
+  return ok;
+}
+
+}  // namespace dgmx

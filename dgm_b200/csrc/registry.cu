@@ -1,0 +1,62 @@
+// Kernel registry and small utility kernels.
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "dgmx_internal.hpp"
+
+namespace dgmx {
+namespace {
+std::map<std::tuple<int, int, int>, KernelOps> &table() {
+  static std::map<std::tuple<int, int, int>, KernelOps> t;
+  return t;
+}
+std::mutex &table_mutex() {
+  static std::mutex m;
+  return m;
+}
+}  // namespace
+
+void register_ops(int physics, int L, int Q, const KernelOps &ops) {
+  std::lock_guard<std::mutex> lk(table_mutex());
+  table()[std::make_tuple(physics, L, Q)] = ops;
+}
+
+const KernelOps *find_ops(int physics, int L, int Q) {
+  std::lock_guard<std::mutex> lk(table_mutex());
+  auto it = table().find(std::make_tuple(physics, L, Q));
+  return it == table().end() ? nullptr : &it->second;
+}
+
+void list_ops(std::vector<std::vector<int>> &out) {
+  std::lock_guard<std::mutex> lk(table_mutex());
+  for (auto &kv : table())
+    out.push_back({std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first), kv.second.epb,
+                   kv.second.nt, (int)kv.second.smem});
+}
+
+// out[n] = c_d * sum_e J_e Um[e][n][0]: the integral of field n (the
+// orthonormal mode 0 carries the element mean).  One block per field,
+// FP64 tree reduction.
+__global__ void integrals_kernel(int nf, int ne, int ld, double c_d, const double *Um, const double *J,
+                                 double *out) {
+  __shared__ double red[256];
+  const int n = blockIdx.x;
+  double acc = 0.0;
+  for (int e = threadIdx.x; e < ne; e += blockDim.x) acc += J[e] * Um[((size_t)e * nf + n) * ld];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[n] = c_d * red[0];
+}
+
+cudaError_t launch_integrals(int nf, int ne, int ld, double c_d, const double *Um, const double *J, double *out,
+                             cudaStream_t s) {
+  integrals_kernel<<<nf, 256, 0, s>>>(nf, ne, ld, c_d, Um, J, out);
+  return cudaGetLastError();
+}
+
+}  // namespace dgmx

@@ -1,0 +1,561 @@
+// Fused DG stage kernels for sm_100a (FP64).
+//
+// One launch evaluates Domain::time_derivative on a modal register and folds
+// the RK stage update and the next stage's face traces into the same pass:
+//   1. load the element's modal coefficients (element-major, one contiguous
+//      block per element)
+//   2. own face traces at the side Gauss points (modal -> Gauss, the
+//      polynomial equivalent of fill_sides' GL2G interpolation,
+//      src/Hex.cpp:933-947)
+//   3. backward transform to the GLL points (src/Hex.cpp:795-812)
+//   4. volume term: contravariant fluxes and collocation derivatives
+//      (algebraically Sum_dir d/dx_dir F_dir, src/Euler3d.cpp:506-566)
+//   5. numerical flux on every face point against the neighbour's traces
+//      from the previous stage (src/Euler3d.cpp:584-817)
+//   6. lift: G2GL interpolation and 1/w_end scaling onto the boundary GLL
+//      points (src/Hex.cpp:1768-1952)
+//   7. projection: w-weighted inner product with the orthonormal basis
+//      (the J of wJ cancels the 1/J mass, src/Hex.cpp:200-205, :652-685)
+//   8. RK stage update on the modal registers (src/TimeInt.cpp:266-302,
+//      :826-860, :1989-2013)
+//   9. traces of the updated register for the next stage
+// Traces are double buffered, so an element may overwrite its own register
+// in place: neighbours only ever read its traces.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace dgmx {
+
+constexpr int phys_dim(int p) { return (p == DGMX_EULER3D || p == DGMX_NS3D) ? 3 : 2; }
+constexpr int phys_nf(int p) { return p == DGMX_SHALLOW ? 3 : (phys_dim(p) == 3 ? 5 : 4); }
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+template <int PHYS, int L_, int Q_, int EPB_>
+struct Cfg {
+  static constexpr int DIM = phys_dim(PHYS), NF = phys_nf(PHYS);
+  static constexpr int L = L_, Q = Q_, G = Q_ - 1, EPB = EPB_;
+  static constexpr int NFACE = 2 * DIM;
+  static constexpr int LD = Pow<L, DIM>::v, QD = Pow<Q, DIM>::v;
+  static constexpr int GF = Pow<G, DIM - 1>::v, QF = Pow<Q, DIM - 1>::v, LF = Pow<L, DIM - 1>::v;
+  static constexpr int NT = cmax(64, ((EPB * QD + 31) / 32) * 32 > 1024 ? 1024 : ((EPB * QD + 31) / 32) * 32);
+  // per-slot region sizes (doubles)
+  static constexpr int SZ_A = NF * LD;                 // modal register
+  static constexpr int SZ_B = NF * QD;                 // GLL values
+  static constexpr int SZ_C = NF * QD;                 // flux / scratch
+  static constexpr int SZ_D = NF * QD;                 // divergence + lift
+  static constexpr int SZ_E = NFACE * NF * GF;         // face traces / lift input
+  static constexpr int SZ_R = NF * LD;                 // projected RHS (modal)
+  static constexpr int SZ_S = cmax(cmax(NF * Q * LF, NFACE * NF * LF), DIM == 3 ? NFACE * NF * Q * G : 0);
+  static constexpr int SZ_SLOT = SZ_A + SZ_B + SZ_C + SZ_D + SZ_E + SZ_R + SZ_S;
+  static constexpr size_t SMEM = (size_t)EPB * SZ_SLOT * sizeof(double) +
+                                 (size_t)EPB * (sizeof(GeomClass) + NFACE * sizeof(FaceLink) + 16);
+  static_assert(NFACE * QF <= 2 * QD, "lift face buffer must fit in the B+C regions");
+  static_assert(DIM == 2 || NFACE * G * L <= 2 * QD, "trace intermediate must fit in the B+C regions");
+  static_assert(SMEM <= 227 * 1024, "element slot does not fit in shared memory");
+};
+
+// Trailing-1 shapes so one contraction routine serves 2-D and 3-D.
+template <int DIM, int N> struct Sh3 { static constexpr int a = N, b = N, c = (DIM == 3 ? N : 1); };
+
+template <class K>
+struct Smem {
+  double *A, *B, *C, *D, *E, *R, *S;
+  GeomClass *geo;
+  FaceLink *lnk;
+  int *eid;
+  __device__ Smem(double *base) {
+    A = base;
+    B = A + K::EPB * K::SZ_A;
+    C = B + K::EPB * K::SZ_B;
+    D = C + K::EPB * K::SZ_C;
+    E = D + K::EPB * K::SZ_D;
+    R = E + K::EPB * K::SZ_E;
+    S = R + K::EPB * K::SZ_R;
+    geo = reinterpret_cast<GeomClass *>(S + K::EPB * K::SZ_S);
+    lnk = reinterpret_cast<FaceLink *>(geo + K::EPB);
+    eid = reinterpret_cast<int *>(lnk + K::EPB * K::NFACE);
+  }
+};
+
+// ---- face-local helpers ----------------------------------------------------
+// Face f: normal axis and end (0 = first GLL point, 1 = last).
+// 3-D: 0 k=0, 1 j=0, 2 i=Q-1, 3 j=Q-1, 4 i=0, 5 k=Q-1 (src/Hex.cpp:815-865)
+// 2-D: 0 j=0, 1 i=Q-1, 2 j=Q-1, 3 i=0 (src/Quad.cpp:767-790)
+template <int DIM> __device__ __host__ constexpr int face_axis(int f) {
+  return DIM == 3 ? (f == 0 || f == 5 ? 2 : (f == 1 || f == 3 ? 1 : 0)) : (f == 0 || f == 2 ? 1 : 0);
+}
+template <int DIM> __device__ __host__ constexpr int face_end(int f) {
+  return DIM == 3 ? (f == 2 || f == 3 || f == 5) : (f == 1 || f == 2);
+}
+
+template <int L, int Q, int END>
+struct MatEnd { static __device__ __forceinline__ double get(int a, int) { return cEnd<L, Q>[END * L + a]; } };
+
+// Endpoint reduction of one face for a batch of modal arrays (L^DIM each),
+// output face-local L^(DIM-1) arrays.
+template <class C, int F>
+__device__ __forceinline__ void face_reduce(const double *A, double *out, int tid, int nthr) {
+  constexpr int DIM = C::DIM, L = C::L, Q = C::Q;
+  constexpr int AX = face_axis<DIM>(F), END = face_end<DIM>(F);
+  using Sh = Sh3<DIM, L>;
+  contract<Sh::a, Sh::b, Sh::c, AX, L, 1, MatEnd<L, Q, END>, false>(A, out + F * C::EPB * C::NF * C::LF,
+                                                                     C::EPB * C::NF, C::LD, C::LF, tid, nthr);
+}
+
+// Traces at the side Gauss points of a modal register held in smem A.
+// Result in E, face-major [f][slot][n][gf].  Uses S and B+C as scratch.
+template <class C>
+__device__ __forceinline__ void modal_traces(const double *A, double *E, double *S, double *Cs, int tid, int nthr) {
+  constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G;
+  face_reduce<C, 0>(A, S, tid, nthr);
+  face_reduce<C, 1>(A, S, tid, nthr);
+  face_reduce<C, 2>(A, S, tid, nthr);
+  face_reduce<C, 3>(A, S, tid, nthr);
+  if constexpr (DIM == 3) {
+    face_reduce<C, 4>(A, S, tid, nthr);
+    face_reduce<C, 5>(A, S, tid, nthr);
+  }
+  __syncthreads();
+  constexpr int NB = C::NFACE * C::EPB * C::NF;
+  if constexpr (DIM == 3) {
+    contract<L, L, 1, 0, L, G, MatBg<L, Q>, false>(S, Cs, NB, L * L, G * L, tid, nthr);
+    __syncthreads();
+    contract<G, L, 1, 1, L, G, MatBg<L, Q>, false>(Cs, E, NB, G * L, G * G, tid, nthr);
+  } else {
+    contract<L, 1, 1, 0, L, G, MatBg<L, Q>, false>(S, E, NB, L, G, tid, nthr);
+  }
+  __syncthreads();
+}
+
+// Backward transform: modal A [slot][n][LD] -> GLL B [slot][n][QD].
+template <class C>
+__device__ __forceinline__ void backward(const double *A, double *B, double *S, double *Cs, int tid, int nthr) {
+  constexpr int L = C::L, Q = C::Q, NB = C::EPB * C::NF;
+  if constexpr (C::DIM == 3) {
+    contract<L, L, L, 0, L, Q, MatB<L, Q>, false>(A, S, NB, C::LD, Q * L * L, tid, nthr);
+    __syncthreads();
+    contract<Q, L, L, 1, L, Q, MatB<L, Q>, false>(S, Cs, NB, Q * L * L, Q * Q * L, tid, nthr);
+    __syncthreads();
+    contract<Q, Q, L, 2, L, Q, MatB<L, Q>, false>(Cs, B, NB, Q * Q * L, C::QD, tid, nthr);
+  } else {
+    contract<L, L, 1, 0, L, Q, MatB<L, Q>, false>(A, S, NB, C::LD, Q * L, tid, nthr);
+    __syncthreads();
+    contract<Q, L, 1, 1, L, Q, MatB<L, Q>, false>(S, B, NB, Q * L, C::QD, tid, nthr);
+  }
+  __syncthreads();
+}
+
+// Forward projection: GLL D [slot][n][QD] (already w-weighted) -> modal R.
+template <class C>
+__device__ __forceinline__ void forward(const double *D, double *R, double *Cs, double *Bs, int tid, int nthr) {
+  constexpr int L = C::L, Q = C::Q, NB = C::EPB * C::NF;
+  if constexpr (C::DIM == 3) {
+    contract<Q, Q, Q, 0, Q, L, MatBt<L, Q>, false>(D, Cs, NB, C::QD, L * Q * Q, tid, nthr);
+    __syncthreads();
+    contract<L, Q, Q, 1, Q, L, MatBt<L, Q>, false>(Cs, Bs, NB, L * Q * Q, L * L * Q, tid, nthr);
+    __syncthreads();
+    contract<L, L, Q, 2, Q, L, MatBt<L, Q>, false>(Bs, R, NB, L * L * Q, C::LD, tid, nthr);
+  } else {
+    contract<Q, Q, 1, 0, Q, L, MatBt<L, Q>, false>(D, Cs, NB, C::QD, L * Q, tid, nthr);
+    __syncthreads();
+    contract<L, Q, 1, 1, Q, L, MatBt<L, Q>, false>(Cs, R, NB, L * Q, C::LD, tid, nthr);
+  }
+  __syncthreads();
+}
+
+// Volume term: D = Sum_r d/dxi_r (metric_r . F(U)) for every field.
+// With at most one point per thread the physical fluxes stay in registers
+// across the DIM passes; otherwise they are re-evaluated per pass.
+template <class C, int PHYS>
+__device__ __forceinline__ void volume(const Smem<C> &sm, double gamma, int tid) {
+  constexpr int DIM = C::DIM, NF = C::NF, Q = C::Q, QD = C::QD, NB = C::EPB * C::NF;
+  constexpr bool ONE = C::EPB * QD <= C::NT;
+  double F[3][5];
+  if constexpr (ONE) {
+    if (tid < C::EPB * QD) {
+      const int slot = tid / QD, p = tid - slot * QD;
+      double U[5];
+#pragma unroll
+      for (int n = 0; n < NF; ++n) U[n] = sm.B[(slot * NF + n) * QD + p];
+      volume_flux<PHYS>(U, gamma, F);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < DIM; ++r) {
+    for (int w = tid; w < C::EPB * QD; w += C::NT) {
+      const int slot = w / QD, p = w - slot * QD;
+      if constexpr (!ONE) {
+        double U[5];
+#pragma unroll
+        for (int n = 0; n < NF; ++n) U[n] = sm.B[(slot * NF + n) * QD + p];
+        volume_flux<PHYS>(U, gamma, F);
+      }
+      const double *met = sm.geo[slot].metric;
+#pragma unroll
+      for (int n = 0; n < NF; ++n) {
+        double g = met[3 * r + 0] * F[0][n];
+        g = fma(met[3 * r + 1], F[1][n], g);
+        if (DIM == 3) g = fma(met[3 * r + 2], F[2][n], g);
+        sm.C[(slot * NF + n) * QD + p] = g;
+      }
+    }
+    __syncthreads();
+    using Sh = Sh3<DIM, Q>;
+    if (r == 0) contract<Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<C::L, Q>, false>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
+    else if (r == 1) contract<Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<C::L, Q>, true>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
+    else contract<Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<C::L, Q>, true>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
+    __syncthreads();
+  }
+}
+
+// Numerical flux on all face points; E holds own traces on entry and
+// (F^ - F).J on exit.  Neighbour traces come from Tin.
+template <class C, int PHYS>
+__device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &a, int tid) {
+  constexpr int NF = C::NF, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
+  for (int w = tid; w < NFACE * EPB * GF; w += C::NT) {
+    const int f = w / (EPB * GF), rem = w - f * EPB * GF, slot = rem / GF, g = rem - slot * GF;
+    const int e = sm.eid[slot];
+    if (e < 0) continue;
+    const FaceLink lk = sm.lnk[slot * NFACE + f];
+    const GeomClass &gc = sm.geo[slot];
+    const int gn = a.perm[lk.perm + g];
+    double Uo[5], Un[5], Fh[5], FL[5], FR[5];
+    double *eo = sm.E + ((f * EPB + slot) * NF) * GF + g;
+    const double *tn = a.Tin + ((size_t)(lk.elem * NFACE + lk.face) * NF) * GF + gn;
+#pragma unroll
+    for (int n = 0; n < NF; ++n) { Uo[n] = eo[n * GF]; Un[n] = tn[n * GF]; }
+    const bool master = (gc.master >> f) & 1;
+    bool ok;
+    if (master) ok = face_flux<PHYS>(Uo, Un, gc.nrm[f], a.gamma, a.flux, Fh, FL, FR);
+    else ok = face_flux<PHYS>(Un, Uo, gc.nrm[f], a.gamma, a.flux, Fh, FL, FR);
+    const double jr = gc.jr[f];
+#pragma unroll
+    for (int n = 0; n < NF; ++n) eo[n * GF] = master ? (Fh[n] - FL[n]) * jr : (FR[n] - Fh[n]) * jr;
+    if (!ok) {
+      atomicOr(a.err, 1);
+      atomicMin(a.err + 1, e);
+    }
+  }
+  __syncthreads();
+}
+
+// Lift: interpolate E (Gauss) to the face GLL points and add W_f * value to
+// the boundary points of D, faces in increasing order as the reference.
+template <class C>
+__device__ __forceinline__ void lift(const Smem<C> &sm, int tid) {
+  constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G, NF = C::NF, EPB = C::EPB, QD = C::QD, QF = C::QF;
+  constexpr int NB = C::NFACE * EPB * NF;
+  double *LFc = sm.B;  // face-major [f][slot][n][QF], spans B and C
+  if constexpr (DIM == 3) {
+    contract<G, G, 1, 0, G, Q, MatG2GL<L, Q>, false>(sm.E, sm.S, NB, G * G, Q * G, tid, C::NT);
+    __syncthreads();
+    contract<Q, G, 1, 1, G, Q, MatG2GL<L, Q>, false>(sm.S, LFc, NB, Q * G, Q * Q, tid, C::NT);
+  } else {
+    contract<G, 1, 1, 0, G, Q, MatG2GL<L, Q>, false>(sm.E, LFc, NB, G, Q, tid, C::NT);
+  }
+  __syncthreads();
+  const double w0 = 1.0 / cW<L, Q>[0], w1 = 1.0 / cW<L, Q>[Q - 1];
+  for (int w = tid; w < EPB * NF * QD; w += C::NT) {
+    const int slot = w / (NF * QD), rem = w - slot * NF * QD, n = rem / QD, p = rem - n * QD;
+    double acc = sm.D[w];
+    if constexpr (DIM == 3) {
+      const int i = p / (Q * Q), j = (p / Q) % Q, k = p % Q;
+      auto lf = [&](int f, int x, int y) { return LFc[((f * EPB + slot) * NF + n) * QF + x * Q + y]; };
+      if (k == 0) acc = fma(w0, lf(0, i, j), acc);
+      if (j == 0) acc = fma(w0, lf(1, i, k), acc);
+      if (i == Q - 1) acc = fma(w1, lf(2, j, k), acc);
+      if (j == Q - 1) acc = fma(w1, lf(3, i, k), acc);
+      if (i == 0) acc = fma(w0, lf(4, j, k), acc);
+      if (k == Q - 1) acc = fma(w1, lf(5, i, j), acc);
+    } else {
+      const int i = p / Q, j = p % Q;
+      auto lf = [&](int f, int x) { return LFc[((f * EPB + slot) * NF + n) * QF + x]; };
+      if (j == 0) acc = fma(w0, lf(0, i), acc);
+      if (i == Q - 1) acc = fma(w1, lf(1, j), acc);
+      if (j == Q - 1) acc = fma(w1, lf(2, i), acc);
+      if (i == 0) acc = fma(w0, lf(3, j), acc);
+    }
+    // quadrature weights of the projection (the J of wJ cancels the mass)
+    double wq;
+    if constexpr (DIM == 3) wq = cW<L, Q>[p / (Q * Q)] * cW<L, Q>[(p / Q) % Q] * cW<L, Q>[p % Q];
+    else wq = cW<L, Q>[p / Q] * cW<L, Q>[p % Q];
+    sm.D[w] = wq * acc;
+  }
+  __syncthreads();
+}
+
+template <class C>
+__device__ __forceinline__ void load_geometry(const Smem<C> &sm, const StageArgs &a, int e0, int tid) {
+  for (int s = tid; s < C::EPB; s += C::NT) {
+    const int e = e0 + s;
+    sm.eid[s] = e < a.ne ? e : -1;
+    sm.geo[s] = a.classes[e < a.ne ? a.gclass[e] : 0];
+  }
+  for (int w = tid; w < C::EPB * C::NFACE; w += C::NT) {
+    const int s = w / C::NFACE, f = w - s * C::NFACE, e = e0 + s;
+    sm.lnk[w] = e < a.ne ? a.links[(size_t)e * C::NFACE + f] : FaceLink{0, 0, 0, 0};
+  }
+}
+
+// Element-major modal register block of the slot's element: NF*LD doubles.
+template <class C>
+__device__ __forceinline__ void load_modal(double *dst, const double *src, int e0, int ne, int tid) {
+  constexpr int BLK = C::NF * C::LD;
+  for (int w = tid; w < C::EPB * BLK; w += C::NT) {
+    const int s = w / BLK, e = e0 + s;
+    dst[w] = e < ne ? src[(size_t)e0 * BLK + w] : (w % C::LD == 0 ? 1.0 : 0.0);
+  }
+}
+
+template <class C>
+__device__ __forceinline__ void store_traces(const double *E, double *T, int e0, int ne, int tid) {
+  constexpr int NF = C::NF, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
+  for (int w = tid; w < EPB * NFACE * NF * GF; w += C::NT) {
+    // global order [e][f][n][g]; smem order [f][slot][n][g]
+    const int s = w / (NFACE * NF * GF), rem = w - s * NFACE * NF * GF;
+    const int f = rem / (NF * GF), ng = rem - f * NF * GF;
+    const int e = e0 + s;
+    if (e < ne) T[(size_t)e * NFACE * NF * GF + rem] = E[(f * EPB + s) * NF * GF + ng];
+  }
+}
+
+// ---------------------------------------------------------------- kernels
+template <class C, int PHYS>
+__global__ void __launch_bounds__(C::NT) stage_kernel(StageArgs a) {
+  extern __shared__ __align__(16) double smem_raw[];
+  Smem<C> sm(smem_raw);
+  const int tid = threadIdx.x;
+  const int e0 = blockIdx.x * C::EPB;
+  load_geometry<C>(sm, a, e0, tid);
+  load_modal<C>(sm.A, a.X, e0, a.ne, tid);
+  __syncthreads();
+  modal_traces<C>(sm.A, sm.E, sm.S, sm.B, tid, C::NT);
+  backward<C>(sm.A, sm.B, sm.S, sm.C, tid, C::NT);
+  volume<C, PHYS>(sm, a.gamma, tid);
+  face_fluxes<C, PHYS>(sm, a, tid);
+  lift<C>(sm, tid);
+  forward<C>(sm.D, sm.R, sm.C, sm.B, tid, C::NT);
+  // RK stage update on the modal registers
+  constexpr int BLK = C::NF * C::LD;
+  for (int w = tid; w < C::EPB * BLK; w += C::NT) {
+    const int s = w / BLK, e = e0 + s;
+    if (e >= a.ne) continue;
+    const size_t gi = (size_t)e0 * BLK + w;
+    const double x = sm.A[w];
+    double r = sm.R[w];
+    if (a.Rcap) a.Rcap[gi] = r;          // first RHS (shallow-water balance)
+    if (a.Rsub) r = r - a.Rsub[gi];
+    double next;
+    switch (a.kind) {
+      case kLSRK: {
+        double ut = a.c0 * a.Ut[gi];
+        ut = fma(-a.dt, r, ut);
+        const double u = fma(a.c1, ut, x);
+        a.Ut[gi] = ut; a.U[gi] = u; next = u;
+        break;
+      }
+      case kTVD0: {
+        const double ut = fma(-a.dt, r, x);
+        a.Ut[gi] = ut; next = ut;
+        break;
+      }
+      case kTVD1: {
+        const double t = fma(-a.dt, r, x);
+        double ut = a.c1 * t;
+        ut = fma(a.c0, a.U[gi], ut);
+        a.Ut[gi] = ut; next = ut;
+        break;
+      }
+      case kTVD2: {
+        const double t = fma(-a.dt, r, x);
+        double u = a.c0 * a.U[gi];
+        u = fma(a.c1, t, u);
+        a.U[gi] = u; next = u;
+        break;
+      }
+      case kRK40: {
+        const double ut = fma(a.c0, r, x);
+        a.Ut[gi] = ut; a.A[gi] = a.c1 * r; next = ut;
+        break;
+      }
+      case kRK41: {
+        const double ut = fma(a.c0, r, a.U[gi]);
+        a.A[gi] = fma(a.c1, r, a.A[gi]);
+        a.Ut[gi] = ut; next = ut;
+        break;
+      }
+      case kRHS: {
+        a.A[gi] = r; next = x;
+        break;
+      }
+      default: {  // kRK43
+        const double acc = fma(a.c1, r, a.A[gi]);
+        const double u = fma(a.c0, acc, a.U[gi]);
+        a.U[gi] = u; next = u;
+        break;
+      }
+    }
+    sm.A[w] = next;
+  }
+  __syncthreads();
+  modal_traces<C>(sm.A, sm.E, sm.S, sm.B, tid, C::NT);
+  store_traces<C>(sm.E, a.Tout, e0, a.ne, tid);
+}
+
+// Traces of a modal register (start of a run, after set_state).
+template <class C>
+__global__ void __launch_bounds__(C::NT) traces_modal_kernel(StageArgs a, const double *Xm, double *T) {
+  extern __shared__ __align__(16) double smem_raw[];
+  Smem<C> sm(smem_raw);
+  const int tid = threadIdx.x, e0 = blockIdx.x * C::EPB;
+  load_modal<C>(sm.A, Xm, e0, a.ne, tid);
+  __syncthreads();
+  modal_traces<C>(sm.A, sm.E, sm.S, sm.B, tid, C::NT);
+  store_traces<C>(sm.E, T, e0, a.ne, tid);
+}
+
+// Load GLL values from Field layout [n][e][QD] into B.
+template <class C>
+__device__ __forceinline__ void load_nodal(double *B, const double *Xn, int e0, int ne, int tid) {
+  constexpr int NF = C::NF, QD = C::QD;
+  for (int w = tid; w < C::EPB * NF * QD; w += C::NT) {
+    const int s = w / (NF * QD), rem = w - s * NF * QD, n = rem / QD, p = rem - n * QD;
+    const int e = e0 + s;
+    B[w] = e < ne ? Xn[((size_t)n * ne + e) * QD + p] : (n == 0 ? 1.0 : 0.0);
+  }
+}
+
+// GL2G traces of GLL values (fill_sides, src/Hex.cpp:933-947,
+// src/Quad.cpp:884-905) for the Domain::time_derivative path.
+template <class C>
+__global__ void __launch_bounds__(C::NT) traces_nodal_kernel(StageArgs a) {
+  extern __shared__ __align__(16) double smem_raw[];
+  Smem<C> sm(smem_raw);
+  constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G, NF = C::NF, EPB = C::EPB, QD = C::QD, QF = C::QF;
+  const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
+  load_nodal<C>(sm.B, a.Xn, e0, a.ne, tid);
+  __syncthreads();
+  // gather face GLL values, face-major [f][slot][n][QF]
+  for (int w = tid; w < C::NFACE * EPB * NF * QF; w += C::NT) {
+    const int f = w / (EPB * NF * QF), rem = w - f * EPB * NF * QF;
+    const int sn = rem / QF, x = rem - sn * QF;
+    const double *src = sm.B + sn * QD;
+    int p;
+    if constexpr (DIM == 3) {
+      const int u = x / Q, v = x % Q;
+      switch (f) {
+        case 0: p = (u * Q + v) * Q + 0; break;
+        case 1: p = (u * Q + 0) * Q + v; break;
+        case 2: p = ((Q - 1) * Q + u) * Q + v; break;
+        case 3: p = (u * Q + (Q - 1)) * Q + v; break;
+        case 4: p = (0 * Q + u) * Q + v; break;
+        default: p = (u * Q + v) * Q + (Q - 1); break;
+      }
+    } else {
+      switch (f) {
+        case 0: p = x * Q + 0; break;
+        case 1: p = (Q - 1) * Q + x; break;
+        case 2: p = x * Q + (Q - 1); break;
+        default: p = 0 * Q + x; break;
+      }
+    }
+    sm.C[w] = src[p];
+  }
+  __syncthreads();
+  constexpr int NB = C::NFACE * EPB * NF;
+  if constexpr (DIM == 3) {
+    contract<Q, Q, 1, 0, Q, G, MatGL2G<L, Q>, false>(sm.C, sm.S, NB, Q * Q, G * Q, tid, C::NT);
+    __syncthreads();
+    contract<G, Q, 1, 1, Q, G, MatGL2G<L, Q>, false>(sm.S, sm.E, NB, G * Q, G * G, tid, C::NT);
+  } else {
+    contract<Q, 1, 1, 0, Q, G, MatGL2G<L, Q>, false>(sm.C, sm.E, NB, Q, G, tid, C::NT);
+  }
+  __syncthreads();
+  store_traces<C>(sm.E, a.Tout, e0, a.ne, tid);
+}
+
+// Domain::time_derivative on GLL values: F = -dU/dt at GLL points (projected).
+template <class C, int PHYS>
+__global__ void __launch_bounds__(C::NT) rhs_nodal_kernel(StageArgs a) {
+  extern __shared__ __align__(16) double smem_raw[];
+  Smem<C> sm(smem_raw);
+  constexpr int NF = C::NF, QD = C::QD, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
+  const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
+  load_geometry<C>(sm, a, e0, tid);
+  load_nodal<C>(sm.B, a.Xn, e0, a.ne, tid);
+  // own traces from Tin (written by traces_nodal_kernel)
+  for (int w = tid; w < EPB * NFACE * NF * GF; w += C::NT) {
+    const int s = w / (NFACE * NF * GF), rem = w - s * NFACE * NF * GF;
+    const int f = rem / (NF * GF), ng = rem - f * NF * GF;
+    const int e = e0 + s;
+    sm.E[(f * EPB + s) * NF * GF + ng] = e < a.ne ? a.Tin[(size_t)e * NFACE * NF * GF + rem] : (ng < GF ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  volume<C, PHYS>(sm, a.gamma, tid);
+  face_fluxes<C, PHYS>(sm, a, tid);
+  lift<C>(sm, tid);
+  forward<C>(sm.D, sm.R, sm.C, sm.B, tid, C::NT);
+  if (a.Rcap || a.Rsub) {
+    constexpr int BLK = NF * C::LD;
+    for (int w = tid; w < EPB * BLK; w += C::NT) {
+      const int e = e0 + w / BLK;
+      if (e >= a.ne) continue;
+      const size_t gi = (size_t)e0 * BLK + w;
+      if (a.Rcap) a.Rcap[gi] = sm.R[w];
+      if (a.Rsub) sm.R[w] = sm.R[w] - a.Rsub[gi];
+    }
+    __syncthreads();
+  }
+  backward<C>(sm.R, sm.B, sm.S, sm.C, tid, C::NT);
+  for (int w = tid; w < EPB * NF * QD; w += C::NT) {
+    const int s = w / (NF * QD), rem = w - s * NF * QD, n = rem / QD, p = rem - n * QD;
+    const int e = e0 + s;
+    if (e < a.ne) a.Fn[((size_t)n * a.ne + e) * QD + p] = sm.B[w];
+  }
+}
+
+// GLL values (Field layout) -> projected modal register (element-major).
+template <class C>
+__global__ void __launch_bounds__(C::NT) forward_kernel(StageArgs a, const double *Un, double *Um) {
+  extern __shared__ __align__(16) double smem_raw[];
+  Smem<C> sm(smem_raw);
+  constexpr int L = C::L, Q = C::Q, NF = C::NF, QD = C::QD, EPB = C::EPB;
+  const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
+  load_nodal<C>(sm.D, Un, e0, a.ne, tid);
+  __syncthreads();
+  for (int w = tid; w < EPB * NF * QD; w += C::NT) {
+    const int p = w % QD;
+    double wq;
+    if constexpr (C::DIM == 3) wq = cW<L, Q>[p / (Q * Q)] * cW<L, Q>[(p / Q) % Q] * cW<L, Q>[p % Q];
+    else wq = cW<L, Q>[p / Q] * cW<L, Q>[p % Q];
+    sm.D[w] = wq * sm.D[w];
+  }
+  __syncthreads();
+  forward<C>(sm.D, sm.R, sm.C, sm.B, tid, C::NT);
+  constexpr int BLK = NF * C::LD;
+  for (int w = tid; w < EPB * BLK; w += C::NT) {
+    const int e = e0 + w / BLK;
+    if (e < a.ne) Um[(size_t)e0 * BLK + w] = sm.R[w];
+  }
+}
+
+// Modal register -> GLL values (Field layout).
+template <class C>
+__global__ void __launch_bounds__(C::NT) backward_kernel(StageArgs a, const double *Um, double *Un) {
+  extern __shared__ __align__(16) double smem_raw[];
+  Smem<C> sm(smem_raw);
+  constexpr int NF = C::NF, QD = C::QD, EPB = C::EPB;
+  const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
+  load_modal<C>(sm.A, Um, e0, a.ne, tid);
+  __syncthreads();
+  backward<C>(sm.A, sm.B, sm.S, sm.C, tid, C::NT);
+  for (int w = tid; w < EPB * NF * QD; w += C::NT) {
+    const int s = w / (NF * QD), rem = w - s * NF * QD, n = rem / QD, p = rem - n * QD;
+    const int e = e0 + s;
+    if (e < a.ne) Un[((size_t)n * a.ne + e) * QD + p] = sm.B[w];
+  }
+}
+
+}  // namespace dgmx

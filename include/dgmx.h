@@ -1,0 +1,152 @@
+/*
+ * dgmx.h -- C ABI of the B200 DG residual and RK-stage engine.
+ *
+ * One opaque handle (dgmx_domain) stands for one DGM Domain on one GPU: the
+ * mesh, the discretisation tables, the conserved-variable state and the
+ * integrator registers all live in device memory.  Every entry point returns
+ * a dgmx_status; none throws, traps or aborts.  Calls on one handle are not
+ * thread-safe; each handle owns one CUDA stream.
+ *
+ * Array layouts at this boundary are DGM's own (src/vField.cpp:88-111,
+ * src/Field.cpp:3042-3123): a vField of nf Fields, each Field a contiguous
+ * element-major array of element values, element e holding Q^d values at its
+ * Gauss-Lobatto-Legendre points with the last direction fastest
+ * (Quad: j + Q*i, src/Quad.cpp:772; Hex: k + Q*(j + Q*i), src/Hex.cpp:817).
+ * Modal (restart) layouts follow src/vField.cpp:1102-1179: per field, per
+ * element, L^d orthonormal-Legendre coefficients, index c + L*(b + L*a).
+ */
+#ifndef DGMX_H
+#define DGMX_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dgmx_domain dgmx_domain;
+
+typedef enum {
+  DGMX_OK = 0,
+  DGMX_ERR_ARGUMENT = 1,      /* bad pointer, size or parameter            */
+  DGMX_ERR_UNSUPPORTED = 2,   /* order/physics/flux combination not built  */
+  DGMX_ERR_CUDA = 3,          /* a CUDA runtime call failed                */
+  DGMX_ERR_NONPHYSICAL = 4,   /* density or pressure below eps^(2/3) on a
+                                 face point (src/Euler3d.cpp:706-762)      */
+  DGMX_ERR_IO = 5,            /* input file missing or malformed           */
+  DGMX_ERR_MEMORY = 6         /* device allocation failed                  */
+} dgmx_status;
+
+/* Physics codes are DGM's eqntype values (src/ReoProblem.cpp:75-156). */
+enum { DGMX_EULER2D = 1, DGMX_NS2D = 2, DGMX_EULER3D = 8, DGMX_NS3D = 9, DGMX_SHALLOW = 30 };
+/* Numerical flux (src/Euler.cpp:104-113). */
+enum { DGMX_FLUX_LF = 0, DGMX_FLUX_ROE = 1 };
+/* Integrators are DGM's inttype values (src/TimeInt.hpp:62-85). */
+enum { DGMX_TVD3 = 3, DGMX_RK4 = 4, DGMX_LSRK14 = 14 };
+/* Arithmetic of the stage kernels. */
+enum { DGMX_FP64 = 0, DGMX_MIXED = 1 };
+
+typedef struct {
+  int dim;               /* 2 (Quad) or 3 (Hex)                              */
+  int ne;                /* number of elements                               */
+  const double *verts;   /* ne * (4|8) * 3 vertex coordinates, DGM order     */
+  int ncon;              /* number of connectivity records                   */
+  const int *con;        /* ncon * 4: eid, side, link eid, link side (.con)  */
+  const int *porder;     /* ne polynomial orders (p)                         */
+  const int *qorder;     /* ne GLL point counts per direction (q, 0 = p+2)   */
+} dgmx_mesh;
+
+typedef struct {
+  int physics;           /* DGMX_EULER2D ... DGMX_SHALLOW                    */
+  int flux;              /* DGMX_FLUX_LF / DGMX_FLUX_ROE                     */
+  int inttype;           /* DGMX_TVD3 / DGMX_RK4 / DGMX_LSRK14               */
+  int precision;         /* DGMX_FP64 / DGMX_MIXED                           */
+  int sw_balance;        /* shallow water: subtract the first RHS
+                            (REO_SHALLOW_ENFORCE_BALANCE, src/Shallow.cpp:251) */
+  int device;            /* CUDA device ordinal                              */
+  double gamma;          /* ratio of specific heats (default 1.4)           */
+  double vis;            /* dynamic viscosity mu ("vis" key)                 */
+  double Pr;             /* Prandtl number (default 0.72)                    */
+} dgmx_params;
+
+/* Builds a Domain from an in-memory mesh.  Replaces the Field/Element
+ * construction of Domain::Domain + Field::Field (src/Field.cpp:2257-2735)
+ * and the physics constructors (src/Euler3d.cpp:47-142, src/Euler.cpp:80-180). */
+dgmx_status dgmx_create(const dgmx_mesh *mesh, const dgmx_params *params, dgmx_domain **out);
+
+/* Builds a Domain from DGM input files root.inp/.msh/.con/.ord (the same keys
+ * and formats Reo::Problem::setup reads, src/ReoProblem.cpp:48-156).
+ * Fields of *params that are not in root.inp keep the caller's values. */
+dgmx_status dgmx_create_from_files(const char *root, const dgmx_params *params, dgmx_domain **out);
+
+dgmx_status dgmx_destroy(dgmx_domain *d);
+
+/* nf fields, nq = total GLL points per field, nm = total modes per field. */
+dgmx_status dgmx_sizes(const dgmx_domain *d, long *nf, long *nq, long *nm);
+
+/* GLL point coordinates in Field layout (z ignored in 2-D; may be NULL). */
+dgmx_status dgmx_coordinates(const dgmx_domain *d, double *x, double *y, double *z);
+
+/* Sets the solution from GLL values (host, Field layout) and projects it to
+ * the polynomial space, as set_ic + project do (src/Euler3d.cpp:1040-1047).
+ * Resets the integrator registers. */
+dgmx_status dgmx_set_state(dgmx_domain *d, const double *U);
+/* Same with device-resident input. */
+dgmx_status dgmx_set_state_device(dgmx_domain *d, const double *U_dev);
+/* Current solution at GLL points (host, Field layout). */
+dgmx_status dgmx_get_state(dgmx_domain *d, double *U);
+dgmx_status dgmx_get_state_device(dgmx_domain *d, double *U_dev);
+/* Current solution as restart modal coefficients (host). */
+dgmx_status dgmx_get_modes(dgmx_domain *d, double *Uh);
+
+/* Domain::time_derivative(U, F) (src/Domain.hpp:243): F = -dU/dt at GLL
+ * points, projected, for U given at GLL points.  Host buffers, Field layout. */
+dgmx_status dgmx_time_derivative(dgmx_domain *d, const double *U, double *F);
+/* Same with device buffers (Field layout), enqueued on the handle's stream. */
+dgmx_status dgmx_time_derivative_device(dgmx_domain *d, const double *U_dev, double *F_dev);
+
+/* TimeInt::advance repeated nsteps times with a fixed dt (TVD3:
+ * src/TimeInt.cpp:826-860; RK4: :266-302; LSRK14: :1989-2013).  The state
+ * stays on the device; the whole step is replayed from a CUDA graph.
+ * Returns DGMX_ERR_NONPHYSICAL if a stage saw a non-realizable face state. */
+dgmx_status dgmx_advance(dgmx_domain *d, double dt, int nsteps);
+
+/* Same, but only enqueues the work on the handle's stream (no host sync,
+ * no error readback); dgmx_sync collects the status. */
+dgmx_status dgmx_advance_async(dgmx_domain *d, double dt, int nsteps);
+dgmx_status dgmx_sync(dgmx_domain *d);
+
+/* Conserved totals (integral of each field, FP64 device reduction). */
+dgmx_status dgmx_integrals(dgmx_domain *d, double *totals);
+
+/* Text of the last error on this handle (or of the last failed create when
+ * d is NULL). */
+const char *dgmx_last_error(const dgmx_domain *d);
+
+/* Number of kernel launches the handle has issued since creation. */
+long dgmx_launch_count(const dgmx_domain *d);
+
+/* The handle's CUDA stream (cudaStream_t), for callers that record events or
+ * order their own work against the engine. */
+void *dgmx_stream(const dgmx_domain *d);
+
+/* Kernel instantiations in this library: rows of (physics, L, Q, elements
+ * per CTA, threads per CTA, shared bytes); returns the row count and writes
+ * at most cap rows. */
+int dgmx_kernel_list(int *rows, int cap);
+
+/* Host-only inspection, no CUDA calls.  1-D tables for L modes and Q GLL
+ * points (G = Q-1 Gauss points): GLL z, w (Q); collocation D (QxQ,
+ * src/Polylib.tpp:1008-1049); orthonormal Legendre on GLL B (LxQ) and on
+ * Gauss Bg (LxG) (src/Basis.cpp:74-102); GL2G (GxQ) and G2GL (QxG)
+ * interpolation (src/Hex.cpp:866-884). */
+dgmx_status dgmx_tables(int L, int Q, double *z, double *w, double *D, double *B, double *Bg,
+                        double *gl2g, double *g2gl);
+/* Processed connectivity of a mesh: per element face (neighbour, neighbour
+ * face, master flag, geometry class) and the neighbour's point index for
+ * each own face point (src/Field.cpp:416-680, :3478-3540,
+ * src/BaseHex.hpp:291-333). */
+dgmx_status dgmx_mesh_links(const dgmx_mesh *mesh, int *links, int *perm_pairs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DGMX_H */

@@ -51,3 +51,48 @@ def passes_dgm_diff(norms, aeps, reps, repsM=float(np.sqrt(np.finfo(float).eps))
         if f["ref_l2"] > repsM and f["l2"] / f["ref_l2"] > reps:
             return False
     return True
+
+
+# Face vertex lists (Hex: src/Hex.cpp:68-69; Quad edges: consecutive vertices)
+HEX_FACES = [(0, 1, 2, 3), (0, 1, 5, 4), (1, 2, 6, 5), (3, 2, 6, 7), (0, 3, 7, 4), (4, 5, 6, 7)]
+QUAD_EDGES = [(0, 1), (1, 2), (3, 2), (0, 3)]
+
+
+def rotated_box(dim, n, lo, hi, p, q=0, seed=0):
+    """Periodic box whose elements have randomly rotated local frames (vertex
+    lists cycled about the z axis, and for Hexes optionally turned upside
+    down), with the connectivity rebuilt from face centroids.  Exercises the
+    side orientation flags (src/Field.cpp:416-680)."""
+    base = dgm_io.box_mesh(dim, n, lo, hi, p, q)
+    rng = np.random.default_rng(seed)
+    verts = base.verts.copy()
+    for e in range(base.ne):
+        r = int(rng.integers(4))
+        if dim == 2:
+            order = [(v + r) % 4 for v in range(4)]
+        else:
+            bot = [(v + r) % 4 for v in range(4)]
+            order = bot + [b + 4 for b in bot]
+            if rng.integers(2):  # turn upside down: swap bottom/top, keep orientation
+                order = [order[4], order[7], order[6], order[5], order[0], order[3], order[2], order[1]]
+        verts[e] = base.verts[e][order]
+    lo_a = np.broadcast_to(np.asarray(lo, float), (dim,))
+    L = np.broadcast_to(np.asarray(hi, float), (dim,)) - lo_a
+    faces = HEX_FACES if dim == 3 else QUAD_EDGES
+    key = {}
+    for e in range(base.ne):
+        for f, fv in enumerate(faces):
+            c = verts[e][list(fv)][:, :dim].mean(axis=0)
+            c = np.mod(c - lo_a + 1e-9 * L, L) - 1e-9 * L
+            k = tuple(np.round(c / L * 4 * max(n if hasattr(n, "__len__") else [n]), 6))
+            key.setdefault(k, []).append((e, f))
+    con = []
+    for e in range(base.ne):
+        for f, fv in enumerate(faces):
+            c = verts[e][list(fv)][:, :dim].mean(axis=0)
+            c = np.mod(c - lo_a + 1e-9 * L, L) - 1e-9 * L
+            k = tuple(np.round(c / L * 4 * max(n if hasattr(n, "__len__") else [n]), 6))
+            pair = [x for x in key[k] if x != (e, f)]
+            assert len(pair) == 1, (e, f, key[k])
+            con.append([e, f, pair[0][0], pair[0][1]])
+    return dgm_io.Mesh(dim, verts, np.array(con, np.int32), base.porder, base.qorder)
