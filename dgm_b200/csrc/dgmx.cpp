@@ -593,3 +593,22 @@ dgmx_status dgmx_mesh_links(const dgmx_mesh *m, int *links, int *perm_pairs) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------
+// Read-only view of a handle for entry points compiled in other units.
+namespace dgmx {
+bool domain_view(dgmx_domain *d, DomainView *v) {
+  if (!d || !v) return false;
+  v->ops = d->ops;
+  v->stream = d->stream;
+  v->base = d->base_args();
+  v->ntrace = d->ntrace();
+  v->device = d->prm.device;
+  v->sw_balance = d->prm.physics == DGMX_SHALLOW && d->prm.sw_balance;
+  v->Rsw = d->Rsw;
+  v->sw_captured = &d->sw_captured;
+  v->errmsg = &d->errmsg;
+  v->launches = &d->launches;
+  return true;
+}
+}  // namespace dgmx

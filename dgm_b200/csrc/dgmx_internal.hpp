@@ -130,6 +130,21 @@ void list_ops(std::vector<std::vector<int>> &out);
 cudaError_t launch_integrals(int nf, int ne, int ld, double c_d, const double *Um, const double *J,
                              double *out, cudaStream_t s);
 
+// What an entry point in another compilation unit needs from a handle.
+struct DomainView {
+  const KernelOps *ops;
+  cudaStream_t stream;
+  StageArgs base;           // mesh pointers and physics parameters
+  size_t ntrace;            // doubles in one trace buffer
+  int device;
+  bool sw_balance;
+  double *Rsw;
+  bool *sw_captured;
+  std::string *errmsg;
+  long *launches;
+};
+bool domain_view(dgmx_domain *d, DomainView *v);
+
 inline int nfields_of(int physics) {
   return physics == DGMX_SHALLOW ? 3 : (physics == DGMX_EULER3D || physics == DGMX_NS3D ? 5 : 4);
 }
