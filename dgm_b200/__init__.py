@@ -88,11 +88,11 @@ def _dp(a):
 
 
 def kernel_list():
-    """Compiled instantiations: rows of (physics, L, Q, elements/CTA, threads, smem bytes)."""
+    """Compiled instantiations: rows of (physics, L, Q, elements/CTA, threads, smem bytes, min CTAs/SM)."""
     n = 4096
-    buf = (ctypes.c_int * (6 * n))()
+    buf = (ctypes.c_int * (7 * n))()
     k = lib().dgmx_kernel_list(buf, n)
-    return np.frombuffer(buf, dtype=np.int32)[: 6 * k].reshape(k, 6).copy()
+    return np.frombuffer(buf, dtype=np.int32)[: 7 * k].reshape(k, 7).copy()
 
 
 class Domain:
@@ -220,6 +220,18 @@ class Domain:
 
     def launch_count(self) -> int:
         return lib().dgmx_launch_count(self.h)
+
+    def autotune(self, reps: int = 20):
+        """Pick the fastest compiled tile variant on this mesh; returns
+        (rows of (epb, minb, threads, us per launch), chosen index)."""
+        L = lib()
+        f = L.dgmx_autotune
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        rows = np.zeros((64, 4))
+        nv, ch = ctypes.c_int(), ctypes.c_int()
+        self._check(f(self.h, int(reps), _dp(rows), 64, ctypes.byref(nv), ctypes.byref(ch)))
+        return rows[: nv.value].copy(), ch.value
 
     def stream(self) -> int:
         """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""

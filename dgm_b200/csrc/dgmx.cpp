@@ -540,8 +540,62 @@ int dgmx_kernel_list(int *rows, int cap) {
   std::vector<std::vector<int>> v;
   list_ops(v);
   for (int i = 0; i < (int)v.size() && i < cap; ++i)
-    for (int k = 0; k < 6; ++k) rows[i * 6 + k] = v[i][k];
+    for (int k = 0; k < 7; ++k) rows[i * 7 + k] = v[i][k];
   return (int)v.size();
+}
+
+// Autotuner: times every compiled tile variant (elements per CTA, register
+// cap) of this handle's (physics, L, Q) on the handle's own mesh with
+// right-hand-side-only stage launches (the state is not modified) and keeps
+// the fastest.  rows (optional, cap rows of 4 doubles): epb, minb, threads,
+// microseconds per launch.  Returns the variant count in *nvariants and the
+// chosen index in *chosen.
+dgmx_status dgmx_autotune(dgmx_domain *d, int reps, double *rows, int cap, int *nvariants, int *chosen) {
+  if (!d || reps <= 0) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(d->prm.device);
+  const std::vector<KernelOps> *vs = find_variants(d->prm.physics, d->L, d->Q);
+  if (!vs || vs->empty()) return d->fail(DGMX_ERR_UNSUPPORTED, "no kernel variants");
+  double *scratch = nullptr;
+  cudaError_t e = dalloc(&scratch, d->nmodal());
+  if (e != cudaSuccess) return d->cuda(e, "autotune scratch");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int best = -1;
+  float best_ms = 0.f;
+  dgmx_status st = DGMX_OK;
+  for (size_t i = 0; i < vs->size() && st == DGMX_OK; ++i) {
+    const KernelOps &v = (*vs)[i];
+    if ((e = v.init(d->tab)) != cudaSuccess) { st = d->cuda(e, "variant init"); break; }
+    StageArgs a = d->base_args();
+    a.kind = kRHS; a.X = d->U; a.U = d->U; a.Ut = d->Ut; a.A = scratch;
+    a.Tin = d->T[d->tcur]; a.Tout = d->T[d->tcur ^ 1];
+    for (int w = 0; w < 2; ++w) e = v.stage(a, d->stream);
+    cudaEventRecord(e0, d->stream);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) e = v.stage(a, d->stream);
+    cudaEventRecord(e1, d->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) { st = d->cuda(e, "autotune launch"); break; }
+    d->launches += 2 + reps;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= reps;
+    if ((int)i < cap && rows) {
+      rows[4 * i + 0] = v.epb; rows[4 * i + 1] = v.minb; rows[4 * i + 2] = v.nt; rows[4 * i + 3] = 1e3 * ms;
+    }
+    if (best < 0 || ms < best_ms) { best = (int)i; best_ms = ms; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(scratch);
+  if (st != DGMX_OK) return st;
+  const KernelOps &chosen_ops = (*vs)[best];
+  if ((e = chosen_ops.init(d->tab)) != cudaSuccess) return d->cuda(e, "variant init");
+  d->ops = &chosen_ops;
+  if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  if (nvariants) *nvariants = (int)vs->size();
+  if (chosen) *chosen = best;
+  return DGMX_OK;
 }
 
 }  // extern "C"

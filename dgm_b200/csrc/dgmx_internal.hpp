@@ -112,7 +112,7 @@ struct StageArgs {
 
 // Launchers for one (physics, L, Q) instantiation; all enqueue on stream s.
 struct KernelOps {
-  int epb = 0, nt = 0;
+  int epb = 0, nt = 0, minb = 0;
   size_t smem = 0;
   cudaError_t (*init)(const Tables1D &t) = nullptr;   // tables + smem attributes, current device
   cudaError_t (*stage)(const StageArgs &a, cudaStream_t s) = nullptr;
@@ -123,7 +123,8 @@ struct KernelOps {
   cudaError_t (*backward)(const StageArgs &a, const double *Um, double *Un, cudaStream_t s) = nullptr;
 };
 void register_ops(int physics, int L, int Q, const KernelOps &ops);
-const KernelOps *find_ops(int physics, int L, int Q);
+const KernelOps *find_ops(int physics, int L, int Q);            // default variant
+const std::vector<KernelOps> *find_variants(int physics, int L, int Q);
 void list_ops(std::vector<std::vector<int>> &out);
 
 // Field integrals from modal register mode 0: out[n] = sum_e J_e c_d Um[e][n][0].

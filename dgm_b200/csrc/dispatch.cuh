@@ -20,9 +20,9 @@ cudaError_t upload_tables_lq(const Tables1D &t) {
   return cudaMemcpyToSymbol(cEnd<L, Q>, end, sizeof(end));
 }
 
-template <int PHYS, int L, int Q, int EPB>
+template <int PHYS, int L, int Q, int EPB, int MINB>
 struct Launch {
-  using C = Cfg<PHYS, L, Q, EPB>;
+  using C = Cfg<PHYS, L, Q, EPB, MINB>;
   static dim3 grid(int ne) { return dim3((unsigned)((ne + EPB - 1) / EPB)); }
   static cudaError_t init(const Tables1D &t) {
     cudaError_t e = upload_tables_lq<L, Q>(t);
@@ -61,7 +61,7 @@ struct Launch {
   }
   static KernelOps ops() {
     KernelOps o;
-    o.epb = EPB; o.nt = C::NT; o.smem = C::SMEM;
+    o.epb = EPB; o.nt = C::NT; o.smem = C::SMEM; o.minb = MINB;
     o.init = init; o.stage = stage; o.traces_modal = traces_modal; o.traces_nodal = traces_nodal;
     o.rhs_nodal = rhs_nodal; o.forward = forward; o.backward = backward;
     return o;
@@ -74,10 +74,38 @@ constexpr int default_epb(int dim, int Q) {
                   : (Q * Q >= 100 ? 1 : (128 / (Q * Q) > 8 ? 8 : 128 / (Q * Q)));
 }
 
+// CTAs per SM that the shared memory of one tile allows (228 KB per SM,
+// 1 KB reserved per CTA).
+template <class C>
+constexpr int smem_blocks() { return (int)((228 * 1024) / (C::SMEM + 1024)); }
+
+// Register variant (EPB, MINB) when it is distinct and sensible: the
+// register cap 64K/(NT*MINB) stays >= 48 and the tile fits shared memory.
+template <int PHYS, int P, int Q, int EPB, int MINB>
+void reg_variant() {
+  using C = Cfg<PHYS, P + 1, Q, EPB, MINB>;
+  if constexpr (MINB == 0 || (65536 / (C::NT * MINB) >= 48 && smem_blocks<C>() >= MINB)) {
+    register_ops(PHYS, P + 1, Q, Launch<PHYS, P + 1, Q, EPB, MINB>::ops());
+  }
+}
+
+// Tile variants for (physics, p, q): the default packing without and with a
+// register cap at the shared-memory occupancy, and twice the packing.  The
+// first registered variant is the default; dgmx_autotune picks among all.
 template <int PHYS, int P, int Q>
 void reg() {
-  constexpr int EPB = default_epb(phys_dim(PHYS), Q);
-  register_ops(PHYS, P + 1, Q, Launch<PHYS, P + 1, Q, EPB>::ops());
+  constexpr int E1 = default_epb(phys_dim(PHYS), Q);
+  using C1 = Cfg<PHYS, P + 1, Q, E1, 0>;
+  constexpr int B1 = smem_blocks<C1>() > 8 ? 8 : smem_blocks<C1>();
+  reg_variant<PHYS, P, Q, E1, 0>();
+  if constexpr (B1 >= 2) reg_variant<PHYS, P, Q, E1, B1>();
+  if constexpr (B1 >= 4) reg_variant<PHYS, P, Q, E1, (B1 * 3) / 4>();
+  constexpr int E2 = 2 * E1;
+  if constexpr (Cfg<PHYS, P + 1, Q, E2, 0>::NT <= 1024 && Cfg<PHYS, P + 1, Q, E2, 0>::SMEM <= 200 * 1024) {
+    using C2 = Cfg<PHYS, P + 1, Q, E2, 0>;
+    constexpr int B2 = smem_blocks<C2>() > 8 ? 8 : smem_blocks<C2>();
+    if constexpr (B2 >= 2) reg_variant<PHYS, P, Q, E2, B2>();
+  }
 }
 
 }  // namespace dgmx

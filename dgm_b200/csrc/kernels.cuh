@@ -82,7 +82,8 @@ __device__ __forceinline__ void volume_flux(const double *U, double gamma, doubl
   if constexpr (PHYS == DGMX_EULER2D || PHYS == DGMX_NS2D) {
     const double gm1 = gamma - 1.0, m5g = -0.5 * gm1;
     const double r = U[0], ru = U[1], rv = U[2], rE = U[3];
-    const double u = ru / r, v = rv / r;
+    const double ir = 1.0 / r;
+    const double u = ru * ir, v = rv * ir;
     double p = u * ru;
     p = v * rv + p;
     p = m5g * p;
@@ -95,7 +96,8 @@ __device__ __forceinline__ void volume_flux(const double *U, double gamma, doubl
   } else if constexpr (PHYS == DGMX_EULER3D || PHYS == DGMX_NS3D) {
     const double gm1 = gamma - 1.0, m5g = -0.5 * gm1;
     const double r = U[0], ru = U[1], rv = U[2], rw = U[3], rE = U[4];
-    const double u = ru / r, v = rv / r, w = rw / r;
+    const double ir = 1.0 / r;
+    const double u = ru * ir, v = rv * ir, w = rw * ir;
     double p = u * ru;
     p = fma(v, rv, p);
     p = fma(w, rw, p);
@@ -109,7 +111,8 @@ __device__ __forceinline__ void volume_flux(const double *U, double gamma, doubl
     F[0][4] = u * e; F[1][4] = v * e; F[2][4] = w * e;
   } else {  // shallow water, geopotential form
     const double phi = U[0], uphi = U[1], vphi = U[2];
-    const double u = uphi / phi, v = vphi / phi;
+    const double iphi = 1.0 / phi;
+    const double u = uphi * iphi, v = vphi * iphi;
     const double p = 0.5 * (phi * phi);
     F[0][0] = uphi;            F[1][0] = vphi;
     F[0][1] = fma(uphi, u, p); F[1][1] = uphi * v;

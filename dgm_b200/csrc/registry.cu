@@ -7,8 +7,8 @@
 
 namespace dgmx {
 namespace {
-std::map<std::tuple<int, int, int>, KernelOps> &table() {
-  static std::map<std::tuple<int, int, int>, KernelOps> t;
+std::map<std::tuple<int, int, int>, std::vector<KernelOps>> &table() {
+  static std::map<std::tuple<int, int, int>, std::vector<KernelOps>> t;
   return t;
 }
 std::mutex &table_mutex() {
@@ -19,10 +19,16 @@ std::mutex &table_mutex() {
 
 void register_ops(int physics, int L, int Q, const KernelOps &ops) {
   std::lock_guard<std::mutex> lk(table_mutex());
-  table()[std::make_tuple(physics, L, Q)] = ops;
+  table()[std::make_tuple(physics, L, Q)].push_back(ops);
 }
 
 const KernelOps *find_ops(int physics, int L, int Q) {
+  std::lock_guard<std::mutex> lk(table_mutex());
+  auto it = table().find(std::make_tuple(physics, L, Q));
+  return it == table().end() || it->second.empty() ? nullptr : &it->second.front();
+}
+
+const std::vector<KernelOps> *find_variants(int physics, int L, int Q) {
   std::lock_guard<std::mutex> lk(table_mutex());
   auto it = table().find(std::make_tuple(physics, L, Q));
   return it == table().end() ? nullptr : &it->second;
@@ -31,8 +37,9 @@ const KernelOps *find_ops(int physics, int L, int Q) {
 void list_ops(std::vector<std::vector<int>> &out) {
   std::lock_guard<std::mutex> lk(table_mutex());
   for (auto &kv : table())
-    out.push_back({std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first), kv.second.epb,
-                   kv.second.nt, (int)kv.second.smem});
+    for (auto &o : kv.second)
+      out.push_back({std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first), o.epb, o.nt,
+                     (int)o.smem, o.minb});
 }
 
 // out[n] = c_d * sum_e J_e Um[e][n][0]: the integral of field n (the

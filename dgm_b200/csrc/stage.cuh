@@ -31,10 +31,13 @@ constexpr int phys_dim(int p) { return (p == DGMX_EULER3D || p == DGMX_NS3D) ? 3
 constexpr int phys_nf(int p) { return p == DGMX_SHALLOW ? 3 : (phys_dim(p) == 3 ? 5 : 4); }
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
-template <int PHYS, int L_, int Q_, int EPB_>
+// One kernel tile: PHYS physics, L modes and Q GLL points per direction,
+// EPB elements per CTA, MINB CTAs per SM requested from the register
+// allocator (__launch_bounds__ minimum blocks; 0 = no request).
+template <int PHYS, int L_, int Q_, int EPB_, int MINB_ = 0>
 struct Cfg {
   static constexpr int DIM = phys_dim(PHYS), NF = phys_nf(PHYS);
-  static constexpr int L = L_, Q = Q_, G = Q_ - 1, EPB = EPB_;
+  static constexpr int L = L_, Q = Q_, G = Q_ - 1, EPB = EPB_, MINB = MINB_ > 0 ? MINB_ : 1;
   static constexpr int NFACE = 2 * DIM;
   static constexpr int LD = Pow<L, DIM>::v, QD = Pow<Q, DIM>::v;
   static constexpr int GF = Pow<G, DIM - 1>::v, QF = Pow<Q, DIM - 1>::v, LF = Pow<L, DIM - 1>::v;
@@ -45,14 +48,17 @@ struct Cfg {
   static constexpr int SZ_C = NF * QD;                 // flux / scratch
   static constexpr int SZ_D = NF * QD;                 // divergence + lift
   static constexpr int SZ_E = NFACE * NF * GF;         // face traces / lift input
-  static constexpr int SZ_R = NF * LD;                 // projected RHS (modal)
+  // projected RHS (modal); shares the E region when it fits (E is dead
+  // between the lift and the next-trace phase)
+  static constexpr bool R_IN_E = NFACE * NF * GF >= NF * LD;
+  static constexpr int SZ_R = R_IN_E ? 0 : NF * LD;
   static constexpr int SZ_S = cmax(cmax(NF * Q * LF, NFACE * NF * LF), DIM == 3 ? NFACE * NF * Q * G : 0);
   static constexpr int SZ_SLOT = SZ_A + SZ_B + SZ_C + SZ_D + SZ_E + SZ_R + SZ_S;
   static constexpr size_t SMEM = (size_t)EPB * SZ_SLOT * sizeof(double) +
                                  (size_t)EPB * (sizeof(GeomClass) + NFACE * sizeof(FaceLink) + 16);
   static_assert(NFACE * QF <= 2 * QD, "lift face buffer must fit in the B+C regions");
   static_assert(DIM == 2 || NFACE * G * L <= 2 * QD, "trace intermediate must fit in the B+C regions");
-  static_assert(SMEM <= 227 * 1024, "element slot does not fit in shared memory");
+  static_assert(SMEM <= 227 * 1024 || EPB > 1, "element slot does not fit in shared memory");
 };
 
 // Trailing-1 shapes so one contraction routine serves 2-D and 3-D.
@@ -70,8 +76,8 @@ struct Smem {
     C = B + K::EPB * K::SZ_B;
     D = C + K::EPB * K::SZ_C;
     E = D + K::EPB * K::SZ_D;
-    R = E + K::EPB * K::SZ_E;
-    S = R + K::EPB * K::SZ_R;
+    R = K::R_IN_E ? E : E + K::EPB * K::SZ_E;
+    S = E + K::EPB * K::SZ_E + K::EPB * K::SZ_R;
     geo = reinterpret_cast<GeomClass *>(S + K::EPB * K::SZ_S);
     lnk = reinterpret_cast<FaceLink *>(geo + K::EPB);
     eid = reinterpret_cast<int *>(lnk + K::EPB * K::NFACE);
@@ -321,17 +327,30 @@ __device__ __forceinline__ void store_traces(const double *E, double *T, int e0,
   }
 }
 
+// The element's own traces, written by the previous stage (or the trace
+// kernel), global [e][f][n][g] -> smem face-major [f][slot][n][g].
+template <class C>
+__device__ __forceinline__ void load_own_traces(double *E, const double *T, int e0, int ne, int tid) {
+  constexpr int NF = C::NF, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
+  for (int w = tid; w < EPB * NFACE * NF * GF; w += C::NT) {
+    const int s = w / (NFACE * NF * GF), rem = w - s * NFACE * NF * GF;
+    const int f = rem / (NF * GF), ng = rem - f * NF * GF;
+    const int e = e0 + s;
+    E[(f * EPB + s) * NF * GF + ng] = e < ne ? T[(size_t)e * NFACE * NF * GF + rem] : (ng < GF ? 1.0 : 0.0);
+  }
+}
+
 // ---------------------------------------------------------------- kernels
 template <class C, int PHYS>
-__global__ void __launch_bounds__(C::NT) stage_kernel(StageArgs a) {
+__global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
   extern __shared__ __align__(16) double smem_raw[];
   Smem<C> sm(smem_raw);
   const int tid = threadIdx.x;
   const int e0 = blockIdx.x * C::EPB;
   load_geometry<C>(sm, a, e0, tid);
   load_modal<C>(sm.A, a.X, e0, a.ne, tid);
+  load_own_traces<C>(sm.E, a.Tin, e0, a.ne, tid);
   __syncthreads();
-  modal_traces<C>(sm.A, sm.E, sm.S, sm.B, tid, C::NT);
   backward<C>(sm.A, sm.B, sm.S, sm.C, tid, C::NT);
   volume<C, PHYS>(sm, a.gamma, tid);
   face_fluxes<C, PHYS>(sm, a, tid);
@@ -406,7 +425,7 @@ __global__ void __launch_bounds__(C::NT) stage_kernel(StageArgs a) {
 
 // Traces of a modal register (start of a run, after set_state).
 template <class C>
-__global__ void __launch_bounds__(C::NT) traces_modal_kernel(StageArgs a, const double *Xm, double *T) {
+__global__ void __launch_bounds__(C::NT, C::MINB) traces_modal_kernel(StageArgs a, const double *Xm, double *T) {
   extern __shared__ __align__(16) double smem_raw[];
   Smem<C> sm(smem_raw);
   const int tid = threadIdx.x, e0 = blockIdx.x * C::EPB;
@@ -430,7 +449,7 @@ __device__ __forceinline__ void load_nodal(double *B, const double *Xn, int e0, 
 // GL2G traces of GLL values (fill_sides, src/Hex.cpp:933-947,
 // src/Quad.cpp:884-905) for the Domain::time_derivative path.
 template <class C>
-__global__ void __launch_bounds__(C::NT) traces_nodal_kernel(StageArgs a) {
+__global__ void __launch_bounds__(C::NT, C::MINB) traces_nodal_kernel(StageArgs a) {
   extern __shared__ __align__(16) double smem_raw[];
   Smem<C> sm(smem_raw);
   constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G, NF = C::NF, EPB = C::EPB, QD = C::QD, QF = C::QF;
@@ -478,7 +497,7 @@ __global__ void __launch_bounds__(C::NT) traces_nodal_kernel(StageArgs a) {
 
 // Domain::time_derivative on GLL values: F = -dU/dt at GLL points (projected).
 template <class C, int PHYS>
-__global__ void __launch_bounds__(C::NT) rhs_nodal_kernel(StageArgs a) {
+__global__ void __launch_bounds__(C::NT, C::MINB) rhs_nodal_kernel(StageArgs a) {
   extern __shared__ __align__(16) double smem_raw[];
   Smem<C> sm(smem_raw);
   constexpr int NF = C::NF, QD = C::QD, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
@@ -486,12 +505,7 @@ __global__ void __launch_bounds__(C::NT) rhs_nodal_kernel(StageArgs a) {
   load_geometry<C>(sm, a, e0, tid);
   load_nodal<C>(sm.B, a.Xn, e0, a.ne, tid);
   // own traces from Tin (written by traces_nodal_kernel)
-  for (int w = tid; w < EPB * NFACE * NF * GF; w += C::NT) {
-    const int s = w / (NFACE * NF * GF), rem = w - s * NFACE * NF * GF;
-    const int f = rem / (NF * GF), ng = rem - f * NF * GF;
-    const int e = e0 + s;
-    sm.E[(f * EPB + s) * NF * GF + ng] = e < a.ne ? a.Tin[(size_t)e * NFACE * NF * GF + rem] : (ng < GF ? 1.0 : 0.0);
-  }
+  load_own_traces<C>(sm.E, a.Tin, e0, a.ne, tid);
   __syncthreads();
   volume<C, PHYS>(sm, a.gamma, tid);
   face_fluxes<C, PHYS>(sm, a, tid);
@@ -518,7 +532,7 @@ __global__ void __launch_bounds__(C::NT) rhs_nodal_kernel(StageArgs a) {
 
 // GLL values (Field layout) -> projected modal register (element-major).
 template <class C>
-__global__ void __launch_bounds__(C::NT) forward_kernel(StageArgs a, const double *Un, double *Um) {
+__global__ void __launch_bounds__(C::NT, C::MINB) forward_kernel(StageArgs a, const double *Un, double *Um) {
   extern __shared__ __align__(16) double smem_raw[];
   Smem<C> sm(smem_raw);
   constexpr int L = C::L, Q = C::Q, NF = C::NF, QD = C::QD, EPB = C::EPB;
@@ -543,7 +557,7 @@ __global__ void __launch_bounds__(C::NT) forward_kernel(StageArgs a, const doubl
 
 // Modal register -> GLL values (Field layout).
 template <class C>
-__global__ void __launch_bounds__(C::NT) backward_kernel(StageArgs a, const double *Um, double *Un) {
+__global__ void __launch_bounds__(C::NT, C::MINB) backward_kernel(StageArgs a, const double *Um, double *Un) {
   extern __shared__ __align__(16) double smem_raw[];
   Smem<C> sm(smem_raw);
   constexpr int NF = C::NF, QD = C::QD, EPB = C::EPB;

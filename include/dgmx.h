@@ -142,9 +142,16 @@ dgmx_status dgmx_time_derivative_static(dgmx_domain *d, const double *U_dev, dou
 void *dgmx_stream(const dgmx_domain *d);
 
 /* Kernel instantiations in this library: rows of (physics, L, Q, elements
- * per CTA, threads per CTA, shared bytes); returns the row count and writes
- * at most cap rows. */
+ * per CTA, threads per CTA, shared bytes, min CTAs per SM); returns the row
+ * count and writes at most cap rows. */
 int dgmx_kernel_list(int *rows, int cap);
+
+/* Autotuner (no counterpart in the reference): times every compiled tile
+ * variant for this handle's physics and order on its own mesh with
+ * right-hand-side-only launches (the state is unchanged) and keeps the
+ * fastest.  rows (optional): cap rows of (elements per CTA, min CTAs per SM,
+ * threads per CTA, microseconds per launch). */
+dgmx_status dgmx_autotune(dgmx_domain *d, int reps, double *rows, int cap, int *nvariants, int *chosen);
 
 /* Host-only inspection, no CUDA calls.  1-D tables for L modes and Q GLL
  * points (G = Q-1 Gauss points): GLL z, w (Q); collocation D (QxQ,

@@ -86,6 +86,24 @@ def test_rhs_and_advance_match_oracle(case):
     assert D.launch_count() >= stages * steps
 
 
+def test_autotune_keeps_results_and_state():
+    """The tile autotuner only changes launch shapes: the state is untouched
+    by tuning and every variant gives the oracle's answer."""
+    P, D = build(oracle.EULER3D, 3, (3, 3, 3), 0, 2 * np.pi, 3, 0, "roe", 14)
+    x, y, z = P.coords()
+    f = TG(x, y, z)
+    U0 = P.project(f)
+    D.set_state(f)
+    before = D.state()
+    rows, pick = D.autotune(reps=3)
+    assert len(rows) >= 2 and 0 <= pick < len(rows)
+    assert np.array_equal(D.state(), before)
+    P.set_state(U0)
+    P.advance(14, 0.002, 2)
+    D.advance(0.002, 2)
+    assert rel(D.state(), P.state()) < TOL_STATE
+
+
 def test_shallow_balance_keeps_state_steady():
     """REO_SHALLOW_ENFORCE_BALANCE subtracts the first RHS (src/Shallow.cpp:255-267),
     so the bump stays exactly where it is on both sides."""
