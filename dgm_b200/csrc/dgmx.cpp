@@ -57,6 +57,7 @@ struct dgmx_domain {
   double *U = nullptr, *Ut = nullptr, *Acc = nullptr;   // modal registers [e][n][ld]
   double *T[2] = {nullptr, nullptr};                     // traces [e][f][n][gf]
   double *Rsw = nullptr;                                 // shallow-water first RHS (modal)
+  double *Ghat = nullptr, *Vtr = nullptr, *Pv = nullptr; // Navier-Stokes BR1 work
   double *nod_in = nullptr, *nod_out = nullptr;          // Field-layout staging
   double *Jdev = nullptr, *integ = nullptr;
   int *gclass = nullptr, *perm = nullptr, *err = nullptr;
@@ -92,17 +93,21 @@ struct dgmx_domain {
     a.gclass = gclass; a.classes = classes; a.links = links; a.perm = perm;
     a.ne = ne; a.gamma = prm.gamma; a.vis = prm.vis; a.Pr = prm.Pr; a.flux = prm.flux;
     a.err = err;
+    a.Ghat = Ghat; a.V = Vtr; a.Pv = Pv;
     return a;
   }
+  bool ns() const { return prm.physics == DGMX_NS2D || prm.physics == DGMX_NS3D; }
 
   void release() {
     if (graph) cudaGraphExecDestroy(graph);
     graph = nullptr;
-    void *ptrs[] = {U, Ut, Acc, T[0], T[1], Rsw, nod_in, nod_out, Jdev, integ, gclass, perm, err, classes, links};
+    void *ptrs[] = {U, Ut, Acc, T[0], T[1], Rsw, nod_in, nod_out, Jdev, integ, gclass, perm, err, classes, links,
+                    Ghat, Vtr, Pv};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (host_pinned) cudaFreeHost(host_pinned);
     if (stream) cudaStreamDestroy(stream);
     U = Ut = Acc = Rsw = nod_in = nod_out = Jdev = integ = host_pinned = nullptr;
+    Ghat = Vtr = Pv = nullptr;
     T[0] = T[1] = nullptr; gclass = perm = err = nullptr; classes = nullptr; links = nullptr; stream = nullptr;
   }
 };
@@ -118,7 +123,13 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
   auto run = [&](int kind, const double *X, double c0, double c1) -> dgmx_status {
     a.kind = kind; a.X = X; a.c0 = c0; a.c1 = c1;
     a.Tin = d->T[d->tcur]; a.Tout = d->T[d->tcur ^ 1];
-    cudaError_t e = d->ops->stage(a, d->stream);
+    cudaError_t e;
+    if (d->ns()) {
+      if ((e = d->ops->ns_grad(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous gradient kernel");
+      if ((e = d->ops->ns_visc(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
+      d->launches += 2;
+    }
+    e = d->ops->stage(a, d->stream);
     if (e != cudaSuccess) return d->cuda(e, "stage kernel launch");
     d->tcur ^= 1;
     ++d->launches;
@@ -147,6 +158,7 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
 }
 
 int stages_per_step(int inttype) { return inttype == DGMX_LSRK14 ? 14 : (inttype == DGMX_TVD3 ? 3 : 4); }
+int launches_per_stage(const dgmx_domain *d) { return d->ns() ? 3 : 1; }
 
 // traces of U into T[tcur]
 dgmx_status refresh_traces(dgmx_domain *d) {
@@ -253,7 +265,10 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
             chk(dalloc(&d->classes, d->mesh.classes.size()), "alloc classes") &&
             chk(dalloc(&d->links, d->mesh.links.size()), "alloc links") &&
             chk(dalloc(&d->perm, d->mesh.perm.size()), "alloc perm") && chk(dalloc(&d->err, (size_t)2), "alloc err") &&
-            (phys != DGMX_SHALLOW || chk(dalloc(&d->Rsw, d->nmodal()), "alloc sw source"));
+            (phys != DGMX_SHALLOW || chk(dalloc(&d->Rsw, d->nmodal()), "alloc sw source")) &&
+            (!d->ns() || (chk(dalloc(&d->Ghat, (size_t)d->ne * (d->dim + 1) * d->dim * d->ld), "alloc gradients") &&
+                          chk(dalloc(&d->Vtr, (size_t)d->ne * d->nfaces * (d->nf - 1) * d->gf), "alloc viscous traces") &&
+                          chk(dalloc(&d->Pv, (size_t)d->ne * (d->nf - 1) * d->ld), "alloc viscous divergence")));
   if (ok) {
     ok = chk(cudaMemcpy(d->gclass, d->mesh.gclass.data(), sizeof(int) * d->ne, cudaMemcpyHostToDevice), "upload") &&
          chk(cudaMemcpy(d->classes, d->mesh.classes.data(), sizeof(GeomClass) * d->mesh.classes.size(),
@@ -428,6 +443,11 @@ dgmx_status dgmx_time_derivative_device(dgmx_domain *d, const double *U_dev, dou
     if (!d->sw_captured) { a.Rcap = d->Rsw; d->sw_captured = true; }
     a.Rsub = d->Rsw;
   }
+  if (d->ns()) {
+    if ((e = d->ops->ns_grad(a, true, d->stream)) != cudaSuccess) return d->cuda(e, "viscous gradient kernel");
+    if ((e = d->ops->ns_visc(a, true, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
+    d->launches += 2;
+  }
   e = d->ops->rhs_nodal(a, d->stream);
   ++d->launches;
   if (e != cudaSuccess) return d->cuda(e, "nodal rhs kernel");
@@ -492,7 +512,7 @@ dgmx_status dgmx_advance_async(dgmx_domain *d, double dt, int nsteps) {
   for (; d->graph && s + reps <= nsteps; s += reps) {
     cudaError_t e = cudaGraphLaunch(d->graph, d->stream);
     if (e != cudaSuccess) return d->cuda(e, "graph launch");
-    d->launches += (long)nst * reps;
+    d->launches += (long)nst * reps * launches_per_stage(d);
   }
   for (; s < nsteps; ++s)
     if ((st = enqueue_step(d, dt)) != DGMX_OK) return st;

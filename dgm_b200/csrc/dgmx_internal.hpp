@@ -32,6 +32,7 @@ struct GeomClass {
   double metric[9];     // rx ry rz sx sy sz tx ty tz (2-D: rx ry 0 sx sy 0 ...)
   double J;             // element Jacobian
   double nrm[6][3];     // unit normal of face f in the frame of its master side
+  double onrm[6][3];    // this element's own outward unit normal of face f
   double jr[6];         // side Jacobian / element Jacobian on this element's side
   int master;           // bit f set: this element owns (is master of) face f
   int pad;
@@ -108,6 +109,10 @@ struct StageArgs {
   // shallow-water balance (REO_SHALLOW_ENFORCE_BALANCE, src/Shallow.cpp:251-267)
   double *Rcap;           // if set, the projected RHS is stored here (modal)
   const double *Rsub;     // if set, subtracted from the projected RHS
+  // Navier-Stokes BR1 (src/Navier_Stokes3d.cpp:182-391)
+  double *Ghat;           // projected primitive gradients, modal [e][comp][dir][L^d]
+  double *V;              // viscous normal-flux traces [e][face][field-1][gf]
+  double *Pv;             // projected viscous divergence, modal [e][field-1][L^d]
 };
 
 // Launchers for one (physics, L, Q) instantiation; all enqueue on stream s.
@@ -121,6 +126,10 @@ struct KernelOps {
   cudaError_t (*rhs_nodal)(const StageArgs &a, cudaStream_t s) = nullptr;
   cudaError_t (*forward)(const StageArgs &a, const double *Un, double *Um, cudaStream_t s) = nullptr;
   cudaError_t (*backward)(const StageArgs &a, const double *Um, double *Un, cudaStream_t s) = nullptr;
+  // Navier-Stokes only: lifted gradients, then viscous traces + divergence;
+  // nodal = read GLL values from a.Xn instead of the modal register a.X
+  cudaError_t (*ns_grad)(const StageArgs &a, bool nodal, cudaStream_t s) = nullptr;
+  cudaError_t (*ns_visc)(const StageArgs &a, bool nodal, cudaStream_t s) = nullptr;
 };
 void register_ops(int physics, int L, int Q, const KernelOps &ops);
 const KernelOps *find_ops(int physics, int L, int Q);            // default variant

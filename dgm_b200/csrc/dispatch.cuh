@@ -2,7 +2,7 @@
 // per-physics compilation units (k_*.cu).
 #pragma once
 
-#include "stage.cuh"
+#include "ns.cuh"
 
 namespace dgmx {
 
@@ -33,7 +33,36 @@ struct Launch {
     if ((e = cudaFuncSetAttribute(traces_nodal_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
     if ((e = cudaFuncSetAttribute(rhs_nodal_kernel<C, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
     if ((e = cudaFuncSetAttribute(forward_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-    return cudaFuncSetAttribute(backward_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if ((e = cudaFuncSetAttribute(backward_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+    if constexpr (is_ns(PHYS)) {
+      using N = NsCfg<C>;
+      const int sg = (int)N::Grad::SMEM, sv = (int)N::Visc::SMEM;
+      if ((e = cudaFuncSetAttribute(ns_grad_kernel<C, PHYS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
+      if ((e = cudaFuncSetAttribute(ns_grad_kernel<C, PHYS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
+      if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+      if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+    }
+    return cudaSuccess;
+  }
+  static cudaError_t ns_grad(const StageArgs &a, bool nodal, cudaStream_t s) {
+    if constexpr (is_ns(PHYS)) {
+      using N = NsCfg<C>;
+      if (nodal) ns_grad_kernel<C, PHYS, true><<<grid(a.ne), C::NT, N::Grad::SMEM, s>>>(a);
+      else ns_grad_kernel<C, PHYS, false><<<grid(a.ne), C::NT, N::Grad::SMEM, s>>>(a);
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
+  }
+  static cudaError_t ns_visc(const StageArgs &a, bool nodal, cudaStream_t s) {
+    if constexpr (is_ns(PHYS)) {
+      using N = NsCfg<C>;
+      if (nodal) ns_visc_kernel<C, PHYS, true><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
+      else ns_visc_kernel<C, PHYS, false><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
   }
   static cudaError_t stage(const StageArgs &a, cudaStream_t s) {
     stage_kernel<C, PHYS><<<grid(a.ne), C::NT, C::SMEM, s>>>(a);
@@ -64,6 +93,7 @@ struct Launch {
     o.epb = EPB; o.nt = C::NT; o.smem = C::SMEM; o.minb = MINB;
     o.init = init; o.stage = stage; o.traces_modal = traces_modal; o.traces_nodal = traces_nodal;
     o.rhs_nodal = rhs_nodal; o.forward = forward; o.backward = backward;
+    if constexpr (is_ns(PHYS)) { o.ns_grad = ns_grad; o.ns_visc = ns_visc; }
     return o;
   }
 };
@@ -79,12 +109,19 @@ constexpr int default_epb(int dim, int Q) {
 template <class C>
 constexpr int smem_blocks() { return (int)((228 * 1024) / (C::SMEM + 1024)); }
 
+// Navier-Stokes tiles also need their viscous kernels to fit shared memory.
+template <int PHYS, class C>
+constexpr bool ns_fits() {
+  if constexpr (is_ns(PHYS)) return NsCfg<C>::Grad::SMEM <= 227 * 1024 && NsCfg<C>::Visc::SMEM <= 227 * 1024;
+  else return true;
+}
+
 // Register variant (EPB, MINB) when it is distinct and sensible: the
 // register cap 64K/(NT*MINB) stays >= 48 and the tile fits shared memory.
 template <int PHYS, int P, int Q, int EPB, int MINB>
 void reg_variant() {
   using C = Cfg<PHYS, P + 1, Q, EPB, MINB>;
-  if constexpr (MINB == 0 || (65536 / (C::NT * MINB) >= 48 && smem_blocks<C>() >= MINB)) {
+  if constexpr (ns_fits<PHYS, C>() && (MINB == 0 || (65536 / (C::NT * MINB) >= 48 && smem_blocks<C>() >= MINB))) {
     register_ops(PHYS, P + 1, Q, Launch<PHYS, P + 1, Q, EPB, MINB>::ops());
   }
 }

@@ -239,6 +239,7 @@ bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::strin
       const SideInfo &S = side[(size_t)e * nfaces + s];
       const double *n = S.master ? geo[e].nrm[s] : geo[S.le].nrm[S.ls];
       for (int k = 0; k < 3; ++k) c.nrm[s][k] = n[k];
+      for (int k = 0; k < 3; ++k) c.onrm[s][k] = geo[e].nrm[s][k];
       c.jr[s] = geo[e].jr[s];
       if (S.master) c.master |= 1 << s;
     }

@@ -58,6 +58,11 @@ cudaError_t scratch_address(int dev, double **out) {
 extern "C" dgmx_status dgmx_time_derivative_static(dgmx_domain *d, const double *U_dev, double *F_dev) {
   dgmx::DomainView v;
   if (!U_dev || !F_dev || !dgmx::domain_view(d, &v)) return DGMX_ERR_ARGUMENT;
+  if (v.base.V) {
+    *v.errmsg = "the static-scratch RHS covers Euler and shallow water; Navier-Stokes needs the handle's "
+                "viscous work buffers (use dgmx_time_derivative_device)";
+    return DGMX_ERR_UNSUPPORTED;
+  }
   if (v.device < 0 || v.device >= kMaxDevices) {
     *v.errmsg = "device ordinal out of range for the static trace scratch";
     return DGMX_ERR_ARGUMENT;

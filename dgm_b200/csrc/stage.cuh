@@ -239,6 +239,19 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
     const double jr = gc.jr[f];
 #pragma unroll
     for (int n = 0; n < NF; ++n) eo[n * GF] = master ? (Fh[n] - FL[n]) * jr : (FR[n] - Fh[n]) * jr;
+    if constexpr (PHYS == DGMX_NS2D || PHYS == DGMX_NS3D) {
+      // BR1 viscous lift: '-' average of the viscous normal-flux traces in
+      // the master frame (src/Domain.cpp:1883-1937), subtracted like
+      // scale(-1, Uv); Ur += Uv (src/Navier_Stokes3d.cpp:377-390)
+      const double *vo = a.V + ((size_t)(e * NFACE + f) * (NF - 1)) * GF + g;
+      const double *vn = a.V + ((size_t)(lk.elem * NFACE + lk.face) * (NF - 1)) * GF + gn;
+#pragma unroll
+      for (int n = 1; n < NF; ++n) {
+        const double Vo = vo[(n - 1) * GF], Vn = vn[(n - 1) * GF];
+        const double fs = master ? 0.5 * (Vo - Vn) : -(0.5 * (Vn - Vo));
+        eo[n * GF] = eo[n * GF] - (fs - Vo) * jr;
+      }
+    }
     if (!ok) {
       atomicOr(a.err, 1);
       atomicMin(a.err + 1, e);
@@ -366,6 +379,10 @@ __global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
     double r = sm.R[w];
     if (a.Rcap) a.Rcap[gi] = r;          // first RHS (shallow-water balance)
     if (a.Rsub) r = r - a.Rsub[gi];
+    if constexpr (PHYS == DGMX_NS2D || PHYS == DGMX_NS3D) {
+      const int n = (w % BLK) / C::LD, m = w % C::LD;
+      if (n >= 1) r = r - a.Pv[((size_t)e * (C::NF - 1) + (n - 1)) * C::LD + m];
+    }
     double next;
     switch (a.kind) {
       case kLSRK: {
@@ -511,6 +528,14 @@ __global__ void __launch_bounds__(C::NT, C::MINB) rhs_nodal_kernel(StageArgs a) 
   face_fluxes<C, PHYS>(sm, a, tid);
   lift<C>(sm, tid);
   forward<C>(sm.D, sm.R, sm.C, sm.B, tid, C::NT);
+  if constexpr (PHYS == DGMX_NS2D || PHYS == DGMX_NS3D) {
+    constexpr int BLK = NF * C::LD;
+    for (int w = tid; w < EPB * BLK; w += C::NT) {
+      const int e = e0 + w / BLK, n = (w % BLK) / C::LD, m = w % C::LD;
+      if (e < a.ne && n >= 1) sm.R[w] = sm.R[w] - a.Pv[((size_t)e * (NF - 1) + (n - 1)) * C::LD + m];
+    }
+    __syncthreads();
+  }
   if (a.Rcap || a.Rsub) {
     constexpr int BLK = NF * C::LD;
     for (int w = tid; w < EPB * BLK; w += C::NT) {

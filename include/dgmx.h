@@ -134,7 +134,8 @@ long dgmx_launch_count(const dgmx_domain *d);
  * shared by all calls on a device and keeps the last call's contents, so
  * calls that overlap on the GPU race; the first call on a device resolves
  * the array's address and should come before any stream capture.  Enqueued
- * on the handle's stream; no cudaMalloc, cudaFree or other allocation. */
+ * on the handle's stream; no cudaMalloc, cudaFree or other allocation.
+ * Euler and shallow water only (Navier-Stokes returns DGMX_ERR_UNSUPPORTED). */
 dgmx_status dgmx_time_derivative_static(dgmx_domain *d, const double *U_dev, double *F_dev);
 
 /* The handle's CUDA stream (cudaStream_t), for callers that record events or

@@ -22,14 +22,14 @@ def rel(a, b):
     return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
 
 
-def build(phys, dim, n, lo, hi, p, q, flux, inttype, sw_balance=True, rotated=False):
+def build(phys, dim, n, lo, hi, p, q, flux, inttype, sw_balance=True, rotated=False, vis=0.0):
     import dgm_b200
     from tests.cases import rotated_box
     m = rotated_box(dim, n, lo, hi, p, q, seed=3) if rotated else dgm_b200.meshgen.box(dim, n, lo, hi, p, q)
-    P = oracle.Problem(dgm_io.Mesh(m.dim, m.verts, m.con, m.porder, m.qorder), phys, flux=flux)
+    P = oracle.Problem(dgm_io.Mesh(m.dim, m.verts, m.con, m.porder, m.qorder), phys, flux=flux, vis=vis)
     if phys == oracle.SHALLOW:
         P.set_sw_balance(sw_balance)
-    D = dgm_b200.Domain(m, phys, flux=flux, inttype=inttype, sw_balance=sw_balance)
+    D = dgm_b200.Domain(m, phys, flux=flux, inttype=inttype, sw_balance=sw_balance, vis=vis)
     return P, D
 
 
@@ -84,6 +84,43 @@ def test_rhs_and_advance_match_oracle(case):
     # the kernels really ran: one launch per stage
     stages = {14: 14, 3: 3, 4: 4}[inttype]
     assert D.launch_count() >= stages * steps
+
+
+NS_CASES = [
+    # name, physics, dim, n, lo, hi, p, q, flux, inttype, ic, dt, steps, vis, rotated
+    ("ns2d-vquad-like", 2, 2, (3, 3), 0, 4, 4, 0, "laxfriedrichs", 3, "vortex", 0.001, 5, 0.02, False),
+    ("ns2d-rk4-q=p+1", 2, 2, (4, 3), 0, 4, 3, 4, "laxfriedrichs", 4, "vortex", 0.001, 4, 0.05, False),
+    ("ns2d-rotated-roe", 2, 2, (3, 4), 0, 4, 3, 0, "roe", 14, "vortex", 0.001, 3, 0.02, True),
+    ("ns2d-p7", 2, 2, (2, 2), 0, 4, 7, 0, "laxfriedrichs", 14, "vortex", 0.0005, 2, 0.01, False),
+    ("ns3d-tgv-p3", 9, 3, (3, 3, 3), 0, 2 * np.pi, 3, 0, "laxfriedrichs", 14, "tgv", 0.002, 3, 0.01, False),
+    ("ns3d-tvd-p2-ragged", 9, 3, (3, 2, 4), 0, 2 * np.pi, 2, 0, "laxfriedrichs", 3, "tgv", 0.002, 3, 0.05, False),
+    ("ns3d-rotated-p4", 9, 3, (2, 3, 2), 0, 2 * np.pi, 4, 0, "laxfriedrichs", 14, "tgv", 0.001, 2, 0.01, True),
+    ("ns3d-p7", 9, 3, (2, 2, 2), 0, 2 * np.pi, 7, 0, "laxfriedrichs", 14, "tgv", 0.0005, 1, 1.0 / 1600, False),
+]
+
+
+@pytest.mark.parametrize("case", NS_CASES, ids=[c[0] for c in NS_CASES])
+def test_navier_stokes_br1_matches_oracle(case):
+    _, phys, dim, n, lo, hi, p, q, flux, inttype, ic, dt, steps, vis, rotated = case
+    P, D = build(phys, dim, n, lo, hi, p, q, flux, inttype, rotated=rotated, vis=vis)
+    x, y, z = P.coords()
+    if ic == "vortex":
+        f = ics.vortex_ic(x, y, [(2.0, 2.0, 0.3, 1.0, 0.5)], nf=4)
+    else:
+        f = TG(x, y, z)
+    U0 = P.project(f)
+    F_o, F_g = P.rhs(U0), D.time_derivative(U0)
+    scale = np.sqrt((F_o ** 2).sum()) + np.sqrt((U0 ** 2).sum())
+    assert np.sqrt(((F_g - F_o) ** 2).sum()) / scale < 1e-12
+    P.set_state(U0)
+    D.set_state(f)
+    assert P.advance(inttype, dt, steps) == 0
+    D.advance(dt, steps)
+    assert rel(D.state(), P.state()) < TOL_STATE
+    # viscosity matters in these cases: the Euler RHS differs
+    E = oracle.Problem(dgm_io.Mesh(dim, P.mesh.verts, P.mesh.con, P.mesh.porder, P.mesh.qorder),
+                       oracle.EULER2D if dim == 2 else oracle.EULER3D, flux=flux)
+    assert rel(E.rhs(U0), F_o) > 1e-8
 
 
 def test_autotune_keeps_results_and_state():
