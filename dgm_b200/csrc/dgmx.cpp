@@ -51,13 +51,15 @@ struct dgmx_domain {
   int dim = 0, nf = 0, ne = 0, L = 0, Q = 0, G = 0, nfaces = 0, gf = 0, ld = 0, qd = 0;
   HostMesh mesh;
   Tables1D tab;
-  const KernelOps *ops = nullptr;
+  const KernelOps *ops = nullptr;     // FP64 tiles (also the nodal path)
+  const KernelOps *ops_m = nullptr;   // mixed-precision stage tiles (precision = DGMX_MIXED)
   cudaStream_t stream = nullptr;
   // device state
   double *U = nullptr, *Ut = nullptr, *Acc = nullptr;   // modal registers [e][n][ld]
   double *T[2] = {nullptr, nullptr};                     // traces [e][f][n][gf]
   double *Rsw = nullptr;                                 // shallow-water first RHS (modal)
   double *Ghat = nullptr, *Vtr = nullptr, *Pv = nullptr; // Navier-Stokes BR1 work
+  float *Utf = nullptr, *Tf[2] = {nullptr, nullptr};     // mixed form: FP32 register and traces
   double *nod_in = nullptr, *nod_out = nullptr;          // Field-layout staging
   double *Jdev = nullptr, *integ = nullptr;
   int *gclass = nullptr, *perm = nullptr, *err = nullptr;
@@ -97,17 +99,20 @@ struct dgmx_domain {
     return a;
   }
   bool ns() const { return prm.physics == DGMX_NS2D || prm.physics == DGMX_NS3D; }
+  bool mixed() const { return prm.precision == DGMX_MIXED; }
+  const KernelOps *stage_ops() const { return mixed() ? ops_m : ops; }
 
   void release() {
     if (graph) cudaGraphExecDestroy(graph);
     graph = nullptr;
     void *ptrs[] = {U, Ut, Acc, T[0], T[1], Rsw, nod_in, nod_out, Jdev, integ, gclass, perm, err, classes, links,
-                    Ghat, Vtr, Pv};
+                    Ghat, Vtr, Pv, Utf, Tf[0], Tf[1]};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (host_pinned) cudaFreeHost(host_pinned);
     if (stream) cudaStreamDestroy(stream);
     U = Ut = Acc = Rsw = nod_in = nod_out = Jdev = integ = host_pinned = nullptr;
     Ghat = Vtr = Pv = nullptr;
+    Utf = Tf[0] = Tf[1] = nullptr;
     T[0] = T[1] = nullptr; gclass = perm = err = nullptr; classes = nullptr; links = nullptr; stream = nullptr;
   }
 };
@@ -123,13 +128,14 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
   auto run = [&](int kind, const double *X, double c0, double c1) -> dgmx_status {
     a.kind = kind; a.X = X; a.c0 = c0; a.c1 = c1;
     a.Tin = d->T[d->tcur]; a.Tout = d->T[d->tcur ^ 1];
+    if (d->mixed()) { a.Utf = d->Utf; a.Tinf = d->Tf[d->tcur]; a.Toutf = d->Tf[d->tcur ^ 1]; }
     cudaError_t e;
     if (d->ns()) {
       if ((e = d->ops->ns_grad(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous gradient kernel");
       if ((e = d->ops->ns_visc(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
       d->launches += 2;
     }
-    e = d->ops->stage(a, d->stream);
+    e = d->stage_ops()->stage(a, d->stream);
     if (e != cudaSuccess) return d->cuda(e, "stage kernel launch");
     d->tcur ^= 1;
     ++d->launches;
@@ -163,7 +169,8 @@ int launches_per_stage(const dgmx_domain *d) { return d->ns() ? 3 : 1; }
 // traces of U into T[tcur]
 dgmx_status refresh_traces(dgmx_domain *d) {
   StageArgs a = d->base_args();
-  cudaError_t e = d->ops->traces_modal(a, d->U, d->T[d->tcur], d->stream);
+  cudaError_t e = d->mixed() ? d->ops_m->traces_modal(a, d->U, d->Tf[d->tcur], d->stream)
+                             : d->ops->traces_modal(a, d->U, d->T[d->tcur], d->stream);
   ++d->launches;
   return d->cuda(e, "trace kernel launch");
 }
@@ -174,7 +181,8 @@ dgmx_status capture_sw_source(dgmx_domain *d) {
   StageArgs a = d->base_args();
   a.kind = kRHS; a.X = d->U; a.U = d->U; a.Ut = d->Ut; a.A = d->Rsw;
   a.Tin = d->T[d->tcur]; a.Tout = d->T[d->tcur ^ 1];
-  cudaError_t e = d->ops->stage(a, d->stream);
+  if (d->mixed()) { a.Utf = d->Utf; a.Tinf = d->Tf[d->tcur]; a.Toutf = d->Tf[d->tcur ^ 1]; }
+  cudaError_t e = d->stage_ops()->stage(a, d->stream);
   ++d->launches;
   d->tcur ^= 1;
   d->sw_captured = true;
@@ -219,7 +227,11 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
   }
   if (p->flux != DGMX_FLUX_LF && p->flux != DGMX_FLUX_ROE) { g_create_error = "flux must be LF or Roe"; return DGMX_ERR_UNSUPPORTED; }
   if (phys == DGMX_SHALLOW && p->flux != DGMX_FLUX_LF) { g_create_error = "shallow water supports Lax-Friedrichs only"; return DGMX_ERR_UNSUPPORTED; }
-  if (p->precision != DGMX_FP64) { g_create_error = "only the FP64 kernels are built"; return DGMX_ERR_UNSUPPORTED; }
+  if (p->precision != DGMX_FP64 && p->precision != DGMX_MIXED) { g_create_error = "precision must be FP64 or MIXED"; return DGMX_ERR_ARGUMENT; }
+  if (p->precision == DGMX_MIXED && (p->inttype != DGMX_LSRK14 || phys == DGMX_NS2D || phys == DGMX_NS3D)) {
+    g_create_error = "the mixed-precision form is built for LSRK14 with Euler and shallow water";
+    return DGMX_ERR_UNSUPPORTED;
+  }
   if (!m->porder || m->ne <= 0) { g_create_error = "mesh needs porder"; return DGMX_ERR_ARGUMENT; }
   const int pp = m->porder[0];
   const int qq = (m->qorder && m->qorder[0]) ? m->qorder[0] : pp + 2;
@@ -231,6 +243,13 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
     }
   }
   d->ops = find_ops(phys, pp + 1, qq);
+  if (d->ops && p->precision == DGMX_MIXED) {
+    d->ops_m = find_ops(phys + kMixedKey, pp + 1, qq);
+    if (!d->ops_m) {
+      g_create_error = "no mixed-precision kernels built for p=" + std::to_string(pp) + ", q=" + std::to_string(qq);
+      return DGMX_ERR_UNSUPPORTED;
+    }
+  }
   if (!d->ops) {
     g_create_error = "no kernels built for physics " + std::to_string(phys) + ", p=" + std::to_string(pp) +
                      ", q=" + std::to_string(qq);
@@ -255,6 +274,7 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
   };
   st = DGMX_OK;
   if (!chk(d->ops->init(d->tab), "kernel table upload")) { g_create_error = d->errmsg; d->release(); return st; }
+  if (d->ops_m && !chk(d->ops_m->init(d->tab), "kernel table upload")) { g_create_error = d->errmsg; d->release(); return st; }
   if (!chk(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking), "stream")) { g_create_error = d->errmsg; d->release(); return st; }
   bool ok = chk(dalloc(&d->U, d->nmodal()), "alloc U") && chk(dalloc(&d->Ut, d->nmodal()), "alloc Ut") &&
             chk(dalloc(&d->Acc, d->nmodal()), "alloc Acc") && chk(dalloc(&d->T[0], d->ntrace()), "alloc T0") &&
@@ -266,6 +286,9 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
             chk(dalloc(&d->links, d->mesh.links.size()), "alloc links") &&
             chk(dalloc(&d->perm, d->mesh.perm.size()), "alloc perm") && chk(dalloc(&d->err, (size_t)2), "alloc err") &&
             (phys != DGMX_SHALLOW || chk(dalloc(&d->Rsw, d->nmodal()), "alloc sw source")) &&
+            (!d->mixed() || (chk(dalloc(&d->Utf, d->nmodal()), "alloc Ut (FP32)") &&
+                             chk(dalloc(&d->Tf[0], d->ntrace()), "alloc T0 (FP32)") &&
+                             chk(dalloc(&d->Tf[1], d->ntrace()), "alloc T1 (FP32)"))) &&
             (!d->ns() || (chk(dalloc(&d->Ghat, (size_t)d->ne * (d->dim + 1) * d->dim * d->ld), "alloc gradients") &&
                           chk(dalloc(&d->Vtr, (size_t)d->ne * d->nfaces * (d->nf - 1) * d->gf), "alloc viscous traces") &&
                           chk(dalloc(&d->Pv, (size_t)d->ne * (d->nf - 1) * d->ld), "alloc viscous divergence")));
@@ -300,6 +323,7 @@ dgmx_status set_state_from_device_nodal(dgmx_domain *d, const double *Un_dev) {
   if (e != cudaSuccess) return d->cuda(e, "forward kernel");
   if ((e = cudaMemsetAsync(d->Ut, 0, sizeof(double) * d->nmodal(), d->stream))) return d->cuda(e, "memset");
   if ((e = cudaMemsetAsync(d->Acc, 0, sizeof(double) * d->nmodal(), d->stream))) return d->cuda(e, "memset");
+  if (d->Utf && (e = cudaMemsetAsync(d->Utf, 0, sizeof(float) * d->nmodal(), d->stream))) return d->cuda(e, "memset");
   d->tcur = 0;
   d->sw_captured = false;
   dgmx_status st = refresh_traces(d);
@@ -573,7 +597,8 @@ int dgmx_kernel_list(int *rows, int cap) {
 dgmx_status dgmx_autotune(dgmx_domain *d, int reps, double *rows, int cap, int *nvariants, int *chosen) {
   if (!d || reps <= 0) return DGMX_ERR_ARGUMENT;
   cudaSetDevice(d->prm.device);
-  const std::vector<KernelOps> *vs = find_variants(d->prm.physics, d->L, d->Q);
+  const std::vector<KernelOps> *vs =
+      find_variants(d->prm.physics + (d->mixed() ? kMixedKey : 0), d->L, d->Q);
   if (!vs || vs->empty()) return d->fail(DGMX_ERR_UNSUPPORTED, "no kernel variants");
   double *scratch = nullptr;
   cudaError_t e = dalloc(&scratch, d->nmodal());
@@ -590,6 +615,7 @@ dgmx_status dgmx_autotune(dgmx_domain *d, int reps, double *rows, int cap, int *
     StageArgs a = d->base_args();
     a.kind = kRHS; a.X = d->U; a.U = d->U; a.Ut = d->Ut; a.A = scratch;
     a.Tin = d->T[d->tcur]; a.Tout = d->T[d->tcur ^ 1];
+    if (d->mixed()) { a.Utf = d->Utf; a.Tinf = d->Tf[d->tcur]; a.Toutf = d->Tf[d->tcur ^ 1]; }
     for (int w = 0; w < 2; ++w) e = v.stage(a, d->stream);
     cudaEventRecord(e0, d->stream);
     for (int r = 0; r < reps && e == cudaSuccess; ++r) e = v.stage(a, d->stream);
@@ -611,7 +637,7 @@ dgmx_status dgmx_autotune(dgmx_domain *d, int reps, double *rows, int cap, int *
   if (st != DGMX_OK) return st;
   const KernelOps &chosen_ops = (*vs)[best];
   if ((e = chosen_ops.init(d->tab)) != cudaSuccess) return d->cuda(e, "variant init");
-  d->ops = &chosen_ops;
+  if (d->mixed()) d->ops_m = &chosen_ops; else d->ops = &chosen_ops;
   if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
   if (nvariants) *nvariants = (int)vs->size();
   if (chosen) *chosen = best;

@@ -110,18 +110,26 @@ struct StageArgs {
   double *Rcap;           // if set, the projected RHS is stored here (modal)
   const double *Rsub;     // if set, subtracted from the projected RHS
   // Navier-Stokes BR1 (src/Navier_Stokes3d.cpp:182-391)
+  // mixed-precision form: FP32 second register and traces
+  float *Utf;
+  const float *Tinf;
+  float *Toutf;
   double *Ghat;           // projected primitive gradients, modal [e][comp][dir][L^d]
   double *V;              // viscous normal-flux traces [e][face][field-1][gf]
   double *Pv;             // projected viscous divergence, modal [e][field-1][L^d]
 };
 
+// Registry key offset of the mixed-precision (FP32 working precision) tiles.
+constexpr int kMixedKey = 1000;
+
 // Launchers for one (physics, L, Q) instantiation; all enqueue on stream s.
 struct KernelOps {
-  int epb = 0, nt = 0, minb = 0;
+  int epb = 0, nt = 0, minb = 0, mixed = 0;
   size_t smem = 0;
   cudaError_t (*init)(const Tables1D &t) = nullptr;   // tables + smem attributes, current device
   cudaError_t (*stage)(const StageArgs &a, cudaStream_t s) = nullptr;
-  cudaError_t (*traces_modal)(const StageArgs &a, const double *Xm, double *T, cudaStream_t s) = nullptr;
+  // T is double* (FP64 tiles) or float* (mixed tiles)
+  cudaError_t (*traces_modal)(const StageArgs &a, const double *Xm, void *T, cudaStream_t s) = nullptr;
   cudaError_t (*traces_nodal)(const StageArgs &a, cudaStream_t s) = nullptr;
   cudaError_t (*rhs_nodal)(const StageArgs &a, cudaStream_t s) = nullptr;
   cudaError_t (*forward)(const StageArgs &a, const double *Un, double *Um, cudaStream_t s) = nullptr;

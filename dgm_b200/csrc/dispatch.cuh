@@ -6,35 +6,42 @@
 
 namespace dgmx {
 
-template <int L, int Q>
+template <int L, int Q, class T>
 cudaError_t upload_tables_lq(const Tables1D &t) {
+  auto put = [](const auto &sym, const std::vector<double> &v, size_t n) {
+    std::vector<T> c(n);
+    for (size_t i = 0; i < n; ++i) c[i] = T(v[i]);
+    return cudaMemcpyToSymbol(sym, c.data(), sizeof(T) * n);
+  };
   cudaError_t e;
-  if ((e = cudaMemcpyToSymbol(cB<L, Q>, t.B.data(), sizeof(double) * L * Q)) != cudaSuccess) return e;
-  if ((e = cudaMemcpyToSymbol(cBg<L, Q>, t.Bg.data(), sizeof(double) * L * (Q - 1))) != cudaSuccess) return e;
-  if ((e = cudaMemcpyToSymbol(cD<L, Q>, t.D.data(), sizeof(double) * Q * Q)) != cudaSuccess) return e;
-  if ((e = cudaMemcpyToSymbol(cG2GL<L, Q>, t.g2gl.data(), sizeof(double) * Q * (Q - 1))) != cudaSuccess) return e;
-  if ((e = cudaMemcpyToSymbol(cGL2G<L, Q>, t.gl2g.data(), sizeof(double) * (Q - 1) * Q)) != cudaSuccess) return e;
-  if ((e = cudaMemcpyToSymbol(cW<L, Q>, t.w.data(), sizeof(double) * Q)) != cudaSuccess) return e;
-  double end[2 * L];
+  if ((e = put(cB<T, L, Q>, t.B, (size_t)L * Q)) != cudaSuccess) return e;
+  if ((e = put(cBg<T, L, Q>, t.Bg, (size_t)L * (Q - 1))) != cudaSuccess) return e;
+  if ((e = put(cD<T, L, Q>, t.D, (size_t)Q * Q)) != cudaSuccess) return e;
+  if ((e = put(cG2GL<T, L, Q>, t.g2gl, (size_t)Q * (Q - 1))) != cudaSuccess) return e;
+  if ((e = put(cGL2G<T, L, Q>, t.gl2g, (size_t)(Q - 1) * Q)) != cudaSuccess) return e;
+  if ((e = put(cW<T, L, Q>, t.w, (size_t)Q)) != cudaSuccess) return e;
+  std::vector<double> end(2 * L);
   for (int a = 0; a < L; ++a) { end[a] = t.B[a * Q + 0]; end[L + a] = t.B[a * Q + Q - 1]; }
-  return cudaMemcpyToSymbol(cEnd<L, Q>, end, sizeof(end));
+  return put(cEnd<T, L, Q>, end, (size_t)2 * L);
 }
 
-template <int PHYS, int L, int Q, int EPB, int MINB>
+template <int PHYS, int L, int Q, int EPB, int MINB, bool MIXED = false>
 struct Launch {
-  using C = Cfg<PHYS, L, Q, EPB, MINB>;
+  using C = Cfg<PHYS, L, Q, EPB, MINB, MIXED>;
   static dim3 grid(int ne) { return dim3((unsigned)((ne + EPB - 1) / EPB)); }
   static cudaError_t init(const Tables1D &t) {
-    cudaError_t e = upload_tables_lq<L, Q>(t);
+    cudaError_t e = upload_tables_lq<L, Q, typename C::R>(t);
     if (e != cudaSuccess) return e;
     const int sm = (int)C::SMEM;
     if ((e = cudaFuncSetAttribute(stage_kernel<C, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
     if ((e = cudaFuncSetAttribute(traces_modal_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-    if ((e = cudaFuncSetAttribute(traces_nodal_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-    if ((e = cudaFuncSetAttribute(rhs_nodal_kernel<C, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-    if ((e = cudaFuncSetAttribute(forward_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-    if ((e = cudaFuncSetAttribute(backward_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-    if constexpr (is_ns(PHYS)) {
+    if constexpr (!MIXED) {
+      if ((e = cudaFuncSetAttribute(traces_nodal_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+      if ((e = cudaFuncSetAttribute(rhs_nodal_kernel<C, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+      if ((e = cudaFuncSetAttribute(forward_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+      if ((e = cudaFuncSetAttribute(backward_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+    }
+    if constexpr (is_ns(PHYS) && !MIXED) {
       using N = NsCfg<C>;
       const int sg = (int)N::Grad::SMEM, sv = (int)N::Visc::SMEM;
       if ((e = cudaFuncSetAttribute(ns_grad_kernel<C, PHYS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
@@ -45,7 +52,7 @@ struct Launch {
     return cudaSuccess;
   }
   static cudaError_t ns_grad(const StageArgs &a, bool nodal, cudaStream_t s) {
-    if constexpr (is_ns(PHYS)) {
+    if constexpr (is_ns(PHYS) && !MIXED) {
       using N = NsCfg<C>;
       if (nodal) ns_grad_kernel<C, PHYS, true><<<grid(a.ne), C::NT, N::Grad::SMEM, s>>>(a);
       else ns_grad_kernel<C, PHYS, false><<<grid(a.ne), C::NT, N::Grad::SMEM, s>>>(a);
@@ -55,7 +62,7 @@ struct Launch {
     }
   }
   static cudaError_t ns_visc(const StageArgs &a, bool nodal, cudaStream_t s) {
-    if constexpr (is_ns(PHYS)) {
+    if constexpr (is_ns(PHYS) && !MIXED) {
       using N = NsCfg<C>;
       if (nodal) ns_visc_kernel<C, PHYS, true><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
       else ns_visc_kernel<C, PHYS, false><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
@@ -68,32 +75,48 @@ struct Launch {
     stage_kernel<C, PHYS><<<grid(a.ne), C::NT, C::SMEM, s>>>(a);
     return cudaGetLastError();
   }
-  static cudaError_t traces_modal(const StageArgs &a, const double *X, double *T, cudaStream_t s) {
-    traces_modal_kernel<C><<<grid(a.ne), C::NT, C::SMEM, s>>>(a, X, T);
+  static cudaError_t traces_modal(const StageArgs &a, const double *X, void *T, cudaStream_t s) {
+    traces_modal_kernel<C><<<grid(a.ne), C::NT, C::SMEM, s>>>(a, X, static_cast<typename C::R *>(T));
     return cudaGetLastError();
   }
   static cudaError_t traces_nodal(const StageArgs &a, cudaStream_t s) {
-    traces_nodal_kernel<C><<<grid(a.ne), C::NT, C::SMEM, s>>>(a);
-    return cudaGetLastError();
+    if constexpr (!MIXED) {
+      traces_nodal_kernel<C><<<grid(a.ne), C::NT, C::SMEM, s>>>(a);
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
   }
   static cudaError_t rhs_nodal(const StageArgs &a, cudaStream_t s) {
-    rhs_nodal_kernel<C, PHYS><<<grid(a.ne), C::NT, C::SMEM, s>>>(a);
-    return cudaGetLastError();
+    if constexpr (!MIXED) {
+      rhs_nodal_kernel<C, PHYS><<<grid(a.ne), C::NT, C::SMEM, s>>>(a);
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
   }
   static cudaError_t forward(const StageArgs &a, const double *Un, double *Um, cudaStream_t s) {
-    forward_kernel<C><<<grid(a.ne), C::NT, C::SMEM, s>>>(a, Un, Um);
-    return cudaGetLastError();
+    if constexpr (!MIXED) {
+      forward_kernel<C><<<grid(a.ne), C::NT, C::SMEM, s>>>(a, Un, Um);
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
   }
   static cudaError_t backward(const StageArgs &a, const double *Um, double *Un, cudaStream_t s) {
-    backward_kernel<C><<<grid(a.ne), C::NT, C::SMEM, s>>>(a, Um, Un);
-    return cudaGetLastError();
+    if constexpr (!MIXED) {
+      backward_kernel<C><<<grid(a.ne), C::NT, C::SMEM, s>>>(a, Um, Un);
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
   }
   static KernelOps ops() {
     KernelOps o;
-    o.epb = EPB; o.nt = C::NT; o.smem = C::SMEM; o.minb = MINB;
+    o.epb = EPB; o.nt = C::NT; o.smem = C::SMEM; o.minb = MINB; o.mixed = MIXED;
     o.init = init; o.stage = stage; o.traces_modal = traces_modal; o.traces_nodal = traces_nodal;
     o.rhs_nodal = rhs_nodal; o.forward = forward; o.backward = backward;
-    if constexpr (is_ns(PHYS)) { o.ns_grad = ns_grad; o.ns_visc = ns_visc; }
+    if constexpr (is_ns(PHYS) && !MIXED) { o.ns_grad = ns_grad; o.ns_visc = ns_visc; }
     return o;
   }
 };
@@ -118,30 +141,30 @@ constexpr bool ns_fits() {
 
 // Register variant (EPB, MINB) when it is distinct and sensible: the
 // register cap 64K/(NT*MINB) stays >= 48 and the tile fits shared memory.
-template <int PHYS, int P, int Q, int EPB, int MINB>
+template <int PHYS, int P, int Q, int EPB, int MINB, bool MIXED>
 void reg_variant() {
-  using C = Cfg<PHYS, P + 1, Q, EPB, MINB>;
+  using C = Cfg<PHYS, P + 1, Q, EPB, MINB, MIXED>;
   if constexpr (ns_fits<PHYS, C>() && (MINB == 0 || (65536 / (C::NT * MINB) >= 48 && smem_blocks<C>() >= MINB))) {
-    register_ops(PHYS, P + 1, Q, Launch<PHYS, P + 1, Q, EPB, MINB>::ops());
+    register_ops(PHYS + (MIXED ? kMixedKey : 0), P + 1, Q, Launch<PHYS, P + 1, Q, EPB, MINB, MIXED>::ops());
   }
 }
 
 // Tile variants for (physics, p, q): the default packing without and with a
 // register cap at the shared-memory occupancy, and twice the packing.  The
 // first registered variant is the default; dgmx_autotune picks among all.
-template <int PHYS, int P, int Q>
+template <int PHYS, int P, int Q, bool MIXED = false>
 void reg() {
   constexpr int E1 = default_epb(phys_dim(PHYS), Q);
-  using C1 = Cfg<PHYS, P + 1, Q, E1, 0>;
+  using C1 = Cfg<PHYS, P + 1, Q, E1, 0, MIXED>;
   constexpr int B1 = smem_blocks<C1>() > 8 ? 8 : smem_blocks<C1>();
-  reg_variant<PHYS, P, Q, E1, 0>();
-  if constexpr (B1 >= 2) reg_variant<PHYS, P, Q, E1, B1>();
-  if constexpr (B1 >= 4) reg_variant<PHYS, P, Q, E1, (B1 * 3) / 4>();
+  reg_variant<PHYS, P, Q, E1, 0, MIXED>();
+  if constexpr (B1 >= 2) reg_variant<PHYS, P, Q, E1, B1, MIXED>();
+  if constexpr (B1 >= 4) reg_variant<PHYS, P, Q, E1, (B1 * 3) / 4, MIXED>();
   constexpr int E2 = 2 * E1;
-  if constexpr (Cfg<PHYS, P + 1, Q, E2, 0>::NT <= 1024 && Cfg<PHYS, P + 1, Q, E2, 0>::SMEM <= 200 * 1024) {
-    using C2 = Cfg<PHYS, P + 1, Q, E2, 0>;
+  if constexpr (Cfg<PHYS, P + 1, Q, E2, 0, MIXED>::NT <= 1024 && Cfg<PHYS, P + 1, Q, E2, 0, MIXED>::SMEM <= 200 * 1024) {
+    using C2 = Cfg<PHYS, P + 1, Q, E2, 0, MIXED>;
     constexpr int B2 = smem_blocks<C2>() > 8 ? 8 : smem_blocks<C2>();
-    if constexpr (B2 >= 2) reg_variant<PHYS, P, Q, E2, B2>();
+    if constexpr (B2 >= 2) reg_variant<PHYS, P, Q, E2, B2, MIXED>();
   }
 }
 

@@ -14,31 +14,32 @@ struct Pow { static constexpr int v = B * Pow<B, E - 1>::v; };
 template <int B>
 struct Pow<B, 0> { static constexpr int v = 1; };
 
-// 1-D tables for one (L, Q) pair in constant memory.  With the contraction
-// loops fully unrolled the indices are compile-time constants, so the
+// 1-D tables for one (L, Q) pair in constant memory, in the working
+// precision T of the kernels that use them.  With the contraction loops
+// fully unrolled the indices are compile-time constants, so the
 // coefficients become constant-bank operands of the FMAs.
-template <int L, int Q> __constant__ double cB[L * Q];          // B[a*Q+i]
-template <int L, int Q> __constant__ double cBg[L * (Q - 1)];   // Bg[a*G+g]
-template <int L, int Q> __constant__ double cD[Q * Q];          // D[i*Q+m]
-template <int L, int Q> __constant__ double cG2GL[Q * (Q - 1)]; // [i*G+g]
-template <int L, int Q> __constant__ double cGL2G[(Q - 1) * Q]; // [g*Q+i]
-template <int L, int Q> __constant__ double cW[Q];              // GLL weights
-template <int L, int Q> __constant__ double cEnd[2 * L];        // B[a][0], B[a][Q-1]
+template <class T, int L, int Q> __constant__ T cB[L * Q];          // B[a*Q+i]
+template <class T, int L, int Q> __constant__ T cBg[L * (Q - 1)];   // Bg[a*G+g]
+template <class T, int L, int Q> __constant__ T cD[Q * Q];          // D[i*Q+m]
+template <class T, int L, int Q> __constant__ T cG2GL[Q * (Q - 1)]; // [i*G+g]
+template <class T, int L, int Q> __constant__ T cGL2G[(Q - 1) * Q]; // [g*Q+i]
+template <class T, int L, int Q> __constant__ T cW[Q];              // GLL weights
+template <class T, int L, int Q> __constant__ T cEnd[2 * L];        // B[a][0], B[a][Q-1]
 
 // Matrix accessors: M::get(in_index, out_index)
-template <int L, int Q> struct MatB   { static __device__ __forceinline__ double get(int a, int i) { return cB<L, Q>[a * Q + i]; } };
-template <int L, int Q> struct MatBt  { static __device__ __forceinline__ double get(int i, int a) { return cB<L, Q>[a * Q + i]; } };
-template <int L, int Q> struct MatBg  { static __device__ __forceinline__ double get(int a, int g) { return cBg<L, Q>[a * (Q - 1) + g]; } };
-template <int L, int Q> struct MatD   { static __device__ __forceinline__ double get(int m, int i) { return cD<L, Q>[i * Q + m]; } };
-template <int L, int Q> struct MatG2GL{ static __device__ __forceinline__ double get(int g, int i) { return cG2GL<L, Q>[i * (Q - 1) + g]; } };
-template <int L, int Q> struct MatGL2G{ static __device__ __forceinline__ double get(int i, int g) { return cGL2G<L, Q>[g * Q + i]; } };
+template <int L, int Q, class T = double> struct MatB   { static __device__ __forceinline__ T get(int a, int i) { return cB<T, L, Q>[a * Q + i]; } };
+template <int L, int Q, class T = double> struct MatBt  { static __device__ __forceinline__ T get(int i, int a) { return cB<T, L, Q>[a * Q + i]; } };
+template <int L, int Q, class T = double> struct MatBg  { static __device__ __forceinline__ T get(int a, int g) { return cBg<T, L, Q>[a * (Q - 1) + g]; } };
+template <int L, int Q, class T = double> struct MatD   { static __device__ __forceinline__ T get(int m, int i) { return cD<T, L, Q>[i * Q + m]; } };
+template <int L, int Q, class T = double> struct MatG2GL{ static __device__ __forceinline__ T get(int g, int i) { return cG2GL<T, L, Q>[i * (Q - 1) + g]; } };
+template <int L, int Q, class T = double> struct MatGL2G{ static __device__ __forceinline__ T get(int i, int g) { return cGL2G<T, L, Q>[g * Q + i]; } };
 
 // Contraction along axis AX of a batch of 3-D arrays (I0, I1, I2) with
 // I_AX = K: out[...n...] = sum_k M(k, n) in[...k...], N outputs per pencil.
 // Each thread owns one pencil: K loads, K*N FMAs with uniform coefficients.
 // Batch b reads in + b*sin and writes out + b*sout.
-template <int I0, int I1, int I2, int AX, int K, int N, class M, bool ACC>
-__device__ __forceinline__ void contract(const double *__restrict__ in, double *__restrict__ out, int nbatch,
+template <int I0, int I1, int I2, int AX, int K, int N, class M, bool ACC, class T>
+__device__ __forceinline__ void contract(const T *__restrict__ in, T *__restrict__ out, int nbatch,
                                          int sin, int sout, int tid, int nthr) {
   constexpr int O1 = AX == 1 ? N : I1, O2 = AX == 2 ? N : I2;
   constexpr int P0 = AX == 0 ? I1 : I0;
@@ -55,14 +56,14 @@ __device__ __forceinline__ void contract(const double *__restrict__ in, double *
     if (AX == 0) { io = pa * is1 + pb; oo = pa * os1 + pb; }
     else if (AX == 1) { io = pa * is0 + pb; oo = pa * os0 + pb; }
     else { io = pa * is0 + pb * is1; oo = pa * os0 + pb * os1; }
-    const double *src = in + (size_t)b * sin + io;
-    double *dst = out + (size_t)b * sout + oo;
-    double v[K];
+    const T *src = in + (size_t)b * sin + io;
+    T *dst = out + (size_t)b * sout + oo;
+    T v[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] = src[k * isA];
 #pragma unroll
     for (int n = 0; n < N; ++n) {
-      double acc = 0.0;
+      T acc = T(0);
 #pragma unroll
       for (int k = 0; k < K; ++k) acc = fma(M::get(k, n), v[k], acc);
       if (ACC) dst[n * osA] += acc; else dst[n * osA] = acc;
@@ -77,28 +78,28 @@ __device__ constexpr double kAeps = 4.8148248609680896e-11;
 // Physical flux components for one point.  Operation order follows the
 // reference volume loops (src/Euler.cpp:335-384, src/Euler3d.cpp:506-566,
 // src/Shallow.cpp:305-339).  Fills F[d][n] for d < DIM.
-template <int PHYS>
-__device__ __forceinline__ void volume_flux(const double *U, double gamma, double (*F)[5]) {
+template <int PHYS, class T>
+__device__ __forceinline__ void volume_flux(const T *U, T gamma, T (*F)[5]) {
   if constexpr (PHYS == DGMX_EULER2D || PHYS == DGMX_NS2D) {
-    const double gm1 = gamma - 1.0, m5g = -0.5 * gm1;
-    const double r = U[0], ru = U[1], rv = U[2], rE = U[3];
-    const double ir = 1.0 / r;
-    const double u = ru * ir, v = rv * ir;
-    double p = u * ru;
+    const T gm1 = gamma - T(1.0), m5g = -T(0.5) * gm1;
+    const T r = U[0], ru = U[1], rv = U[2], rE = U[3];
+    const T ir = T(1.0) / r;
+    const T u = ru * ir, v = rv * ir;
+    T p = u * ru;
     p = v * rv + p;
     p = m5g * p;
     p = fma(gm1, rE, p);
     F[0][0] = ru;            F[1][0] = rv;
     F[0][1] = ru * u + p;    F[1][1] = ru * v;
     F[0][2] = rv * u;        F[1][2] = rv * v + p;
-    const double e = rE + p;
+    const T e = rE + p;
     F[0][3] = u * e;         F[1][3] = v * e;
   } else if constexpr (PHYS == DGMX_EULER3D || PHYS == DGMX_NS3D) {
-    const double gm1 = gamma - 1.0, m5g = -0.5 * gm1;
-    const double r = U[0], ru = U[1], rv = U[2], rw = U[3], rE = U[4];
-    const double ir = 1.0 / r;
-    const double u = ru * ir, v = rv * ir, w = rw * ir;
-    double p = u * ru;
+    const T gm1 = gamma - T(1.0), m5g = -T(0.5) * gm1;
+    const T r = U[0], ru = U[1], rv = U[2], rw = U[3], rE = U[4];
+    const T ir = T(1.0) / r;
+    const T u = ru * ir, v = rv * ir, w = rw * ir;
+    T p = u * ru;
     p = fma(v, rv, p);
     p = fma(w, rw, p);
     p = m5g * p;
@@ -107,13 +108,13 @@ __device__ __forceinline__ void volume_flux(const double *U, double gamma, doubl
     F[0][1] = fma(ru, u, p); F[1][1] = ru * v;        F[2][1] = ru * w;
     F[0][2] = rv * u;        F[1][2] = fma(rv, v, p); F[2][2] = rv * w;
     F[0][3] = rw * u;        F[1][3] = rw * v;        F[2][3] = fma(rw, w, p);
-    const double e = rE + p;
+    const T e = rE + p;
     F[0][4] = u * e; F[1][4] = v * e; F[2][4] = w * e;
   } else {  // shallow water, geopotential form
-    const double phi = U[0], uphi = U[1], vphi = U[2];
-    const double iphi = 1.0 / phi;
-    const double u = uphi * iphi, v = vphi * iphi;
-    const double p = 0.5 * (phi * phi);
+    const T phi = U[0], uphi = U[1], vphi = U[2];
+    const T iphi = T(1.0) / phi;
+    const T u = uphi * iphi, v = vphi * iphi;
+    const T p = T(0.5) * (phi * phi);
     F[0][0] = uphi;            F[1][0] = vphi;
     F[0][1] = fma(uphi, u, p); F[1][1] = uphi * v;
     F[0][2] = vphi * u;        F[1][2] = fma(vphi, v, p);
@@ -127,43 +128,43 @@ __device__ __forceinline__ void volume_flux(const double *U, double gamma, doubl
 // Euler 2-D: src/Euler.cpp:443-741 (LF and Roe); Euler 3-D:
 // src/Euler3d.cpp:601-816 (LF) plus the rotated-frame Roe extension;
 // shallow water: src/Shallow.cpp:380-510.
-template <int PHYS>
-__device__ __forceinline__ bool face_flux(const double *UL, const double *UR, const double *n, double gamma,
-                                          int flux, double *Fh, double *FL, double *FR) {
+template <int PHYS, class T>
+__device__ __forceinline__ bool face_flux(const T *UL, const T *UR, const T *n, T gamma,
+                                          int flux, T *Fh, T *FL, T *FR) {
   bool ok = true;
   if constexpr (PHYS == DGMX_EULER2D || PHYS == DGMX_NS2D) {
-    const double gm1 = gamma - 1.0;
-    const double nx = n[0], ny = n[1];
-    const double rl = UL[0], rul = UL[1] * nx + UL[2] * ny, rvl = UL[2] * nx - UL[1] * ny, rEl = UL[3];
-    const double irl = 1.0 / rl, ul = irl * rul, vl = irl * rvl;
-    const double pl = gm1 * (rEl - 0.5 * (rul * ul + rvl * vl));
-    const double Hl = irl * (rEl + pl);
-    ok = ok && rl >= kAeps && pl >= kAeps;
+    const T gm1 = gamma - T(1.0);
+    const T nx = n[0], ny = n[1];
+    const T rl = UL[0], rul = UL[1] * nx + UL[2] * ny, rvl = UL[2] * nx - UL[1] * ny, rEl = UL[3];
+    const T irl = T(1.0) / rl, ul = irl * rul, vl = irl * rvl;
+    const T pl = gm1 * (rEl - T(0.5) * (rul * ul + rvl * vl));
+    const T Hl = irl * (rEl + pl);
+    ok = ok && rl >= T(kAeps) && pl >= T(kAeps);
     FL[0] = rul;
     FL[1] = (rul * ul + pl) * nx - (rvl * ul) * ny;
     FL[2] = (rul * ul + pl) * ny + (rvl * ul) * nx;
     FL[3] = ul * (rEl + pl);
-    const double rr = UR[0], rur = UR[1] * nx + UR[2] * ny, rvr = UR[2] * nx - UR[1] * ny, rEr = UR[3];
-    const double irr = 1.0 / rr, ur = irr * rur, vr = irr * rvr;
-    const double pr = gm1 * (rEr - 0.5 * (rur * ur + rvr * vr));
-    const double Hr = irr * (rEr + pr);
-    ok = ok && rr >= kAeps && pr >= kAeps;
+    const T rr = UR[0], rur = UR[1] * nx + UR[2] * ny, rvr = UR[2] * nx - UR[1] * ny, rEr = UR[3];
+    const T irr = T(1.0) / rr, ur = irr * rur, vr = irr * rvr;
+    const T pr = gm1 * (rEr - T(0.5) * (rur * ur + rvr * vr));
+    const T Hr = irr * (rEr + pr);
+    ok = ok && rr >= T(kAeps) && pr >= T(kAeps);
     FR[0] = rr * ur;
     FR[1] = (rur * ur + pr) * nx - (rvr * ur) * ny;
     FR[2] = (rur * ur + pr) * ny + (rvr * ur) * nx;
     FR[3] = ur * (rEr + pr);
     if (flux == DGMX_FLUX_ROE) {
-      const double R = sqrt(rr / rl), iRp1 = 1.0 / (1.0 + R);
-      const double u = (ul + R * ur) * iRp1, v = (vl + R * vr) * iRp1, H = (Hl + R * Hr) * iRp1;
-      const double a = sqrt(gm1 * (H - 0.5 * (u * u + v * v)));
-      const double ainv = 1.0 / a, c1inv = 1.0 / (gm1 * ainv * ainv);
-      double al[4], G[4];
+      const T R = sqrt(rr / rl), iRp1 = T(1.0) / (T(1.0) + R);
+      const T u = (ul + R * ur) * iRp1, v = (vl + R * vr) * iRp1, H = (Hl + R * Hr) * iRp1;
+      const T a = sqrt(gm1 * (H - T(0.5) * (u * u + v * v)));
+      const T ainv = T(1.0) / a, c1inv = T(1.0) / (gm1 * ainv * ainv);
+      T al[4], G[4];
       al[2] = (rvr - rvl) - v * (rr - rl);
       al[1] = gm1 * ainv * ainv * ((rr - rl) * (H - u * u) + u * (rur - rul) -
                                    ((rEr - rEl) - ((rvr - rvl) - v * (rr - rl)) * v));
-      al[0] = 0.5 * ainv * ((rr - rl) * (u + a) - (rur - rul) - a * al[1]);
+      al[0] = T(0.5) * ainv * ((rr - rl) * (u + a) - (rur - rul) - a * al[1]);
       al[3] = (rr - rl) - (al[0] + al[1]);
-      const double l0 = fmin(u - a, 0.0), l1 = fmin(u, 0.0), l3 = fmin(u + a, 0.0);
+      const T l0 = fmin(u - a, T(0.0)), l1 = fmin(u, T(0.0)), l3 = fmin(u + a, T(0.0));
       G[0] = l0 * al[0]; G[1] = l0 * (u - a) * al[0]; G[2] = l0 * v * al[0]; G[3] = l0 * (H - u * a) * al[0];
       G[0] += l1 * al[1]; G[1] += l1 * u * al[1]; G[2] += l1 * v * al[1]; G[3] += l1 * (H - c1inv) * al[1];
       G[2] += l1 * al[2]; G[3] += l1 * v * al[2];
@@ -173,54 +174,54 @@ __device__ __forceinline__ bool face_flux(const double *UL, const double *UR, co
       Fh[2] = FL[2] + G[1] * ny + G[2] * nx;
       Fh[3] = FL[3] + G[3];
     } else {
-      const double al = sqrt(gm1 * (Hl - 0.5 * (ul * ul + vl * vl)));
-      const double ar = sqrt(gm1 * (Hr - 0.5 * (ur * ur + vr * vr)));
-      double lmax = fmax(fabs(ul - al), fabs(ul));
+      const T al = sqrt(gm1 * (Hl - T(0.5) * (ul * ul + vl * vl)));
+      const T ar = sqrt(gm1 * (Hr - T(0.5) * (ur * ur + vr * vr)));
+      T lmax = fmax(fabs(ul - al), fabs(ul));
       lmax = fmax(lmax, fabs(ul + al));
       lmax = fmax(lmax, fmax(fabs(ur - ar), fabs(ur)));
       lmax = fmax(lmax, fabs(ur + ar));
 #pragma unroll
-      for (int k = 0; k < 4; ++k) Fh[k] = 0.5 * (FL[k] + FR[k] + lmax * (UL[k] - UR[k]));
+      for (int k = 0; k < 4; ++k) Fh[k] = T(0.5) * (FL[k] + FR[k] + lmax * (UL[k] - UR[k]));
     }
   } else if constexpr (PHYS == DGMX_EULER3D || PHYS == DGMX_NS3D) {
-    const double gm1 = gamma - 1.0;
-    const double nx = n[0], ny = n[1], nz = n[2];
-    double sx = ny, sy = nz, sz = nx;
-    const double sdn = nx * sx + ny * sy + nz * sz;
+    const T gm1 = gamma - T(1.0);
+    const T nx = n[0], ny = n[1], nz = n[2];
+    T sx = ny, sy = nz, sz = nx;
+    const T sdn = nx * sx + ny * sy + nz * sz;
     sx -= sdn * nx; sy -= sdn * ny; sz -= sdn * nz;
-    const double sni = 1.0 / sqrt(sx * sx + sy * sy + sz * sz);
+    const T sni = T(1.0) / sqrt(sx * sx + sy * sy + sz * sz);
     sx *= sni; sy *= sni; sz *= sni;
-    double tx = ny * sz - sy * nz, ty = nz * sx - sz * nx, tz = nx * sy - sx * ny;
-    const double tni = 1.0 / sqrt(tx * tx + ty * ty + tz * tz);
+    T tx = ny * sz - sy * nz, ty = nz * sx - sz * nx, tz = nx * sy - sx * ny;
+    const T tni = T(1.0) / sqrt(tx * tx + ty * ty + tz * tz);
     tx *= tni; ty *= tni; tz *= tni;
-    const double detA = (nx * sy * tz + sx * ty * nz + tx * sz * ny) - (nz * sy * tx + sz * ty * nx + tz * sx * ny);
-    const double id = 1.0 / detA;
-    const double xn = (sy * tz - sz * ty) * id, yn = -(sx * tz - sz * tx) * id, zn = (sx * ty - sy * tx) * id;
-    const double xs = -(ny * tz - nz * ty) * id, ys = (nx * tz - nz * tx) * id, zs = -(nx * ty - ny * tx) * id;
-    const double xt = (ny * sz - nz * sy) * id, yt = -(nx * sz - nz * sx) * id, zt = (nx * sy - ny * sx) * id;
-    const double rl = UL[0];
-    const double rul = UL[1] * nx + UL[2] * ny + UL[3] * nz;
-    const double rvl = UL[1] * sx + UL[2] * sy + UL[3] * sz;
-    const double rwl = UL[1] * tx + UL[2] * ty + UL[3] * tz;
-    const double rEl = UL[4];
-    const double irl = 1.0 / rl, ul = irl * rul, vl = irl * rvl, wl = irl * rwl;
-    const double pl = gm1 * (rEl - 0.5 * (rul * ul + rvl * vl + rwl * wl));
-    const double Hl = irl * (rEl + pl);
-    ok = ok && rl >= kAeps && pl >= kAeps;
+    const T detA = (nx * sy * tz + sx * ty * nz + tx * sz * ny) - (nz * sy * tx + sz * ty * nx + tz * sx * ny);
+    const T id = T(1.0) / detA;
+    const T xn = (sy * tz - sz * ty) * id, yn = -(sx * tz - sz * tx) * id, zn = (sx * ty - sy * tx) * id;
+    const T xs = -(ny * tz - nz * ty) * id, ys = (nx * tz - nz * tx) * id, zs = -(nx * ty - ny * tx) * id;
+    const T xt = (ny * sz - nz * sy) * id, yt = -(nx * sz - nz * sx) * id, zt = (nx * sy - ny * sx) * id;
+    const T rl = UL[0];
+    const T rul = UL[1] * nx + UL[2] * ny + UL[3] * nz;
+    const T rvl = UL[1] * sx + UL[2] * sy + UL[3] * sz;
+    const T rwl = UL[1] * tx + UL[2] * ty + UL[3] * tz;
+    const T rEl = UL[4];
+    const T irl = T(1.0) / rl, ul = irl * rul, vl = irl * rvl, wl = irl * rwl;
+    const T pl = gm1 * (rEl - T(0.5) * (rul * ul + rvl * vl + rwl * wl));
+    const T Hl = irl * (rEl + pl);
+    ok = ok && rl >= T(kAeps) && pl >= T(kAeps);
     FL[0] = rl * ul;
     FL[1] = (rul * ul + pl) * xn + (rvl * ul) * xs + (rwl * ul) * xt;
     FL[2] = (rul * ul + pl) * yn + (rvl * ul) * ys + (rwl * ul) * yt;
     FL[3] = (rul * ul + pl) * zn + (rvl * ul) * zs + (rwl * ul) * zt;
     FL[4] = ul * (rEl + pl);
-    const double rr = UR[0];
-    const double rur = UR[1] * nx + UR[2] * ny + UR[3] * nz;
-    const double rvr = UR[1] * sx + UR[2] * sy + UR[3] * sz;
-    const double rwr = UR[1] * tx + UR[2] * ty + UR[3] * tz;
-    const double rEr = UR[4];
-    const double irr = 1.0 / rr, ur = irr * rur, vr = irr * rvr, wr = irr * rwr;
-    const double pr = gm1 * (rEr - 0.5 * (rur * ur + rvr * vr + rwr * wr));
-    const double Hr = irr * (rEr + pr);
-    ok = ok && rr >= kAeps && pr >= kAeps;
+    const T rr = UR[0];
+    const T rur = UR[1] * nx + UR[2] * ny + UR[3] * nz;
+    const T rvr = UR[1] * sx + UR[2] * sy + UR[3] * sz;
+    const T rwr = UR[1] * tx + UR[2] * ty + UR[3] * tz;
+    const T rEr = UR[4];
+    const T irr = T(1.0) / rr, ur = irr * rur, vr = irr * rvr, wr = irr * rwr;
+    const T pr = gm1 * (rEr - T(0.5) * (rur * ur + rvr * vr + rwr * wr));
+    const T Hr = irr * (rEr + pr);
+    ok = ok && rr >= T(kAeps) && pr >= T(kAeps);
     FR[0] = rr * ur;
     FR[1] = (rur * ur + pr) * xn + (rvr * ur) * xs + (rwr * ur) * xt;
     FR[2] = (rur * ur + pr) * yn + (rvr * ur) * ys + (rwr * ur) * yt;
@@ -229,19 +230,19 @@ __device__ __forceinline__ bool face_flux(const double *UL, const double *UR, co
     if (flux == DGMX_FLUX_ROE) {
       // Roe average in the (n, s, t) frame; the 2-D Roe of src/Euler.cpp
       // with a second tangential velocity carried like the first.
-      const double R = sqrt(rr / rl), iRp1 = 1.0 / (1.0 + R);
-      const double u = (ul + R * ur) * iRp1, v = (vl + R * vr) * iRp1, w = (wl + R * wr) * iRp1;
-      const double H = (Hl + R * Hr) * iRp1;
-      const double a2 = gm1 * (H - 0.5 * (u * u + v * v + w * w));
-      const double a = sqrt(a2), ainv = 1.0 / a, c1inv = a2 / gm1;
-      const double dr = rr - rl, dru = rur - rul, drv = rvr - rvl, drw = rwr - rwl, drE = rEr - rEl;
-      double al[5], G[5];
+      const T R = sqrt(rr / rl), iRp1 = T(1.0) / (T(1.0) + R);
+      const T u = (ul + R * ur) * iRp1, v = (vl + R * vr) * iRp1, w = (wl + R * wr) * iRp1;
+      const T H = (Hl + R * Hr) * iRp1;
+      const T a2 = gm1 * (H - T(0.5) * (u * u + v * v + w * w));
+      const T a = sqrt(a2), ainv = T(1.0) / a, c1inv = a2 / gm1;
+      const T dr = rr - rl, dru = rur - rul, drv = rvr - rvl, drw = rwr - rwl, drE = rEr - rEl;
+      T al[5], G[5];
       al[2] = drv - v * dr;
       al[3] = drw - w * dr;
       al[1] = gm1 * ainv * ainv * (dr * (H - u * u) + u * dru - ((drE - al[2] * v - al[3] * w)));
-      al[0] = 0.5 * ainv * (dr * (u + a) - dru - a * al[1]);
+      al[0] = T(0.5) * ainv * (dr * (u + a) - dru - a * al[1]);
       al[4] = dr - (al[0] + al[1]);
-      const double l0 = fmin(u - a, 0.0), l1 = fmin(u, 0.0), l4 = fmin(u + a, 0.0);
+      const T l0 = fmin(u - a, T(0.0)), l1 = fmin(u, T(0.0)), l4 = fmin(u + a, T(0.0));
       G[0] = l0 * al[0]; G[1] = l0 * (u - a) * al[0]; G[2] = l0 * v * al[0]; G[3] = l0 * w * al[0];
       G[4] = l0 * (H - u * a) * al[0];
       G[0] += l1 * al[1]; G[1] += l1 * u * al[1]; G[2] += l1 * v * al[1]; G[3] += l1 * w * al[1];
@@ -256,36 +257,36 @@ __device__ __forceinline__ bool face_flux(const double *UL, const double *UR, co
       Fh[3] = FL[3] + G[1] * zn + G[2] * zs + G[3] * zt;
       Fh[4] = FL[4] + G[4];
     } else {
-      const double al = sqrt(gm1 * (Hl - 0.5 * (ul * ul + vl * vl + wl * wl)));
-      const double ar = sqrt(gm1 * (Hr - 0.5 * (ur * ur + vr * vr + wr * wr)));
-      double lmax = fmax(fabs(ul - al), fabs(ul));
+      const T al = sqrt(gm1 * (Hl - T(0.5) * (ul * ul + vl * vl + wl * wl)));
+      const T ar = sqrt(gm1 * (Hr - T(0.5) * (ur * ur + vr * vr + wr * wr)));
+      T lmax = fmax(fabs(ul - al), fabs(ul));
       lmax = fmax(lmax, fabs(ul + al));
       lmax = fmax(lmax, fmax(fabs(ur - ar), fabs(ur)));
       lmax = fmax(lmax, fabs(ur + ar));
 #pragma unroll
-      for (int k = 0; k < 5; ++k) Fh[k] = 0.5 * (FL[k] + FR[k] + lmax * (UL[k] - UR[k]));
+      for (int k = 0; k < 5; ++k) Fh[k] = T(0.5) * (FL[k] + FR[k] + lmax * (UL[k] - UR[k]));
     }
   } else {  // shallow water LF
-    const double nx = n[0], ny = n[1];
-    const double phil = UL[0], upl = UL[1] * nx + UL[2] * ny, vpl = UL[2] * nx - UL[1] * ny;
-    const double ul = upl / phil, pl = 0.5 * phil * phil;
-    ok = ok && phil >= kAeps && pl >= kAeps;
+    const T nx = n[0], ny = n[1];
+    const T phil = UL[0], upl = UL[1] * nx + UL[2] * ny, vpl = UL[2] * nx - UL[1] * ny;
+    const T ul = upl / phil, pl = T(0.5) * phil * phil;
+    ok = ok && phil >= T(kAeps) && pl >= T(kAeps);
     FL[0] = upl;
     FL[1] = (upl * ul + pl) * nx - (vpl * ul) * ny;
     FL[2] = (upl * ul + pl) * ny + (vpl * ul) * nx;
-    const double phir = UR[0], upr = UR[1] * nx + UR[2] * ny, vpr = UR[2] * nx - UR[1] * ny;
-    const double ur = upr / phir, pr = 0.5 * phir * phir;
-    ok = ok && phir >= kAeps && pr >= kAeps;
+    const T phir = UR[0], upr = UR[1] * nx + UR[2] * ny, vpr = UR[2] * nx - UR[1] * ny;
+    const T ur = upr / phir, pr = T(0.5) * phir * phir;
+    ok = ok && phir >= T(kAeps) && pr >= T(kAeps);
     FR[0] = upr;
     FR[1] = (upr * ur + pr) * nx - (vpr * ur) * ny;
     FR[2] = (upr * ur + pr) * ny + (vpr * ur) * nx;
-    const double al = sqrt(phil), ar = sqrt(phir);
-    double lmax = fmax(fabs(ul - al), fabs(ul));
+    const T al = sqrt(phil), ar = sqrt(phir);
+    T lmax = fmax(fabs(ul - al), fabs(ul));
     lmax = fmax(lmax, fabs(ul + al));
     lmax = fmax(lmax, fmax(fabs(ur - ar), fabs(ur)));
     lmax = fmax(lmax, fabs(ur + ar));
 #pragma unroll
-    for (int k = 0; k < 3; ++k) Fh[k] = 0.5 * (FL[k] + FR[k] + lmax * (UL[k] - UR[k]));
+    for (int k = 0; k < 3; ++k) Fh[k] = T(0.5) * (FL[k] + FR[k] + lmax * (UL[k] - UR[k]));
   }
   return ok;
 }

@@ -111,7 +111,7 @@ __device__ __forceinline__ void lift_batch(const double *Fg, double *LFc, double
     contract<G, 1, 1, 0, G, Q, MatG2GL<L, Q>, false>(Fg, LFc, NBT, G, Q, tid, C::NT);
   }
   __syncthreads();
-  const double w0 = 1.0 / cW<L, Q>[0], w1 = 1.0 / cW<L, Q>[Q - 1];
+  const double w0 = 1.0 / cW<double, L, Q>[0], w1 = 1.0 / cW<double, L, Q>[Q - 1];
   for (int w = tid; w < EPB * NB * QD; w += C::NT) {
     const int slot = w / (NB * QD), rem = w - slot * NB * QD, b = rem / QD, p = rem - b * QD;
     double acc = dst[w];
@@ -145,8 +145,8 @@ __device__ __forceinline__ void forward_batch(double *src, double *dst, double *
   for (int w = tid; w < NBT * QD; w += C::NT) {
     const int p = w % QD;
     double wq;
-    if constexpr (DIM == 3) wq = cW<L, Q>[p / (Q * Q)] * cW<L, Q>[(p / Q) % Q] * cW<L, Q>[p % Q];
-    else wq = cW<L, Q>[p / Q] * cW<L, Q>[p % Q];
+    if constexpr (DIM == 3) wq = cW<double, L, Q>[p / (Q * Q)] * cW<double, L, Q>[(p / Q) % Q] * cW<double, L, Q>[p % Q];
+    else wq = cW<double, L, Q>[p / Q] * cW<double, L, Q>[p % Q];
     src[w] = wq * src[w];
   }
   __syncthreads();
@@ -203,7 +203,8 @@ __global__ void __launch_bounds__(C::NT, C::MINB) ns_grad_kernel(StageArgs a) {
   using R = typename N::Grad;
   constexpr int DIM = C::DIM, NF = C::NF, Q = C::Q, L = C::L, EPB = C::EPB, QD = C::QD, GF = C::GF;
   constexpr int NFACE = C::NFACE, NVC = N::NVC, LD = C::LD;
-  extern __shared__ __align__(16) double smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_bytes[];
+  double *smem_raw = reinterpret_cast<double *>(smem_bytes);
   double *A = smem_raw, *B = A + EPB * R::A, *E = B + EPB * R::B, *E2 = E + EPB * R::E;
   double *Qc = E2 + EPB * R::E2, *Gd = Qc + EPB * R::Qc, *Fc = Gd + EPB * R::Gd, *LFc = Fc + EPB * R::Fc;
   double *S1 = LFc + EPB * R::LFc, *S2 = S1 + EPB * R::S1;
@@ -294,7 +295,8 @@ __global__ void __launch_bounds__(C::NT, C::MINB) ns_visc_kernel(StageArgs a) {
   using R = typename N::Visc;
   constexpr int DIM = C::DIM, NF = C::NF, Q = C::Q, L = C::L, G = C::G, EPB = C::EPB, QD = C::QD;
   constexpr int GF = C::GF, QF = C::QF, NFACE = C::NFACE, NG = N::NG, NV = N::NV, NVC = N::NVC, LD = C::LD;
-  extern __shared__ __align__(16) double smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_bytes[];
+  double *smem_raw = reinterpret_cast<double *>(smem_bytes);
   double *B = smem_raw, *Gg = B + EPB * R::B, *Gh = Gg + EPB * R::G, *FF = Gh + EPB * R::Gh;
   double *Fg = FF + EPB * R::FF, *S1 = Fg + EPB * R::Fg, *S2 = S1 + EPB * R::S1;
   double *Cv = S2 + EPB * R::S2, *Dv = Cv + EPB * R::Cv;

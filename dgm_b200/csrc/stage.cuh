@@ -1,4 +1,5 @@
-// Fused DG stage kernels for sm_100a (FP64).
+// Fused DG stage kernels for sm_100a (FP64, and FP32 with an FP64 solution
+// register for the mixed-precision form).
 //
 // One launch evaluates Domain::time_derivative on a modal register and folds
 // the RK stage update and the next stage's face traces into the same pass:
@@ -23,6 +24,8 @@
 // in place: neighbours only ever read its traces.
 #pragma once
 
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace dgmx {
@@ -34,8 +37,12 @@ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 // One kernel tile: PHYS physics, L modes and Q GLL points per direction,
 // EPB elements per CTA, MINB CTAs per SM requested from the register
 // allocator (__launch_bounds__ minimum blocks; 0 = no request).
-template <int PHYS, int L_, int Q_, int EPB_, int MINB_ = 0>
+template <int PHYS, int L_, int Q_, int EPB_, int MINB_ = 0, bool MIXED_ = false>
 struct Cfg {
+  // working precision: FP64, or FP32 for the mixed form (the solution
+  // register U stays FP64 in global memory)
+  static constexpr bool MIXED = MIXED_;
+  using R = std::conditional_t<MIXED_, float, double>;
   static constexpr int DIM = phys_dim(PHYS), NF = phys_nf(PHYS);
   static constexpr int L = L_, Q = Q_, G = Q_ - 1, EPB = EPB_, MINB = MINB_ > 0 ? MINB_ : 1;
   static constexpr int NFACE = 2 * DIM;
@@ -54,8 +61,8 @@ struct Cfg {
   static constexpr int SZ_R = R_IN_E ? 0 : NF * LD;
   static constexpr int SZ_S = cmax(cmax(NF * Q * LF, NFACE * NF * LF), DIM == 3 ? NFACE * NF * Q * G : 0);
   static constexpr int SZ_SLOT = SZ_A + SZ_B + SZ_C + SZ_D + SZ_E + SZ_R + SZ_S;
-  static constexpr size_t SMEM = (size_t)EPB * SZ_SLOT * sizeof(double) +
-                                 (size_t)EPB * (sizeof(GeomClass) + NFACE * sizeof(FaceLink) + 16);
+  static constexpr size_t DATA = ((size_t)EPB * SZ_SLOT * sizeof(R) + 15) / 16 * 16;
+  static constexpr size_t SMEM = DATA + (size_t)EPB * (sizeof(GeomClass) + NFACE * sizeof(FaceLink) + 16);
   static_assert(NFACE * QF <= 2 * QD, "lift face buffer must fit in the B+C regions");
   static_assert(DIM == 2 || NFACE * G * L <= 2 * QD, "trace intermediate must fit in the B+C regions");
   static_assert(SMEM <= 227 * 1024 || EPB > 1, "element slot does not fit in shared memory");
@@ -66,11 +73,13 @@ template <int DIM, int N> struct Sh3 { static constexpr int a = N, b = N, c = (D
 
 template <class K>
 struct Smem {
-  double *A, *B, *C, *D, *E, *R, *S;
+  using T = typename K::R;
+  T *A, *B, *C, *D, *E, *R, *S;
   GeomClass *geo;
   FaceLink *lnk;
   int *eid;
-  __device__ Smem(double *base) {
+  __device__ Smem(unsigned char *raw) {
+    T *base = reinterpret_cast<T *>(raw);
     A = base;
     B = A + K::EPB * K::SZ_A;
     C = B + K::EPB * K::SZ_B;
@@ -78,7 +87,7 @@ struct Smem {
     E = D + K::EPB * K::SZ_D;
     R = K::R_IN_E ? E : E + K::EPB * K::SZ_E;
     S = E + K::EPB * K::SZ_E + K::EPB * K::SZ_R;
-    geo = reinterpret_cast<GeomClass *>(S + K::EPB * K::SZ_S);
+    geo = reinterpret_cast<GeomClass *>(raw + K::DATA);
     lnk = reinterpret_cast<FaceLink *>(geo + K::EPB);
     eid = reinterpret_cast<int *>(lnk + K::EPB * K::NFACE);
   }
@@ -95,24 +104,26 @@ template <int DIM> __device__ __host__ constexpr int face_end(int f) {
   return DIM == 3 ? (f == 2 || f == 3 || f == 5) : (f == 1 || f == 2);
 }
 
-template <int L, int Q, int END>
-struct MatEnd { static __device__ __forceinline__ double get(int a, int) { return cEnd<L, Q>[END * L + a]; } };
+template <int L, int Q, int END, class T>
+struct MatEnd { static __device__ __forceinline__ T get(int a, int) { return cEnd<T, L, Q>[END * L + a]; } };
 
 // Endpoint reduction of one face for a batch of modal arrays (L^DIM each),
 // output face-local L^(DIM-1) arrays.
 template <class C, int F>
-__device__ __forceinline__ void face_reduce(const double *A, double *out, int tid, int nthr) {
+__device__ __forceinline__ void face_reduce(const typename C::R *A, typename C::R *out, int tid, int nthr) {
   constexpr int DIM = C::DIM, L = C::L, Q = C::Q;
   constexpr int AX = face_axis<DIM>(F), END = face_end<DIM>(F);
   using Sh = Sh3<DIM, L>;
-  contract<Sh::a, Sh::b, Sh::c, AX, L, 1, MatEnd<L, Q, END>, false>(A, out + F * C::EPB * C::NF * C::LF,
+  contract<Sh::a, Sh::b, Sh::c, AX, L, 1, MatEnd<L, Q, END, typename C::R>, false>(A, out + F * C::EPB * C::NF * C::LF,
                                                                      C::EPB * C::NF, C::LD, C::LF, tid, nthr);
 }
 
 // Traces at the side Gauss points of a modal register held in smem A.
 // Result in E, face-major [f][slot][n][gf].  Uses S and B+C as scratch.
 template <class C>
-__device__ __forceinline__ void modal_traces(const double *A, double *E, double *S, double *Cs, int tid, int nthr) {
+__device__ __forceinline__ void modal_traces(const typename C::R *A, typename C::R *E, typename C::R *S,
+                                             typename C::R *Cs, int tid, int nthr) {
+  using T = typename C::R;
   constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G;
   face_reduce<C, 0>(A, S, tid, nthr);
   face_reduce<C, 1>(A, S, tid, nthr);
@@ -125,47 +136,51 @@ __device__ __forceinline__ void modal_traces(const double *A, double *E, double 
   __syncthreads();
   constexpr int NB = C::NFACE * C::EPB * C::NF;
   if constexpr (DIM == 3) {
-    contract<L, L, 1, 0, L, G, MatBg<L, Q>, false>(S, Cs, NB, L * L, G * L, tid, nthr);
+    contract<L, L, 1, 0, L, G, MatBg<L, Q, T>, false>(S, Cs, NB, L * L, G * L, tid, nthr);
     __syncthreads();
-    contract<G, L, 1, 1, L, G, MatBg<L, Q>, false>(Cs, E, NB, G * L, G * G, tid, nthr);
+    contract<G, L, 1, 1, L, G, MatBg<L, Q, T>, false>(Cs, E, NB, G * L, G * G, tid, nthr);
   } else {
-    contract<L, 1, 1, 0, L, G, MatBg<L, Q>, false>(S, E, NB, L, G, tid, nthr);
+    contract<L, 1, 1, 0, L, G, MatBg<L, Q, T>, false>(S, E, NB, L, G, tid, nthr);
   }
   __syncthreads();
 }
 
 // Backward transform: modal A [slot][n][LD] -> GLL B [slot][n][QD].
 template <class C>
-__device__ __forceinline__ void backward(const double *A, double *B, double *S, double *Cs, int tid, int nthr) {
+__device__ __forceinline__ void backward(const typename C::R *A, typename C::R *B, typename C::R *S,
+                                         typename C::R *Cs, int tid, int nthr) {
+  using T = typename C::R;
   constexpr int L = C::L, Q = C::Q, NB = C::EPB * C::NF;
   if constexpr (C::DIM == 3) {
-    contract<L, L, L, 0, L, Q, MatB<L, Q>, false>(A, S, NB, C::LD, Q * L * L, tid, nthr);
+    contract<L, L, L, 0, L, Q, MatB<L, Q, T>, false>(A, S, NB, C::LD, Q * L * L, tid, nthr);
     __syncthreads();
-    contract<Q, L, L, 1, L, Q, MatB<L, Q>, false>(S, Cs, NB, Q * L * L, Q * Q * L, tid, nthr);
+    contract<Q, L, L, 1, L, Q, MatB<L, Q, T>, false>(S, Cs, NB, Q * L * L, Q * Q * L, tid, nthr);
     __syncthreads();
-    contract<Q, Q, L, 2, L, Q, MatB<L, Q>, false>(Cs, B, NB, Q * Q * L, C::QD, tid, nthr);
+    contract<Q, Q, L, 2, L, Q, MatB<L, Q, T>, false>(Cs, B, NB, Q * Q * L, C::QD, tid, nthr);
   } else {
-    contract<L, L, 1, 0, L, Q, MatB<L, Q>, false>(A, S, NB, C::LD, Q * L, tid, nthr);
+    contract<L, L, 1, 0, L, Q, MatB<L, Q, T>, false>(A, S, NB, C::LD, Q * L, tid, nthr);
     __syncthreads();
-    contract<Q, L, 1, 1, L, Q, MatB<L, Q>, false>(S, B, NB, Q * L, C::QD, tid, nthr);
+    contract<Q, L, 1, 1, L, Q, MatB<L, Q, T>, false>(S, B, NB, Q * L, C::QD, tid, nthr);
   }
   __syncthreads();
 }
 
 // Forward projection: GLL D [slot][n][QD] (already w-weighted) -> modal R.
 template <class C>
-__device__ __forceinline__ void forward(const double *D, double *R, double *Cs, double *Bs, int tid, int nthr) {
+__device__ __forceinline__ void forward(const typename C::R *D, typename C::R *R, typename C::R *Cs,
+                                        typename C::R *Bs, int tid, int nthr) {
+  using T = typename C::R;
   constexpr int L = C::L, Q = C::Q, NB = C::EPB * C::NF;
   if constexpr (C::DIM == 3) {
-    contract<Q, Q, Q, 0, Q, L, MatBt<L, Q>, false>(D, Cs, NB, C::QD, L * Q * Q, tid, nthr);
+    contract<Q, Q, Q, 0, Q, L, MatBt<L, Q, T>, false>(D, Cs, NB, C::QD, L * Q * Q, tid, nthr);
     __syncthreads();
-    contract<L, Q, Q, 1, Q, L, MatBt<L, Q>, false>(Cs, Bs, NB, L * Q * Q, L * L * Q, tid, nthr);
+    contract<L, Q, Q, 1, Q, L, MatBt<L, Q, T>, false>(Cs, Bs, NB, L * Q * Q, L * L * Q, tid, nthr);
     __syncthreads();
-    contract<L, L, Q, 2, Q, L, MatBt<L, Q>, false>(Bs, R, NB, L * L * Q, C::LD, tid, nthr);
+    contract<L, L, Q, 2, Q, L, MatBt<L, Q, T>, false>(Bs, R, NB, L * L * Q, C::LD, tid, nthr);
   } else {
-    contract<Q, Q, 1, 0, Q, L, MatBt<L, Q>, false>(D, Cs, NB, C::QD, L * Q, tid, nthr);
+    contract<Q, Q, 1, 0, Q, L, MatBt<L, Q, T>, false>(D, Cs, NB, C::QD, L * Q, tid, nthr);
     __syncthreads();
-    contract<L, Q, 1, 1, Q, L, MatBt<L, Q>, false>(Cs, R, NB, L * Q, C::LD, tid, nthr);
+    contract<L, Q, 1, 1, Q, L, MatBt<L, Q, T>, false>(Cs, R, NB, L * Q, C::LD, tid, nthr);
   }
   __syncthreads();
 }
@@ -174,17 +189,19 @@ __device__ __forceinline__ void forward(const double *D, double *R, double *Cs, 
 // With at most one point per thread the physical fluxes stay in registers
 // across the DIM passes; otherwise they are re-evaluated per pass.
 template <class C, int PHYS>
-__device__ __forceinline__ void volume(const Smem<C> &sm, double gamma, int tid) {
+__device__ __forceinline__ void volume(const Smem<C> &sm, double gamma_, int tid) {
+  using T = typename C::R;
   constexpr int DIM = C::DIM, NF = C::NF, Q = C::Q, QD = C::QD, NB = C::EPB * C::NF;
   constexpr bool ONE = C::EPB * QD <= C::NT;
-  double F[3][5];
+  const T gamma = T(gamma_);
+  T F[3][5];
   if constexpr (ONE) {
     if (tid < C::EPB * QD) {
       const int slot = tid / QD, p = tid - slot * QD;
-      double U[5];
+      T U[5];
 #pragma unroll
       for (int n = 0; n < NF; ++n) U[n] = sm.B[(slot * NF + n) * QD + p];
-      volume_flux<PHYS>(U, gamma, F);
+      volume_flux<PHYS, T>(U, gamma, F);
     }
   }
 #pragma unroll
@@ -192,34 +209,46 @@ __device__ __forceinline__ void volume(const Smem<C> &sm, double gamma, int tid)
     for (int w = tid; w < C::EPB * QD; w += C::NT) {
       const int slot = w / QD, p = w - slot * QD;
       if constexpr (!ONE) {
-        double U[5];
+        T U[5];
 #pragma unroll
         for (int n = 0; n < NF; ++n) U[n] = sm.B[(slot * NF + n) * QD + p];
-        volume_flux<PHYS>(U, gamma, F);
+        volume_flux<PHYS, T>(U, gamma, F);
       }
       const double *met = sm.geo[slot].metric;
 #pragma unroll
       for (int n = 0; n < NF; ++n) {
-        double g = met[3 * r + 0] * F[0][n];
-        g = fma(met[3 * r + 1], F[1][n], g);
-        if (DIM == 3) g = fma(met[3 * r + 2], F[2][n], g);
+        T g = T(met[3 * r + 0]) * F[0][n];
+        g = fma(T(met[3 * r + 1]), F[1][n], g);
+        if (DIM == 3) g = fma(T(met[3 * r + 2]), F[2][n], g);
         sm.C[(slot * NF + n) * QD + p] = g;
       }
     }
     __syncthreads();
     using Sh = Sh3<DIM, Q>;
-    if (r == 0) contract<Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<C::L, Q>, false>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
-    else if (r == 1) contract<Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<C::L, Q>, true>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
-    else contract<Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<C::L, Q>, true>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
+    if (r == 0) contract<Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<C::L, Q, T>, false>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
+    else if (r == 1) contract<Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<C::L, Q, T>, true>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
+    else contract<Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<C::L, Q, T>, true>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
     __syncthreads();
   }
+}
+
+// Trace buffers and the second register are FP32 in the mixed form.
+template <class C>
+__device__ __forceinline__ const typename C::R *trace_in(const StageArgs &a) {
+  if constexpr (C::MIXED) return a.Tinf; else return a.Tin;
+}
+template <class C>
+__device__ __forceinline__ typename C::R *trace_out(const StageArgs &a) {
+  if constexpr (C::MIXED) return a.Toutf; else return a.Tout;
 }
 
 // Numerical flux on all face points; E holds own traces on entry and
 // (F^ - F).J on exit.  Neighbour traces come from Tin.
 template <class C, int PHYS>
 __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &a, int tid) {
+  using T = typename C::R;
   constexpr int NF = C::NF, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
+  const T *Tin = trace_in<C>(a);
   for (int w = tid; w < NFACE * EPB * GF; w += C::NT) {
     const int f = w / (EPB * GF), rem = w - f * EPB * GF, slot = rem / GF, g = rem - slot * GF;
     const int e = sm.eid[slot];
@@ -227,16 +256,17 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
     const FaceLink lk = sm.lnk[slot * NFACE + f];
     const GeomClass &gc = sm.geo[slot];
     const int gn = a.perm[lk.perm + g];
-    double Uo[5], Un[5], Fh[5], FL[5], FR[5];
-    double *eo = sm.E + ((f * EPB + slot) * NF) * GF + g;
-    const double *tn = a.Tin + ((size_t)(lk.elem * NFACE + lk.face) * NF) * GF + gn;
+    T Uo[5], Un[5], Fh[5], FL[5], FR[5];
+    T *eo = sm.E + ((f * EPB + slot) * NF) * GF + g;
+    const T *tn = Tin + ((size_t)(lk.elem * NFACE + lk.face) * NF) * GF + gn;
+    const T nm[3] = {T(gc.nrm[f][0]), T(gc.nrm[f][1]), T(gc.nrm[f][2])};
 #pragma unroll
     for (int n = 0; n < NF; ++n) { Uo[n] = eo[n * GF]; Un[n] = tn[n * GF]; }
     const bool master = (gc.master >> f) & 1;
     bool ok;
-    if (master) ok = face_flux<PHYS>(Uo, Un, gc.nrm[f], a.gamma, a.flux, Fh, FL, FR);
-    else ok = face_flux<PHYS>(Un, Uo, gc.nrm[f], a.gamma, a.flux, Fh, FL, FR);
-    const double jr = gc.jr[f];
+    if (master) ok = face_flux<PHYS, T>(Uo, Un, nm, T(a.gamma), a.flux, Fh, FL, FR);
+    else ok = face_flux<PHYS, T>(Un, Uo, nm, T(a.gamma), a.flux, Fh, FL, FR);
+    const T jr = T(gc.jr[f]);
 #pragma unroll
     for (int n = 0; n < NF; ++n) eo[n * GF] = master ? (Fh[n] - FL[n]) * jr : (FR[n] - Fh[n]) * jr;
     if constexpr (PHYS == DGMX_NS2D || PHYS == DGMX_NS3D) {
@@ -264,21 +294,22 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
 // the boundary points of D, faces in increasing order as the reference.
 template <class C>
 __device__ __forceinline__ void lift(const Smem<C> &sm, int tid) {
+  using T = typename C::R;
   constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G, NF = C::NF, EPB = C::EPB, QD = C::QD, QF = C::QF;
   constexpr int NB = C::NFACE * EPB * NF;
-  double *LFc = sm.B;  // face-major [f][slot][n][QF], spans B and C
+  T *LFc = sm.B;  // face-major [f][slot][n][QF], spans B and C
   if constexpr (DIM == 3) {
-    contract<G, G, 1, 0, G, Q, MatG2GL<L, Q>, false>(sm.E, sm.S, NB, G * G, Q * G, tid, C::NT);
+    contract<G, G, 1, 0, G, Q, MatG2GL<L, Q, T>, false>(sm.E, sm.S, NB, G * G, Q * G, tid, C::NT);
     __syncthreads();
-    contract<Q, G, 1, 1, G, Q, MatG2GL<L, Q>, false>(sm.S, LFc, NB, Q * G, Q * Q, tid, C::NT);
+    contract<Q, G, 1, 1, G, Q, MatG2GL<L, Q, T>, false>(sm.S, LFc, NB, Q * G, Q * Q, tid, C::NT);
   } else {
-    contract<G, 1, 1, 0, G, Q, MatG2GL<L, Q>, false>(sm.E, LFc, NB, G, Q, tid, C::NT);
+    contract<G, 1, 1, 0, G, Q, MatG2GL<L, Q, T>, false>(sm.E, LFc, NB, G, Q, tid, C::NT);
   }
   __syncthreads();
-  const double w0 = 1.0 / cW<L, Q>[0], w1 = 1.0 / cW<L, Q>[Q - 1];
+  const T w0 = T(1) / cW<T, L, Q>[0], w1 = T(1) / cW<T, L, Q>[Q - 1];
   for (int w = tid; w < EPB * NF * QD; w += C::NT) {
     const int slot = w / (NF * QD), rem = w - slot * NF * QD, n = rem / QD, p = rem - n * QD;
-    double acc = sm.D[w];
+    T acc = sm.D[w];
     if constexpr (DIM == 3) {
       const int i = p / (Q * Q), j = (p / Q) % Q, k = p % Q;
       auto lf = [&](int f, int x, int y) { return LFc[((f * EPB + slot) * NF + n) * QF + x * Q + y]; };
@@ -297,9 +328,9 @@ __device__ __forceinline__ void lift(const Smem<C> &sm, int tid) {
       if (i == 0) acc = fma(w0, lf(3, j), acc);
     }
     // quadrature weights of the projection (the J of wJ cancels the mass)
-    double wq;
-    if constexpr (DIM == 3) wq = cW<L, Q>[p / (Q * Q)] * cW<L, Q>[(p / Q) % Q] * cW<L, Q>[p % Q];
-    else wq = cW<L, Q>[p / Q] * cW<L, Q>[p % Q];
+    T wq;
+    if constexpr (DIM == 3) wq = cW<T, L, Q>[p / (Q * Q)] * cW<T, L, Q>[(p / Q) % Q] * cW<T, L, Q>[p % Q];
+    else wq = cW<T, L, Q>[p / Q] * cW<T, L, Q>[p % Q];
     sm.D[w] = wq * acc;
   }
   __syncthreads();
@@ -319,50 +350,53 @@ __device__ __forceinline__ void load_geometry(const Smem<C> &sm, const StageArgs
 }
 
 // Element-major modal register block of the slot's element: NF*LD doubles.
-template <class C>
-__device__ __forceinline__ void load_modal(double *dst, const double *src, int e0, int ne, int tid) {
+template <class C, class S>
+__device__ __forceinline__ void load_modal(typename C::R *dst, const S *src, int e0, int ne, int tid) {
+  using T = typename C::R;
   constexpr int BLK = C::NF * C::LD;
   for (int w = tid; w < C::EPB * BLK; w += C::NT) {
     const int s = w / BLK, e = e0 + s;
-    dst[w] = e < ne ? src[(size_t)e0 * BLK + w] : (w % C::LD == 0 ? 1.0 : 0.0);
+    dst[w] = e < ne ? T(src[(size_t)e0 * BLK + w]) : T(w % C::LD == 0 ? 1.0 : 0.0);
   }
 }
 
-template <class C>
-__device__ __forceinline__ void store_traces(const double *E, double *T, int e0, int ne, int tid) {
+template <class C, class TT>
+__device__ __forceinline__ void store_traces(const typename C::R *E, TT *T, int e0, int ne, int tid) {
   constexpr int NF = C::NF, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
   for (int w = tid; w < EPB * NFACE * NF * GF; w += C::NT) {
     // global order [e][f][n][g]; smem order [f][slot][n][g]
     const int s = w / (NFACE * NF * GF), rem = w - s * NFACE * NF * GF;
     const int f = rem / (NF * GF), ng = rem - f * NF * GF;
     const int e = e0 + s;
-    if (e < ne) T[(size_t)e * NFACE * NF * GF + rem] = E[(f * EPB + s) * NF * GF + ng];
+    if (e < ne) T[(size_t)e * NFACE * NF * GF + rem] = TT(E[(f * EPB + s) * NF * GF + ng]);
   }
 }
 
 // The element's own traces, written by the previous stage (or the trace
 // kernel), global [e][f][n][g] -> smem face-major [f][slot][n][g].
-template <class C>
-__device__ __forceinline__ void load_own_traces(double *E, const double *T, int e0, int ne, int tid) {
+template <class C, class TT>
+__device__ __forceinline__ void load_own_traces(typename C::R *E, const TT *T, int e0, int ne, int tid) {
+  using R = typename C::R;
   constexpr int NF = C::NF, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
   for (int w = tid; w < EPB * NFACE * NF * GF; w += C::NT) {
     const int s = w / (NFACE * NF * GF), rem = w - s * NFACE * NF * GF;
     const int f = rem / (NF * GF), ng = rem - f * NF * GF;
     const int e = e0 + s;
-    E[(f * EPB + s) * NF * GF + ng] = e < ne ? T[(size_t)e * NFACE * NF * GF + rem] : (ng < GF ? 1.0 : 0.0);
+    E[(f * EPB + s) * NF * GF + ng] = e < ne ? R(T[(size_t)e * NFACE * NF * GF + rem]) : R(ng < GF ? 1.0 : 0.0);
   }
 }
 
 // ---------------------------------------------------------------- kernels
 template <class C, int PHYS>
 __global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
-  extern __shared__ __align__(16) double smem_raw[];
+  using T = typename C::R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<C> sm(smem_raw);
   const int tid = threadIdx.x;
   const int e0 = blockIdx.x * C::EPB;
   load_geometry<C>(sm, a, e0, tid);
   load_modal<C>(sm.A, a.X, e0, a.ne, tid);
-  load_own_traces<C>(sm.E, a.Tin, e0, a.ne, tid);
+  load_own_traces<C>(sm.E, trace_in<C>(a), e0, a.ne, tid);
   __syncthreads();
   backward<C>(sm.A, sm.B, sm.S, sm.C, tid, C::NT);
   volume<C, PHYS>(sm, a.gamma, tid);
@@ -375,75 +409,93 @@ __global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
     const int s = w / BLK, e = e0 + s;
     if (e >= a.ne) continue;
     const size_t gi = (size_t)e0 * BLK + w;
-    const double x = sm.A[w];
-    double r = sm.R[w];
-    if (a.Rcap) a.Rcap[gi] = r;          // first RHS (shallow-water balance)
-    if (a.Rsub) r = r - a.Rsub[gi];
-    if constexpr (PHYS == DGMX_NS2D || PHYS == DGMX_NS3D) {
-      const int n = (w % BLK) / C::LD, m = w % C::LD;
-      if (n >= 1) r = r - a.Pv[((size_t)e * (C::NF - 1) + (n - 1)) * C::LD + m];
-    }
-    double next;
-    switch (a.kind) {
-      case kLSRK: {
-        double ut = a.c0 * a.Ut[gi];
-        ut = fma(-a.dt, r, ut);
-        const double u = fma(a.c1, ut, x);
-        a.Ut[gi] = ut; a.U[gi] = u; next = u;
-        break;
+    if constexpr (C::MIXED) {
+      // FP32 right-hand side and second register, FP64 solution register:
+      // Ut = A Ut - dt R in FP32; U = U + B Ut accumulated in FP64.
+      float r = sm.R[w];
+      if (a.Rsub) r = r - float(a.Rsub[gi]);
+      float next;
+      if (a.kind == kRHS) {
+        a.A[gi] = r;
+        next = sm.A[w];
+      } else {
+        float ut = float(a.c0) * a.Utf[gi];
+        ut = fmaf(-float(a.dt), r, ut);
+        const double u = fma(a.c1, double(ut), a.U[gi]);
+        a.Utf[gi] = ut; a.U[gi] = u; next = float(u);
       }
-      case kTVD0: {
-        const double ut = fma(-a.dt, r, x);
-        a.Ut[gi] = ut; next = ut;
-        break;
+      sm.A[w] = next;
+      continue;
+    } else {
+      const double x = sm.A[w];
+      double r = sm.R[w];
+      if (a.Rcap) a.Rcap[gi] = r;          // first RHS (shallow-water balance)
+      if (a.Rsub) r = r - a.Rsub[gi];
+      if constexpr (PHYS == DGMX_NS2D || PHYS == DGMX_NS3D) {
+        const int n = (w % BLK) / C::LD, m = w % C::LD;
+        if (n >= 1) r = r - a.Pv[((size_t)e * (C::NF - 1) + (n - 1)) * C::LD + m];
       }
-      case kTVD1: {
-        const double t = fma(-a.dt, r, x);
-        double ut = a.c1 * t;
-        ut = fma(a.c0, a.U[gi], ut);
-        a.Ut[gi] = ut; next = ut;
-        break;
+      double next;
+      switch (a.kind) {
+        case kLSRK: {
+          double ut = a.c0 * a.Ut[gi];
+          ut = fma(-a.dt, r, ut);
+          const double u = fma(a.c1, ut, x);
+          a.Ut[gi] = ut; a.U[gi] = u; next = u;
+          break;
+        }
+        case kTVD0: {
+          const double ut = fma(-a.dt, r, x);
+          a.Ut[gi] = ut; next = ut;
+          break;
+        }
+        case kTVD1: {
+          const double t = fma(-a.dt, r, x);
+          double ut = a.c1 * t;
+          ut = fma(a.c0, a.U[gi], ut);
+          a.Ut[gi] = ut; next = ut;
+          break;
+        }
+        case kTVD2: {
+          const double t = fma(-a.dt, r, x);
+          double u = a.c0 * a.U[gi];
+          u = fma(a.c1, t, u);
+          a.U[gi] = u; next = u;
+          break;
+        }
+        case kRK40: {
+          const double ut = fma(a.c0, r, x);
+          a.Ut[gi] = ut; a.A[gi] = a.c1 * r; next = ut;
+          break;
+        }
+        case kRK41: {
+          const double ut = fma(a.c0, r, a.U[gi]);
+          a.A[gi] = fma(a.c1, r, a.A[gi]);
+          a.Ut[gi] = ut; next = ut;
+          break;
+        }
+        case kRHS: {
+          a.A[gi] = r; next = x;
+          break;
+        }
+        default: {  // kRK43
+          const double acc = fma(a.c1, r, a.A[gi]);
+          const double u = fma(a.c0, acc, a.U[gi]);
+          a.U[gi] = u; next = u;
+          break;
+        }
       }
-      case kTVD2: {
-        const double t = fma(-a.dt, r, x);
-        double u = a.c0 * a.U[gi];
-        u = fma(a.c1, t, u);
-        a.U[gi] = u; next = u;
-        break;
-      }
-      case kRK40: {
-        const double ut = fma(a.c0, r, x);
-        a.Ut[gi] = ut; a.A[gi] = a.c1 * r; next = ut;
-        break;
-      }
-      case kRK41: {
-        const double ut = fma(a.c0, r, a.U[gi]);
-        a.A[gi] = fma(a.c1, r, a.A[gi]);
-        a.Ut[gi] = ut; next = ut;
-        break;
-      }
-      case kRHS: {
-        a.A[gi] = r; next = x;
-        break;
-      }
-      default: {  // kRK43
-        const double acc = fma(a.c1, r, a.A[gi]);
-        const double u = fma(a.c0, acc, a.U[gi]);
-        a.U[gi] = u; next = u;
-        break;
-      }
-    }
-    sm.A[w] = next;
-  }
+  sm.A[w] = next;
+    }  }
   __syncthreads();
   modal_traces<C>(sm.A, sm.E, sm.S, sm.B, tid, C::NT);
-  store_traces<C>(sm.E, a.Tout, e0, a.ne, tid);
+  store_traces<C>(sm.E, trace_out<C>(a), e0, a.ne, tid);
 }
 
 // Traces of a modal register (start of a run, after set_state).
 template <class C>
-__global__ void __launch_bounds__(C::NT, C::MINB) traces_modal_kernel(StageArgs a, const double *Xm, double *T) {
-  extern __shared__ __align__(16) double smem_raw[];
+__global__ void __launch_bounds__(C::NT, C::MINB) traces_modal_kernel(StageArgs a, const double *Xm, typename C::R *T) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<C> sm(smem_raw);
   const int tid = threadIdx.x, e0 = blockIdx.x * C::EPB;
   load_modal<C>(sm.A, Xm, e0, a.ne, tid);
@@ -467,7 +519,8 @@ __device__ __forceinline__ void load_nodal(double *B, const double *Xn, int e0, 
 // src/Quad.cpp:884-905) for the Domain::time_derivative path.
 template <class C>
 __global__ void __launch_bounds__(C::NT, C::MINB) traces_nodal_kernel(StageArgs a) {
-  extern __shared__ __align__(16) double smem_raw[];
+  using T = typename C::R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<C> sm(smem_raw);
   constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G, NF = C::NF, EPB = C::EPB, QD = C::QD, QF = C::QF;
   const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
@@ -502,11 +555,11 @@ __global__ void __launch_bounds__(C::NT, C::MINB) traces_nodal_kernel(StageArgs 
   __syncthreads();
   constexpr int NB = C::NFACE * EPB * NF;
   if constexpr (DIM == 3) {
-    contract<Q, Q, 1, 0, Q, G, MatGL2G<L, Q>, false>(sm.C, sm.S, NB, Q * Q, G * Q, tid, C::NT);
+    contract<Q, Q, 1, 0, Q, G, MatGL2G<L, Q, T>, false>(sm.C, sm.S, NB, Q * Q, G * Q, tid, C::NT);
     __syncthreads();
-    contract<G, Q, 1, 1, Q, G, MatGL2G<L, Q>, false>(sm.S, sm.E, NB, G * Q, G * G, tid, C::NT);
+    contract<G, Q, 1, 1, Q, G, MatGL2G<L, Q, T>, false>(sm.S, sm.E, NB, G * Q, G * G, tid, C::NT);
   } else {
-    contract<Q, 1, 1, 0, Q, G, MatGL2G<L, Q>, false>(sm.C, sm.E, NB, Q, G, tid, C::NT);
+    contract<Q, 1, 1, 0, Q, G, MatGL2G<L, Q, T>, false>(sm.C, sm.E, NB, Q, G, tid, C::NT);
   }
   __syncthreads();
   store_traces<C>(sm.E, a.Tout, e0, a.ne, tid);
@@ -515,7 +568,8 @@ __global__ void __launch_bounds__(C::NT, C::MINB) traces_nodal_kernel(StageArgs 
 // Domain::time_derivative on GLL values: F = -dU/dt at GLL points (projected).
 template <class C, int PHYS>
 __global__ void __launch_bounds__(C::NT, C::MINB) rhs_nodal_kernel(StageArgs a) {
-  extern __shared__ __align__(16) double smem_raw[];
+  using T = typename C::R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<C> sm(smem_raw);
   constexpr int NF = C::NF, QD = C::QD, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
   const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
@@ -558,7 +612,8 @@ __global__ void __launch_bounds__(C::NT, C::MINB) rhs_nodal_kernel(StageArgs a) 
 // GLL values (Field layout) -> projected modal register (element-major).
 template <class C>
 __global__ void __launch_bounds__(C::NT, C::MINB) forward_kernel(StageArgs a, const double *Un, double *Um) {
-  extern __shared__ __align__(16) double smem_raw[];
+  using T = typename C::R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<C> sm(smem_raw);
   constexpr int L = C::L, Q = C::Q, NF = C::NF, QD = C::QD, EPB = C::EPB;
   const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
@@ -567,8 +622,8 @@ __global__ void __launch_bounds__(C::NT, C::MINB) forward_kernel(StageArgs a, co
   for (int w = tid; w < EPB * NF * QD; w += C::NT) {
     const int p = w % QD;
     double wq;
-    if constexpr (C::DIM == 3) wq = cW<L, Q>[p / (Q * Q)] * cW<L, Q>[(p / Q) % Q] * cW<L, Q>[p % Q];
-    else wq = cW<L, Q>[p / Q] * cW<L, Q>[p % Q];
+    if constexpr (C::DIM == 3) wq = cW<double, L, Q>[p / (Q * Q)] * cW<double, L, Q>[(p / Q) % Q] * cW<double, L, Q>[p % Q];
+    else wq = cW<double, L, Q>[p / Q] * cW<double, L, Q>[p % Q];
     sm.D[w] = wq * sm.D[w];
   }
   __syncthreads();
@@ -583,7 +638,8 @@ __global__ void __launch_bounds__(C::NT, C::MINB) forward_kernel(StageArgs a, co
 // Modal register -> GLL values (Field layout).
 template <class C>
 __global__ void __launch_bounds__(C::NT, C::MINB) backward_kernel(StageArgs a, const double *Um, double *Un) {
-  extern __shared__ __align__(16) double smem_raw[];
+  using T = typename C::R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<C> sm(smem_raw);
   constexpr int NF = C::NF, QD = C::QD, EPB = C::EPB;
   const int tid = threadIdx.x, e0 = blockIdx.x * EPB;

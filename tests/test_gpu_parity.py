@@ -123,6 +123,39 @@ def test_navier_stokes_br1_matches_oracle(case):
     assert rel(E.rhs(U0), F_o) > 1e-8
 
 
+MIXED_CASES = [
+    ("euler3d-tgv", 8, 3, (4, 4, 4), 0, 2 * np.pi, 3, "laxfriedrichs", TG, 0.002, 20),
+    ("euler3d-roe-p5", 8, 3, (2, 2, 2), 0, 2 * np.pi, 5, "roe", TG, 0.001, 10),
+    ("euler2d-vortex", 1, 2, (6, 6), -5, 5, 4, "laxfriedrichs", IV, 0.01, 20),
+    ("shallow", 30, 2, (4, 4), -2, 2, 3, "laxfriedrichs", GB, 0.001, 20),
+]
+
+
+@pytest.mark.parametrize("case", MIXED_CASES, ids=[c[0] for c in MIXED_CASES])
+def test_mixed_precision_within_1e6_of_fp64_oracle(case):
+    """FP32 states, fluxes and contractions with the FP64 solution register
+    (LSRK14): relative L2 error against the FP64 oracle stays <= 1e-6."""
+    import dgm_b200
+    _, phys, dim, n, lo, hi, p, flux, ic, dt, steps = case
+    m = dgm_b200.meshgen.box(dim, n, lo, hi, p)
+    P = oracle.Problem(dgm_io.Mesh(m.dim, m.verts, m.con, m.porder, m.qorder), phys, flux=flux)
+    if phys == oracle.SHALLOW:
+        P.set_sw_balance(False)
+    D = dgm_b200.Domain(m, phys, flux=flux, inttype=dgm_b200.LSRK14, precision=dgm_b200.MIXED, sw_balance=False)
+    x, y, z = P.coords()
+    f = ic(x, y, z)
+    U0 = P.project(f)
+    P.set_state(U0)
+    D.set_state(f)
+    P.advance(14, dt, steps)
+    D.advance(dt, steps)
+    err = rel(D.state(), P.state())
+    assert err < 1e-6, err
+    assert err > 1e-13  # it really ran in FP32
+    # the state actually moved by much more than the error
+    assert rel(P.state(), U0) > 10 * err
+
+
 def test_autotune_keeps_results_and_state():
     """The tile autotuner only changes launch shapes: the state is untouched
     by tuning and every variant gives the oracle's answer."""
