@@ -6,8 +6,13 @@
 
 namespace dgmx {
 
+// Every k_*.cu is its own device module with its own copy of the __constant__
+// tables, whose host shadows have internal linkage.  The uploader must have
+// internal linkage too: an ordinary (weak) template instantiation would be
+// merged across compilation units by the linker and write only one module's
+// tables.
 template <int L, int Q, class T>
-cudaError_t upload_tables_lq(const Tables1D &t) {
+static cudaError_t upload_tables_lq(const Tables1D &t) {
   auto put = [](const auto &sym, const std::vector<double> &v, size_t n) {
     std::vector<T> c(n);
     for (size_t i = 0; i < n; ++i) c[i] = T(v[i]);
