@@ -60,6 +60,7 @@ struct dgmx_domain {
   double *Rsw = nullptr;                                 // shallow-water first RHS (modal)
   double *Ghat = nullptr, *Vtr = nullptr, *Pv = nullptr; // Navier-Stokes BR1 work
   float *Utf = nullptr, *Tf[2] = {nullptr, nullptr};     // mixed form: FP32 register and traces
+  double *uref = nullptr;                                // mixed form: reference state (10 doubles)
   double *nod_in = nullptr, *nod_out = nullptr;          // Field-layout staging
   double *Jdev = nullptr, *integ = nullptr;
   int *gclass = nullptr, *perm = nullptr, *err = nullptr;
@@ -96,6 +97,7 @@ struct dgmx_domain {
     a.ne = ne; a.gamma = prm.gamma; a.vis = prm.vis; a.Pr = prm.Pr; a.flux = prm.flux;
     a.err = err;
     a.Ghat = Ghat; a.V = Vtr; a.Pv = Pv;
+    a.uref = uref;
     return a;
   }
   bool ns() const { return prm.physics == DGMX_NS2D || prm.physics == DGMX_NS3D; }
@@ -106,13 +108,14 @@ struct dgmx_domain {
     if (graph) cudaGraphExecDestroy(graph);
     graph = nullptr;
     void *ptrs[] = {U, Ut, Acc, T[0], T[1], Rsw, nod_in, nod_out, Jdev, integ, gclass, perm, err, classes, links,
-                    Ghat, Vtr, Pv, Utf, Tf[0], Tf[1]};
+                    Ghat, Vtr, Pv, Utf, Tf[0], Tf[1], uref};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (host_pinned) cudaFreeHost(host_pinned);
     if (stream) cudaStreamDestroy(stream);
     U = Ut = Acc = Rsw = nod_in = nod_out = Jdev = integ = host_pinned = nullptr;
     Ghat = Vtr = Pv = nullptr;
     Utf = Tf[0] = Tf[1] = nullptr;
+    uref = nullptr;
     T[0] = T[1] = nullptr; gclass = perm = err = nullptr; classes = nullptr; links = nullptr; stream = nullptr;
   }
 };
@@ -166,8 +169,35 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
 int stages_per_step(int inttype) { return inttype == DGMX_LSRK14 ? 14 : (inttype == DGMX_TVD3 ? 3 : 4); }
 int launches_per_stage(const dgmx_domain *d) { return d->ns() ? 3 : 1; }
 
+// Mixed form: the reference state the FP32 working copies are perturbations
+// about is the domain mean of U (any constant gives the same scheme; the
+// mean keeps the perturbations small).  uref[n] = mean, uref[5 + n] = its
+// constant-mode coefficient.
+dgmx_status update_reference(dgmx_domain *d) {
+  const double c = std::pow(std::sqrt(2.0), d->dim);
+  cudaError_t e = launch_integrals(d->nf, d->ne, d->ld, c, d->U, d->Jdev, d->integ, d->stream);
+  ++d->launches;
+  double tot[5] = {0, 0, 0, 0, 0};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(tot, d->integ, sizeof(double) * d->nf, cudaMemcpyDeviceToHost, d->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+  if (e != cudaSuccess) return d->cuda(e, "reference state");
+  double vol = 0.0;
+  for (int k = 0; k < d->ne; ++k) vol += d->mesh.J[k];
+  vol *= std::pow(2.0, d->dim);
+  const double phi0 = std::pow(d->tab.B[0], d->dim);   // constant mode's value
+  double h[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int n = 0; n < d->nf; ++n) { h[n] = tot[n] / vol; h[5 + n] = h[n] / phi0; }
+  e = cudaMemcpyAsync(d->uref, h, sizeof(h), cudaMemcpyHostToDevice, d->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+  return d->cuda(e, "reference state upload");
+}
+
 // traces of U into T[tcur]
 dgmx_status refresh_traces(dgmx_domain *d) {
+  if (d->mixed()) {
+    const dgmx_status st = update_reference(d);
+    if (st != DGMX_OK) return st;
+  }
   StageArgs a = d->base_args();
   cudaError_t e = d->mixed() ? d->ops_m->traces_modal(a, d->U, d->Tf[d->tcur], d->stream)
                              : d->ops->traces_modal(a, d->U, d->T[d->tcur], d->stream);
@@ -288,7 +318,8 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
             (phys != DGMX_SHALLOW || chk(dalloc(&d->Rsw, d->nmodal()), "alloc sw source")) &&
             (!d->mixed() || (chk(dalloc(&d->Utf, d->nmodal()), "alloc Ut (FP32)") &&
                              chk(dalloc(&d->Tf[0], d->ntrace()), "alloc T0 (FP32)") &&
-                             chk(dalloc(&d->Tf[1], d->ntrace()), "alloc T1 (FP32)"))) &&
+                             chk(dalloc(&d->Tf[1], d->ntrace()), "alloc T1 (FP32)") &&
+                             chk(dalloc(&d->uref, (size_t)10), "alloc reference state"))) &&
             (!d->ns() || (chk(dalloc(&d->Ghat, (size_t)d->ne * (d->dim + 1) * d->dim * d->ld), "alloc gradients") &&
                           chk(dalloc(&d->Vtr, (size_t)d->ne * d->nfaces * (d->nf - 1) * d->gf), "alloc viscous traces") &&
                           chk(dalloc(&d->Pv, (size_t)d->ne * (d->nf - 1) * d->ld), "alloc viscous divergence")));

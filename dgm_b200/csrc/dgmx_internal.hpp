@@ -109,11 +109,21 @@ struct StageArgs {
   // shallow-water balance (REO_SHALLOW_ENFORCE_BALANCE, src/Shallow.cpp:251-267)
   double *Rcap;           // if set, the projected RHS is stored here (modal)
   const double *Rsub;     // if set, subtracted from the projected RHS
-  // Navier-Stokes BR1 (src/Navier_Stokes3d.cpp:182-391)
-  // mixed-precision form: FP32 second register and traces
+  // mixed-precision form: FP32 second register and traces; the working
+  // copies are perturbations about a reference state per solve:
+  // uref[10 s + n] conserved values, uref[10 s + 5 + n] its constant-mode
+  // coefficient; esolve[e] = solve of element e (null: solve 0)
   float *Utf;
   const float *Tinf;
   float *Toutf;
+  const double *uref;
+  const int *esolve;
+  // element pools: persistent loop over tiles[0 .. *ntiles) (null: one
+  // tile per CTA) and a per-element step (null: dt)
+  const int *tiles;
+  const int *ntiles;
+  const double *dte;
+  // Navier-Stokes BR1 (src/Navier_Stokes3d.cpp:182-391)
   double *Ghat;           // projected primitive gradients, modal [e][comp][dir][L^d]
   double *V;              // viscous normal-flux traces [e][face][field-1][gf]
   double *Pv;             // projected viscous divergence, modal [e][field-1][L^d]

@@ -291,4 +291,186 @@ __device__ __forceinline__ bool face_flux(const T *UL, const T *UR, const T *n, 
   return ok;
 }
 
+// ---- perturbation form (FP32 working precision) ----------------------------
+// The mixed form splits every state as U = Ub + d, Ub a constant reference
+// state of the solve, and evaluates F(Ub + d) - F(Ub).  The derivative of
+// that difference equals the derivative of F, and its jump across a face
+// equals the jump of F, so the scheme is unchanged algebraically; but it is
+// formed from products that each carry a perturbation factor, so its FP32
+// rounding error scales with |d| instead of |U| (at Mach 0.1 the pressure
+// is ~70x the dynamic part).  Euler: with u' = (m' - ub rho')/rho,
+//   p' = (g-1)(E' - (m'.ub + m.u')/2),  F'_rho = m',
+//   F'_m = m' ub_d + m u'_d + p' e_d,   F'_E = H' ub_d + H u'_d  (H = E + p);
+// shallow water: p' = phi'(phi_b + phi'/2) for the phi^2/2 pressure.
+template <class T>
+struct RefState {
+  T r, m[3], E;   // reference density (geopotential), momentum, energy
+  T u[3], H, p;   // its velocity, E + p and pressure
+  T pad[5];
+};
+
+template <int PHYS, class T>
+__device__ __forceinline__ RefState<T> make_ref(const double *Ub, double gamma) {
+  constexpr bool SW = PHYS == DGMX_SHALLOW;
+  constexpr int DIM = (PHYS == DGMX_EULER3D || PHYS == DGMX_NS3D) ? 3 : 2, NF = SW ? 3 : DIM + 2;
+  RefState<T> rs{};
+  const double r = Ub[0];
+  double q = 0.0, u[3] = {0.0, 0.0, 0.0};
+  for (int i = 0; i < DIM; ++i) { u[i] = Ub[1 + i] / r; q += Ub[1 + i] * u[i]; }
+  const double p = SW ? 0.5 * r * r : (gamma - 1.0) * (Ub[NF - 1] - 0.5 * q);
+  rs.r = T(r);
+  for (int i = 0; i < DIM; ++i) { rs.m[i] = T(Ub[1 + i]); rs.u[i] = T(u[i]); }
+  rs.E = SW ? T(0) : T(Ub[NF - 1]);
+  rs.p = T(p);
+  rs.H = SW ? T(0) : T(Ub[NF - 1] + p);
+  return rs;
+}
+
+// F(Ub + d) - F(Ub) in every direction (volume term).
+template <int PHYS, class T>
+__device__ __forceinline__ void volume_flux_pert(const RefState<T> &b, const T *d, T gamma, T (*F)[5]) {
+  constexpr bool SW = PHYS == DGMX_SHALLOW;
+  constexpr int DIM = (PHYS == DGMX_EULER3D || PHYS == DGMX_NS3D) ? 3 : 2, NF = SW ? 3 : DIM + 2;
+  const T rho = b.r + d[0], ir = T(1.0) / rho;
+  T m[3], up[3];
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) { m[i] = b.m[i] + d[1 + i]; up[i] = (d[1 + i] - b.u[i] * d[0]) * ir; }
+  T pp, Hp = T(0), H = T(0);
+  if constexpr (SW) {
+    pp = d[0] * fma(T(0.5), d[0], b.r);
+  } else {
+    T s = T(0);
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) { s = fma(d[1 + i], b.u[i], s); s = fma(m[i], up[i], s); }
+    pp = (gamma - T(1.0)) * fma(T(-0.5), s, d[NF - 1]);
+    Hp = d[NF - 1] + pp;
+    H = b.H + Hp;
+  }
+#pragma unroll
+  for (int k = 0; k < DIM; ++k) {
+    F[k][0] = d[1 + k];
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) F[k][1 + i] = fma(d[1 + i], b.u[k], m[i] * up[k]) + (i == k ? pp : T(0));
+    if constexpr (!SW) F[k][NF - 1] = fma(Hp, b.u[k], H * up[k]);
+  }
+}
+
+// Normal component of F(Ub + d) - F(Ub) plus the full state's normal
+// velocity, sound speed (sqrt(phi) for shallow water) and realizability.
+template <int PHYS, class T>
+__device__ __forceinline__ bool normal_flux_pert(const RefState<T> &b, const T *d, const T *n, T gamma, T *Fn,
+                                                 T &rho, T &un, T &c, T *vel, T &Hs) {
+  constexpr bool SW = PHYS == DGMX_SHALLOW;
+  constexpr int DIM = (PHYS == DGMX_EULER3D || PHYS == DGMX_NS3D) ? 3 : 2, NF = SW ? 3 : DIM + 2;
+  rho = b.r + d[0];
+  const T ir = T(1.0) / rho;
+  T m[3], up[3], ubn = T(0), upn = T(0), mpn = T(0);
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) {
+    m[i] = b.m[i] + d[1 + i];
+    up[i] = (d[1 + i] - b.u[i] * d[0]) * ir;
+    vel[i] = b.u[i] + up[i];
+    ubn = fma(b.u[i], n[i], ubn);
+    upn = fma(up[i], n[i], upn);
+    mpn = fma(d[1 + i], n[i], mpn);
+  }
+  un = ubn + upn;
+  T pp, p;
+  if constexpr (SW) {
+    pp = d[0] * fma(T(0.5), d[0], b.r);
+    p = T(0.5) * rho * rho;
+    c = sqrt(rho);
+    Hs = T(0);
+  } else {
+    T s = T(0);
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) { s = fma(d[1 + i], b.u[i], s); s = fma(m[i], up[i], s); }
+    pp = (gamma - T(1.0)) * fma(T(-0.5), s, d[NF - 1]);
+    p = b.p + pp;
+    const T Hp = d[NF - 1] + pp, H = b.H + Hp;
+    Fn[NF - 1] = fma(Hp, ubn, H * upn);
+    Hs = H * ir;                                   // total enthalpy per unit mass
+    c = sqrt(gamma * fmax(p, T(0)) * ir);
+  }
+  Fn[0] = mpn;
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) Fn[1 + i] = fma(d[1 + i], ubn, m[i] * upn) + pp * n[i];
+  return rho >= T(kAeps) && p >= T(kAeps);
+}
+
+// Face flux in perturbation form, in the master's frame: dl = master-side
+// perturbation, dr = slave side, n = master normal.  Returns
+// Dm = F^ - F(UL).n and DF = F(UR).n - F(UL).n, which is all the lift needs
+// (master: Dm, slave: DF - Dm).  Lax-Friedrichs as src/Euler3d.cpp:601-816
+// and src/Shallow.cpp:380-510; Roe as src/Euler.cpp:682-741 (rotated to the
+// face frame in 3-D), its upwind dissipation formed from the state jump.
+template <int PHYS, class T>
+__device__ __forceinline__ bool face_flux_pert(const RefState<T> &b, const T *dl, const T *dr, const T *n,
+                                               T gamma, int flux, T *Dm, T *DF) {
+  constexpr bool SW = PHYS == DGMX_SHALLOW;
+  constexpr int DIM = (PHYS == DGMX_EULER3D || PHYS == DGMX_NS3D) ? 3 : 2, NF = SW ? 3 : DIM + 2;
+  T FL[5], FR[5], rl, rr, ul, ur, cl, cr, vl[3], vr[3], Hl, Hr;
+  bool ok = normal_flux_pert<PHYS, T>(b, dl, n, gamma, FL, rl, ul, cl, vl, Hl);
+  ok = normal_flux_pert<PHYS, T>(b, dr, n, gamma, FR, rr, ur, cr, vr, Hr) && ok;
+  T dU[5];
+#pragma unroll
+  for (int k = 0; k < NF; ++k) { DF[k] = FR[k] - FL[k]; dU[k] = dr[k] - dl[k]; }
+  if constexpr (!SW) {
+    if (flux == DGMX_FLUX_ROE) {
+      const T gm1 = gamma - T(1.0);
+      // face frame: n, s (and t in 3-D)
+      T s[3], t[3] = {T(0), T(0), T(0)};
+      if constexpr (DIM == 2) {
+        s[0] = -n[1]; s[1] = n[0]; s[2] = T(0);
+      } else {
+        s[0] = n[1]; s[1] = n[2]; s[2] = n[0];
+        const T sdn = n[0] * s[0] + n[1] * s[1] + n[2] * s[2];
+        s[0] -= sdn * n[0]; s[1] -= sdn * n[1]; s[2] -= sdn * n[2];
+        const T sni = T(1.0) / sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+        s[0] *= sni; s[1] *= sni; s[2] *= sni;
+        t[0] = n[1] * s[2] - s[1] * n[2]; t[1] = n[2] * s[0] - s[2] * n[0]; t[2] = n[0] * s[1] - s[0] * n[1];
+        const T tni = T(1.0) / sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        t[0] *= tni; t[1] *= tni; t[2] *= tni;
+      }
+      T vsl = T(0), vsr = T(0), vtl = T(0), vtr = T(0), dms = T(0), dmt = T(0), dmn = T(0);
+#pragma unroll
+      for (int i = 0; i < DIM; ++i) {
+        vsl = fma(vl[i], s[i], vsl); vsr = fma(vr[i], s[i], vsr);
+        vtl = fma(vl[i], t[i], vtl); vtr = fma(vr[i], t[i], vtr);
+        dmn = fma(dU[1 + i], n[i], dmn); dms = fma(dU[1 + i], s[i], dms); dmt = fma(dU[1 + i], t[i], dmt);
+      }
+      const T R = sqrt(rr / rl), iRp1 = T(1.0) / (T(1.0) + R);
+      const T u = (ul + R * ur) * iRp1, v = (vsl + R * vsr) * iRp1, w = (vtl + R * vtr) * iRp1;
+      const T H = (Hl + R * Hr) * iRp1;
+      const T a2 = gm1 * (H - T(0.5) * (u * u + v * v + w * w));
+      const T a = sqrt(a2), ainv = T(1.0) / a, c1inv = a2 / gm1;
+      const T d0 = dU[0], dE = dU[NF - 1];
+      T al[5];
+      al[2] = dms - v * d0;
+      al[3] = dmt - w * d0;
+      al[1] = gm1 * ainv * ainv * (d0 * (H - u * u) + u * dmn - (dE - al[2] * v - al[3] * w));
+      al[0] = T(0.5) * ainv * (d0 * (u + a) - dmn - a * al[1]);
+      al[4] = d0 - (al[0] + al[1]);
+      const T l0 = fmin(u - a, T(0.0)), l1 = fmin(u, T(0.0)), l4 = fmin(u + a, T(0.0));
+      T G0 = l0 * al[0], Gn = l0 * (u - a) * al[0], Gs = l0 * v * al[0], Gt = l0 * w * al[0];
+      T GE = l0 * (H - u * a) * al[0];
+      G0 += l1 * al[1]; Gn += l1 * u * al[1]; Gs += l1 * v * al[1]; Gt += l1 * w * al[1];
+      GE += l1 * (H - c1inv) * al[1];
+      Gs += l1 * al[2]; GE += l1 * v * al[2];
+      Gt += l1 * al[3]; GE += l1 * w * al[3];
+      G0 += l4 * al[4]; Gn += l4 * (u + a) * al[4]; Gs += l4 * v * al[4]; Gt += l4 * w * al[4];
+      GE += l4 * (H + u * a) * al[4];
+      Dm[0] = G0;
+#pragma unroll
+      for (int i = 0; i < DIM; ++i) Dm[1 + i] = Gn * n[i] + Gs * s[i] + Gt * t[i];
+      Dm[NF - 1] = GE;
+      return ok;
+    }
+  }
+  const T lmax = fmax(fabs(ul) + cl, fabs(ur) + cr);
+#pragma unroll
+  for (int k = 0; k < NF; ++k) Dm[k] = T(0.5) * (DF[k] - lmax * dU[k]);
+  return ok;
+}
+
 }  // namespace dgmx

@@ -42,6 +42,7 @@ struct Cfg {
   // working precision: FP64, or FP32 for the mixed form (the solution
   // register U stays FP64 in global memory)
   static constexpr bool MIXED = MIXED_;
+  static constexpr int PHYSICS = PHYS;
   using R = std::conditional_t<MIXED_, float, double>;
   static constexpr int DIM = phys_dim(PHYS), NF = phys_nf(PHYS);
   static constexpr int L = L_, Q = Q_, G = Q_ - 1, EPB = EPB_, MINB = MINB_ > 0 ? MINB_ : 1;
@@ -62,7 +63,8 @@ struct Cfg {
   static constexpr int SZ_S = cmax(cmax(NF * Q * LF, NFACE * NF * LF), DIM == 3 ? NFACE * NF * Q * G : 0);
   static constexpr int SZ_SLOT = SZ_A + SZ_B + SZ_C + SZ_D + SZ_E + SZ_R + SZ_S;
   static constexpr size_t DATA = ((size_t)EPB * SZ_SLOT * sizeof(R) + 15) / 16 * 16;
-  static constexpr size_t SMEM = DATA + (size_t)EPB * (sizeof(GeomClass) + NFACE * sizeof(FaceLink) + 16);
+  static constexpr size_t SMEM = DATA + (size_t)EPB * (sizeof(GeomClass) + NFACE * sizeof(FaceLink) + 16 +
+                                                     (MIXED_ ? sizeof(RefState<R>) : 0));
   static_assert(NFACE * QF <= 2 * QD, "lift face buffer must fit in the B+C regions");
   static_assert(DIM == 2 || NFACE * G * L <= 2 * QD, "trace intermediate must fit in the B+C regions");
   static_assert(SMEM <= 227 * 1024 || EPB > 1, "element slot does not fit in shared memory");
@@ -78,6 +80,7 @@ struct Smem {
   GeomClass *geo;
   FaceLink *lnk;
   int *eid;
+  RefState<T> *ref;  // mixed form: the reference state of each slot's solve
   __device__ Smem(unsigned char *raw) {
     T *base = reinterpret_cast<T *>(raw);
     A = base;
@@ -90,6 +93,7 @@ struct Smem {
     geo = reinterpret_cast<GeomClass *>(raw + K::DATA);
     lnk = reinterpret_cast<FaceLink *>(geo + K::EPB);
     eid = reinterpret_cast<int *>(lnk + K::EPB * K::NFACE);
+    ref = reinterpret_cast<RefState<T> *>(eid + 4 * K::EPB);
   }
 };
 
@@ -201,7 +205,8 @@ __device__ __forceinline__ void volume(const Smem<C> &sm, double gamma_, int tid
       T U[5];
 #pragma unroll
       for (int n = 0; n < NF; ++n) U[n] = sm.B[(slot * NF + n) * QD + p];
-      volume_flux<PHYS, T>(U, gamma, F);
+      if constexpr (C::MIXED) volume_flux_pert<PHYS, T>(sm.ref[slot], U, gamma, F);
+      else volume_flux<PHYS, T>(U, gamma, F);
     }
   }
 #pragma unroll
@@ -212,7 +217,8 @@ __device__ __forceinline__ void volume(const Smem<C> &sm, double gamma_, int tid
         T U[5];
 #pragma unroll
         for (int n = 0; n < NF; ++n) U[n] = sm.B[(slot * NF + n) * QD + p];
-        volume_flux<PHYS, T>(U, gamma, F);
+        if constexpr (C::MIXED) volume_flux_pert<PHYS, T>(sm.ref[slot], U, gamma, F);
+        else volume_flux<PHYS, T>(U, gamma, F);
       }
       const double *met = sm.geo[slot].metric;
 #pragma unroll
@@ -263,12 +269,21 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
 #pragma unroll
     for (int n = 0; n < NF; ++n) { Uo[n] = eo[n * GF]; Un[n] = tn[n * GF]; }
     const bool master = (gc.master >> f) & 1;
-    bool ok;
-    if (master) ok = face_flux<PHYS, T>(Uo, Un, nm, T(a.gamma), a.flux, Fh, FL, FR);
-    else ok = face_flux<PHYS, T>(Un, Uo, nm, T(a.gamma), a.flux, Fh, FL, FR);
     const T jr = T(gc.jr[f]);
+    bool ok;
+    if constexpr (C::MIXED) {
+      // traces are perturbations about the solve's reference state
+      // (Fh - FL = Dm, FR - Fh = DF - Dm)
+      if (master) ok = face_flux_pert<PHYS, T>(sm.ref[slot], Uo, Un, nm, T(a.gamma), a.flux, Fh, FR);
+      else ok = face_flux_pert<PHYS, T>(sm.ref[slot], Un, Uo, nm, T(a.gamma), a.flux, Fh, FR);
 #pragma unroll
-    for (int n = 0; n < NF; ++n) eo[n * GF] = master ? (Fh[n] - FL[n]) * jr : (FR[n] - Fh[n]) * jr;
+      for (int n = 0; n < NF; ++n) eo[n * GF] = master ? Fh[n] * jr : (FR[n] - Fh[n]) * jr;
+    } else {
+      if (master) ok = face_flux<PHYS, T>(Uo, Un, nm, T(a.gamma), a.flux, Fh, FL, FR);
+      else ok = face_flux<PHYS, T>(Un, Uo, nm, T(a.gamma), a.flux, Fh, FL, FR);
+#pragma unroll
+      for (int n = 0; n < NF; ++n) eo[n * GF] = master ? (Fh[n] - FL[n]) * jr : (FR[n] - Fh[n]) * jr;
+    }
     if constexpr (PHYS == DGMX_NS2D || PHYS == DGMX_NS3D) {
       // BR1 viscous lift: '-' average of the viscous normal-flux traces in
       // the master frame (src/Domain.cpp:1883-1937), subtracted like
@@ -336,12 +351,21 @@ __device__ __forceinline__ void lift(const Smem<C> &sm, int tid) {
   __syncthreads();
 }
 
+// Solve (reference-state row) of element e; 0 for a single-solve domain.
+__device__ __forceinline__ int solve_of(const StageArgs &a, int e) {
+  return (e >= 0 && a.esolve) ? a.esolve[e] : 0;
+}
+
 template <class C>
 __device__ __forceinline__ void load_geometry(const Smem<C> &sm, const StageArgs &a, int e0, int tid) {
   for (int s = tid; s < C::EPB; s += C::NT) {
     const int e = e0 + s;
-    sm.eid[s] = e < a.ne ? e : -1;
-    sm.geo[s] = a.classes[e < a.ne ? a.gclass[e] : 0];
+    // elements past the end, and unallocated pool elements (class < 0),
+    // are skipped
+    const int gc = e < a.ne ? a.gclass[e] : -1;
+    sm.eid[s] = gc >= 0 ? e : -1;
+    sm.geo[s] = a.classes[gc >= 0 ? gc : 0];
+    if constexpr (C::MIXED) sm.ref[s] = make_ref<C::PHYSICS, typename C::R>(a.uref + 10 * solve_of(a, gc >= 0 ? e : -1), a.gamma);
   }
   for (int w = tid; w < C::EPB * C::NFACE; w += C::NT) {
     const int s = w / C::NFACE, f = w - s * C::NFACE, e = e0 + s;
@@ -357,6 +381,24 @@ __device__ __forceinline__ void load_modal(typename C::R *dst, const S *src, int
   for (int w = tid; w < C::EPB * BLK; w += C::NT) {
     const int s = w / BLK, e = e0 + s;
     dst[w] = e < ne ? T(src[(size_t)e0 * BLK + w]) : T(w % C::LD == 0 ? 1.0 : 0.0);
+  }
+}
+
+// Mixed form: the FP32 working copy of a modal register is the perturbation
+// about the solve's reference state, formed in FP64 (only the constant mode
+// carries the reference: uref[10 s + 5 + n]).
+template <class C>
+__device__ __forceinline__ void load_modal_pert(float *dst, const double *src, const StageArgs &a, int e0,
+                                                int tid) {
+  constexpr int BLK = C::NF * C::LD;
+  for (int w = tid; w < C::EPB * BLK; w += C::NT) {
+    const int s = w / BLK, e = e0 + s, m = w % C::LD;
+    double x = 0.0;
+    if (e < a.ne) {
+      x = src[(size_t)e0 * BLK + w];
+      if (m == 0) x -= a.uref[10 * solve_of(a, e) + 5 + (w % BLK) / C::LD];
+    }
+    dst[w] = float(x);
   }
 }
 
@@ -393,9 +435,16 @@ __global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<C> sm(smem_raw);
   const int tid = threadIdx.x;
-  const int e0 = blockIdx.x * C::EPB;
+  // One tile per CTA, or, with a tile list (element pools), a persistent
+  // loop over the listed tiles; the count is read on the device so a
+  // captured graph stays valid while solves join and leave.
+  const int ntile = a.tiles ? *a.ntiles : (int)gridDim.x;
+  for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
+  if (t != (int)blockIdx.x) __syncthreads();
+  const int e0 = (a.tiles ? a.tiles[t] : t) * C::EPB;
   load_geometry<C>(sm, a, e0, tid);
-  load_modal<C>(sm.A, a.X, e0, a.ne, tid);
+  if constexpr (C::MIXED) load_modal_pert<C>(sm.A, a.X, a, e0, tid);
+  else load_modal<C>(sm.A, a.X, e0, a.ne, tid);
   load_own_traces<C>(sm.E, trace_in<C>(a), e0, a.ne, tid);
   __syncthreads();
   backward<C>(sm.A, sm.B, sm.S, sm.C, tid, C::NT);
@@ -407,8 +456,9 @@ __global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
   constexpr int BLK = C::NF * C::LD;
   for (int w = tid; w < C::EPB * BLK; w += C::NT) {
     const int s = w / BLK, e = e0 + s;
-    if (e >= a.ne) continue;
+    if (sm.eid[s] < 0) continue;
     const size_t gi = (size_t)e0 * BLK + w;
+    const double dt = a.dte ? a.dte[e] : a.dt;   // per-element step (pools)
     if constexpr (C::MIXED) {
       // FP32 right-hand side and second register, FP64 solution register:
       // Ut = A Ut - dt R in FP32; U = U + B Ut accumulated in FP64.
@@ -420,9 +470,11 @@ __global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
         next = sm.A[w];
       } else {
         float ut = float(a.c0) * a.Utf[gi];
-        ut = fmaf(-float(a.dt), r, ut);
+        ut = fmaf(-float(dt), r, ut);
         const double u = fma(a.c1, double(ut), a.U[gi]);
-        a.Utf[gi] = ut; a.U[gi] = u; next = float(u);
+        a.Utf[gi] = ut; a.U[gi] = u;
+        const int m = w % C::LD;
+        next = float(m == 0 ? u - a.uref[10 * solve_of(a, e) + 5 + (w % BLK) / C::LD] : u);
       }
       sm.A[w] = next;
       continue;
@@ -439,25 +491,25 @@ __global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
       switch (a.kind) {
         case kLSRK: {
           double ut = a.c0 * a.Ut[gi];
-          ut = fma(-a.dt, r, ut);
+          ut = fma(-dt, r, ut);
           const double u = fma(a.c1, ut, x);
           a.Ut[gi] = ut; a.U[gi] = u; next = u;
           break;
         }
         case kTVD0: {
-          const double ut = fma(-a.dt, r, x);
+          const double ut = fma(-dt, r, x);
           a.Ut[gi] = ut; next = ut;
           break;
         }
         case kTVD1: {
-          const double t = fma(-a.dt, r, x);
+          const double t = fma(-dt, r, x);
           double ut = a.c1 * t;
           ut = fma(a.c0, a.U[gi], ut);
           a.Ut[gi] = ut; next = ut;
           break;
         }
         case kTVD2: {
-          const double t = fma(-a.dt, r, x);
+          const double t = fma(-dt, r, x);
           double u = a.c0 * a.U[gi];
           u = fma(a.c1, t, u);
           a.U[gi] = u; next = u;
@@ -490,6 +542,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
   __syncthreads();
   modal_traces<C>(sm.A, sm.E, sm.S, sm.B, tid, C::NT);
   store_traces<C>(sm.E, trace_out<C>(a), e0, a.ne, tid);
+  }
 }
 
 // Traces of a modal register (start of a run, after set_state).
@@ -498,7 +551,8 @@ __global__ void __launch_bounds__(C::NT, C::MINB) traces_modal_kernel(StageArgs 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<C> sm(smem_raw);
   const int tid = threadIdx.x, e0 = blockIdx.x * C::EPB;
-  load_modal<C>(sm.A, Xm, e0, a.ne, tid);
+  if constexpr (C::MIXED) load_modal_pert<C>(sm.A, Xm, a, e0, tid);
+  else load_modal<C>(sm.A, Xm, e0, a.ne, tid);
   __syncthreads();
   modal_traces<C>(sm.A, sm.E, sm.S, sm.B, tid, C::NT);
   store_traces<C>(sm.E, T, e0, a.ne, tid);
