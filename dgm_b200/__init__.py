@@ -237,3 +237,134 @@ class Domain:
     def stream(self) -> int:
         """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
         return lib().dgmx_stream(self.h) or 0
+
+
+class _PoolParams(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("flux", ctypes.c_int), ("device", ctypes.c_int),
+                ("autotune", ctypes.c_int), ("gamma", ctypes.c_double), ("budget_bytes", ctypes.c_size_t)]
+
+
+def _pool_lib():
+    L = lib()
+    if not getattr(L, "_pool_ready", False):
+        P, D, I = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int
+        L.dgmx_pool_create.argtypes = [ctypes.POINTER(_PoolParams), ctypes.POINTER(P)]
+        L.dgmx_pool_destroy.argtypes = [P]
+        L.dgmx_pool_prepare.argtypes = [P, I, I, I, I]
+        L.dgmx_pool_add.argtypes = [P, ctypes.POINTER(_Mesh), I, D, ctypes.c_double, ctypes.c_double,
+                                    ctypes.POINTER(I)]
+        L.dgmx_pool_step.argtypes = [P, I]
+        L.dgmx_pool_finished.argtypes = [P, ctypes.POINTER(I), I, ctypes.POINTER(I)]
+        L.dgmx_pool_get_state.argtypes = [P, I, D]
+        L.dgmx_pool_solve_info.argtypes = [P, I, D, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(I)]
+        L.dgmx_pool_remove.argtypes = [P, I]
+        L.dgmx_pool_stats.argtypes = [P, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(I), ctypes.POINTER(I),
+                                      ctypes.POINTER(ctypes.c_longlong)]
+        L.dgmx_pool_launch_count.argtypes = [P]
+        L.dgmx_pool_launch_count.restype = ctypes.c_long
+        L.dgmx_pool_last_error.argtypes = [P]
+        L.dgmx_pool_last_error.restype = ctypes.c_char_p
+        L._pool_ready = True
+    return L
+
+
+class PoolFull(DgmxError):
+    """The solve does not fit the pool's device-memory budget right now."""
+
+
+class Pool:
+    """Many independent LSRK14 solves on one GPU (include/dgmx_pool.h).
+
+    ``add`` admits a solve (mesh, physics, initial GLL values, step, end
+    time); ``step`` advances every unfinished solve; ``finished`` lists the
+    solves that reached their end time; ``state`` reads one back.
+    """
+
+    def __init__(self, precision: int = FP64, flux: str = "laxfriedrichs", gamma: float = 1.4,
+                 budget_bytes: int = 0, autotune: bool = True, device: int = 0):
+        p = _PoolParams(precision, FLUX[flux.lower()], device, 1 if autotune else 0, gamma, int(budget_bytes))
+        h = ctypes.c_void_p()
+        st = _pool_lib().dgmx_pool_create(ctypes.byref(p), ctypes.byref(h))
+        if st != 0:
+            raise DgmxError(st, "pool creation failed")
+        self.h = h
+        self.nf, self.nq = {}, {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            _pool_lib().dgmx_pool_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != 0:
+            msg = _pool_lib().dgmx_pool_last_error(self.h).decode()
+            cls = NonPhysicalState if st == 4 else (PoolFull if st == 6 else DgmxError)
+            raise cls(st, msg)
+
+    def prepare(self, physics: int, p: int, q: int = 0, elements: int = 0):
+        self._check(_pool_lib().dgmx_pool_prepare(self.h, physics, p, q, elements))
+
+    def add(self, mesh, physics: int, U0, dt: float, t_end: float) -> int:
+        verts = np.ascontiguousarray(mesh.verts, dtype=np.float64)
+        con = np.ascontiguousarray(mesh.con, dtype=np.int32)
+        por = np.ascontiguousarray(mesh.porder, dtype=np.int32)
+        qor = np.ascontiguousarray(mesh.qorder, dtype=np.int32)
+        ne = int(verts.shape[0])
+        nf = 3 if physics == SHALLOW else (5 if mesh.dim == 3 else 4)
+        q = int(qor[0]) if qor[0] else int(por[0]) + 2
+        nq = ne * q ** mesh.dim
+        U0 = np.ascontiguousarray(U0, dtype=np.float64).reshape(nf, nq)
+        m = _Mesh(int(mesh.dim), ne, _dp(verts), int(con.shape[0]),
+                  con.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                  por.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                  qor.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        sid = ctypes.c_int()
+        self._check(_pool_lib().dgmx_pool_add(self.h, ctypes.byref(m), physics, _dp(U0), float(dt),
+                                              float(t_end), ctypes.byref(sid)))
+        self.nf[sid.value], self.nq[sid.value] = nf, nq
+        return sid.value
+
+    def step(self, nsteps: int = 1):
+        self._check(_pool_lib().dgmx_pool_step(self.h, int(nsteps)))
+
+    def finished(self):
+        buf = (ctypes.c_int * 4096)()
+        out, n = [], ctypes.c_int()
+        while True:
+            self._check(_pool_lib().dgmx_pool_finished(self.h, buf, 4096, ctypes.byref(n)))
+            out += list(buf[: n.value])
+            if n.value < 4096:
+                return out
+
+    def state(self, sid: int):
+        U = np.zeros((self.nf[sid], self.nq[sid]))
+        self._check(_pool_lib().dgmx_pool_get_state(self.h, int(sid), _dp(U)))
+        return U
+
+    def info(self, sid: int):
+        """(time, steps taken, finished)."""
+        t, s, f = ctypes.c_double(), ctypes.c_long(), ctypes.c_int()
+        self._check(_pool_lib().dgmx_pool_solve_info(self.h, int(sid), ctypes.byref(t), ctypes.byref(s),
+                                                     ctypes.byref(f)))
+        return t.value, s.value, bool(f.value)
+
+    def remove(self, sid: int):
+        self._check(_pool_lib().dgmx_pool_remove(self.h, int(sid)))
+        self.nf.pop(sid, None)
+        self.nq.pop(sid, None)
+
+    def stats(self):
+        """(device bytes, resident solves, unfinished solves, unfinished modal DOF)."""
+        b, r, a, d = ctypes.c_size_t(), ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        self._check(_pool_lib().dgmx_pool_stats(self.h, ctypes.byref(b), ctypes.byref(r), ctypes.byref(a),
+                                                ctypes.byref(d)))
+        return b.value, r.value, a.value, d.value
+
+    def launch_count(self) -> int:
+        return _pool_lib().dgmx_pool_launch_count(self.h)

@@ -17,21 +17,11 @@ namespace {
 
 thread_local std::string g_create_error;
 
-// TVD-RK3 (src/TimeInt.cpp:738-740), RK4 (:204-209), LSRK14 (:1870-1917)
+// TVD-RK3 (src/TimeInt.cpp:738-740), RK4 (:204-209); LSRK14 is in dgmx_internal.hpp
 const double kTvdA[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0};
 const double kTvdB[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
 const double kRk4A[3] = {0.5, 0.5, 1.0};
 const double kRk4B[4] = {0.16666666666666667, 0.33333333333333333, 0.33333333333333333, 0.16666666666666667};
-const double kLsrkA[14] = {0.0, -0.7188012108672410, -0.7785331173421570, -0.0053282796654044,
-                           -0.8552979934029281, -3.9564138245774565, -1.5780575380587385,
-                           -2.0837094552574054, -0.7483334182761610, -0.7032861106563359,
-                           0.0013917096117681, -0.0932075369637460, -0.9514200470875948,
-                           -7.1151571693922548};
-const double kLsrkB[14] = {0.0367762454319673, 0.3136296607553959, 0.1531848691869027, 0.0030097086818182,
-                           0.3326293790646110, 0.2440251405350864, 0.3718879239592277, 0.6204126221582444,
-                           0.1524043173028741, 0.0760894927419266, 0.0077604214040978, 0.0024647284755382,
-                           0.0780348340049386, 5.5059777270269628};
-
 template <class T>
 cudaError_t dalloc(T **p, size_t n) {
   return cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * (n ? n : 1));

@@ -72,6 +72,17 @@ struct FileCase {
 };
 bool read_case_files(const std::string &root, FileCase &fc, std::string &err);
 
+// LSRK14 coefficients A and B (src/TimeInt.cpp:1870-1917)
+inline constexpr double kLsrkA[14] = {0.0, -0.7188012108672410, -0.7785331173421570, -0.0053282796654044,
+                           -0.8552979934029281, -3.9564138245774565, -1.5780575380587385,
+                           -2.0837094552574054, -0.7483334182761610, -0.7032861106563359,
+                           0.0013917096117681, -0.0932075369637460, -0.9514200470875948,
+                           -7.1151571693922548};
+inline constexpr double kLsrkB[14] = {0.0367762454319673, 0.3136296607553959, 0.1531848691869027, 0.0030097086818182,
+                           0.3326293790646110, 0.2440251405350864, 0.3718879239592277, 0.6204126221582444,
+                           0.1524043173028741, 0.0760894927419266, 0.0077604214040978, 0.0024647284755382,
+                           0.0780348340049386, 5.5059777270269628};
+
 // ------------------------------------------------------------------ kernels
 // Integrator stage kinds.  X is the register the RHS is evaluated on.
 enum StageKind : int {
@@ -119,10 +130,10 @@ struct StageArgs {
   const double *uref;
   const int *esolve;
   // element pools: persistent loop over tiles[0 .. *ntiles) (null: one
-  // tile per CTA) and a per-element step (null: dt)
+  // tile per CTA) and a step per solve, dts[esolve[e]] (null: dt)
   const int *tiles;
   const int *ntiles;
-  const double *dte;
+  const double *dts;
   // Navier-Stokes BR1 (src/Navier_Stokes3d.cpp:182-391)
   double *Ghat;           // projected primitive gradients, modal [e][comp][dir][L^d]
   double *V;              // viscous normal-flux traces [e][face][field-1][gf]
@@ -138,6 +149,9 @@ struct KernelOps {
   size_t smem = 0;
   cudaError_t (*init)(const Tables1D &t) = nullptr;   // tables + smem attributes, current device
   cudaError_t (*stage)(const StageArgs &a, cudaStream_t s) = nullptr;
+  // stage kernel on an explicit grid (persistent launch over a tile list)
+  cudaError_t (*stage_grid)(const StageArgs &a, int grid, cudaStream_t s) = nullptr;
+  int (*blocks_per_sm)() = nullptr;                    // resident stage CTAs per SM
   // T is double* (FP64 tiles) or float* (mixed tiles)
   cudaError_t (*traces_modal)(const StageArgs &a, const double *Xm, void *T, cudaStream_t s) = nullptr;
   cudaError_t (*traces_nodal)(const StageArgs &a, cudaStream_t s) = nullptr;

@@ -116,8 +116,21 @@ struct Launch {
       return cudaErrorNotSupported;
     }
   }
+  static cudaError_t stage_grid(const StageArgs &a, int g, cudaStream_t s) {
+    stage_kernel<C, PHYS><<<g, C::NT, C::SMEM, s>>>(a);
+    return cudaGetLastError();
+  }
+  static int blocks_per_sm() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_kernel<C, PHYS>, C::NT, C::SMEM) != cudaSuccess) {
+      cudaGetLastError();
+      return 1;
+    }
+    return n > 0 ? n : 1;
+  }
   static KernelOps ops() {
     KernelOps o;
+    o.stage_grid = stage_grid; o.blocks_per_sm = blocks_per_sm;
     o.epb = EPB; o.nt = C::NT; o.smem = C::SMEM; o.minb = MINB; o.mixed = MIXED;
     o.init = init; o.stage = stage; o.traces_modal = traces_modal; o.traces_nodal = traces_nodal;
     o.rhs_nodal = rhs_nodal; o.forward = forward; o.backward = backward;

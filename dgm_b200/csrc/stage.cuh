@@ -458,7 +458,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
     const int s = w / BLK, e = e0 + s;
     if (sm.eid[s] < 0) continue;
     const size_t gi = (size_t)e0 * BLK + w;
-    const double dt = a.dte ? a.dte[e] : a.dt;   // per-element step (pools)
+    const double dt = a.dts ? a.dts[solve_of(a, e)] : a.dt;   // per-solve step (pools)
     if constexpr (C::MIXED) {
       // FP32 right-hand side and second register, FP64 solution register:
       // Ut = A Ut - dt R in FP32; U = U + B Ut accumulated in FP64.
