@@ -1,18 +1,27 @@
 #!/usr/bin/env python3
-"""DOF-stage-updates/s of the B200 DG engine on the 3-D Euler Taylor-Green case.
+"""DOF-stage-updates/s of the B200 DG engine, mixed precision vs FP64 at
+matched L2 error, on the 3-D Euler Taylor-Green case; plus the batched
+ensemble and the serving loop (p50/p99 latency).
 
 Workload (the single-GPU configuration the metric is quoted on): periodic
 [0, 2pi]^3, 32^3 Hex elements, p = 3 (q = 5 GLL points per direction),
-compressible Euler, Lax-Friedrichs flux, low-storage RK (LSRK14, 14 stages),
-Mach 0.1 Taylor-Green initial condition, FP64.  dt is fixed once from CFL 0.5
-on the initial state.  A "step" is one LSRK14 step (14 fused stage launches).
+compressible Euler, Roe flux, low-storage RK (LSRK14, 14 stages), Mach 0.1
+Taylor-Green initial condition.  dt is fixed once from CFL 0.5 on the
+initial state.  A "step" is one LSRK14 step (14 fused stage launches).
 
-  value  device-resident throughput: modal DOF x 14 stages x K / time (CUDA
-         events on the engine's stream, max over ranks)
+  value  device-resident throughput of the mixed form (FP32 working
+         precision, FP64 solution register): modal DOF x 14 stages x K /
+         time (CUDA events on the engine's stream, max over ranks); the
+         plain FP64 path is measured the same way under "fp64", and
+         "accuracy" gives the mixed form's relative L2 distance from the
+         FP64 path after a fixed number of steps
   e2e    the same metric through the public C ABI with host buffers: every
          step uploads the state from pinned host memory (dgmx_set_state),
          advances one step (dgmx_advance) and reads the state back
          (dgmx_get_state)
+  forms  (one GPU) the batched ensemble of 1024 independent 2-D vortex
+         solves and a Poisson-arrival serving trace, both through the
+         element pool (include/dgmx_pool.h), FP64 and mixed
 Ranks (torchrun, N > 1) run independent replicas of the workload (weak
 scaling, no collective in the data path; NCCL only for the barrier and the
 max-over-ranks time).  --impl reference times the CPU restatement of the
@@ -35,9 +44,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = dict(name="euler3d_taylor_green_32^3_p3_lsrk14", n=32, p=3, q=5, Ma=0.1, gamma=1.4, cfl=0.5)
-METRIC = "DOF-stage-updates/s"
-BYTES_PER_DOF_STAGE = 32  # read U, read Ut, write Ut, write U (FP64)
+WORKLOAD = dict(name="euler3d_taylor_green_32^3_p3_roe_lsrk14", n=32, p=3, q=5, Ma=0.1, gamma=1.4, cfl=0.5,
+                flux="roe")
+METRIC = "DOF-stage-updates/s mixed vs FP64 at matched L2 err; p50/p99 solve latency"
+UNIT = "DOF-stage-updates/s"
+# algorithmic bytes per modal DOF and stage: read U, read Ut, write Ut, write U
+BYTES_PER_DOF_STAGE = {"fp64": 32, "mixed": 24}   # mixed: U FP64, Ut FP32
 
 
 def parse():
@@ -48,6 +60,10 @@ def parse():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n", type=int, default=WORKLOAD["n"], help="elements per direction")
+    ap.add_argument("--no-forms", action="store_true", help="skip the ensemble and serving legs")
+    ap.add_argument("--l2-steps", type=int, default=100, help="steps of the mixed-vs-FP64 accuracy run")
+    ap.add_argument("--ensemble", type=int, default=1024, help="solves in the batched ensemble")
+    ap.add_argument("--trace", type=int, default=200, help="requests in the serving trace")
     return ap.parse_args()
 
 
@@ -76,9 +92,9 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per stage launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "euler3d_tgv_p3_stage_kernel.md")
+def profile_traffic(name):
+    """DRAM bytes per stage launch from a committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_launch_full_workload:"):
@@ -142,7 +158,7 @@ def build_oracle_problem(n, p, q):
     import oracle
     from oracle import dgm_io
     mesh = dgm_io.box_mesh(3, (n, n, n), 0.0, 2 * math.pi, p, q)
-    return oracle.Problem(mesh, oracle.EULER3D)
+    return oracle.Problem(mesh, oracle.EULER3D, flux=WORKLOAD["flux"])
 
 
 def cpu_measure(n, p, q, stages_sample, threads):
@@ -163,11 +179,13 @@ def cpu_measure(n, p, q, stages_sample, threads):
 
 
 def config_dict(n, p, q, dof):
-    return {"workload": WORKLOAD["name"] if n == WORKLOAD["n"] else f"euler3d_taylor_green_{n}^3_p{p}_lsrk14",
+    return {"workload": WORKLOAD["name"] if n == WORKLOAD["n"] else f"euler3d_taylor_green_{n}^3_p{p}_roe_lsrk14",
             "mesh": f"{n}^3 Hex, periodic [0,2pi]^3", "p": p, "q": q, "physics": "Euler 3-D",
-            "flux": "Lax-Friedrichs", "integrator": "LSRK14 (14 stages/step)", "Mach": WORKLOAD["Ma"],
+            "flux": "Roe", "integrator": "LSRK14 (14 stages/step)", "Mach": WORKLOAD["Ma"],
             "modal_dof": dof, "cfl": WORKLOAD["cfl"],
-            "l2": "inputs larger than L2 (modal U+Ut 168 MB, traces 2x126 MB per replica)"}
+            "precision": "mixed: FP32 states, fluxes and contractions, FP64 solution register",
+            "l2": "inputs larger than L2 (modal U 84 MB + Ut 42 MB, traces 2x63 MB per replica in the mixed "
+                  "form; 168 + 2x126 MB in FP64)"}
 
 
 def run_reference(args):
@@ -191,15 +209,119 @@ def run_reference(args):
         P.advance(14, dt, 1)
     t = time.perf_counter() - t0
     v = dof * 14 * args.steps / t
-    out = {"metric": METRIC, "value": v, "unit": "DOF-stage-updates/s", "impl": "reference",
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference",
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (Taylor-Green initial condition)", "config": config_dict(n, p, q, dof),
-           "cpu_baseline": {"value": v, "unit": "DOF-stage-updates/s", "cores": threads, "kind": "port",
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                             "sample": f"{args.steps} LSRK14 steps of the full workload after {args.warmup} warm-up"},
-           "e2e": {"value": v, "unit": "DOF-stage-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return 0
+
+
+def rel_l2(a, b):
+    return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
+
+
+def time_steps(D, stream, dt, steps, warmup, barrier, max_over_ranks, clk=None):
+    """Device time of `steps` LSRK14 steps (CUDA events on the engine's stream)."""
+    import torch
+    for _ in range(warmup):
+        D.advance_async(dt, 1)
+    D.sync()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = D.launch_count()
+    if clk is not None:
+        clk.__enter__()
+    ev0.record(stream)
+    for _ in range(steps):
+        D.advance_async(dt, 1)
+    ev1.record(stream)
+    ev1.synchronize()
+    if clk is not None:
+        clk.__exit__(None, None, None)
+    launches = D.launch_count() - l0
+    D.sync()
+    barrier()
+    return max_over_ranks(ev0.elapsed_time(ev1) / 1e3), launches
+
+
+def forms(dgm_b200, args):
+    """The batched ensemble and the serving trace on this GPU (pool path)."""
+    from dgm_b200 import serving
+    res = {}
+    specs = serving.ensemble_requests(args.ensemble, seed=0)
+    ens = {}
+    for name, prec in (("fp64", dgm_b200.FP64), ("mixed", dgm_b200.MIXED)):
+        pool = dgm_b200.Pool(prec)
+        dof = 0
+        t0 = time.perf_counter()
+        for spec in specs:
+            r = serving.build(spec)
+            pool.add(r.mesh, r.physics, r.U0, r.dt, r.t_end)
+            dof += r.dof
+        setup = time.perf_counter() - t0
+        pool.step(3)
+        l0 = pool.launch_count()
+        k = 5
+        t0 = time.perf_counter()
+        pool.step(k)            # returns after the GPU has finished
+        t = time.perf_counter() - t0
+        ens[name] = {"value": dof * 14 * k / t, "unit": UNIT, "ms_per_step": 1e3 * t / k,
+                     "device_bytes": pool.stats()[0], "launches_per_step": (pool.launch_count() - l0) // k,
+                     "admission_s": round(setup, 2)}
+        pool.close()
+    ens["speedup_mixed_vs_fp64"] = ens["mixed"]["value"] / ens["fp64"]["value"]
+    ens["config"] = {"solves": args.ensemble, "modal_dof": dof, "physics": "Euler 2-D isentropic vortex, LF",
+                     "mesh": "N x N periodic Quad on [-5,5]^2, N ~ U{8..64}", "p": "U{2..7}, q = p+2",
+                     "beta": "U[1,5]", "centre": "U[-2,2]^2", "seed": 0,
+                     "launch": "one persistent stage launch per (order) arena per stage, one CUDA graph per "
+                               "arena step, arenas on concurrent streams; tiles autotuned per (physics, p)",
+                     "timing": f"{k} steps after 3, host clock around synchronous pool steps"}
+    res["ensemble"] = ens
+
+    trace = serving.poisson_trace(args.trace, rate=200.0, seed=1)
+    reqs = [serving.build(s) for s in trace]
+    work = sum(r.dof * 14 * int(math.ceil(r.t_end / r.dt)) for r in reqs)
+    span = reqs[-1].arrival
+    srv = {}
+    for name, prec in (("mixed", dgm_b200.MIXED), ("fp64", dgm_b200.FP64)):
+        pool = dgm_b200.Pool(prec, budget_bytes=40 << 30)
+        for ph in (dgm_b200.EULER2D, dgm_b200.SHALLOW):
+            for p in range(2, 7):
+                pool.prepare(ph, p, 0, 4096)
+        out = serving.serve(pool, reqs, readback=True)
+        # alone vs in the mix: re-run three served requests alone, compare
+        same = True
+        for rec_i in (0, len(out["records"]) // 2, len(out["records"]) - 1):
+            rec = sorted(out["records"], key=lambda x: x["arrival"])[rec_i]
+            r = next(q for q in reqs if q.arrival == rec["arrival"])
+            solo = dgm_b200.Pool(prec)
+            sid = solo.add(r.mesh, r.physics, r.U0, r.dt, r.t_end)
+            while not solo.info(sid)[2]:
+                solo.step(50)
+            same = same and bool(np.array_equal(solo.state(sid), rec["state"]))
+            solo.close()
+        cap = ens[name]["value"]
+        bound = 1.25 * (span + work / cap)
+        lat = np.array([x["latency"] for x in out["records"]])
+        srv[name] = {"p50_s": out["p50"], "p99_s": out["p99"], "p90_s": float(np.percentile(lat, 90)),
+                     "max_s": float(lat.max()), "throughput": out["throughput"], "unit": UNIT,
+                     "makespan_s": out["makespan"], "passes": out["passes"], "p99_bound_s": bound,
+                     "meets_p99_bound": bool(out["p99"] <= bound), "alone_equals_mix": same}
+        pool.close()
+    srv["config"] = {"requests": len(reqs), "rate_per_s": 200.0, "arrival_span_s": span, "seed": 1,
+                     "mix": "1/2 shallow-water Gaussian bump (a~U[0.1,0.5], w~U[0.2,1], g=9.81, still water), "
+                            "1/2 Euler vortex (beta~U[1,5], centre~U[-2,2]^2)",
+                     "dof": "log-uniform 1e3..1e6 modal", "p": "U{2..6}", "t_end": "U[0.5,5]",
+                     "budget_bytes": 40 << 30, "offered_work_dof_stages": work,
+                     "p99_bound": "1.25 x (arrival span + offered work / ensemble throughput of the same "
+                                  "precision): within 25% of a work-conserving schedule at batched throughput",
+                     "latency": "arrival to state read back on the host, wall clock"}
+    res["serving"] = srv
+    return res
 
 
 def main():
@@ -220,18 +342,7 @@ def main():
                                 device_id=torch.device("cuda", local))
     n, p, q = args.n, WORKLOAD["p"], WORKLOAD["q"]
     mesh = dgm_b200.meshgen.box(3, (n, n, n), 0.0, 2 * math.pi, p, q)
-    D = dgm_b200.Domain(mesh, dgm_b200.EULER3D, flux="laxfriedrichs", inttype=dgm_b200.LSRK14, device=local)
-    x, y, z = D.coordinates()
-    U_ic = taylor_green(x, y, z, WORKLOAD["Ma"], WORKLOAD["gamma"])
-    D.set_state(U_ic)
-    dt = cfl_dt(U_ic, 2 * math.pi / n, p, WORKLOAD["gamma"], WORKLOAD["cfl"])
     dof = 5 * n ** 3 * (p + 1) ** 3
-    stream = torch.cuda.ExternalStream(D.stream(), device=torch.device("cuda", local))
-    # tile autotuning is set-up, outside the timed region
-    tune_rows, tune_pick = D.autotune(reps=10)
-    tile = {"elements_per_cta": int(tune_rows[tune_pick][0]), "min_ctas_per_sm": int(tune_rows[tune_pick][1]),
-            "threads_per_cta": int(tune_rows[tune_pick][2]),
-            "candidates_us": [round(float(r[3]), 1) for r in tune_rows]}
 
     def barrier():
         if dist is not None:
@@ -245,27 +356,42 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---- device-resident fused LSRK14 steps
-    for _ in range(args.warmup):
-        D.advance_async(dt, 1)
-    D.sync()
-    barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    l0 = D.launch_count()
-    with ClockSampler(local) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            D.advance_async(dt, 1)
-        ev1.record(stream)
-        ev1.synchronize()
-    launches = D.launch_count() - l0
-    D.sync()
-    barrier()
-    t = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
-    value = world * dof * 14 * args.steps / t
-    stage_s = t / (14 * args.steps)
+    doms, tiles, results = {}, {}, {}
+    U_ic = dt = None
+    for name, prec in (("fp64", dgm_b200.FP64), ("mixed", dgm_b200.MIXED)):
+        D = dgm_b200.Domain(mesh, dgm_b200.EULER3D, flux=WORKLOAD["flux"], inttype=dgm_b200.LSRK14,
+                            device=local, precision=prec)
+        if U_ic is None:
+            x, y, z = D.coordinates()
+            U_ic = taylor_green(x, y, z, WORKLOAD["Ma"], WORKLOAD["gamma"])
+            dt = cfl_dt(U_ic, 2 * math.pi / n, p, WORKLOAD["gamma"], WORKLOAD["cfl"])
+        D.set_state(U_ic)
+        # tile autotuning is set-up, outside the timed region
+        rows, pick = D.autotune(reps=10)
+        tiles[name] = {"elements_per_cta": int(rows[pick][0]), "min_ctas_per_sm": int(rows[pick][1]),
+                       "threads_per_cta": int(rows[pick][2]), "candidates_us": [round(float(r[3]), 1) for r in rows]}
+        doms[name] = D
+    streams = {k: torch.cuda.ExternalStream(D.stream(), device=torch.device("cuda", local)) for k, D in doms.items()}
 
-    # ---- end to end through the C ABI with pinned host buffers
+    clk = ClockSampler(local)
+    t64, _ = time_steps(doms["fp64"], streams["fp64"], dt, args.steps, args.warmup, barrier, max_over_ranks)
+    tmx, launches = time_steps(doms["mixed"], streams["mixed"], dt, args.steps, args.warmup, barrier,
+                               max_over_ranks, clk)
+    value = world * dof * 14 * args.steps / tmx
+    v64 = world * dof * 14 * args.steps / t64
+
+    # accuracy: mixed vs the FP64 path (parity-tested against the oracle) from the same state
+    for D in doms.values():
+        D.set_state(U_ic)
+        D.advance(dt, args.l2_steps)
+    S64, Smx = doms["fp64"].state(), doms["mixed"].state()
+    accuracy = {"steps": args.l2_steps, "t": args.l2_steps * dt, "rel_l2_mixed_vs_fp64": rel_l2(Smx, S64),
+                "rel_l2_per_field": [rel_l2(Smx[k], S64[k]) for k in range(5)],
+                "rel_l2_of_state_change_fp64": rel_l2(S64, U_ic),
+                "note": "relative L2 over all GLL values; the FP64 path matches the FP64 oracle to 1e-12"}
+
+    # ---- end to end through the C ABI with pinned host buffers (mixed form)
+    D = doms["mixed"]
     Uh = torch.empty((5, D.nq), dtype=torch.float64, pin_memory=True).numpy()
     Uh[:] = D.state()
     for _ in range(max(1, args.warmup)):
@@ -275,45 +401,58 @@ def main():
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ke = max(3, args.steps // 2)
-    e0.record(stream)
+    e0.record(streams["mixed"])
     for _ in range(ke):
         D.set_state(Uh)
         D.advance(dt, 1)
         D.state_into(Uh)
-    e1.record(stream)
+    e1.record(streams["mixed"])
     e1.synchronize()
     barrier()
     te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
     e2e = world * dof * 14 * ke / te
     nbytes = 5 * D.nq * 8
 
-    out = {"metric": METRIC, "value": value, "unit": "DOF-stage-updates/s", "n_gpus": world,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
-           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+    peak, kind = peaks()
+    stage_mx, stage_64 = tmx / (14 * args.steps), t64 / (14 * args.steps)
+
+    def roof(prec, stage_s, prof):
+        a = BYTES_PER_DOF_STAGE[prec] * dof / stage_s / 1e9
+        return {"bound": "hbm", "achieved": a, "peak": peak, "unit": "GB/s", "frac": a / peak,
+                "peak_kind": kind, "traffic": profile_traffic(prof),
+                "kernel": f"stage_kernel<Euler3D, L=4, Q=5, {prec}> (one launch per LSRK stage)",
+                "algorithmic_bytes_per_launch": BYTES_PER_DOF_STAGE[prec] * dof,
+                "stage_us": 1e6 * stage_s}
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tmx / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 solution register)",
            "data": "synthetic (Taylor-Green initial condition, no dataset)",
            "config": config_dict(n, p, q, dof) | {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                                                  "tile": tile},
-           "e2e": {"value": e2e, "unit": "DOF-stage-updates/s", "h2d_bytes_per_step": nbytes,
+                                                  "tile": tiles["mixed"]},
+           "fp64": {"value": v64, "unit": UNIT, "ms_per_step": 1e3 * t64 / args.steps, "tile": tiles["fp64"],
+                    "roofline": roof("fp64", stage_64, "euler3d_tgv_p3_stage_kernel.md")},
+           "speedup_mixed_vs_fp64": value / v64,
+           "accuracy": accuracy,
+           "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                    "d2h_bytes_per_step": nbytes, "steps": ke,
-                   "path": "dgmx_set_state + dgmx_advance(1 step) + dgmx_get_state, pinned host buffers"},
-           "gpu_launches": int(launches), "clocks": clk.summary()}
-    peak, kind = peaks()
-    achieved = BYTES_PER_DOF_STAGE * dof / stage_s / 1e9
-    out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                       "frac": achieved / peak, "peak_kind": kind, "traffic": profile_traffic(),
-                       "kernel": "stage_kernel<Euler3D, L=4, Q=5> (one launch per LSRK stage)",
-                       "algorithmic_bytes_per_launch": BYTES_PER_DOF_STAGE * dof}
+                   "path": "dgmx_set_state + dgmx_advance(1 step) + dgmx_get_state, pinned host buffers, mixed form"},
+           "gpu_launches": int(launches), "clocks": clk.summary(),
+           "roofline": roof("mixed", stage_mx, "euler3d_tgv_p3_stage_mixed.md")}
+    for Dx in doms.values():
+        Dx.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         try:
             v, tc = cpu_measure(n, p, q, 1, threads)
-            out["cpu_baseline"] = {"value": v, "unit": "DOF-stage-updates/s", "cores": threads, "kind": "port",
-                                   "sample": f"1 LSRK14 step (14 stages) of the full workload, {tc:.1f} s"}
+            out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                                   "sample": f"1 LSRK14 step (14 stages) of the full workload, FP64, {tc:.1f} s"}
         except Exception as ex:  # the baseline never blocks the GPU number
             out["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
+    if rank == 0 and world == 1 and not args.no_forms:
+        out["forms"] = forms(dgm_b200, args)
     if rank == 0:
         print(json.dumps(out), flush=True)
-    D.close()
     if dist is not None:
         dist.destroy_process_group()
     return 0
