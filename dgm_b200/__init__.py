@@ -234,6 +234,21 @@ class Domain:
         self._check(f(self.h, int(reps), _dp(rows), 64, ctypes.byref(nv), ctypes.byref(ch)))
         return rows[: nv.value].copy(), ch.value
 
+    def set_variant(self, index: int):
+        """Use compiled tile variant `index`; returns (variant count, one element per warp)."""
+        f = lib().dgmx_set_variant
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        n, w = ctypes.c_int(), ctypes.c_int()
+        self._check(f(self.h, int(index), ctypes.byref(n), ctypes.byref(w)))
+        return n.value, bool(w.value)
+
+    def variant_count(self) -> int:
+        f = lib().dgmx_set_variant
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        n, w = ctypes.c_int(), ctypes.c_int()
+        f(self.h, -1, ctypes.byref(n), ctypes.byref(w))
+        return n.value
+
     def stream(self) -> int:
         """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
         return lib().dgmx_stream(self.h) or 0

@@ -214,6 +214,7 @@ dgmx_status check_error_word(dgmx_domain *d) {
   cudaError_t e = cudaMemcpyAsync(h, d->err, sizeof(h), cudaMemcpyDeviceToHost, d->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
   if (e != cudaSuccess) return d->cuda(e, "error word readback");
+  if (h[0] & 2) return d->fail(DGMX_ERR_CUDA, "a stage kernel's copy pipeline did not complete in time");
   if (h[0] & 1) {
     char buf[160];
     std::snprintf(buf, sizeof(buf), "non-physical state (density or pressure below eps^(2/3)) on element %d", h[1]);
@@ -662,6 +663,22 @@ dgmx_status dgmx_autotune(dgmx_domain *d, int reps, double *rows, int cap, int *
   if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
   if (nvariants) *nvariants = (int)vs->size();
   if (chosen) *chosen = best;
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_set_variant(dgmx_domain *d, int index, int *count, int *warp) {
+  if (!d) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(d->prm.device);
+  const std::vector<KernelOps> *vs = find_variants(d->prm.physics + (d->mixed() ? kMixedKey : 0), d->L, d->Q);
+  if (!vs || vs->empty()) return d->fail(DGMX_ERR_UNSUPPORTED, "no kernel variants");
+  if (count) *count = (int)vs->size();
+  if (index < 0 || index >= (int)vs->size()) return d->fail(DGMX_ERR_ARGUMENT, "no such variant");
+  const KernelOps &v = (*vs)[index];
+  const cudaError_t e = v.init(d->tab);
+  if (e != cudaSuccess) return d->cuda(e, "variant init");
+  if (d->mixed()) d->ops_m = &v; else d->ops = &v;
+  if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  if (warp) *warp = v.warp;
   return DGMX_OK;
 }
 

@@ -42,7 +42,7 @@ struct FaceLink {
   int elem;             // neighbour element
   int face;             // neighbour's face id
   int perm;             // offset of the point permutation in the perm table
-  int pad;
+  int cls;              // on face 0: the element's geometry class (-1: unallocated)
 };
 
 struct HostMesh {
@@ -146,6 +146,7 @@ constexpr int kMixedKey = 1000;
 // Launchers for one (physics, L, Q) instantiation; all enqueue on stream s.
 struct KernelOps {
   int epb = 0, nt = 0, minb = 0, mixed = 0;
+  int warp = 0;                                        // 1: one element per warp (epb = warps per CTA)
   size_t smem = 0;
   cudaError_t (*init)(const Tables1D &t) = nullptr;   // tables + smem attributes, current device
   cudaError_t (*stage)(const StageArgs &a, cudaStream_t s) = nullptr;

@@ -37,36 +37,47 @@ template <int L, int Q, class T = double> struct MatGL2G{ static __device__ __fo
 // Contraction along axis AX of a batch of 3-D arrays (I0, I1, I2) with
 // I_AX = K: out[...n...] = sum_k M(k, n) in[...k...], N outputs per pencil.
 // Each thread owns one pencil: K loads, K*N FMAs with uniform coefficients.
-// Batch b reads in + b*sin and writes out + b*sout.
-template <int I0, int I1, int I2, int AX, int K, int N, class M, bool ACC, class T>
+// Batch b reads in + b*sin and writes out + b*sout.  Axis 2 is contiguous;
+// the strides of axes 0 and 1 default to the dense layout and may be given
+// (IS0, IS1 input; OS0, OS1 output) to address rows padded to an odd pitch,
+// which keeps a warp's pencils on distinct shared-memory banks.
+//
+// FPT > 1 gives each thread the same pencil of FPT consecutive batches (the
+// fields of one element): one index computation serves FPT pencils and the
+// thread has FPT independent FMA chains (the one-element-per-warp tiles).
+template <int I0, int I1, int I2, int AX, int K, int N, class M, bool ACC, class T, int IS0 = -1, int IS1 = -1,
+          int OS0 = -1, int OS1 = -1, int FPT = 1>
 __device__ __forceinline__ void contract(const T *__restrict__ in, T *__restrict__ out, int nbatch,
                                          int sin, int sout, int tid, int nthr) {
   constexpr int O1 = AX == 1 ? N : I1, O2 = AX == 2 ? N : I2;
   constexpr int P0 = AX == 0 ? I1 : I0;
   constexpr int P1 = AX == 2 ? I1 : I2;
   constexpr int NP = P0 * P1;
-  constexpr int is0 = I1 * I2, is1 = I2;
-  constexpr int os0 = O1 * O2, os1 = O2;
+  constexpr int is1 = IS1 >= 0 ? IS1 : I2, is0 = IS0 >= 0 ? IS0 : I1 * is1;
+  constexpr int os1 = OS1 >= 0 ? OS1 : O2, os0 = OS0 >= 0 ? OS0 : O1 * os1;
   constexpr int isA = AX == 0 ? is0 : (AX == 1 ? is1 : 1);
   constexpr int osA = AX == 0 ? os0 : (AX == 1 ? os1 : 1);
-  for (int w = tid; w < nbatch * NP; w += nthr) {
-    const int b = w / NP, p = w - b * NP;
+  for (int w = tid; w < (nbatch / FPT) * NP; w += nthr) {
+    const int b = (w / NP) * FPT, p = w - (w / NP) * NP;
     const int pa = p / P1, pb = p - pa * P1;
     int io, oo;
     if (AX == 0) { io = pa * is1 + pb; oo = pa * os1 + pb; }
     else if (AX == 1) { io = pa * is0 + pb; oo = pa * os0 + pb; }
     else { io = pa * is0 + pb * is1; oo = pa * os0 + pb * os1; }
-    const T *src = in + (size_t)b * sin + io;
-    T *dst = out + (size_t)b * sout + oo;
-    T v[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = src[k * isA];
+    for (int f = 0; f < FPT; ++f) {
+      const T *src = in + (size_t)(b + f) * sin + io;
+      T *dst = out + (size_t)(b + f) * sout + oo;
+      T v[K];
 #pragma unroll
-    for (int n = 0; n < N; ++n) {
-      T acc = T(0);
+      for (int k = 0; k < K; ++k) v[k] = src[k * isA];
 #pragma unroll
-      for (int k = 0; k < K; ++k) acc = fma(M::get(k, n), v[k], acc);
-      if (ACC) dst[n * osA] += acc; else dst[n * osA] = acc;
+      for (int n = 0; n < N; ++n) {
+        T acc = T(0);
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc = fma(M::get(k, n), v[k], acc);
+        if (ACC) dst[n * osA] += acc; else dst[n * osA] = acc;
+      }
     }
   }
 }

@@ -253,6 +253,7 @@ bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::strin
     } else {
       out.gclass[e] = it->second;
     }
+    out.links[(size_t)e * nfaces].cls = out.gclass[e];
   }
   return true;
 }

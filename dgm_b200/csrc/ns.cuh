@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) ns_grad_kernel(StageArgs a) {
   } else {
     load_modal<C>(A, a.X, e0, a.ne, tid);
   }
-  load_own_traces<C>(E, a.Tin, e0, a.ne, tid);
+  load_own_traces<C, double, false>(E, a.Tin, e0, a.ne, tid);
   __syncthreads();
   load_nbr_traces<C>(E2, a.Tin, lnk, eid, a.perm, tid);
   if constexpr (!NODAL) {

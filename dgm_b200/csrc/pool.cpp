@@ -432,6 +432,7 @@ dgmx_status check_arena_error(dgmx_pool *P, int ai) {
   cudaError_t e = cudaMemcpyAsync(h, a.err, sizeof(h), cudaMemcpyDeviceToHost, a.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(a.stream);
   if (e != cudaSuccess) return P->cuda(e, "error word readback");
+  if (h[0] & 2) return P->fail(DGMX_ERR_CUDA, "a stage kernel's copy pipeline did not complete in time");
   if (!(h[0] & 1)) return DGMX_OK;
   int sid = -1;
   for (auto &kv : P->solves)
@@ -523,7 +524,7 @@ dgmx_status add_impl(dgmx_pool *P, const dgmx_mesh *m, int phys, const double *U
   }
   // host records of the range; padding slots keep class -1
   std::vector<int> gcl(nalloc, -1), es(nalloc, slot);
-  std::vector<FaceLink> lks((size_t)nalloc * a.nfaces, FaceLink{0, 0, 0, 0});
+  std::vector<FaceLink> lks((size_t)nalloc * a.nfaces, FaceLink{0, 0, 0, -1});
   for (int e = 0; e < ne; ++e) {
     gcl[e] = cmap[hm.gclass[e]];
     for (int f = 0; f < a.nfaces; ++f) {
@@ -532,6 +533,7 @@ dgmx_status add_impl(dgmx_pool *P, const dgmx_mesh *m, int phys, const double *U
       lk.perm = pmap[lk.perm];
       lks[(size_t)e * a.nfaces + f] = lk;
     }
+    lks[(size_t)e * a.nfaces].cls = gcl[e];
   }
   // reference state of the mixed form: the J- and GLL-weighted mean of U0
   double ref[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};

@@ -42,6 +42,8 @@ struct Cfg {
   // working precision: FP64, or FP32 for the mixed form (the solution
   // register U stays FP64 in global memory)
   static constexpr bool MIXED = MIXED_;
+  static constexpr bool WARP = false;   // the helpers' team is the whole CTA
+  static constexpr int FPT = 1;         // fields per contraction task
   static constexpr int PHYSICS = PHYS;
   using R = std::conditional_t<MIXED_, float, double>;
   static constexpr int DIM = phys_dim(PHYS), NF = phys_nf(PHYS);
@@ -51,24 +53,57 @@ struct Cfg {
   static constexpr int GF = Pow<G, DIM - 1>::v, QF = Pow<Q, DIM - 1>::v, LF = Pow<L, DIM - 1>::v;
   static constexpr int NT = cmax(64, ((EPB * QD + 31) / 32) * 32 > 1024 ? 1024 : ((EPB * QD + 31) / 32) * 32);
   // per-slot region sizes (doubles)
-  static constexpr int SZ_A = NF * LD;                 // modal register
+  // Rows of an even number of values are stored at an odd pitch in shared
+  // memory, so the pencils a warp reads (one per lane, K apart) fall on
+  // distinct banks: modal rows of L (when L + 1 <= Q, so the padded
+  // intermediates still fit their regions) and face-trace rows of G.
+  static constexpr int PL = (L_ % 2 == 0 && L_ + 1 <= Q_) ? L_ + 1 : L_;
+  static constexpr int PG = (G % 2 == 0) ? G + 1 : G;
+  static constexpr int AB = DIM == 3 ? L_ * L_ * PL : L_ * PL;   // modal block (slot, field), padded
+  static constexpr int EB = DIM == 3 ? G * PG : PG;              // face-trace block (face, slot, field)
+  static constexpr int SZ_A = NF * AB;                 // modal register
   static constexpr int SZ_B = NF * QD;                 // GLL values
   static constexpr int SZ_C = NF * QD;                 // flux / scratch
   static constexpr int SZ_D = NF * QD;                 // divergence + lift
-  static constexpr int SZ_E = NFACE * NF * GF;         // face traces / lift input
+  static constexpr int SZ_E = NFACE * NF * EB;         // face traces / lift input
   // projected RHS (modal); shares the E region when it fits (E is dead
   // between the lift and the next-trace phase)
-  static constexpr bool R_IN_E = NFACE * NF * GF >= NF * LD;
+  static constexpr bool R_IN_E = NFACE * NF * EB >= NF * LD;
   static constexpr int SZ_R = R_IN_E ? 0 : NF * LD;
-  static constexpr int SZ_S = cmax(cmax(NF * Q * LF, NFACE * NF * LF), DIM == 3 ? NFACE * NF * Q * G : 0);
+  static constexpr int SZ_S = cmax(cmax(NF * Q * (DIM == 3 ? LF : PL), NFACE * NF * (DIM == 3 ? LF : PL)),
+                                   DIM == 3 ? NFACE * NF * Q * PG : 0);
   static constexpr int SZ_SLOT = SZ_A + SZ_B + SZ_C + SZ_D + SZ_E + SZ_R + SZ_S;
   static constexpr size_t DATA = ((size_t)EPB * SZ_SLOT * sizeof(R) + 15) / 16 * 16;
   static constexpr size_t SMEM = DATA + (size_t)EPB * (sizeof(GeomClass) + NFACE * sizeof(FaceLink) + 16 +
                                                      (MIXED_ ? sizeof(RefState<R>) : 0));
   static_assert(NFACE * QF <= 2 * QD, "lift face buffer must fit in the B+C regions");
-  static_assert(DIM == 2 || NFACE * G * L <= 2 * QD, "trace intermediate must fit in the B+C regions");
+  static_assert(DIM == 2 || NFACE * G * PL <= 2 * QD, "trace intermediate must fit in the B+C regions");
+  static_assert(PL <= Q, "padded modal rows must fit the GLL-sized scratch");
   static_assert(SMEM <= 227 * 1024 || EPB > 1, "element slot does not fit in shared memory");
 };
+
+// One element per warp: the per-element regions of the EPB = 1 tile C1,
+// WPB of them per CTA (one per warp).  The helpers run with the warp as
+// their team: NT = 32 threads and __syncwarp between phases, so the warps of
+// a CTA never wait for one another.
+template <class C1, int WPB_, int MINB_ = 0>
+struct WarpCfg : C1 {
+  static_assert(C1::EPB == 1, "a warp holds one element");
+  static constexpr bool WARP = true;
+  static constexpr int NT = 32;
+  static constexpr int FPT = C1::NF;
+  static constexpr int WPB = WPB_;
+  static constexpr int CTA_NT = 32 * WPB_;
+  static constexpr int MINB = MINB_ > 0 ? MINB_ : 1;
+  static constexpr size_t SLOT = (C1::SMEM + 127) / 128 * 128;   // shared bytes per warp
+  static constexpr size_t SMEM_CTA = SLOT * WPB_;
+};
+
+// Barrier of the helpers' team.
+template <class C>
+__device__ __forceinline__ void csync() {
+  if constexpr (C::WARP) __syncwarp(); else __syncthreads();
+}
 
 // Trailing-1 shapes so one contraction routine serves 2-D and 3-D.
 template <int DIM, int N> struct Sh3 { static constexpr int a = N, b = N, c = (DIM == 3 ? N : 1); };
@@ -108,6 +143,16 @@ template <int DIM> __device__ __host__ constexpr int face_end(int f) {
   return DIM == 3 ? (f == 2 || f == 3 || f == 5) : (f == 1 || f == 2);
 }
 
+// Offset of face point g (0 .. GF-1) inside a padded trace block, and of
+// modal entry m (row-major, rows of L) inside a padded modal block.
+template <class C>
+__device__ __forceinline__ int epos(int g) {
+  if constexpr (C::DIM == 3) return (g / C::G) * C::PG + g % C::G;
+  else return g;
+}
+template <class C>
+__device__ __forceinline__ int apos(int m) { return (m / C::L) * C::PL + m % C::L; }
+
 template <int L, int Q, int END, class T>
 struct MatEnd { static __device__ __forceinline__ T get(int a, int) { return cEnd<T, L, Q>[END * L + a]; } };
 
@@ -118,8 +163,10 @@ __device__ __forceinline__ void face_reduce(const typename C::R *A, typename C::
   constexpr int DIM = C::DIM, L = C::L, Q = C::Q;
   constexpr int AX = face_axis<DIM>(F), END = face_end<DIM>(F);
   using Sh = Sh3<DIM, L>;
-  contract<Sh::a, Sh::b, Sh::c, AX, L, 1, MatEnd<L, Q, END, typename C::R>, false>(A, out + F * C::EPB * C::NF * C::LF,
-                                                                     C::EPB * C::NF, C::LD, C::LF, tid, nthr);
+  constexpr int IS0 = DIM == 3 ? L * C::PL : C::PL, IS1 = DIM == 3 ? C::PL : 1;
+  constexpr int OB = DIM == 3 ? C::LF : C::PL;   // output block: an L x L plane, or a padded line
+  contract<Sh::a, Sh::b, Sh::c, AX, L, 1, MatEnd<L, Q, END, typename C::R>, false, typename C::R, IS0, IS1, -1, -1, C::FPT>(
+      A, out + F * C::EPB * C::NF * OB, C::EPB * C::NF, C::AB, OB, tid, nthr);
 }
 
 // Traces at the side Gauss points of a modal register held in smem A.
@@ -137,36 +184,39 @@ __device__ __forceinline__ void modal_traces(const typename C::R *A, typename C:
     face_reduce<C, 4>(A, S, tid, nthr);
     face_reduce<C, 5>(A, S, tid, nthr);
   }
-  __syncthreads();
-  constexpr int NB = C::NFACE * C::EPB * C::NF;
+  csync<C>();
+  constexpr int NB = C::NFACE * C::EPB * C::NF, PL = C::PL, PG = C::PG;
   if constexpr (DIM == 3) {
-    contract<L, L, 1, 0, L, G, MatBg<L, Q, T>, false>(S, Cs, NB, L * L, G * L, tid, nthr);
-    __syncthreads();
-    contract<G, L, 1, 1, L, G, MatBg<L, Q, T>, false>(Cs, E, NB, G * L, G * G, tid, nthr);
+    contract<L, L, 1, 0, L, G, MatBg<L, Q, T>, false, T, -1, -1, PL, 1, C::FPT>(S, Cs, NB, L * L, G * PL, tid, nthr);
+    csync<C>();
+    contract<G, L, 1, 1, L, G, MatBg<L, Q, T>, false, T, PL, 1, PG, 1, C::FPT>(Cs, E, NB, G * PL, C::EB, tid, nthr);
   } else {
-    contract<L, 1, 1, 0, L, G, MatBg<L, Q, T>, false>(S, E, NB, L, G, tid, nthr);
+    contract<L, 1, 1, 0, L, G, MatBg<L, Q, T>, false, typename C::R, -1, -1, -1, -1, C::FPT>(S, E, NB, PL, C::EB, tid, nthr);
   }
-  __syncthreads();
+  csync<C>();
 }
 
-// Backward transform: modal A [slot][n][LD] -> GLL B [slot][n][QD].
-template <class C>
+// Backward transform: modal A [slot][n][L^d] -> GLL B [slot][n][QD].  A is
+// the padded modal block (PADDED) or a dense one.
+template <class C, bool PADDED = true>
 __device__ __forceinline__ void backward(const typename C::R *A, typename C::R *B, typename C::R *S,
                                          typename C::R *Cs, int tid, int nthr) {
   using T = typename C::R;
-  constexpr int L = C::L, Q = C::Q, NB = C::EPB * C::NF;
+  constexpr int L = C::L, Q = C::Q, NB = C::EPB * C::NF, PL = C::PL;
+  constexpr int AP = PADDED ? PL : L, ABLK = PADDED ? C::AB : C::LD;
   if constexpr (C::DIM == 3) {
-    contract<L, L, L, 0, L, Q, MatB<L, Q, T>, false>(A, S, NB, C::LD, Q * L * L, tid, nthr);
-    __syncthreads();
-    contract<Q, L, L, 1, L, Q, MatB<L, Q, T>, false>(S, Cs, NB, Q * L * L, Q * Q * L, tid, nthr);
-    __syncthreads();
-    contract<Q, Q, L, 2, L, Q, MatB<L, Q, T>, false>(Cs, B, NB, Q * Q * L, C::QD, tid, nthr);
+    contract<L, L, L, 0, L, Q, MatB<L, Q, T>, false, T, L * AP, AP, -1, -1, C::FPT>(A, S, NB, ABLK, Q * L * L, tid, nthr);
+    csync<C>();
+    contract<Q, L, L, 1, L, Q, MatB<L, Q, T>, false, T, -1, -1, Q * PL, PL, C::FPT>(S, Cs, NB, Q * L * L, Q * Q * PL, tid,
+                                                                            nthr);
+    csync<C>();
+    contract<Q, Q, L, 2, L, Q, MatB<L, Q, T>, false, T, Q * PL, PL, -1, -1, C::FPT>(Cs, B, NB, Q * Q * PL, C::QD, tid, nthr);
   } else {
-    contract<L, L, 1, 0, L, Q, MatB<L, Q, T>, false>(A, S, NB, C::LD, Q * L, tid, nthr);
-    __syncthreads();
-    contract<Q, L, 1, 1, L, Q, MatB<L, Q, T>, false>(S, B, NB, Q * L, C::QD, tid, nthr);
+    contract<L, L, 1, 0, L, Q, MatB<L, Q, T>, false, T, AP, 1, PL, 1, C::FPT>(A, S, NB, ABLK, Q * PL, tid, nthr);
+    csync<C>();
+    contract<Q, L, 1, 1, L, Q, MatB<L, Q, T>, false, T, PL, 1, -1, -1, C::FPT>(S, B, NB, Q * PL, C::QD, tid, nthr);
   }
-  __syncthreads();
+  csync<C>();
 }
 
 // Forward projection: GLL D [slot][n][QD] (already w-weighted) -> modal R.
@@ -174,19 +224,20 @@ template <class C>
 __device__ __forceinline__ void forward(const typename C::R *D, typename C::R *R, typename C::R *Cs,
                                         typename C::R *Bs, int tid, int nthr) {
   using T = typename C::R;
-  constexpr int L = C::L, Q = C::Q, NB = C::EPB * C::NF;
+  constexpr int L = C::L, Q = C::Q, NB = C::EPB * C::NF, PL = C::PL;
+  // the contiguous axis first, into rows of L at the odd pitch PL
   if constexpr (C::DIM == 3) {
-    contract<Q, Q, Q, 0, Q, L, MatBt<L, Q, T>, false>(D, Cs, NB, C::QD, L * Q * Q, tid, nthr);
-    __syncthreads();
-    contract<L, Q, Q, 1, Q, L, MatBt<L, Q, T>, false>(Cs, Bs, NB, L * Q * Q, L * L * Q, tid, nthr);
-    __syncthreads();
-    contract<L, L, Q, 2, Q, L, MatBt<L, Q, T>, false>(Bs, R, NB, L * L * Q, C::LD, tid, nthr);
+    contract<Q, Q, Q, 2, Q, L, MatBt<L, Q, T>, false, T, -1, -1, Q * PL, PL, C::FPT>(D, Cs, NB, C::QD, Q * Q * PL, tid, nthr);
+    csync<C>();
+    contract<Q, Q, L, 1, Q, L, MatBt<L, Q, T>, false, T, Q * PL, PL, -1, -1, C::FPT>(Cs, Bs, NB, Q * Q * PL, Q * L * L, tid, nthr);
+    csync<C>();
+    contract<Q, L, L, 0, Q, L, MatBt<L, Q, T>, false, typename C::R, -1, -1, -1, -1, C::FPT>(Bs, R, NB, Q * L * L, C::LD, tid, nthr);
   } else {
-    contract<Q, Q, 1, 0, Q, L, MatBt<L, Q, T>, false>(D, Cs, NB, C::QD, L * Q, tid, nthr);
-    __syncthreads();
-    contract<L, Q, 1, 1, Q, L, MatBt<L, Q, T>, false>(Cs, R, NB, L * Q, C::LD, tid, nthr);
+    contract<Q, Q, 1, 1, Q, L, MatBt<L, Q, T>, false, T, -1, -1, PL, 1, C::FPT>(D, Cs, NB, C::QD, Q * PL, tid, nthr);
+    csync<C>();
+    contract<Q, L, 1, 0, Q, L, MatBt<L, Q, T>, false, T, PL, 1, -1, -1, C::FPT>(Cs, R, NB, Q * PL, C::LD, tid, nthr);
   }
-  __syncthreads();
+  csync<C>();
 }
 
 // Volume term: D = Sum_r d/dxi_r (metric_r . F(U)) for every field.
@@ -229,12 +280,12 @@ __device__ __forceinline__ void volume(const Smem<C> &sm, double gamma_, int tid
         sm.C[(slot * NF + n) * QD + p] = g;
       }
     }
-    __syncthreads();
+    csync<C>();
     using Sh = Sh3<DIM, Q>;
-    if (r == 0) contract<Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<C::L, Q, T>, false>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
-    else if (r == 1) contract<Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<C::L, Q, T>, true>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
-    else contract<Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<C::L, Q, T>, true>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
-    __syncthreads();
+    if (r == 0) contract<Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<C::L, Q, T>, false, typename C::R, -1, -1, -1, -1, C::FPT>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
+    else if (r == 1) contract<Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<C::L, Q, T>, true, typename C::R, -1, -1, -1, -1, C::FPT>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
+    else contract<Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<C::L, Q, T>, true, typename C::R, -1, -1, -1, -1, C::FPT>(sm.C, sm.D, NB, QD, QD, tid, C::NT);
+    csync<C>();
   }
 }
 
@@ -263,11 +314,12 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
     const GeomClass &gc = sm.geo[slot];
     const int gn = a.perm[lk.perm + g];
     T Uo[5], Un[5], Fh[5], FL[5], FR[5];
-    T *eo = sm.E + ((f * EPB + slot) * NF) * GF + g;
+    constexpr int EB = C::EB;
+    T *eo = sm.E + ((f * EPB + slot) * NF) * EB + epos<C>(g);
     const T *tn = Tin + ((size_t)(lk.elem * NFACE + lk.face) * NF) * GF + gn;
     const T nm[3] = {T(gc.nrm[f][0]), T(gc.nrm[f][1]), T(gc.nrm[f][2])};
 #pragma unroll
-    for (int n = 0; n < NF; ++n) { Uo[n] = eo[n * GF]; Un[n] = tn[n * GF]; }
+    for (int n = 0; n < NF; ++n) { Uo[n] = eo[n * EB]; Un[n] = tn[n * GF]; }
     const bool master = (gc.master >> f) & 1;
     const T jr = T(gc.jr[f]);
     bool ok;
@@ -277,12 +329,12 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
       if (master) ok = face_flux_pert<PHYS, T>(sm.ref[slot], Uo, Un, nm, T(a.gamma), a.flux, Fh, FR);
       else ok = face_flux_pert<PHYS, T>(sm.ref[slot], Un, Uo, nm, T(a.gamma), a.flux, Fh, FR);
 #pragma unroll
-      for (int n = 0; n < NF; ++n) eo[n * GF] = master ? Fh[n] * jr : (FR[n] - Fh[n]) * jr;
+      for (int n = 0; n < NF; ++n) eo[n * EB] = master ? Fh[n] * jr : (FR[n] - Fh[n]) * jr;
     } else {
       if (master) ok = face_flux<PHYS, T>(Uo, Un, nm, T(a.gamma), a.flux, Fh, FL, FR);
       else ok = face_flux<PHYS, T>(Un, Uo, nm, T(a.gamma), a.flux, Fh, FL, FR);
 #pragma unroll
-      for (int n = 0; n < NF; ++n) eo[n * GF] = master ? (Fh[n] - FL[n]) * jr : (FR[n] - Fh[n]) * jr;
+      for (int n = 0; n < NF; ++n) eo[n * EB] = master ? (Fh[n] - FL[n]) * jr : (FR[n] - Fh[n]) * jr;
     }
     if constexpr (PHYS == DGMX_NS2D || PHYS == DGMX_NS3D) {
       // BR1 viscous lift: '-' average of the viscous normal-flux traces in
@@ -294,7 +346,7 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
       for (int n = 1; n < NF; ++n) {
         const double Vo = vo[(n - 1) * GF], Vn = vn[(n - 1) * GF];
         const double fs = master ? 0.5 * (Vo - Vn) : -(0.5 * (Vn - Vo));
-        eo[n * GF] = eo[n * GF] - (fs - Vo) * jr;
+        eo[n * EB] = eo[n * EB] - (fs - Vo) * jr;
       }
     }
     if (!ok) {
@@ -302,7 +354,7 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
       atomicMin(a.err + 1, e);
     }
   }
-  __syncthreads();
+  csync<C>();
 }
 
 // Lift: interpolate E (Gauss) to the face GLL points and add W_f * value to
@@ -313,14 +365,15 @@ __device__ __forceinline__ void lift(const Smem<C> &sm, int tid) {
   constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G, NF = C::NF, EPB = C::EPB, QD = C::QD, QF = C::QF;
   constexpr int NB = C::NFACE * EPB * NF;
   T *LFc = sm.B;  // face-major [f][slot][n][QF], spans B and C
+  constexpr int PG = C::PG;
   if constexpr (DIM == 3) {
-    contract<G, G, 1, 0, G, Q, MatG2GL<L, Q, T>, false>(sm.E, sm.S, NB, G * G, Q * G, tid, C::NT);
-    __syncthreads();
-    contract<Q, G, 1, 1, G, Q, MatG2GL<L, Q, T>, false>(sm.S, LFc, NB, Q * G, Q * Q, tid, C::NT);
+    contract<G, G, 1, 0, G, Q, MatG2GL<L, Q, T>, false, T, PG, 1, PG, 1, C::FPT>(sm.E, sm.S, NB, C::EB, Q * PG, tid, C::NT);
+    csync<C>();
+    contract<Q, G, 1, 1, G, Q, MatG2GL<L, Q, T>, false, T, PG, 1, -1, -1, C::FPT>(sm.S, LFc, NB, Q * PG, Q * Q, tid, C::NT);
   } else {
-    contract<G, 1, 1, 0, G, Q, MatG2GL<L, Q, T>, false>(sm.E, LFc, NB, G, Q, tid, C::NT);
+    contract<G, 1, 1, 0, G, Q, MatG2GL<L, Q, T>, false, typename C::R, -1, -1, -1, -1, C::FPT>(sm.E, LFc, NB, C::EB, Q, tid, C::NT);
   }
-  __syncthreads();
+  csync<C>();
   const T w0 = T(1) / cW<T, L, Q>[0], w1 = T(1) / cW<T, L, Q>[Q - 1];
   for (int w = tid; w < EPB * NF * QD; w += C::NT) {
     const int slot = w / (NF * QD), rem = w - slot * NF * QD, n = rem / QD, p = rem - n * QD;
@@ -348,7 +401,7 @@ __device__ __forceinline__ void lift(const Smem<C> &sm, int tid) {
     else wq = cW<T, L, Q>[p / Q] * cW<T, L, Q>[p % Q];
     sm.D[w] = wq * acc;
   }
-  __syncthreads();
+  csync<C>();
 }
 
 // Solve (reference-state row) of element e; 0 for a single-solve domain.
@@ -358,14 +411,20 @@ __device__ __forceinline__ int solve_of(const StageArgs &a, int e) {
 
 template <class C>
 __device__ __forceinline__ void load_geometry(const Smem<C> &sm, const StageArgs &a, int e0, int tid) {
-  for (int s = tid; s < C::EPB; s += C::NT) {
-    const int e = e0 + s;
+  // the geometry class is copied word by word by the whole team
+  constexpr int GW = (int)(sizeof(GeomClass) / sizeof(double));
+  static_assert(sizeof(GeomClass) % sizeof(double) == 0, "GeomClass is copied as doubles");
+  for (int k = tid; k < C::EPB * GW; k += C::NT) {
+    const int s = k / GW, j = k - s * GW, e = e0 + s;
     // elements past the end, and unallocated pool elements (class < 0),
     // are skipped
     const int gc = e < a.ne ? a.gclass[e] : -1;
-    sm.eid[s] = gc >= 0 ? e : -1;
-    sm.geo[s] = a.classes[gc >= 0 ? gc : 0];
-    if constexpr (C::MIXED) sm.ref[s] = make_ref<C::PHYSICS, typename C::R>(a.uref + 10 * solve_of(a, gc >= 0 ? e : -1), a.gamma);
+    reinterpret_cast<double *>(sm.geo + s)[j] = reinterpret_cast<const double *>(a.classes + (gc >= 0 ? gc : 0))[j];
+    if (j == 0) {
+      sm.eid[s] = gc >= 0 ? e : -1;
+      if constexpr (C::MIXED)
+        sm.ref[s] = make_ref<C::PHYSICS, typename C::R>(a.uref + 10 * solve_of(a, gc >= 0 ? e : -1), a.gamma);
+    }
   }
   for (int w = tid; w < C::EPB * C::NFACE; w += C::NT) {
     const int s = w / C::NFACE, f = w - s * C::NFACE, e = e0 + s;
@@ -384,6 +443,17 @@ __device__ __forceinline__ void load_modal(typename C::R *dst, const S *src, int
   }
 }
 
+// The same into the padded modal block (rows of L at pitch PL).
+template <class C, class S>
+__device__ __forceinline__ void load_modal_pad(typename C::R *dst, const S *src, int e0, int ne, int tid) {
+  using T = typename C::R;
+  constexpr int BLK = C::NF * C::LD;
+  for (int w = tid; w < C::EPB * BLK; w += C::NT) {
+    const int s = w / BLK, e = e0 + s;
+    dst[apos<C>(w)] = e < ne ? T(src[(size_t)e0 * BLK + w]) : T(w % C::LD == 0 ? 1.0 : 0.0);
+  }
+}
+
 // Mixed form: the FP32 working copy of a modal register is the perturbation
 // about the solve's reference state, formed in FP64 (only the constant mode
 // carries the reference: uref[10 s + 5 + n]).
@@ -398,7 +468,7 @@ __device__ __forceinline__ void load_modal_pert(float *dst, const double *src, c
       x = src[(size_t)e0 * BLK + w];
       if (m == 0) x -= a.uref[10 * solve_of(a, e) + 5 + (w % BLK) / C::LD];
     }
-    dst[w] = float(x);
+    dst[apos<C>(w)] = float(x);
   }
 }
 
@@ -410,13 +480,15 @@ __device__ __forceinline__ void store_traces(const typename C::R *E, TT *T, int 
     const int s = w / (NFACE * NF * GF), rem = w - s * NFACE * NF * GF;
     const int f = rem / (NF * GF), ng = rem - f * NF * GF;
     const int e = e0 + s;
-    if (e < ne) T[(size_t)e * NFACE * NF * GF + rem] = TT(E[(f * EPB + s) * NF * GF + ng]);
+    const int n = ng / GF, g = ng - n * GF;
+    if (e < ne) T[(size_t)e * NFACE * NF * GF + rem] = TT(E[((f * EPB + s) * NF + n) * C::EB + epos<C>(g)]);
   }
 }
 
 // The element's own traces, written by the previous stage (or the trace
-// kernel), global [e][f][n][g] -> smem face-major [f][slot][n][g].
-template <class C, class TT>
+// kernel), global [e][f][n][g] -> smem face-major [f][slot][n][g], into
+// padded blocks (PAD) or dense ones.
+template <class C, class TT, bool PAD = true>
 __device__ __forceinline__ void load_own_traces(typename C::R *E, const TT *T, int e0, int ne, int tid) {
   using R = typename C::R;
   constexpr int NF = C::NF, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
@@ -424,29 +496,22 @@ __device__ __forceinline__ void load_own_traces(typename C::R *E, const TT *T, i
     const int s = w / (NFACE * NF * GF), rem = w - s * NFACE * NF * GF;
     const int f = rem / (NF * GF), ng = rem - f * NF * GF;
     const int e = e0 + s;
-    E[(f * EPB + s) * NF * GF + ng] = e < ne ? R(T[(size_t)e * NFACE * NF * GF + rem]) : R(ng < GF ? 1.0 : 0.0);
+    const int n = ng / GF, g = ng - n * GF;
+    const int at = PAD ? ((f * EPB + s) * NF + n) * C::EB + epos<C>(g) : (f * EPB + s) * NF * GF + ng;
+    E[at] = e < ne ? R(T[(size_t)e * NFACE * NF * GF + rem]) : R(ng < GF ? 1.0 : 0.0);
   }
 }
 
 // ---------------------------------------------------------------- kernels
+// One fused RK stage on the EPB elements from e0, run by the team of C
+// (the CTA, or one warp for WarpCfg).
 template <class C, int PHYS>
-__global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
-  using T = typename C::R;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem<C> sm(smem_raw);
-  const int tid = threadIdx.x;
-  // One tile per CTA, or, with a tile list (element pools), a persistent
-  // loop over the listed tiles; the count is read on the device so a
-  // captured graph stays valid while solves join and leave.
-  const int ntile = a.tiles ? *a.ntiles : (int)gridDim.x;
-  for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
-  if (t != (int)blockIdx.x) __syncthreads();
-  const int e0 = (a.tiles ? a.tiles[t] : t) * C::EPB;
+__device__ __forceinline__ void stage_tile(const Smem<C> &sm, const StageArgs &a, int e0, int tid) {
   load_geometry<C>(sm, a, e0, tid);
   if constexpr (C::MIXED) load_modal_pert<C>(sm.A, a.X, a, e0, tid);
-  else load_modal<C>(sm.A, a.X, e0, a.ne, tid);
+  else load_modal_pad<C>(sm.A, a.X, e0, a.ne, tid);
   load_own_traces<C>(sm.E, trace_in<C>(a), e0, a.ne, tid);
-  __syncthreads();
+  csync<C>();
   backward<C>(sm.A, sm.B, sm.S, sm.C, tid, C::NT);
   volume<C, PHYS>(sm, a.gamma, tid);
   face_fluxes<C, PHYS>(sm, a, tid);
@@ -467,7 +532,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
       float next;
       if (a.kind == kRHS) {
         a.A[gi] = r;
-        next = sm.A[w];
+        next = sm.A[apos<C>(w)];
       } else {
         float ut = float(a.c0) * a.Utf[gi];
         ut = fmaf(-float(dt), r, ut);
@@ -476,10 +541,10 @@ __global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
         const int m = w % C::LD;
         next = float(m == 0 ? u - a.uref[10 * solve_of(a, e) + 5 + (w % BLK) / C::LD] : u);
       }
-      sm.A[w] = next;
+      sm.A[apos<C>(w)] = next;
       continue;
     } else {
-      const double x = sm.A[w];
+      const double x = sm.A[apos<C>(w)];
       double r = sm.R[w];
       if (a.Rcap) a.Rcap[gi] = r;          // first RHS (shallow-water balance)
       if (a.Rsub) r = r - a.Rsub[gi];
@@ -537,11 +602,41 @@ __global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
           break;
         }
       }
-  sm.A[w] = next;
+  sm.A[apos<C>(w)] = next;
     }  }
-  __syncthreads();
+  csync<C>();
   modal_traces<C>(sm.A, sm.E, sm.S, sm.B, tid, C::NT);
   store_traces<C>(sm.E, trace_out<C>(a), e0, a.ne, tid);
+}
+
+// One tile per CTA, or, with a tile list (element pools), a persistent loop
+// over the listed tiles; the count is read on the device so a captured
+// graph stays valid while solves join and leave.
+template <class C, int PHYS>
+__global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem<C> sm(smem_raw);
+  const int ntile = a.tiles ? *a.ntiles : (int)gridDim.x;
+  for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
+    if (t != (int)blockIdx.x) __syncthreads();
+    stage_tile<C, PHYS>(sm, a, (a.tiles ? a.tiles[t] : t) * C::EPB, threadIdx.x);
+  }
+}
+
+// The same with one element per warp (W = WarpCfg): each warp works through
+// its element alone, with no CTA-wide barrier; elements past the end or not
+// allocated in a pool are skipped by their warp.
+template <class W, int PHYS>
+__global__ void __launch_bounds__(W::CTA_NT, W::MINB) wstage_kernel(StageArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  Smem<W> sm(smem_raw + warp * W::SLOT);
+  const int ntile = a.tiles ? *a.ntiles : (int)gridDim.x;
+  for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const int e = (a.tiles ? a.tiles[t] : t) * W::WPB + warp;
+    if (e >= a.ne || a.gclass[e] < 0) continue;
+    __syncwarp();
+    stage_tile<W, PHYS>(sm, a, e, lane);
   }
 }
 
@@ -552,8 +647,8 @@ __global__ void __launch_bounds__(C::NT, C::MINB) traces_modal_kernel(StageArgs 
   Smem<C> sm(smem_raw);
   const int tid = threadIdx.x, e0 = blockIdx.x * C::EPB;
   if constexpr (C::MIXED) load_modal_pert<C>(sm.A, Xm, a, e0, tid);
-  else load_modal<C>(sm.A, Xm, e0, a.ne, tid);
-  __syncthreads();
+  else load_modal_pad<C>(sm.A, Xm, e0, a.ne, tid);
+  csync<C>();
   modal_traces<C>(sm.A, sm.E, sm.S, sm.B, tid, C::NT);
   store_traces<C>(sm.E, T, e0, a.ne, tid);
 }
@@ -579,7 +674,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) traces_nodal_kernel(StageArgs 
   constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G, NF = C::NF, EPB = C::EPB, QD = C::QD, QF = C::QF;
   const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
   load_nodal<C>(sm.B, a.Xn, e0, a.ne, tid);
-  __syncthreads();
+  csync<C>();
   // gather face GLL values, face-major [f][slot][n][QF]
   for (int w = tid; w < C::NFACE * EPB * NF * QF; w += C::NT) {
     const int f = w / (EPB * NF * QF), rem = w - f * EPB * NF * QF;
@@ -606,16 +701,17 @@ __global__ void __launch_bounds__(C::NT, C::MINB) traces_nodal_kernel(StageArgs 
     }
     sm.C[w] = src[p];
   }
-  __syncthreads();
+  csync<C>();
   constexpr int NB = C::NFACE * EPB * NF;
   if constexpr (DIM == 3) {
-    contract<Q, Q, 1, 0, Q, G, MatGL2G<L, Q, T>, false>(sm.C, sm.S, NB, Q * Q, G * Q, tid, C::NT);
-    __syncthreads();
-    contract<G, Q, 1, 1, Q, G, MatGL2G<L, Q, T>, false>(sm.S, sm.E, NB, G * Q, G * G, tid, C::NT);
+    contract<Q, Q, 1, 0, Q, G, MatGL2G<L, Q, T>, false, typename C::R, -1, -1, -1, -1, C::FPT>(sm.C, sm.S, NB, Q * Q, G * Q, tid, C::NT);
+    csync<C>();
+    contract<G, Q, 1, 1, Q, G, MatGL2G<L, Q, T>, false, T, -1, -1, C::PG, 1, C::FPT>(sm.S, sm.E, NB, G * Q, C::EB, tid,
+                                                                             C::NT);
   } else {
-    contract<Q, 1, 1, 0, Q, G, MatGL2G<L, Q, T>, false>(sm.C, sm.E, NB, Q, G, tid, C::NT);
+    contract<Q, 1, 1, 0, Q, G, MatGL2G<L, Q, T>, false, typename C::R, -1, -1, -1, -1, C::FPT>(sm.C, sm.E, NB, Q, C::EB, tid, C::NT);
   }
-  __syncthreads();
+  csync<C>();
   store_traces<C>(sm.E, a.Tout, e0, a.ne, tid);
 }
 
@@ -631,7 +727,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) rhs_nodal_kernel(StageArgs a) 
   load_nodal<C>(sm.B, a.Xn, e0, a.ne, tid);
   // own traces from Tin (written by traces_nodal_kernel)
   load_own_traces<C>(sm.E, a.Tin, e0, a.ne, tid);
-  __syncthreads();
+  csync<C>();
   volume<C, PHYS>(sm, a.gamma, tid);
   face_fluxes<C, PHYS>(sm, a, tid);
   lift<C>(sm, tid);
@@ -642,7 +738,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) rhs_nodal_kernel(StageArgs a) 
       const int e = e0 + w / BLK, n = (w % BLK) / C::LD, m = w % C::LD;
       if (e < a.ne && n >= 1) sm.R[w] = sm.R[w] - a.Pv[((size_t)e * (NF - 1) + (n - 1)) * C::LD + m];
     }
-    __syncthreads();
+    csync<C>();
   }
   if (a.Rcap || a.Rsub) {
     constexpr int BLK = NF * C::LD;
@@ -653,9 +749,9 @@ __global__ void __launch_bounds__(C::NT, C::MINB) rhs_nodal_kernel(StageArgs a) 
       if (a.Rcap) a.Rcap[gi] = sm.R[w];
       if (a.Rsub) sm.R[w] = sm.R[w] - a.Rsub[gi];
     }
-    __syncthreads();
+    csync<C>();
   }
-  backward<C>(sm.R, sm.B, sm.S, sm.C, tid, C::NT);
+  backward<C, false>(sm.R, sm.B, sm.S, sm.C, tid, C::NT);
   for (int w = tid; w < EPB * NF * QD; w += C::NT) {
     const int s = w / (NF * QD), rem = w - s * NF * QD, n = rem / QD, p = rem - n * QD;
     const int e = e0 + s;
@@ -672,7 +768,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) forward_kernel(StageArgs a, co
   constexpr int L = C::L, Q = C::Q, NF = C::NF, QD = C::QD, EPB = C::EPB;
   const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
   load_nodal<C>(sm.D, Un, e0, a.ne, tid);
-  __syncthreads();
+  csync<C>();
   for (int w = tid; w < EPB * NF * QD; w += C::NT) {
     const int p = w % QD;
     double wq;
@@ -680,7 +776,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) forward_kernel(StageArgs a, co
     else wq = cW<double, L, Q>[p / Q] * cW<double, L, Q>[p % Q];
     sm.D[w] = wq * sm.D[w];
   }
-  __syncthreads();
+  csync<C>();
   forward<C>(sm.D, sm.R, sm.C, sm.B, tid, C::NT);
   constexpr int BLK = NF * C::LD;
   for (int w = tid; w < EPB * BLK; w += C::NT) {
@@ -698,8 +794,8 @@ __global__ void __launch_bounds__(C::NT, C::MINB) backward_kernel(StageArgs a, c
   constexpr int NF = C::NF, QD = C::QD, EPB = C::EPB;
   const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
   load_modal<C>(sm.A, Um, e0, a.ne, tid);
-  __syncthreads();
-  backward<C>(sm.A, sm.B, sm.S, sm.C, tid, C::NT);
+  csync<C>();
+  backward<C, false>(sm.A, sm.B, sm.S, sm.C, tid, C::NT);
   for (int w = tid; w < EPB * NF * QD; w += C::NT) {
     const int s = w / (NF * QD), rem = w - s * NF * QD, n = rem / QD, p = rem - n * QD;
     const int e = e0 + s;

@@ -154,6 +154,12 @@ int dgmx_kernel_list(int *rows, int cap);
  * threads per CTA, microseconds per launch). */
 dgmx_status dgmx_autotune(dgmx_domain *d, int reps, double *rows, int cap, int *nvariants, int *chosen);
 
+/* Selects compiled tile variant `index` (0 .. nvariants-1, the order of
+ * dgmx_autotune's rows) for the stage kernel of this handle; *count gets the
+ * number of variants and *warp whether the chosen one runs one element per
+ * warp.  No counterpart in the reference (tile choice is a GPU matter). */
+dgmx_status dgmx_set_variant(dgmx_domain *d, int index, int *count, int *warp);
+
 /* Host-only inspection, no CUDA calls.  1-D tables for L modes and Q GLL
  * points (G = Q-1 Gauss points): GLL z, w (Q); collocation D (QxQ,
  * src/Polylib.tpp:1008-1049); orthonormal Legendre on GLL B (LxQ) and on

@@ -174,6 +174,49 @@ def test_autotune_keeps_results_and_state():
     assert rel(D.state(), P.state()) < TOL_STATE
 
 
+VARIANT_CASES = [
+    # physics, dim, n, lo, hi, p, flux, inttype, ic, dt, steps, precision
+    ("euler3d-roe-p3", 8, 3, (3, 2, 3), 0, 2 * np.pi, 3, "roe", 14, TG, 0.002, 2, 0),
+    ("euler3d-lf-p4-tvd", 8, 3, (2, 2, 2), 0, 2 * np.pi, 4, "laxfriedrichs", 3, TG, 0.001, 2, 0),
+    ("euler2d-roe-p3-rk4", 1, 2, (4, 3), -5, 5, 3, "roe", 4, IV, 0.01, 3, 0),
+    ("shallow-p2", 30, 2, (4, 4), -2, 2, 2, "laxfriedrichs", 14, GB, 0.001, 3, 0),
+    ("ns3d-p3", 9, 3, (2, 2, 2), 0, 2 * np.pi, 3, "laxfriedrichs", 14, TG, 0.002, 2, 0),
+    ("euler3d-roe-p3-mixed", 8, 3, (3, 2, 3), 0, 2 * np.pi, 3, "roe", 14, TG, 0.002, 2, 1),
+    ("euler2d-p5-mixed", 1, 2, (3, 3), -5, 5, 5, "laxfriedrichs", 14, IV, 0.005, 3, 1),
+]
+
+
+@pytest.mark.parametrize("case", VARIANT_CASES, ids=[c[0] for c in VARIANT_CASES])
+def test_every_tile_variant_matches_oracle(case):
+    """Every compiled tile of the stage kernel -- elements per CTA, register
+    caps, and one element per warp -- gives the oracle's answer (FP64:
+    1e-12; mixed form: 1e-6)."""
+    import dgm_b200
+    _, phys, dim, n, lo, hi, p, flux, inttype, ic, dt, steps, prec = case
+    m = dgm_b200.meshgen.box(dim, n, lo, hi, p)
+    vis = 0.05 if phys == oracle.NS3D else 0.0
+    P = oracle.Problem(dgm_io.Mesh(m.dim, m.verts, m.con, m.porder, m.qorder), phys, flux=flux, vis=vis)
+    if phys == oracle.SHALLOW:
+        P.set_sw_balance(False)
+    x, y, z = P.coords()
+    f = ic(x, y, z)
+    P.set_state(P.project(f))
+    P.advance(inttype, dt, steps)
+    ref = P.state()
+    D = dgm_b200.Domain(m, phys, flux=flux, inttype=inttype, sw_balance=False, vis=vis, precision=prec)
+    count = D.variant_count()
+    assert count >= 2
+    warps = 0
+    for k in range(count):
+        _, warp = D.set_variant(k)
+        warps += warp
+        D.set_state(f)
+        D.advance(dt, steps)
+        err = rel(D.state(), ref)
+        assert err < (1e-6 if prec else TOL_STATE), (k, warp, err)
+    assert warps >= 1
+
+
 def test_shallow_balance_keeps_state_steady():
     """REO_SHALLOW_ENFORCE_BALANCE subtracts the first RHS (src/Shallow.cpp:255-267),
     so the bump stays exactly where it is on both sides."""
