@@ -28,7 +28,15 @@ static cudaError_t upload_tables_lq(const Tables1D &t) {
   if ((e = put(cW<T, L, Q>, t.w, (size_t)Q)) != cudaSuccess) return e;
   std::vector<double> end(2 * L);
   for (int a = 0; a < L; ++a) { end[a] = t.B[a * Q + 0]; end[L + a] = t.B[a * Q + Q - 1]; }
-  return put(cEnd<T, L, Q>, end, (size_t)2 * L);
+  if ((e = put(cEnd<T, L, Q>, end, (size_t)2 * L)) != cudaSuccess) return e;
+  // projection with the GLL weights folded in, and lift with 1/w_end folded in
+  std::vector<double> bw((size_t)L * Q), gw((size_t)2 * Q * (Q - 1));
+  for (int a = 0; a < L; ++a)
+    for (int i = 0; i < Q; ++i) bw[(size_t)a * Q + i] = t.B[(size_t)a * Q + i] * t.w[i];
+  for (int end_ = 0; end_ < 2; ++end_)
+    for (size_t k = 0; k < (size_t)Q * (Q - 1); ++k) gw[end_ * Q * (Q - 1) + k] = t.g2gl[k] / t.w[end_ ? Q - 1 : 0];
+  if ((e = put(cBw<T, L, Q>, bw, (size_t)L * Q)) != cudaSuccess) return e;
+  return put(cG2GLw<T, L, Q>, gw, (size_t)2 * Q * (Q - 1));
 }
 
 template <int PHYS, int L, int Q, int EPB, int MINB, bool MIXED = false>

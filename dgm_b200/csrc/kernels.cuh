@@ -25,6 +25,8 @@ template <class T, int L, int Q> __constant__ T cG2GL[Q * (Q - 1)]; // [i*G+g]
 template <class T, int L, int Q> __constant__ T cGL2G[(Q - 1) * Q]; // [g*Q+i]
 template <class T, int L, int Q> __constant__ T cW[Q];              // GLL weights
 template <class T, int L, int Q> __constant__ T cEnd[2 * L];        // B[a][0], B[a][Q-1]
+template <class T, int L, int Q> __constant__ T cBw[L * Q];         // B[a][i] w[i] (weighted projection)
+template <class T, int L, int Q> __constant__ T cG2GLw[2 * Q * (Q - 1)];  // G2GL / w_end, ends 0 and 1
 
 // Matrix accessors: M::get(in_index, out_index)
 template <int L, int Q, class T = double> struct MatB   { static __device__ __forceinline__ T get(int a, int i) { return cB<T, L, Q>[a * Q + i]; } };
@@ -32,6 +34,8 @@ template <int L, int Q, class T = double> struct MatBt  { static __device__ __fo
 template <int L, int Q, class T = double> struct MatBg  { static __device__ __forceinline__ T get(int a, int g) { return cBg<T, L, Q>[a * (Q - 1) + g]; } };
 template <int L, int Q, class T = double> struct MatD   { static __device__ __forceinline__ T get(int m, int i) { return cD<T, L, Q>[i * Q + m]; } };
 template <int L, int Q, class T = double> struct MatG2GL{ static __device__ __forceinline__ T get(int g, int i) { return cG2GL<T, L, Q>[i * (Q - 1) + g]; } };
+template <int L, int Q, class T = double> struct MatBtw { static __device__ __forceinline__ T get(int i, int a) { return cBw<T, L, Q>[a * Q + i]; } };
+template <int L, int Q, int END, class T = double> struct MatG2GLw { static __device__ __forceinline__ T get(int g, int i) { return cG2GLw<T, L, Q>[END * Q * (Q - 1) + i * (Q - 1) + g]; } };
 template <int L, int Q, class T = double> struct MatGL2G{ static __device__ __forceinline__ T get(int i, int g) { return cGL2G<T, L, Q>[g * Q + i]; } };
 
 // Contraction along axis AX of a batch of 3-D arrays (I0, I1, I2) with
@@ -42,11 +46,13 @@ template <int L, int Q, class T = double> struct MatGL2G{ static __device__ __fo
 // (IS0, IS1 input; OS0, OS1 output) to address rows padded to an odd pitch,
 // which keeps a warp's pencils on distinct shared-memory banks.
 //
+// OSA (nonzero) overrides the output stride along AX (outputs of one pencil
+// scattered to separate arrays, e.g. the two end faces of an axis).
 // FPT > 1 gives each thread the same pencil of FPT consecutive batches (the
 // fields of one element): one index computation serves FPT pencils and the
 // thread has FPT independent FMA chains (the one-element-per-warp tiles).
 template <int I0, int I1, int I2, int AX, int K, int N, class M, bool ACC, class T, int IS0 = -1, int IS1 = -1,
-          int OS0 = -1, int OS1 = -1, int FPT = 1>
+          int OS0 = -1, int OS1 = -1, int FPT = 1, int OSA = 0>
 __device__ __forceinline__ void contract(const T *__restrict__ in, T *__restrict__ out, int nbatch,
                                          int sin, int sout, int tid, int nthr) {
   constexpr int O1 = AX == 1 ? N : I1, O2 = AX == 2 ? N : I2;
@@ -56,7 +62,7 @@ __device__ __forceinline__ void contract(const T *__restrict__ in, T *__restrict
   constexpr int is1 = IS1 >= 0 ? IS1 : I2, is0 = IS0 >= 0 ? IS0 : I1 * is1;
   constexpr int os1 = OS1 >= 0 ? OS1 : O2, os0 = OS0 >= 0 ? OS0 : O1 * os1;
   constexpr int isA = AX == 0 ? is0 : (AX == 1 ? is1 : 1);
-  constexpr int osA = AX == 0 ? os0 : (AX == 1 ? os1 : 1);
+  constexpr int osA = OSA != 0 ? OSA : (AX == 0 ? os0 : (AX == 1 ? os1 : 1));
   for (int w = tid; w < (nbatch / FPT) * NP; w += nthr) {
     const int b = (w / NP) * FPT, p = w - (w / NP) * NP;
     const int pa = p / P1, pb = p - pa * P1;

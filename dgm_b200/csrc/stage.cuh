@@ -153,20 +153,25 @@ __device__ __forceinline__ int epos(int g) {
 template <class C>
 __device__ __forceinline__ int apos(int m) { return (m / C::L) * C::PL + m % C::L; }
 
-template <int L, int Q, int END, class T>
-struct MatEnd { static __device__ __forceinline__ T get(int a, int) { return cEnd<T, L, Q>[END * L + a]; } };
 
-// Endpoint reduction of one face for a batch of modal arrays (L^DIM each),
-// output face-local L^(DIM-1) arrays.
-template <class C, int F>
+template <int L, int Q, class T>
+struct MatEnd2 { static __device__ __forceinline__ T get(int a, int end) { return cEnd<T, L, Q>[end * L + a]; } };
+
+// Endpoint reduction along axis AX of a batch of padded modal arrays: both
+// end faces at once (FLO = the face at the first GLL point, FHI = the last),
+// each into its face-local L^(DIM-1) array (planes, or padded 2-D lines).
+template <class C, int AX, int FLO, int FHI>
 __device__ __forceinline__ void face_reduce(const typename C::R *A, typename C::R *out, int tid, int nthr) {
   constexpr int DIM = C::DIM, L = C::L, Q = C::Q;
-  constexpr int AX = face_axis<DIM>(F), END = face_end<DIM>(F);
   using Sh = Sh3<DIM, L>;
   constexpr int IS0 = DIM == 3 ? L * C::PL : C::PL, IS1 = DIM == 3 ? C::PL : 1;
   constexpr int OB = DIM == 3 ? C::LF : C::PL;   // output block: an L x L plane, or a padded line
-  contract<Sh::a, Sh::b, Sh::c, AX, L, 1, MatEnd<L, Q, END, typename C::R>, false, typename C::R, IS0, IS1, -1, -1, C::FPT>(
-      A, out + F * C::EPB * C::NF * OB, C::EPB * C::NF, C::AB, OB, tid, nthr);
+  constexpr int FS = C::EPB * C::NF * OB;       // one face's blocks
+  // plane strides of the outputs: (b, c) for AX 0, (a, c) for AX 1, (a, b) for AX 2
+  constexpr int OS0 = DIM == 3 ? (AX == 1 ? L : (AX == 2 ? L : -1)) : (AX == 1 ? 1 : -1);
+  constexpr int OS1 = DIM == 3 ? (AX == 0 ? L : (AX == 2 ? 1 : -1)) : (AX == 0 ? 1 : -1);
+  contract<Sh::a, Sh::b, Sh::c, AX, L, 2, MatEnd2<L, Q, typename C::R>, false, typename C::R, IS0, IS1, OS0, OS1,
+           C::FPT, (FHI - FLO) * FS>(A, out + FLO * FS, C::EPB * C::NF, C::AB, OB, tid, nthr);
 }
 
 // Traces at the side Gauss points of a modal register held in smem A.
@@ -176,13 +181,15 @@ __device__ __forceinline__ void modal_traces(const typename C::R *A, typename C:
                                              typename C::R *Cs, int tid, int nthr) {
   using T = typename C::R;
   constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G;
-  face_reduce<C, 0>(A, S, tid, nthr);
-  face_reduce<C, 1>(A, S, tid, nthr);
-  face_reduce<C, 2>(A, S, tid, nthr);
-  face_reduce<C, 3>(A, S, tid, nthr);
   if constexpr (DIM == 3) {
-    face_reduce<C, 4>(A, S, tid, nthr);
-    face_reduce<C, 5>(A, S, tid, nthr);
+    // faces: 0 k=0, 1 j=0, 2 i=Q-1, 3 j=Q-1, 4 i=0, 5 k=Q-1
+    face_reduce<C, 0, 4, 2>(A, S, tid, nthr);
+    face_reduce<C, 1, 1, 3>(A, S, tid, nthr);
+    face_reduce<C, 2, 0, 5>(A, S, tid, nthr);
+  } else {
+    // faces: 0 j=0, 1 i=Q-1, 2 j=Q-1, 3 i=0
+    face_reduce<C, 0, 3, 1>(A, S, tid, nthr);
+    face_reduce<C, 1, 0, 2>(A, S, tid, nthr);
   }
   csync<C>();
   constexpr int NB = C::NFACE * C::EPB * C::NF, PL = C::PL, PG = C::PG;
@@ -219,7 +226,9 @@ __device__ __forceinline__ void backward(const typename C::R *A, typename C::R *
   csync<C>();
 }
 
-// Forward projection: GLL D [slot][n][QD] (already w-weighted) -> modal R.
+// Forward projection: GLL D [slot][n][QD] -> modal R, the GLL quadrature
+// weights applied by the weighted matrices (B w; the J of wJ cancels the
+// 1/J mass of the orthonormal basis).
 template <class C>
 __device__ __forceinline__ void forward(const typename C::R *D, typename C::R *R, typename C::R *Cs,
                                         typename C::R *Bs, int tid, int nthr) {
@@ -227,15 +236,15 @@ __device__ __forceinline__ void forward(const typename C::R *D, typename C::R *R
   constexpr int L = C::L, Q = C::Q, NB = C::EPB * C::NF, PL = C::PL;
   // the contiguous axis first, into rows of L at the odd pitch PL
   if constexpr (C::DIM == 3) {
-    contract<Q, Q, Q, 2, Q, L, MatBt<L, Q, T>, false, T, -1, -1, Q * PL, PL, C::FPT>(D, Cs, NB, C::QD, Q * Q * PL, tid, nthr);
+    contract<Q, Q, Q, 2, Q, L, MatBtw<L, Q, T>, false, T, -1, -1, Q * PL, PL, C::FPT>(D, Cs, NB, C::QD, Q * Q * PL, tid, nthr);
     csync<C>();
-    contract<Q, Q, L, 1, Q, L, MatBt<L, Q, T>, false, T, Q * PL, PL, -1, -1, C::FPT>(Cs, Bs, NB, Q * Q * PL, Q * L * L, tid, nthr);
+    contract<Q, Q, L, 1, Q, L, MatBtw<L, Q, T>, false, T, Q * PL, PL, -1, -1, C::FPT>(Cs, Bs, NB, Q * Q * PL, Q * L * L, tid, nthr);
     csync<C>();
-    contract<Q, L, L, 0, Q, L, MatBt<L, Q, T>, false, typename C::R, -1, -1, -1, -1, C::FPT>(Bs, R, NB, Q * L * L, C::LD, tid, nthr);
+    contract<Q, L, L, 0, Q, L, MatBtw<L, Q, T>, false, typename C::R, -1, -1, -1, -1, C::FPT>(Bs, R, NB, Q * L * L, C::LD, tid, nthr);
   } else {
-    contract<Q, Q, 1, 1, Q, L, MatBt<L, Q, T>, false, T, -1, -1, PL, 1, C::FPT>(D, Cs, NB, C::QD, Q * PL, tid, nthr);
+    contract<Q, Q, 1, 1, Q, L, MatBtw<L, Q, T>, false, T, -1, -1, PL, 1, C::FPT>(D, Cs, NB, C::QD, Q * PL, tid, nthr);
     csync<C>();
-    contract<Q, L, 1, 0, Q, L, MatBt<L, Q, T>, false, T, PL, 1, -1, -1, C::FPT>(Cs, R, NB, Q * PL, C::LD, tid, nthr);
+    contract<Q, L, 1, 0, Q, L, MatBtw<L, Q, T>, false, T, PL, 1, -1, -1, C::FPT>(Cs, R, NB, Q * PL, C::LD, tid, nthr);
   }
   csync<C>();
 }
@@ -357,49 +366,58 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
   csync<C>();
 }
 
-// Lift: interpolate E (Gauss) to the face GLL points and add W_f * value to
-// the boundary points of D, faces in increasing order as the reference.
+// One face of the lift: G2GL (second pass in 3-D) straight into the face
+// plane of D, scaled by 1/w_end (src/Hex.cpp:1942-1947).  Face plane (x, y)
+// -> D offset OFF + x OX + y OY.
+template <class C, int F>
+__device__ __forceinline__ void lift_face(const Smem<C> &sm, int tid) {
+  using T = typename C::R;
+  constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G, FB = C::EPB * C::NF, QD = C::QD, PG = C::PG;
+  constexpr int END = face_end<DIM>(F);
+  if constexpr (DIM == 3) {
+    // 0 k=0 (i,j), 1 j=0 (i,k), 2 i=Q-1 (j,k), 3 j=Q-1 (i,k), 4 i=0 (j,k), 5 k=Q-1 (i,j)
+    constexpr int OX = (F == 2 || F == 4) ? Q : Q * Q;
+    constexpr int OY = (F == 0 || F == 5) ? Q : 1;
+    constexpr int OFF = F == 2 ? (Q - 1) * Q * Q : (F == 3 ? (Q - 1) * Q : (F == 5 ? Q - 1 : 0));
+    contract<Q, G, 1, 1, G, Q, MatG2GLw<L, Q, END, T>, true, T, PG, 1, OX, OY, C::FPT>(
+        sm.S + F * FB * Q * PG, sm.D + OFF, FB, Q * PG, QD, tid, C::NT);
+  } else {
+    // 0 j=0 (i), 1 i=Q-1 (j), 2 j=Q-1 (i), 3 i=0 (j)
+    constexpr int OX = (F == 0 || F == 2) ? Q : 1;
+    constexpr int OFF = F == 1 ? (Q - 1) * Q : (F == 2 ? Q - 1 : 0);
+    contract<G, 1, 1, 0, G, Q, MatG2GLw<L, Q, END, T>, true, T, -1, -1, OX, 1, C::FPT>(
+        sm.E + F * FB * C::EB, sm.D + OFF, FB, C::EB, QD, tid, C::NT);
+  }
+}
+
+// Lift: the face terms E (Gauss points) are interpolated to the face GLL
+// points and added to the boundary points of D (src/Hex.cpp:1768-1952,
+// src/Quad.cpp:1971-2038).  The two faces normal to one axis touch disjoint
+// points and go together; the axes follow one another.  The quadrature
+// weights of the projection are in the forward transform.
 template <class C>
 __device__ __forceinline__ void lift(const Smem<C> &sm, int tid) {
   using T = typename C::R;
-  constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G, NF = C::NF, EPB = C::EPB, QD = C::QD, QF = C::QF;
-  constexpr int NB = C::NFACE * EPB * NF;
-  T *LFc = sm.B;  // face-major [f][slot][n][QF], spans B and C
-  constexpr int PG = C::PG;
+  constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G, PG = C::PG;
+  constexpr int NB = C::NFACE * C::EPB * C::NF;
   if constexpr (DIM == 3) {
-    contract<G, G, 1, 0, G, Q, MatG2GL<L, Q, T>, false, T, PG, 1, PG, 1, C::FPT>(sm.E, sm.S, NB, C::EB, Q * PG, tid, C::NT);
+    contract<G, G, 1, 0, G, Q, MatG2GL<L, Q, T>, false, T, PG, 1, PG, 1, C::FPT>(sm.E, sm.S, NB, C::EB, Q * PG,
+                                                                                tid, C::NT);
     csync<C>();
-    contract<Q, G, 1, 1, G, Q, MatG2GL<L, Q, T>, false, T, PG, 1, -1, -1, C::FPT>(sm.S, LFc, NB, Q * PG, Q * Q, tid, C::NT);
+    lift_face<C, 2>(sm, tid);
+    lift_face<C, 4>(sm, tid);
+    csync<C>();
+    lift_face<C, 1>(sm, tid);
+    lift_face<C, 3>(sm, tid);
+    csync<C>();
+    lift_face<C, 0>(sm, tid);
+    lift_face<C, 5>(sm, tid);
   } else {
-    contract<G, 1, 1, 0, G, Q, MatG2GL<L, Q, T>, false, typename C::R, -1, -1, -1, -1, C::FPT>(sm.E, LFc, NB, C::EB, Q, tid, C::NT);
-  }
-  csync<C>();
-  const T w0 = T(1) / cW<T, L, Q>[0], w1 = T(1) / cW<T, L, Q>[Q - 1];
-  for (int w = tid; w < EPB * NF * QD; w += C::NT) {
-    const int slot = w / (NF * QD), rem = w - slot * NF * QD, n = rem / QD, p = rem - n * QD;
-    T acc = sm.D[w];
-    if constexpr (DIM == 3) {
-      const int i = p / (Q * Q), j = (p / Q) % Q, k = p % Q;
-      auto lf = [&](int f, int x, int y) { return LFc[((f * EPB + slot) * NF + n) * QF + x * Q + y]; };
-      if (k == 0) acc = fma(w0, lf(0, i, j), acc);
-      if (j == 0) acc = fma(w0, lf(1, i, k), acc);
-      if (i == Q - 1) acc = fma(w1, lf(2, j, k), acc);
-      if (j == Q - 1) acc = fma(w1, lf(3, i, k), acc);
-      if (i == 0) acc = fma(w0, lf(4, j, k), acc);
-      if (k == Q - 1) acc = fma(w1, lf(5, i, j), acc);
-    } else {
-      const int i = p / Q, j = p % Q;
-      auto lf = [&](int f, int x) { return LFc[((f * EPB + slot) * NF + n) * QF + x]; };
-      if (j == 0) acc = fma(w0, lf(0, i), acc);
-      if (i == Q - 1) acc = fma(w1, lf(1, j), acc);
-      if (j == Q - 1) acc = fma(w1, lf(2, i), acc);
-      if (i == 0) acc = fma(w0, lf(3, j), acc);
-    }
-    // quadrature weights of the projection (the J of wJ cancels the mass)
-    T wq;
-    if constexpr (DIM == 3) wq = cW<T, L, Q>[p / (Q * Q)] * cW<T, L, Q>[(p / Q) % Q] * cW<T, L, Q>[p % Q];
-    else wq = cW<T, L, Q>[p / Q] * cW<T, L, Q>[p % Q];
-    sm.D[w] = wq * acc;
+    lift_face<C, 1>(sm, tid);
+    lift_face<C, 3>(sm, tid);
+    csync<C>();
+    lift_face<C, 0>(sm, tid);
+    lift_face<C, 2>(sm, tid);
   }
   csync<C>();
 }
@@ -768,14 +786,6 @@ __global__ void __launch_bounds__(C::NT, C::MINB) forward_kernel(StageArgs a, co
   constexpr int L = C::L, Q = C::Q, NF = C::NF, QD = C::QD, EPB = C::EPB;
   const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
   load_nodal<C>(sm.D, Un, e0, a.ne, tid);
-  csync<C>();
-  for (int w = tid; w < EPB * NF * QD; w += C::NT) {
-    const int p = w % QD;
-    double wq;
-    if constexpr (C::DIM == 3) wq = cW<double, L, Q>[p / (Q * Q)] * cW<double, L, Q>[(p / Q) % Q] * cW<double, L, Q>[p % Q];
-    else wq = cW<double, L, Q>[p / Q] * cW<double, L, Q>[p % Q];
-    sm.D[w] = wq * sm.D[w];
-  }
   csync<C>();
   forward<C>(sm.D, sm.R, sm.C, sm.B, tid, C::NT);
   constexpr int BLK = NF * C::LD;
