@@ -235,12 +235,13 @@ class Domain:
         return rows[: nv.value].copy(), ch.value
 
     def set_variant(self, index: int):
-        """Use compiled tile variant `index`; returns (variant count, one element per warp)."""
+        """Use compiled tile variant `index`; returns (variant count, kind): kind 0 is a
+        CTA tile, 2 the prefetching persistent kernel."""
         f = lib().dgmx_set_variant
         f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         n, w = ctypes.c_int(), ctypes.c_int()
         self._check(f(self.h, int(index), ctypes.byref(n), ctypes.byref(w)))
-        return n.value, bool(w.value)
+        return n.value, int(w.value)
 
     def variant_count(self) -> int:
         f = lib().dgmx_set_variant

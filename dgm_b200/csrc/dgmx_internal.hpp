@@ -146,7 +146,7 @@ constexpr int kMixedKey = 1000;
 // Launchers for one (physics, L, Q) instantiation; all enqueue on stream s.
 struct KernelOps {
   int epb = 0, nt = 0, minb = 0, mixed = 0;
-  int warp = 0;                                        // 1: one element per warp (epb = warps per CTA)
+  int warp = 0;                                        // kind: 0 CTA tile, 2 prefetching persistent kernel
   size_t smem = 0;
   cudaError_t (*init)(const Tables1D &t) = nullptr;   // tables + smem attributes, current device
   cudaError_t (*stage)(const StageArgs &a, cudaStream_t s) = nullptr;

@@ -154,45 +154,6 @@ constexpr int default_epb(int dim, int Q) {
                   : (Q * Q >= 100 ? 1 : (128 / (Q * Q) > 8 ? 8 : 128 / (Q * Q)));
 }
 
-// One element per warp, WPB warps per CTA (wstage_kernel).  The
-// projection, trace and nodal kernels come from the default CTA tile: their
-// layouts in global memory are the same.
-template <int PHYS, int L, int Q, int WPB, bool MIXED = false>
-struct WLaunch {
-  using C1 = Cfg<PHYS, L, Q, 1, 0, MIXED>;
-  using W = WarpCfg<C1, WPB>;
-  using Base = Launch<PHYS, L, Q, default_epb(phys_dim(PHYS), Q), 0, MIXED>;
-  static dim3 grid(int ne) { return dim3((unsigned)((ne + WPB - 1) / WPB)); }
-  static cudaError_t init(const Tables1D &t) {
-    cudaError_t e = Base::init(t);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(wstage_kernel<W, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)W::SMEM_CTA);
-  }
-  static cudaError_t stage(const StageArgs &a, cudaStream_t s) {
-    wstage_kernel<W, PHYS><<<grid(a.ne), W::CTA_NT, W::SMEM_CTA, s>>>(a);
-    return cudaGetLastError();
-  }
-  static cudaError_t stage_grid(const StageArgs &a, int g, cudaStream_t s) {
-    wstage_kernel<W, PHYS><<<g, W::CTA_NT, W::SMEM_CTA, s>>>(a);
-    return cudaGetLastError();
-  }
-  static int blocks_per_sm() {
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wstage_kernel<W, PHYS>, W::CTA_NT, W::SMEM_CTA) !=
-        cudaSuccess) {
-      cudaGetLastError();
-      return 1;
-    }
-    return n > 0 ? n : 1;
-  }
-  static KernelOps ops() {
-    KernelOps o = Base::ops();
-    o.epb = WPB; o.nt = W::CTA_NT; o.smem = W::SMEM_CTA; o.minb = 0; o.warp = 1;
-    o.init = init; o.stage = stage; o.stage_grid = stage_grid; o.blocks_per_sm = blocks_per_sm;
-    return o;
-  }
-};
 
 // Streaming multiprocessors of the current device (cached per device).
 inline int sm_count() {
@@ -264,12 +225,8 @@ void reg_pipe() {
   }
 }
 
-template <int PHYS, int P, int Q, int WPB, bool MIXED>
-void reg_warp() {
-  using W = typename WLaunch<PHYS, P + 1, Q, WPB, MIXED>::W;
-  if constexpr (W::SMEM_CTA <= 227 * 1024)
-    register_ops(PHYS + (MIXED ? kMixedKey : 0), P + 1, Q, WLaunch<PHYS, P + 1, Q, WPB, MIXED>::ops());
-}
+
+
 
 // CTAs per SM that the shared memory of one tile allows (228 KB per SM,
 // 1 KB reserved per CTA).
@@ -293,6 +250,7 @@ void reg_variant() {
   }
 }
 
+
 // Tile variants for (physics, p, q): the default packing without and with a
 // register cap at the shared-memory occupancy, and twice the packing.  The
 // first registered variant is the default; dgmx_autotune picks among all.
@@ -310,9 +268,6 @@ void reg() {
     constexpr int B2 = smem_blocks<C2>() > 8 ? 8 : smem_blocks<C2>();
     if constexpr (B2 >= 2) reg_variant<PHYS, P, Q, E2, B2, MIXED>();
   }
-  reg_warp<PHYS, P, Q, 1, MIXED>();
-  reg_warp<PHYS, P, Q, 2, MIXED>();
-  reg_warp<PHYS, P, Q, 4, MIXED>();
   if constexpr (Pipe<C1>::OK) {
     constexpr int PB = (int)((228 * 1024) / (Pipe<C1>::SMEM + 1024)) > 8 ? 8 : (int)((228 * 1024) / (Pipe<C1>::SMEM + 1024));
     reg_pipe<PHYS, P, Q, E1, 0, MIXED>();

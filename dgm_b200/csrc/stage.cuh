@@ -43,7 +43,7 @@ struct Cfg {
   // register U stays FP64 in global memory)
   static constexpr bool MIXED = MIXED_;
   static constexpr bool WARP = false;   // the helpers' team is the whole CTA
-  static constexpr int FPT = 1;         // fields per contraction task
+  static constexpr int FPT = 1;         // fields per contraction task (see contract)
   static constexpr int PHYSICS = PHYS;
   using R = std::conditional_t<MIXED_, float, double>;
   static constexpr int DIM = phys_dim(PHYS), NF = phys_nf(PHYS);
@@ -82,22 +82,7 @@ struct Cfg {
   static_assert(SMEM <= 227 * 1024 || EPB > 1, "element slot does not fit in shared memory");
 };
 
-// One element per warp: the per-element regions of the EPB = 1 tile C1,
-// WPB of them per CTA (one per warp).  The helpers run with the warp as
-// their team: NT = 32 threads and __syncwarp between phases, so the warps of
-// a CTA never wait for one another.
-template <class C1, int WPB_, int MINB_ = 0>
-struct WarpCfg : C1 {
-  static_assert(C1::EPB == 1, "a warp holds one element");
-  static constexpr bool WARP = true;
-  static constexpr int NT = 32;
-  static constexpr int FPT = C1::NF;
-  static constexpr int WPB = WPB_;
-  static constexpr int CTA_NT = 32 * WPB_;
-  static constexpr int MINB = MINB_ > 0 ? MINB_ : 1;
-  static constexpr size_t SLOT = (C1::SMEM + 127) / 128 * 128;   // shared bytes per warp
-  static constexpr size_t SMEM_CTA = SLOT * WPB_;
-};
+
 
 // Barrier of the helpers' team.
 template <class C>
@@ -521,8 +506,7 @@ __device__ __forceinline__ void load_own_traces(typename C::R *E, const TT *T, i
 }
 
 // ---------------------------------------------------------------- kernels
-// One fused RK stage on the EPB elements from e0, run by the team of C
-// (the CTA, or one warp for WarpCfg).
+// One fused RK stage on the EPB elements from e0, run by the CTA.
 template <class C, int PHYS>
 __device__ __forceinline__ void stage_tile(const Smem<C> &sm, const StageArgs &a, int e0, int tid) {
   load_geometry<C>(sm, a, e0, tid);
@@ -641,22 +625,6 @@ __global__ void __launch_bounds__(C::NT, C::MINB) stage_kernel(StageArgs a) {
   }
 }
 
-// The same with one element per warp (W = WarpCfg): each warp works through
-// its element alone, with no CTA-wide barrier; elements past the end or not
-// allocated in a pool are skipped by their warp.
-template <class W, int PHYS>
-__global__ void __launch_bounds__(W::CTA_NT, W::MINB) wstage_kernel(StageArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  Smem<W> sm(smem_raw + warp * W::SLOT);
-  const int ntile = a.tiles ? *a.ntiles : (int)gridDim.x;
-  for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
-    const int e = (a.tiles ? a.tiles[t] : t) * W::WPB + warp;
-    if (e >= a.ne || a.gclass[e] < 0) continue;
-    __syncwarp();
-    stage_tile<W, PHYS>(sm, a, e, lane);
-  }
-}
 
 // Traces of a modal register (start of a run, after set_state).
 template <class C>

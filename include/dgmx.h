@@ -156,8 +156,9 @@ dgmx_status dgmx_autotune(dgmx_domain *d, int reps, double *rows, int cap, int *
 
 /* Selects compiled tile variant `index` (0 .. nvariants-1, the order of
  * dgmx_autotune's rows) for the stage kernel of this handle; *count gets the
- * number of variants and *warp whether the chosen one runs one element per
- * warp.  No counterpart in the reference (tile choice is a GPU matter). */
+ * number of variants and *warp the kind of the chosen one: 0 a CTA tile,
+ * 2 the persistent kernel with a bulk-copy prefetch pipeline.  No
+ * counterpart in the reference (tile choice is a GPU matter). */
 dgmx_status dgmx_set_variant(dgmx_domain *d, int index, int *count, int *warp);
 
 /* Host-only inspection, no CUDA calls.  1-D tables for L modes and Q GLL
