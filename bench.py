@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--l2-steps", type=int, default=100, help="steps of the mixed-vs-FP64 accuracy run")
     ap.add_argument("--ensemble", type=int, default=1024, help="solves in the batched ensemble")
     ap.add_argument("--trace", type=int, default=200, help="requests in the serving trace")
+    ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both",
+                    help="time one form only (profiling runs); the default line needs both")
     return ap.parse_args()
 
 
@@ -358,7 +360,9 @@ def main():
 
     doms, tiles, results = {}, {}, {}
     U_ic = dt = None
-    for name, prec in (("fp64", dgm_b200.FP64), ("mixed", dgm_b200.MIXED)):
+    forms_run = [(k, v) for k, v in (("fp64", dgm_b200.FP64), ("mixed", dgm_b200.MIXED))
+                 if args.precision in ("both", k)]
+    for name, prec in forms_run:
         D = dgm_b200.Domain(mesh, dgm_b200.EULER3D, flux=WORKLOAD["flux"], inttype=dgm_b200.LSRK14,
                             device=local, precision=prec)
         if U_ic is None:
@@ -374,6 +378,19 @@ def main():
     streams = {k: torch.cuda.ExternalStream(D.stream(), device=torch.device("cuda", local)) for k, D in doms.items()}
 
     clk = ClockSampler(local)
+    if args.precision != "both":
+        # one form alone (profiling): its device time, nothing else
+        t1, _ = time_steps(doms[args.precision], streams[args.precision], dt, args.steps, args.warmup, barrier,
+                           max_over_ranks)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": world * dof * 14 * args.steps / t1, "unit": UNIT,
+                              "precision": args.precision, "ms_per_step": 1e3 * t1 / args.steps,
+                              "tile": tiles[args.precision], "note": "single-form profiling run"}), flush=True)
+        for Dx in doms.values():
+            Dx.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
     t64, _ = time_steps(doms["fp64"], streams["fp64"], dt, args.steps, args.warmup, barrier, max_over_ranks)
     tmx, launches = time_steps(doms["mixed"], streams["mixed"], dt, args.steps, args.warmup, barrier,
                                max_over_ranks, clk)
