@@ -250,9 +250,103 @@ class Domain:
         f(self.h, -1, ctypes.byref(n), ctypes.byref(w))
         return n.value
 
+    # --- restart files (DGM format) -------------------------------------
+    def set_modes(self, Uh):
+        """Set the state from restart-layout modal coefficients [field][element][L^d]."""
+        Uh = np.ascontiguousarray(Uh, dtype=np.float64).reshape(self.nf, self.nm)
+        f = lib().dgmx_set_modes
+        f.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        self._check(f(self.h, _dp(Uh)))
+
+    def write_restart(self, path: str, step: int = 0, t: float = 0.0, dt: float = 0.0):
+        f = lib().dgmx_write_restart
+        f.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        self._check(f(self.h, path.encode(), int(step), float(t), float(dt)))
+
+    def read_restart(self, path: str):
+        """Load a restart file into the state; returns (step, time)."""
+        f = lib().dgmx_read_restart
+        f.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+        step, t = ctypes.c_int(), ctypes.c_double()
+        self._check(f(self.h, path.encode(), ctypes.byref(step), ctypes.byref(t)))
+        return step.value, t.value
+
     def stream(self) -> int:
         """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
         return lib().dgmx_stream(self.h) or 0
+
+
+# ---- restart files and Domain::diff (host only, no GPU needed) -----------
+def _restart_err():
+    f = lib().dgmx_restart_last_error
+    f.restype = ctypes.c_char_p
+    return f().decode()
+
+
+def restart_write(path: str, physics: int, modes, step: int = 0, t: float = 0.0, dt: float = 0.0,
+                  vis: float = 0.0):
+    """Write modes [field][element][nmodes] as a DGM restart file."""
+    modes = np.ascontiguousarray(modes, dtype=np.float64)
+    nf, ne, nm = modes.shape
+    f = lib().dgmx_restart_write
+    f.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                  ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+    st = f(path.encode(), int(physics), ne, nm, int(step), float(t), float(dt), float(vis), _dp(modes))
+    if st != 0:
+        raise DgmxError(st, _restart_err())
+
+
+def restart_info(path: str) -> dict:
+    f = lib().dgmx_restart_info
+    I, D = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+    f.argtypes = [ctypes.c_char_p, I, I, I, I, D, D, D]
+    ne, nsd, lmax, step = (ctypes.c_int() for _ in range(4))
+    t, dt, vis = (ctypes.c_double() for _ in range(3))
+    st = f(path.encode(), ctypes.byref(ne), ctypes.byref(nsd), ctypes.byref(lmax), ctypes.byref(step),
+           ctypes.byref(t), ctypes.byref(dt), ctypes.byref(vis))
+    if st != 0:
+        raise DgmxError(st, _restart_err())
+    return dict(ne=ne.value, nsd=nsd.value, lmax=lmax.value, step=step.value, t=t.value, dt=dt.value,
+                vis=vis.value)
+
+
+def restart_read(path: str, nf: int):
+    """(per-element mode counts, list of per-field coefficient arrays, header info)."""
+    info = restart_info(path)
+    ne = info["ne"]
+    cap = nf * ne * info["lmax"]
+    nmodes = np.zeros(ne, dtype=np.int32)
+    modes = np.zeros(cap)
+    f = lib().dgmx_restart_read
+    f.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                  ctypes.POINTER(ctypes.c_double), ctypes.c_longlong]
+    st = f(path.encode(), nf, ne, nmodes.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(modes), cap)
+    if st != 0:
+        raise DgmxError(st, _restart_err())
+    tot = int(nmodes.sum())
+    return nmodes, [modes[k * tot:(k + 1) * tot].copy() for k in range(nf)], info
+
+
+def restart_diff(mesh, physics: int, rst1: str, rst2: str, aeps: float = -1.0, reps: float = -1.0):
+    """Domain::diff of two restart files on `mesh`: (status bits, norms[nf][6])."""
+    verts = np.ascontiguousarray(mesh.verts, dtype=np.float64)
+    con = np.ascontiguousarray(mesh.con, dtype=np.int32)
+    por = np.ascontiguousarray(mesh.porder, dtype=np.int32)
+    qor = np.ascontiguousarray(mesh.qorder, dtype=np.int32)
+    m = _Mesh(int(mesh.dim), int(verts.shape[0]), _dp(verts), int(con.shape[0]),
+              con.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), por.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+              qor.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    nf = 3 if physics == SHALLOW else (5 if mesh.dim == 3 else 4)
+    norms = np.zeros((nf, 6))
+    status = ctypes.c_int()
+    f = lib().dgmx_restart_diff
+    f.argtypes = [ctypes.POINTER(_Mesh), ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double,
+                  ctypes.c_double, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
+    st = f(ctypes.byref(m), int(physics), rst1.encode(), rst2.encode(), float(aeps), float(reps), _dp(norms),
+           ctypes.byref(status))
+    if st != 0:
+        raise DgmxError(st, _restart_err())
+    return status.value, norms
 
 
 class _PoolParams(ctypes.Structure):

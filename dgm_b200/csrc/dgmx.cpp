@@ -475,6 +475,58 @@ dgmx_status dgmx_get_modes(dgmx_domain *d, double *Uh) {
   return DGMX_OK;
 }
 
+dgmx_status dgmx_set_modes(dgmx_domain *d, const double *Uh) {
+  if (!d || !Uh) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(d->prm.device);
+  // restart layout [n][e][m] -> element-major [e][n][m]
+  std::vector<double> em(d->nmodal());
+  for (int el = 0; el < d->ne; ++el)
+    for (int n = 0; n < d->nf; ++n)
+      std::memcpy(em.data() + ((size_t)el * d->nf + n) * d->ld, Uh + ((size_t)n * d->ne + el) * d->ld,
+                  sizeof(double) * d->ld);
+  cudaError_t e = cudaMemcpyAsync(d->U, em.data(), sizeof(double) * em.size(), cudaMemcpyHostToDevice, d->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d->Ut, 0, sizeof(double) * d->nmodal(), d->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d->Acc, 0, sizeof(double) * d->nmodal(), d->stream);
+  if (e == cudaSuccess && d->Utf) e = cudaMemsetAsync(d->Utf, 0, sizeof(float) * d->nmodal(), d->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+  if (e != cudaSuccess) return d->cuda(e, "set_modes");
+  d->tcur = 0;
+  d->sw_captured = false;
+  const dgmx_status st = refresh_traces(d);
+  if (st != DGMX_OK) return st;
+  return d->cuda(cudaStreamSynchronize(d->stream), "set_modes");
+}
+
+dgmx_status dgmx_write_restart(dgmx_domain *d, const char *path, int step, double t, double dt) {
+  if (!d || !path) return DGMX_ERR_ARGUMENT;
+  std::vector<double> Uh((size_t)d->nf * d->ne * d->ld);
+  dgmx_status st = dgmx_get_modes(d, Uh.data());
+  if (st != DGMX_OK) return st;
+  st = dgmx_restart_write(path, d->prm.physics, d->ne, d->ld, step, t, dt, d->prm.vis, Uh.data());
+  if (st != DGMX_OK) d->errmsg = dgmx_restart_last_error();
+  return st;
+}
+
+dgmx_status dgmx_read_restart(dgmx_domain *d, const char *path, int *step, double *t) {
+  if (!d || !path) return DGMX_ERR_ARGUMENT;
+  int ne = 0, nsd = 0, lmax = 0, stp = 0;
+  double tt = 0, dt = 0, vis = 0;
+  dgmx_status st = dgmx_restart_info(path, &ne, &nsd, &lmax, &stp, &tt, &dt, &vis);
+  if (st != DGMX_OK) { d->errmsg = dgmx_restart_last_error(); return st; }
+  if (ne != d->ne || nsd != d->dim) return d->fail(DGMX_ERR_ARGUMENT, "restart: mesh size or dimension differs");
+  std::vector<int> nm(ne);
+  std::vector<double> Uh((size_t)d->nf * d->ne * d->ld);
+  st = dgmx_restart_read(path, d->nf, ne, nm.data(), Uh.data(), (long long)Uh.size());
+  if (st != DGMX_OK) { d->errmsg = dgmx_restart_last_error(); return st; }
+  for (int e = 0; e < ne; ++e)
+    if (nm[e] != d->ld) return d->fail(DGMX_ERR_ARGUMENT, "restart: mode count differs from this domain's order");
+  st = dgmx_set_modes(d, Uh.data());
+  if (st != DGMX_OK) return st;
+  if (step) *step = stp;
+  if (t) *t = tt;
+  return DGMX_OK;
+}
+
 dgmx_status dgmx_time_derivative_device(dgmx_domain *d, const double *U_dev, double *F_dev) {
   if (!d || !U_dev || !F_dev) return DGMX_ERR_ARGUMENT;
   cudaSetDevice(d->prm.device);

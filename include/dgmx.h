@@ -97,6 +97,40 @@ dgmx_status dgmx_get_state_device(dgmx_domain *d, double *U_dev);
 /* Current solution as restart modal coefficients (host). */
 dgmx_status dgmx_get_modes(dgmx_domain *d, double *Uh);
 
+/* Sets the solution from restart-layout modal coefficients (the inverse of
+ * dgmx_get_modes; no projection) and resets the integrator registers. */
+dgmx_status dgmx_set_modes(dgmx_domain *d, const double *Uh);
+
+/* Restart files in DGM's format (text header, src/Domain.cpp:1721-1785;
+ * per-field mode counts, displacements and orthonormal coefficients,
+ * src/vField.cpp:1082-1200).  Write the current state; read one back into
+ * the state (the file's element count and order must match the domain). */
+dgmx_status dgmx_write_restart(dgmx_domain *d, const char *path, int step, double t, double dt);
+dgmx_status dgmx_read_restart(dgmx_domain *d, const char *path, int *step, double *t);
+
+/* Host-only restart helpers (no CUDA calls).  dgmx_restart_write writes
+ * modes in restart layout (nf x ne x nmodes) with a text header;
+ * dgmx_restart_info reads the header; dgmx_restart_read reads nf fields
+ * (per-element mode counts into nmodes[ne], coefficients into modes, at most
+ * cap values). */
+dgmx_status dgmx_restart_write(const char *path, int physics, int ne, int nmodes, int step, double t, double dt,
+                               double vis, const double *modes);
+dgmx_status dgmx_restart_info(const char *path, int *ne, int *nsd, int *lmax, int *step, double *t, double *dt,
+                              double *vis);
+dgmx_status dgmx_restart_read(const char *path, int nf, int ne, int *nmodes, double *modes, long long cap);
+
+/* Domain::diff (src/Domain.cpp:1000-1066), host only: reads two restart
+ * files on the given mesh, computes per field the Linf, L2 and H1 norms
+ * (src/Field.cpp:4675-4697) of their difference and of the first, and sets
+ * *status bits as the reference does: 1/2/4 absolute Linf/L2/H1 above aeps,
+ * 8/16/32 relative Linf/L2/H1 above reps (where the first file's norm is above
+ * sqrt(machine epsilon)); a negative tolerance skips its test.  norms
+ * (optional) gets nf rows of (Linf, L2, H1 of the difference, Linf, L2, H1 of
+ * the first file). */
+dgmx_status dgmx_restart_diff(const dgmx_mesh *mesh, int physics, const char *rst1, const char *rst2, double aeps,
+                              double reps, double *norms, int *status);
+const char *dgmx_restart_last_error(void);
+
 /* Domain::time_derivative(U, F) (src/Domain.hpp:243): F = -dU/dt at GLL
  * points, projected, for U given at GLL points.  Host buffers, Field layout. */
 dgmx_status dgmx_time_derivative(dgmx_domain *d, const double *U, double *F);
