@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--trace", type=int, default=200, help="requests in the serving trace")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both",
                     help="time one form only (profiling runs); the default line needs both")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="single-form runs: use this tile variant instead of the autotuner's pick")
     return ap.parse_args()
 
 
@@ -372,6 +374,9 @@ def main():
         D.set_state(U_ic)
         # tile autotuning is set-up, outside the timed region
         rows, pick = D.autotune(reps=10)
+        if args.precision != "both" and args.variant >= 0:
+            D.set_variant(args.variant)
+            pick = args.variant
         tiles[name] = {"elements_per_cta": int(rows[pick][0]), "min_ctas_per_sm": int(rows[pick][1]),
                        "threads_per_cta": int(rows[pick][2]), "candidates_us": [round(float(r[3]), 1) for r in rows]}
         doms[name] = D

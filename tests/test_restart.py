@@ -113,7 +113,7 @@ def test_diff_norms_match_field_norm():
 def test_domain_restart_round_trip_and_diff_against_oracle():
     """A GPU state written and read back is the same state; a GPU run written
     as a restart passes DGM's diff against the oracle's run of the same case
-    at 1e-12 absolute and relative tolerances."""
+    (1e-12 absolute, 1e-8 relative)."""
     import dgm_b200
     m = dgm_b200.meshgen.box(3, (3, 3, 3), 0.0, 2 * np.pi, 3)
     mesh = dgm_io.Mesh(m.dim, m.verts, m.con, m.porder, m.qorder)
@@ -130,8 +130,11 @@ def test_domain_restart_round_trip_and_diff_against_oracle():
         gpu, ora = os.path.join(d, "gpu.rst"), os.path.join(d, "oracle.rst")
         D.write_restart(gpu, step=3, t=0.006, dt=0.002)
         dgm_b200.restart_write(ora, dgm_b200.EULER3D, P.forward(P.state()).reshape(5, ne, -1), step=3, t=0.006)
-        status, norms = dgm_b200.restart_diff(m, dgm_b200.EULER3D, ora, gpu, aeps=1e-12, reps=1e-12)
+        # the w-momentum of the Taylor-Green case is ~1e-6 after three steps, so
+        # its relative error at round-off is ~1e-9: the relative test uses 1e-8
+        status, norms = dgm_b200.restart_diff(m, dgm_b200.EULER3D, ora, gpu, aeps=1e-12, reps=1e-8)
         assert status == 0, norms
+        assert norms[:, :3].max() < 1e-12
         D2 = dgm_b200.Domain(m, dgm_b200.EULER3D, inttype=dgm_b200.TVD3)
         step, t = D2.read_restart(gpu)
         assert step == 3 and t == 0.006
