@@ -50,7 +50,7 @@ struct dgmx_domain {
   double *Rsw = nullptr;                                 // shallow-water first RHS (modal)
   double *Ghat = nullptr, *Vtr = nullptr, *Pv = nullptr; // Navier-Stokes BR1 work
   float *Utf = nullptr, *Tf[2] = {nullptr, nullptr};     // mixed form: FP32 register and traces
-  double *uref = nullptr;                                // mixed form: reference state (10 doubles)
+  double *uref = nullptr;                                // mixed form: reference state row (kUrefStride)
   double *nod_in = nullptr, *nod_out = nullptr;          // Field-layout staging
   double *Jdev = nullptr, *integ = nullptr;
   int *gclass = nullptr, *perm = nullptr, *err = nullptr;
@@ -161,8 +161,7 @@ int launches_per_stage(const dgmx_domain *d) { return d->ns() ? 3 : 1; }
 
 // Mixed form: the reference state the FP32 working copies are perturbations
 // about is the domain mean of U (any constant gives the same scheme; the
-// mean keeps the perturbations small).  uref[n] = mean, uref[5 + n] = its
-// constant-mode coefficient.
+// mean keeps the perturbations small); one row, see fill_reference_row.
 dgmx_status update_reference(dgmx_domain *d) {
   const double c = std::pow(std::sqrt(2.0), d->dim);
   cudaError_t e = launch_integrals(d->nf, d->ne, d->ld, c, d->U, d->Jdev, d->integ, d->stream);
@@ -175,8 +174,9 @@ dgmx_status update_reference(dgmx_domain *d) {
   for (int k = 0; k < d->ne; ++k) vol += d->mesh.J[k];
   vol *= std::pow(2.0, d->dim);
   const double phi0 = std::pow(d->tab.B[0], d->dim);   // constant mode's value
-  double h[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (int n = 0; n < d->nf; ++n) { h[n] = tot[n] / vol; h[5 + n] = h[n] / phi0; }
+  double h[kUrefStride] = {};
+  for (int n = 0; n < d->nf; ++n) h[n] = tot[n] / vol;
+  fill_reference_row(d->prm.physics, d->prm.gamma, phi0, h);
   e = cudaMemcpyAsync(d->uref, h, sizeof(h), cudaMemcpyHostToDevice, d->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
   return d->cuda(e, "reference state upload");
@@ -310,7 +310,7 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
             (!d->mixed() || (chk(dalloc(&d->Utf, d->nmodal()), "alloc Ut (FP32)") &&
                              chk(dalloc(&d->Tf[0], d->ntrace()), "alloc T0 (FP32)") &&
                              chk(dalloc(&d->Tf[1], d->ntrace()), "alloc T1 (FP32)") &&
-                             chk(dalloc(&d->uref, (size_t)10), "alloc reference state"))) &&
+                             chk(dalloc(&d->uref, (size_t)kUrefStride), "alloc reference state"))) &&
             (!d->ns() || (chk(dalloc(&d->Ghat, (size_t)d->ne * (d->dim + 1) * d->dim * d->ld), "alloc gradients") &&
                           chk(dalloc(&d->Vtr, (size_t)d->ne * d->nfaces * (d->nf - 1) * d->gf), "alloc viscous traces") &&
                           chk(dalloc(&d->Pv, (size_t)d->ne * (d->nf - 1) * d->ld), "alloc viscous divergence")));

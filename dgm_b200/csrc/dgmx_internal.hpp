@@ -83,6 +83,42 @@ inline constexpr double kLsrkB[14] = {0.0367762454319673, 0.3136296607553959, 0.
                            0.1524043173028741, 0.0760894927419266, 0.0077604214040978, 0.0024647284755382,
                            0.0780348340049386, 5.5059777270269628};
 
+// ------------------------------------------------------------ mixed form
+// Reference state of a solve (the working copies of the mixed form are
+// perturbations about it): the conserved values, their velocity, E + p and
+// pressure.  Built once per solve on the host.
+template <class T>
+struct RefState {
+  T r, m[3], E;   // reference density (geopotential), momentum, energy
+  T u[3], H, p;   // its velocity, E + p and pressure
+  T pad[6];
+};
+
+// One row per solve in the reference-state array: [0, 5) the conserved
+// reference values, [5, 10) their constant-mode coefficients, [10, 18) the
+// FP32 RefState packed as doubles.
+constexpr int kUrefStride = 24;
+
+// Fills row[5..] from row[0..nf): phi0 is the constant basis function's
+// value (the constant mode of a constant c is c / phi0).
+inline void fill_reference_row(int physics, double gamma, double phi0, double *row) {
+  const bool sw = physics == DGMX_SHALLOW;
+  const int dim = (physics == DGMX_EULER3D || physics == DGMX_NS3D) ? 3 : 2, nf = sw ? 3 : dim + 2;
+  for (int n = 0; n < nf; ++n) row[5 + n] = row[n] / phi0;
+  RefState<float> rs{};
+  const double r = row[0];
+  double q = 0.0, u[3] = {0.0, 0.0, 0.0};
+  for (int i = 0; i < dim; ++i) { u[i] = row[1 + i] / r; q += row[1 + i] * u[i]; }
+  const double p = sw ? 0.5 * r * r : (gamma - 1.0) * (row[nf - 1] - 0.5 * q);
+  rs.r = (float)r;
+  for (int i = 0; i < dim; ++i) { rs.m[i] = (float)row[1 + i]; rs.u[i] = (float)u[i]; }
+  rs.E = sw ? 0.0f : (float)row[nf - 1];
+  rs.p = (float)p;
+  rs.H = sw ? 0.0f : (float)(row[nf - 1] + p);
+  static_assert(sizeof(RefState<float>) == 8 * sizeof(double), "RefState<float> packs into 8 doubles");
+  __builtin_memcpy(row + 10, &rs, sizeof(rs));
+}
+
 // ------------------------------------------------------------------ kernels
 // Integrator stage kinds.  X is the register the RHS is evaluated on.
 enum StageKind : int {

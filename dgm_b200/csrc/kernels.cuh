@@ -319,30 +319,6 @@ __device__ __forceinline__ bool face_flux(const T *UL, const T *UR, const T *n, 
 //   p' = (g-1)(E' - (m'.ub + m.u')/2),  F'_rho = m',
 //   F'_m = m' ub_d + m u'_d + p' e_d,   F'_E = H' ub_d + H u'_d  (H = E + p);
 // shallow water: p' = phi'(phi_b + phi'/2) for the phi^2/2 pressure.
-template <class T>
-struct RefState {
-  T r, m[3], E;   // reference density (geopotential), momentum, energy
-  T u[3], H, p;   // its velocity, E + p and pressure
-  T pad[5];
-};
-
-template <int PHYS, class T>
-__device__ __forceinline__ RefState<T> make_ref(const double *Ub, double gamma) {
-  constexpr bool SW = PHYS == DGMX_SHALLOW;
-  constexpr int DIM = (PHYS == DGMX_EULER3D || PHYS == DGMX_NS3D) ? 3 : 2, NF = SW ? 3 : DIM + 2;
-  RefState<T> rs{};
-  const double r = Ub[0];
-  double q = 0.0, u[3] = {0.0, 0.0, 0.0};
-  for (int i = 0; i < DIM; ++i) { u[i] = Ub[1 + i] / r; q += Ub[1 + i] * u[i]; }
-  const double p = SW ? 0.5 * r * r : (gamma - 1.0) * (Ub[NF - 1] - 0.5 * q);
-  rs.r = T(r);
-  for (int i = 0; i < DIM; ++i) { rs.m[i] = T(Ub[1 + i]); rs.u[i] = T(u[i]); }
-  rs.E = SW ? T(0) : T(Ub[NF - 1]);
-  rs.p = T(p);
-  rs.H = SW ? T(0) : T(Ub[NF - 1] + p);
-  return rs;
-}
-
 // F(Ub + d) - F(Ub) in every direction (volume term).
 template <int PHYS, class T>
 __device__ __forceinline__ void volume_flux_pert(const RefState<T> &b, const T *d, T gamma, T (*F)[5]) {

@@ -178,8 +178,10 @@ __device__ __forceinline__ void stage_tile_pipe(const Smem<C> &sm, const StageAr
                                                 const unsigned char *buf, int tid) {
   using T = typename C::R;
   using P = Pipe<C>;
-  constexpr int NF = C::NF, LD = C::LD, BLK = NF * LD, NFACE = C::NFACE, GF = C::GF, EPB = C::EPB;
-  // geometry (class from the first face link), links, and the reference state
+  constexpr int NF = C::NF, LD = C::LD, NFACE = C::NFACE, GF = C::GF, G = C::G, EPB = C::EPB, L = C::L;
+  constexpr int RPF = LD / L, RPS = NF * RPF;                  // modal rows
+  constexpr int TPF = GF / G, TPS = NFACE * NF * TPF;          // trace rows
+  // geometry (class from the first face link), and the reference state
   constexpr int GW = (int)(sizeof(GeomClass) / sizeof(double));
   for (int k = tid; k < EPB * GW; k += C::NT) {
     const int s = k / GW, j = k - s * GW, e = e0 + s;
@@ -188,29 +190,30 @@ __device__ __forceinline__ void stage_tile_pipe(const Smem<C> &sm, const StageAr
     if (j == 0) {
       sm.eid[s] = gc >= 0 ? e : -1;
       if constexpr (C::MIXED)
-        sm.ref[s] = make_ref<C::PHYSICS, T>(a.uref + 10 * solve_of(a, gc >= 0 ? e : -1), a.gamma);
+        sm.ref[s] = *reinterpret_cast<const RefState<float> *>(a.uref + kUrefStride * solve_of(a, gc >= 0 ? e : -1) + 10);
     }
   }
-  // modal register (padded, perturbation form when mixed) and own traces
-  for (int w = tid; w < EPB * BLK; w += C::NT) {
-    const int s = w / BLK, r = w - s * BLK, e = e0 + s;
-    double x = 0.0;
-    if (e < a.ne && sm.lnk[s * NFACE].cls >= 0) {
-      x = reinterpret_cast<const double *>(buf + P::u_off(s))[r];
-      if constexpr (C::MIXED)
-        if (r % LD == 0) x -= a.uref[10 * solve_of(a, e) + 5 + r / LD];
-    } else if (r % LD == 0) {
-      x = 1.0;
-    }
-    sm.A[apos<C>(w)] = T(x);
+  // modal register (padded, perturbation form when mixed), a row per thread
+  for (int r = tid; r < EPB * RPS; r += C::NT) {
+    const int s = r / RPS, rr = r - s * RPS, e = e0 + s;
+    const double *src = reinterpret_cast<const double *>(buf + P::u_off(s)) + rr * L;
+    const bool live = e < a.ne && sm.lnk[s * NFACE].cls >= 0;
+    double ref0 = 0.0;
+    if constexpr (C::MIXED)
+      if (live && rr % RPF == 0) ref0 = a.uref[kUrefStride * solve_of(a, e) + 5 + rr / RPF];
+#pragma unroll
+    for (int k = 0; k < L; ++k)
+      sm.A[r * C::PL + k] = live ? T(k == 0 ? src[k] - ref0 : src[k]) : T(k == 0 && rr % RPF == 0 ? 1.0 : 0.0);
   }
-  for (int w = tid; w < EPB * NFACE * NF * GF; w += C::NT) {
-    const int s = w / (NFACE * NF * GF), rem = w - s * NFACE * NF * GF;
-    const int f = rem / (NF * GF), ng = rem - f * NF * GF, n = ng / GF, g = ng - n * GF;
+  // own traces, a row of G per thread
+  for (int r = tid; r < EPB * TPS; r += C::NT) {
+    const int s = r / TPS, rr = r - s * TPS, fn = rr / TPF, g1 = rr - fn * TPF, f = fn / NF, n = fn - f * NF;
     const int e = e0 + s;
     const bool live = e < a.ne && sm.lnk[s * NFACE].cls >= 0;
-    sm.E[((f * EPB + s) * NF + n) * C::EB + epos<C>(g)] =
-        live ? reinterpret_cast<const T *>(buf + P::own_off(s))[rem] : T(ng < GF ? 1.0 : 0.0);
+    const T *src = reinterpret_cast<const T *>(buf + P::own_off(s)) + rr * G;
+    T *dst = sm.E + ((f * EPB + s) * NF + n) * C::EB + g1 * C::PG;
+#pragma unroll
+    for (int k = 0; k < G; ++k) dst[k] = live ? src[k] : T(n == 0 ? 1.0 : 0.0);
   }
   csync<C>();
   backward<C>(sm.A, sm.B, sm.S, sm.C, tid, C::NT);
@@ -218,43 +221,65 @@ __device__ __forceinline__ void stage_tile_pipe(const Smem<C> &sm, const StageAr
   face_fluxes_pipe<C, PHYS>(sm, a, buf, tid);
   lift<C>(sm, tid);
   forward<C>(sm.D, sm.R, sm.C, sm.B, tid, C::NT);
-  for (int w = tid; w < EPB * BLK; w += C::NT) {
-    const int s = w / BLK, r = w - s * BLK, e = e0 + s;
+  // LSRK update, a row of L modes per thread (U and Ut from the buffer)
+  for (int r = tid; r < EPB * RPS; r += C::NT) {
+    const int s = r / RPS, rr = r - s * RPS, e = e0 + s;
     if (sm.eid[s] < 0) continue;
-    const size_t gi = (size_t)e0 * BLK + w;
+    const size_t gi = ((size_t)e0 * RPS + r) * L;
     const double dt = a.dts ? a.dts[solve_of(a, e)] : a.dt;
-    const double u0 = reinterpret_cast<const double *>(buf + P::u_off(s))[r];
-    const typename P::UT ut0 = reinterpret_cast<const typename P::UT *>(buf + P::ut_off(s))[r];
+    const double *u0 = reinterpret_cast<const double *>(buf + P::u_off(s)) + rr * L;
+    const typename P::UT *ut0 = reinterpret_cast<const typename P::UT *>(buf + P::ut_off(s)) + rr * L;
+    T *Ar = sm.A + r * C::PL;
+    const T *Rr = sm.R + r * L;
     if constexpr (C::MIXED) {
-      float rr = sm.R[w];
-      if (a.Rsub) rr = rr - float(a.Rsub[gi]);
-      float next;
+      float q[L];
+#pragma unroll
+      for (int k = 0; k < L; ++k) q[k] = Rr[k];
+      if (a.Rsub)
+#pragma unroll
+        for (int k = 0; k < L; ++k) q[k] -= float(a.Rsub[gi + k]);
       if (a.kind == kRHS) {
-        a.A[gi] = rr;
-        next = sm.A[apos<C>(w)];
-      } else {
-        float ut = float(a.c0) * ut0;
-        ut = fmaf(-float(dt), rr, ut);
-        const double u = fma(a.c1, double(ut), u0);
-        a.Utf[gi] = ut; a.U[gi] = u;
-        next = float(r % LD == 0 ? u - a.uref[10 * solve_of(a, e) + 5 + r / LD] : u);
+#pragma unroll
+        for (int k = 0; k < L; ++k) a.A[gi + k] = q[k];
+        continue;
       }
-      sm.A[apos<C>(w)] = next;
+      float ut[L];
+      double u[L];
+      const float c0 = float(a.c0), mdt = -float(dt);
+#pragma unroll
+      for (int k = 0; k < L; ++k) {
+        ut[k] = fmaf(mdt, q[k], c0 * ut0[k]);
+        u[k] = fma(a.c1, double(ut[k]), u0[k]);
+      }
+      st_row<L>(a.Utf + gi, ut);
+      st_row<L>(a.U + gi, u);
+      const double ref0 = rr % RPF == 0 ? a.uref[kUrefStride * solve_of(a, e) + 5 + rr / RPF] : 0.0;
+#pragma unroll
+      for (int k = 0; k < L; ++k) Ar[k] = float(k == 0 ? u[k] - ref0 : u[k]);
     } else {
-      double rr = sm.R[w];
-      if (a.Rcap) a.Rcap[gi] = rr;
-      if (a.Rsub) rr = rr - a.Rsub[gi];
-      double next;
+      double q[L];
+#pragma unroll
+      for (int k = 0; k < L; ++k) q[k] = Rr[k];
+      if (a.Rcap)
+#pragma unroll
+        for (int k = 0; k < L; ++k) a.Rcap[gi + k] = q[k];
+      if (a.Rsub)
+#pragma unroll
+        for (int k = 0; k < L; ++k) q[k] -= a.Rsub[gi + k];
       if (a.kind == kRHS) {
-        a.A[gi] = rr;
-        next = u0;
-      } else {
-        double ut = a.c0 * ut0;
-        ut = fma(-dt, rr, ut);
-        const double u = fma(a.c1, ut, u0);
-        a.Ut[gi] = ut; a.U[gi] = u; next = u;
+#pragma unroll
+        for (int k = 0; k < L; ++k) a.A[gi + k] = q[k];
+        continue;
       }
-      sm.A[apos<C>(w)] = next;
+      double ut[L], u[L];
+#pragma unroll
+      for (int k = 0; k < L; ++k) {
+        ut[k] = fma(-dt, q[k], a.c0 * ut0[k]);
+        u[k] = fma(a.c1, ut[k], u0[k]);
+        Ar[k] = u[k];
+      }
+      st_row<L>(a.Ut + gi, ut);
+      st_row<L>(a.U + gi, u);
     }
   }
   csync<C>();

@@ -151,7 +151,7 @@ struct Arena {
   bool tiles_dirty = true, dts_dirty = true;
   int *tiles_pin = nullptr;           // pinned: [0] = count, then tiles
   double *dts_pin = nullptr;          // pinned: one step per solve slot
-  double *uref_pin = nullptr;         // pinned: 10 doubles per solve slot
+  double *uref_pin = nullptr;         // pinned: kUrefStride doubles per solve slot
   cudaGraphExec_t graph = nullptr;
   int tcur = 0;
 
@@ -311,7 +311,8 @@ dgmx_status get_arena(dgmx_pool *P, int phys, int L, int Q, Arena **out) {
   if (!a->fops || !vs || vs->empty())
     return P->fail(DGMX_ERR_UNSUPPORTED, "no kernels built for physics " + std::to_string(phys) + ", p=" +
                                              std::to_string(L - 1) + ", q=" + std::to_string(Q));
-  const size_t fixed = sizeof(GeomClass) * kClassCap + sizeof(int) * kPermCap + sizeof(double) * 11 * kSlotCap + 8;
+  const size_t fixed = sizeof(GeomClass) * kClassCap + sizeof(int) * kPermCap +
+                       sizeof(double) * (kUrefStride + 1) * kSlotCap + 8;
   if (!P->fits(fixed)) return P->fail(DGMX_ERR_MEMORY, "pool budget exceeded");
   const int v = P->prm.autotune ? tuned_variant(phys, mixed, L, Q, P->prm.gamma, P->prm.flux, P->prm.device) : -1;
   a->sops = (v >= 0 && v < (int)vs->size()) ? &(*vs)[v] : &(*vs)[0];
@@ -323,21 +324,22 @@ dgmx_status get_arena(dgmx_pool *P, int phys, int L, int Q, Arena **out) {
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&a->uploaded, cudaEventDisableTiming);
   if (e == cudaSuccess) e = dalloc(&a->classes, (size_t)kClassCap);
   if (e == cudaSuccess) e = dalloc(&a->perm, (size_t)kPermCap);
-  if (e == cudaSuccess) e = dalloc(&a->uref, (size_t)10 * kSlotCap);
+  if (e == cudaSuccess) e = dalloc(&a->uref, (size_t)kUrefStride * kSlotCap);
   if (e == cudaSuccess) e = dalloc(&a->dts, (size_t)kSlotCap);
   if (e == cudaSuccess) e = dalloc(&a->err, (size_t)2);
-  if (e == cudaSuccess) e = cudaMemsetAsync(a->uref, 0, sizeof(double) * 10 * kSlotCap, a->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(a->uref, 0, sizeof(double) * kUrefStride * kSlotCap, a->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(a->dts, 0, sizeof(double) * kSlotCap, a->stream);
   if (e == cudaSuccess)
     e = cudaHostAlloc(reinterpret_cast<void **>(&a->dts_pin), sizeof(double) * kSlotCap, cudaHostAllocDefault);
   if (e == cudaSuccess)
-    e = cudaHostAlloc(reinterpret_cast<void **>(&a->uref_pin), sizeof(double) * 10 * kSlotCap, cudaHostAllocDefault);
+    e = cudaHostAlloc(reinterpret_cast<void **>(&a->uref_pin), sizeof(double) * kUrefStride * kSlotCap,
+                      cudaHostAllocDefault);
   const int init[2] = {0, 0x7fffffff};
   if (e == cudaSuccess) e = cudaMemcpyAsync(a->err, init, sizeof(init), cudaMemcpyHostToDevice, a->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(a->stream);
   if (e != cudaSuccess) { free_arena(*a); return P->cuda(e, "arena setup"); }
   std::memset(a->dts_pin, 0, sizeof(double) * kSlotCap);
-  std::memset(a->uref_pin, 0, sizeof(double) * 10 * kSlotCap);
+  std::memset(a->uref_pin, 0, sizeof(double) * kUrefStride * kSlotCap);
   a->slot_cap = kSlotCap; a->class_cap = kClassCap; a->perm_cap = kPermCap;
   P->bytes += fixed;
   *out = a.get();
@@ -536,7 +538,7 @@ dgmx_status add_impl(dgmx_pool *P, const dgmx_mesh *m, int phys, const double *U
     lks[(size_t)e * a.nfaces].cls = gcl[e];
   }
   // reference state of the mixed form: the J- and GLL-weighted mean of U0
-  double ref[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double ref[kUrefStride] = {};
   {
     std::vector<double> wq(a.qd);
     for (int i = 0; i < a.qd; ++i) {
@@ -551,8 +553,8 @@ dgmx_status add_impl(dgmx_pool *P, const dgmx_mesh *m, int phys, const double *U
       for (int e = 0; e < ne; ++e)
         for (int i = 0; i < a.qd; ++i) s += hm.J[e] * wq[i] * U0[((size_t)n * ne + e) * a.qd + i];
       ref[n] = s / vol;
-      ref[5 + n] = ref[n] / std::pow(a.tab.B[0], a.dim);
     }
+    fill_reference_row(phys, P->prm.gamma, std::pow(a.tab.B[0], a.dim), ref);
   }
   // uploads (the arena stream is idle between steps)
   cudaError_t e = cudaStreamSynchronize(a.stream);
@@ -564,8 +566,8 @@ dgmx_status add_impl(dgmx_pool *P, const dgmx_mesh *m, int phys, const double *U
   up(a.gclass + e0, gcl.data(), sizeof(int) * nalloc);
   up(a.esolve + e0, es.data(), sizeof(int) * nalloc);
   up(a.links + (size_t)e0 * a.nfaces, lks.data(), sizeof(FaceLink) * lks.size());
-  std::memcpy(a.uref_pin + 10 * slot, ref, sizeof(ref));
-  up(a.uref + 10 * slot, a.uref_pin + 10 * slot, sizeof(ref));
+  std::memcpy(a.uref_pin + (size_t)kUrefStride * slot, ref, sizeof(ref));
+  up(a.uref + (size_t)kUrefStride * slot, a.uref_pin + (size_t)kUrefStride * slot, sizeof(ref));
   up(P->scratch, U0, sizeof(double) * nodal);
   // projection of U0 into the range, zero second register, traces
   StageArgs s = arena_args(P, a);

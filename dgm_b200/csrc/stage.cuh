@@ -426,7 +426,7 @@ __device__ __forceinline__ void load_geometry(const Smem<C> &sm, const StageArgs
     if (j == 0) {
       sm.eid[s] = gc >= 0 ? e : -1;
       if constexpr (C::MIXED)
-        sm.ref[s] = make_ref<C::PHYSICS, typename C::R>(a.uref + 10 * solve_of(a, gc >= 0 ? e : -1), a.gamma);
+        sm.ref[s] = *reinterpret_cast<const RefState<float> *>(a.uref + kUrefStride * solve_of(a, gc >= 0 ? e : -1) + 10);
     }
   }
   for (int w = tid; w < C::EPB * C::NFACE; w += C::NT) {
@@ -446,62 +446,135 @@ __device__ __forceinline__ void load_modal(typename C::R *dst, const S *src, int
   }
 }
 
-// The same into the padded modal block (rows of L at pitch PL).
+// Row copies: N values of S between memory and registers, as 16-byte
+// vectors when a row is a whole number of them (rows are then 16-byte
+// aligned, as every row of these arrays starts at a multiple of its size).
+template <int N, class S>
+__device__ __forceinline__ void ld_row(const S *p, S (&v)[N]) {
+  if constexpr ((N * sizeof(S)) % 16 == 0) {
+    constexpr int V = 16 / (int)sizeof(S);
+#pragma unroll
+    for (int k = 0; k < N / V; ++k) {
+      const uint4 q = reinterpret_cast<const uint4 *>(p)[k];
+      S t[V];
+      __builtin_memcpy(t, &q, 16);
+#pragma unroll
+      for (int j = 0; j < V; ++j) v[k * V + j] = t[j];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = p[k];
+  }
+}
+template <int N, class S>
+__device__ __forceinline__ void st_row(S *p, const S (&v)[N]) {
+  if constexpr ((N * sizeof(S)) % 16 == 0) {
+    constexpr int V = 16 / (int)sizeof(S);
+#pragma unroll
+    for (int k = 0; k < N / V; ++k) {
+      S t[V];
+#pragma unroll
+      for (int j = 0; j < V; ++j) t[j] = v[k * V + j];
+      uint4 q;
+      __builtin_memcpy(&q, t, 16);
+      reinterpret_cast<uint4 *>(p)[k] = q;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; ++k) p[k] = v[k];
+  }
+}
+
+// The modal register into the padded modal block, a row of L values per
+// thread (row r of the tile lands at r * PL).  Rows of elements past the end
+// get the constant state 1 (their results are discarded).
 template <class C, class S>
 __device__ __forceinline__ void load_modal_pad(typename C::R *dst, const S *src, int e0, int ne, int tid) {
   using T = typename C::R;
-  constexpr int BLK = C::NF * C::LD;
-  for (int w = tid; w < C::EPB * BLK; w += C::NT) {
-    const int s = w / BLK, e = e0 + s;
-    dst[apos<C>(w)] = e < ne ? T(src[(size_t)e0 * BLK + w]) : T(w % C::LD == 0 ? 1.0 : 0.0);
+  constexpr int L = C::L, RPF = C::LD / L, RPS = C::NF * RPF;
+  for (int r = tid; r < C::EPB * RPS; r += C::NT) {
+    const int e = e0 + r / RPS;
+    S v[L];
+    if (e < ne) {
+      ld_row<L>(src + ((size_t)e0 * RPS + r) * L, v);
+    } else {
+#pragma unroll
+      for (int k = 0; k < L; ++k) v[k] = S(k == 0 && r % RPF == 0 ? 1.0 : 0.0);
+    }
+#pragma unroll
+    for (int k = 0; k < L; ++k) dst[r * C::PL + k] = T(v[k]);
   }
 }
 
 // Mixed form: the FP32 working copy of a modal register is the perturbation
 // about the solve's reference state, formed in FP64 (only the constant mode
-// carries the reference: uref[10 s + 5 + n]).
+// carries the reference: row[5 + n] of the solve's reference row).
 template <class C>
 __device__ __forceinline__ void load_modal_pert(float *dst, const double *src, const StageArgs &a, int e0,
                                                 int tid) {
-  constexpr int BLK = C::NF * C::LD;
-  for (int w = tid; w < C::EPB * BLK; w += C::NT) {
-    const int s = w / BLK, e = e0 + s, m = w % C::LD;
-    double x = 0.0;
+  constexpr int L = C::L, RPF = C::LD / L, RPS = C::NF * RPF;
+  for (int r = tid; r < C::EPB * RPS; r += C::NT) {
+    const int s = r / RPS, e = e0 + s;
+    double v[L];
     if (e < a.ne) {
-      x = src[(size_t)e0 * BLK + w];
-      if (m == 0) x -= a.uref[10 * solve_of(a, e) + 5 + (w % BLK) / C::LD];
+      ld_row<L>(src + ((size_t)e0 * RPS + r) * L, v);
+      if (r % RPF == 0) v[0] -= a.uref[kUrefStride * solve_of(a, e) + 5 + (r - s * RPS) / RPF];
+    } else {
+#pragma unroll
+      for (int k = 0; k < L; ++k) v[k] = 0.0;
     }
-    dst[apos<C>(w)] = float(x);
+#pragma unroll
+    for (int k = 0; k < L; ++k) dst[r * C::PL + k] = float(v[k]);
   }
 }
 
+// Traces: global [e][f][n][g] <-> shared face-major [f][slot][n][padded g],
+// a row of G values per thread (a face block holds GF / G rows).
 template <class C, class TT>
 __device__ __forceinline__ void store_traces(const typename C::R *E, TT *T, int e0, int ne, int tid) {
-  constexpr int NF = C::NF, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
-  for (int w = tid; w < EPB * NFACE * NF * GF; w += C::NT) {
-    // global order [e][f][n][g]; smem order [f][slot][n][g]
-    const int s = w / (NFACE * NF * GF), rem = w - s * NFACE * NF * GF;
-    const int f = rem / (NF * GF), ng = rem - f * NF * GF;
+  constexpr int NF = C::NF, GF = C::GF, G = C::G, NFACE = C::NFACE, EPB = C::EPB;
+  constexpr int RPF = GF / G, RPS = NFACE * NF * RPF;
+  for (int r = tid; r < EPB * RPS; r += C::NT) {
+    const int s = r / RPS, rr = r - s * RPS, fn = rr / RPF, g1 = rr - fn * RPF, f = fn / NF, n = fn - f * NF;
     const int e = e0 + s;
-    const int n = ng / GF, g = ng - n * GF;
-    if (e < ne) T[(size_t)e * NFACE * NF * GF + rem] = TT(E[((f * EPB + s) * NF + n) * C::EB + epos<C>(g)]);
+    if (e >= ne) continue;
+    const typename C::R *src = E + ((f * EPB + s) * NF + n) * C::EB + g1 * C::PG;
+    TT v[G];
+#pragma unroll
+    for (int k = 0; k < G; ++k) v[k] = TT(src[k]);
+    st_row<G>(T + (size_t)e * NFACE * NF * GF + rr * G, v);
   }
 }
 
 // The element's own traces, written by the previous stage (or the trace
-// kernel), global [e][f][n][g] -> smem face-major [f][slot][n][g], into
-// padded blocks (PAD) or dense ones.
+// kernel), into padded blocks (PAD) or dense ones [f][slot][n][g].
 template <class C, class TT, bool PAD = true>
 __device__ __forceinline__ void load_own_traces(typename C::R *E, const TT *T, int e0, int ne, int tid) {
   using R = typename C::R;
-  constexpr int NF = C::NF, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
-  for (int w = tid; w < EPB * NFACE * NF * GF; w += C::NT) {
-    const int s = w / (NFACE * NF * GF), rem = w - s * NFACE * NF * GF;
-    const int f = rem / (NF * GF), ng = rem - f * NF * GF;
-    const int e = e0 + s;
-    const int n = ng / GF, g = ng - n * GF;
-    const int at = PAD ? ((f * EPB + s) * NF + n) * C::EB + epos<C>(g) : (f * EPB + s) * NF * GF + ng;
-    E[at] = e < ne ? R(T[(size_t)e * NFACE * NF * GF + rem]) : R(ng < GF ? 1.0 : 0.0);
+  constexpr int NF = C::NF, GF = C::GF, G = C::G, NFACE = C::NFACE, EPB = C::EPB;
+  if constexpr (PAD) {
+    constexpr int RPF = GF / G, RPS = NFACE * NF * RPF;
+    for (int r = tid; r < EPB * RPS; r += C::NT) {
+      const int s = r / RPS, rr = r - s * RPS, fn = rr / RPF, g1 = rr - fn * RPF, f = fn / NF, n = fn - f * NF;
+      const int e = e0 + s;
+      TT v[G];
+      if (e < ne) {
+        ld_row<G>(T + (size_t)e * NFACE * NF * GF + rr * G, v);
+      } else {
+#pragma unroll
+        for (int k = 0; k < G; ++k) v[k] = TT(n == 0 ? 1.0 : 0.0);
+      }
+      R *dst = E + ((f * EPB + s) * NF + n) * C::EB + g1 * C::PG;
+#pragma unroll
+      for (int k = 0; k < G; ++k) dst[k] = R(v[k]);
+    }
+  } else {
+    for (int w = tid; w < EPB * NFACE * NF * GF; w += C::NT) {
+      const int s = w / (NFACE * NF * GF), rem = w - s * NFACE * NF * GF;
+      const int f = rem / (NF * GF), ng = rem - f * NF * GF;
+      const int e = e0 + s;
+      E[(f * EPB + s) * NF * GF + ng] = e < ne ? R(T[(size_t)e * NFACE * NF * GF + rem]) : R(ng < GF ? 1.0 : 0.0);
+    }
   }
 }
 
@@ -519,93 +592,124 @@ __device__ __forceinline__ void stage_tile(const Smem<C> &sm, const StageArgs &a
   face_fluxes<C, PHYS>(sm, a, tid);
   lift<C>(sm, tid);
   forward<C>(sm.D, sm.R, sm.C, sm.B, tid, C::NT);
-  // RK stage update on the modal registers
-  constexpr int BLK = C::NF * C::LD;
-  for (int w = tid; w < C::EPB * BLK; w += C::NT) {
-    const int s = w / BLK, e = e0 + s;
+  // RK stage update on the modal registers, a row of L modes per thread
+  constexpr int L = C::L, RPF = C::LD / L, RPS = C::NF * RPF;
+  for (int r = tid; r < C::EPB * RPS; r += C::NT) {
+    const int s = r / RPS, e = e0 + s;
     if (sm.eid[s] < 0) continue;
-    const size_t gi = (size_t)e0 * BLK + w;
+    const int n = (r - s * RPS) / RPF, m0 = (r % RPF) * L;   // field, first mode of the row
+    const size_t gi = ((size_t)e0 * RPS + r) * L;
     const double dt = a.dts ? a.dts[solve_of(a, e)] : a.dt;   // per-solve step (pools)
+    typename C::R *Ar = sm.A + r * C::PL;
+    const typename C::R *Rr = sm.R + r * L;
     if constexpr (C::MIXED) {
       // FP32 right-hand side and second register, FP64 solution register:
       // Ut = A Ut - dt R in FP32; U = U + B Ut accumulated in FP64.
-      float r = sm.R[w];
-      if (a.Rsub) r = r - float(a.Rsub[gi]);
-      float next;
+      float rr[L];
+#pragma unroll
+      for (int k = 0; k < L; ++k) rr[k] = Rr[k];
+      if (a.Rsub)
+#pragma unroll
+        for (int k = 0; k < L; ++k) rr[k] -= float(a.Rsub[gi + k]);
       if (a.kind == kRHS) {
-        a.A[gi] = r;
-        next = sm.A[apos<C>(w)];
-      } else {
-        float ut = float(a.c0) * a.Utf[gi];
-        ut = fmaf(-float(dt), r, ut);
-        const double u = fma(a.c1, double(ut), a.U[gi]);
-        a.Utf[gi] = ut; a.U[gi] = u;
-        const int m = w % C::LD;
-        next = float(m == 0 ? u - a.uref[10 * solve_of(a, e) + 5 + (w % BLK) / C::LD] : u);
+#pragma unroll
+        for (int k = 0; k < L; ++k) a.A[gi + k] = rr[k];
+        continue;
       }
-      sm.A[apos<C>(w)] = next;
-      continue;
+      float ut[L];
+      double u[L];
+      ld_row<L>(a.Utf + gi, ut);
+      ld_row<L>(a.U + gi, u);
+      const float c0 = float(a.c0), mdt = -float(dt);
+#pragma unroll
+      for (int k = 0; k < L; ++k) {
+        ut[k] = fmaf(mdt, rr[k], c0 * ut[k]);
+        u[k] = fma(a.c1, double(ut[k]), u[k]);
+      }
+      st_row<L>(a.Utf + gi, ut);
+      st_row<L>(a.U + gi, u);
+      const double ref0 = m0 == 0 ? a.uref[kUrefStride * solve_of(a, e) + 5 + n] : 0.0;
+#pragma unroll
+      for (int k = 0; k < L; ++k) Ar[k] = float(k == 0 ? u[k] - ref0 : u[k]);
     } else {
-      const double x = sm.A[apos<C>(w)];
-      double r = sm.R[w];
-      if (a.Rcap) a.Rcap[gi] = r;          // first RHS (shallow-water balance)
-      if (a.Rsub) r = r - a.Rsub[gi];
+      double rr[L];
+#pragma unroll
+      for (int k = 0; k < L; ++k) rr[k] = Rr[k];
+      if (a.Rcap)   // first RHS (shallow-water balance)
+#pragma unroll
+        for (int k = 0; k < L; ++k) a.Rcap[gi + k] = rr[k];
+      if (a.Rsub)
+#pragma unroll
+        for (int k = 0; k < L; ++k) rr[k] -= a.Rsub[gi + k];
       if constexpr (PHYS == DGMX_NS2D || PHYS == DGMX_NS3D) {
-        const int n = (w % BLK) / C::LD, m = w % C::LD;
-        if (n >= 1) r = r - a.Pv[((size_t)e * (C::NF - 1) + (n - 1)) * C::LD + m];
+        if (n >= 1)
+#pragma unroll
+          for (int k = 0; k < L; ++k) rr[k] -= a.Pv[((size_t)e * (C::NF - 1) + (n - 1)) * C::LD + m0 + k];
       }
-      double next;
-      switch (a.kind) {
-        case kLSRK: {
-          double ut = a.c0 * a.Ut[gi];
-          ut = fma(-dt, r, ut);
-          const double u = fma(a.c1, ut, x);
-          a.Ut[gi] = ut; a.U[gi] = u; next = u;
-          break;
+      if (a.kind == kLSRK) {
+        double ut[L], u[L];
+        ld_row<L>(a.Ut + gi, ut);
+#pragma unroll
+        for (int k = 0; k < L; ++k) {
+          ut[k] = fma(-dt, rr[k], a.c0 * ut[k]);
+          u[k] = fma(a.c1, ut[k], Ar[k]);
+          Ar[k] = u[k];
         }
-        case kTVD0: {
-          const double ut = fma(-dt, r, x);
-          a.Ut[gi] = ut; next = ut;
-          break;
-        }
-        case kTVD1: {
-          const double t = fma(-dt, r, x);
-          double ut = a.c1 * t;
-          ut = fma(a.c0, a.U[gi], ut);
-          a.Ut[gi] = ut; next = ut;
-          break;
-        }
-        case kTVD2: {
-          const double t = fma(-dt, r, x);
-          double u = a.c0 * a.U[gi];
-          u = fma(a.c1, t, u);
-          a.U[gi] = u; next = u;
-          break;
-        }
-        case kRK40: {
-          const double ut = fma(a.c0, r, x);
-          a.Ut[gi] = ut; a.A[gi] = a.c1 * r; next = ut;
-          break;
-        }
-        case kRK41: {
-          const double ut = fma(a.c0, r, a.U[gi]);
-          a.A[gi] = fma(a.c1, r, a.A[gi]);
-          a.Ut[gi] = ut; next = ut;
-          break;
-        }
-        case kRHS: {
-          a.A[gi] = r; next = x;
-          break;
-        }
-        default: {  // kRK43
-          const double acc = fma(a.c1, r, a.A[gi]);
-          const double u = fma(a.c0, acc, a.U[gi]);
-          a.U[gi] = u; next = u;
-          break;
-        }
+        st_row<L>(a.Ut + gi, ut);
+        st_row<L>(a.U + gi, u);
+        continue;
       }
-  sm.A[apos<C>(w)] = next;
-    }  }
+#pragma unroll
+      for (int k = 0; k < L; ++k) {
+        const size_t g = gi + k;
+        const double x = Ar[k], q = rr[k];
+        double next;
+        switch (a.kind) {
+          case kTVD0: {
+            const double ut = fma(-dt, q, x);
+            a.Ut[g] = ut; next = ut;
+            break;
+          }
+          case kTVD1: {
+            const double t = fma(-dt, q, x);
+            double ut = a.c1 * t;
+            ut = fma(a.c0, a.U[g], ut);
+            a.Ut[g] = ut; next = ut;
+            break;
+          }
+          case kTVD2: {
+            const double t = fma(-dt, q, x);
+            double u = a.c0 * a.U[g];
+            u = fma(a.c1, t, u);
+            a.U[g] = u; next = u;
+            break;
+          }
+          case kRK40: {
+            const double ut = fma(a.c0, q, x);
+            a.Ut[g] = ut; a.A[g] = a.c1 * q; next = ut;
+            break;
+          }
+          case kRK41: {
+            const double ut = fma(a.c0, q, a.U[g]);
+            a.A[g] = fma(a.c1, q, a.A[g]);
+            a.Ut[g] = ut; next = ut;
+            break;
+          }
+          case kRHS: {
+            a.A[g] = q; next = x;
+            break;
+          }
+          default: {  // kRK43
+            const double acc = fma(a.c1, q, a.A[g]);
+            const double u = fma(a.c0, acc, a.U[g]);
+            a.U[g] = u; next = u;
+            break;
+          }
+        }
+        Ar[k] = next;
+      }
+    }
+  }
   csync<C>();
   modal_traces<C>(sm.A, sm.E, sm.S, sm.B, tid, C::NT);
   store_traces<C>(sm.E, trace_out<C>(a), e0, a.ne, tid);
