@@ -319,12 +319,27 @@ __device__ __forceinline__ bool face_flux(const T *UL, const T *UR, const T *n, 
 //   p' = (g-1)(E' - (m'.ub + m.u')/2),  F'_rho = m',
 //   F'_m = m' ub_d + m u'_d + p' e_d,   F'_E = H' ub_d + H u'_d  (H = E + p);
 // shallow water: p' = phi'(phi_b + phi'/2) for the phi^2/2 pressure.
+// Reciprocal, square root and reciprocal square root of the perturbation
+// fluxes: the hardware approximations in FP32 (a few ulp, well inside the
+// FP32 form's error, which its rounding of U sets), the correctly rounded
+// operations in FP64.
+template <class T> __device__ __forceinline__ T p_rcp(T x) { return T(1) / x; }
+template <> __device__ __forceinline__ float p_rcp<float>(float x) { return __fdividef(1.0f, x); }
+template <class T> __device__ __forceinline__ T p_sqrt(T x) { return sqrt(x); }
+template <> __device__ __forceinline__ float p_sqrt<float>(float x) {
+  float y;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+template <class T> __device__ __forceinline__ T p_rsqrt(T x) { return T(1) / sqrt(x); }
+template <> __device__ __forceinline__ float p_rsqrt<float>(float x) { return rsqrtf(x); }
+
 // F(Ub + d) - F(Ub) in every direction (volume term).
 template <int PHYS, class T>
 __device__ __forceinline__ void volume_flux_pert(const RefState<T> &b, const T *d, T gamma, T (*F)[5]) {
   constexpr bool SW = PHYS == DGMX_SHALLOW;
   constexpr int DIM = (PHYS == DGMX_EULER3D || PHYS == DGMX_NS3D) ? 3 : 2, NF = SW ? 3 : DIM + 2;
-  const T rho = b.r + d[0], ir = T(1.0) / rho;
+  const T rho = b.r + d[0], ir = p_rcp(rho);
   T m[3], up[3];
 #pragma unroll
   for (int i = 0; i < DIM; ++i) { m[i] = b.m[i] + d[1 + i]; up[i] = (d[1 + i] - b.u[i] * d[0]) * ir; }
@@ -356,7 +371,7 @@ __device__ __forceinline__ bool normal_flux_pert(const RefState<T> &b, const T *
   constexpr bool SW = PHYS == DGMX_SHALLOW;
   constexpr int DIM = (PHYS == DGMX_EULER3D || PHYS == DGMX_NS3D) ? 3 : 2, NF = SW ? 3 : DIM + 2;
   rho = b.r + d[0];
-  const T ir = T(1.0) / rho;
+  const T ir = p_rcp(rho);
   T m[3], up[3], ubn = T(0), upn = T(0), mpn = T(0);
 #pragma unroll
   for (int i = 0; i < DIM; ++i) {
@@ -372,7 +387,7 @@ __device__ __forceinline__ bool normal_flux_pert(const RefState<T> &b, const T *
   if constexpr (SW) {
     pp = d[0] * fma(T(0.5), d[0], b.r);
     p = T(0.5) * rho * rho;
-    c = sqrt(rho);
+    c = p_sqrt(rho);
     Hs = T(0);
   } else {
     T s = T(0);
@@ -383,7 +398,7 @@ __device__ __forceinline__ bool normal_flux_pert(const RefState<T> &b, const T *
     const T Hp = d[NF - 1] + pp, H = b.H + Hp;
     Fn[NF - 1] = fma(Hp, ubn, H * upn);
     Hs = H * ir;                                   // total enthalpy per unit mass
-    c = sqrt(gamma * fmax(p, T(0)) * ir);
+    c = p_sqrt(gamma * fmax(p, T(0)) * ir);
   }
   Fn[0] = mpn;
 #pragma unroll
@@ -419,10 +434,10 @@ __device__ __forceinline__ bool face_flux_pert(const RefState<T> &b, const T *dl
         s[0] = n[1]; s[1] = n[2]; s[2] = n[0];
         const T sdn = n[0] * s[0] + n[1] * s[1] + n[2] * s[2];
         s[0] -= sdn * n[0]; s[1] -= sdn * n[1]; s[2] -= sdn * n[2];
-        const T sni = T(1.0) / sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+        const T sni = p_rsqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
         s[0] *= sni; s[1] *= sni; s[2] *= sni;
         t[0] = n[1] * s[2] - s[1] * n[2]; t[1] = n[2] * s[0] - s[2] * n[0]; t[2] = n[0] * s[1] - s[0] * n[1];
-        const T tni = T(1.0) / sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        const T tni = p_rsqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
         t[0] *= tni; t[1] *= tni; t[2] *= tni;
       }
       T vsl = T(0), vsr = T(0), vtl = T(0), vtr = T(0), dms = T(0), dmt = T(0), dmn = T(0);
@@ -432,11 +447,11 @@ __device__ __forceinline__ bool face_flux_pert(const RefState<T> &b, const T *dl
         vtl = fma(vl[i], t[i], vtl); vtr = fma(vr[i], t[i], vtr);
         dmn = fma(dU[1 + i], n[i], dmn); dms = fma(dU[1 + i], s[i], dms); dmt = fma(dU[1 + i], t[i], dmt);
       }
-      const T R = sqrt(rr / rl), iRp1 = T(1.0) / (T(1.0) + R);
+      const T R = p_sqrt(rr * p_rcp(rl)), iRp1 = p_rcp(T(1.0) + R);
       const T u = (ul + R * ur) * iRp1, v = (vsl + R * vsr) * iRp1, w = (vtl + R * vtr) * iRp1;
       const T H = (Hl + R * Hr) * iRp1;
       const T a2 = gm1 * (H - T(0.5) * (u * u + v * v + w * w));
-      const T a = sqrt(a2), ainv = T(1.0) / a, c1inv = a2 / gm1;
+      const T ainv = p_rsqrt(a2), a = a2 * ainv, c1inv = a2 * p_rcp(gm1);
       const T d0 = dU[0], dE = dU[NF - 1];
       T al[5];
       al[2] = dms - v * d0;
