@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -34,6 +35,7 @@ struct GeomClass {
   double nrm[6][3];     // unit normal of face f in the frame of its master side
   double onrm[6][3];    // this element's own outward unit normal of face f
   double jr[6];         // side Jacobian / element Jacobian on this element's side
+  double fr[6][15];     // 3-D: face frame of nrm[f]: s (3), t (3), inverse rows (9)
   int master;           // bit f set: this element owns (is master of) face f
   int pad;
 };
@@ -54,6 +56,29 @@ struct HostMesh {
   std::vector<FaceLink> links;       // ne * nfaces
   std::vector<int> perm;             // concatenated permutations (gf each)
 };
+
+// The face frame of the 3-D fluxes for a unit normal n (src/Euler3d.cpp:
+// 601-650): s from (ny, nz, nx) by Gram-Schmidt, t = n x s, both normalised,
+// and the inverse of the rotation [n; s; t] by cofactors over its
+// determinant.  out: s (3), t (3), then xn yn zn xs ys zs xt yt zt.
+inline void face_frame(const double *n, double *out) {
+  const double nx = n[0], ny = n[1], nz = n[2];
+  double sx = ny, sy = nz, sz = nx;
+  const double sdn = nx * sx + ny * sy + nz * sz;
+  sx -= sdn * nx; sy -= sdn * ny; sz -= sdn * nz;
+  const double sni = 1.0 / std::sqrt(sx * sx + sy * sy + sz * sz);
+  sx *= sni; sy *= sni; sz *= sni;
+  double tx = ny * sz - sy * nz, ty = nz * sx - sz * nx, tz = nx * sy - sx * ny;
+  const double tni = 1.0 / std::sqrt(tx * tx + ty * ty + tz * tz);
+  tx *= tni; ty *= tni; tz *= tni;
+  const double detA = (nx * sy * tz + sx * ty * nz + tx * sz * ny) - (nz * sy * tx + sz * ty * nx + tz * sx * ny);
+  const double id = 1.0 / detA;
+  const double v[15] = {sx, sy, sz, tx, ty, tz,
+                        (sy * tz - sz * ty) * id, -(sx * tz - sz * tx) * id, (sx * ty - sy * tx) * id,
+                        -(ny * tz - nz * ty) * id, (nx * tz - nz * tx) * id, -(nx * ty - ny * tx) * id,
+                        (ny * sz - nz * sy) * id, -(nx * sz - nz * sx) * id, (nx * sy - ny * sx) * id};
+  for (int k = 0; k < 15; ++k) out[k] = v[k];
+}
 
 // Processes a DGM mesh: connectivity masters (src/Field.cpp:3478-3540),
 // orientation flags (src/Field.cpp:416-680), affine geometry

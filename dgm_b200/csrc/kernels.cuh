@@ -147,7 +147,7 @@ __device__ __forceinline__ void volume_flux(const T *U, T gamma, T (*F)[5]) {
 // shallow water: src/Shallow.cpp:380-510.
 template <int PHYS, class T>
 __device__ __forceinline__ bool face_flux(const T *UL, const T *UR, const T *n, T gamma,
-                                          int flux, T *Fh, T *FL, T *FR) {
+                                          int flux, T *Fh, T *FL, T *FR, const double *frame = nullptr) {
   bool ok = true;
   if constexpr (PHYS == DGMX_EULER2D || PHYS == DGMX_NS2D) {
     const T gm1 = gamma - T(1.0);
@@ -203,19 +203,29 @@ __device__ __forceinline__ bool face_flux(const T *UL, const T *UR, const T *n, 
   } else if constexpr (PHYS == DGMX_EULER3D || PHYS == DGMX_NS3D) {
     const T gm1 = gamma - T(1.0);
     const T nx = n[0], ny = n[1], nz = n[2];
-    T sx = ny, sy = nz, sz = nx;
-    const T sdn = nx * sx + ny * sy + nz * sz;
-    sx -= sdn * nx; sy -= sdn * ny; sz -= sdn * nz;
-    const T sni = T(1.0) / sqrt(sx * sx + sy * sy + sz * sz);
-    sx *= sni; sy *= sni; sz *= sni;
-    T tx = ny * sz - sy * nz, ty = nz * sx - sz * nx, tz = nx * sy - sx * ny;
-    const T tni = T(1.0) / sqrt(tx * tx + ty * ty + tz * tz);
-    tx *= tni; ty *= tni; tz *= tni;
-    const T detA = (nx * sy * tz + sx * ty * nz + tx * sz * ny) - (nz * sy * tx + sz * ty * nx + tz * sx * ny);
-    const T id = T(1.0) / detA;
-    const T xn = (sy * tz - sz * ty) * id, yn = -(sx * tz - sz * tx) * id, zn = (sx * ty - sy * tx) * id;
-    const T xs = -(ny * tz - nz * ty) * id, ys = (nx * tz - nz * tx) * id, zs = -(nx * ty - ny * tx) * id;
-    const T xt = (ny * sz - nz * sy) * id, yt = -(nx * sz - nz * sx) * id, zt = (nx * sy - ny * sx) * id;
+    // the face frame: precomputed per geometry class (face_frame), or here
+    T sx, sy, sz, tx, ty, tz, xn, yn, zn, xs, ys, zs, xt, yt, zt;
+    if (frame) {
+      sx = T(frame[0]); sy = T(frame[1]); sz = T(frame[2]);
+      tx = T(frame[3]); ty = T(frame[4]); tz = T(frame[5]);
+      xn = T(frame[6]); yn = T(frame[7]); zn = T(frame[8]);
+      xs = T(frame[9]); ys = T(frame[10]); zs = T(frame[11]);
+      xt = T(frame[12]); yt = T(frame[13]); zt = T(frame[14]);
+    } else {
+      sx = ny; sy = nz; sz = nx;
+      const T sdn = nx * sx + ny * sy + nz * sz;
+      sx -= sdn * nx; sy -= sdn * ny; sz -= sdn * nz;
+      const T sni = T(1.0) / sqrt(sx * sx + sy * sy + sz * sz);
+      sx *= sni; sy *= sni; sz *= sni;
+      tx = ny * sz - sy * nz; ty = nz * sx - sz * nx; tz = nx * sy - sx * ny;
+      const T tni = T(1.0) / sqrt(tx * tx + ty * ty + tz * tz);
+      tx *= tni; ty *= tni; tz *= tni;
+      const T detA = (nx * sy * tz + sx * ty * nz + tx * sz * ny) - (nz * sy * tx + sz * ty * nx + tz * sx * ny);
+      const T id = T(1.0) / detA;
+      xn = (sy * tz - sz * ty) * id; yn = -(sx * tz - sz * tx) * id; zn = (sx * ty - sy * tx) * id;
+      xs = -(ny * tz - nz * ty) * id; ys = (nx * tz - nz * tx) * id; zs = -(nx * ty - ny * tx) * id;
+      xt = (ny * sz - nz * sy) * id; yt = -(nx * sz - nz * sx) * id; zt = (nx * sy - ny * sx) * id;
+    }
     const T rl = UL[0];
     const T rul = UL[1] * nx + UL[2] * ny + UL[3] * nz;
     const T rvl = UL[1] * sx + UL[2] * sy + UL[3] * sz;
@@ -414,7 +424,7 @@ __device__ __forceinline__ bool normal_flux_pert(const RefState<T> &b, const T *
 // face frame in 3-D), its upwind dissipation formed from the state jump.
 template <int PHYS, class T>
 __device__ __forceinline__ bool face_flux_pert(const RefState<T> &b, const T *dl, const T *dr, const T *n,
-                                               T gamma, int flux, T *Dm, T *DF) {
+                                               T gamma, int flux, T *Dm, T *DF, const double *frame = nullptr) {
   constexpr bool SW = PHYS == DGMX_SHALLOW;
   constexpr int DIM = (PHYS == DGMX_EULER3D || PHYS == DGMX_NS3D) ? 3 : 2, NF = SW ? 3 : DIM + 2;
   T FL[5], FR[5], rl, rr, ul, ur, cl, cr, vl[3], vr[3], Hl, Hr;
@@ -430,6 +440,8 @@ __device__ __forceinline__ bool face_flux_pert(const RefState<T> &b, const T *dl
       T s[3], t[3] = {T(0), T(0), T(0)};
       if constexpr (DIM == 2) {
         s[0] = -n[1]; s[1] = n[0]; s[2] = T(0);
+      } else if (frame) {
+        for (int k = 0; k < 3; ++k) { s[k] = T(frame[k]); t[k] = T(frame[3 + k]); }
       } else {
         s[0] = n[1]; s[1] = n[2]; s[2] = n[0];
         const T sdn = n[0] * s[0] + n[1] * s[1] + n[2] * s[2];

@@ -241,6 +241,7 @@ bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::strin
       for (int k = 0; k < 3; ++k) c.nrm[s][k] = n[k];
       for (int k = 0; k < 3; ++k) c.onrm[s][k] = geo[e].nrm[s][k];
       c.jr[s] = geo[e].jr[s];
+      if (dim == 3) face_frame(c.nrm[s], c.fr[s]);
       if (S.master) c.master |= 1 << s;
     }
     std::string key(reinterpret_cast<const char *>(&c), sizeof(c));

@@ -320,13 +320,13 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
     if constexpr (C::MIXED) {
       // traces are perturbations about the solve's reference state
       // (Fh - FL = Dm, FR - Fh = DF - Dm)
-      if (master) ok = face_flux_pert<PHYS, T>(sm.ref[slot], Uo, Un, nm, T(a.gamma), a.flux, Fh, FR);
-      else ok = face_flux_pert<PHYS, T>(sm.ref[slot], Un, Uo, nm, T(a.gamma), a.flux, Fh, FR);
+      if (master) ok = face_flux_pert<PHYS, T>(sm.ref[slot], Uo, Un, nm, T(a.gamma), a.flux, Fh, FR, gc.fr[f]);
+      else ok = face_flux_pert<PHYS, T>(sm.ref[slot], Un, Uo, nm, T(a.gamma), a.flux, Fh, FR, gc.fr[f]);
 #pragma unroll
       for (int n = 0; n < NF; ++n) eo[n * EB] = master ? Fh[n] * jr : (FR[n] - Fh[n]) * jr;
     } else {
-      if (master) ok = face_flux<PHYS, T>(Uo, Un, nm, T(a.gamma), a.flux, Fh, FL, FR);
-      else ok = face_flux<PHYS, T>(Un, Uo, nm, T(a.gamma), a.flux, Fh, FL, FR);
+      if (master) ok = face_flux<PHYS, T>(Uo, Un, nm, T(a.gamma), a.flux, Fh, FL, FR, gc.fr[f]);
+      else ok = face_flux<PHYS, T>(Un, Uo, nm, T(a.gamma), a.flux, Fh, FL, FR, gc.fr[f]);
 #pragma unroll
       for (int n = 0; n < NF; ++n) eo[n * EB] = master ? (Fh[n] - FL[n]) * jr : (FR[n] - Fh[n]) * jr;
     }
