@@ -96,6 +96,8 @@ NS_CASES = [
     ("ns3d-tvd-p2-ragged", 9, 3, (3, 2, 4), 0, 2 * np.pi, 2, 0, "laxfriedrichs", 3, "tgv", 0.002, 3, 0.05, False),
     ("ns3d-rotated-p4", 9, 3, (2, 3, 2), 0, 2 * np.pi, 4, 0, "laxfriedrichs", 14, "tgv", 0.001, 2, 0.01, True),
     ("ns3d-p7", 9, 3, (2, 2, 2), 0, 2 * np.pi, 7, 0, "laxfriedrichs", 14, "tgv", 0.0005, 1, 1.0 / 1600, False),
+    ("ns3d-p7-q=p+1-roe", 9, 3, (2, 2, 2), 0, 2 * np.pi, 7, 8, "roe", 14, "tgv", 0.0005, 1, 1.0 / 1600, False),
+    ("ns3d-p3-q=p+1-ragged", 9, 3, (3, 2, 2), 0, 2 * np.pi, 3, 4, "laxfriedrichs", 4, "tgv", 0.002, 2, 0.02, False),
 ]
 
 
