@@ -484,9 +484,10 @@ def main():
         # tile autotuning is set-up, outside the timed region
         rows, pick = D.autotune(reps=10)
         if args.precision != "both" and args.variant >= 0:
-            D.set_variant(args.variant)
             pick = args.variant
-        tiles[name] = {"elements_per_cta": int(rows[pick][0]), "min_ctas_per_sm": int(rows[pick][1]),
+        _, kind = D.set_variant(pick)
+        tiles[name] = {"variant": pick, "kernel": "stage_pipe_kernel" if kind == 2 else "stage_kernel",
+                       "elements_per_cta": int(rows[pick][0]), "min_ctas_per_sm": int(rows[pick][1]),
                        "threads_per_cta": int(rows[pick][2]), "candidates_us": [round(float(r[3]), 1) for r in rows]}
         doms[name] = D
     streams = {k: torch.cuda.ExternalStream(D.stream(), device=torch.device("cuda", local)) for k, D in doms.items()}
@@ -551,7 +552,7 @@ def main():
         a = BYTES_PER_DOF_STAGE[prec] * dof / stage_s / 1e9
         return {"bound": "hbm", "achieved": a, "peak": peak, "unit": "GB/s", "frac": a / peak,
                 "peak_kind": kind, "traffic": profile_traffic(prof),
-                "kernel": f"stage_kernel<Euler3D, L=4, Q=5, {prec}> (one launch per LSRK stage)",
+                "kernel": f"{tiles[prec]['kernel']}<Euler3D, L=4, Q=5, {prec}> (one launch per LSRK stage)",
                 "algorithmic_bytes_per_launch": BYTES_PER_DOF_STAGE[prec] * dof,
                 "stage_us": 1e6 * stage_s}
 
