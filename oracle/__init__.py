@@ -50,6 +50,8 @@ def lib():
         L.ora_error.argtypes = [P]
         L.ora_set_threads.argtypes = [ctypes.c_int]
         L.ora_set_sw_balance.argtypes = [P, ctypes.c_int]
+        L.ora_set_bc.argtypes = [P, ctypes.c_int, I, D]
+        L.ora_set_hold_bulk.argtypes = [P, ctypes.c_int]
         L.ora_coords.argtypes = [P, D, D, D]
         L.ora_wj.argtypes = [P, D]
         L.ora_set_state.argtypes = [P, D]
@@ -159,6 +161,19 @@ class Problem:
 
     def advance(self, inttype: int, dt: float, nsteps: int) -> int:
         return lib().ora_advance(self.h, inttype, dt, nsteps)
+
+    def set_bc(self, records):
+        """Boundary sides: records of (eid, sid, kind, a, b); kind 1 is the
+        Euler 3-D slip wall, 2 the Navier-Stokes 3-D isothermal wall with
+        a = Tw, b = Eref."""
+        r = np.asarray(records, dtype=np.float64).reshape(-1, 5)
+        esk = np.ascontiguousarray(r[:, :3].astype(np.int32))
+        par = np.ascontiguousarray(r[:, 3:5])
+        if lib().ora_set_bc(self.h, len(r), _ip(esk), _dp(par)) != 0:
+            raise ValueError("oracle: bad boundary record")
+
+    def set_hold_bulk(self, on: bool):
+        lib().ora_set_hold_bulk(self.h, 1 if on else 0)
 
     def set_sw_balance(self, on: bool):
         lib().ora_set_sw_balance(self.h, 1 if on else 0)

@@ -18,6 +18,8 @@ from __future__ import annotations
 import dataclasses
 import re
 
+import json
+
 import numpy as np
 
 
@@ -141,16 +143,72 @@ def box_mesh(dim: int, n, lo, hi, p: int, q: int = 0, periodic: bool = True) -> 
     return Mesh(dim, verts, np.array(con, dtype=np.int32), porder, qorder)
 
 
+def read_bc(path: str):
+    """Boundary sides of a DGM .bc file (src/Field.cpp:4469-4490,
+    src/Boundary.cpp:25-75): a header line, the count, then one
+    `type eid sid` record per side.  Returns [(type, eid, sid)]."""
+    lines = open(path).read().splitlines()
+    i = 0
+    while not lines[i].split() or not lines[i].split()[0].isdigit():
+        i += 1
+    nbc = int(lines[i].split()[0])
+    out = []
+    for line in lines[i + 1:]:
+        t = line.split()
+        if len(t) >= 3:
+            out.append((t[0], int(t[1]), int(t[2])))
+        if len(out) == nbc:
+            break
+    return out
+
+
+def read_bct(path: str) -> dict:
+    """BC type database of a DGM .bct file: `Code Tag { values }` blocks
+    (src/Navier_Stokes3d.cpp:416-455).  Returns {tag: (code, [values])}."""
+    toks = open(path).read().replace("{", " { ").replace("}", " } ").split()
+    out, i = {}, 0
+    while i + 1 < len(toks):
+        code, tag = toks[i], toks[i + 1]
+        i += 2
+        vals = []
+        if i < len(toks) and toks[i] == "{":
+            i += 1
+            while toks[i] != "}":
+                vals.append(float(toks[i]))
+                i += 1
+            i += 1
+        out[tag] = (code.lower(), vals)
+    return out
+
+
 def read_restart(path: str, nfields: int, ne: int, int_bytes: int = 4):
     """Decode a DGM restart file; returns (header lines, list of per-field
     modal arrays concatenated over elements, nModes per element)."""
     raw = open(path, "rb").read()
     pos = 0
     header = []
-    for _ in range(10):
-        nl = raw.index(b"\n", pos)
-        header.append(raw[pos:nl].decode("latin-1"))
-        pos = nl + 1
+    if raw[:1] == b"{":
+        # JSON header (src/Domain.cpp:1368-1466): the object, then the rest
+        # of its closing line; the binary body follows
+        depth, instr = 0, False
+        for i, c in enumerate(raw):
+            if instr:
+                instr = c != ord('"')
+            elif c == ord('"'):
+                instr = True
+            elif c == ord("{"):
+                depth += 1
+            elif c == ord("}"):
+                depth -= 1
+                if depth == 0:
+                    break
+        header = json.loads(raw[:i + 1].decode("latin-1"))
+        pos = raw.index(b"\n", i) + 1
+    else:
+        for _ in range(10):
+            nl = raw.index(b"\n", pos)
+            header.append(raw[pos:nl].decode("latin-1"))
+            pos = nl + 1
     idt = np.int32 if int_bytes == 4 else np.int64
     fields = []
     nmodes = None

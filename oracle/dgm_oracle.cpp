@@ -285,6 +285,7 @@ struct Side {
   int q1 = 0, q2 = 1, qtot = 0;  // Gauss points per direction (q2=1 in 2-D)
   bool master = false;
   int link_e = -1, link_s = -1;
+  int bc = -1;                    // boundary: index of the boundary record / ghost side
   bool flip_a = false, flip_b = false, transp = false;
   size_t off = 0;                 // offset into one field's side storage
   vec nx, ny, nz, J;              // J = surface Jacobian / interior Jacobian
@@ -671,7 +672,26 @@ struct Problem {
   // work fields: interior [nf][ntot] and sides [nf][nstot]
   vec Us_s, Uf_s, Uv_u, Uv_s, Usrc;
   vec U, Ut, R0, R1;               // integrator registers
+  // boundary sides (src/Boundary.cpp:25-75, src/Field.cpp:4426-4460): the
+  // record names the element side, the BC kind and its two parameters; the
+  // ghost side gs[b] is the clone that holds the boundary state
+  struct BCRec { int e, s, kind; double a, b; };
+  std::vector<BCRec> bcs;
+  std::vector<Side> gs;
+  bool hold_bulk = false;          // Channel::holdBulkMassFlow (src/Channel.hpp:116-163)
 };
+
+// BC kinds: the Euler 3-D slip wall (Euler3d::WallBC, src/Euler3d.cpp:875-903)
+// and the Navier-Stokes 3-D isothermal wall (slip-wall state in the inviscid
+// flux, Navier_Stokes3d::Isothermal_WallBC in the viscous terms,
+// src/Navier_Stokes3d.cpp:472-513)
+enum BCKind { BC_SLIP_WALL = 1, BC_ISOTHERMAL_WALL = 2 };
+
+// The side a master side is paired with: the neighbour's side, or for a
+// boundary side its ghost clone (src/Field.cpp:4451).
+static inline const Side &link(const Problem &P, const Side &S) {
+  return S.bc >= 0 ? P.gs[S.bc] : P.el[S.link_e].side[S.link_s];
+}
 
 static void elem_setup(Problem &P, Elem &E) {
   const int Q = E.Q;
@@ -950,6 +970,83 @@ static void lift_all(Problem &P, double *Fbase, int nfirst) {
     }
 }
 
+// Boundary states on the ghost sides from the element sides' traces
+// (Domain::enforce_bc looping BC::apply).  Navier_Stokes3d keeps a second BC
+// database beside the Domain's (src/Navier_Stokes3d.hpp:83): the inviscid
+// flux calls Euler3d::enforce_bc (src/Euler3d.cpp:476), which reads the
+// Domain's database where every "*wall*" code is Euler3d::WallBC
+// (src/Euler3d.cpp:862-866), while the viscous terms call
+// Navier_Stokes3d::enforce_bc (src/Navier_Stokes3d.cpp:192, :457-461) and see
+// the isothermal wall.  So `viscous` selects the database:
+//   slip wall       B = (r, m - (m.n) n, rE - |m|^2/2r + |m_t|^2/2r)
+//                   (src/Euler3d.cpp:875-903)
+//   isothermal wall B = (r, 0, 0, 0, (Eref - 1/2) r Tw)
+//                   (src/Navier_Stokes3d.cpp:472-494; a = Tw, b = Eref)
+static void enforce_bc(Problem &P, bool viscous) {
+  for (size_t b = 0; b < P.bcs.size(); ++b) {
+    const Problem::BCRec &R = P.bcs[b];
+    const Side &S = P.el[R.e].side[R.s];
+    const Side &G = P.gs[b];
+    double *s[5], *g[5];
+    for (int n = 0; n < P.nf; ++n) { s[n] = sfld(P, P.Us_s, n) + S.off; g[n] = sfld(P, P.Us_s, n) + G.off; }
+    for (int i = 0; i < S.qtot; ++i) {
+      if (viscous && R.kind == BC_ISOTHERMAL_WALL) {
+        g[0][i] = s[0][i];
+        g[1][i] = 0.0; g[2][i] = 0.0; g[3][i] = 0.0;
+        g[4][i] = (R.b - 0.5) * g[0][i] * R.a;
+      } else {
+        double up = s[1][i], vp = s[2][i], wp = s[3][i];
+        const double dot = up * S.nx[i] + vp * S.ny[i] + wp * S.nz[i];
+        up = up - dot * S.nx[i]; vp = vp - dot * S.ny[i]; wp = wp - dot * S.nz[i];
+        g[0][i] = s[0][i]; g[1][i] = up; g[2][i] = vp; g[3][i] = wp;
+        g[4][i] = s[4][i] - 0.5 * (s[1][i] * s[1][i] + s[2][i] * s[2][i] + s[3][i] * s[3][i]) / s[0][i] +
+                  0.5 * (g[1][i] * g[1][i] + g[2][i] * g[2][i] + g[3][i] * g[3][i]) / g[0][i];
+      }
+    }
+  }
+}
+
+// Boundary viscous fluxes (Domain::enforce_flux_bc, BC::apply_flux): the
+// isothermal wall mirrors every field, B = -S, so that average_flux('-')
+// returns the element's own viscous flux (src/Navier_Stokes3d.cpp:496-513).
+static void enforce_flux_bc(Problem &P) {
+  for (size_t b = 0; b < P.bcs.size(); ++b) {
+    const Problem::BCRec &R = P.bcs[b];
+    const Side &S = P.el[R.e].side[R.s];
+    const Side &G = P.gs[b];
+    for (int n = 0; n < P.nf; ++n) {
+      const double *s = sfld(P, P.Us_s, n) + S.off;
+      double *g = sfld(P, P.Us_s, n) + G.off;
+      for (int i = 0; i < S.qtot; ++i) g[i] = -s[i];
+    }
+  }
+}
+
+// Channel::holdBulkMassFlow (src/Channel.hpp:116-163): subtract the volume
+// mean of the density, x-momentum and energy rates from every point.
+static void hold_bulk_mass_flow(Problem &P, double *Fb) {
+  double sum[5] = {0, 0, 0, 0, 0}, vol = 0.0;
+  for (int e = 0; e < P.ne; ++e) {
+    const Elem &E = P.el[e];
+    double lvol = 0.0;
+    for (int i = 0; i < E.qtot; ++i) lvol += E.wJ[i];
+    for (int n = 0; n < 5; ++n) {
+      const double *f = Fb + (size_t)n * P.ntot + E.off;
+      double acc = 0.0;
+      for (int i = 0; i < E.qtot; ++i) acc += E.wJ[i] * f[i];
+      sum[n] += acc;
+    }
+    vol += lvol;
+  }
+  const int held[3] = {0, 1, 4};
+  for (int h = 0; h < 3; ++h) {
+    const int n = held[h];
+    const double m = sum[n] / vol;
+    double *f = Fb + (size_t)n * P.ntot;
+    for (size_t i = 0; i < P.ntot; ++i) f[i] -= m;
+  }
+}
+
 // positivity threshold aepsM = eps^(2/3) (src/Constants.hpp:27, :43)
 static const double kAeps = std::pow(2.220446049250313e-16, 0.6666666666666666667);
 static void report_bad(Problem &P) { P.err = 1; }
@@ -964,8 +1061,7 @@ static void euler2d_flux(Problem &P) {
     for (int i = 0; i < 4; ++i) {
       const Side &S = E.side[i];
       if (!S.master) continue;
-      const Elem &ER = P.el[S.link_e];
-      const Side &SR = ER.side[S.link_s];
+      const Side &SR = link(P, S);
       double *sl[4], *sr[4], *fl[4], *fr[4];
       for (int n = 0; n < 4; ++n) {
         sl[n] = sfld(P, P.Us_s, n) + S.off;  sr[n] = sfld(P, P.Us_s, n) + SR.off;
@@ -1136,7 +1232,7 @@ static void euler3d_flux(Problem &P) {
     for (int i = 0; i < 6; ++i) {
       const Side &S = E.side[i];
       if (!S.master) continue;
-      const Side &SR = P.el[S.link_e].side[S.link_s];
+      const Side &SR = link(P, S);
       double *sl[5], *sr[5], *fl[5], *fr[5];
       for (int n = 0; n < 5; ++n) {
         sl[n] = sfld(P, P.Us_s, n) + S.off;  sr[n] = sfld(P, P.Us_s, n) + SR.off;
@@ -1230,7 +1326,7 @@ static void shallow_flux(Problem &P) {
     for (int i = 0; i < 4; ++i) {
       const Side &S = E.side[i];
       if (!S.master) continue;
-      const Side &SR = P.el[S.link_e].side[S.link_s];
+      const Side &SR = link(P, S);
       double *sl[3], *sr[3], *fl[3], *fr[3];
       for (int n = 0; n < 3; ++n) {
         sl[n] = sfld(P, P.Us_s, n) + S.off;  sr[n] = sfld(P, P.Us_s, n) + SR.off;
@@ -1391,7 +1487,7 @@ static void primitive_sides(Problem &P) {
     for (int i = 0; i < E.nsides; ++i) {
       const Side &S = E.side[i];
       if (!S.master) continue;
-      const Side &SR = P.el[S.link_e].side[S.link_s];
+      const Side &SR = link(P, S);
       for (int pass = 0; pass < 2; ++pass) {
         const Side &X = pass == 0 ? S : SR;
         double *r = sfld(P, P.Us_s, 0) + X.off;
@@ -1419,7 +1515,7 @@ static void average_flux(Problem &P, double fact) {
       for (int i = 0; i < E.nsides; ++i) {
         const Side &S = E.side[i];
         if (!S.master) continue;
-        const Side &SR = P.el[S.link_e].side[S.link_s];
+        const Side &SR = link(P, S);
         double *us = sfld(P, P.Us_s, n), *fs = sfld(P, P.Uv_s, n);
         for (int q = 0; q < S.qtot; ++q) {
           const int ql = side_map(P.dim, S, q), qr = side_map(P.dim, SR, q);
@@ -1507,6 +1603,7 @@ static void ns3d_diffusion(Problem &P, const double *Ub, double *Rb) {
   const size_t N = P.ntot;
   const double gPr = P.gamma / P.Pr, muv = P.vis;
   fill_all_sides(P, const_cast<double *>(Ub));
+  if (!P.bcs.empty()) enforce_bc(P, true);
   primitive_sides(P);
   average_flux(P, 1.0);
 #pragma omp parallel for schedule(static)
@@ -1564,6 +1661,7 @@ static void ns3d_diffusion(Problem &P, const double *Ub, double *Rb) {
     for (int i = 0; i < n; ++i) F[4][i] = wk[i] + ux[i];
     gradient_dir(E, uz.data(), wk.data(), 'z'); for (int i = 0; i < n; ++i) F[4][i] = wk[i] + F[4][i];
   }
+  if (!P.bcs.empty()) enforce_flux_bc(P);
   average_flux(P, -1.0);
 #pragma omp parallel for schedule(static)
   for (int k = 0; k < P.ne; ++k)
@@ -1592,6 +1690,7 @@ static void project_all(Problem &P, double *Fb) {
 // src/Navier_Stokes3d.cpp:135-161, src/Shallow.cpp:255-267)
 static void time_derivative(Problem &P, const double *Ub, double *Fb) {
   fill_all_sides(P, const_cast<double *>(Ub));
+  if (!P.bcs.empty()) enforce_bc(P, false);
   switch (P.physics) {
     case EULER2D: case NS2D: euler2d_volume(P, Ub, Fb); euler2d_flux(P); break;
     case EULER3D: case NS3D: euler3d_volume(P, Ub, Fb); euler3d_flux(P); break;
@@ -1601,6 +1700,7 @@ static void time_derivative(Problem &P, const double *Ub, double *Fb) {
   if (P.physics == NS2D) ns2d_diffusion(P, Ub, Fb);
   if (P.physics == NS3D) ns3d_diffusion(P, Ub, Fb);
   project_all(P, Fb);
+  if (P.physics == NS3D && P.hold_bulk) hold_bulk_mass_flow(P, Fb);
   if (P.physics == SHALLOW && P.sw_balance) {
     const size_t M = (size_t)P.nf * P.ntot;
     if (P.sw_first) { P.Usrc.assign(Fb, Fb + M); P.sw_first = false; }
@@ -1688,6 +1788,46 @@ void *ora_create(int dim, int ne, const double *verts, const int *porder,
   }
 }
 void ora_free(void *h) { delete (Problem *)h; }
+// Boundary sides (3-D only): nbc records (element, side, kind) with two
+// parameters each.  A record replaces the side's connectivity link; a
+// linked partner must be named too.  Returns 0, or -1 on a bad record.
+// Call once, before any state is set.
+int ora_set_bc(void *h, int nbc, const int *es_kind, const double *par) {
+  auto *P = (Problem *)h;
+  if (P->dim != 3 || !P->bcs.empty()) return -1;
+  size_t off = P->nstot;
+  for (int b = 0; b < nbc; ++b) {
+    const int e = es_kind[3 * b], s = es_kind[3 * b + 1], kind = es_kind[3 * b + 2];
+    if (e < 0 || e >= P->ne || s < 0 || s >= 6) return -1;
+    if (kind != BC_SLIP_WALL && kind != BC_ISOTHERMAL_WALL) return -1;
+    if (kind == BC_ISOTHERMAL_WALL && P->physics != NS3D) return -1;
+    if (kind == BC_SLIP_WALL && P->physics != EULER3D) return -1;
+    Side &S = P->el[e].side[s];
+    if (S.bc >= 0) return -1;
+    S.master = true; S.bc = b;
+    S.flip_a = S.flip_b = S.transp = false;
+    Side G = S;
+    G.master = false; G.bc = -1; G.off = off; off += S.qtot;
+    P->gs.push_back(G);
+    P->bcs.push_back({e, s, kind, par[2 * b], par[2 * b + 1]});
+  }
+  // a boundary record replaces the side's connectivity link
+  // (src/Field.cpp:4451); its former partner must be a boundary side too
+  for (auto &R : P->bcs) {
+    Side &S = P->el[R.e].side[R.s];
+    if (S.link_e >= 0 && P->el[S.link_e].side[S.link_s].bc < 0) return -1;
+  }
+  for (auto &R : P->bcs) { Side &S = P->el[R.e].side[R.s]; S.link_e = S.link_s = -1; }
+  for (auto &G : P->gs) G.link_e = G.link_s = -1;
+  const size_t nf = P->nf;
+  P->nstot = off;
+  P->Us_s.assign(nf * P->nstot, 0.0); P->Uf_s.assign(nf * P->nstot, 0.0);
+  P->Uv_s.assign(nf * P->nstot, 0.0);
+  return 0;
+}
+// Channel forcing: hold the bulk density, x-momentum and energy (NS 3-D).
+void ora_set_hold_bulk(void *h, int on) { ((Problem *)h)->hold_bulk = on != 0; }
+
 long ora_ntot(void *h) { return (long)((Problem *)h)->ntot; }
 int ora_nfields(void *h) { return ((Problem *)h)->nf; }
 int ora_error(void *h) { return ((Problem *)h)->err; }

@@ -18,6 +18,36 @@ def load_golden(case):
     return mesh, meta, z["modal"]
 
 
+# boundary kinds of the oracle and of the engine (ora_set_bc / dgmx_set_boundary)
+BC_SLIP_WALL, BC_ISOTHERMAL_WALL = 1, 2
+
+
+def bc_records(tags, sides, bct, physics):
+    """(eid, sid, kind, a, b) records from .bc tags and the .bct database:
+    every "*wall*" code is a slip wall for Euler 3-D; for Navier-Stokes 3-D an
+    isothermal_wall block {Tw Eref} is the isothermal wall."""
+    out = []
+    for t, (e, s) in zip(tags, sides):
+        code, vals = bct[t]
+        if physics == 9:
+            assert code == "isothermal_wall", code
+            out.append((int(e), int(s), BC_ISOTHERMAL_WALL, float(vals[0]), float(vals[1])))
+        else:
+            assert "wall" in code, code
+            out.append((int(e), int(s), BC_SLIP_WALL, 0.0, 0.0))
+    return out
+
+
+def load_wall_golden(case):
+    """A golden case with boundary sides: mesh, meta, final modal state,
+    initial modal state and the boundary records."""
+    z = np.load(os.path.join(GOLDEN, case + ".npz"))
+    meta = json.loads(str(z["meta"]))
+    mesh = dgm_io.Mesh(int(z["dim"]), z["verts"], z["con"], z["porder"], z["qorder"])
+    rec = bc_records(meta["bc_tags"], z["bc_sides"], meta["bct"], meta["inp"]["eqntype"])
+    return mesh, meta, z["modal"], z["ic_modal"], rec
+
+
 def golden_ic(meta, x, y, z, nf, gamma=1.4):
     code, toks = meta["ic_code"].lower(), meta["ic_tokens"]
     if code == "acousticpulse":

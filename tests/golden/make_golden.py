@@ -6,10 +6,14 @@ per-element p/q), the .inp parameters, the first initial condition of the .ic
 file, the .tst tolerances and the golden restart's modal coefficients
 (runs/<case>.ref, decoded with oracle.dgm_io.read_restart).
 
-Cases (all affine, periodic, modal Quad/Hex):
+Cases (all affine, modal Quad/Hex):
   vhex    Euler3d, TVD-RK3, p=10, 8 hexes, 1000 steps   (runs/vhex.tst)
   vquad   Navier-Stokes 2-D (mu=0.02), TVD-RK3, p=10     (runs/vquad.tst)
   vortex  Navier-Stokes 2-D (mu=0), RK4, p=5/10 mixed     (runs/vortex.tst)
+  chan    Navier-Stokes 3-D channel (mu=0.01), TVD-RK3, p=3, 512 hexes, 100
+          steps, isothermal walls (runs/chan/chan.{bc,bct}), bulk-flow hold
+          (runs/chan/chan.chn), restart initial condition runs/chan/chan.ini
+          (runs/chan/chan.tst)
 """
 from __future__ import annotations
 
@@ -24,6 +28,7 @@ sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), ".."
 from oracle import dgm_io  # noqa: E402
 
 CASES = ["vhex", "vquad", "vortex"]
+WALL_CASES = ["chan/chan"]
 
 
 def tolerances(tst_path):
@@ -50,6 +55,28 @@ def main(ref_root):
             meta=json.dumps(dict(inp=inp, ic_code=code, ic_tokens=toks, aeps=aeps, reps=reps,
                                  header=header, source="runs/%s.{inp,msh,con,ord,ic,ref,tst}" % case)))
         print(case, mesh.ne, nf, int(nmodes.sum()))
+    for case in WALL_CASES:
+        root = os.path.join(ref_root, "runs", case)
+        name = os.path.basename(case)
+        inp = dgm_io.read_inp(root + ".inp")
+        mesh = dgm_io.read_case(root, inp["p"], inp.get("q", 0))
+        code, toks = dgm_io.parse_ic(root + ".ic")
+        nf = {8: 5, 9: 5}[inp["eqntype"]]
+        _, ic_fields, _ = dgm_io.read_restart(os.path.join(os.path.dirname(root), toks[0]), nf, mesh.ne)
+        header, fields, nmodes = dgm_io.read_restart(root + ".ref", nf, mesh.ne)
+        bcs = dgm_io.read_bc(root + ".bc")
+        bct = dgm_io.read_bct(root + ".bct")
+        aeps, reps = tolerances(root + ".tst")
+        np.savez_compressed(
+            os.path.join(out_dir, name + ".npz"),
+            verts=mesh.verts, con=mesh.con, porder=mesh.porder, qorder=mesh.qorder,
+            dim=mesh.dim, modal=np.stack(fields), nmodes=nmodes, ic_modal=np.stack(ic_fields),
+            bc_sides=np.array([[e, s_] for _, e, s_ in bcs], dtype=np.int32),
+            meta=json.dumps(dict(inp=inp, ic_code=code, ic_tokens=toks, aeps=aeps, reps=reps,
+                                 header=header, bc_tags=[t for t, _, _ in bcs], bct=bct,
+                                 channel=os.path.exists(root + ".chn"),
+                                 source="runs/%s.{inp,msh,con,bc,bct,chn,ic,ini,ref,tst}" % case)))
+        print(name, mesh.ne, nf, int(nmodes.sum()), len(bcs))
 
 
 if __name__ == "__main__":

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import oracle
-from tests.cases import diff_norms, golden_ic, load_golden, passes_dgm_diff
+from tests.cases import diff_norms, golden_ic, load_golden, load_wall_golden, passes_dgm_diff
 
 
 @pytest.mark.parametrize("case", ["vhex", "vquad", "vortex"])
@@ -32,3 +32,41 @@ def test_golden_fixture_shapes():
     for case in ["vhex", "vquad", "vortex"]:
         mesh, meta, modal = load_golden(case)
         assert modal.shape[1] == sum((p + 1) ** mesh.dim for p in mesh.porder)
+
+
+def test_oracle_matches_channel_golden():
+    """runs/chan: Navier-Stokes 3-D channel, 512 hexes at p=3, isothermal
+    walls, bulk-flow hold, restart initial condition, 100 TVD-RK3 steps; the
+    final state passes dgm_diff against chan.ref at the .tst tolerances
+    (aeps 5e-10, reps 1e-8)."""
+    mesh, meta, modal, ic_modal, rec = load_wall_golden("chan")
+    inp = meta["inp"]
+    assert meta["channel"] and len(rec) == 128
+    P = oracle.Problem(mesh, inp["eqntype"], vis=float(inp["vis"]))
+    P.set_bc(rec)
+    P.set_hold_bulk(True)
+    P.set_state(P.backward(ic_modal))
+    assert P.advance(inp["inttype"], float(inp["dt"]), int(inp["Nt"])) == 0
+    U = P.state()
+    norms = diff_norms(U, P.backward(modal), P.wj())
+    assert passes_dgm_diff(norms, meta["aeps"], meta["reps"]), norms
+    assert max(f["linf"] for f in norms) < 1e-10
+
+
+def test_channel_hold_matters():
+    """The bulk-flow hold is not a no-op on this case: 20 steps without it
+    differ from 20 steps with it by more than the golden tolerance."""
+    mesh, meta, modal, ic_modal, rec = load_wall_golden("chan")
+    inp = meta["inp"]
+    P = oracle.Problem(mesh, inp["eqntype"], vis=float(inp["vis"]))
+    P.set_bc(rec)
+    P.set_hold_bulk(False)
+    P.set_state(P.backward(ic_modal))
+    P.advance(inp["inttype"], float(inp["dt"]), 20)
+    Q = oracle.Problem(mesh, inp["eqntype"], vis=float(inp["vis"]))
+    Q.set_bc(rec)
+    Q.set_hold_bulk(True)
+    Q.set_state(Q.backward(ic_modal))
+    Q.advance(inp["inttype"], float(inp["dt"]), 20)
+    d = diff_norms(P.state(), Q.state(), P.wj())
+    assert max(f["linf"] for f in d) > 1e-8
