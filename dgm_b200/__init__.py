@@ -96,12 +96,20 @@ def kernel_list():
     return np.frombuffer(buf, dtype=np.int32)[: 7 * k].reshape(k, 7).copy()
 
 
+# boundary kinds (include/dgmx.h)
+BC_SLIP_WALL, BC_ISOTHERMAL_WALL = 1, 2
+
+
 class Domain:
     """One DGM Domain on one GPU (Field layout [field][element][Q^d])."""
 
     def __init__(self, mesh, physics: int, flux: str = "laxfriedrichs", inttype: int = LSRK14,
                  gamma: float = 1.4, vis: float = 0.0, Pr: float = 0.72, sw_balance: bool = True,
-                 device: int = 0, precision: int = 0):
+                 device: int = 0, precision: int = 0, boundaries=None, bulk_hold: bool = False):
+        """boundaries: optional (element, side, kind, a, b) records
+        (BC_SLIP_WALL for Euler 3-D; BC_ISOTHERMAL_WALL with a = Tw,
+        b = Eref for Navier-Stokes 3-D); bulk_hold: the channel's bulk-flow
+        hold (Navier-Stokes 3-D)."""
         self._keep = []
         verts = np.ascontiguousarray(mesh.verts, dtype=np.float64)
         con = np.ascontiguousarray(mesh.con, dtype=np.int32)
@@ -115,10 +123,22 @@ class Domain:
         p = _Params(physics, FLUX[flux.lower()], inttype, precision, 1 if sw_balance else 0, device,
                     gamma, vis, Pr)
         h = ctypes.c_void_p()
-        st = lib().dgmx_create(ctypes.byref(m), ctypes.byref(p), ctypes.byref(h))
+        if boundaries is None:
+            st = lib().dgmx_create(ctypes.byref(m), ctypes.byref(p), ctypes.byref(h))
+        else:
+            r = np.asarray(boundaries, dtype=np.float64).reshape(-1, 5)
+            sides = np.ascontiguousarray(r[:, :3].astype(np.int32))
+            par = np.ascontiguousarray(r[:, 3:5])
+            f = lib().dgmx_create_with_boundaries
+            f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                          ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+            st = f(ctypes.byref(m), ctypes.byref(p), len(r), sides.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                   _dp(par), ctypes.byref(h))
         if st != 0:
             raise DgmxError(st, lib().dgmx_last_error(None).decode())
         self._init(h, mesh.dim)
+        if bulk_hold:
+            self.set_bulk_hold(True)
 
     @classmethod
     def from_files(cls, root: str, inttype: int = TVD3, physics: int = EULER3D, device: int = 0):
@@ -233,6 +253,12 @@ class Domain:
         nv, ch = ctypes.c_int(), ctypes.c_int()
         self._check(f(self.h, int(reps), _dp(rows), 64, ctypes.byref(nv), ctypes.byref(ch)))
         return rows[: nv.value].copy(), ch.value
+
+    def set_bulk_hold(self, on: bool):
+        """Channel::holdBulkMassFlow after every projected RHS (Navier-Stokes 3-D)."""
+        f = lib().dgmx_set_bulk_hold
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        self._check(f(self.h, 1 if on else 0))
 
     def set_variant(self, index: int):
         """Use compiled tile variant `index`; returns (variant count, kind): kind 0 is a

@@ -57,6 +57,12 @@ struct dgmx_domain {
   GeomClass *classes = nullptr;
   FaceLink *links = nullptr;
   double *host_pinned = nullptr;                         // pinned staging for host I/O
+  // boundary types 1..nbct (kind, two parameters) and the bulk-flow hold
+  int nbct = 0;
+  int bckind[kMaxBcTypes + 1] = {};
+  double bcpar[kMaxBcTypes + 1][2] = {};
+  bool hold = false;
+  double *R0 = nullptr, *cbar = nullptr;                 // hold: [e][n] constant coefficients, [n] means
   int tcur = 0;
   bool sw_captured = false;
   long launches = 0;
@@ -88,7 +94,21 @@ struct dgmx_domain {
     a.err = err;
     a.Ghat = Ghat; a.V = Vtr; a.Pv = Pv;
     a.uref = uref;
+    for (int t = 0; t <= kMaxBcTypes; ++t) {
+      a.bckind[t] = bckind[t];
+      a.bcpar[t][0] = bcpar[t][0]; a.bcpar[t][1] = bcpar[t][1];
+    }
     return a;
+  }
+  // bulk-flow hold after a stage of kind a.kind (hold.cu); Fn: nodal RHS
+  cudaError_t hold_after(const StageArgs &a, double *Tout, double *Fn) {
+    HoldArgs h;
+    h.ne = ne; h.nf = nf; h.ld = ld; h.gf = gf; h.qd = qd; h.nfaces = nfaces;
+    h.R0 = R0; h.J = Jdev; h.cbar = cbar;
+    h.kind = a.kind; h.c0 = a.c0; h.c1 = a.c1; h.dt = a.dt;
+    h.U = a.U; h.Ut = a.Ut; h.A = a.A; h.Tout = Tout; h.Fn = Fn;
+    launches += 2;
+    return launch_hold(h, stream);
   }
   bool ns() const { return prm.physics == DGMX_NS2D || prm.physics == DGMX_NS3D; }
   bool mixed() const { return prm.precision == DGMX_MIXED; }
@@ -98,7 +118,7 @@ struct dgmx_domain {
     if (graph) cudaGraphExecDestroy(graph);
     graph = nullptr;
     void *ptrs[] = {U, Ut, Acc, T[0], T[1], Rsw, nod_in, nod_out, Jdev, integ, gclass, perm, err, classes, links,
-                    Ghat, Vtr, Pv, Utf, Tf[0], Tf[1], uref};
+                    Ghat, Vtr, Pv, Utf, Tf[0], Tf[1], uref, R0, cbar};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (host_pinned) cudaFreeHost(host_pinned);
     if (stream) cudaStreamDestroy(stream);
@@ -106,6 +126,7 @@ struct dgmx_domain {
     Ghat = Vtr = Pv = nullptr;
     Utf = Tf[0] = Tf[1] = nullptr;
     uref = nullptr;
+    R0 = cbar = nullptr;
     T[0] = T[1] = nullptr; gclass = perm = err = nullptr; classes = nullptr; links = nullptr; stream = nullptr;
   }
 };
@@ -128,10 +149,13 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
       if ((e = d->ops->ns_visc(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
       d->launches += 2;
     }
+    a.R0 = d->hold ? d->R0 : nullptr;
     e = d->stage_ops()->stage(a, d->stream);
     if (e != cudaSuccess) return d->cuda(e, "stage kernel launch");
-    d->tcur ^= 1;
     ++d->launches;
+    if (d->hold && (e = d->hold_after(a, d->T[d->tcur ^ 1], nullptr)) != cudaSuccess)
+      return d->cuda(e, "bulk-flow hold");
+    d->tcur ^= 1;
     return DGMX_OK;
   };
   dgmx_status st = DGMX_OK;
@@ -157,7 +181,7 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
 }
 
 int stages_per_step(int inttype) { return inttype == DGMX_LSRK14 ? 14 : (inttype == DGMX_TVD3 ? 3 : 4); }
-int launches_per_stage(const dgmx_domain *d) { return d->ns() ? 3 : 1; }
+int launches_per_stage(const dgmx_domain *d) { return (d->ns() ? 3 : 1) + (d->hold ? 2 : 0); }
 
 // Mixed form: the reference state the FP32 working copies are perturbations
 // about is the domain mean of U (any constant gives the same scheme; the
@@ -228,11 +252,52 @@ dgmx_status reset_error_word(dgmx_domain *d) {
   return d->cuda(cudaMemcpyAsync(d->err, init, sizeof(init), cudaMemcpyHostToDevice, d->stream), "error reset");
 }
 
-dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **out) {
+// Boundary sides and their (kind, parameter) types, and the bulk-flow hold.
+struct BoundarySpec {
+  std::vector<BoundarySide> sides;
+  int ntypes = 0;
+  int kind[kMaxBcTypes + 1] = {};
+  double par[kMaxBcTypes + 1][2] = {};
+  bool hold = false;
+  // type index of (kind, a, b), added on first use; 0 when the table is full
+  int type_of(int k, double a, double b) {
+    if (k == DGMX_BC_SLIP_WALL) a = b = 0.0;
+    for (int t = 1; t <= ntypes; ++t)
+      if (kind[t] == k && par[t][0] == a && par[t][1] == b) return t;
+    if (ntypes == kMaxBcTypes) return 0;
+    ++ntypes;
+    kind[ntypes] = k; par[ntypes][0] = a; par[ntypes][1] = b;
+    return ntypes;
+  }
+};
+
+dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **out,
+                        const BoundarySpec *bspec = nullptr) {
   if (!m || !p || !out) { g_create_error = "null argument"; return DGMX_ERR_ARGUMENT; }
   *out = nullptr;
   auto d = std::make_unique<dgmx_domain>();
   d->prm = *p;
+  if (bspec && !bspec->sides.empty()) {
+    if (p->precision != DGMX_FP64) { g_create_error = "boundary sides are supported in FP64"; return DGMX_ERR_UNSUPPORTED; }
+    for (int t = 1; t <= bspec->ntypes; ++t) {
+      const int k = bspec->kind[t];
+      if (!(k == DGMX_BC_SLIP_WALL && p->physics == DGMX_EULER3D) &&
+          !(k == DGMX_BC_ISOTHERMAL_WALL && p->physics == DGMX_NS3D)) {
+        g_create_error = "boundary kind " + std::to_string(k) +
+                         " is not built for this physics (Euler 3-D: slip wall; Navier-Stokes 3-D: isothermal wall)";
+        return DGMX_ERR_UNSUPPORTED;
+      }
+    }
+    d->nbct = bspec->ntypes;
+    for (int t = 0; t <= kMaxBcTypes; ++t) {
+      d->bckind[t] = bspec->kind[t];
+      d->bcpar[t][0] = bspec->par[t][0]; d->bcpar[t][1] = bspec->par[t][1];
+    }
+  }
+  if (bspec && bspec->hold) {
+    if (p->physics != DGMX_NS3D) { g_create_error = "the bulk-flow hold is a Navier-Stokes 3-D option"; return DGMX_ERR_UNSUPPORTED; }
+    d->hold = true;
+  }
   if (d->prm.gamma <= 0) d->prm.gamma = 1.4;
   if (d->prm.Pr <= 0) d->prm.Pr = 0.72;
   const int phys = p->physics;
@@ -284,7 +349,10 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
   d->qd = d->dim == 2 ? d->Q * d->Q : d->Q * d->Q * d->Q;
   d->tab = make_tables(d->L, d->Q, d->G);
   std::string err;
-  if (!build_mesh(*m, d->tab, d->mesh, err)) { g_create_error = err; return DGMX_ERR_ARGUMENT; }
+  if (!build_mesh(*m, d->tab, d->mesh, err, bspec ? &bspec->sides : nullptr)) {
+    g_create_error = err;
+    return DGMX_ERR_ARGUMENT;
+  }
 
   cudaError_t e = cudaSetDevice(p->device);
   if (e != cudaSuccess) { g_create_error = std::string("cudaSetDevice: ") + cudaGetErrorString(e); return DGMX_ERR_CUDA; }
@@ -313,7 +381,9 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
                              chk(dalloc(&d->uref, (size_t)kUrefStride), "alloc reference state"))) &&
             (!d->ns() || (chk(dalloc(&d->Ghat, (size_t)d->ne * (d->dim + 1) * d->dim * d->ld), "alloc gradients") &&
                           chk(dalloc(&d->Vtr, (size_t)d->ne * d->nfaces * (d->nf - 1) * d->gf), "alloc viscous traces") &&
-                          chk(dalloc(&d->Pv, (size_t)d->ne * (d->nf - 1) * d->ld), "alloc viscous divergence")));
+                          chk(dalloc(&d->Pv, (size_t)d->ne * (d->nf - 1) * d->ld), "alloc viscous divergence"))) &&
+            (!d->ns() || d->dim != 3 || (chk(dalloc(&d->R0, (size_t)d->ne * d->nf), "alloc hold coefficients") &&
+                                          chk(dalloc(&d->cbar, (size_t)d->nf), "alloc hold means")));
   if (ok) {
     ok = chk(cudaMemcpy(d->gclass, d->mesh.gclass.data(), sizeof(int) * d->ne, cudaMemcpyHostToDevice), "upload") &&
          chk(cudaMemcpy(d->classes, d->mesh.classes.data(), sizeof(GeomClass) * d->mesh.classes.size(),
@@ -366,6 +436,41 @@ dgmx_status dgmx_create(const dgmx_mesh *mesh, const dgmx_params *params, dgmx_d
   }
 }
 
+dgmx_status dgmx_create_with_boundaries(const dgmx_mesh *mesh, const dgmx_params *params, int nbc,
+                                        const int *bc_sides, const double *bc_params, dgmx_domain **out) {
+  if (!mesh || !params || !out || nbc < 0 || (nbc > 0 && (!bc_sides || !bc_params))) {
+    g_create_error = "null argument";
+    return DGMX_ERR_ARGUMENT;
+  }
+  try {
+    BoundarySpec b;
+    for (int i = 0; i < nbc; ++i) {
+      const int k = bc_sides[3 * i + 2];
+      if (k != DGMX_BC_SLIP_WALL && k != DGMX_BC_ISOTHERMAL_WALL) {
+        g_create_error = "unknown boundary kind " + std::to_string(k);
+        return DGMX_ERR_ARGUMENT;
+      }
+      const int t = b.type_of(k, bc_params[2 * i], bc_params[2 * i + 1]);
+      if (!t) { g_create_error = "more than 15 distinct boundary types"; return DGMX_ERR_UNSUPPORTED; }
+      b.sides.push_back(BoundarySide{bc_sides[3 * i], bc_sides[3 * i + 1], t});
+    }
+    return create_impl(mesh, params, out, &b);
+  } catch (const std::exception &ex) {
+    g_create_error = ex.what();
+    return DGMX_ERR_ARGUMENT;
+  }
+}
+
+dgmx_status dgmx_set_bulk_hold(dgmx_domain *d, int on) {
+  if (!d) return DGMX_ERR_ARGUMENT;
+  if (on && !d->R0) return d->fail(DGMX_ERR_UNSUPPORTED, "the bulk-flow hold is a Navier-Stokes 3-D option");
+  if (d->hold != (on != 0)) {
+    d->hold = on != 0;
+    if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  }
+  return DGMX_OK;
+}
+
 dgmx_status dgmx_create_from_files(const char *root, const dgmx_params *params, dgmx_domain **out) {
   if (!root || !params || !out) { g_create_error = "null argument"; return DGMX_ERR_ARGUMENT; }
   try {
@@ -383,7 +488,36 @@ dgmx_status dgmx_create_from_files(const char *root, const dgmx_params *params, 
     m.dim = fc.dim; m.ne = fc.ne; m.verts = fc.verts.data();
     m.ncon = (int)(fc.con.size() / 4); m.con = fc.con.data();
     m.porder = fc.porder.data(); m.qorder = fc.qorder.data();
-    return create_impl(&m, &p, out);
+    // boundary sides: root.bc records typed by root.bct blocks; the kind
+    // follows the physics' BC databases (src/Euler3d.cpp:855-870,
+    // src/Navier_Stokes3d.cpp:430-455)
+    BoundarySpec b;
+    b.hold = p.physics == DGMX_NS3D && fc.channel;
+    for (const auto &r : fc.bcs) {
+      auto it = fc.bct.find(r.tag);
+      std::string code;
+      std::vector<double> vals;
+      if (it != fc.bct.end()) { code = it->second.first; vals = it->second.second; }
+      int k = 0;
+      double pa = 0.0, pb = 0.0;
+      if (p.physics == DGMX_EULER3D && code.find("wall") != std::string::npos) {
+        k = DGMX_BC_SLIP_WALL;
+      } else if (p.physics == DGMX_EULER3D && code.empty() && r.tag == "W") {
+        k = DGMX_BC_SLIP_WALL;                 // default "W" (src/Euler3d.cpp:835)
+      } else if (p.physics == DGMX_NS3D && code == "isothermal_wall" && vals.size() >= 2) {
+        k = DGMX_BC_ISOTHERMAL_WALL; pa = vals[0]; pb = vals[1];
+      } else if (p.physics == DGMX_NS3D && code.empty() && r.tag == "W") {
+        k = DGMX_BC_ISOTHERMAL_WALL; pa = 1.0; pb = 20.34126984126985;   // src/Navier_Stokes3d.cpp:403-410
+      } else {
+        g_create_error = std::string(root) + ".bc: boundary type '" + r.tag + "' (" +
+                         (code.empty() ? "no .bct entry" : code) + ") is not built for this physics";
+        return DGMX_ERR_UNSUPPORTED;
+      }
+      const int t = b.type_of(k, pa, pb);
+      if (!t) { g_create_error = "more than 15 distinct boundary types"; return DGMX_ERR_UNSUPPORTED; }
+      b.sides.push_back(BoundarySide{r.e, r.s, t});
+    }
+    return create_impl(&m, &p, out, &b);
   } catch (const std::exception &ex) {
     g_create_error = ex.what();
     return DGMX_ERR_IO;
@@ -546,9 +680,14 @@ dgmx_status dgmx_time_derivative_device(dgmx_domain *d, const double *U_dev, dou
     if ((e = d->ops->ns_visc(a, true, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
     d->launches += 2;
   }
+  a.R0 = d->hold ? d->R0 : nullptr;
   e = d->ops->rhs_nodal(a, d->stream);
   ++d->launches;
   if (e != cudaSuccess) return d->cuda(e, "nodal rhs kernel");
+  if (d->hold) {
+    a.kind = kRHS; a.A = nullptr;
+    if ((e = d->hold_after(a, nullptr, F_dev)) != cudaSuccess) return d->cuda(e, "bulk-flow hold");
+  }
   // the traces of the current modal register live in T[tcur]; T[tcur^1]
   // was used as scratch and is rewritten by the next stage.
   return DGMX_OK;
@@ -685,6 +824,12 @@ dgmx_status dgmx_autotune(dgmx_domain *d, int reps, double *rows, int cap, int *
   dgmx_status st = DGMX_OK;
   for (size_t i = 0; i < vs->size() && st == DGMX_OK; ++i) {
     const KernelOps &v = (*vs)[i];
+    if (d->nbct && v.warp != 0) {   // the prefetching kernel has no boundary sides
+      if ((int)i < cap && rows) {
+        rows[4 * i + 0] = v.epb; rows[4 * i + 1] = v.minb; rows[4 * i + 2] = v.nt; rows[4 * i + 3] = 0.0;
+      }
+      continue;
+    }
     if ((e = v.init(d->tab)) != cudaSuccess) { st = d->cuda(e, "variant init"); break; }
     StageArgs a = d->base_args();
     a.kind = kRHS; a.X = d->U; a.U = d->U; a.Ut = d->Ut; a.A = scratch;
@@ -726,6 +871,10 @@ dgmx_status dgmx_set_variant(dgmx_domain *d, int index, int *count, int *warp) {
   if (count) *count = (int)vs->size();
   if (index < 0 || index >= (int)vs->size()) return d->fail(DGMX_ERR_ARGUMENT, "no such variant");
   const KernelOps &v = (*vs)[index];
+  if (d->nbct && v.warp != 0) {
+    if (warp) *warp = v.warp;
+    return d->fail(DGMX_ERR_UNSUPPORTED, "the prefetching kernel does not handle boundary sides");
+  }
   const cudaError_t e = v.init(d->tab);
   if (e != cudaSuccess) return d->cuda(e, "variant init");
   if (d->mixed()) d->ops_m = &v; else d->ops = &v;

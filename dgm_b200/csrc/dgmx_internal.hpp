@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -37,7 +38,7 @@ struct GeomClass {
   double jr[6];         // side Jacobian / element Jacobian on this element's side
   double fr[6][15];     // 3-D: face frame of nrm[f]: s (3), t (3), inverse rows (9)
   int master;           // bit f set: this element owns (is master of) face f
-  int pad;
+  int bc;               // bits 4f..4f+3: boundary type of face f (0: interior)
 };
 
 struct FaceLink {
@@ -84,7 +85,12 @@ inline void face_frame(const double *n, double *out) {
 // orientation flags (src/Field.cpp:416-680), affine geometry
 // (src/Quad.cpp:1227-1285, src/Hex.cpp:1130-1280) and side geometry
 // (src/Quad.cpp:1367-1455, src/Hex.cpp:1385-1497).
-bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::string &err);
+// A boundary side: element, face and its boundary type (1..kMaxBcTypes,
+// an index into the domain's table of (kind, parameters)).
+struct BoundarySide { int e, s, type; };
+constexpr int kMaxBcTypes = 15;
+bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::string &err,
+                const std::vector<BoundarySide> *bcs = nullptr);
 
 // DGM input files (.inp/.msh/.con/.ord)
 struct FileCase {
@@ -94,6 +100,11 @@ struct FileCase {
   int eqntype = -1, inttype = -1, p = -1, q = 0;
   double gamma = -1, vis = -1, Pr = -1;
   std::string flux;
+  // root.bc records, root.bct blocks (code, values) by tag, root.chn present
+  struct BcRecord { std::string tag; int e, s; };
+  std::vector<BcRecord> bcs;
+  std::map<std::string, std::pair<std::string, std::vector<double>>> bct;
+  bool channel = false;
 };
 bool read_case_files(const std::string &root, FileCase &fc, std::string &err);
 
@@ -199,7 +210,27 @@ struct StageArgs {
   double *Ghat;           // projected primitive gradients, modal [e][comp][dir][L^d]
   double *V;              // viscous normal-flux traces [e][face][field-1][gf]
   double *Pv;             // projected viscous divergence, modal [e][field-1][L^d]
+  // boundary types t = 1..15 (GeomClass::bc): kind (DGMX_BC_*) and parameters
+  int bckind[kMaxBcTypes + 1];
+  double bcpar[kMaxBcTypes + 1][2];
+  // if set, the constant-mode coefficient of every field's final projected
+  // RHS, [e][field] (bulk-flow hold)
+  double *R0;
 };
+
+// Bulk-flow hold (hold.cu): cbar[n] = sum_e J_e R0[e][n] / sum_e J_e for the
+// held fields (density, x-momentum, energy), then the stage kind's linear
+// response to -cbar on the constant coefficients of U / Ut / A, on the next
+// state's traces Tout and, if Fn is set, on the nodal right-hand side.
+struct HoldArgs {
+  int ne, nf, ld, gf, qd, nfaces;
+  const double *R0, *J;
+  double *cbar;
+  int kind;
+  double c0, c1, dt;
+  double *U, *Ut, *A, *Tout, *Fn;
+};
+cudaError_t launch_hold(const HoldArgs &h, cudaStream_t s);
 
 // Registry key offset of the mixed-precision (FP32 working precision) tiles.
 constexpr int kMixedKey = 1000;

@@ -25,6 +25,7 @@ struct SideInfo {
   bool master = false;
   int le = -1, ls = -1;
   bool flip_a = false, flip_b = false, transp = false;
+  int bc = 0;           // boundary type (0: interior side)
 };
 
 // Side point index map with flips and transpose (src/BaseQuad.hpp:53-57,
@@ -54,7 +55,8 @@ double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1]
 
 }  // namespace
 
-bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::string &err) {
+bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::string &err,
+                const std::vector<BoundarySide> *bcs) {
   const int dim = m.dim, ne = m.ne;
   if ((dim != 2 && dim != 3) || ne <= 0 || !m.verts || !m.con || m.ncon <= 0) {
     err = "mesh: dim must be 2 or 3 and verts/con must be given";
@@ -83,10 +85,37 @@ bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::strin
     me.master = true; me.le = le; me.ls = ls;
     nb.master = false; nb.le = e; nb.ls = s;
   }
+  // --- boundary sides (src/Field.cpp:4440-4460): the record replaces the
+  // side's link; the side becomes master with no flips
+  if (bcs && !bcs->empty()) {
+    if (dim != 3) { err = "mesh: boundary sides are supported on Hex meshes"; return false; }
+    for (const BoundarySide &b : *bcs) {
+      if (b.e < 0 || b.e >= ne || b.s < 0 || b.s >= nfaces || b.type < 1 || b.type > kMaxBcTypes) {
+        err = "mesh: boundary record out of range";
+        return false;
+      }
+      SideInfo &S = side[(size_t)b.e * nfaces + b.s];
+      if (S.bc) { err = "mesh: element " + std::to_string(b.e) + " side " + std::to_string(b.s) + " named twice"; return false; }
+      S.bc = b.type;
+    }
+    for (const BoundarySide &b : *bcs) {
+      const SideInfo &S = side[(size_t)b.e * nfaces + b.s];
+      if (S.le >= 0 && !side[(size_t)S.le * nfaces + S.ls].bc) {
+        err = "mesh: boundary side " + std::to_string(b.e) + ":" + std::to_string(b.s) +
+              " is linked to an interior side";
+        return false;
+      }
+    }
+    for (const BoundarySide &b : *bcs) {
+      SideInfo &S = side[(size_t)b.e * nfaces + b.s];
+      S.master = true; S.le = -1; S.ls = -1;
+      S.flip_a = S.flip_b = S.transp = false;
+    }
+  }
   for (size_t i = 0; i < side.size(); ++i)
-    if (side[i].le < 0) {
+    if (side[i].le < 0 && !side[i].bc) {
       err = "mesh: element " + std::to_string(i / nfaces) + " side " + std::to_string(i % nfaces) +
-            " has no neighbour (boundary conditions are not supported by the GPU path)";
+            " has no neighbour and no boundary condition";
       return false;
     }
 
@@ -96,7 +125,7 @@ bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::strin
   for (int e = 0; e < ne; ++e)
     for (int s = 0; s < nfaces; ++s) {
       SideInfo &S = side[(size_t)e * nfaces + s];
-      if (!S.master) continue;
+      if (!S.master || S.bc) continue;
       if (dim == 2) { S.flip_a = kQuadFlip[s][S.ls] != 0; continue; }
       const int *f0 = kHexFace[s], *f1 = kHexFace[S.ls];
       double A[4][3], B[4][3];
@@ -223,7 +252,9 @@ bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::strin
       } else {
         off = it->second;
       }
-      out.links[(size_t)e * nfaces + s] = FaceLink{S.le, S.ls, off, 0};
+      // a boundary side points at itself (identity order); its neighbour
+      // state is made from its own trace
+      out.links[(size_t)e * nfaces + s] = S.bc ? FaceLink{e, s, off, 0} : FaceLink{S.le, S.ls, off, 0};
     }
 
   // --- geometry classes
@@ -238,6 +269,7 @@ bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::strin
     for (int s = 0; s < nfaces; ++s) {
       const SideInfo &S = side[(size_t)e * nfaces + s];
       const double *n = S.master ? geo[e].nrm[s] : geo[S.le].nrm[S.ls];
+      c.bc |= S.bc << (4 * s);
       for (int k = 0; k < 3; ++k) c.nrm[s][k] = n[k];
       for (int k = 0; k < 3; ++k) c.onrm[s][k] = geo[e].nrm[s][k];
       c.jr[s] = geo[e].jr[s];
@@ -350,6 +382,45 @@ bool read_case_files(const std::string &root, FileCase &fc, std::string &err) {
       }
     }
   }
+  // root.bc (optional): a header line, the count, then `type eid sid`
+  // records (src/Field.cpp:4469-4490, src/Boundary.cpp:83-87)
+  {
+    std::ifstream in(root + ".bc");
+    if (in) {
+      std::string line;
+      std::getline(in, line);
+      int nbc = 0;
+      while (std::getline(in, line)) {
+        std::stringstream ls(line);
+        if (ls >> nbc) break;
+      }
+      for (int i = 0; i < nbc; ++i) {
+        FileCase::BcRecord r;
+        if (!(in >> r.tag >> r.e >> r.s)) { err = root + ".bc: short record"; return false; }
+        if (r.e < 0 || r.e >= fc.ne) { err = root + ".bc: bad element id"; return false; }
+        std::getline(in, line);
+        fc.bcs.push_back(r);
+      }
+    }
+  }
+  // root.bct (optional): `Code Tag { values }` blocks
+  // (src/Navier_Stokes3d.cpp:416-455; braces scanned as src/BC.hpp:159)
+  {
+    std::ifstream in(root + ".bct");
+    if (in) {
+      std::string code, tag, tok;
+      while (in >> code >> tag) {
+        std::vector<double> vals;
+        if (in >> tok && tok == "{") {
+          while (in >> tok && tok != "}") vals.push_back(std::stod(tok));
+        }
+        fc.bct[tag] = {lower(code), vals};
+      }
+    }
+  }
+  // root.chn (optional): its presence makes Euler3d build a Channel
+  // (src/Euler3d.cpp:75-77, src/Channel.hpp:40-70)
+  fc.channel = static_cast<bool>(std::ifstream(root + ".chn"));
   return true;
 }
 

@@ -80,10 +80,13 @@ __device__ __forceinline__ void primitive(const double *U, double *q) {
 }
 
 // Gather the neighbour's state traces into face-major smem E2 in the own
-// point order.
+// point order.  A boundary side's neighbour is its ghost state
+// (Navier_Stokes3d::enforce_bc, src/Navier_Stokes3d.cpp:457-461): for the
+// isothermal wall B = (r, 0, 0, 0, (Eref - 1/2) r Tw) from the own trace
+// (src/Navier_Stokes3d.cpp:472-494).
 template <class C>
 __device__ __forceinline__ void load_nbr_traces(double *E2, const double *T, const FaceLink *lnk, const int *eid,
-                                                const int *perm, int tid) {
+                                                const GeomClass *geo, const StageArgs &a, int tid) {
   constexpr int NF = C::NF, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
   for (int w = tid; w < NFACE * EPB * NF * GF; w += C::NT) {
     const int f = w / (EPB * NF * GF), rem = w - f * EPB * NF * GF;
@@ -91,7 +94,13 @@ __device__ __forceinline__ void load_nbr_traces(double *E2, const double *T, con
     double v = n == 0 ? 1.0 : 0.0;
     if (eid[s] >= 0) {
       const FaceLink lk = lnk[s * NFACE + f];
-      v = T[((size_t)(lk.elem * NFACE + lk.face) * NF + n) * GF + perm[lk.perm + g]];
+      const int bt = (geo[s].bc >> (4 * f)) & 15;
+      if (bt && a.bckind[bt] == DGMX_BC_ISOTHERMAL_WALL && n > 0) {
+        const double r = T[((size_t)(lk.elem * NFACE + lk.face) * NF) * GF + a.perm[lk.perm + g]];
+        v = n == NF - 1 ? (a.bcpar[bt][1] - 0.5) * r * a.bcpar[bt][0] : 0.0;
+      } else {
+        v = T[((size_t)(lk.elem * NFACE + lk.face) * NF + n) * GF + a.perm[lk.perm + g]];
+      }
     }
     E2[w] = v;
   }
@@ -220,7 +229,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) ns_grad_kernel(StageArgs a) {
   }
   load_own_traces<C, double, false>(E, a.Tin, e0, a.ne, tid);
   __syncthreads();
-  load_nbr_traces<C>(E2, a.Tin, lnk, eid, a.perm, tid);
+  load_nbr_traces<C>(E2, a.Tin, lnk, eid, geo, a, tid);
   if constexpr (!NODAL) {
     __syncthreads();
     backward_batch<C, NF>(A, B, S1, S2, tid);

@@ -6,8 +6,10 @@
 // Viscosity, Field names, Format "Normalized"), then per field: the global
 // length (int32), the number of modes of every element (int32), their
 // displacements (int32), and the orthonormal modal coefficients (float64,
-// element by element, index c + L*(b + L*a)).  Only this text header is
-// written and read; files with the newer JSON header are refused.
+// element by element, index c + L*(b + L*a)).  This text header is what is
+// written; the reader also takes the newer JSON header (a JSON object, then
+// the rest of its closing line, src/Domain.cpp:1368-1466) with int32 sizes,
+// float64 scalars, little-endian byte order and the normalized basis.
 //
 // Domain::diff (src/Domain.cpp:1000-1066) reads two restart files, takes the
 // Linf / L2 / H1 norms (Field::norm, src/Field.cpp:4675-4697; Hex::norm_*,
@@ -16,6 +18,7 @@
 // relative to the first file's exceeds reps where that norm is above
 // sqrt(machine epsilon).  Everything here runs on the host.
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -59,14 +62,79 @@ struct Header {
   size_t bytes = 0;   // header length
 };
 
+// Value of "key" in a JSON object text (keys are unique in DGM's restart
+// header, nested ones included); strings come back without quotes.
+bool json_value(const std::string &js, const std::string &key, std::string &out) {
+  const std::string q = "\"" + key + "\"";
+  size_t at = 0;
+  while ((at = js.find(q, at)) != std::string::npos) {
+    size_t c = js.find_first_not_of(" \t\r\n", at + q.size());
+    if (c == std::string::npos || js[c] != ':') { at += q.size(); continue; }
+    c = js.find_first_not_of(" \t\r\n", c + 1);
+    if (c == std::string::npos) return false;
+    if (js[c] == '"') {
+      const size_t e = js.find('"', c + 1);
+      if (e == std::string::npos) return false;
+      out = js.substr(c + 1, e - c - 1);
+    } else {
+      const size_t e = js.find_first_of(",}\r\n", c);
+      out = js.substr(c, e == std::string::npos ? std::string::npos : e - c);
+      while (!out.empty() && std::isspace((unsigned char)out.back())) out.pop_back();
+    }
+    return true;
+  }
+  return false;
+}
+
+bool read_json_header(std::ifstream &f, Header &h) {
+  std::string js;
+  int depth = 0;
+  bool instr = false;
+  char c;
+  while (f.get(c)) {
+    js.push_back(c);
+    if (instr) { if (c == '"') instr = false; continue; }
+    if (c == '"') instr = true;
+    else if (c == '{') ++depth;
+    else if (c == '}' && --depth == 0) break;
+  }
+  std::string rest;
+  if (depth != 0 || !std::getline(f, rest)) { g_restart_error = "restart: unterminated JSON header"; return false; }
+  std::string v;
+  auto num = [&](const char *k, double &x, bool need) {
+    if (!json_value(js, k, v)) {
+      if (need) g_restart_error = std::string("restart: JSON header has no \"") + k + "\"";
+      return !need;
+    }
+    x = std::stod(v);
+    return true;
+  };
+  double ne = 0, nsd = 0, lmax = 0, step = 0;
+  if (!num("Nel", ne, true) || !num("Nsd", nsd, true) || !num("Lmax", lmax, true) || !num("Step", step, true) ||
+      !num("Time", h.t, true) || !num("Time step", h.dt, false) || !num("Viscosity", h.vis, false))
+    return false;
+  h.ne = (int)ne; h.nsd = (int)nsd; h.lmax = (int)lmax; h.step = (int)step;
+  std::string basis;
+  if (!json_value(js, "Basis type", basis) || (basis != "Normalized" && basis != "normalized")) {
+    g_restart_error = "restart: only the normalized (orthonormal) basis is supported";
+    return false;
+  }
+  const char *want[][2] = {{"GlobalSize", "int32"}, {"LocalSize", "int32"}, {"Scalar", "float64"},
+                           {"ByteOrder", "LittleEndian"}};
+  for (auto &w : want)
+    if (json_value(js, w[0], v) && v != w[1]) {
+      g_restart_error = std::string("restart: ") + w[0] + " = " + v + " is not supported (" + w[1] + " is)";
+      return false;
+    }
+  h.bytes = (size_t)f.tellg();
+  return true;
+}
+
 bool read_header(std::ifstream &f, Header &h) {
+  if (f.peek() == '{') return read_json_header(f, h);
   std::vector<std::string> lines(10);
   for (auto &l : lines)
     if (!std::getline(f, l)) { g_restart_error = "restart: header is shorter than ten lines"; return false; }
-  if (!lines[0].empty() && lines[0][0] == '{') {
-    g_restart_error = "restart: JSON headers are not supported, only the text header";
-    return false;
-  }
   std::istringstream a(lines[3]);
   if (!(a >> h.ne >> h.nsd >> h.lmax) || lines[3].find("Nel") == std::string::npos) {
     g_restart_error = "restart: malformed 'Nel, Nsd, Lmax' line";

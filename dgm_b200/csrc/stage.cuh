@@ -314,6 +314,21 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
     const T nm[3] = {T(gc.nrm[f][0]), T(gc.nrm[f][1]), T(gc.nrm[f][2])};
 #pragma unroll
     for (int n = 0; n < NF; ++n) { Uo[n] = eo[n * EB]; Un[n] = tn[n * GF]; }
+    const int bt = (gc.bc >> (4 * f)) & 15;
+    if constexpr (C::DIM == 3 && !C::MIXED) {
+      if (bt) {
+        // boundary side: the neighbour is the Domain database's wall state,
+        // Euler3d::WallBC (src/Euler3d.cpp:875-903), for both the Euler slip
+        // wall and the Navier-Stokes isothermal wall (whose inviscid flux
+        // reads the Domain's database, src/Euler3d.cpp:476)
+        T up = Uo[1], vp = Uo[2], wp = Uo[3];
+        const T dot = up * nm[0] + vp * nm[1] + wp * nm[2];
+        up = up - dot * nm[0]; vp = vp - dot * nm[1]; wp = wp - dot * nm[2];
+        Un[0] = Uo[0]; Un[1] = up; Un[2] = vp; Un[3] = wp;
+        Un[4] = Uo[4] - T(0.5) * (Uo[1] * Uo[1] + Uo[2] * Uo[2] + Uo[3] * Uo[3]) / Uo[0] +
+                T(0.5) * (up * up + vp * vp + wp * wp) / Un[0];
+      }
+    }
     const bool master = (gc.master >> f) & 1;
     const T jr = T(gc.jr[f]);
     bool ok;
@@ -334,14 +349,18 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
       // BR1 viscous lift: '-' average of the viscous normal-flux traces in
       // the master frame (src/Domain.cpp:1883-1937), subtracted like
       // scale(-1, Uv); Ur += Uv (src/Navier_Stokes3d.cpp:377-390)
+      // a boundary side's ghost flux is -Vo (isothermal wall apply_flux,
+      // src/Navier_Stokes3d.cpp:496-513), so the average is Vo and the
+      // lift term vanishes
       const double *vo = a.V + ((size_t)(e * NFACE + f) * (NF - 1)) * GF + g;
       const double *vn = a.V + ((size_t)(lk.elem * NFACE + lk.face) * (NF - 1)) * GF + gn;
+      if (!bt)
 #pragma unroll
-      for (int n = 1; n < NF; ++n) {
-        const double Vo = vo[(n - 1) * GF], Vn = vn[(n - 1) * GF];
-        const double fs = master ? 0.5 * (Vo - Vn) : -(0.5 * (Vn - Vo));
-        eo[n * EB] = eo[n * EB] - (fs - Vo) * jr;
-      }
+        for (int n = 1; n < NF; ++n) {
+          const double Vo = vo[(n - 1) * GF], Vn = vn[(n - 1) * GF];
+          const double fs = master ? 0.5 * (Vo - Vn) : -(0.5 * (Vn - Vo));
+          eo[n * EB] = eo[n * EB] - (fs - Vo) * jr;
+        }
     }
     if (!ok) {
       atomicOr(a.err, 1);
@@ -646,6 +665,7 @@ __device__ __forceinline__ void stage_tile(const Smem<C> &sm, const StageArgs &a
 #pragma unroll
           for (int k = 0; k < L; ++k) rr[k] -= a.Pv[((size_t)e * (C::NF - 1) + (n - 1)) * C::LD + m0 + k];
       }
+      if (a.R0 && m0 == 0) a.R0[(size_t)e * C::NF + n] = rr[0];   // bulk-flow hold
       if (a.kind == kLSRK) {
         double ut[L], u[L];
         ld_row<L>(a.Ut + gi, ut);
@@ -838,6 +858,13 @@ __global__ void __launch_bounds__(C::NT, C::MINB) rhs_nodal_kernel(StageArgs a) 
       const size_t gi = (size_t)e0 * BLK + w;
       if (a.Rcap) a.Rcap[gi] = sm.R[w];
       if (a.Rsub) sm.R[w] = sm.R[w] - a.Rsub[gi];
+    }
+    csync<C>();
+  }
+  if (a.R0) {   // bulk-flow hold: constant coefficients of the projected RHS
+    for (int w = tid; w < EPB * NF; w += C::NT) {
+      const int e = e0 + w / NF;
+      if (e < a.ne) a.R0[(size_t)e * NF + w % NF] = sm.R[(w / NF) * NF * C::LD + (w % NF) * C::LD];
     }
     csync<C>();
   }

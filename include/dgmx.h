@@ -43,6 +43,15 @@ enum { DGMX_FLUX_LF = 0, DGMX_FLUX_ROE = 1 };
 enum { DGMX_TVD3 = 3, DGMX_RK4 = 4, DGMX_LSRK14 = 14 };
 /* Arithmetic of the stage kernels. */
 enum { DGMX_FP64 = 0, DGMX_MIXED = 1 };
+/* Boundary kinds (3-D, FP64).  DGMX_BC_SLIP_WALL: Euler 3-D solid wall,
+ * Euler3d::WallBC (src/Euler3d.cpp:862-903).  DGMX_BC_ISOTHERMAL_WALL:
+ * Navier-Stokes 3-D wall with parameters (Tw, Eref); its inviscid flux sees
+ * the slip wall of the Domain's BC database and its viscous terms
+ * Navier_Stokes3d::Isothermal_WallBC (src/Navier_Stokes3d.hpp:25-48,
+ * src/Navier_Stokes3d.cpp:472-513), as in the reference, where
+ * Navier_Stokes3d keeps its own database beside the Domain's
+ * (src/Navier_Stokes3d.hpp:83). */
+enum { DGMX_BC_SLIP_WALL = 1, DGMX_BC_ISOTHERMAL_WALL = 2 };
 
 typedef struct {
   int dim;               /* 2 (Quad) or 3 (Hex)                              */
@@ -76,6 +85,24 @@ dgmx_status dgmx_create(const dgmx_mesh *mesh, const dgmx_params *params, dgmx_d
  * and formats Reo::Problem::setup reads, src/ReoProblem.cpp:48-156).
  * Fields of *params that are not in root.inp keep the caller's values. */
 dgmx_status dgmx_create_from_files(const char *root, const dgmx_params *params, dgmx_domain **out);
+
+/* dgmx_create for a mesh with boundary sides (Field::initialize_bc,
+ * src/Field.cpp:4426-4460, with the records of root.bc read by
+ * src/Field.cpp:4469-4490).  bc_sides holds nbc records (element, side,
+ * kind); bc_params two doubles per record (DGMX_BC_ISOTHERMAL_WALL: Tw,
+ * Eref; ignored for the slip wall).  A record replaces the side's
+ * connectivity link; a linked partner side must be named too.  At most 15
+ * distinct (kind, parameters) pairs; FP64 only; 3-D only.
+ * dgmx_create_from_files reads root.bc and root.bct the same way when they
+ * exist, and switches the bulk-flow hold on when root.chn exists. */
+dgmx_status dgmx_create_with_boundaries(const dgmx_mesh *mesh, const dgmx_params *params, int nbc,
+                                        const int *bc_sides, const double *bc_params, dgmx_domain **out);
+
+/* Navier-Stokes 3-D channel forcing, Channel::holdBulkMassFlow
+ * (src/Channel.hpp:116-163, called from src/Navier_Stokes3d.cpp:160): after
+ * each projected right-hand side, its volume means of density, x-momentum
+ * and energy are subtracted.  on = 0 switches it off. */
+dgmx_status dgmx_set_bulk_hold(dgmx_domain *d, int on);
 
 dgmx_status dgmx_destroy(dgmx_domain *d);
 

@@ -19,6 +19,7 @@ from oracle import dgm_io, ics
 from tests.cases import diff_norms
 
 REF = "/root/reference/runs/vhex.ref"
+CHAN_REF = "/root/reference/runs/chan/chan.ref"
 
 
 def test_reads_the_references_golden_restart():
@@ -31,6 +32,47 @@ def test_reads_the_references_golden_restart():
     assert info["t"] == 1.0 and info["dt"] == 0.001
     assert np.array_equal(nm, g["nmodes"])
     assert np.array_equal(np.stack(fields), g["modal"])
+
+
+def _json_restart(path, modes, step, t, dt, scalar="float64"):
+    """A restart file with the JSON header the reference writes
+    (src/Domain.cpp:1500-1560): the object, a newline, the binary body."""
+    nf, ne, nm = modes.shape
+    hdr = ('{\n   "Basis type" : "Normalized",\n   "Field names" : [ "r", "ru", "rv", "rw", "rE" ],\n'
+           '   "Lmax" : %d,\n   "Nel" : %d,\n   "Nsd" : 3,\n   "Step" : %d,\n   "Time" : %r,\n'
+           '   "Time step" : %r,\n   "Types" : {\n      "ByteOrder" : "LittleEndian",\n'
+           '      "GlobalSize" : "int32",\n      "LocalSize" : "int32",\n      "Scalar" : "%s"\n   }\n}\n'
+           % (nm, ne, step, t, dt, scalar))
+    with open(path, "wb") as f:
+        f.write(hdr.encode())
+        for n in range(nf):
+            f.write(np.int32(ne * nm).tobytes())
+            f.write(np.full(ne, nm, np.int32).tobytes())
+            f.write((np.arange(ne, dtype=np.int32) * nm).tobytes())
+            f.write(modes[n].astype(np.float64).tobytes())
+
+
+def test_reads_json_headers():
+    import dgm_b200
+    rng = np.random.default_rng(7)
+    modes = rng.standard_normal((5, 6, 27))
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "j.rst")
+        _json_restart(path, modes, 40, 0.5, 0.0125)
+        nm, fields, info = dgm_b200.restart_read(path, 5)
+        assert np.array_equal(np.stack(fields).reshape(5, 6, 27), modes)
+        assert info["ne"] == 6 and info["lmax"] == 27 and info["step"] == 40 and info["t"] == 0.5
+        assert info["dt"] == 0.0125
+        header, ofields, _ = dgm_io.read_restart(path, 5, 6)
+        assert header["Step"] == 40 and np.array_equal(np.stack(ofields).reshape(5, 6, 27), modes)
+        bad = os.path.join(d, "f32.rst")
+        _json_restart(bad, modes, 1, 0.0, 0.1, scalar="float32")
+        with pytest.raises(Exception):
+            dgm_b200.restart_read(bad, 5)
+    if os.path.exists(CHAN_REF):
+        g = np.load(os.path.join(os.path.dirname(__file__), "golden", "chan.npz"))
+        nm, fields, info = dgm_b200.restart_read(CHAN_REF, 5)
+        assert info["step"] == 100 and np.array_equal(np.stack(fields), g["modal"])
 
 
 def test_write_then_read_round_trip():
