@@ -358,6 +358,49 @@ def other_configs(dgm_b200, args):
                       "dissipation_rate": (ke[0] - ke[-1]) / (k3 * dt), "dissipation_rate_t0_exact": 0.75 / 1600.0,
                       "note": "FP64 BR1; the 1000-step run and the TF32 contraction form are not timed here"}
     D.close()
+    # the reference's channel regression case (runs/chan: NS 3-D, 512 hexes, p=3,
+    # isothermal walls, bulk-flow hold, TVD3, 100 steps from its restart initial
+    # condition), inputs and golden result from the committed fixture
+    z = np.load(os.path.join(ROOT, "tests", "golden", "chan.npz"))
+    meta = json.loads(str(z["meta"]))
+    inp = meta["inp"]
+    mesh = dgm_b200.meshgen.Mesh(3, z["verts"], z["con"], z["porder"], z["qorder"])
+    tw, eref = meta["bct"][meta["bc_tags"][0]][1][:2]
+    rec = [(int(e), int(s_), dgm_b200.BC_ISOTHERMAL_WALL, tw, eref) for e, s_ in z["bc_sides"]]
+    D = dgm_b200.Domain(mesh, dgm_b200.NS3D, inttype=inp["inttype"], vis=float(inp["vis"]), boundaries=rec,
+                        bulk_hold=True)
+    D.set_modes(z["ic_modal"])
+    D.advance(float(inp["dt"]), 2)
+    D.set_modes(z["ic_modal"])
+    st = torch.cuda.ExternalStream(D.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    D.advance_async(float(inp["dt"]), int(inp["Nt"]))
+    e1.record(st)
+    e1.synchronize()
+    D.sync()
+    t = e0.elapsed_time(e1) / 1e3
+    nsteps = int(inp["Nt"])
+    dof = 5 * mesh.verts.shape[0] * 64
+    chan = {"workload": "runs/chan (NS 3-D channel, 512 hexes, p=3, isothermal walls, bulk-flow hold, TVD3)",
+            "steps": nsteps, "ms_per_step": 1e3 * t / nsteps, "value": dof * 3 * nsteps / t, "unit": UNIT,
+            "max_abs_modal_diff_vs_golden": float(np.abs(D.modes() - z["modal"]).max())}
+    D.close()
+    if not args.no_cpu_baseline:
+        import oracle
+        from oracle import dgm_io
+        oracle.set_threads(os.cpu_count() or 1)
+        P = oracle.Problem(dgm_io.Mesh(3, mesh.verts, mesh.con, mesh.porder, mesh.qorder), oracle.NS3D,
+                           vis=float(inp["vis"]))
+        P.set_bc(rec)
+        P.set_hold_bulk(True)
+        P.set_state(P.backward(z["ic_modal"]))
+        t0 = time.perf_counter()
+        P.advance(3, float(inp["dt"]), nsteps)
+        tc = time.perf_counter() - t0
+        chan["cpu_oracle_ms_per_step"] = 1e3 * tc / nsteps
+        chan["cpu_oracle_cores"] = os.cpu_count() or 1
+    res["channel"] = chan
     return res
 
 

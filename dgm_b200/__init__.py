@@ -141,6 +141,46 @@ class Domain:
             self.set_bulk_hold(True)
 
     @classmethod
+    def partition(cls, mesh, physics: int, part, nranks: int, rank: int, flux: str = "laxfriedrichs",
+                  inttype: int = LSRK14, gamma: float = 1.4, vis: float = 0.0, Pr: float = 0.72,
+                  sw_balance: bool = True, device: int = 0):
+        """The rank's part of an element partition (part[e] = owning rank);
+        its arrays cover its own elements in increasing global order.  Call
+        set_exchange_nccl on every rank before stepping."""
+        m, keep = _mesh_struct(mesh)
+        part = np.ascontiguousarray(part, dtype=np.int32)
+        p = _Params(physics, FLUX[flux.lower()], inttype, 0, 1 if sw_balance else 0, device, gamma, vis, Pr)
+        h = ctypes.c_void_p()
+        f = lib().dgmx_create_partition
+        f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+                      ctypes.c_void_p]
+        st = f(ctypes.byref(m), ctypes.byref(p), part.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), int(nranks),
+               int(rank), ctypes.byref(h))
+        if st != 0:
+            raise DgmxError(st, lib().dgmx_last_error(None).decode())
+        self = cls.__new__(cls)
+        self._keep = keep + [part]
+        self._init(h, mesh.dim)
+        return self
+
+    def set_exchange_nccl(self, nccl_id: bytes):
+        """NCCL communicator for the halo exchange (collective over the ranks)."""
+        f = lib().dgmx_set_exchange_nccl
+        f.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        self._check(f(self.h, bytes(nccl_id)))
+
+    def partition_info(self):
+        """(local element count, ghost slots, global id of every local element)."""
+        ne, ng = ctypes.c_int(), ctypes.c_int()
+        f = lib().dgmx_partition_info
+        f.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                      ctypes.POINTER(ctypes.c_int)]
+        self._check(f(self.h, ctypes.byref(ne), ctypes.byref(ng), None))
+        g = np.zeros(ne.value, dtype=np.int32)
+        self._check(f(self.h, None, None, g.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        return ne.value, ng.value, g
+
+    @classmethod
     def from_files(cls, root: str, inttype: int = TVD3, physics: int = EULER3D, device: int = 0):
         """Domain from DGM input files root.inp/.msh/.con/.ord."""
         p = _Params(physics, 0, inttype, 0, 1, device, 1.4, 0.0, 0.72)
@@ -402,6 +442,110 @@ def _pool_lib():
         L.dgmx_pool_last_error.restype = ctypes.c_char_p
         L._pool_ready = True
     return L
+
+
+def _mesh_struct(mesh):
+    verts = np.ascontiguousarray(mesh.verts, dtype=np.float64)
+    con = np.ascontiguousarray(mesh.con, dtype=np.int32)
+    por = np.ascontiguousarray(mesh.porder, dtype=np.int32)
+    qor = np.ascontiguousarray(mesh.qorder, dtype=np.int32)
+    m = _Mesh(int(mesh.dim), int(verts.shape[0]), _dp(verts), int(con.shape[0]),
+              con.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+              por.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+              qor.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    return m, [verts, con, por, qor]
+
+
+def nccl_unique_id() -> bytes:
+    """A fresh NCCL unique id (rank 0 makes it and shares it with the others)."""
+    buf = ctypes.create_string_buffer(128)
+    f = lib().dgmx_nccl_unique_id
+    f.argtypes = [ctypes.c_char_p]
+    st = f(buf)
+    if st != 0:
+        raise DgmxError(st, lib().dgmx_last_error(None).decode())
+    return buf.raw
+
+
+def partition_plan(mesh, part, nranks: int, rank: int) -> dict:
+    """Host-only partition plan of one rank: local and ghost element ids, the
+    per-peer block counts and the send / receive block lists."""
+    m, keep = _mesh_struct(mesh)
+    part = np.ascontiguousarray(part, dtype=np.int32)
+    P = ctypes.POINTER(ctypes.c_int)
+    f = lib().dgmx_partition_plan
+    f.argtypes = [ctypes.c_void_p, P, ctypes.c_int, ctypes.c_int, P, P, P, P, P, P]
+    sizes = np.zeros(3, dtype=np.int32)
+    ip = lambda a: a.ctypes.data_as(P)
+    st = f(ctypes.byref(m), ip(part), int(nranks), int(rank), ip(sizes), None, None, None, None, None)
+    if st != 0:
+        raise DgmxError(st, lib().dgmx_last_error(None).decode())
+    gl, gg = np.zeros(sizes[0], np.int32), np.zeros(sizes[1], np.int32)
+    cnt = np.zeros(nranks, np.int32)
+    snd, rcv = np.zeros(sizes[2], np.int32), np.zeros(sizes[2], np.int32)
+    st = f(ctypes.byref(m), ip(part), int(nranks), int(rank), ip(sizes), ip(gl), ip(gg), ip(cnt), ip(snd), ip(rcv))
+    if st != 0:
+        raise DgmxError(st, lib().dgmx_last_error(None).decode())
+    return {"global_of_local": gl, "global_of_ghost": gg, "peer_counts": cnt, "send": snd, "recv": rcv}
+
+
+class Group:
+    """Every part of an element partition as a handle on one device, stepped
+    in lockstep with the halo exchange done by device copies.  State arrays
+    are global (Field layout over all elements)."""
+
+    def __init__(self, mesh, physics: int, part, flux: str = "laxfriedrichs", inttype: int = LSRK14,
+                 gamma: float = 1.4, vis: float = 0.0, Pr: float = 0.72, device: int = 0):
+        m, self._keep = _mesh_struct(mesh)
+        part = np.ascontiguousarray(part, dtype=np.int32)
+        self._keep.append(part)
+        self.nparts = int(part.max()) + 1
+        p = _Params(physics, FLUX[flux.lower()], inttype, 0, 0, device, gamma, vis, Pr)
+        L = lib()
+        L.dgmx_group_create.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                        ctypes.c_void_p]
+        L.dgmx_group_last_error.restype = ctypes.c_char_p
+        L.dgmx_group_last_error.argtypes = [ctypes.c_void_p]
+        for n in ("dgmx_group_set_state", "dgmx_group_get_state"):
+            getattr(L, n).argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        L.dgmx_group_advance.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        L.dgmx_group_destroy.argtypes = [ctypes.c_void_p]
+        h = ctypes.c_void_p()
+        st = L.dgmx_group_create(ctypes.byref(m), ctypes.byref(p), part.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                 self.nparts, ctypes.byref(h))
+        if st != 0:
+            raise DgmxError(st, L.dgmx_group_last_error(None).decode())
+        self.h = h
+        self.nf = 3 if physics == SHALLOW else (5 if physics in (EULER3D, NS3D) else 4)
+        q = int(mesh.qorder[0]) or int(mesh.porder[0]) + 2
+        self.nq = int(mesh.verts.shape[0]) * q ** int(mesh.dim)
+
+    def _check(self, st):
+        if st != 0:
+            raise DgmxError(st, lib().dgmx_group_last_error(self.h).decode())
+
+    def set_state(self, U):
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(self.nf, self.nq)
+        self._check(lib().dgmx_group_set_state(self.h, _dp(U)))
+
+    def state(self):
+        U = np.zeros((self.nf, self.nq))
+        self._check(lib().dgmx_group_get_state(self.h, _dp(U)))
+        return U
+
+    def advance(self, dt: float, nsteps: int = 1):
+        self._check(lib().dgmx_group_advance(self.h, float(dt), int(nsteps)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dgmx_group_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class PoolFull(DgmxError):

@@ -2,6 +2,10 @@
 // buffers, and the integrator stage sequences replayed from CUDA graphs.
 #include <cuda_runtime.h>
 
+#include <dlfcn.h>
+#include <nccl.h>
+
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -25,6 +29,45 @@ const double kRk4B[4] = {0.16666666666666667, 0.33333333333333333, 0.33333333333
 template <class T>
 cudaError_t dalloc(T **p, size_t n) {
   return cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * (n ? n : 1));
+}
+
+// NCCL entry points, resolved at first use from the libnccl.so.2 the process
+// already has (PyTorch loads one) or finds on the library path, so the
+// library has no link-time dependency on NCCL.
+struct NcclApi {
+  bool ok = false;
+  std::string why;
+  ncclResult_t (*GetUniqueId)(ncclUniqueId *) = nullptr;
+  ncclResult_t (*CommInitRank)(ncclComm_t *, int, ncclUniqueId, int) = nullptr;
+  ncclResult_t (*CommDestroy)(ncclComm_t) = nullptr;
+  ncclResult_t (*GroupStart)() = nullptr;
+  ncclResult_t (*GroupEnd)() = nullptr;
+  ncclResult_t (*Send)(const void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
+  ncclResult_t (*Recv)(void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
+  const char *(*GetErrorString)(ncclResult_t) = nullptr;
+};
+const NcclApi &nccl_api() {
+  static NcclApi api = [] {
+    NcclApi a;
+    void *h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_NOLOAD);
+    if (!h) h = dlopen("libnccl.so.2", RTLD_NOW);
+    if (!h) h = dlopen("libnccl.so", RTLD_NOW);
+    if (!h) { a.why = "libnccl.so.2 not found"; return a; }
+    auto sym = [&](const char *n) { return dlsym(h, n); };
+    a.GetUniqueId = reinterpret_cast<decltype(a.GetUniqueId)>(sym("ncclGetUniqueId"));
+    a.CommInitRank = reinterpret_cast<decltype(a.CommInitRank)>(sym("ncclCommInitRank"));
+    a.CommDestroy = reinterpret_cast<decltype(a.CommDestroy)>(sym("ncclCommDestroy"));
+    a.GroupStart = reinterpret_cast<decltype(a.GroupStart)>(sym("ncclGroupStart"));
+    a.GroupEnd = reinterpret_cast<decltype(a.GroupEnd)>(sym("ncclGroupEnd"));
+    a.Send = reinterpret_cast<decltype(a.Send)>(sym("ncclSend"));
+    a.Recv = reinterpret_cast<decltype(a.Recv)>(sym("ncclRecv"));
+    a.GetErrorString = reinterpret_cast<decltype(a.GetErrorString)>(sym("ncclGetErrorString"));
+    a.ok = a.GetUniqueId && a.CommInitRank && a.CommDestroy && a.GroupStart && a.GroupEnd && a.Send && a.Recv &&
+           a.GetErrorString;
+    if (!a.ok) a.why = "libnccl.so.2 lacks a needed symbol";
+    return a;
+  }();
+  return api;
 }
 
 // true if p is page-locked host memory the copy engines can read directly
@@ -63,6 +106,16 @@ struct dgmx_domain {
   double bcpar[kMaxBcTypes + 1][2] = {};
   bool hold = false;
   double *R0 = nullptr, *cbar = nullptr;                 // hold: [e][n] constant coefficients, [n] means
+  // element partition: ghost slots in the trace buffers and the halo
+  // exchange lists (plan.nranks == 1: the whole mesh, no exchange)
+  PartitionPlan plan;
+  int nslot = 0;                                         // ne + ghost slots
+  int *x_send = nullptr, *x_recv = nullptr;              // concatenated block lists (device)
+  std::vector<int> x_cnt, x_off;                         // per peer block counts and offsets
+  int x_total = 0;
+  double *x_sbuf = nullptr, *x_rbuf = nullptr;           // nf*gf doubles per block
+  ncclComm_t nccl = nullptr;                             // multi-rank transport
+  bool in_group = false;                                 // in-process partitions: the group exchanges
   int tcur = 0;
   bool sw_captured = false;
   long launches = 0;
@@ -74,7 +127,8 @@ struct dgmx_domain {
 
   size_t nmodal() const { return (size_t)ne * nf * ld; }
   size_t nnodal() const { return (size_t)ne * nf * qd; }
-  size_t ntrace() const { return (size_t)ne * nfaces * nf * gf; }
+  size_t ntrace() const { return (size_t)nslot * nfaces * nf * gf; }
+  bool partitioned() const { return plan.nranks > 1; }
 
   dgmx_status fail(dgmx_status s, const std::string &m) {
     errmsg = m;
@@ -118,70 +172,119 @@ struct dgmx_domain {
     if (graph) cudaGraphExecDestroy(graph);
     graph = nullptr;
     void *ptrs[] = {U, Ut, Acc, T[0], T[1], Rsw, nod_in, nod_out, Jdev, integ, gclass, perm, err, classes, links,
-                    Ghat, Vtr, Pv, Utf, Tf[0], Tf[1], uref, R0, cbar};
+                    Ghat, Vtr, Pv, Utf, Tf[0], Tf[1], uref, R0, cbar, x_send, x_recv, x_sbuf, x_rbuf};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (host_pinned) cudaFreeHost(host_pinned);
+    if (nccl && nccl_api().ok) nccl_api().CommDestroy(nccl);
+    nccl = nullptr;
     if (stream) cudaStreamDestroy(stream);
     U = Ut = Acc = Rsw = nod_in = nod_out = Jdev = integ = host_pinned = nullptr;
     Ghat = Vtr = Pv = nullptr;
     Utf = Tf[0] = Tf[1] = nullptr;
     uref = nullptr;
     R0 = cbar = nullptr;
+    x_send = x_recv = nullptr; x_sbuf = x_rbuf = nullptr;
     T[0] = T[1] = nullptr; gclass = perm = err = nullptr; classes = nullptr; links = nullptr; stream = nullptr;
   }
 };
 
 namespace {
 
-// enqueue the stages of one time step on d->stream
-dgmx_status enqueue_step(dgmx_domain *d, double dt) {
+// Halo exchange of one trace buffer (blk doubles per face block) between the
+// ranks of a partitioned domain over NCCL: pack, grouped send/receive with
+// every peer, unpack into the ghost slots.  A no-op when the domain is not
+// partitioned or belongs to an in-process group (the group exchanges).
+dgmx_status exchange(dgmx_domain *d, double *T, int blk) {
+  if (!d->partitioned() || d->in_group) return DGMX_OK;
+  if (!d->nccl) return d->fail(DGMX_ERR_ARGUMENT, "partitioned domain without an exchange (dgmx_set_exchange_nccl)");
+  cudaError_t e = launch_pack(T, d->x_send, d->x_total, blk, d->x_sbuf, d->stream);
+  if (e != cudaSuccess) return d->cuda(e, "halo pack");
+  const NcclApi &nc = nccl_api();
+  ncclResult_t r = nc.GroupStart();
+  for (int q = 0; q < d->plan.nranks && r == ncclSuccess; ++q) {
+    if (!d->x_cnt[q]) continue;
+    const size_t off = (size_t)d->x_off[q] * blk, n = (size_t)d->x_cnt[q] * blk;
+    r = nc.Send(d->x_sbuf + off, n, ncclFloat64, q, d->nccl, d->stream);
+    if (r == ncclSuccess) r = nc.Recv(d->x_rbuf + off, n, ncclFloat64, q, d->nccl, d->stream);
+  }
+  const ncclResult_t r2 = nc.GroupEnd();
+  if (r == ncclSuccess) r = r2;
+  if (r != ncclSuccess) return d->fail(DGMX_ERR_CUDA, std::string("halo exchange: ") + nc.GetErrorString(r));
+  e = launch_unpack(d->x_rbuf, d->x_recv, d->x_total, blk, T, d->stream);
+  d->launches += 2;
+  return d->cuda(e, "halo unpack");
+}
+
+// The stages of one step: kind, whether the RHS is evaluated on Ut (else U)
+// and the two stage coefficients.
+struct StageSpec { int kind; bool on_ut; double c0, c1; };
+std::vector<StageSpec> stage_specs(int inttype, double dt) {
+  std::vector<StageSpec> v;
+  switch (inttype) {
+    case DGMX_LSRK14:
+      for (int s = 0; s < 14; ++s) v.push_back({kLSRK, false, kLsrkA[s], kLsrkB[s]});
+      break;
+    case DGMX_TVD3:
+      v.push_back({kTVD0, false, 0.0, 0.0});
+      v.push_back({kTVD1, true, kTvdA[1], kTvdB[1]});
+      v.push_back({kTVD2, true, kTvdA[2], kTvdB[2]});
+      break;
+    case DGMX_RK4:
+      v.push_back({kRK40, false, -kRk4A[0] * dt, -kRk4B[0]});
+      v.push_back({kRK41, true, -kRk4A[1] * dt, -kRk4B[1]});
+      v.push_back({kRK41, true, -kRk4A[2] * dt, -kRk4B[2]});
+      v.push_back({kRK43, true, dt, -kRk4B[3]});
+      break;
+    default:
+      break;
+  }
+  return v;
+}
+
+// Arguments of one stage of d (traces T[tcur] in, T[tcur^1] out).
+StageArgs stage_args(const dgmx_domain *d, const StageSpec &sp, double dt) {
   StageArgs a = d->base_args();
   a.dt = dt;
   a.U = d->U; a.Ut = d->Ut; a.A = d->Acc;
   if (d->prm.physics == DGMX_SHALLOW && d->prm.sw_balance) a.Rsub = d->Rsw;
-  auto run = [&](int kind, const double *X, double c0, double c1) -> dgmx_status {
-    a.kind = kind; a.X = X; a.c0 = c0; a.c1 = c1;
-    a.Tin = d->T[d->tcur]; a.Tout = d->T[d->tcur ^ 1];
-    if (d->mixed()) { a.Utf = d->Utf; a.Tinf = d->Tf[d->tcur]; a.Toutf = d->Tf[d->tcur ^ 1]; }
+  a.kind = sp.kind; a.X = sp.on_ut ? d->Ut : d->U; a.c0 = sp.c0; a.c1 = sp.c1;
+  a.Tin = d->T[d->tcur]; a.Tout = d->T[d->tcur ^ 1];
+  if (d->mixed()) { a.Utf = d->Utf; a.Tinf = d->Tf[d->tcur]; a.Toutf = d->Tf[d->tcur ^ 1]; }
+  a.R0 = d->hold ? d->R0 : nullptr;
+  return a;
+}
+
+// enqueue the stages of one time step on d->stream
+dgmx_status enqueue_step(dgmx_domain *d, double dt) {
+  const std::vector<StageSpec> specs = stage_specs(d->prm.inttype, dt);
+  if (specs.empty()) return d->fail(DGMX_ERR_UNSUPPORTED, "inttype must be 3, 4 or 14");
+  for (const StageSpec &sp : specs) {
+    const StageArgs a = stage_args(d, sp, dt);
     cudaError_t e;
     if (d->ns()) {
       if ((e = d->ops->ns_grad(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous gradient kernel");
       if ((e = d->ops->ns_visc(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
       d->launches += 2;
+      dgmx_status xs = exchange(d, d->Vtr, (d->nf - 1) * d->gf);
+      if (xs != DGMX_OK) return xs;
     }
-    a.R0 = d->hold ? d->R0 : nullptr;
     e = d->stage_ops()->stage(a, d->stream);
     if (e != cudaSuccess) return d->cuda(e, "stage kernel launch");
     ++d->launches;
     if (d->hold && (e = d->hold_after(a, d->T[d->tcur ^ 1], nullptr)) != cudaSuccess)
       return d->cuda(e, "bulk-flow hold");
+    dgmx_status xs = exchange(d, d->T[d->tcur ^ 1], d->nf * d->gf);
+    if (xs != DGMX_OK) return xs;
     d->tcur ^= 1;
-    return DGMX_OK;
-  };
-  dgmx_status st = DGMX_OK;
-  switch (d->prm.inttype) {
-    case DGMX_LSRK14:
-      for (int s = 0; s < 14 && st == DGMX_OK; ++s) st = run(kLSRK, d->U, kLsrkA[s], kLsrkB[s]);
-      break;
-    case DGMX_TVD3:
-      st = run(kTVD0, d->U, 0.0, 0.0);
-      if (st == DGMX_OK) st = run(kTVD1, d->Ut, kTvdA[1], kTvdB[1]);
-      if (st == DGMX_OK) st = run(kTVD2, d->Ut, kTvdA[2], kTvdB[2]);
-      break;
-    case DGMX_RK4:
-      st = run(kRK40, d->U, -kRk4A[0] * dt, -kRk4B[0]);
-      if (st == DGMX_OK) st = run(kRK41, d->Ut, -kRk4A[1] * dt, -kRk4B[1]);
-      if (st == DGMX_OK) st = run(kRK41, d->Ut, -kRk4A[2] * dt, -kRk4B[2]);
-      if (st == DGMX_OK) st = run(kRK43, d->Ut, dt, -kRk4B[3]);
-      break;
-    default:
-      return d->fail(DGMX_ERR_UNSUPPORTED, "inttype must be 3, 4 or 14");
   }
-  return st;
+  return DGMX_OK;
 }
 
 int stages_per_step(int inttype) { return inttype == DGMX_LSRK14 ? 14 : (inttype == DGMX_TVD3 ? 3 : 4); }
-int launches_per_stage(const dgmx_domain *d) { return (d->ns() ? 3 : 1) + (d->hold ? 2 : 0); }
+int launches_per_stage(const dgmx_domain *d) {
+  const int halo = d->partitioned() && !d->in_group ? (d->ns() ? 4 : 2) : 0;   // pack + unpack per exchange
+  return (d->ns() ? 3 : 1) + (d->hold ? 2 : 0) + halo;
+}
 
 // Mixed form: the reference state the FP32 working copies are perturbations
 // about is the domain mean of U (any constant gives the same scheme; the
@@ -216,7 +319,8 @@ dgmx_status refresh_traces(dgmx_domain *d) {
   cudaError_t e = d->mixed() ? d->ops_m->traces_modal(a, d->U, d->Tf[d->tcur], d->stream)
                              : d->ops->traces_modal(a, d->U, d->T[d->tcur], d->stream);
   ++d->launches;
-  return d->cuda(e, "trace kernel launch");
+  if (e != cudaSuccess) return d->cuda(e, "trace kernel launch");
+  return exchange(d, d->T[d->tcur], d->nf * d->gf);
 }
 
 // Shallow-water balance: the first RHS ever evaluated is subtracted from all
@@ -230,7 +334,8 @@ dgmx_status capture_sw_source(dgmx_domain *d) {
   ++d->launches;
   d->tcur ^= 1;
   d->sw_captured = true;
-  return d->cuda(e, "shallow-water source capture");
+  if (e != cudaSuccess) return d->cuda(e, "shallow-water source capture");
+  return exchange(d, d->T[d->tcur], d->nf * d->gf);
 }
 
 dgmx_status check_error_word(dgmx_domain *d) {
@@ -271,8 +376,15 @@ struct BoundarySpec {
   }
 };
 
+// The rank's part of an element partition (part[e] = owning rank).
+struct PartitionSpec {
+  const int *part = nullptr;
+  int nranks = 1, rank = 0;
+  bool group = false;     // in-process partitions: the group performs the exchange
+};
+
 dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **out,
-                        const BoundarySpec *bspec = nullptr) {
+                        const BoundarySpec *bspec = nullptr, const PartitionSpec *pspec = nullptr) {
   if (!m || !p || !out) { g_create_error = "null argument"; return DGMX_ERR_ARGUMENT; }
   *out = nullptr;
   auto d = std::make_unique<dgmx_domain>();
@@ -353,6 +465,25 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
     g_create_error = err;
     return DGMX_ERR_ARGUMENT;
   }
+  if (pspec && pspec->nranks > 1) {
+    if (d->mixed() || d->hold) {
+      g_create_error = "partitioned domains are FP64 without the bulk-flow hold";
+      return DGMX_ERR_UNSUPPORTED;
+    }
+    if (pspec->group && phys == DGMX_SHALLOW && p->sw_balance) {
+      g_create_error = "in-process partitions of shallow water need sw_balance = 0";
+      return DGMX_ERR_UNSUPPORTED;
+    }
+    HostMesh local;
+    if (!partition_mesh(d->mesh, pspec->part, pspec->nranks, pspec->rank, local, d->plan, err)) {
+      g_create_error = err;
+      return DGMX_ERR_ARGUMENT;
+    }
+    d->mesh = std::move(local);
+    d->ne = d->plan.ne_local;
+    d->in_group = pspec->group;
+  }
+  d->nslot = d->ne + d->plan.nghost;
 
   cudaError_t e = cudaSetDevice(p->device);
   if (e != cudaSuccess) { g_create_error = std::string("cudaSetDevice: ") + cudaGetErrorString(e); return DGMX_ERR_CUDA; }
@@ -380,7 +511,7 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
                              chk(dalloc(&d->Tf[1], d->ntrace()), "alloc T1 (FP32)") &&
                              chk(dalloc(&d->uref, (size_t)kUrefStride), "alloc reference state"))) &&
             (!d->ns() || (chk(dalloc(&d->Ghat, (size_t)d->ne * (d->dim + 1) * d->dim * d->ld), "alloc gradients") &&
-                          chk(dalloc(&d->Vtr, (size_t)d->ne * d->nfaces * (d->nf - 1) * d->gf), "alloc viscous traces") &&
+                          chk(dalloc(&d->Vtr, (size_t)d->nslot * d->nfaces * (d->nf - 1) * d->gf), "alloc viscous traces") &&
                           chk(dalloc(&d->Pv, (size_t)d->ne * (d->nf - 1) * d->ld), "alloc viscous divergence"))) &&
             (!d->ns() || d->dim != 3 || (chk(dalloc(&d->R0, (size_t)d->ne * d->nf), "alloc hold coefficients") &&
                                           chk(dalloc(&d->cbar, (size_t)d->nf), "alloc hold means")));
@@ -400,6 +531,25 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
          chk(cudaMemset(d->T[1], 0, sizeof(double) * d->ntrace()), "memset") &&
          chk(cudaHostAlloc(reinterpret_cast<void **>(&d->host_pinned), sizeof(double) * d->nnodal() * 2,
                            cudaHostAllocDefault), "pinned staging");
+  }
+  if (ok && d->partitioned()) {
+    // exchange lists, concatenated over peers in rank order
+    std::vector<int> snd, rcv;
+    d->x_cnt.assign(d->plan.nranks, 0);
+    d->x_off.assign(d->plan.nranks, 0);
+    for (int q = 0; q < d->plan.nranks; ++q) {
+      d->x_off[q] = (int)snd.size();
+      d->x_cnt[q] = (int)d->plan.send[q].size();
+      snd.insert(snd.end(), d->plan.send[q].begin(), d->plan.send[q].end());
+      rcv.insert(rcv.end(), d->plan.recv[q].begin(), d->plan.recv[q].end());
+    }
+    d->x_total = (int)snd.size();
+    const size_t blk = (size_t)d->nf * d->gf;
+    ok = chk(dalloc(&d->x_send, snd.size()), "alloc halo lists") && chk(dalloc(&d->x_recv, rcv.size()), "alloc halo lists") &&
+         chk(dalloc(&d->x_sbuf, snd.size() * blk), "alloc halo buffers") &&
+         chk(dalloc(&d->x_rbuf, rcv.size() * blk), "alloc halo buffers") &&
+         (snd.empty() || (chk(cudaMemcpy(d->x_send, snd.data(), sizeof(int) * snd.size(), cudaMemcpyHostToDevice), "upload") &&
+                          chk(cudaMemcpy(d->x_recv, rcv.data(), sizeof(int) * rcv.size(), cudaMemcpyHostToDevice), "upload")));
   }
   if (!ok) { g_create_error = d->errmsg; d->release(); return st; }
   if ((st = reset_error_word(d.get())) != DGMX_OK) { g_create_error = d->errmsg; d->release(); return st; }
@@ -461,9 +611,61 @@ dgmx_status dgmx_create_with_boundaries(const dgmx_mesh *mesh, const dgmx_params
   }
 }
 
+dgmx_status dgmx_create_partition(const dgmx_mesh *mesh, const dgmx_params *params, const int *part, int nranks,
+                                  int rank, dgmx_domain **out) {
+  if (!mesh || !params || !part || !out || nranks < 1) { g_create_error = "null argument"; return DGMX_ERR_ARGUMENT; }
+  try {
+    PartitionSpec ps;
+    ps.part = part; ps.nranks = nranks; ps.rank = rank;
+    return create_impl(mesh, params, out, nullptr, &ps);
+  } catch (const std::exception &ex) {
+    g_create_error = ex.what();
+    return DGMX_ERR_ARGUMENT;
+  }
+}
+
+dgmx_status dgmx_nccl_unique_id(unsigned char *id) {
+  if (!id) return DGMX_ERR_ARGUMENT;
+  const NcclApi &nc = nccl_api();
+  if (!nc.ok) { g_create_error = nc.why; return DGMX_ERR_UNSUPPORTED; }
+  ncclUniqueId u;
+  const ncclResult_t r = nc.GetUniqueId(&u);
+  if (r != ncclSuccess) { g_create_error = nc.GetErrorString(r); return DGMX_ERR_CUDA; }
+  static_assert(sizeof(u.internal) == DGMX_NCCL_ID_BYTES, "NCCL unique id size");
+  std::memcpy(id, u.internal, DGMX_NCCL_ID_BYTES);
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_set_exchange_nccl(dgmx_domain *d, const unsigned char *id) {
+  if (!d || !id) return DGMX_ERR_ARGUMENT;
+  if (!d->partitioned() || d->in_group) return d->fail(DGMX_ERR_ARGUMENT, "not a rank of a partitioned domain");
+  const NcclApi &nc = nccl_api();
+  if (!nc.ok) return d->fail(DGMX_ERR_UNSUPPORTED, nc.why);
+  cudaSetDevice(d->prm.device);
+  ncclUniqueId u;
+  std::memcpy(u.internal, id, DGMX_NCCL_ID_BYTES);
+  if (d->nccl) { nc.CommDestroy(d->nccl); d->nccl = nullptr; }
+  const ncclResult_t r = nc.CommInitRank(&d->nccl, d->plan.nranks, u, d->plan.rank);
+  if (r != ncclSuccess) { d->nccl = nullptr; return d->fail(DGMX_ERR_CUDA, std::string("ncclCommInitRank: ") + nc.GetErrorString(r)); }
+  if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_partition_info(const dgmx_domain *d, int *ne_local, int *nghost, int *global_of_local) {
+  if (!d) return DGMX_ERR_ARGUMENT;
+  if (ne_local) *ne_local = d->ne;
+  if (nghost) *nghost = d->plan.nghost;
+  if (global_of_local) {
+    if (d->partitioned()) std::memcpy(global_of_local, d->plan.global_of_local.data(), sizeof(int) * d->ne);
+    else for (int e = 0; e < d->ne; ++e) global_of_local[e] = e;
+  }
+  return DGMX_OK;
+}
+
 dgmx_status dgmx_set_bulk_hold(dgmx_domain *d, int on) {
   if (!d) return DGMX_ERR_ARGUMENT;
   if (on && !d->R0) return d->fail(DGMX_ERR_UNSUPPORTED, "the bulk-flow hold is a Navier-Stokes 3-D option");
+  if (on && d->partitioned()) return d->fail(DGMX_ERR_UNSUPPORTED, "the bulk-flow hold is not built for partitions");
   if (d->hold != (on != 0)) {
     d->hold = on != 0;
     if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
@@ -670,6 +872,8 @@ dgmx_status dgmx_time_derivative_device(dgmx_domain *d, const double *U_dev, dou
   cudaError_t e = d->ops->traces_nodal(a, d->stream);
   ++d->launches;
   if (e != cudaSuccess) return d->cuda(e, "nodal trace kernel");
+  dgmx_status xs = exchange(d, d->T[d->tcur ^ 1], d->nf * d->gf);
+  if (xs != DGMX_OK) return xs;
   a.Tin = d->T[d->tcur ^ 1];
   if (d->prm.physics == DGMX_SHALLOW && d->prm.sw_balance) {
     if (!d->sw_captured) { a.Rcap = d->Rsw; d->sw_captured = true; }
@@ -679,6 +883,7 @@ dgmx_status dgmx_time_derivative_device(dgmx_domain *d, const double *U_dev, dou
     if ((e = d->ops->ns_grad(a, true, d->stream)) != cudaSuccess) return d->cuda(e, "viscous gradient kernel");
     if ((e = d->ops->ns_visc(a, true, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
     d->launches += 2;
+    if ((xs = exchange(d, d->Vtr, (d->nf - 1) * d->gf)) != DGMX_OK) return xs;
   }
   a.R0 = d->hold ? d->R0 : nullptr;
   e = d->ops->rhs_nodal(a, d->stream);
@@ -886,6 +1091,183 @@ dgmx_status dgmx_set_variant(dgmx_domain *d, int index, int *count, int *warp) {
 }  // extern "C"
 
 // ------------------------------------------------------------------------
+// In-process partitions: every part of an element partition as its own
+// handle on one device, stepped in lockstep on one stream with the halo
+// exchange done by device copies between the parts' buffers (pack on the
+// owner, copy, unpack into the receiver's ghost slots: the same lists and
+// kernels the NCCL path uses).  It runs the partitioned path where only one
+// GPU is present.
+struct dgmx_group {
+  std::vector<dgmx_domain *> parts;
+  std::vector<int> part;
+  int ne = 0;
+  std::string errmsg;
+  ~dgmx_group() {
+    for (dgmx_domain *d : parts) {
+      if (!d) continue;
+      cudaSetDevice(d->prm.device);
+      if (d->stream) cudaStreamSynchronize(d->stream);
+      d->release();
+      delete d;
+    }
+  }
+  cudaStream_t stream() const { return parts[0]->stream; }
+};
+
+namespace {
+
+// which = 0: T[tcur], 1: T[tcur ^ 1], 2: viscous traces
+dgmx_status group_exchange(dgmx_group *g, int which) {
+  const cudaStream_t s = g->stream();
+  auto buf = [&](dgmx_domain *d) { return which == 2 ? d->Vtr : d->T[which == 0 ? d->tcur : d->tcur ^ 1]; };
+  dgmx_domain *d0 = g->parts[0];
+  const int blk = which == 2 ? (d0->nf - 1) * d0->gf : d0->nf * d0->gf;
+  cudaError_t e = cudaSuccess;
+  for (dgmx_domain *d : g->parts) {
+    if (e == cudaSuccess) e = launch_pack(buf(d), d->x_send, d->x_total, blk, d->x_sbuf, s);
+    ++d->launches;
+  }
+  const int n = (int)g->parts.size();
+  for (int r = 0; r < n && e == cudaSuccess; ++r)
+    for (int q = 0; q < n && e == cudaSuccess; ++q) {
+      dgmx_domain *dr = g->parts[r], *dq = g->parts[q];
+      if (!dr->x_cnt[q]) continue;
+      e = cudaMemcpyAsync(dr->x_rbuf + (size_t)dr->x_off[q] * blk, dq->x_sbuf + (size_t)dq->x_off[r] * blk,
+                          sizeof(double) * blk * dr->x_cnt[q], cudaMemcpyDeviceToDevice, s);
+    }
+  for (dgmx_domain *d : g->parts) {
+    if (e == cudaSuccess) e = launch_unpack(d->x_rbuf, d->x_recv, d->x_total, blk, buf(d), s);
+    ++d->launches;
+  }
+  if (e != cudaSuccess) { g->errmsg = std::string("group halo exchange: ") + cudaGetErrorString(e); return DGMX_ERR_CUDA; }
+  return DGMX_OK;
+}
+
+dgmx_status group_fail(dgmx_group *g, dgmx_domain *d, dgmx_status st) {
+  g->errmsg = d->errmsg;
+  return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+dgmx_status dgmx_group_create(const dgmx_mesh *mesh, const dgmx_params *params, const int *part, int nparts,
+                              dgmx_group **out) {
+  if (!mesh || !params || !part || !out || nparts < 2) { g_create_error = "group: null argument or nparts < 2"; return DGMX_ERR_ARGUMENT; }
+  *out = nullptr;
+  auto g = std::make_unique<dgmx_group>();
+  g->ne = mesh->ne;
+  g->part.assign(part, part + mesh->ne);
+  for (int r = 0; r < nparts; ++r) {
+    PartitionSpec ps;
+    ps.part = part; ps.nranks = nparts; ps.rank = r; ps.group = true;
+    dgmx_domain *d = nullptr;
+    dgmx_status st;
+    try {
+      st = create_impl(mesh, params, &d, nullptr, &ps);
+    } catch (const std::exception &ex) {
+      g_create_error = ex.what();
+      st = DGMX_ERR_ARGUMENT;
+    }
+    if (st != DGMX_OK) return st;
+    g->parts.push_back(d);
+  }
+  *out = g.release();
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_group_destroy(dgmx_group *g) {
+  if (!g) return DGMX_ERR_ARGUMENT;
+  delete g;
+  return DGMX_OK;
+}
+
+dgmx_domain *dgmx_group_part(dgmx_group *g, int r) {
+  return g && r >= 0 && r < (int)g->parts.size() ? g->parts[r] : nullptr;
+}
+
+const char *dgmx_group_last_error(const dgmx_group *g) { return g ? g->errmsg.c_str() : g_create_error.c_str(); }
+
+dgmx_status dgmx_group_set_state(dgmx_group *g, const double *U) {
+  if (!g || !U) return DGMX_ERR_ARGUMENT;
+  dgmx_domain *d0 = g->parts[0];
+  const size_t qd = d0->qd;
+  for (dgmx_domain *d : g->parts) {
+    std::vector<double> loc((size_t)d->nf * d->ne * qd);
+    for (int n = 0; n < d->nf; ++n)
+      for (int e = 0; e < d->ne; ++e)
+        std::memcpy(&loc[((size_t)n * d->ne + e) * qd], U + ((size_t)n * g->ne + d->plan.global_of_local[e]) * qd,
+                    sizeof(double) * qd);
+    const dgmx_status st = dgmx_set_state(d, loc.data());
+    if (st != DGMX_OK) return group_fail(g, d, st);
+  }
+  cudaSetDevice(d0->prm.device);
+  dgmx_status st = group_exchange(g, 0);
+  if (st != DGMX_OK) return st;
+  return cudaStreamSynchronize(g->stream()) == cudaSuccess ? DGMX_OK : DGMX_ERR_CUDA;
+}
+
+dgmx_status dgmx_group_get_state(dgmx_group *g, double *U) {
+  if (!g || !U) return DGMX_ERR_ARGUMENT;
+  const size_t qd = g->parts[0]->qd;
+  for (dgmx_domain *d : g->parts) {
+    std::vector<double> loc((size_t)d->nf * d->ne * qd);
+    const dgmx_status st = dgmx_get_state(d, loc.data());
+    if (st != DGMX_OK) return group_fail(g, d, st);
+    for (int n = 0; n < d->nf; ++n)
+      for (int e = 0; e < d->ne; ++e)
+        std::memcpy(U + ((size_t)n * g->ne + d->plan.global_of_local[e]) * qd, &loc[((size_t)n * d->ne + e) * qd],
+                    sizeof(double) * qd);
+  }
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_group_advance(dgmx_group *g, double dt, int nsteps) {
+  if (!g || nsteps < 0) return DGMX_ERR_ARGUMENT;
+  dgmx_domain *d0 = g->parts[0];
+  cudaSetDevice(d0->prm.device);
+  const cudaStream_t s = g->stream();
+  const std::vector<StageSpec> specs = stage_specs(d0->prm.inttype, dt);
+  if (specs.empty()) { g->errmsg = "inttype must be 3, 4 or 14"; return DGMX_ERR_UNSUPPORTED; }
+  for (dgmx_domain *d : g->parts) {
+    if (d->prm.physics == DGMX_SHALLOW && d->prm.sw_balance) { g->errmsg = "shallow-water balance is off in groups"; return DGMX_ERR_UNSUPPORTED; }
+    if (reset_error_word(d) != DGMX_OK || cudaStreamSynchronize(d->stream) != cudaSuccess) return group_fail(g, d, DGMX_ERR_CUDA);
+  }
+  cudaError_t e = cudaSuccess;
+  dgmx_status st = DGMX_OK;
+  for (int step = 0; step < nsteps && st == DGMX_OK; ++step)
+    for (const StageSpec &sp : specs) {
+      if (d0->ns()) {
+        for (dgmx_domain *d : g->parts) {
+          const StageArgs a = stage_args(d, sp, dt);
+          if (e == cudaSuccess) e = d->ops->ns_grad(a, false, s);
+          if (e == cudaSuccess) e = d->ops->ns_visc(a, false, s);
+          d->launches += 2;
+        }
+        if (e == cudaSuccess && (st = group_exchange(g, 2)) != DGMX_OK) return st;
+      }
+      for (dgmx_domain *d : g->parts) {
+        const StageArgs a = stage_args(d, sp, dt);
+        if (e == cudaSuccess) e = d->stage_ops()->stage(a, s);
+        ++d->launches;
+      }
+      if (e == cudaSuccess && (st = group_exchange(g, 1)) != DGMX_OK) return st;
+      for (dgmx_domain *d : g->parts) d->tcur ^= 1;
+      if (e != cudaSuccess) break;
+    }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) { g->errmsg = std::string("group advance: ") + cudaGetErrorString(e); return DGMX_ERR_CUDA; }
+  for (dgmx_domain *d : g->parts) {
+    st = check_error_word(d);
+    if (st != DGMX_OK) return group_fail(g, d, st);
+  }
+  return DGMX_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------
 // Host-only inspection entry points (no CUDA calls): the 1-D tables and the
 // processed connectivity, so the setup can be checked on machines without a
 // GPU.
@@ -903,6 +1285,43 @@ dgmx_status dgmx_tables(int L, int Q, double *z, double *w, double *D, double *B
   std::memcpy(gl2g, t.gl2g.data(), sizeof(double) * (Q - 1) * Q);
   std::memcpy(g2gl, t.g2gl.data(), sizeof(double) * Q * (Q - 1));
   return DGMX_OK;
+}
+
+// The partition plan of one rank (host only).  sizes[0..2] = local
+// elements, ghost slots, exchanged blocks; the arrays (each may be NULL, e.g.
+// on a first call for the sizes) get the global ids of the local elements
+// and of the ghosts, the per-peer block counts (nranks) and the concatenated
+// send blocks (local element * nfaces + face) and receive blocks (slot *
+// nfaces + face), peers in rank order.
+dgmx_status dgmx_partition_plan(const dgmx_mesh *m, const int *part, int nranks, int rank, int *sizes,
+                                int *global_of_local, int *global_of_ghost, int *peer_counts, int *send, int *recv) {
+  if (!m || !part || !sizes || !m->porder) return DGMX_ERR_ARGUMENT;
+  try {
+    const int p = m->porder[0], q = (m->qorder && m->qorder[0]) ? m->qorder[0] : p + 2;
+    const Tables1D t = make_tables(p + 1, q, q - 1);
+    HostMesh hm, loc;
+    PartitionPlan plan;
+    std::string err;
+    if (!build_mesh(*m, t, hm, err) || !partition_mesh(hm, part, nranks, rank, loc, plan, err)) {
+      g_create_error = err;
+      return DGMX_ERR_ARGUMENT;
+    }
+    int nb = 0;
+    for (int r = 0; r < nranks; ++r) nb += (int)plan.send[r].size();
+    sizes[0] = plan.ne_local; sizes[1] = plan.nghost; sizes[2] = nb;
+    if (global_of_local) std::copy(plan.global_of_local.begin(), plan.global_of_local.end(), global_of_local);
+    if (global_of_ghost) std::copy(plan.global_of_ghost.begin(), plan.global_of_ghost.end(), global_of_ghost);
+    for (int r = 0, at = 0; r < nranks; ++r) {
+      if (peer_counts) peer_counts[r] = (int)plan.send[r].size();
+      if (send) std::copy(plan.send[r].begin(), plan.send[r].end(), send + at);
+      if (recv) std::copy(plan.recv[r].begin(), plan.recv[r].end(), recv + at);
+      at += (int)plan.send[r].size();
+    }
+    return DGMX_OK;
+  } catch (const std::exception &ex) {
+    g_create_error = ex.what();
+    return DGMX_ERR_ARGUMENT;
+  }
 }
 
 // links: ne*nfaces*4 ints (neighbour, neighbour face, master flag, class id);
@@ -937,7 +1356,7 @@ dgmx_status dgmx_mesh_links(const dgmx_mesh *m, int *links, int *perm_pairs) {
 // Read-only view of a handle for entry points compiled in other units.
 namespace dgmx {
 bool domain_view(dgmx_domain *d, DomainView *v) {
-  if (!d || !v) return false;
+  if (!d || !v || d->partitioned()) return false;
   v->ops = d->ops;
   v->stream = d->stream;
   v->base = d->base_args();

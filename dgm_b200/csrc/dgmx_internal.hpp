@@ -92,6 +92,26 @@ constexpr int kMaxBcTypes = 15;
 bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::string &err,
                 const std::vector<BoundarySide> *bcs = nullptr);
 
+// Element partition of a processed mesh (the reference's root.part.N /
+// Zoltan partitions, src/Field.cpp make_partition).  The local mesh holds the
+// rank's elements in increasing global order; a face whose neighbour lives
+// on another rank links to a ghost slot ne_local + g (ghosts in increasing
+// global order) whose face trace the halo exchange fills.  For every peer
+// q, send[q] lists the local (element * nfaces + face) blocks q needs and
+// recv[q] the (slot * nfaces + face) blocks q sends here, both in the order
+// of the global (element, face) they hold, so the two sides agree without
+// exchanging metadata (src/vField.cpp:146-200 is the reference's exchange).
+struct PartitionPlan {
+  int nranks = 1, rank = 0, ne_local = 0, nghost = 0;
+  std::vector<int> global_of_local, global_of_ghost;
+  std::vector<std::vector<int>> send, recv;
+};
+bool partition_mesh(const HostMesh &g, const int *part, int nranks, int rank, HostMesh &local, PartitionPlan &plan,
+                    std::string &err);
+// Pack / unpack of blk-double blocks by index (exchange.cu).
+cudaError_t launch_pack(const double *T, const int *idx, int n, int blk, double *buf, cudaStream_t s);
+cudaError_t launch_unpack(const double *buf, const int *idx, int n, int blk, double *T, cudaStream_t s);
+
 // DGM input files (.inp/.msh/.con/.ord)
 struct FileCase {
   int dim = 0, ne = 0;

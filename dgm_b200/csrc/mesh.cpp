@@ -291,6 +291,76 @@ bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::strin
   return true;
 }
 
+// ---------------------------------------------------------------- partitions
+bool partition_mesh(const HostMesh &g, const int *part, int nranks, int rank, HostMesh &local, PartitionPlan &plan,
+                    std::string &err) {
+  const int ne = g.ne, nf = g.nfaces;
+  if (nranks < 1 || rank < 0 || rank >= nranks) { err = "partition: rank out of range"; return false; }
+  for (int e = 0; e < ne; ++e)
+    if (part[e] < 0 || part[e] >= nranks) { err = "partition: element " + std::to_string(e) + " has no rank"; return false; }
+  plan = PartitionPlan();
+  plan.nranks = nranks; plan.rank = rank;
+  std::vector<int> local_of(ne, -1), ghost_of(ne, -1);
+  for (int e = 0; e < ne; ++e)
+    if (part[e] == rank) { local_of[e] = (int)plan.global_of_local.size(); plan.global_of_local.push_back(e); }
+  plan.ne_local = (int)plan.global_of_local.size();
+  if (!plan.ne_local) { err = "partition: rank " + std::to_string(rank) + " owns no element"; return false; }
+  // ghosts: remote neighbours of local faces, in global order
+  std::vector<char> need(ne, 0);
+  for (int e : plan.global_of_local)
+    for (int f = 0; f < nf; ++f) {
+      const FaceLink &l = g.links[(size_t)e * nf + f];
+      if (part[l.elem] != rank) need[l.elem] = 1;
+    }
+  for (int e = 0; e < ne; ++e)
+    if (need[e]) { ghost_of[e] = plan.ne_local + (int)plan.global_of_ghost.size(); plan.global_of_ghost.push_back(e); }
+  plan.nghost = (int)plan.global_of_ghost.size();
+  // local mesh: the rank's elements, links remapped to local indices or ghost slots
+  local = HostMesh();
+  local.dim = g.dim; local.ne = plan.ne_local; local.p = g.p; local.L = g.L; local.Q = g.Q; local.G = g.G;
+  local.nfaces = nf; local.gf = g.gf;
+  local.classes = g.classes;
+  local.perm = g.perm;
+  const size_t qd = g.cx.size() / (size_t)ne;
+  for (int e : plan.global_of_local) {
+    local.gclass.push_back(g.gclass[e]);
+    local.J.push_back(g.J[e]);
+    local.cx.insert(local.cx.end(), g.cx.begin() + (size_t)e * qd, g.cx.begin() + (size_t)(e + 1) * qd);
+    local.cy.insert(local.cy.end(), g.cy.begin() + (size_t)e * qd, g.cy.begin() + (size_t)(e + 1) * qd);
+    local.cz.insert(local.cz.end(), g.cz.begin() + (size_t)e * qd, g.cz.begin() + (size_t)(e + 1) * qd);
+    for (int f = 0; f < nf; ++f) {
+      FaceLink l = g.links[(size_t)e * nf + f];
+      l.elem = part[l.elem] == rank ? local_of[l.elem] : ghost_of[l.elem];
+      l.cls = f == 0 ? g.gclass[e] : 0;
+      local.links.push_back(l);
+    }
+  }
+  // exchange lists, ordered by the global (element, face) of the block
+  plan.send.assign(nranks, {});
+  plan.recv.assign(nranks, {});
+  for (int e : plan.global_of_local)
+    for (int f = 0; f < nf; ++f) {
+      const FaceLink &l = g.links[(size_t)e * nf + f];
+      const int q = part[l.elem];
+      if (q == rank) continue;
+      // q needs this face's trace (the neighbour side of its face l)
+      plan.send[q].push_back(local_of[e] * nf + f);
+      plan.recv[q].push_back(ghost_of[l.elem] * nf + l.face);
+    }
+  auto gkey = [&](int v, bool ghost) {
+    const int slot = v / nf, f = v % nf;
+    const int ge = ghost ? plan.global_of_ghost[slot - plan.ne_local] : plan.global_of_local[slot];
+    return (long long)ge * nf + f;
+  };
+  for (int q = 0; q < nranks; ++q) {
+    std::sort(plan.send[q].begin(), plan.send[q].end(),
+              [&](int a, int b) { return gkey(a, false) < gkey(b, false); });
+    std::sort(plan.recv[q].begin(), plan.recv[q].end(),
+              [&](int a, int b) { return gkey(a, true) < gkey(b, true); });
+  }
+  return true;
+}
+
 // ---------------------------------------------------------------- file input
 namespace {
 std::string lower(std::string s) {

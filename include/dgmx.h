@@ -98,6 +98,41 @@ dgmx_status dgmx_create_from_files(const char *root, const dgmx_params *params, 
 dgmx_status dgmx_create_with_boundaries(const dgmx_mesh *mesh, const dgmx_params *params, int nbc,
                                         const int *bc_sides, const double *bc_params, dgmx_domain **out);
 
+/* ---- element partitions (the reference's MPI decomposition: root.part.N
+ * partitions, side exchange in src/vField.cpp:146-200) ----
+ * A partitioned handle owns the elements e with part[e] == rank (in
+ * increasing global order: its Field-layout arrays are over those elements);
+ * faces whose neighbour lives on another rank read ghost slots that a halo
+ * exchange fills after every stage (and after the viscous flux kernel for
+ * Navier-Stokes).  FP64 only, no bulk-flow hold. */
+dgmx_status dgmx_create_partition(const dgmx_mesh *mesh, const dgmx_params *params, const int *part, int nranks,
+                                  int rank, dgmx_domain **out);
+/* NCCL transport for the multi-rank exchange: rank 0 makes the id, every
+ * rank passes the same id (collective over the ranks). */
+#define DGMX_NCCL_ID_BYTES 128
+dgmx_status dgmx_nccl_unique_id(unsigned char *id);
+dgmx_status dgmx_set_exchange_nccl(dgmx_domain *d, const unsigned char *id);
+/* local element count, ghost slots and the global id of every local element */
+dgmx_status dgmx_partition_info(const dgmx_domain *d, int *ne_local, int *nghost, int *global_of_local);
+/* Host-only partition plan (see dgmx.cpp): sizes[3] = local elements, ghost
+ * slots, exchanged face blocks; then the lists.  Any array may be NULL. */
+dgmx_status dgmx_partition_plan(const dgmx_mesh *mesh, const int *part, int nranks, int rank, int *sizes,
+                                int *global_of_local, int *global_of_ghost, int *peer_counts, int *send,
+                                int *recv);
+
+/* In-process partitions: every part as a handle on one device, stepped in
+ * lockstep with the exchange done by device copies (runs the partitioned
+ * path on one GPU).  State arrays are global, Field layout. */
+typedef struct dgmx_group dgmx_group;
+dgmx_status dgmx_group_create(const dgmx_mesh *mesh, const dgmx_params *params, const int *part, int nparts,
+                              dgmx_group **out);
+dgmx_status dgmx_group_destroy(dgmx_group *g);
+dgmx_domain *dgmx_group_part(dgmx_group *g, int r);
+dgmx_status dgmx_group_set_state(dgmx_group *g, const double *U);
+dgmx_status dgmx_group_get_state(dgmx_group *g, double *U);
+dgmx_status dgmx_group_advance(dgmx_group *g, double dt, int nsteps);
+const char *dgmx_group_last_error(const dgmx_group *g);
+
 /* Navier-Stokes 3-D channel forcing, Channel::holdBulkMassFlow
  * (src/Channel.hpp:116-163, called from src/Navier_Stokes3d.cpp:160): after
  * each projected right-hand side, its volume means of density, x-momentum

@@ -1,0 +1,72 @@
+"""Element partitions on the GPU: the in-process group (every part a handle
+on one device, the halo exchange by device copies through the same pack /
+unpack lists as the NCCL path) steps exactly like the unpartitioned domain,
+and like the oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from oracle import dgm_io, ics
+
+pytestmark = pytest.mark.gpu
+
+
+CASES = [
+    # name, physics, dim, n, lo, hi, p, flux, inttype, dt, steps, vis, nparts, kind
+    ("euler3d-lsrk14-2-slabs", 8, 3, (3, 2, 4), 0.0, 2 * np.pi, 3, "roe", 14, 0.002, 2, 0.0, 2, "slabs"),
+    ("euler3d-tvd3-3-random", 8, 3, (3, 3, 2), 0.0, 2 * np.pi, 2, "laxfriedrichs", 3, 0.002, 3, 0.0, 3, "random"),
+    ("ns3d-rk4-4-random", 9, 3, (2, 3, 3), 0.0, 2 * np.pi, 3, "laxfriedrichs", 4, 0.002, 2, 0.02, 4, "random"),
+    ("euler2d-lsrk14-3-slabs", 1, 2, (5, 4), -5.0, 5.0, 4, "laxfriedrichs", 14, 0.005, 2, 0.0, 3, "slabs"),
+    ("ns2d-tvd3-2-random", 2, 2, (4, 4), 0.0, 4.0, 3, "laxfriedrichs", 3, 0.001, 3, 0.02, 2, "random"),
+]
+
+
+def _ic(phys, x, y, z):
+    if phys in (8, 9):
+        return ics.taylor_green(x, y, z, Ma=0.1)
+    if phys == 2:
+        return ics.vortex_ic(x, y, [(2.0, 2.0, 0.3, 1.0, 0.5)], nf=4)
+    return ics.isentropic_vortex(x, y, beta=5.0, period=(10.0, 10.0))
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_group_equals_single_domain(case):
+    import dgm_b200
+    _, phys, dim, n, lo, hi, p, flux, inttype, dt, steps, vis, nparts, kind = case
+    m = dgm_b200.meshgen.box(dim, n, lo, hi, p)
+    ne = m.verts.shape[0]
+    part = ((np.arange(ne) * nparts) // ne if kind == "slabs"
+            else np.random.default_rng(5).permutation(np.arange(ne) % nparts))
+    D = dgm_b200.Domain(m, phys, flux=flux, inttype=inttype, vis=vis, sw_balance=False)
+    G = dgm_b200.Group(m, phys, part, flux=flux, inttype=inttype, vis=vis)
+    x, y, z = D.coordinates()
+    f = _ic(phys, x, y, z)
+    D.set_state(f)
+    G.set_state(f)
+    assert np.array_equal(G.state(), D.state())
+    D.advance(dt, steps)
+    G.advance(dt, steps)
+    S = D.state()
+    assert np.array_equal(G.state(), S)
+    P = oracle.Problem(dgm_io.Mesh(m.dim, m.verts, m.con, m.porder, m.qorder), phys, flux=flux, vis=vis)
+    P.set_state(P.project(f))
+    P.advance(inttype, dt, steps)
+    O = P.state()
+    assert float(np.sqrt(((S - O) ** 2).sum() / (O ** 2).sum())) < 1e-12
+    G.close()
+
+
+def test_partition_handles_and_nccl_id():
+    """A rank's handle covers its own elements; the NCCL id is made through
+    the lazily loaded NCCL library; stepping without an exchange is refused."""
+    import dgm_b200
+    m = dgm_b200.meshgen.box(3, (2, 2, 2), 0.0, 2 * np.pi, 2)
+    part = np.array([0, 0, 0, 0, 1, 1, 1, 1])
+    R = dgm_b200.Domain.partition(m, dgm_b200.EULER3D, part, 2, 1)
+    ne, ng, gl = R.partition_info()
+    assert ne == 4 and ng == 4 and list(gl) == [4, 5, 6, 7]
+    nid = dgm_b200.nccl_unique_id()
+    assert len(nid) == 128 and any(nid)
+    x, y, z = R.coordinates()
+    with pytest.raises(dgm_b200.DgmxError):
+        R.set_state(ics.taylor_green(x, y, z, Ma=0.1))
