@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--trace", type=int, default=200, help="requests in the serving trace")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both",
                     help="time one form only (profiling runs); the default line needs both")
+    ap.add_argument("--only", choices=["config1", "config3", "channel"], default=None,
+                    help="run one of the other configurations alone and print its JSON (profiling)")
     ap.add_argument("--variant", type=int, default=-1,
                     help="single-form runs: use this tile variant instead of the autotuner's pick")
     return ap.parse_args()
@@ -252,7 +254,7 @@ def time_steps(D, stream, dt, steps, warmup, barrier, max_over_ranks, clk=None):
     return max_over_ranks(ev0.elapsed_time(ev1) / 1e3), launches
 
 
-def other_configs(dgm_b200, args):
+def other_configs(dgm_b200, args, only=None):
     """BASELINE configs 1 and 3 on this GPU.  Config 1: the 2-D isentropic
     vortex (16 x 16 Quads on [-5,5]^2, p=4, beta=5, LF, LSRK14, dt from CFL
     0.5, 200 steps) with its L2 distance from the FP64 oracle and from the
@@ -262,145 +264,150 @@ def other_configs(dgm_b200, args):
     which each run first reports a non-physical state.  Config 3: the 3-D
     Navier-Stokes Taylor-Green vortex (24^3 Hex, p=7, q=8, Re=1600, Pr=0.71,
     Mach 0.1, Roe, LSRK14) timed over its first steps, with the
-    kinetic-energy history (FP64)."""
+    kinetic-energy history (FP64).  And the reference's runs/chan regression
+    case (walls, bulk-flow hold) against its golden restart.  `only` runs one
+    of them."""
     import torch
     from dgm_b200 import requests as R
     res = {}
-    n, p, steps, block = 16, 4, 200, 10
-    for q in (6, 5):
-        mesh = dgm_b200.meshgen.box(2, (n, n), -5.0, 5.0, p, q)
-        D = dgm_b200.Domain(mesh, dgm_b200.EULER2D, flux="laxfriedrichs", inttype=dgm_b200.LSRK14)
-        x, y = D.coordinates()[:2]
-        U0 = R.vortex(x, y, beta=5.0)
-        dt = R.cfl_dt(U0, 10.0 / n, p, dgm_b200.EULER2D, 0.5)
-        c1 = {"workload": f"euler2d_isentropic_vortex_16^2_p4_q{q}_lf_lsrk14_{steps}steps", "dt": dt}
-        D.set_state(U0)
-        gpu_fail = None
-        if q == 6:
-            D.advance(dt, 3)
+    if only in (None, "config1"):
+        n, p, steps, block = 16, 4, 200, 10
+        for q in (6, 5):
+            mesh = dgm_b200.meshgen.box(2, (n, n), -5.0, 5.0, p, q)
+            D = dgm_b200.Domain(mesh, dgm_b200.EULER2D, flux="laxfriedrichs", inttype=dgm_b200.LSRK14)
+            x, y = D.coordinates()[:2]
+            U0 = R.vortex(x, y, beta=5.0)
+            dt = R.cfl_dt(U0, 10.0 / n, p, dgm_b200.EULER2D, 0.5)
+            c1 = {"workload": f"euler2d_isentropic_vortex_16^2_p4_q{q}_lf_lsrk14_{steps}steps", "dt": dt}
             D.set_state(U0)
-            st = torch.cuda.ExternalStream(D.stream())
+            gpu_fail = None
+            if q == 6:
+                D.advance(dt, 3)
+                D.set_state(U0)
+                st = torch.cuda.ExternalStream(D.stream())
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                D.advance_async(dt, steps)
+                e1.record(st)
+                e1.synchronize()
+                D.sync()
+                t = e0.elapsed_time(e1) / 1e3
+                c1.update({"value": 4 * n * n * (p + 1) ** 2 * 14 * steps / t, "unit": UNIT,
+                           "ms_per_step": 1e3 * t / steps})
+            else:
+                for b in range(steps // block):
+                    try:
+                        D.advance(dt, block)
+                    except dgm_b200.NonPhysicalState:
+                        gpu_fail = (b + 1) * block
+                        break
+            if not args.no_cpu_baseline:
+                import oracle
+                from oracle import dgm_io
+                P = oracle.Problem(dgm_io.Mesh(2, mesh.verts, mesh.con, mesh.porder, mesh.qorder), oracle.EULER2D)
+                P.set_state(P.project(U0))
+                if q == 6:
+                    P.advance(14, dt, steps)
+                    G, O = D.state(), P.state()
+                    c1["rel_l2_vs_oracle_per_field"] = [rel_l2(G[k], O[k]) for k in range(4)]
+                else:
+                    ora_fail = None
+                    for b in range(steps // block):
+                        if P.advance(14, dt, block) != 0:
+                            ora_fail = (b + 1) * block
+                            break
+                    c1["nonphysical_within_steps"] = {"gpu": gpu_fail, "oracle": ora_fail}
+            if q == 6:
+                # the vortex rides the free stream (u=1, v=0): the exact state at T is the initial one shifted by T
+                c1["rel_l2_vs_exact_per_field"] = [rel_l2(a, b) for a, b in
+                                                   zip(D.state(), R.vortex(x, y, beta=5.0, x0=dt * steps))]
+            D.close()
+            res[f"config1_q{q}"] = c1
+    if only in (None, "config3"):
+        # config 3
+        n, p, q, k3 = 24, 7, 8, 10
+        mesh = dgm_b200.meshgen.box(3, (n, n, n), 0.0, 2 * math.pi, p, q)
+        D = dgm_b200.Domain(mesh, dgm_b200.NS3D, flux="roe", inttype=dgm_b200.LSRK14, vis=1.0 / 1600.0, Pr=0.71)
+        x, y, z = D.coordinates()
+        U0 = taylor_green(x, y, z, 0.1, 1.4)
+        dt = cfl_dt(U0, 2 * math.pi / n, p, 1.4, 0.5)
+        D.set_state(U0)
+        rows, _ = D.autotune(reps=3)
+        D.set_state(U0)
+        xg = R.gll_points(q)
+        c = np.zeros(q)
+        c[-1] = 1.0
+        w1 = 2.0 / ((q - 1) * q * np.polynomial.legendre.legval(xg, c) ** 2)
+        w = np.einsum("i,j,k->kji", w1, w1, w1).reshape(-1)
+
+        def kinetic_energy(U):
+            # volume mean of rho |u|^2 / 2 (GLL quadrature; equal elements)
+            e = 0.5 * (U[1] ** 2 + U[2] ** 2 + U[3] ** 2) / U[0]
+            return float((e.reshape(-1, q ** 3) * w).sum() / (w.sum() * e.size / q ** 3))
+
+        st = torch.cuda.ExternalStream(D.stream())
+        ke, t = [kinetic_energy(D.state())], 0.0
+        for _ in range(k3):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(st)
-            D.advance_async(dt, steps)
+            D.advance_async(dt, 1)
             e1.record(st)
             e1.synchronize()
             D.sync()
-            t = e0.elapsed_time(e1) / 1e3
-            c1.update({"value": 4 * n * n * (p + 1) ** 2 * 14 * steps / t, "unit": UNIT,
-                       "ms_per_step": 1e3 * t / steps})
-        else:
-            for b in range(steps // block):
-                try:
-                    D.advance(dt, block)
-                except dgm_b200.NonPhysicalState:
-                    gpu_fail = (b + 1) * block
-                    break
-        if not args.no_cpu_baseline:
-            import oracle
-            from oracle import dgm_io
-            P = oracle.Problem(dgm_io.Mesh(2, mesh.verts, mesh.con, mesh.porder, mesh.qorder), oracle.EULER2D)
-            P.set_state(P.project(U0))
-            if q == 6:
-                P.advance(14, dt, steps)
-                G, O = D.state(), P.state()
-                c1["rel_l2_vs_oracle_per_field"] = [rel_l2(G[k], O[k]) for k in range(4)]
-            else:
-                ora_fail = None
-                for b in range(steps // block):
-                    if P.advance(14, dt, block) != 0:
-                        ora_fail = (b + 1) * block
-                        break
-                c1["nonphysical_within_steps"] = {"gpu": gpu_fail, "oracle": ora_fail}
-        if q == 6:
-            # the vortex rides the free stream (u=1, v=0): the exact state at T is the initial one shifted by T
-            c1["rel_l2_vs_exact_per_field"] = [rel_l2(a, b) for a, b in
-                                               zip(D.state(), R.vortex(x, y, beta=5.0, x0=dt * steps))]
+            t += e0.elapsed_time(e1) / 1e3
+            ke.append(kinetic_energy(D.state()))
+        dof = 5 * n ** 3 * (p + 1) ** 3
+        res["config3"] = {"workload": "ns3d_taylor_green_24^3_p7_q8_re1600_pr0.71_roe_lsrk14", "steps_timed": k3,
+                          "dt": dt, "value": dof * 14 * k3 / t, "unit": UNIT, "ms_per_step": 1e3 * t / k3,
+                          "kinetic_energy": ke, "tile_us": [round(float(r[3]), 1) for r in rows],
+                          # -dKE/dt at t=0 of the incompressible limit is nu <|grad u|^2> = 3 nu / 4
+                          "dissipation_rate": (ke[0] - ke[-1]) / (k3 * dt), "dissipation_rate_t0_exact": 0.75 / 1600.0,
+                          "note": "FP64 BR1; the 1000-step run and the TF32 contraction form are not timed here"}
         D.close()
-        res[f"config1_q{q}"] = c1
-    # config 3
-    n, p, q, k3 = 24, 7, 8, 10
-    mesh = dgm_b200.meshgen.box(3, (n, n, n), 0.0, 2 * math.pi, p, q)
-    D = dgm_b200.Domain(mesh, dgm_b200.NS3D, flux="roe", inttype=dgm_b200.LSRK14, vis=1.0 / 1600.0, Pr=0.71)
-    x, y, z = D.coordinates()
-    U0 = taylor_green(x, y, z, 0.1, 1.4)
-    dt = cfl_dt(U0, 2 * math.pi / n, p, 1.4, 0.5)
-    D.set_state(U0)
-    rows, _ = D.autotune(reps=3)
-    D.set_state(U0)
-    xg = R.gll_points(q)
-    c = np.zeros(q)
-    c[-1] = 1.0
-    w1 = 2.0 / ((q - 1) * q * np.polynomial.legendre.legval(xg, c) ** 2)
-    w = np.einsum("i,j,k->kji", w1, w1, w1).reshape(-1)
-
-    def kinetic_energy(U):
-        # volume mean of rho |u|^2 / 2 (GLL quadrature; equal elements)
-        e = 0.5 * (U[1] ** 2 + U[2] ** 2 + U[3] ** 2) / U[0]
-        return float((e.reshape(-1, q ** 3) * w).sum() / (w.sum() * e.size / q ** 3))
-
-    st = torch.cuda.ExternalStream(D.stream())
-    ke, t = [kinetic_energy(D.state())], 0.0
-    for _ in range(k3):
+    if only in (None, "channel"):
+        # the reference's channel regression case (runs/chan: NS 3-D, 512 hexes, p=3,
+        # isothermal walls, bulk-flow hold, TVD3, 100 steps from its restart initial
+        # condition), inputs and golden result from the committed fixture
+        z = np.load(os.path.join(ROOT, "tests", "golden", "chan.npz"))
+        meta = json.loads(str(z["meta"]))
+        inp = meta["inp"]
+        mesh = dgm_b200.meshgen.Mesh(3, z["verts"], z["con"], z["porder"], z["qorder"])
+        tw, eref = meta["bct"][meta["bc_tags"][0]][1][:2]
+        rec = [(int(e), int(s_), dgm_b200.BC_ISOTHERMAL_WALL, tw, eref) for e, s_ in z["bc_sides"]]
+        D = dgm_b200.Domain(mesh, dgm_b200.NS3D, inttype=inp["inttype"], vis=float(inp["vis"]), boundaries=rec,
+                            bulk_hold=True)
+        D.set_modes(z["ic_modal"])
+        D.advance(float(inp["dt"]), 2)
+        D.set_modes(z["ic_modal"])
+        st = torch.cuda.ExternalStream(D.stream())
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
-        D.advance_async(dt, 1)
+        D.advance_async(float(inp["dt"]), int(inp["Nt"]))
         e1.record(st)
         e1.synchronize()
         D.sync()
-        t += e0.elapsed_time(e1) / 1e3
-        ke.append(kinetic_energy(D.state()))
-    dof = 5 * n ** 3 * (p + 1) ** 3
-    res["config3"] = {"workload": "ns3d_taylor_green_24^3_p7_q8_re1600_pr0.71_roe_lsrk14", "steps_timed": k3,
-                      "dt": dt, "value": dof * 14 * k3 / t, "unit": UNIT, "ms_per_step": 1e3 * t / k3,
-                      "kinetic_energy": ke, "tile_us": [round(float(r[3]), 1) for r in rows],
-                      # -dKE/dt at t=0 of the incompressible limit is nu <|grad u|^2> = 3 nu / 4
-                      "dissipation_rate": (ke[0] - ke[-1]) / (k3 * dt), "dissipation_rate_t0_exact": 0.75 / 1600.0,
-                      "note": "FP64 BR1; the 1000-step run and the TF32 contraction form are not timed here"}
-    D.close()
-    # the reference's channel regression case (runs/chan: NS 3-D, 512 hexes, p=3,
-    # isothermal walls, bulk-flow hold, TVD3, 100 steps from its restart initial
-    # condition), inputs and golden result from the committed fixture
-    z = np.load(os.path.join(ROOT, "tests", "golden", "chan.npz"))
-    meta = json.loads(str(z["meta"]))
-    inp = meta["inp"]
-    mesh = dgm_b200.meshgen.Mesh(3, z["verts"], z["con"], z["porder"], z["qorder"])
-    tw, eref = meta["bct"][meta["bc_tags"][0]][1][:2]
-    rec = [(int(e), int(s_), dgm_b200.BC_ISOTHERMAL_WALL, tw, eref) for e, s_ in z["bc_sides"]]
-    D = dgm_b200.Domain(mesh, dgm_b200.NS3D, inttype=inp["inttype"], vis=float(inp["vis"]), boundaries=rec,
-                        bulk_hold=True)
-    D.set_modes(z["ic_modal"])
-    D.advance(float(inp["dt"]), 2)
-    D.set_modes(z["ic_modal"])
-    st = torch.cuda.ExternalStream(D.stream())
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    D.advance_async(float(inp["dt"]), int(inp["Nt"]))
-    e1.record(st)
-    e1.synchronize()
-    D.sync()
-    t = e0.elapsed_time(e1) / 1e3
-    nsteps = int(inp["Nt"])
-    dof = 5 * mesh.verts.shape[0] * 64
-    chan = {"workload": "runs/chan (NS 3-D channel, 512 hexes, p=3, isothermal walls, bulk-flow hold, TVD3)",
-            "steps": nsteps, "ms_per_step": 1e3 * t / nsteps, "value": dof * 3 * nsteps / t, "unit": UNIT,
-            "max_abs_modal_diff_vs_golden": float(np.abs(D.modes() - z["modal"]).max())}
-    D.close()
-    if not args.no_cpu_baseline:
-        import oracle
-        from oracle import dgm_io
-        oracle.set_threads(os.cpu_count() or 1)
-        P = oracle.Problem(dgm_io.Mesh(3, mesh.verts, mesh.con, mesh.porder, mesh.qorder), oracle.NS3D,
-                           vis=float(inp["vis"]))
-        P.set_bc(rec)
-        P.set_hold_bulk(True)
-        P.set_state(P.backward(z["ic_modal"]))
-        t0 = time.perf_counter()
-        P.advance(3, float(inp["dt"]), nsteps)
-        tc = time.perf_counter() - t0
-        chan["cpu_oracle_ms_per_step"] = 1e3 * tc / nsteps
-        chan["cpu_oracle_cores"] = os.cpu_count() or 1
-    res["channel"] = chan
+        t = e0.elapsed_time(e1) / 1e3
+        nsteps = int(inp["Nt"])
+        dof = 5 * mesh.verts.shape[0] * 64
+        chan = {"workload": "runs/chan (NS 3-D channel, 512 hexes, p=3, isothermal walls, bulk-flow hold, TVD3)",
+                "steps": nsteps, "ms_per_step": 1e3 * t / nsteps, "value": dof * 3 * nsteps / t, "unit": UNIT,
+                "max_abs_modal_diff_vs_golden": float(np.abs(D.modes() - z["modal"]).max())}
+        D.close()
+        if not args.no_cpu_baseline:
+            import oracle
+            from oracle import dgm_io
+            oracle.set_threads(os.cpu_count() or 1)
+            P = oracle.Problem(dgm_io.Mesh(3, mesh.verts, mesh.con, mesh.porder, mesh.qorder), oracle.NS3D,
+                               vis=float(inp["vis"]))
+            P.set_bc(rec)
+            P.set_hold_bulk(True)
+            P.set_state(P.backward(z["ic_modal"]))
+            t0 = time.perf_counter()
+            P.advance(3, float(inp["dt"]), nsteps)
+            tc = time.perf_counter() - t0
+            chan["cpu_oracle_ms_per_step"] = 1e3 * tc / nsteps
+            chan["cpu_oracle_cores"] = os.cpu_count() or 1
+        res["channel"] = chan
     return res
 
 
@@ -490,6 +497,10 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    if args.only:
+        if rank == 0:
+            print(json.dumps(other_configs(dgm_b200, args, args.only)), flush=True)
+        return 0
     dist = None
     if world > 1:
         import datetime
