@@ -165,6 +165,7 @@ class Domain:
 
     def set_exchange_nccl(self, nccl_id: bytes):
         """NCCL communicator for the halo exchange (collective over the ranks)."""
+        _nccl_first()
         f = lib().dgmx_set_exchange_nccl
         f.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         self._check(f(self.h, bytes(nccl_id)))
@@ -456,8 +457,15 @@ def _mesh_struct(mesh):
     return m, [verts, con, por, qor]
 
 
+def _nccl_first():
+    # one libnccl.so.2 per process: PyTorch's, loaded before the engine
+    # resolves NCCL, so that a later PyTorch import finds the same library
+    import torch  # noqa: F401
+
+
 def nccl_unique_id() -> bytes:
     """A fresh NCCL unique id (rank 0 makes it and shares it with the others)."""
+    _nccl_first()
     buf = ctypes.create_string_buffer(128)
     f = lib().dgmx_nccl_unique_id
     f.argtypes = [ctypes.c_char_p]

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -31,9 +32,11 @@ cudaError_t dalloc(T **p, size_t n) {
   return cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * (n ? n : 1));
 }
 
-// NCCL entry points, resolved at first use from the libnccl.so.2 the process
-// already has (PyTorch loads one) or finds on the library path, so the
-// library has no link-time dependency on NCCL.
+// NCCL entry points, resolved at first use so the library has no link-time
+// dependency on NCCL: the file named by DGMX_NCCL_LIBRARY, else the
+// libnccl.so.2 the process already has, else the one on the library path.
+// Only one libnccl.so.2 can live in a process: a host that also uses another
+// NCCL user (PyTorch) loads that one first.
 struct NcclApi {
   bool ok = false;
   std::string why;
@@ -49,7 +52,9 @@ struct NcclApi {
 const NcclApi &nccl_api() {
   static NcclApi api = [] {
     NcclApi a;
-    void *h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_NOLOAD);
+    void *h = nullptr;
+    if (const char *path = std::getenv("DGMX_NCCL_LIBRARY")) h = dlopen(path, RTLD_NOW);
+    if (!h) h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_NOLOAD);
     if (!h) h = dlopen("libnccl.so.2", RTLD_NOW);
     if (!h) h = dlopen("libnccl.so", RTLD_NOW);
     if (!h) { a.why = "libnccl.so.2 not found"; return a; }

@@ -136,3 +136,14 @@ def test_halo_exchange_between_gloo_ranks(kind):
         pr.join(timeout=120)
         assert pr.exitcode == 0
     assert dict(result) == {0: 1, 1: 1}
+
+
+def test_nccl_resolution_keeps_torch_importable():
+    """The engine resolves NCCL lazily; making an id before the host's own
+    PyTorch import must not leave a different libnccl.so.2 in the process."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, %r); import dgm_b200; i = dgm_b200.nccl_unique_id(); "
+            "import torch; assert len(i) == 128" % os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
