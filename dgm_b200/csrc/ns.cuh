@@ -36,13 +36,20 @@ struct NsCfg {
   static constexpr int P2 = DIM == 3 ? Q * Q * L : 0;         // backward pass-2 size
   static constexpr int F1 = DIM == 3 ? L * Q * Q : L * Q;     // forward pass-1 size
   static constexpr int F2 = DIM == 3 ? L * L * Q : 0;         // forward pass-2 size
-  // ns_grad_kernel regions (per slot, doubles)
+  // fields per backward-transform batch: one slot's fields in two batches
+  // (at most 3 at a time) keep the transform scratch at the size the
+  // per-component passes need
+  static constexpr int NB1 = (EPB == 1 && NF > 3) ? 3 : NF;
+  // ns_grad_kernel regions (per slot, doubles); the modal input A is dead
+  // after the backward transform, so the primitive component Qc and its
+  // gradient Gd live in it
   struct Grad {
-    static constexpr int A = NF * LD, B = NF * QD, E = NFACE * NF * GF, E2 = NFACE * NF * GF;
-    static constexpr int Qc = QD, Gd = DIM * QD, Fc = NFACE * DIM * GF, LFc = cmax(NFACE * DIM * QF, DIM * F2);
-    static constexpr int S1 = cmax(cmax(NF * P1, DIM == 3 ? NFACE * DIM * Q * G : 0), DIM * F1);
-    static constexpr int S2 = cmax(cmax(NF * P2, DIM * F2), DIM * LD);
-    static constexpr int SLOT = A + B + E + E2 + Qc + Gd + Fc + LFc + S1 + S2;
+    static constexpr int Qc = QD, Gd = DIM * QD;
+    static constexpr int A = cmax(NF * LD, Qc + Gd), B = NF * QD, E = NFACE * NF * GF, E2 = NFACE * NF * GF;
+    static constexpr int Fc = NFACE * DIM * GF, LFc = cmax(NFACE * DIM * QF, DIM * F2);
+    static constexpr int S1 = cmax(cmax(NB1 * P1, DIM == 3 ? NFACE * DIM * Q * G : 0), DIM * F1);
+    static constexpr int S2 = cmax(cmax(NB1 * P2, DIM * F2), DIM * LD);
+    static constexpr int SLOT = A + B + E + E2 + Fc + LFc + S1 + S2;
     static constexpr size_t SMEM = (size_t)EPB * SLOT * 8 + (size_t)EPB * (sizeof(GeomClass) + NFACE * 16 + 16);
   };
   // ns_visc_kernel regions
@@ -56,6 +63,17 @@ struct NsCfg {
     static constexpr size_t SMEM = (size_t)EPB * SLOT * 8 + (size_t)EPB * (sizeof(GeomClass) + NFACE * 16 + 16);
     static_assert(NF * LD <= NG * QD, "modal input must fit in the gradient region");
   };
+  // CTAs per SM for a viscous kernel of smem bytes: the tile's register cap
+  // when it has one, else as many as shared memory holds while the register
+  // budget stays at 64 or more per thread
+  static constexpr int minb(size_t smem) {
+    if (C::MINB_REQ > 0) return C::MINB_REQ;
+    const int by_smem = (int)((228 * 1024) / (smem + 1024));
+    const int by_regs = 65536 / (NT * 64);
+    const int b = by_smem < by_regs ? by_smem : by_regs;
+    return b < 1 ? 1 : (b > 8 ? 8 : b);
+  }
+  static constexpr int GRAD_MINB = minb(Grad::SMEM), VISC_MINB = minb(Visc::SMEM);
 };
 
 // Primitive variables of one conserved state (src/Euler3d.cpp:1170-1182):
@@ -207,7 +225,7 @@ __device__ __forceinline__ void load_geo_slots(GeomClass *geo, FaceLink *lnk, in
 
 // ---------------------------------------------------------------- gradients
 template <class C, int PHYS, bool NODAL>
-__global__ void __launch_bounds__(C::NT, C::MINB) ns_grad_kernel(StageArgs a) {
+__global__ void __launch_bounds__(C::NT, NsCfg<C>::GRAD_MINB) ns_grad_kernel(StageArgs a) {
   using N = NsCfg<C>;
   using R = typename N::Grad;
   constexpr int DIM = C::DIM, NF = C::NF, Q = C::Q, L = C::L, EPB = C::EPB, QD = C::QD, GF = C::GF;
@@ -215,8 +233,9 @@ __global__ void __launch_bounds__(C::NT, C::MINB) ns_grad_kernel(StageArgs a) {
   extern __shared__ __align__(16) unsigned char smem_bytes[];
   double *smem_raw = reinterpret_cast<double *>(smem_bytes);
   double *A = smem_raw, *B = A + EPB * R::A, *E = B + EPB * R::B, *E2 = E + EPB * R::E;
-  double *Qc = E2 + EPB * R::E2, *Gd = Qc + EPB * R::Qc, *Fc = Gd + EPB * R::Gd, *LFc = Fc + EPB * R::Fc;
+  double *Fc = E2 + EPB * R::E2, *LFc = Fc + EPB * R::Fc;
   double *S1 = LFc + EPB * R::LFc, *S2 = S1 + EPB * R::S1;
+  double *Qc = A, *Gd = A + EPB * R::Qc;     // in the modal input, dead after the backward transform
   GeomClass *geo = reinterpret_cast<GeomClass *>(S2 + EPB * R::S2);
   FaceLink *lnk = reinterpret_cast<FaceLink *>(geo + EPB);
   int *eid = reinterpret_cast<int *>(lnk + EPB * NFACE);
@@ -232,7 +251,12 @@ __global__ void __launch_bounds__(C::NT, C::MINB) ns_grad_kernel(StageArgs a) {
   load_nbr_traces<C>(E2, a.Tin, lnk, eid, geo, a, tid);
   if constexpr (!NODAL) {
     __syncthreads();
-    backward_batch<C, NF>(A, B, S1, S2, tid);
+    if constexpr (N::NB1 == NF) {
+      backward_batch<C, NF>(A, B, S1, S2, tid);
+    } else {   // one slot: fields [0, NB1) then [NB1, NF)
+      backward_batch<C, N::NB1>(A, B, S1, S2, tid);
+      backward_batch<C, NF - N::NB1>(A + N::NB1 * LD, B + N::NB1 * QD, S1, S2, tid);
+    }
   }
   __syncthreads();
   for (int c = 0; c < NVC; ++c) {
@@ -299,7 +323,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) ns_grad_kernel(StageArgs a) {
 
 // ----------------------------------------------- stresses, traces, divergence
 template <class C, int PHYS, bool NODAL>
-__global__ void __launch_bounds__(C::NT, C::MINB) ns_visc_kernel(StageArgs a) {
+__global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(StageArgs a) {
   using N = NsCfg<C>;
   using R = typename N::Visc;
   constexpr int DIM = C::DIM, NF = C::NF, Q = C::Q, L = C::L, G = C::G, EPB = C::EPB, QD = C::QD;

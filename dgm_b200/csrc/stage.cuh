@@ -48,6 +48,7 @@ struct Cfg {
   using R = std::conditional_t<MIXED_, float, double>;
   static constexpr int DIM = phys_dim(PHYS), NF = phys_nf(PHYS);
   static constexpr int L = L_, Q = Q_, G = Q_ - 1, EPB = EPB_, MINB = MINB_ > 0 ? MINB_ : 1;
+  static constexpr int MINB_REQ = MINB_;   // 0: no register cap requested
   static constexpr int NFACE = 2 * DIM;
   static constexpr int LD = Pow<L, DIM>::v, QD = Pow<Q, DIM>::v;
   static constexpr int GF = Pow<G, DIM - 1>::v, QF = Pow<Q, DIM - 1>::v, LF = Pow<L, DIM - 1>::v;
