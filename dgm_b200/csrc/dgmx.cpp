@@ -398,10 +398,11 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
     if (p->precision != DGMX_FP64) { g_create_error = "boundary sides are supported in FP64"; return DGMX_ERR_UNSUPPORTED; }
     for (int t = 1; t <= bspec->ntypes; ++t) {
       const int k = bspec->kind[t];
-      if (!(k == DGMX_BC_SLIP_WALL && p->physics == DGMX_EULER3D) &&
-          !(k == DGMX_BC_ISOTHERMAL_WALL && p->physics == DGMX_NS3D)) {
+      const bool euler = p->physics == DGMX_EULER3D || p->physics == DGMX_EULER2D;
+      const bool ns = p->physics == DGMX_NS3D || p->physics == DGMX_NS2D;
+      if (!(k == DGMX_BC_SLIP_WALL && euler) && !(k == DGMX_BC_ISOTHERMAL_WALL && ns)) {
         g_create_error = "boundary kind " + std::to_string(k) +
-                         " is not built for this physics (Euler 3-D: slip wall; Navier-Stokes 3-D: isothermal wall)";
+                         " is not built for this physics (Euler: slip wall; Navier-Stokes: isothermal wall)";
         return DGMX_ERR_UNSUPPORTED;
       }
     }
@@ -707,14 +708,17 @@ dgmx_status dgmx_create_from_files(const char *root, const dgmx_params *params, 
       if (it != fc.bct.end()) { code = it->second.first; vals = it->second.second; }
       int k = 0;
       double pa = 0.0, pb = 0.0;
-      if (p.physics == DGMX_EULER3D && code.find("wall") != std::string::npos) {
-        k = DGMX_BC_SLIP_WALL;
-      } else if (p.physics == DGMX_EULER3D && code.empty() && r.tag == "W") {
-        k = DGMX_BC_SLIP_WALL;                 // default "W" (src/Euler3d.cpp:835)
-      } else if (p.physics == DGMX_NS3D && code == "isothermal_wall" && vals.size() >= 2) {
+      const bool euler = p.physics == DGMX_EULER3D || p.physics == DGMX_EULER2D;
+      const bool ns = p.physics == DGMX_NS3D || p.physics == DGMX_NS2D;
+      if (euler && code.find("wall") != std::string::npos) {
+        k = DGMX_BC_SLIP_WALL;                 // src/Euler.cpp:1241-1243, src/Euler3d.cpp:862-866
+      } else if (euler && code.empty() && r.tag == "W") {
+        k = DGMX_BC_SLIP_WALL;                 // default "W" (src/Euler.cpp:1208, src/Euler3d.cpp:835)
+      } else if (ns && code == "isothermal_wall" && vals.size() >= 2) {
         k = DGMX_BC_ISOTHERMAL_WALL; pa = vals[0]; pb = vals[1];
-      } else if (p.physics == DGMX_NS3D && code.empty() && r.tag == "W") {
-        k = DGMX_BC_ISOTHERMAL_WALL; pa = 1.0; pb = 20.34126984126985;   // src/Navier_Stokes3d.cpp:403-410
+      } else if (ns && code.empty() && r.tag == "W") {
+        // default "W" (src/Navier_Stokes.cpp:263-270, src/Navier_Stokes3d.cpp:403-410)
+        k = DGMX_BC_ISOTHERMAL_WALL; pa = 1.0; pb = 20.34126984126985;
       } else {
         g_create_error = std::string(root) + ".bc: boundary type '" + r.tag + "' (" +
                          (code.empty() ? "no .bct entry" : code) + ") is not built for this physics";

@@ -88,7 +88,6 @@ bool build_mesh(const dgmx_mesh &m, const Tables1D &t, HostMesh &out, std::strin
   // --- boundary sides (src/Field.cpp:4440-4460): the record replaces the
   // side's link; the side becomes master with no flips
   if (bcs && !bcs->empty()) {
-    if (dim != 3) { err = "mesh: boundary sides are supported on Hex meshes"; return false; }
     for (const BoundarySide &b : *bcs) {
       if (b.e < 0 || b.e >= ne || b.s < 0 || b.s >= nfaces || b.type < 1 || b.type > kMaxBcTypes) {
         err = "mesh: boundary record out of range";

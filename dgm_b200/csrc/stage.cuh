@@ -316,6 +316,24 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
 #pragma unroll
     for (int n = 0; n < NF; ++n) { Uo[n] = eo[n * EB]; Un[n] = tn[n * GF]; }
     const int bt = (gc.bc >> (4 * f)) & 15;
+    if constexpr (C::DIM == 2 && !C::MIXED && PHYS != DGMX_SHALLOW) {
+      if (bt) {
+        // boundary side, 2-D: the physics' own database serves the inviscid
+        // flux (virtual enforce_bc, src/Euler.cpp:313-316): the isothermal
+        // wall (src/Navier_StokesBC.hpp:47-65) or Euler::WallBC
+        // (src/EulerBC.hpp:43-62)
+        Un[0] = Uo[0];
+        if (a.bckind[bt] == DGMX_BC_ISOTHERMAL_WALL) {
+          Un[1] = T(0); Un[2] = T(0);
+          Un[3] = T(a.bcpar[bt][1] - 0.5) * Uo[0] * T(a.bcpar[bt][0]);
+        } else {
+          Un[1] = (Uo[1] * nm[1] - Uo[2] * nm[0]) * nm[1];
+          Un[2] = (Uo[2] * nm[0] - Uo[1] * nm[1]) * nm[0];
+          Un[3] = Uo[3] - T(0.5) * (Uo[1] * Uo[1] + Uo[2] * Uo[2]) / Uo[0] +
+                  T(0.5) * (Un[1] * Un[1] + Un[2] * Un[2]) / Un[0];
+        }
+      }
+    }
     if constexpr (C::DIM == 3 && !C::MIXED) {
       if (bt) {
         // boundary side: the neighbour is the Domain database's wall state,

@@ -43,14 +43,15 @@ enum { DGMX_FLUX_LF = 0, DGMX_FLUX_ROE = 1 };
 enum { DGMX_TVD3 = 3, DGMX_RK4 = 4, DGMX_LSRK14 = 14 };
 /* Arithmetic of the stage kernels. */
 enum { DGMX_FP64 = 0, DGMX_MIXED = 1 };
-/* Boundary kinds (3-D, FP64).  DGMX_BC_SLIP_WALL: Euler 3-D solid wall,
- * Euler3d::WallBC (src/Euler3d.cpp:862-903).  DGMX_BC_ISOTHERMAL_WALL:
- * Navier-Stokes 3-D wall with parameters (Tw, Eref); its inviscid flux sees
- * the slip wall of the Domain's BC database and its viscous terms
- * Navier_Stokes3d::Isothermal_WallBC (src/Navier_Stokes3d.hpp:25-48,
- * src/Navier_Stokes3d.cpp:472-513), as in the reference, where
- * Navier_Stokes3d keeps its own database beside the Domain's
- * (src/Navier_Stokes3d.hpp:83). */
+/* Boundary kinds (FP64).  DGMX_BC_SLIP_WALL: Euler solid wall,
+ * Euler::WallBC / Euler3d::WallBC (src/EulerBC.hpp:43-62,
+ * src/Euler3d.cpp:862-903).  DGMX_BC_ISOTHERMAL_WALL: Navier-Stokes wall
+ * with parameters (Tw, Eref), src/Navier_StokesBC.hpp:47-85,
+ * src/Navier_Stokes3d.cpp:472-513.  In 3-D its inviscid flux sees the slip
+ * wall of the Domain's BC database (Navier_Stokes3d keeps its own database
+ * beside the Domain's, src/Navier_Stokes3d.hpp:83, and Euler3d::convection
+ * calls Euler3d::enforce_bc); in 2-D the inviscid flux calls the virtual
+ * enforce_bc (src/Euler.cpp:313-316) and sees the isothermal wall too. */
 enum { DGMX_BC_SLIP_WALL = 1, DGMX_BC_ISOTHERMAL_WALL = 2 };
 
 typedef struct {
@@ -92,7 +93,7 @@ dgmx_status dgmx_create_from_files(const char *root, const dgmx_params *params, 
  * kind); bc_params two doubles per record (DGMX_BC_ISOTHERMAL_WALL: Tw,
  * Eref; ignored for the slip wall).  A record replaces the side's
  * connectivity link; a linked partner side must be named too.  At most 15
- * distinct (kind, parameters) pairs; FP64 only; 3-D only.
+ * distinct (kind, parameters) pairs; FP64 only; not for shallow water.
  * dgmx_create_from_files reads root.bc and root.bct the same way when they
  * exist, and switches the bulk-flow hold on when root.chn exists. */
 dgmx_status dgmx_create_with_boundaries(const dgmx_mesh *mesh, const dgmx_params *params, int nbc,

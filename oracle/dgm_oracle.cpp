@@ -977,7 +977,10 @@ static void lift_all(Problem &P, double *Fbase, int nfirst) {
 // Domain's database where every "*wall*" code is Euler3d::WallBC
 // (src/Euler3d.cpp:862-866), while the viscous terms call
 // Navier_Stokes3d::enforce_bc (src/Navier_Stokes3d.cpp:192, :457-461) and see
-// the isothermal wall.  So `viscous` selects the database:
+// the isothermal wall.  So in 3-D `viscous` selects the database.  The 2-D
+// inviscid flux calls the virtual enforce_bc (src/Euler.cpp:313-316, no
+// USE_EULER_BC in any build), so Navier-Stokes 2-D walls are isothermal in
+// both phases and Euler 2-D walls are Euler::WallBC (src/EulerBC.hpp:43-62):
 //   slip wall       B = (r, m - (m.n) n, rE - |m|^2/2r + |m_t|^2/2r)
 //                   (src/Euler3d.cpp:875-903)
 //   isothermal wall B = (r, 0, 0, 0, (Eref - 1/2) r Tw)
@@ -990,7 +993,20 @@ static void enforce_bc(Problem &P, bool viscous) {
     double *s[5], *g[5];
     for (int n = 0; n < P.nf; ++n) { s[n] = sfld(P, P.Us_s, n) + S.off; g[n] = sfld(P, P.Us_s, n) + G.off; }
     for (int i = 0; i < S.qtot; ++i) {
-      if (viscous && R.kind == BC_ISOTHERMAL_WALL) {
+      if (P.dim == 2) {
+        if (R.kind == BC_ISOTHERMAL_WALL) {   // src/Navier_StokesBC.hpp:47-65
+          g[0][i] = s[0][i];
+          g[1][i] = 0.0; g[2][i] = 0.0;
+          g[3][i] = (R.b - 0.5) * g[0][i] * R.a;
+        } else {                               // src/EulerBC.hpp:43-62
+          const double nx = S.nx[i], ny = S.ny[i];
+          g[0][i] = s[0][i];
+          g[1][i] = (s[1][i] * ny - s[2][i] * nx) * ny;
+          g[2][i] = (s[2][i] * nx - s[1][i] * ny) * nx;
+          g[3][i] = s[3][i] - 0.5 * (s[1][i] * s[1][i] + s[2][i] * s[2][i]) / s[0][i] +
+                    0.5 * (g[1][i] * g[1][i] + g[2][i] * g[2][i]) / g[0][i];
+        }
+      } else if (viscous && R.kind == BC_ISOTHERMAL_WALL) {
         g[0][i] = s[0][i];
         g[1][i] = 0.0; g[2][i] = 0.0; g[3][i] = 0.0;
         g[4][i] = (R.b - 0.5) * g[0][i] * R.a;
@@ -1543,6 +1559,7 @@ static void ns2d_diffusion(Problem &P, const double *Ub, double *Rb) {
   const size_t N = P.ntot;
   const double gPr = P.gamma / P.Pr, mu = P.vis;
   fill_all_sides(P, const_cast<double *>(Ub));
+  if (!P.bcs.empty()) enforce_bc(P, true);   // src/Navier_Stokes.cpp:124-125
   primitive_sides(P);
   average_flux(P, 1.0);
 #pragma omp parallel for schedule(static)
@@ -1584,6 +1601,7 @@ static void ns2d_diffusion(Problem &P, const double *Ub, double *Rb) {
     gradient_dir(E, ux.data(), wk.data(), 'x'); gradient_dir(E, uy.data(), ux.data(), 'y');
     for (int i = 0; i < n; ++i) F3[i] = wk[i] + ux[i];
   }
+  if (!P.bcs.empty()) enforce_flux_bc(P);
   average_flux(P, -1.0);
 #pragma omp parallel for schedule(static)
   for (int k = 0; k < P.ne; ++k)
@@ -1788,20 +1806,21 @@ void *ora_create(int dim, int ne, const double *verts, const int *porder,
   }
 }
 void ora_free(void *h) { delete (Problem *)h; }
-// Boundary sides (3-D only): nbc records (element, side, kind) with two
+// Boundary sides: nbc records (element, side, kind) with two
 // parameters each.  A record replaces the side's connectivity link; a
 // linked partner must be named too.  Returns 0, or -1 on a bad record.
 // Call once, before any state is set.
 int ora_set_bc(void *h, int nbc, const int *es_kind, const double *par) {
   auto *P = (Problem *)h;
-  if (P->dim != 3 || !P->bcs.empty()) return -1;
+  if (!P->bcs.empty()) return -1;
+  const int nsides = P->dim == 2 ? 4 : 6;
   size_t off = P->nstot;
   for (int b = 0; b < nbc; ++b) {
     const int e = es_kind[3 * b], s = es_kind[3 * b + 1], kind = es_kind[3 * b + 2];
-    if (e < 0 || e >= P->ne || s < 0 || s >= 6) return -1;
+    if (e < 0 || e >= P->ne || s < 0 || s >= nsides) return -1;
     if (kind != BC_SLIP_WALL && kind != BC_ISOTHERMAL_WALL) return -1;
-    if (kind == BC_ISOTHERMAL_WALL && P->physics != NS3D) return -1;
-    if (kind == BC_SLIP_WALL && P->physics != EULER3D) return -1;
+    if (kind == BC_ISOTHERMAL_WALL && P->physics != NS3D && P->physics != NS2D) return -1;
+    if (kind == BC_SLIP_WALL && P->physics != EULER3D && P->physics != EULER2D) return -1;
     Side &S = P->el[e].side[s];
     if (S.bc >= 0) return -1;
     S.master = true; S.bc = b;

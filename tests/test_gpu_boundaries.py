@@ -1,6 +1,7 @@
-"""GPU parity with boundary sides: Euler 3-D slip walls, Navier-Stokes 3-D
-isothermal walls and the channel's bulk-flow hold, through the C ABI, against
-the CPU oracle (which is pinned to the reference's runs/chan golden restart).
+"""GPU parity with boundary sides: Euler 2-D/3-D slip walls, Navier-Stokes
+2-D/3-D isothermal walls and the channel's bulk-flow hold, through the C ABI,
+against the CPU oracle (which is pinned to the reference's runs/chan golden
+restart).
 
 Bar: relative L2 <= 1e-12 against the oracle; the channel run also passes
 dgm_diff against the golden restart at the case's own tolerances.
@@ -83,6 +84,62 @@ def test_walls_match_oracle(case):
     assert rel(D.state(), P.state()) < 1e-12
     # the walls matter: the periodic run of the same case differs
     Q = oracle.Problem(dgm_io.Mesh(3, m.verts, m.con, m.porder, m.qorder), phys, flux=flux, vis=vis)
+    Q.set_state(U0)
+    Q.advance(inttype, dt, steps)
+    assert rel(Q.state(), P.state()) > 1e-9
+
+
+def wall_records_2d(n, kind, a=0.0, b=0.0):
+    """y- sides of the bottom row and y+ sides of the top row of an
+    n[0] x n[1] Quad box (element index i + nx j; Quad sides 0 y-, 2 y+)."""
+    nx, ny = n
+    rec = []
+    for i in range(nx):
+        rec.append((i, 0, kind, a, b))
+        rec.append((i + nx * (ny - 1), 2, kind, a, b))
+    return rec
+
+
+def channel_ic_2d(x, y):
+    """A wall-bounded perturbed shear flow on [0,2pi] x [0,2] (Mach ~ 0.1)."""
+    u = 1.5 * y * (2.0 - y) + 0.2 * np.sin(x) * np.sin(np.pi * y / 2.0)
+    v = 0.1 * np.cos(x) * np.sin(np.pi * y / 2.0)
+    r = 1.0 + 0.01 * np.cos(x) * np.cos(y)
+    p = 71.43 + 0.05 * np.sin(x)
+    return np.stack([r, r * u, r * v, p / 0.4 + 0.5 * r * (u * u + v * v)])
+
+
+CASES_2D = [
+    # name, physics, n, p, flux, inttype, dt, steps, vis, kind, (a, b)
+    ("euler2d-slip-lf-lsrk14", 1, (4, 3), 4, "laxfriedrichs", 14, 0.002, 2, 0.0, BC_SLIP_WALL, (0, 0)),
+    ("euler2d-slip-roe-tvd3", 1, (3, 4), 3, "roe", 3, 0.002, 3, 0.0, BC_SLIP_WALL, (0, 0)),
+    ("ns2d-isothermal-rk4", 2, (4, 3), 3, "laxfriedrichs", 4, 0.001, 3, 0.02, BC_ISOTHERMAL_WALL, (1.0, 178.575)),
+    ("ns2d-isothermal-lsrk14-p5", 2, (3, 3), 5, "laxfriedrichs", 14, 0.0005, 2, 0.01, BC_ISOTHERMAL_WALL,
+     (1.1, 178.575)),
+]
+
+
+@pytest.mark.parametrize("case", CASES_2D, ids=[c[0] for c in CASES_2D])
+def test_walls_2d_match_oracle(case):
+    import dgm_b200
+    _, phys, n, p, flux, inttype, dt, steps, vis, kind, (a, b) = case
+    m = dgm_b200.meshgen.box(2, n, (0.0, 0.0), (2 * np.pi, 2.0), p)
+    rec = wall_records_2d(n, kind, a, b)
+    P = oracle.Problem(dgm_io.Mesh(2, m.verts, m.con, m.porder, m.qorder), phys, flux=flux, vis=vis)
+    P.set_bc(rec)
+    D = dgm_b200.Domain(m, phys, flux=flux, inttype=inttype, vis=vis, boundaries=rec)
+    x, y, _ = P.coords()
+    f = channel_ic_2d(x, y)
+    U0 = P.project(f)
+    F_o, F_g = P.rhs(U0), D.time_derivative(U0)
+    scale = np.sqrt((F_o ** 2).sum()) + np.sqrt((U0 ** 2).sum())
+    assert np.sqrt(((F_g - F_o) ** 2).sum()) / scale < 1e-12
+    P.set_state(U0)
+    D.set_state(f)
+    assert P.advance(inttype, dt, steps) == 0
+    D.advance(dt, steps)
+    assert rel(D.state(), P.state()) < 1e-12
+    Q = oracle.Problem(dgm_io.Mesh(2, m.verts, m.con, m.porder, m.qorder), phys, flux=flux, vis=vis)
     Q.set_state(U0)
     Q.advance(inttype, dt, steps)
     assert rel(Q.state(), P.state()) > 1e-9
