@@ -97,7 +97,7 @@ def kernel_list():
 
 
 # boundary kinds (include/dgmx.h)
-BC_SLIP_WALL, BC_ISOTHERMAL_WALL = 1, 2
+BC_SLIP_WALL, BC_ISOTHERMAL_WALL, BC_STATE, BC_SUBSONIC_OUTFLOW, BC_SUPERSONIC_OUTFLOW = 1, 2, 3, 4, 5
 
 
 class Domain:
@@ -106,10 +106,11 @@ class Domain:
     def __init__(self, mesh, physics: int, flux: str = "laxfriedrichs", inttype: int = LSRK14,
                  gamma: float = 1.4, vis: float = 0.0, Pr: float = 0.72, sw_balance: bool = True,
                  device: int = 0, precision: int = 0, boundaries=None, bulk_hold: bool = False):
-        """boundaries: optional (element, side, kind, a, b) records
-        (BC_SLIP_WALL for Euler 3-D; BC_ISOTHERMAL_WALL with a = Tw,
-        b = Eref for Navier-Stokes 3-D); bulk_hold: the channel's bulk-flow
-        hold (Navier-Stokes 3-D)."""
+        """boundaries: optional (element, side, kind, params...) records
+        with up to five parameters: BC_SLIP_WALL (Euler), BC_ISOTHERMAL_WALL
+        (Tw, Eref; Navier-Stokes), BC_STATE (the conserved values),
+        BC_SUBSONIC_OUTFLOW (Mref; 2-D), BC_SUPERSONIC_OUTFLOW (2-D);
+        bulk_hold: the channel's bulk-flow hold (Navier-Stokes 3-D)."""
         self._keep = []
         verts = np.ascontiguousarray(mesh.verts, dtype=np.float64)
         con = np.ascontiguousarray(mesh.con, dtype=np.int32)
@@ -126,9 +127,11 @@ class Domain:
         if boundaries is None:
             st = lib().dgmx_create(ctypes.byref(m), ctypes.byref(p), ctypes.byref(h))
         else:
-            r = np.asarray(boundaries, dtype=np.float64).reshape(-1, 5)
+            r = np.zeros((len(boundaries), 8))
+            for i, rec in enumerate(boundaries):
+                r[i, :len(rec)] = rec
             sides = np.ascontiguousarray(r[:, :3].astype(np.int32))
-            par = np.ascontiguousarray(r[:, 3:5])
+            par = np.ascontiguousarray(r[:, 3:8])
             f = lib().dgmx_create_with_boundaries
             f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                           ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]

@@ -108,7 +108,7 @@ struct dgmx_domain {
   // boundary types 1..nbct (kind, two parameters) and the bulk-flow hold
   int nbct = 0;
   int bckind[kMaxBcTypes + 1] = {};
-  double bcpar[kMaxBcTypes + 1][2] = {};
+  double bcpar[kMaxBcTypes + 1][5] = {};
   bool hold = false;
   double *R0 = nullptr, *cbar = nullptr;                 // hold: [e][n] constant coefficients, [n] means
   // element partition: ghost slots in the trace buffers and the halo
@@ -155,7 +155,7 @@ struct dgmx_domain {
     a.uref = uref;
     for (int t = 0; t <= kMaxBcTypes; ++t) {
       a.bckind[t] = bckind[t];
-      a.bcpar[t][0] = bcpar[t][0]; a.bcpar[t][1] = bcpar[t][1];
+      for (int k = 0; k < 5; ++k) a.bcpar[t][k] = bcpar[t][k];
     }
     return a;
   }
@@ -367,16 +367,19 @@ struct BoundarySpec {
   std::vector<BoundarySide> sides;
   int ntypes = 0;
   int kind[kMaxBcTypes + 1] = {};
-  double par[kMaxBcTypes + 1][2] = {};
+  double par[kMaxBcTypes + 1][5] = {};
   bool hold = false;
-  // type index of (kind, a, b), added on first use; 0 when the table is full
-  int type_of(int k, double a, double b) {
-    if (k == DGMX_BC_SLIP_WALL) a = b = 0.0;
+  // type index of (kind, parameters), added on first use; 0 when the table is full
+  int type_of(int k, const double *v) {
+    double w[5] = {0, 0, 0, 0, 0};
+    const int np = k == DGMX_BC_ISOTHERMAL_WALL ? 2 : (k == DGMX_BC_STATE ? 5 : (k == DGMX_BC_SUBSONIC_OUTFLOW ? 1 : 0));
+    for (int i = 0; i < np; ++i) w[i] = v[i];
     for (int t = 1; t <= ntypes; ++t)
-      if (kind[t] == k && par[t][0] == a && par[t][1] == b) return t;
+      if (kind[t] == k && std::equal(w, w + 5, par[t])) return t;
     if (ntypes == kMaxBcTypes) return 0;
     ++ntypes;
-    kind[ntypes] = k; par[ntypes][0] = a; par[ntypes][1] = b;
+    kind[ntypes] = k;
+    std::copy(w, w + 5, par[ntypes]);
     return ntypes;
   }
 };
@@ -400,16 +403,19 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
       const int k = bspec->kind[t];
       const bool euler = p->physics == DGMX_EULER3D || p->physics == DGMX_EULER2D;
       const bool ns = p->physics == DGMX_NS3D || p->physics == DGMX_NS2D;
-      if (!(k == DGMX_BC_SLIP_WALL && euler) && !(k == DGMX_BC_ISOTHERMAL_WALL && ns)) {
+      const bool outflow = k == DGMX_BC_SUBSONIC_OUTFLOW || k == DGMX_BC_SUPERSONIC_OUTFLOW;
+      if (!(k == DGMX_BC_SLIP_WALL && euler) && !(k == DGMX_BC_ISOTHERMAL_WALL && ns) &&
+          !(k == DGMX_BC_STATE && (euler || ns)) && !(outflow && (euler || ns) && m->dim == 2)) {
         g_create_error = "boundary kind " + std::to_string(k) +
-                         " is not built for this physics (Euler: slip wall; Navier-Stokes: isothermal wall)";
+                         " is not built for this physics (Euler: slip wall; Navier-Stokes: isothermal wall; both:"
+                         " fixed state, and the outflows in 2-D)";
         return DGMX_ERR_UNSUPPORTED;
       }
     }
     d->nbct = bspec->ntypes;
     for (int t = 0; t <= kMaxBcTypes; ++t) {
       d->bckind[t] = bspec->kind[t];
-      d->bcpar[t][0] = bspec->par[t][0]; d->bcpar[t][1] = bspec->par[t][1];
+      for (int k = 0; k < 5; ++k) d->bcpar[t][k] = bspec->par[t][k];
     }
   }
   if (bspec && bspec->hold) {
@@ -602,11 +608,11 @@ dgmx_status dgmx_create_with_boundaries(const dgmx_mesh *mesh, const dgmx_params
     BoundarySpec b;
     for (int i = 0; i < nbc; ++i) {
       const int k = bc_sides[3 * i + 2];
-      if (k != DGMX_BC_SLIP_WALL && k != DGMX_BC_ISOTHERMAL_WALL) {
+      if (k < DGMX_BC_SLIP_WALL || k > DGMX_BC_SUPERSONIC_OUTFLOW) {
         g_create_error = "unknown boundary kind " + std::to_string(k);
         return DGMX_ERR_ARGUMENT;
       }
-      const int t = b.type_of(k, bc_params[2 * i], bc_params[2 * i + 1]);
+      const int t = b.type_of(k, bc_params + 5 * i);
       if (!t) { g_create_error = "more than 15 distinct boundary types"; return DGMX_ERR_UNSUPPORTED; }
       b.sides.push_back(BoundarySide{bc_sides[3 * i], bc_sides[3 * i + 1], t});
     }
@@ -707,10 +713,26 @@ dgmx_status dgmx_create_from_files(const char *root, const dgmx_params *params, 
       std::vector<double> vals;
       if (it != fc.bct.end()) { code = it->second.first; vals = it->second.second; }
       int k = 0;
-      double pa = 0.0, pb = 0.0;
+      double pa = 0.0, pb = 0.0, st[5] = {0, 0, 0, 0, 0};
       const bool euler = p.physics == DGMX_EULER3D || p.physics == DGMX_EULER2D;
       const bool ns = p.physics == DGMX_NS3D || p.physics == DGMX_NS2D;
-      if (euler && code.find("wall") != std::string::npos) {
+      const int nfp = nfields_of(p.physics);
+      if ((euler || ns) && code == "state" && (int)vals.size() == nfp) {
+        k = DGMX_BC_STATE;                     // StateBC(tag, in, nf): src/BC.hpp:184-193
+        for (int i = 0; i < nfp; ++i) st[i] = vals[i];
+      } else if ((euler || ns) && code.empty() && r.tag == "S") {
+        // default "S": Ma 0.3 uniform flow (src/Euler.cpp:1202-1207, src/Euler3d.cpp:828-834,
+        // src/Navier_Stokes.cpp:263-269, src/Navier_Stokes3d.cpp:402-409)
+        k = DGMX_BC_STATE;
+        st[0] = 1.0; st[1] = 1.0; st[nfp - 1] = 20.34126984126985;
+      } else if (fc.dim == 2 && (euler || ns) && code.find("outflow") != std::string::npos && vals.size() >= 1 &&
+                 (code.find("subsonicoutflow") != std::string::npos ||
+                  code.find("supersonicoutflow") != std::string::npos)) {
+        // both codes build SubsonicOutflowBC (src/Euler.cpp:1253-1258, src/Navier_Stokes.cpp:348-354)
+        k = DGMX_BC_SUBSONIC_OUTFLOW; st[0] = vals[0];
+      } else if (fc.dim == 2 && euler && code.empty() && r.tag == "O") {
+        k = DGMX_BC_SUPERSONIC_OUTFLOW;        // default "O" (src/Euler.cpp:1209)
+      } else if (euler && code.find("wall") != std::string::npos) {
         k = DGMX_BC_SLIP_WALL;                 // src/Euler.cpp:1241-1243, src/Euler3d.cpp:862-866
       } else if (euler && code.empty() && r.tag == "W") {
         k = DGMX_BC_SLIP_WALL;                 // default "W" (src/Euler.cpp:1208, src/Euler3d.cpp:835)
@@ -724,7 +746,8 @@ dgmx_status dgmx_create_from_files(const char *root, const dgmx_params *params, 
                          (code.empty() ? "no .bct entry" : code) + ") is not built for this physics";
         return DGMX_ERR_UNSUPPORTED;
       }
-      const int t = b.type_of(k, pa, pb);
+      if (k == DGMX_BC_ISOTHERMAL_WALL) { st[0] = pa; st[1] = pb; }
+      const int t = b.type_of(k, st);
       if (!t) { g_create_error = "more than 15 distinct boundary types"; return DGMX_ERR_UNSUPPORTED; }
       b.sides.push_back(BoundarySide{r.e, r.s, t});
     }

@@ -232,7 +232,7 @@ struct StageArgs {
   double *Pv;             // projected viscous divergence, modal [e][field-1][L^d]
   // boundary types t = 1..15 (GeomClass::bc): kind (DGMX_BC_*) and parameters
   int bckind[kMaxBcTypes + 1];
-  double bcpar[kMaxBcTypes + 1][2];
+  double bcpar[kMaxBcTypes + 1][5];
   // if set, the constant-mode coefficient of every field's final projected
   // RHS, [e][field] (bulk-flow hold)
   double *R0;

@@ -98,10 +98,9 @@ __device__ __forceinline__ void primitive(const double *U, double *q) {
 }
 
 // Gather the neighbour's state traces into face-major smem E2 in the own
-// point order.  A boundary side's neighbour is its ghost state
-// (Navier_Stokes3d::enforce_bc, src/Navier_Stokes3d.cpp:457-461): for the
-// isothermal wall B = (r, 0, 0, 0, (Eref - 1/2) r Tw) from the own trace
-// (src/Navier_Stokes3d.cpp:472-494).
+// point order.  A boundary side's neighbour is its ghost state in the
+// viscous BC database (Navier_Stokes3d::enforce_bc,
+// src/Navier_Stokes3d.cpp:457-461; ghost_state) made from the own trace.
 template <class C>
 __device__ __forceinline__ void load_nbr_traces(double *E2, const double *T, const FaceLink *lnk, const int *eid,
                                                 const GeomClass *geo, const StageArgs &a, int tid) {
@@ -113,11 +112,15 @@ __device__ __forceinline__ void load_nbr_traces(double *E2, const double *T, con
     if (eid[s] >= 0) {
       const FaceLink lk = lnk[s * NFACE + f];
       const int bt = (geo[s].bc >> (4 * f)) & 15;
-      if (bt && a.bckind[bt] == DGMX_BC_ISOTHERMAL_WALL && n > 0) {
-        const double r = T[((size_t)(lk.elem * NFACE + lk.face) * NF) * GF + a.perm[lk.perm + g]];
-        v = n == NF - 1 ? (a.bcpar[bt][1] - 0.5) * r * a.bcpar[bt][0] : 0.0;
+      const double *t = T + ((size_t)(lk.elem * NFACE + lk.face) * NF) * GF + a.perm[lk.perm + g];
+      if (bt) {
+        double Uo[5], Un[5];
+#pragma unroll
+        for (int k = 0; k < NF; ++k) Uo[k] = t[k * GF];
+        ghost_state<C::DIM, NF>(a.bckind[bt], a.bcpar[bt], Uo, geo[s].onrm[f], true, Un);
+        v = Un[n];
       } else {
-        v = T[((size_t)(lk.elem * NFACE + lk.face) * NF + n) * GF + a.perm[lk.perm + g]];
+        v = t[n * GF];
       }
     }
     E2[w] = v;

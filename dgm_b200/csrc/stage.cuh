@@ -296,6 +296,57 @@ __device__ __forceinline__ typename C::R *trace_out(const StageArgs &a) {
 
 // Numerical flux on all face points; E holds own traces on entry and
 // (F^ - F).J on exit.  Neighbour traces come from Tin.
+// Ghost state of a boundary side from the side's own state Uo and outward
+// unit normal n (Domain::enforce_bc looping BC::apply).  `viscous` selects
+// the database: Navier_Stokes3d keeps its own beside the Domain's
+// (src/Navier_Stokes3d.hpp:83) and Euler3d::convection reads the Domain's
+// (src/Euler3d.cpp:476), where every "*wall*" code is Euler3d::WallBC; the
+// 2-D inviscid flux calls the virtual enforce_bc (src/Euler.cpp:313-316) and
+// sees the physics' own database.
+//   slip wall          m -> m - (m.n) n, energy with the new kinetic energy
+//                      (src/Euler3d.cpp:875-903, src/EulerBC.hpp:43-62)
+//   isothermal wall    (r, 0, [0,] 0, (Eref - 1/2) r Tw), par = (Tw, Eref)
+//                      (src/Navier_Stokes3d.cpp:472-494, src/Navier_StokesBC.hpp:47-65)
+//   state              par (StateBC::apply, src/BC.cpp:17-28)
+//   subsonic outflow   r, m kept, pressure of Mach par[0] (src/EulerBC.hpp:138-167)
+//   supersonic outflow the own state (src/EulerBC.hpp:214-241)
+template <int DIM, int NF>
+__device__ __forceinline__ void ghost_state(int kind, const double *par, const double *Uo, const double *n,
+                                            bool viscous, double *Un) {
+  if (kind == DGMX_BC_STATE) {
+#pragma unroll
+    for (int k = 0; k < NF; ++k) Un[k] = par[k];
+  } else if (kind == DGMX_BC_SUPERSONIC_OUTFLOW) {
+#pragma unroll
+    for (int k = 0; k < NF; ++k) Un[k] = Uo[k];
+  } else if (kind == DGMX_BC_SUBSONIC_OUTFLOW && DIM == 2) {
+    const double gam = 1.4, Mref = par[0];
+    const double Eref = 1.0 / (gam * (gam - 1.0) * (Mref * Mref)) + 0.5;
+    const double pref = (gam - 1.0) * (Eref - 0.5 * (1.0 - 0.0));
+    const double rl = Uo[0], ml = Uo[1], nl = Uo[2];
+    const double ul = ml / rl, vl = nl / rl;
+    Un[0] = rl; Un[1] = ml; Un[2] = nl;
+    Un[3] = pref / (gam - 1.0) + 0.5 * (ml * ul + nl * vl);
+  } else if (kind == DGMX_BC_ISOTHERMAL_WALL && (viscous || DIM == 2)) {
+    Un[0] = Uo[0];
+#pragma unroll
+    for (int k = 1; k < NF - 1; ++k) Un[k] = 0.0;
+    Un[NF - 1] = (par[1] - 0.5) * Uo[0] * par[0];
+  } else if constexpr (DIM == 3) {   // slip wall (and the 3-D isothermal wall's inviscid side)
+    double up = Uo[1], vp = Uo[2], wp = Uo[3];
+    const double dot = up * n[0] + vp * n[1] + wp * n[2];
+    up = up - dot * n[0]; vp = vp - dot * n[1]; wp = wp - dot * n[2];
+    Un[0] = Uo[0]; Un[1] = up; Un[2] = vp; Un[3] = wp;
+    Un[4] = Uo[4] - 0.5 * (Uo[1] * Uo[1] + Uo[2] * Uo[2] + Uo[3] * Uo[3]) / Uo[0] +
+            0.5 * (up * up + vp * vp + wp * wp) / Un[0];
+  } else {
+    Un[0] = Uo[0];
+    Un[1] = (Uo[1] * n[1] - Uo[2] * n[0]) * n[1];
+    Un[2] = (Uo[2] * n[0] - Uo[1] * n[1]) * n[0];
+    Un[3] = Uo[3] - 0.5 * (Uo[1] * Uo[1] + Uo[2] * Uo[2]) / Uo[0] + 0.5 * (Un[1] * Un[1] + Un[2] * Un[2]) / Un[0];
+  }
+}
+
 template <class C, int PHYS>
 __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &a, int tid) {
   using T = typename C::R;
@@ -316,37 +367,10 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
 #pragma unroll
     for (int n = 0; n < NF; ++n) { Uo[n] = eo[n * EB]; Un[n] = tn[n * GF]; }
     const int bt = (gc.bc >> (4 * f)) & 15;
-    if constexpr (C::DIM == 2 && !C::MIXED && PHYS != DGMX_SHALLOW) {
-      if (bt) {
-        // boundary side, 2-D: the physics' own database serves the inviscid
-        // flux (virtual enforce_bc, src/Euler.cpp:313-316): the isothermal
-        // wall (src/Navier_StokesBC.hpp:47-65) or Euler::WallBC
-        // (src/EulerBC.hpp:43-62)
-        Un[0] = Uo[0];
-        if (a.bckind[bt] == DGMX_BC_ISOTHERMAL_WALL) {
-          Un[1] = T(0); Un[2] = T(0);
-          Un[3] = T(a.bcpar[bt][1] - 0.5) * Uo[0] * T(a.bcpar[bt][0]);
-        } else {
-          Un[1] = (Uo[1] * nm[1] - Uo[2] * nm[0]) * nm[1];
-          Un[2] = (Uo[2] * nm[0] - Uo[1] * nm[1]) * nm[0];
-          Un[3] = Uo[3] - T(0.5) * (Uo[1] * Uo[1] + Uo[2] * Uo[2]) / Uo[0] +
-                  T(0.5) * (Un[1] * Un[1] + Un[2] * Un[2]) / Un[0];
-        }
-      }
-    }
-    if constexpr (C::DIM == 3 && !C::MIXED) {
-      if (bt) {
-        // boundary side: the neighbour is the Domain database's wall state,
-        // Euler3d::WallBC (src/Euler3d.cpp:875-903), for both the Euler slip
-        // wall and the Navier-Stokes isothermal wall (whose inviscid flux
-        // reads the Domain's database, src/Euler3d.cpp:476)
-        T up = Uo[1], vp = Uo[2], wp = Uo[3];
-        const T dot = up * nm[0] + vp * nm[1] + wp * nm[2];
-        up = up - dot * nm[0]; vp = vp - dot * nm[1]; wp = wp - dot * nm[2];
-        Un[0] = Uo[0]; Un[1] = up; Un[2] = vp; Un[3] = wp;
-        Un[4] = Uo[4] - T(0.5) * (Uo[1] * Uo[1] + Uo[2] * Uo[2] + Uo[3] * Uo[3]) / Uo[0] +
-                T(0.5) * (up * up + vp * vp + wp * wp) / Un[0];
-      }
+    if constexpr (!C::MIXED && PHYS != DGMX_SHALLOW) {
+      // boundary side: the neighbour is the ghost state of the database the
+      // inviscid flux reads (see ghost_state)
+      if (bt) ghost_state<C::DIM, C::NF>(a.bckind[bt], a.bcpar[bt], Uo, nm, false, Un);
     }
     const bool master = (gc.master >> f) & 1;
     const T jr = T(gc.jr[f]);

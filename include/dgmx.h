@@ -52,7 +52,14 @@ enum { DGMX_FP64 = 0, DGMX_MIXED = 1 };
  * beside the Domain's, src/Navier_Stokes3d.hpp:83, and Euler3d::convection
  * calls Euler3d::enforce_bc); in 2-D the inviscid flux calls the virtual
  * enforce_bc (src/Euler.cpp:313-316) and sees the isothermal wall too. */
-enum { DGMX_BC_SLIP_WALL = 1, DGMX_BC_ISOTHERMAL_WALL = 2 };
+/* DGMX_BC_STATE: fixed conserved state (StateBC, src/BC.cpp:17-42), any
+ * Euler/Navier-Stokes physics, parameters = the nf values.  2-D only:
+ * DGMX_BC_SUBSONIC_OUTFLOW (density and momentum kept, pressure of Mach
+ * parameter 0 with gamma 1.4, src/EulerBC.hpp:114-167) and
+ * DGMX_BC_SUPERSONIC_OUTFLOW (the own state, src/EulerBC.hpp:199-241).
+ * Every kind's viscous flux is the element's own (apply_flux: B = -S). */
+enum { DGMX_BC_SLIP_WALL = 1, DGMX_BC_ISOTHERMAL_WALL = 2, DGMX_BC_STATE = 3, DGMX_BC_SUBSONIC_OUTFLOW = 4,
+       DGMX_BC_SUPERSONIC_OUTFLOW = 5 };
 
 typedef struct {
   int dim;               /* 2 (Quad) or 3 (Hex)                              */
@@ -90,12 +97,15 @@ dgmx_status dgmx_create_from_files(const char *root, const dgmx_params *params, 
 /* dgmx_create for a mesh with boundary sides (Field::initialize_bc,
  * src/Field.cpp:4426-4460, with the records of root.bc read by
  * src/Field.cpp:4469-4490).  bc_sides holds nbc records (element, side,
- * kind); bc_params two doubles per record (DGMX_BC_ISOTHERMAL_WALL: Tw,
- * Eref; ignored for the slip wall).  A record replaces the side's
+ * kind); bc_params five doubles per record (DGMX_BC_ISOTHERMAL_WALL: Tw,
+ * Eref; DGMX_BC_STATE: the conserved values; DGMX_BC_SUBSONIC_OUTFLOW:
+ * Mref; unused entries ignored).  A record replaces the side's
  * connectivity link; a linked partner side must be named too.  At most 15
  * distinct (kind, parameters) pairs; FP64 only; not for shallow water.
  * dgmx_create_from_files reads root.bc and root.bct the same way when they
- * exist, and switches the bulk-flow hold on when root.chn exists. */
+ * exist (codes state, *wall*, isothermal_wall, subsonicoutflow,
+ * supersonicoutflow and the default tags S, W, O as each physics' databases
+ * define them), and switches the bulk-flow hold on when root.chn exists. */
 dgmx_status dgmx_create_with_boundaries(const dgmx_mesh *mesh, const dgmx_params *params, int nbc,
                                         const int *bc_sides, const double *bc_params, dgmx_domain **out);
 

@@ -163,12 +163,15 @@ class Problem:
         return lib().ora_advance(self.h, inttype, dt, nsteps)
 
     def set_bc(self, records):
-        """Boundary sides: records of (eid, sid, kind, a, b); kind 1 is the
-        Euler 3-D slip wall, 2 the Navier-Stokes 3-D isothermal wall with
-        a = Tw, b = Eref."""
-        r = np.asarray(records, dtype=np.float64).reshape(-1, 5)
+        """Boundary sides: records (eid, sid, kind, params...) with up to five
+        parameters; kind 1 slip wall (Euler), 2 isothermal wall (Tw, Eref;
+        Navier-Stokes), 3 fixed state (the conserved values), 4 subsonic
+        outflow (Mref; 2-D), 5 supersonic outflow (2-D)."""
+        r = np.zeros((len(records), 8))
+        for i, rec in enumerate(records):
+            r[i, :len(rec)] = rec
         esk = np.ascontiguousarray(r[:, :3].astype(np.int32))
-        par = np.ascontiguousarray(r[:, 3:5])
+        par = np.ascontiguousarray(r[:, 3:8])
         if lib().ora_set_bc(self.h, len(r), _ip(esk), _dp(par)) != 0:
             raise ValueError("oracle: bad boundary record")
 

@@ -675,7 +675,7 @@ struct Problem {
   // boundary sides (src/Boundary.cpp:25-75, src/Field.cpp:4426-4460): the
   // record names the element side, the BC kind and its two parameters; the
   // ghost side gs[b] is the clone that holds the boundary state
-  struct BCRec { int e, s, kind; double a, b; };
+  struct BCRec { int e, s, kind; double a, b, v[5]; };   // a, b = v[0], v[1]
   std::vector<BCRec> bcs;
   std::vector<Side> gs;
   bool hold_bulk = false;          // Channel::holdBulkMassFlow (src/Channel.hpp:116-163)
@@ -685,7 +685,8 @@ struct Problem {
 // and the Navier-Stokes 3-D isothermal wall (slip-wall state in the inviscid
 // flux, Navier_Stokes3d::Isothermal_WallBC in the viscous terms,
 // src/Navier_Stokes3d.cpp:472-513)
-enum BCKind { BC_SLIP_WALL = 1, BC_ISOTHERMAL_WALL = 2 };
+enum BCKind { BC_SLIP_WALL = 1, BC_ISOTHERMAL_WALL = 2, BC_STATE = 3, BC_SUBSONIC_OUTFLOW = 4,
+              BC_SUPERSONIC_OUTFLOW = 5 };
 
 // The side a master side is paired with: the neighbour's side, or for a
 // boundary side its ghost clone (src/Field.cpp:4451).
@@ -985,6 +986,8 @@ static void lift_all(Problem &P, double *Fbase, int nfirst) {
 //                   (src/Euler3d.cpp:875-903)
 //   isothermal wall B = (r, 0, 0, 0, (Eref - 1/2) r Tw)
 //                   (src/Navier_Stokes3d.cpp:472-494; a = Tw, b = Eref)
+// and in every database: the fixed state B = v (StateBC), and in 2-D the
+// outflows (B = S; or the pressure set from Mach Mref = v[0]).
 static void enforce_bc(Problem &P, bool viscous) {
   for (size_t b = 0; b < P.bcs.size(); ++b) {
     const Problem::BCRec &R = P.bcs[b];
@@ -993,7 +996,19 @@ static void enforce_bc(Problem &P, bool viscous) {
     double *s[5], *g[5];
     for (int n = 0; n < P.nf; ++n) { s[n] = sfld(P, P.Us_s, n) + S.off; g[n] = sfld(P, P.Us_s, n) + G.off; }
     for (int i = 0; i < S.qtot; ++i) {
-      if (P.dim == 2) {
+      if (R.kind == BC_STATE) {                // StateBC::apply, src/BC.cpp:17-28
+        for (int n = 0; n < P.nf; ++n) g[n][i] = R.v[n];
+      } else if (R.kind == BC_SUPERSONIC_OUTFLOW) {   // src/EulerBC.hpp:214-241
+        for (int n = 0; n < P.nf; ++n) g[n][i] = s[n][i];
+      } else if (R.kind == BC_SUBSONIC_OUTFLOW) {     // src/EulerBC.hpp:138-167 (gamma 1.4 fixed)
+        const double gam = 1.4, Mref = R.v[0];
+        const double Eref = 1.0 / (gam * (gam - 1.0) * std::pow(Mref, 2)) + 0.5;
+        const double pref = (gam - 1.0) * (Eref - 0.5 * (1.0 - 0.0));
+        const double rl = s[0][i], ml = s[1][i], nl = s[2][i];
+        const double ul = ml / rl, vl = nl / rl;
+        g[0][i] = rl; g[1][i] = ml; g[2][i] = nl;
+        g[3][i] = pref / (gam - 1.0) + 0.5 * (ml * ul + nl * vl);
+      } else if (P.dim == 2) {
         if (R.kind == BC_ISOTHERMAL_WALL) {   // src/Navier_StokesBC.hpp:47-65
           g[0][i] = s[0][i];
           g[1][i] = 0.0; g[2][i] = 0.0;
@@ -1806,8 +1821,9 @@ void *ora_create(int dim, int ne, const double *verts, const int *porder,
   }
 }
 void ora_free(void *h) { delete (Problem *)h; }
-// Boundary sides: nbc records (element, side, kind) with two
-// parameters each.  A record replaces the side's connectivity link; a
+// Boundary sides: nbc records (element, side, kind) with five
+// parameters each (isothermal wall: Tw, Eref; state: the conserved values;
+// subsonic outflow: Mref).  A record replaces the side's connectivity link; a
 // linked partner must be named too.  Returns 0, or -1 on a bad record.
 // Call once, before any state is set.
 int ora_set_bc(void *h, int nbc, const int *es_kind, const double *par) {
@@ -1818,9 +1834,10 @@ int ora_set_bc(void *h, int nbc, const int *es_kind, const double *par) {
   for (int b = 0; b < nbc; ++b) {
     const int e = es_kind[3 * b], s = es_kind[3 * b + 1], kind = es_kind[3 * b + 2];
     if (e < 0 || e >= P->ne || s < 0 || s >= nsides) return -1;
-    if (kind != BC_SLIP_WALL && kind != BC_ISOTHERMAL_WALL) return -1;
+    if (kind < BC_SLIP_WALL || kind > BC_SUPERSONIC_OUTFLOW || P->physics == SHALLOW) return -1;
     if (kind == BC_ISOTHERMAL_WALL && P->physics != NS3D && P->physics != NS2D) return -1;
     if (kind == BC_SLIP_WALL && P->physics != EULER3D && P->physics != EULER2D) return -1;
+    if ((kind == BC_SUBSONIC_OUTFLOW || kind == BC_SUPERSONIC_OUTFLOW) && P->dim != 2) return -1;
     Side &S = P->el[e].side[s];
     if (S.bc >= 0) return -1;
     S.master = true; S.bc = b;
@@ -1828,7 +1845,9 @@ int ora_set_bc(void *h, int nbc, const int *es_kind, const double *par) {
     Side G = S;
     G.master = false; G.bc = -1; G.off = off; off += S.qtot;
     P->gs.push_back(G);
-    P->bcs.push_back({e, s, kind, par[2 * b], par[2 * b + 1]});
+    Problem::BCRec rec{e, s, kind, par[5 * b], par[5 * b + 1], {}};
+    for (int k = 0; k < 5; ++k) rec.v[k] = par[5 * b + k];
+    P->bcs.push_back(rec);
   }
   // a boundary record replaces the side's connectivity link
   // (src/Field.cpp:4451); its former partner must be a boundary side too

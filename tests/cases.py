@@ -19,7 +19,7 @@ def load_golden(case):
 
 
 # boundary kinds of the oracle and of the engine (ora_set_bc / dgmx_set_boundary)
-BC_SLIP_WALL, BC_ISOTHERMAL_WALL = 1, 2
+BC_SLIP_WALL, BC_ISOTHERMAL_WALL, BC_STATE, BC_SUBSONIC_OUTFLOW, BC_SUPERSONIC_OUTFLOW = 1, 2, 3, 4, 5
 
 
 def bc_records(tags, sides, bct, physics):

@@ -14,8 +14,8 @@ import pytest
 
 import oracle
 from oracle import dgm_io, ics
-from tests.cases import (BC_ISOTHERMAL_WALL, BC_SLIP_WALL, diff_norms, load_wall_golden,
-                         passes_dgm_diff)
+from tests.cases import (BC_ISOTHERMAL_WALL, BC_SLIP_WALL, BC_STATE, BC_SUBSONIC_OUTFLOW,
+                         BC_SUPERSONIC_OUTFLOW, diff_norms, load_wall_golden, passes_dgm_diff)
 
 pytestmark = pytest.mark.gpu
 
@@ -143,6 +143,67 @@ def test_walls_2d_match_oracle(case):
     Q.set_state(U0)
     Q.advance(inttype, dt, steps)
     assert rel(Q.state(), P.state()) > 1e-9
+
+
+def _state(nf, u):
+    """A uniform state of density 1, x-velocity u and pressure 71.43."""
+    v = [1.0, u] + [0.0] * (nf - 3) + [71.43 / 0.4 + 0.5 * u * u]
+    return tuple(v)
+
+
+INOUT = [
+    # name, physics, dim, n, p, flux, inttype, dt, steps, vis, walls, outflow kind
+    ("euler3d-state-in-out-slip", 8, 3, (3, 2, 3), 3, "laxfriedrichs", 14, 0.002, 2, 0.0, BC_SLIP_WALL, BC_STATE),
+    ("ns3d-state-in-out-isothermal", 9, 3, (3, 2, 2), 3, "laxfriedrichs", 3, 0.001, 3, 0.02, BC_ISOTHERMAL_WALL,
+     BC_STATE),
+    ("euler2d-state-subsonic-out", 1, 2, (4, 3), 4, "roe", 4, 0.002, 3, 0.0, BC_SLIP_WALL, BC_SUBSONIC_OUTFLOW),
+    ("euler2d-state-supersonic-out", 1, 2, (4, 3), 3, "laxfriedrichs", 14, 0.002, 2, 0.0, BC_SLIP_WALL,
+     BC_SUPERSONIC_OUTFLOW),
+    ("ns2d-state-subsonic-out", 2, 2, (4, 3), 3, "laxfriedrichs", 3, 0.001, 3, 0.02, BC_ISOTHERMAL_WALL,
+     BC_SUBSONIC_OUTFLOW),
+]
+
+
+@pytest.mark.parametrize("case", INOUT, ids=[c[0] for c in INOUT])
+def test_inflow_outflow_match_oracle(case):
+    """A fixed-state inflow at x-, an outflow (or a second fixed state in
+    3-D) at x+ and walls on the other pair: GPU against the oracle."""
+    import dgm_b200
+    _, phys, dim, n, p, flux, inttype, dt, steps, vis, wall, out = case
+    nf = 5 if dim == 3 else 4
+    hi = (2 * np.pi, 2 * np.pi, 2.0) if dim == 3 else (2 * np.pi, 2.0)
+    m = dgm_b200.meshgen.box(dim, n, (0.0,) * dim, hi, p)
+    wpar = (1.0, 178.575) if wall == BC_ISOTHERMAL_WALL else ()
+    if dim == 3:
+        rec = [r[:3] + wpar for r in wall_records(n, wall)]
+        nx, ny, nz = n
+        xm = [i + nx * (j + ny * k) for k in range(nz) for j in range(ny) for i in [0]]
+        xp = [i + nx * (j + ny * k) for k in range(nz) for j in range(ny) for i in [nx - 1]]
+        rec += [(e, 4, BC_STATE) + _state(nf, 1.0) for e in xm]
+        rec += [(e, 2, BC_STATE) + _state(nf, 0.9) for e in xp]
+        P = oracle.Problem(dgm_io.Mesh(3, m.verts, m.con, m.porder, m.qorder), phys, flux=flux, vis=vis)
+        x, y, z = P.coords()
+        f = channel_ic(x, y, z)
+    else:
+        rec = [r[:3] + wpar for r in wall_records_2d(n, wall)]
+        nx, ny = n
+        rec += [(i + nx * j, 3, BC_STATE) + _state(nf, 1.0) for j in range(ny) for i in [0]]
+        opar = (0.1,) if out == BC_SUBSONIC_OUTFLOW else ()
+        rec += [(i + nx * j, 1, out) + opar for j in range(ny) for i in [nx - 1]]
+        P = oracle.Problem(dgm_io.Mesh(2, m.verts, m.con, m.porder, m.qorder), phys, flux=flux, vis=vis)
+        x, y, _ = P.coords()
+        f = channel_ic_2d(x, y)
+    P.set_bc(rec)
+    D = dgm_b200.Domain(m, phys, flux=flux, inttype=inttype, vis=vis, boundaries=rec)
+    U0 = P.project(f)
+    F_o, F_g = P.rhs(U0), D.time_derivative(U0)
+    scale = np.sqrt((F_o ** 2).sum()) + np.sqrt((U0 ** 2).sum())
+    assert np.sqrt(((F_g - F_o) ** 2).sum()) / scale < 1e-12
+    P.set_state(U0)
+    D.set_state(f)
+    assert P.advance(inttype, dt, steps) == 0
+    D.advance(dt, steps)
+    assert rel(D.state(), P.state()) < 1e-12
 
 
 def test_channel_golden_on_gpu():
