@@ -404,11 +404,12 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
       const bool euler = p->physics == DGMX_EULER3D || p->physics == DGMX_EULER2D;
       const bool ns = p->physics == DGMX_NS3D || p->physics == DGMX_NS2D;
       const bool outflow = k == DGMX_BC_SUBSONIC_OUTFLOW || k == DGMX_BC_SUPERSONIC_OUTFLOW;
-      if (!(k == DGMX_BC_SLIP_WALL && euler) && !(k == DGMX_BC_ISOTHERMAL_WALL && ns) &&
+      const bool sw = p->physics == DGMX_SHALLOW;
+      if (!(k == DGMX_BC_SLIP_WALL && (euler || sw)) && !(k == DGMX_BC_ISOTHERMAL_WALL && ns) &&
           !(k == DGMX_BC_STATE && (euler || ns)) && !(outflow && (euler || ns) && m->dim == 2)) {
         g_create_error = "boundary kind " + std::to_string(k) +
-                         " is not built for this physics (Euler: slip wall; Navier-Stokes: isothermal wall; both:"
-                         " fixed state, and the outflows in 2-D)";
+                         " is not built for this physics (Euler and shallow water: slip wall; Navier-Stokes:"
+                         " isothermal wall; Euler and Navier-Stokes: fixed state, and the outflows in 2-D)";
         return DGMX_ERR_UNSUPPORTED;
       }
     }
@@ -732,9 +733,9 @@ dgmx_status dgmx_create_from_files(const char *root, const dgmx_params *params, 
         k = DGMX_BC_SUBSONIC_OUTFLOW; st[0] = vals[0];
       } else if (fc.dim == 2 && euler && code.empty() && r.tag == "O") {
         k = DGMX_BC_SUPERSONIC_OUTFLOW;        // default "O" (src/Euler.cpp:1209)
-      } else if (euler && code.find("wall") != std::string::npos) {
-        k = DGMX_BC_SLIP_WALL;                 // src/Euler.cpp:1241-1243, src/Euler3d.cpp:862-866
-      } else if (euler && code.empty() && r.tag == "W") {
+      } else if ((euler || p.physics == DGMX_SHALLOW) && code.find("wall") != std::string::npos) {
+        k = DGMX_BC_SLIP_WALL;   // src/Euler.cpp:1241-1243, src/Euler3d.cpp:862-866, src/Shallow.cpp:782-785
+      } else if ((euler || p.physics == DGMX_SHALLOW) && code.empty() && r.tag == "W") {
         k = DGMX_BC_SLIP_WALL;                 // default "W" (src/Euler.cpp:1208, src/Euler3d.cpp:835)
       } else if (ns && code == "isothermal_wall" && vals.size() >= 2) {
         k = DGMX_BC_ISOTHERMAL_WALL; pa = vals[0]; pb = vals[1];

@@ -313,6 +313,12 @@ __device__ __forceinline__ typename C::R *trace_out(const StageArgs &a) {
 template <int DIM, int NF>
 __device__ __forceinline__ void ghost_state(int kind, const double *par, const double *Uo, const double *n,
                                             bool viscous, double *Un) {
+  if constexpr (NF == 3) {   // shallow water: Shallow::WallBC (src/ShallowBC.hpp:45-61)
+    Un[0] = Uo[0];
+    Un[1] = (Uo[1] * n[1] - Uo[2] * n[0]) * n[1];
+    Un[2] = (Uo[2] * n[0] - Uo[1] * n[1]) * n[0];
+    return;
+  }
   if (kind == DGMX_BC_STATE) {
 #pragma unroll
     for (int k = 0; k < NF; ++k) Un[k] = par[k];
@@ -367,7 +373,7 @@ __device__ __forceinline__ void face_fluxes(const Smem<C> &sm, const StageArgs &
 #pragma unroll
     for (int n = 0; n < NF; ++n) { Uo[n] = eo[n * EB]; Un[n] = tn[n * GF]; }
     const int bt = (gc.bc >> (4 * f)) & 15;
-    if constexpr (!C::MIXED && PHYS != DGMX_SHALLOW) {
+    if constexpr (!C::MIXED) {
       // boundary side: the neighbour is the ghost state of the database the
       // inviscid flux reads (see ghost_state)
       if (bt) ghost_state<C::DIM, C::NF>(a.bckind[bt], a.bcpar[bt], Uo, nm, false, Un);

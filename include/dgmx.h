@@ -43,9 +43,9 @@ enum { DGMX_FLUX_LF = 0, DGMX_FLUX_ROE = 1 };
 enum { DGMX_TVD3 = 3, DGMX_RK4 = 4, DGMX_LSRK14 = 14 };
 /* Arithmetic of the stage kernels. */
 enum { DGMX_FP64 = 0, DGMX_MIXED = 1 };
-/* Boundary kinds (FP64).  DGMX_BC_SLIP_WALL: Euler solid wall,
- * Euler::WallBC / Euler3d::WallBC (src/EulerBC.hpp:43-62,
- * src/Euler3d.cpp:862-903).  DGMX_BC_ISOTHERMAL_WALL: Navier-Stokes wall
+/* Boundary kinds (FP64).  DGMX_BC_SLIP_WALL: Euler and shallow-water solid
+ * wall, Euler::WallBC / Euler3d::WallBC / Shallow::WallBC (src/EulerBC.hpp:43-62,
+ * src/Euler3d.cpp:862-903, src/ShallowBC.hpp:45-61).  DGMX_BC_ISOTHERMAL_WALL: Navier-Stokes wall
  * with parameters (Tw, Eref), src/Navier_StokesBC.hpp:47-85,
  * src/Navier_Stokes3d.cpp:472-513.  In 3-D its inviscid flux sees the slip
  * wall of the Domain's BC database (Navier_Stokes3d keeps its own database
@@ -101,7 +101,7 @@ dgmx_status dgmx_create_from_files(const char *root, const dgmx_params *params, 
  * Eref; DGMX_BC_STATE: the conserved values; DGMX_BC_SUBSONIC_OUTFLOW:
  * Mref; unused entries ignored).  A record replaces the side's
  * connectivity link; a linked partner side must be named too.  At most 15
- * distinct (kind, parameters) pairs; FP64 only; not for shallow water.
+ * distinct (kind, parameters) pairs; FP64 only.
  * dgmx_create_from_files reads root.bc and root.bct the same way when they
  * exist (codes state, *wall*, isothermal_wall, subsonicoutflow,
  * supersonicoutflow and the default tags S, W, O as each physics' databases

@@ -996,7 +996,12 @@ static void enforce_bc(Problem &P, bool viscous) {
     double *s[5], *g[5];
     for (int n = 0; n < P.nf; ++n) { s[n] = sfld(P, P.Us_s, n) + S.off; g[n] = sfld(P, P.Us_s, n) + G.off; }
     for (int i = 0; i < S.qtot; ++i) {
-      if (R.kind == BC_STATE) {                // StateBC::apply, src/BC.cpp:17-28
+      if (P.physics == SHALLOW) {              // Shallow::WallBC, src/ShallowBC.hpp:45-61
+        const double nx = S.nx[i], ny = S.ny[i];
+        g[0][i] = s[0][i];
+        g[1][i] = (s[1][i] * ny - s[2][i] * nx) * ny;
+        g[2][i] = (s[2][i] * nx - s[1][i] * ny) * nx;
+      } else if (R.kind == BC_STATE) {                // StateBC::apply, src/BC.cpp:17-28
         for (int n = 0; n < P.nf; ++n) g[n][i] = R.v[n];
       } else if (R.kind == BC_SUPERSONIC_OUTFLOW) {   // src/EulerBC.hpp:214-241
         for (int n = 0; n < P.nf; ++n) g[n][i] = s[n][i];
@@ -1834,9 +1839,10 @@ int ora_set_bc(void *h, int nbc, const int *es_kind, const double *par) {
   for (int b = 0; b < nbc; ++b) {
     const int e = es_kind[3 * b], s = es_kind[3 * b + 1], kind = es_kind[3 * b + 2];
     if (e < 0 || e >= P->ne || s < 0 || s >= nsides) return -1;
-    if (kind < BC_SLIP_WALL || kind > BC_SUPERSONIC_OUTFLOW || P->physics == SHALLOW) return -1;
+    if (kind < BC_SLIP_WALL || kind > BC_SUPERSONIC_OUTFLOW) return -1;
+    if (P->physics == SHALLOW && kind != BC_SLIP_WALL) return -1;
     if (kind == BC_ISOTHERMAL_WALL && P->physics != NS3D && P->physics != NS2D) return -1;
-    if (kind == BC_SLIP_WALL && P->physics != EULER3D && P->physics != EULER2D) return -1;
+    if (kind == BC_SLIP_WALL && P->physics != EULER3D && P->physics != EULER2D && P->physics != SHALLOW) return -1;
     if ((kind == BC_SUBSONIC_OUTFLOW || kind == BC_SUPERSONIC_OUTFLOW) && P->dim != 2) return -1;
     Side &S = P->el[e].side[s];
     if (S.bc >= 0) return -1;

@@ -119,6 +119,30 @@ CASES_2D = [
 ]
 
 
+def test_shallow_water_walls_match_oracle():
+    """A Gaussian bump of water between two walls (y = -2, 2), periodic in
+    x; the balance quirk off (with it on, a still bump would not move)."""
+    import dgm_b200
+    n, p = (4, 4), 3
+    m = dgm_b200.meshgen.box(2, n, (-2.0, -2.0), (2.0, 2.0), p)
+    rec = wall_records_2d(n, BC_SLIP_WALL)
+    P = oracle.Problem(dgm_io.Mesh(2, m.verts, m.con, m.porder, m.qorder), oracle.SHALLOW)
+    P.set_sw_balance(False)
+    P.set_bc(rec)
+    D = dgm_b200.Domain(m, dgm_b200.SHALLOW, inttype=14, sw_balance=False, boundaries=rec)
+    x, y, _ = P.coords()
+    f = ics.gaussian_bump(x, y - 1.0, a=0.3, w=0.5)
+    U0 = P.project(f)
+    F_o, F_g = P.rhs(U0), D.time_derivative(U0)
+    scale = np.sqrt((F_o ** 2).sum()) + np.sqrt((U0 ** 2).sum())
+    assert np.sqrt(((F_g - F_o) ** 2).sum()) / scale < 1e-12
+    P.set_state(U0)
+    D.set_state(f)
+    assert P.advance(14, 0.001, 5) == 0
+    D.advance(0.001, 5)
+    assert rel(D.state(), P.state()) < 1e-12
+
+
 @pytest.mark.parametrize("case", CASES_2D, ids=[c[0] for c in CASES_2D])
 def test_walls_2d_match_oracle(case):
     import dgm_b200
