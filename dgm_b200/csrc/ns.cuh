@@ -52,17 +52,35 @@ struct NsCfg {
     static constexpr int SLOT = A + B + E + E2 + Fc + LFc + S1 + S2;
     static constexpr size_t SMEM = (size_t)EPB * SLOT * 8 + (size_t)EPB * (sizeof(GeomClass) + NFACE * 16 + 16);
   };
-  // ns_visc_kernel regions
+  // ns_visc_kernel regions (per slot, doubles).  G holds the velocity
+  // gradient, then in place the symmetric stress and the heat flux (NGS
+  // slots: 6 + 3 in 3-D, 3 + 2 in 2-D; the modal input is parked there
+  // first); the energy gradient goes to Dv, which then accumulates one
+  // field's divergence at a time.  B holds the state until the stresses are
+  // formed, then the face values FF and the divergence input Cv; X holds the
+  // modal gradient components Gh in the first loop and the face-point
+  // values Fg in the second.
   struct Visc {
-    static constexpr int B = NF * QD, G = NG * QD;     // modal input aliases G
-    static constexpr int Gh = DIM * LD, FF = cmax(NFACE * DIM * QF, NV * F2), Fg = NFACE * DIM * GF;
-    static constexpr int S1 = cmax(cmax(NF * P1, DIM == 3 ? NFACE * DIM * C::G * Q : 0), NV * F1);
-    static constexpr int S2 = cmax(NF * P2, NV * LD);
-    static constexpr int Cv = QD, Dv = NV * QD;
-    static constexpr int SLOT = B + G + Gh + FF + Fg + S1 + S2 + Cv + Dv;
+    static constexpr int NGS = DIM == 3 ? 9 : 5;
+    static constexpr int FF = cmax(NFACE * DIM * QF, F2), Cv = QD;
+    static constexpr int B = cmax(NF * QD, FF + Cv);
+    static constexpr int G = cmax(NGS * QD, NF * LD);
+    static constexpr int X = cmax(DIM * LD, NFACE * DIM * GF);
+    static constexpr int S1 = cmax(cmax(NB1 * P1, DIM * P1), cmax(DIM == 3 ? NFACE * DIM * C::G * Q : 0, F1));
+    static constexpr int S2 = cmax(cmax(NB1 * P2, DIM * P2), LD);
+    static constexpr int Dv = DIM * QD;
+    static constexpr int SLOT = B + G + X + S1 + S2 + Dv;
     static constexpr size_t SMEM = (size_t)EPB * SLOT * 8 + (size_t)EPB * (sizeof(GeomClass) + NFACE * 16 + 16);
-    static_assert(NF * LD <= NG * QD, "modal input must fit in the gradient region");
+    static_assert(DIM * DIM <= NGS, "the velocity gradient fits the stress slots");
   };
+  // slot of component d of the viscous flux vector g_n (n: momentum x, y,
+  // [z], energy) in the symmetric stress / heat-flux layout
+  static constexpr __host__ __device__ int gslot(int n, int d) {
+    if (DIM == 3) {
+      return n == 3 ? 6 + d : (n == 0 ? d : (n == 1 ? (d == 0 ? 1 : 2 + d) : (d == 0 ? 2 : (d == 1 ? 4 : 5))));
+    }
+    return n == 2 ? 3 + d : (n == 0 ? d : 1 + d);
+  }
   // CTAs per SM for a viscous kernel of smem bytes: the tile's register cap
   // when it has one, else as many as shared memory holds while the register
   // budget stays at 64 or more per thread
@@ -330,12 +348,13 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(Sta
   using N = NsCfg<C>;
   using R = typename N::Visc;
   constexpr int DIM = C::DIM, NF = C::NF, Q = C::Q, L = C::L, G = C::G, EPB = C::EPB, QD = C::QD;
-  constexpr int GF = C::GF, QF = C::QF, NFACE = C::NFACE, NG = N::NG, NV = N::NV, NVC = N::NVC, LD = C::LD;
+  constexpr int GF = C::GF, QF = C::QF, NFACE = C::NFACE, NV = N::NV, NVC = N::NVC, LD = C::LD, NGS = R::NGS;
   extern __shared__ __align__(16) unsigned char smem_bytes[];
   double *smem_raw = reinterpret_cast<double *>(smem_bytes);
-  double *B = smem_raw, *Gg = B + EPB * R::B, *Gh = Gg + EPB * R::G, *FF = Gh + EPB * R::Gh;
-  double *Fg = FF + EPB * R::FF, *S1 = Fg + EPB * R::Fg, *S2 = S1 + EPB * R::S1;
-  double *Cv = S2 + EPB * R::S2, *Dv = Cv + EPB * R::Cv;
+  double *B = smem_raw, *Gg = B + EPB * R::B, *X = Gg + EPB * R::G;
+  double *S1 = X + EPB * R::X, *S2 = S1 + EPB * R::S1, *Dv = S2 + EPB * R::S2;
+  double *Gh = X, *Fg = X;                    // first loop / second loop
+  double *FF = B, *Cv = B + EPB * R::FF;      // after the stresses are formed
   GeomClass *geo = reinterpret_cast<GeomClass *>(Dv + EPB * R::Dv);
   FaceLink *lnk = reinterpret_cast<FaceLink *>(geo + EPB);
   int *eid = reinterpret_cast<int *>(lnk + EPB * NFACE);
@@ -346,10 +365,16 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(Sta
   } else {
     load_modal<C>(Gg, a.X, e0, a.ne, tid);  // modal input parked in the gradient region
     __syncthreads();
-    backward_batch<C, NF>(Gg, B, S1, S2, tid);
+    if constexpr (N::NB1 == NF) {
+      backward_batch<C, NF>(Gg, B, S1, S2, tid);
+    } else {   // one slot: fields [0, NB1) then [NB1, NF)
+      backward_batch<C, N::NB1>(Gg, B, S1, S2, tid);
+      backward_batch<C, NF - N::NB1>(Gg + N::NB1 * LD, B + N::NB1 * QD, S1, S2, tid);
+    }
   }
   __syncthreads();
-  // projected gradients at the GLL points, DIM components at a time
+  // projected gradients at the GLL points: velocity components into Gg
+  // (component c, direction d at slot c*DIM+d), the energy gradient into Dv
   for (int c = 0; c < NVC; ++c) {
     for (int w = tid; w < EPB * DIM * LD; w += C::NT) {
       const int s = w / (DIM * LD), rem = w - s * DIM * LD;
@@ -358,18 +383,21 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(Sta
     }
     __syncthreads();
     backward_batch<C, DIM>(Gh, Dv, S1, S2, tid);
-    for (int w = tid; w < EPB * DIM * QD; w += C::NT) {
-      const int s = w / (DIM * QD), rem = w - s * DIM * QD;
-      Gg[(s * NG + c * DIM) * QD + rem] = Dv[w];
+    if (c < DIM) {
+      for (int w = tid; w < EPB * DIM * QD; w += C::NT) {
+        const int s = w / (DIM * QD), rem = w - s * DIM * QD;
+        Gg[(s * NGS + c * DIM) * QD + rem] = Dv[w];
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
-  // stresses and heat flux, in place: slot k*DIM+d holds g_{k+1} component d
+  // stresses and heat flux, in place (slots gslot(n, d))
   const double mu = a.vis, gPr = a.gamma / a.Pr;
   for (int w = tid; w < EPB * QD; w += C::NT) {
     const int s = w / QD, p = w - s * QD;
-    double *g = Gg + s * NG * QD + p;
-    double U[5], q[4];
+    double *g = Gg + s * NGS * QD + p;
+    const double *ge = Dv + s * DIM * QD + p;
+    double U[5];
 #pragma unroll
     for (int n = 0; n < NF; ++n) U[n] = B[(s * NF + n) * QD + p];
     const double r = U[0];
@@ -378,7 +406,7 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(Sta
       const double ux = g[0 * QD], uy = g[1 * QD], uz = g[2 * QD];
       const double vx = g[3 * QD], vy = g[4 * QD], vz = g[5 * QD];
       const double wx = g[6 * QD], wy = g[7 * QD], wz = g[8 * QD];
-      const double ex = g[9 * QD], ey = g[10 * QD], ez = g[11 * QD];
+      const double ex = ge[0], ey = ge[QD], ez = ge[2 * QD];
       double t12 = uy + vx; t12 = mu * t12;
       double t13 = uz + wx; t13 = mu * t13;
       double t23 = vz + wy; t23 = mu * t23;
@@ -393,24 +421,21 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(Sta
       double qz = t13 * u; qz = fma(t23, v, qz); qz = fma(t33, ww, qz);
       qx = fma(gPr, mu * ex, qx); qy = fma(gPr, mu * ey, qy); qz = fma(gPr, mu * ez, qz);
       g[0 * QD] = t11; g[1 * QD] = t12; g[2 * QD] = t13;
-      g[3 * QD] = t12; g[4 * QD] = t22; g[5 * QD] = t23;
-      g[6 * QD] = t13; g[7 * QD] = t23; g[8 * QD] = t33;
-      g[9 * QD] = qx; g[10 * QD] = qy; g[11 * QD] = qz;
+      g[3 * QD] = t22; g[4 * QD] = t23; g[5 * QD] = t33;
+      g[6 * QD] = qx; g[7 * QD] = qy; g[8 * QD] = qz;
     } else {
       const double u = U[1] / r, v = U[2] / r;
       const double ux = g[0 * QD], uy = g[1 * QD], vx = g[2 * QD], vy = g[3 * QD];
-      const double ex = g[4 * QD], ey = g[5 * QD];
+      const double ex = ge[0], ey = ge[QD];
       double t12 = uy + vx; t12 = mu * t12;
       double t11 = 2.0 * ux - vy; t11 = (2.0 / 3.0) * t11; t11 = mu * t11;
       double t22 = 2.0 * vy - ux; t22 = (2.0 / 3.0) * t22; t22 = mu * t22;
       double qx = t11 * u; qx = fma(t12, v, qx);
       double qy = t12 * u; qy = fma(t22, v, qy);
       qx = fma(gPr, mu * ex, qx); qy = fma(gPr, mu * ey, qy);
-      g[0 * QD] = t11; g[1 * QD] = t12;
-      g[2 * QD] = t12; g[3 * QD] = t22;
-      g[4 * QD] = qx; g[5 * QD] = qy;
+      g[0 * QD] = t11; g[1 * QD] = t12; g[2 * QD] = t22;
+      g[3 * QD] = qx; g[4 * QD] = qy;
     }
-    (void)q;
   }
   __syncthreads();
   for (int n = 0; n < NV; ++n) {
@@ -418,7 +443,7 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(Sta
     for (int w = tid; w < NFACE * EPB * DIM * QF; w += C::NT) {
       const int f = w / (EPB * DIM * QF), rem = w - f * EPB * DIM * QF;
       const int s = rem / (DIM * QF), rem2 = rem - s * DIM * QF, d = rem2 / QF, x = rem2 - d * QF;
-      const double *src = Gg + (s * NG + n * DIM + d) * QD;
+      const double *src = Gg + (s * NGS + N::gslot(n, d)) * QD;
       int p;
       if constexpr (DIM == 3) {
         const int u = x / Q, v = x % Q;
@@ -461,31 +486,32 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(Sta
       if (DIM == 3) v = fma(nr[2], Fg[((f * EPB + s) * DIM + 2) * GF + gq], v);
       a.V[(((size_t)e * NFACE + f) * NV + n) * GF + gq] = v;
     }
-    // collocation divergence of g_n (contravariant form)
+    // collocation divergence of g_n (contravariant form) into Dv [slot][QD]
     for (int r = 0; r < DIM; ++r) {
       for (int w = tid; w < EPB * QD; w += C::NT) {
         const int s = w / QD, p = w - s * QD;
         const double *m = geo[s].metric;
-        const double *gn = Gg + (s * NG + n * DIM) * QD + p;
-        double v = m[3 * r + 0] * gn[0];
-        v = fma(m[3 * r + 1], gn[QD], v);
-        if (DIM == 3) v = fma(m[3 * r + 2], gn[2 * QD], v);
+        const double *gs = Gg + s * NGS * QD + p;
+        double v = m[3 * r + 0] * gs[N::gslot(n, 0) * QD];
+        v = fma(m[3 * r + 1], gs[N::gslot(n, 1) * QD], v);
+        if (DIM == 3) v = fma(m[3 * r + 2], gs[N::gslot(n, 2) * QD], v);
         Cv[w] = v;
       }
       __syncthreads();
       using Sh = Sh3<DIM, Q>;
-      double *dv = Dv + n * QD;
-      if (r == 0) contract<Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<L, Q>, false>(Cv, dv, EPB, QD, NV * QD, tid, C::NT);
-      else if (r == 1) contract<Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<L, Q>, true>(Cv, dv, EPB, QD, NV * QD, tid, C::NT);
-      else contract<Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<L, Q>, true>(Cv, dv, EPB, QD, NV * QD, tid, C::NT);
+      if (r == 0) contract<Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<L, Q>, false>(Cv, Dv, EPB, QD, QD, tid, C::NT);
+      else if (r == 1) contract<Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<L, Q>, true>(Cv, Dv, EPB, QD, QD, tid, C::NT);
+      else contract<Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<L, Q>, true>(Cv, Dv, EPB, QD, QD, tid, C::NT);
       __syncthreads();
     }
-  }
-  forward_batch<C, NV>(Dv, S2, S1, FF, tid);
-  for (int w = tid; w < EPB * NV * LD; w += C::NT) {
-    const int s = w / (NV * LD), rem = w - s * NV * LD;
-    const int e = e0 + s;
-    if (e < a.ne) a.Pv[(size_t)e * NV * LD + rem] = S2[w];
+    // projected divergence of this field
+    forward_batch<C, 1>(Dv, S2, S1, FF, tid);
+    for (int w = tid; w < EPB * LD; w += C::NT) {
+      const int s = w / LD, m = w - s * LD;
+      const int e = e0 + s;
+      if (e < a.ne) a.Pv[((size_t)e * NV + n) * LD + m] = S2[w];
+    }
+    __syncthreads();
   }
 }
 
