@@ -121,6 +121,12 @@ struct dgmx_domain {
   double *x_sbuf = nullptr, *x_rbuf = nullptr;           // nf*gf doubles per block
   ncclComm_t nccl = nullptr;                             // multi-rank transport
   bool in_group = false;                                 // in-process partitions: the group exchanges
+  // overlap: tiles with a face on a ghost slot run first, the exchange of
+  // their traces then runs on xstream while the interior tiles run
+  cudaStream_t xstream = nullptr;
+  cudaEvent_t ev_b = nullptr, ev_x = nullptr;
+  int *tiles = nullptr;                                  // [boundary tiles | interior tiles], then the two counts
+  int tiles_epb = 0, ntiles_b = 0, ntiles_i = 0;
   int tcur = 0;
   bool sw_captured = false;
   long launches = 0;
@@ -177,7 +183,7 @@ struct dgmx_domain {
     if (graph) cudaGraphExecDestroy(graph);
     graph = nullptr;
     void *ptrs[] = {U, Ut, Acc, T[0], T[1], Rsw, nod_in, nod_out, Jdev, integ, gclass, perm, err, classes, links,
-                    Ghat, Vtr, Pv, Utf, Tf[0], Tf[1], uref, R0, cbar, x_send, x_recv, x_sbuf, x_rbuf};
+                    Ghat, Vtr, Pv, Utf, Tf[0], Tf[1], uref, R0, cbar, x_send, x_recv, x_sbuf, x_rbuf, tiles};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (host_pinned) cudaFreeHost(host_pinned);
     if (nccl && nccl_api().ok) nccl_api().CommDestroy(nccl);
@@ -188,7 +194,11 @@ struct dgmx_domain {
     Utf = Tf[0] = Tf[1] = nullptr;
     uref = nullptr;
     R0 = cbar = nullptr;
-    x_send = x_recv = nullptr; x_sbuf = x_rbuf = nullptr;
+    x_send = x_recv = nullptr; x_sbuf = x_rbuf = nullptr; tiles = nullptr; tiles_epb = 0;
+    if (ev_b) cudaEventDestroy(ev_b);
+    if (ev_x) cudaEventDestroy(ev_x);
+    if (xstream) cudaStreamDestroy(xstream);
+    ev_b = ev_x = nullptr; xstream = nullptr;
     T[0] = T[1] = nullptr; gclass = perm = err = nullptr; classes = nullptr; links = nullptr; stream = nullptr;
   }
 };
@@ -259,6 +269,78 @@ StageArgs stage_args(const dgmx_domain *d, const StageSpec &sp, double dt) {
   return a;
 }
 
+// Tile lists of a partitioned handle for the stage kernel's tile size:
+// boundary tiles (an element with a face on a ghost slot) first, then the
+// interior ones; the two counts follow the lists (read on the device).
+dgmx_status build_tiles(dgmx_domain *d) {
+  const int epb = d->stage_ops()->epb;
+  if (d->tiles && d->tiles_epb == epb) return DGMX_OK;
+  const int nt = (d->ne + epb - 1) / epb, nf = d->nfaces;
+  std::vector<int> b, in;
+  for (int t = 0; t < nt; ++t) {
+    bool bnd = false;
+    for (int e = t * epb; e < std::min(d->ne, (t + 1) * epb) && !bnd; ++e)
+      for (int f = 0; f < nf; ++f)
+        if (d->mesh.links[(size_t)e * nf + f].elem >= d->ne) { bnd = true; break; }
+    (bnd ? b : in).push_back(t);
+  }
+  std::vector<int> h(b);
+  h.insert(h.end(), in.begin(), in.end());
+  h.push_back((int)b.size());
+  h.push_back((int)in.size());
+  if (d->tiles) { cudaFree(d->tiles); d->tiles = nullptr; }
+  cudaError_t e = dalloc(&d->tiles, h.size());
+  if (e == cudaSuccess) e = cudaMemcpy(d->tiles, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return d->cuda(e, "tile lists");
+  d->tiles_epb = epb; d->ntiles_b = (int)b.size(); d->ntiles_i = (int)in.size();
+  if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  return DGMX_OK;
+}
+
+// The stage kernel over one of the two tile lists (0 boundary, 1 interior).
+cudaError_t stage_tiles(const dgmx_domain *d, StageArgs a, int which, cudaStream_t s) {
+  const int n = which == 0 ? d->ntiles_b : d->ntiles_i;
+  if (!n) return cudaSuccess;
+  const int nt = d->ntiles_b + d->ntiles_i;
+  a.tiles = d->tiles + (which == 0 ? 0 : d->ntiles_b);
+  a.ntiles = d->tiles + nt + which;
+  const KernelOps *o = d->stage_ops();
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->prm.device) != cudaSuccess || sms < 1) sms = 1;
+  const int cap = sms * (o->blocks_per_sm ? o->blocks_per_sm() : 1);
+  return o->stage_grid(a, n < cap ? n : cap, s);
+}
+
+// One stage of an NCCL rank with the exchange overlapped: boundary tiles,
+// then the exchange on xstream while the interior tiles run on stream.
+dgmx_status stage_overlapped(dgmx_domain *d, const StageArgs &a) {
+  cudaError_t e = stage_tiles(d, a, 0, d->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(d->ev_b, d->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(d->xstream, d->ev_b, 0);
+  if (e != cudaSuccess) return d->cuda(e, "boundary tiles");
+  const int blk = d->nf * d->gf;
+  double *T = d->T[d->tcur ^ 1];
+  e = launch_pack(T, d->x_send, d->x_total, blk, d->x_sbuf, d->xstream);
+  if (e != cudaSuccess) return d->cuda(e, "halo pack");
+  const NcclApi &nc = nccl_api();
+  ncclResult_t r = nc.GroupStart();
+  for (int q = 0; q < d->plan.nranks && r == ncclSuccess; ++q) {
+    if (!d->x_cnt[q]) continue;
+    const size_t off = (size_t)d->x_off[q] * blk, n = (size_t)d->x_cnt[q] * blk;
+    r = nc.Send(d->x_sbuf + off, n, ncclFloat64, q, d->nccl, d->xstream);
+    if (r == ncclSuccess) r = nc.Recv(d->x_rbuf + off, n, ncclFloat64, q, d->nccl, d->xstream);
+  }
+  const ncclResult_t r2 = nc.GroupEnd();
+  if (r == ncclSuccess) r = r2;
+  if (r != ncclSuccess) return d->fail(DGMX_ERR_CUDA, std::string("halo exchange: ") + nc.GetErrorString(r));
+  e = launch_unpack(d->x_rbuf, d->x_recv, d->x_total, blk, T, d->xstream);
+  if (e == cudaSuccess) e = cudaEventRecord(d->ev_x, d->xstream);
+  if (e == cudaSuccess) e = stage_tiles(d, a, 1, d->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(d->stream, d->ev_x, 0);
+  d->launches += 4;
+  return d->cuda(e, "overlapped stage");
+}
+
 // enqueue the stages of one time step on d->stream
 dgmx_status enqueue_step(dgmx_domain *d, double dt) {
   const std::vector<StageSpec> specs = stage_specs(d->prm.inttype, dt);
@@ -272,6 +354,12 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
       d->launches += 2;
       dgmx_status xs = exchange(d, d->Vtr, (d->nf - 1) * d->gf);
       if (xs != DGMX_OK) return xs;
+    }
+    if (d->partitioned() && d->nccl && d->xstream) {
+      const dgmx_status xs = stage_overlapped(d, a);
+      if (xs != DGMX_OK) return xs;
+      d->tcur ^= 1;
+      continue;
     }
     e = d->stage_ops()->stage(a, d->stream);
     if (e != cudaSuccess) return d->cuda(e, "stage kernel launch");
@@ -661,7 +749,13 @@ dgmx_status dgmx_set_exchange_nccl(dgmx_domain *d, const unsigned char *id) {
   const ncclResult_t r = nc.CommInitRank(&d->nccl, d->plan.nranks, u, d->plan.rank);
   if (r != ncclSuccess) { d->nccl = nullptr; return d->fail(DGMX_ERR_CUDA, std::string("ncclCommInitRank: ") + nc.GetErrorString(r)); }
   if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
-  return DGMX_OK;
+  // exchange overlapped with the interior tiles
+  cudaError_t e = cudaSuccess;
+  if (!d->xstream) e = cudaStreamCreateWithFlags(&d->xstream, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !d->ev_b) e = cudaEventCreateWithFlags(&d->ev_b, cudaEventDisableTiming);
+  if (e == cudaSuccess && !d->ev_x) e = cudaEventCreateWithFlags(&d->ev_x, cudaEventDisableTiming);
+  if (e != cudaSuccess) return d->cuda(e, "exchange stream");
+  return build_tiles(d);
 }
 
 dgmx_status dgmx_partition_info(const dgmx_domain *d, int *ne_local, int *nghost, int *global_of_local) {
@@ -961,6 +1055,7 @@ dgmx_status dgmx_advance_async(dgmx_domain *d, double dt, int nsteps) {
   // The trace buffers swap once per stage, so a graph holds two steps when a
   // step has an odd stage count (TVD3) and the buffer parity repeats.  The
   // graph is rebuilt when dt or the starting parity changes.
+  if (d->partitioned() && d->nccl && (st = build_tiles(d)) != DGMX_OK) return st;
   const int nst = stages_per_step(d->prm.inttype);
   const int reps = (nst & 1) ? 2 : 1;
   if (nsteps >= reps && (!d->graph || d->graph_dt != dt || d->graph_tcur != d->tcur)) {
@@ -1135,7 +1230,12 @@ struct dgmx_group {
   std::vector<int> part;
   int ne = 0;
   std::string errmsg;
+  cudaStream_t xs = nullptr;                 // the exchange, overlapped with the interior tiles
+  cudaEvent_t ev_b = nullptr, ev_x = nullptr;
   ~dgmx_group() {
+    if (ev_b) cudaEventDestroy(ev_b);
+    if (ev_x) cudaEventDestroy(ev_x);
+    if (xs) cudaStreamDestroy(xs);
     for (dgmx_domain *d : parts) {
       if (!d) continue;
       cudaSetDevice(d->prm.device);
@@ -1149,9 +1249,8 @@ struct dgmx_group {
 
 namespace {
 
-// which = 0: T[tcur], 1: T[tcur ^ 1], 2: viscous traces
-dgmx_status group_exchange(dgmx_group *g, int which) {
-  const cudaStream_t s = g->stream();
+// which = 0: T[tcur], 1: T[tcur ^ 1], 2: viscous traces; on stream s
+dgmx_status group_exchange(dgmx_group *g, int which, cudaStream_t s) {
   auto buf = [&](dgmx_domain *d) { return which == 2 ? d->Vtr : d->T[which == 0 ? d->tcur : d->tcur ^ 1]; };
   dgmx_domain *d0 = g->parts[0];
   const int blk = which == 2 ? (d0->nf - 1) * d0->gf : d0->nf * d0->gf;
@@ -1236,7 +1335,7 @@ dgmx_status dgmx_group_set_state(dgmx_group *g, const double *U) {
     if (st != DGMX_OK) return group_fail(g, d, st);
   }
   cudaSetDevice(d0->prm.device);
-  dgmx_status st = group_exchange(g, 0);
+  dgmx_status st = group_exchange(g, 0, g->stream());
   if (st != DGMX_OK) return st;
   return cudaStreamSynchronize(g->stream()) == cudaSuccess ? DGMX_OK : DGMX_ERR_CUDA;
 }
@@ -1266,6 +1365,13 @@ dgmx_status dgmx_group_advance(dgmx_group *g, double dt, int nsteps) {
   for (dgmx_domain *d : g->parts) {
     if (d->prm.physics == DGMX_SHALLOW && d->prm.sw_balance) { g->errmsg = "shallow-water balance is off in groups"; return DGMX_ERR_UNSUPPORTED; }
     if (reset_error_word(d) != DGMX_OK || cudaStreamSynchronize(d->stream) != cudaSuccess) return group_fail(g, d, DGMX_ERR_CUDA);
+    if (build_tiles(d) != DGMX_OK) return group_fail(g, d, DGMX_ERR_CUDA);
+  }
+  if (!g->xs) {
+    cudaError_t ce = cudaStreamCreateWithFlags(&g->xs, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&g->ev_b, cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&g->ev_x, cudaEventDisableTiming);
+    if (ce != cudaSuccess) { g->errmsg = std::string("group streams: ") + cudaGetErrorString(ce); return DGMX_ERR_CUDA; }
   }
   cudaError_t e = cudaSuccess;
   dgmx_status st = DGMX_OK;
@@ -1278,14 +1384,25 @@ dgmx_status dgmx_group_advance(dgmx_group *g, double dt, int nsteps) {
           if (e == cudaSuccess) e = d->ops->ns_visc(a, false, s);
           d->launches += 2;
         }
-        if (e == cudaSuccess && (st = group_exchange(g, 2)) != DGMX_OK) return st;
+        if (e == cudaSuccess && (st = group_exchange(g, 2, s)) != DGMX_OK) return st;
       }
+      // boundary tiles of every part, then their exchange on the side
+      // stream while the interior tiles run
       for (dgmx_domain *d : g->parts) {
         const StageArgs a = stage_args(d, sp, dt);
-        if (e == cudaSuccess) e = d->stage_ops()->stage(a, s);
+        if (e == cudaSuccess) e = stage_tiles(d, a, 0, s);
         ++d->launches;
       }
-      if (e == cudaSuccess && (st = group_exchange(g, 1)) != DGMX_OK) return st;
+      if (e == cudaSuccess) e = cudaEventRecord(g->ev_b, s);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(g->xs, g->ev_b, 0);
+      if (e == cudaSuccess && (st = group_exchange(g, 1, g->xs)) != DGMX_OK) return st;
+      if (e == cudaSuccess) e = cudaEventRecord(g->ev_x, g->xs);
+      for (dgmx_domain *d : g->parts) {
+        const StageArgs a = stage_args(d, sp, dt);
+        if (e == cudaSuccess) e = stage_tiles(d, a, 1, s);
+        ++d->launches;
+      }
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(s, g->ev_x, 0);
       for (dgmx_domain *d : g->parts) d->tcur ^= 1;
       if (e != cudaSuccess) break;
     }
