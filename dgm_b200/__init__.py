@@ -173,6 +173,48 @@ class Domain:
         f.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         self._check(f(self.h, bytes(nccl_id)))
 
+    def set_exchange_host(self, group=None):
+        """Host-staged halo exchange through torch.distributed (any backend
+        with point-to-point sends, e.g. gloo): at every exchange the packed
+        face blocks come to the host, go to the peers and back.  Collective
+        over the ranks; steps are then not captured into graphs."""
+        import torch
+        import torch.distributed as dist
+        FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                              ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int),
+                              ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int)
+        me = dist.get_rank(group)
+
+        def transport(ctx, send, recv, counts, offsets, blk, nranks):
+            try:
+                total = sum(counts[q] for q in range(nranks)) * blk
+                if total == 0:
+                    return 0
+                sa = np.ctypeslib.as_array(send, shape=(total,))
+                ra = np.ctypeslib.as_array(recv, shape=(total,))
+                sends, recvs = [], []
+                for q in range(nranks):
+                    n = counts[q] * blk
+                    if q == me or n == 0:
+                        continue
+                    o = offsets[q] * blk
+                    sends.append(dist.isend(torch.from_numpy(sa[o:o + n].copy()), q, group=group))
+                    buf = torch.empty(n, dtype=torch.float64)
+                    recvs.append((dist.irecv(buf, q, group=group), buf, o, n))
+                for r in sends:
+                    r.wait()
+                for r, buf, o, n in recvs:
+                    r.wait()
+                    ra[o:o + n] = buf.numpy()
+                return 0
+            except Exception:
+                return 1
+
+        self._xfn = FN(transport)   # kept alive with the handle
+        f = lib().dgmx_set_exchange_host
+        f.argtypes = [ctypes.c_void_p, FN, ctypes.c_void_p]
+        self._check(f(self.h, self._xfn, None))
+
     def partition_info(self):
         """(local element count, ghost slots, global id of every local element)."""
         ne, ng = ctypes.c_int(), ctypes.c_int()

@@ -120,6 +120,11 @@ struct dgmx_domain {
   int x_total = 0;
   double *x_sbuf = nullptr, *x_rbuf = nullptr;           // nf*gf doubles per block
   ncclComm_t nccl = nullptr;                             // multi-rank transport
+  // host-staged transport (alternative to NCCL): packed blocks are copied to
+  // pinned host buffers and handed to the caller's function
+  dgmx_exchange_fn xhost = nullptr;
+  void *xhost_ctx = nullptr;
+  double *xh_send = nullptr, *xh_recv = nullptr;
   bool in_group = false;                                 // in-process partitions: the group exchanges
   // overlap: tiles with a face on a ghost slot run first, the exchange of
   // their traces then runs on xstream while the interior tiles run
@@ -186,6 +191,9 @@ struct dgmx_domain {
                     Ghat, Vtr, Pv, Utf, Tf[0], Tf[1], uref, R0, cbar, x_send, x_recv, x_sbuf, x_rbuf, tiles};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (host_pinned) cudaFreeHost(host_pinned);
+    if (xh_send) cudaFreeHost(xh_send);
+    if (xh_recv) cudaFreeHost(xh_recv);
+    xh_send = xh_recv = nullptr;
     if (nccl && nccl_api().ok) nccl_api().CommDestroy(nccl);
     nccl = nullptr;
     if (stream) cudaStreamDestroy(stream);
@@ -211,9 +219,23 @@ namespace {
 // partitioned or belongs to an in-process group (the group exchanges).
 dgmx_status exchange(dgmx_domain *d, double *T, int blk) {
   if (!d->partitioned() || d->in_group) return DGMX_OK;
-  if (!d->nccl) return d->fail(DGMX_ERR_ARGUMENT, "partitioned domain without an exchange (dgmx_set_exchange_nccl)");
+  if (!d->nccl && !d->xhost)
+    return d->fail(DGMX_ERR_ARGUMENT, "partitioned domain without an exchange (dgmx_set_exchange_nccl)");
   cudaError_t e = launch_pack(T, d->x_send, d->x_total, blk, d->x_sbuf, d->stream);
   if (e != cudaSuccess) return d->cuda(e, "halo pack");
+  if (d->xhost) {
+    // host-staged: blocks to the host, the caller's transport, back, unpack
+    const size_t n = (size_t)d->x_total * blk;
+    if (n) e = cudaMemcpyAsync(d->xh_send, d->x_sbuf, sizeof(double) * n, cudaMemcpyDeviceToHost, d->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+    if (e != cudaSuccess) return d->cuda(e, "halo download");
+    if (d->xhost(d->xhost_ctx, d->xh_send, d->xh_recv, d->x_cnt.data(), d->x_off.data(), blk, d->plan.nranks) != 0)
+      return d->fail(DGMX_ERR_CUDA, "host halo transport reported a failure");
+    if (n) e = cudaMemcpyAsync(d->x_rbuf, d->xh_recv, sizeof(double) * n, cudaMemcpyHostToDevice, d->stream);
+    if (e == cudaSuccess) e = launch_unpack(d->x_rbuf, d->x_recv, d->x_total, blk, T, d->stream);
+    d->launches += 2;
+    return d->cuda(e, "halo unpack");
+  }
   const NcclApi &nc = nccl_api();
   ncclResult_t r = nc.GroupStart();
   for (int q = 0; q < d->plan.nranks && r == ncclSuccess; ++q) {
@@ -355,7 +377,7 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
       dgmx_status xs = exchange(d, d->Vtr, (d->nf - 1) * d->gf);
       if (xs != DGMX_OK) return xs;
     }
-    if (d->partitioned() && d->nccl && d->xstream) {
+    if (d->partitioned() && d->nccl && !d->xhost && d->xstream) {
       const dgmx_status xs = stage_overlapped(d, a);
       if (xs != DGMX_OK) return xs;
       d->tcur ^= 1;
@@ -758,6 +780,21 @@ dgmx_status dgmx_set_exchange_nccl(dgmx_domain *d, const unsigned char *id) {
   return build_tiles(d);
 }
 
+dgmx_status dgmx_set_exchange_host(dgmx_domain *d, dgmx_exchange_fn fn, void *ctx) {
+  if (!d || !fn) return DGMX_ERR_ARGUMENT;
+  if (!d->partitioned() || d->in_group) return d->fail(DGMX_ERR_ARGUMENT, "not a rank of a partitioned domain");
+  cudaSetDevice(d->prm.device);
+  const size_t n = (size_t)std::max(1, d->x_total) * d->nf * d->gf;
+  cudaError_t e = cudaSuccess;
+  if (!d->xh_send) e = cudaHostAlloc(reinterpret_cast<void **>(&d->xh_send), sizeof(double) * n, cudaHostAllocDefault);
+  if (e == cudaSuccess && !d->xh_recv)
+    e = cudaHostAlloc(reinterpret_cast<void **>(&d->xh_recv), sizeof(double) * n, cudaHostAllocDefault);
+  if (e != cudaSuccess) return d->cuda(e, "host halo buffers");
+  d->xhost = fn; d->xhost_ctx = ctx;
+  if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  return DGMX_OK;
+}
+
 dgmx_status dgmx_partition_info(const dgmx_domain *d, int *ne_local, int *nghost, int *global_of_local) {
   if (!d) return DGMX_ERR_ARGUMENT;
   if (ne_local) *ne_local = d->ne;
@@ -1058,6 +1095,11 @@ dgmx_status dgmx_advance_async(dgmx_domain *d, double dt, int nsteps) {
   if (d->partitioned() && d->nccl && (st = build_tiles(d)) != DGMX_OK) return st;
   const int nst = stages_per_step(d->prm.inttype);
   const int reps = (nst & 1) ? 2 : 1;
+  if (d->xhost) {   // host-staged exchanges synchronise every stage: no graph
+    for (int s = 0; s < nsteps; ++s)
+      if ((st = enqueue_step(d, dt)) != DGMX_OK) return st;
+    return DGMX_OK;
+  }
   if (nsteps >= reps && (!d->graph || d->graph_dt != dt || d->graph_tcur != d->tcur)) {
     if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
     const int t0 = d->tcur;

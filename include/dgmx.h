@@ -123,6 +123,15 @@ dgmx_status dgmx_create_partition(const dgmx_mesh *mesh, const dgmx_params *para
 #define DGMX_NCCL_ID_BYTES 128
 dgmx_status dgmx_nccl_unique_id(unsigned char *id);
 dgmx_status dgmx_set_exchange_nccl(dgmx_domain *d, const unsigned char *id);
+/* Host-staged transport instead of NCCL (e.g. MPI, or gloo in tests): at
+ * every exchange the packed face blocks are copied to pinned host memory
+ * and fn is called with them: send holds, for every peer q in rank order,
+ * counts[q] blocks of blk doubles at offsets[q] * blk; fn must fill recv the
+ * same way with the blocks peer q sent here, and return 0.  Exchanges are
+ * then synchronous and steps are not captured into graphs. */
+typedef int (*dgmx_exchange_fn)(void *ctx, const double *send, double *recv, const int *counts,
+                                const int *offsets, int blk, int nranks);
+dgmx_status dgmx_set_exchange_host(dgmx_domain *d, dgmx_exchange_fn fn, void *ctx);
 /* local element count, ghost slots and the global id of every local element */
 dgmx_status dgmx_partition_info(const dgmx_domain *d, int *ne_local, int *nghost, int *global_of_local);
 /* Host-only partition plan (see dgmx.cpp): sizes[3] = local elements, ghost

@@ -70,3 +70,67 @@ def test_partition_handles_and_nccl_id():
     x, y, z = R.coordinates()
     with pytest.raises(dgm_b200.DgmxError):
         R.set_state(ics.taylor_green(x, y, z, Ma=0.1))
+
+
+def _rank_run(rank, nranks, port, case, result):
+    """One rank of a partitioned run: its own process and CUDA context on
+    device 0, halo exchanges staged through the host over gloo (no kernel
+    waits on another process)."""
+    import datetime
+    import os as _os
+    import torch.distributed as dist
+    import dgm_b200
+    _os.environ["MASTER_ADDR"] = "127.0.0.1"
+    _os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=nranks, timeout=datetime.timedelta(seconds=60))
+    phys, n, p, flux, inttype, dt, steps, vis = case
+    m = dgm_b200.meshgen.box(3, n, 0.0, 2 * np.pi, p)
+    ne = m.verts.shape[0]
+    part = (np.arange(ne) * nranks) // ne
+    D = dgm_b200.Domain.partition(m, phys, part, nranks, rank, flux=flux, inttype=inttype, vis=vis)
+    D.set_exchange_host()
+    nl, ng, gids = D.partition_info()
+    x, y, z = D.coordinates()
+    D.set_state(ics.taylor_green(x, y, z, Ma=0.1))
+    D.advance(dt, steps)
+    result[rank] = (gids.copy(), D.state())
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("case", [(8, (3, 2, 4), 3, "roe", 14, 0.002, 2, 0.0),
+                                  (9, (2, 2, 3), 2, "laxfriedrichs", 3, 0.002, 2, 0.02)],
+                         ids=["euler3d-lsrk14", "ns3d-tvd3"])
+def test_two_process_ranks_equal_single_domain(case):
+    """Two processes, each one rank of a partitioned domain, exchanging halos
+    through the host: the gathered state equals the unpartitioned run."""
+    import socket
+    import torch.multiprocessing as mp
+    import dgm_b200
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    result = ctx.Manager().dict()
+    procs = [ctx.Process(target=_rank_run, args=(r, 2, port, case, result)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    for pr in procs:
+        pr.join(timeout=300)
+    for pr in procs:
+        if pr.is_alive():
+            pr.kill()
+        assert pr.exitcode == 0
+    phys, n, p, flux, inttype, dt, steps, vis = case
+    m = dgm_b200.meshgen.box(3, n, 0.0, 2 * np.pi, p)
+    D = dgm_b200.Domain(m, phys, flux=flux, inttype=inttype, vis=vis)
+    x, y, z = D.coordinates()
+    D.set_state(ics.taylor_green(x, y, z, Ma=0.1))
+    D.advance(dt, steps)
+    S = D.state()
+    qd = (p + 2) ** 3
+    G = np.zeros_like(S).reshape(S.shape[0], -1, qd)
+    for r in range(2):
+        gids, loc = result[r]
+        G[:, gids] = loc.reshape(S.shape[0], -1, qd)
+    assert np.array_equal(G.reshape(S.shape), S)
