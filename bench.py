@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--trace", type=int, default=200, help="requests in the serving trace")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both",
                     help="time one form only (profiling runs); the default line needs both")
-    ap.add_argument("--only", choices=["config1", "config3", "channel"], default=None,
+    ap.add_argument("--only", choices=["vortex2d", "ns3d_tgv", "channel"], default=None,
                     help="run one of the other configurations alone and print its JSON (profiling)")
     ap.add_argument("--variant", type=int, default=-1,
                     help="single-form runs: use this tile variant instead of the autotuner's pick")
@@ -255,13 +255,13 @@ def time_steps(D, stream, dt, steps, warmup, barrier, max_over_ranks, clk=None):
 
 
 def other_configs(dgm_b200, args, only=None):
-    """BASELINE configs 1 and 3 on this GPU.  Config 1: the 2-D isentropic
+    """The other benchmark cases on this GPU.  The 2-D isentropic
     vortex (16 x 16 Quads on [-5,5]^2, p=4, beta=5, LF, LSRK14, dt from CFL
     0.5, 200 steps) with its L2 distance from the FP64 oracle and from the
     exact (advected) vortex per conserved field, at q=6 (the reference's
     default q=p+2) and q=5; at q=5 the under-integrated scheme loses
     positivity in the oracle as well, so that leg reports the step block in
-    which each run first reports a non-physical state.  Config 3: the 3-D
+    which each run first reports a non-physical state.  The 3-D
     Navier-Stokes Taylor-Green vortex (24^3 Hex, p=7, q=8, Re=1600, Pr=0.71,
     Mach 0.1, Roe, LSRK14) timed over its first steps, with the
     kinetic-energy history (FP64).  And the reference's runs/chan regression
@@ -270,7 +270,7 @@ def other_configs(dgm_b200, args, only=None):
     import torch
     from dgm_b200 import requests as R
     res = {}
-    if only in (None, "config1"):
+    if only in (None, "vortex2d"):
         n, p, steps, block = 16, 4, 200, 10
         for q in (6, 5):
             mesh = dgm_b200.meshgen.box(2, (n, n), -5.0, 5.0, p, q)
@@ -322,9 +322,9 @@ def other_configs(dgm_b200, args, only=None):
                 c1["rel_l2_vs_exact_per_field"] = [rel_l2(a, b) for a, b in
                                                    zip(D.state(), R.vortex(x, y, beta=5.0, x0=dt * steps))]
             D.close()
-            res[f"config1_q{q}"] = c1
-    if only in (None, "config3"):
-        # config 3
+            res[f"vortex2d_q{q}"] = c1
+    if only in (None, "ns3d_tgv"):
+        # Navier-Stokes Taylor-Green, 24^3, p=7
         n, p, q, k3 = 24, 7, 8, 10
         mesh = dgm_b200.meshgen.box(3, (n, n, n), 0.0, 2 * math.pi, p, q)
         D = dgm_b200.Domain(mesh, dgm_b200.NS3D, flux="roe", inttype=dgm_b200.LSRK14, vis=1.0 / 1600.0, Pr=0.71)
@@ -357,7 +357,7 @@ def other_configs(dgm_b200, args, only=None):
             t += e0.elapsed_time(e1) / 1e3
             ke.append(kinetic_energy(D.state()))
         dof = 5 * n ** 3 * (p + 1) ** 3
-        res["config3"] = {"workload": "ns3d_taylor_green_24^3_p7_q8_re1600_pr0.71_roe_lsrk14", "steps_timed": k3,
+        res["ns3d_tgv"] = {"workload": "ns3d_taylor_green_24^3_p7_q8_re1600_pr0.71_roe_lsrk14", "steps_timed": k3,
                           "dt": dt, "value": dof * 14 * k3 / t, "unit": UNIT, "ms_per_step": 1e3 * t / k3,
                           "kinetic_energy": ke, "tile_us": [round(float(r[3]), 1) for r in rows],
                           # -dKE/dt at t=0 of the incompressible limit is nu <|grad u|^2> = 3 nu / 4
