@@ -262,7 +262,7 @@ def other_configs(dgm_b200, args, only=None):
     default q=p+2) and q=5; at q=5 the under-integrated scheme loses
     positivity in the oracle as well, so that leg reports the step block in
     which each run first reports a non-physical state.  The 3-D
-    Navier-Stokes Taylor-Green vortex (24^3 Hex, p=7, q=8, Re=1600, Pr=0.71,
+    Navier-Stokes Taylor-Green vortex (24^3 Hex, p=7, q=9, Re=1600, Pr=0.71,
     Mach 0.1, Roe, LSRK14) timed over its first steps, with the
     kinetic-energy history (FP64).  And the reference's runs/chan regression
     case (walls, bulk-flow hold) against its golden restart.  `only` runs one
@@ -324,8 +324,9 @@ def other_configs(dgm_b200, args, only=None):
             D.close()
             res[f"vortex2d_q{q}"] = c1
     if only in (None, "ns3d_tgv"):
-        # Navier-Stokes Taylor-Green, 24^3, p=7
-        n, p, q, k3 = 24, 7, 8, 10
+        # Navier-Stokes Taylor-Green, 24^3, p=7, q=p+2 (the reference's
+        # default quadrature; at q=p+1 grid-scale noise grows without bound)
+        n, p, q, k3 = 24, 7, 9, 10
         mesh = dgm_b200.meshgen.box(3, (n, n, n), 0.0, 2 * math.pi, p, q)
         D = dgm_b200.Domain(mesh, dgm_b200.NS3D, flux="roe", inttype=dgm_b200.LSRK14, vis=1.0 / 1600.0, Pr=0.71)
         x, y, z = D.coordinates()
@@ -345,24 +346,43 @@ def other_configs(dgm_b200, args, only=None):
             e = 0.5 * (U[1] ** 2 + U[2] ** 2 + U[3] ** 2) / U[0]
             return float((e.reshape(-1, q ** 3) * w).sum() / (w.sum() * e.size / q ** 3))
 
-        st = torch.cuda.ExternalStream(D.stream())
-        ke, t = [kinetic_energy(D.state())], 0.0
-        for _ in range(k3):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(st)
-            D.advance_async(dt, 1)
-            e1.record(st)
-            e1.synchronize()
-            D.sync()
-            t += e0.elapsed_time(e1) / 1e3
-            ke.append(kinetic_energy(D.state()))
+        def timed_steps(D):
+            st = torch.cuda.ExternalStream(D.stream())
+            ke, t = [kinetic_energy(D.state())], 0.0
+            for _ in range(k3):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                D.advance_async(dt, 1)
+                e1.record(st)
+                e1.synchronize()
+                D.sync()
+                t += e0.elapsed_time(e1) / 1e3
+                ke.append(kinetic_energy(D.state()))
+            return t, ke
+
+        t, ke = timed_steps(D)
         dof = 5 * n ** 3 * (p + 1) ** 3
-        res["ns3d_tgv"] = {"workload": "ns3d_taylor_green_24^3_p7_q8_re1600_pr0.71_roe_lsrk14", "steps_timed": k3,
+        res["ns3d_tgv"] = {"workload": "ns3d_taylor_green_24^3_p7_q9_re1600_pr0.71_roe_lsrk14", "steps_timed": k3,
                           "dt": dt, "value": dof * 14 * k3 / t, "unit": UNIT, "ms_per_step": 1e3 * t / k3,
                           "kinetic_energy": ke, "tile_us": [round(float(r[3]), 1) for r in rows],
                           # -dKE/dt at t=0 of the incompressible limit is nu <|grad u|^2> = 3 nu / 4
                           "dissipation_rate": (ke[0] - ke[-1]) / (k3 * dt), "dissipation_rate_t0_exact": 0.75 / 1600.0,
-                          "note": "FP64 BR1; the 1000-step run and the TF32 contraction form are not timed here"}
+                          "note": "FP64 BR1; the 1000-step run is not timed here"}
+        U64 = D.state()
+        D.close()
+        # the FP32 viscous form (precision MIXED): BR1 gradient and viscous
+        # kernels in FP32, stage kernel, registers and traces in FP64
+        D = dgm_b200.Domain(mesh, dgm_b200.NS3D, flux="roe", inttype=dgm_b200.LSRK14, vis=1.0 / 1600.0, Pr=0.71,
+                            precision=dgm_b200.MIXED)
+        D.set_state(U0)
+        D.advance(dt, 3)
+        D.set_state(U0)
+        t32, ke32 = timed_steps(D)
+        res["ns3d_tgv_fp32_viscous"] = {
+            "workload": "ns3d_taylor_green_24^3_p7_q9_re1600_pr0.71_roe_lsrk14", "steps_timed": k3,
+            "value": dof * 14 * k3 / t32, "unit": UNIT, "ms_per_step": 1e3 * t32 / k3,
+            "rel_l2_vs_fp64_per_field": [rel_l2(a, b) for a, b in zip(D.state(), U64)],
+            "kinetic_energy_rel_diff_vs_fp64": abs(ke32[-1] - ke[-1]) / ke[-1]}
         D.close()
     if only in (None, "channel"):
         # the reference's channel regression case (runs/chan: NS 3-D, 512 hexes, p=3,

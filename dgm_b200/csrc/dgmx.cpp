@@ -111,6 +111,10 @@ struct dgmx_domain {
   double bcpar[kMaxBcTypes + 1][5] = {};
   bool hold = false;
   double *R0 = nullptr, *cbar = nullptr;                 // hold: [e][n] constant coefficients, [n] means
+  // Navier-Stokes with precision = DGMX_MIXED: the BR1 viscous kernels run in
+  // FP32 (from the uncapped tile vops); stage, registers and traces stay FP64
+  bool visc32 = false;
+  const KernelOps *vops = nullptr;
   // element partition: ghost slots in the trace buffers and the halo
   // exchange lists (plan.nranks == 1: the whole mesh, no exchange)
   PartitionPlan plan;
@@ -181,6 +185,12 @@ struct dgmx_domain {
     return launch_hold(h, stream);
   }
   bool ns() const { return prm.physics == DGMX_NS2D || prm.physics == DGMX_NS3D; }
+  cudaError_t ns_grad(const StageArgs &a, bool nodal, cudaStream_t s) const {
+    return visc32 ? vops->ns_grad32(a, nodal, s) : ops->ns_grad(a, nodal, s);
+  }
+  cudaError_t ns_visc(const StageArgs &a, bool nodal, cudaStream_t s) const {
+    return visc32 ? vops->ns_visc32(a, nodal, s) : ops->ns_visc(a, nodal, s);
+  }
   bool mixed() const { return prm.precision == DGMX_MIXED; }
   const KernelOps *stage_ops() const { return mixed() ? ops_m : ops; }
 
@@ -371,8 +381,8 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
     const StageArgs a = stage_args(d, sp, dt);
     cudaError_t e;
     if (d->ns()) {
-      if ((e = d->ops->ns_grad(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous gradient kernel");
-      if ((e = d->ops->ns_visc(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
+      if ((e = d->ns_grad(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous gradient kernel");
+      if ((e = d->ns_visc(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
       d->launches += 2;
       dgmx_status xs = exchange(d, d->Vtr, (d->nf - 1) * d->gf);
       if (xs != DGMX_OK) return xs;
@@ -507,8 +517,12 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
   *out = nullptr;
   auto d = std::make_unique<dgmx_domain>();
   d->prm = *p;
+  const bool ns_phys = p->physics == DGMX_NS2D || p->physics == DGMX_NS3D;
   if (bspec && !bspec->sides.empty()) {
-    if (p->precision != DGMX_FP64) { g_create_error = "boundary sides are supported in FP64"; return DGMX_ERR_UNSUPPORTED; }
+    if (p->precision != DGMX_FP64 && !ns_phys) {
+      g_create_error = "boundary sides are supported in FP64 (and with the FP32 viscous form of Navier-Stokes)";
+      return DGMX_ERR_UNSUPPORTED;
+    }
     for (int t = 1; t <= bspec->ntypes; ++t) {
       const int k = bspec->kind[t];
       const bool euler = p->physics == DGMX_EULER3D || p->physics == DGMX_EULER2D;
@@ -549,9 +563,14 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
   if (p->flux != DGMX_FLUX_LF && p->flux != DGMX_FLUX_ROE) { g_create_error = "flux must be LF or Roe"; return DGMX_ERR_UNSUPPORTED; }
   if (phys == DGMX_SHALLOW && p->flux != DGMX_FLUX_LF) { g_create_error = "shallow water supports Lax-Friedrichs only"; return DGMX_ERR_UNSUPPORTED; }
   if (p->precision != DGMX_FP64 && p->precision != DGMX_MIXED) { g_create_error = "precision must be FP64 or MIXED"; return DGMX_ERR_ARGUMENT; }
-  if (p->precision == DGMX_MIXED && (p->inttype != DGMX_LSRK14 || phys == DGMX_NS2D || phys == DGMX_NS3D)) {
+  if (p->precision == DGMX_MIXED && p->inttype != DGMX_LSRK14 && !ns_phys) {
     g_create_error = "the mixed-precision form is built for LSRK14 with Euler and shallow water";
     return DGMX_ERR_UNSUPPORTED;
+  }
+  if (p->precision == DGMX_MIXED && ns_phys) {
+    // Navier-Stokes: FP32 viscous kernels, FP64 everything else
+    d->visc32 = true;
+    d->prm.precision = DGMX_FP64;
   }
   if (!m->porder || m->ne <= 0) { g_create_error = "mesh needs porder"; return DGMX_ERR_ARGUMENT; }
   const int pp = m->porder[0];
@@ -564,7 +583,14 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
     }
   }
   d->ops = find_ops(phys, pp + 1, qq);
-  if (d->ops && p->precision == DGMX_MIXED) {
+  if (d->visc32) {
+    d->vops = d->ops;
+    if (!d->vops || !d->vops->ns_grad32) {
+      g_create_error = "no FP32 viscous kernels built for p=" + std::to_string(pp) + ", q=" + std::to_string(qq);
+      return DGMX_ERR_UNSUPPORTED;
+    }
+  }
+  if (d->ops && d->prm.precision == DGMX_MIXED) {
     d->ops_m = find_ops(phys + kMixedKey, pp + 1, qq);
     if (!d->ops_m) {
       g_create_error = "no mixed-precision kernels built for p=" + std::to_string(pp) + ", q=" + std::to_string(qq);
@@ -1044,8 +1070,8 @@ dgmx_status dgmx_time_derivative_device(dgmx_domain *d, const double *U_dev, dou
     a.Rsub = d->Rsw;
   }
   if (d->ns()) {
-    if ((e = d->ops->ns_grad(a, true, d->stream)) != cudaSuccess) return d->cuda(e, "viscous gradient kernel");
-    if ((e = d->ops->ns_visc(a, true, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
+    if ((e = d->ns_grad(a, true, d->stream)) != cudaSuccess) return d->cuda(e, "viscous gradient kernel");
+    if ((e = d->ns_visc(a, true, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
     d->launches += 2;
     if ((xs = exchange(d, d->Vtr, (d->nf - 1) * d->gf)) != DGMX_OK) return xs;
   }
@@ -1422,8 +1448,8 @@ dgmx_status dgmx_group_advance(dgmx_group *g, double dt, int nsteps) {
       if (d0->ns()) {
         for (dgmx_domain *d : g->parts) {
           const StageArgs a = stage_args(d, sp, dt);
-          if (e == cudaSuccess) e = d->ops->ns_grad(a, false, s);
-          if (e == cudaSuccess) e = d->ops->ns_visc(a, false, s);
+          if (e == cudaSuccess) e = d->ns_grad(a, false, s);
+          if (e == cudaSuccess) e = d->ns_visc(a, false, s);
           d->launches += 2;
         }
         if (e == cudaSuccess && (st = group_exchange(g, 2, s)) != DGMX_OK) return st;

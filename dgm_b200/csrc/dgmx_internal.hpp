@@ -275,6 +275,10 @@ struct KernelOps {
   // nodal = read GLL values from a.Xn instead of the modal register a.X
   cudaError_t (*ns_grad)(const StageArgs &a, bool nodal, cudaStream_t s) = nullptr;
   cudaError_t (*ns_visc)(const StageArgs &a, bool nodal, cudaStream_t s) = nullptr;
+  // the same in FP32 (Navier-Stokes with precision = DGMX_MIXED); set on the
+  // uncapped tile of each (physics, L, Q, EPB)
+  cudaError_t (*ns_grad32)(const StageArgs &a, bool nodal, cudaStream_t s) = nullptr;
+  cudaError_t (*ns_visc32)(const StageArgs &a, bool nodal, cudaStream_t s) = nullptr;
 };
 void register_ops(int physics, int L, int Q, const KernelOps &ops);
 const KernelOps *find_ops(int physics, int L, int Q);            // default variant

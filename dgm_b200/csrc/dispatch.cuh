@@ -63,7 +63,38 @@ struct Launch {
       if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
       if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
     }
+    if constexpr (is_ns(PHYS) && !MIXED && MINB == 0) {
+      // the FP32 viscous kernels (one set per (physics, L, Q, EPB): the
+      // uncapped tile carries them) and their FP32 tables
+      using N = NsCfg<C, float>;
+      if ((e = upload_tables_lq<L, Q, float>(t)) != cudaSuccess) return e;
+      const int sg = (int)N::Grad::SMEM, sv = (int)N::Visc::SMEM;
+      if ((e = cudaFuncSetAttribute(ns_grad_kernel<C, PHYS, false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
+      if ((e = cudaFuncSetAttribute(ns_grad_kernel<C, PHYS, true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
+      if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+      if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+    }
     return cudaSuccess;
+  }
+  static cudaError_t ns_grad32(const StageArgs &a, bool nodal, cudaStream_t s) {
+    if constexpr (is_ns(PHYS) && !MIXED && MINB == 0) {
+      using N = NsCfg<C, float>;
+      if (nodal) ns_grad_kernel<C, PHYS, true, float><<<grid(a.ne), C::NT, N::Grad::SMEM, s>>>(a);
+      else ns_grad_kernel<C, PHYS, false, float><<<grid(a.ne), C::NT, N::Grad::SMEM, s>>>(a);
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
+  }
+  static cudaError_t ns_visc32(const StageArgs &a, bool nodal, cudaStream_t s) {
+    if constexpr (is_ns(PHYS) && !MIXED && MINB == 0) {
+      using N = NsCfg<C, float>;
+      if (nodal) ns_visc_kernel<C, PHYS, true, float><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
+      else ns_visc_kernel<C, PHYS, false, float><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
   }
   static cudaError_t ns_grad(const StageArgs &a, bool nodal, cudaStream_t s) {
     if constexpr (is_ns(PHYS) && !MIXED) {
@@ -144,6 +175,7 @@ struct Launch {
     o.init = init; o.stage = stage; o.traces_modal = traces_modal; o.traces_nodal = traces_nodal;
     o.rhs_nodal = rhs_nodal; o.forward = forward; o.backward = backward;
     if constexpr (is_ns(PHYS) && !MIXED) { o.ns_grad = ns_grad; o.ns_visc = ns_visc; }
+    if constexpr (is_ns(PHYS) && !MIXED && MINB == 0) { o.ns_grad32 = ns_grad32; o.ns_visc32 = ns_visc32; }
     return o;
   }
 };

@@ -23,7 +23,13 @@ namespace dgmx {
 
 constexpr bool is_ns(int p) { return p == DGMX_NS2D || p == DGMX_NS3D; }
 
-template <class C>
+// Bytes of a viscous kernel's value regions, rounded up to 8: the geometry
+// slots that follow hold doubles, and an odd number of float values would
+// leave them on a 4-byte boundary (a no-op for double values).
+template <class V>
+constexpr size_t ns_data_bytes(int values) { return ((size_t)values * sizeof(V) + 7) & ~(size_t)7; }
+
+template <class C, class V = double>
 struct NsCfg {
   static constexpr int DIM = C::DIM, NF = C::NF, L = C::L, Q = C::Q, G = C::G;
   static constexpr int EPB = C::EPB, NFACE = C::NFACE, NT = C::NT;
@@ -40,19 +46,29 @@ struct NsCfg {
   // (at most 3 at a time) keep the transform scratch at the size the
   // per-component passes need
   static constexpr int NB1 = (EPB == 1 && NF > 3) ? 3 : NF;
-  // ns_grad_kernel regions (per slot, doubles); the modal input A is dead
-  // after the backward transform, so the primitive component Qc and its
-  // gradient Gd live in it
+  // ns_grad_kernel regions (per slot, counted in values of the working
+  // type); the modal input A is dead after the backward transform, so the
+  // primitive component Qc and its gradient Gd live in it.  The state
+  // traces E, E2 are double in both forms (the BR1 lift inputs are formed
+  // from them in double), and the FP32 form keeps each slot's density and
+  // energy means in Rs (double): its GLL state holds rho - rho_mean and
+  // E - E_mean, so the internal energy is formed without the cancellation
+  // of E/rho (about 1/(gamma (gamma-1) Ma^2)) against |u|^2/2 in FP32.
   struct Grad {
+    static constexpr bool F32 = std::is_same<V, float>::value;
+    static constexpr int DW = (int)(sizeof(double) / sizeof(V));   // values per double
+    static constexpr int pad(int n) { return (n + DW - 1) / DW * DW; }
     static constexpr int Qc = QD, Gd = DIM * QD;
-    static constexpr int A = cmax(NF * LD, Qc + Gd), B = NF * QD, E = NFACE * NF * GF, E2 = NFACE * NF * GF;
+    static constexpr int A = pad(cmax(NF * LD, Qc + Gd)), B = pad(NF * QD);
+    static constexpr int E = NFACE * NF * GF * DW, E2 = NFACE * NF * GF * DW, Rs = F32 ? 2 * DW : 0;
     static constexpr int Fc = NFACE * DIM * GF, LFc = cmax(NFACE * DIM * QF, DIM * F2);
     static constexpr int S1 = cmax(cmax(NB1 * P1, DIM == 3 ? NFACE * DIM * Q * G : 0), DIM * F1);
     static constexpr int S2 = cmax(cmax(NB1 * P2, DIM * F2), DIM * LD);
-    static constexpr int SLOT = A + B + E + E2 + Fc + LFc + S1 + S2;
-    static constexpr size_t SMEM = (size_t)EPB * SLOT * 8 + (size_t)EPB * (sizeof(GeomClass) + NFACE * 16 + 16);
+    static constexpr int SLOT = A + B + E + E2 + Rs + Fc + LFc + S1 + S2;
+    static constexpr size_t DATA = ns_data_bytes<V>(EPB * SLOT);
+    static constexpr size_t SMEM = DATA + (size_t)EPB * (sizeof(GeomClass) + NFACE * 16 + 16);
   };
-  // ns_visc_kernel regions (per slot, doubles).  G holds the velocity
+  // ns_visc_kernel regions (per slot, values of the working type).  G holds the velocity
   // gradient, then in place the symmetric stress and the heat flux (NGS
   // slots: 6 + 3 in 3-D, 3 + 2 in 2-D; the modal input is parked there
   // first); the energy gradient goes to Dv, which then accumulates one
@@ -70,8 +86,10 @@ struct NsCfg {
     static constexpr int S2 = cmax(cmax(NB1 * P2, DIM * P2), LD);
     static constexpr int Dv = DIM * QD;
     static constexpr int SLOT = B + G + X + S1 + S2 + Dv;
-    static constexpr size_t SMEM = (size_t)EPB * SLOT * 8 + (size_t)EPB * (sizeof(GeomClass) + NFACE * 16 + 16);
+    static constexpr size_t DATA = ns_data_bytes<V>(EPB * SLOT);
+    static constexpr size_t SMEM = DATA + (size_t)EPB * (sizeof(GeomClass) + NFACE * 16 + 16);
     static_assert(DIM * DIM <= NGS, "the velocity gradient fits the stress slots");
+    static_assert(DATA % 8 == 0 && DATA >= (size_t)EPB * SLOT * sizeof(V), "geometry slots 8-byte aligned");
   };
   // slot of component d of the viscous flux vector g_n (n: momentum x, y,
   // [z], energy) in the symmetric stress / heat-flux layout
@@ -96,21 +114,21 @@ struct NsCfg {
 
 // Primitive variables of one conserved state (src/Euler3d.cpp:1170-1182):
 // q = (u, v, [w], e) with e the internal energy.
-template <int DIM>
-__device__ __forceinline__ void primitive(const double *U, double *q) {
-  const double r = U[0];
-  double wk;
+template <int DIM, class V>
+__device__ __forceinline__ void primitive(const V *U, V *q) {
+  const V r = U[0];
+  V wk;
   if constexpr (DIM == 3) {
-    const double u = U[1] / r, v = U[2] / r, w = U[3] / r;
-    double e = U[4] / r;
+    const V u = U[1] / r, v = U[2] / r, w = U[3] / r;
+    V e = U[4] / r;
     wk = u * u; wk = fma(v, v, wk); wk = fma(w, w, wk);
-    e = fma(-0.5, wk, e);
+    e = fma(V(-0.5), wk, e);
     q[0] = u; q[1] = v; q[2] = w; q[3] = e;
   } else {
-    const double u = U[1] / r, v = U[2] / r;
-    double e = U[3] / r;
+    const V u = U[1] / r, v = U[2] / r;
+    V e = U[3] / r;
     wk = u * u; wk = fma(v, v, wk);
-    e = fma(-0.5, wk, e);
+    e = fma(V(-0.5), wk, e);
     q[0] = u; q[1] = v; q[2] = e;
   }
 }
@@ -119,14 +137,14 @@ __device__ __forceinline__ void primitive(const double *U, double *q) {
 // point order.  A boundary side's neighbour is its ghost state in the
 // viscous BC database (Navier_Stokes3d::enforce_bc,
 // src/Navier_Stokes3d.cpp:457-461; ghost_state) made from the own trace.
-template <class C>
-__device__ __forceinline__ void load_nbr_traces(double *E2, const double *T, const FaceLink *lnk, const int *eid,
+template <class C, class V>
+__device__ __forceinline__ void load_nbr_traces(V *E2, const double *T, const FaceLink *lnk, const int *eid,
                                                 const GeomClass *geo, const StageArgs &a, int tid) {
   constexpr int NF = C::NF, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
   for (int w = tid; w < NFACE * EPB * NF * GF; w += C::NT) {
     const int f = w / (EPB * NF * GF), rem = w - f * EPB * NF * GF;
     const int s = rem / (NF * GF), ng = rem - s * NF * GF, n = ng / GF, g = ng - n * GF;
-    double v = n == 0 ? 1.0 : 0.0;
+    V v = V(n == 0 ? 1.0 : 0.0);
     if (eid[s] >= 0) {
       const FaceLink lk = lnk[s * NFACE + f];
       const int bt = (geo[s].bc >> (4 * f)) & 15;
@@ -136,9 +154,9 @@ __device__ __forceinline__ void load_nbr_traces(double *E2, const double *T, con
 #pragma unroll
         for (int k = 0; k < NF; ++k) Uo[k] = t[k * GF];
         ghost_state<C::DIM, NF>(a.bckind[bt], a.bcpar[bt], Uo, geo[s].onrm[f], true, Un);
-        v = Un[n];
+        v = V(Un[n]);
       } else {
-        v = t[n * GF];
+        v = V(t[n * GF]);
       }
     }
     E2[w] = v;
@@ -147,22 +165,22 @@ __device__ __forceinline__ void load_nbr_traces(double *E2, const double *T, con
 
 // G2GL of NB face-major arrays [f][slot][b][GF] and accumulation with the
 // inverse end weights into dst [slot][b][QD] (faces in increasing order).
-template <class C, int NB>
-__device__ __forceinline__ void lift_batch(const double *Fg, double *LFc, double *S, double *dst, int tid) {
+template <class C, int NB, class V>
+__device__ __forceinline__ void lift_batch(const V *Fg, V *LFc, V *S, V *dst, int tid) {
   constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G, EPB = C::EPB, QD = C::QD, QF = C::QF;
   constexpr int NBT = C::NFACE * EPB * NB;
   if constexpr (DIM == 3) {
-    contract<G, G, 1, 0, G, Q, MatG2GL<L, Q>, false>(Fg, S, NBT, G * G, Q * G, tid, C::NT);
+    contract<G, G, 1, 0, G, Q, MatG2GL<L, Q, V>, false>(Fg, S, NBT, G * G, Q * G, tid, C::NT);
     __syncthreads();
-    contract<Q, G, 1, 1, G, Q, MatG2GL<L, Q>, false>(S, LFc, NBT, Q * G, Q * Q, tid, C::NT);
+    contract<Q, G, 1, 1, G, Q, MatG2GL<L, Q, V>, false>(S, LFc, NBT, Q * G, Q * Q, tid, C::NT);
   } else {
-    contract<G, 1, 1, 0, G, Q, MatG2GL<L, Q>, false>(Fg, LFc, NBT, G, Q, tid, C::NT);
+    contract<G, 1, 1, 0, G, Q, MatG2GL<L, Q, V>, false>(Fg, LFc, NBT, G, Q, tid, C::NT);
   }
   __syncthreads();
-  const double w0 = 1.0 / cW<double, L, Q>[0], w1 = 1.0 / cW<double, L, Q>[Q - 1];
+  const V w0 = V(1.0) / cW<V, L, Q>[0], w1 = V(1.0) / cW<V, L, Q>[Q - 1];
   for (int w = tid; w < EPB * NB * QD; w += C::NT) {
     const int slot = w / (NB * QD), rem = w - slot * NB * QD, b = rem / QD, p = rem - b * QD;
-    double acc = dst[w];
+    V acc = dst[w];
     if constexpr (DIM == 3) {
       const int i = p / (Q * Q), j = (p / Q) % Q, k = p % Q;
       auto lf = [&](int f, int x, int y) { return LFc[((f * EPB + slot) * NB + b) * QF + x * Q + y]; };
@@ -187,45 +205,45 @@ __device__ __forceinline__ void lift_batch(const double *Fg, double *LFc, double
 
 // w-weighted projection of NB arrays [slot][b][QD] (weighted in place) to
 // modal dst [slot][b][LD].
-template <class C, int NB>
-__device__ __forceinline__ void forward_batch(double *src, double *dst, double *S1, double *S2, int tid) {
+template <class C, int NB, class V>
+__device__ __forceinline__ void forward_batch(V *src, V *dst, V *S1, V *S2, int tid) {
   constexpr int DIM = C::DIM, L = C::L, Q = C::Q, QD = C::QD, LD = C::LD, NBT = C::EPB * NB;
   for (int w = tid; w < NBT * QD; w += C::NT) {
     const int p = w % QD;
-    double wq;
-    if constexpr (DIM == 3) wq = cW<double, L, Q>[p / (Q * Q)] * cW<double, L, Q>[(p / Q) % Q] * cW<double, L, Q>[p % Q];
-    else wq = cW<double, L, Q>[p / Q] * cW<double, L, Q>[p % Q];
+    V wq;
+    if constexpr (DIM == 3) wq = cW<V, L, Q>[p / (Q * Q)] * cW<V, L, Q>[(p / Q) % Q] * cW<V, L, Q>[p % Q];
+    else wq = cW<V, L, Q>[p / Q] * cW<V, L, Q>[p % Q];
     src[w] = wq * src[w];
   }
   __syncthreads();
   if constexpr (DIM == 3) {
-    contract<Q, Q, Q, 0, Q, L, MatBt<L, Q>, false>(src, S1, NBT, QD, L * Q * Q, tid, C::NT);
+    contract<Q, Q, Q, 0, Q, L, MatBt<L, Q, V>, false>(src, S1, NBT, QD, L * Q * Q, tid, C::NT);
     __syncthreads();
-    contract<L, Q, Q, 1, Q, L, MatBt<L, Q>, false>(S1, S2, NBT, L * Q * Q, L * L * Q, tid, C::NT);
+    contract<L, Q, Q, 1, Q, L, MatBt<L, Q, V>, false>(S1, S2, NBT, L * Q * Q, L * L * Q, tid, C::NT);
     __syncthreads();
-    contract<L, L, Q, 2, Q, L, MatBt<L, Q>, false>(S2, dst, NBT, L * L * Q, LD, tid, C::NT);
+    contract<L, L, Q, 2, Q, L, MatBt<L, Q, V>, false>(S2, dst, NBT, L * L * Q, LD, tid, C::NT);
   } else {
-    contract<Q, Q, 1, 0, Q, L, MatBt<L, Q>, false>(src, S1, NBT, QD, L * Q, tid, C::NT);
+    contract<Q, Q, 1, 0, Q, L, MatBt<L, Q, V>, false>(src, S1, NBT, QD, L * Q, tid, C::NT);
     __syncthreads();
-    contract<L, Q, 1, 1, Q, L, MatBt<L, Q>, false>(S1, dst, NBT, L * Q, LD, tid, C::NT);
+    contract<L, Q, 1, 1, Q, L, MatBt<L, Q, V>, false>(S1, dst, NBT, L * Q, LD, tid, C::NT);
   }
   __syncthreads();
 }
 
 // modal [slot][b][LD] -> GLL [slot][b][QD]
-template <class C, int NB>
-__device__ __forceinline__ void backward_batch(const double *src, double *dst, double *S1, double *S2, int tid) {
+template <class C, int NB, class V>
+__device__ __forceinline__ void backward_batch(const V *src, V *dst, V *S1, V *S2, int tid) {
   constexpr int L = C::L, Q = C::Q, NBT = C::EPB * NB;
   if constexpr (C::DIM == 3) {
-    contract<L, L, L, 0, L, Q, MatB<L, Q>, false>(src, S1, NBT, C::LD, Q * L * L, tid, C::NT);
+    contract<L, L, L, 0, L, Q, MatB<L, Q, V>, false>(src, S1, NBT, C::LD, Q * L * L, tid, C::NT);
     __syncthreads();
-    contract<Q, L, L, 1, L, Q, MatB<L, Q>, false>(S1, S2, NBT, Q * L * L, Q * Q * L, tid, C::NT);
+    contract<Q, L, L, 1, L, Q, MatB<L, Q, V>, false>(S1, S2, NBT, Q * L * L, Q * Q * L, tid, C::NT);
     __syncthreads();
-    contract<Q, Q, L, 2, L, Q, MatB<L, Q>, false>(S2, dst, NBT, Q * Q * L, C::QD, tid, C::NT);
+    contract<Q, Q, L, 2, L, Q, MatB<L, Q, V>, false>(S2, dst, NBT, Q * Q * L, C::QD, tid, C::NT);
   } else {
-    contract<L, L, 1, 0, L, Q, MatB<L, Q>, false>(src, S1, NBT, C::LD, Q * L, tid, C::NT);
+    contract<L, L, 1, 0, L, Q, MatB<L, Q, V>, false>(src, S1, NBT, C::LD, Q * L, tid, C::NT);
     __syncthreads();
-    contract<Q, L, 1, 1, L, Q, MatB<L, Q>, false>(S1, dst, NBT, Q * L, C::QD, tid, C::NT);
+    contract<Q, L, 1, 1, L, Q, MatB<L, Q, V>, false>(S1, dst, NBT, Q * L, C::QD, tid, C::NT);
   }
   __syncthreads();
 }
@@ -244,30 +262,107 @@ __device__ __forceinline__ void load_geo_slots(GeomClass *geo, FaceLink *lnk, in
   }
 }
 
+// Element-major modal registers, GLL values and own traces of the slot's
+// elements in the working type V (elements past the end read a unit
+// density and zero otherwise).
+template <class C, class V>
+__device__ __forceinline__ void load_modal_v(V *dst, const double *src, int e0, int ne, int tid) {
+  constexpr int BLK = C::NF * C::LD;
+  for (int w = tid; w < C::EPB * BLK; w += C::NT) {
+    const int e = e0 + w / BLK;
+    dst[w] = e < ne ? V(src[(size_t)e0 * BLK + w]) : V(w % C::LD == 0 ? 1.0 : 0.0);
+  }
+}
+
+template <class C, class V>
+__device__ __forceinline__ void load_nodal_v(V *B, const double *Xn, int e0, int ne, int tid) {
+  constexpr int NF = C::NF, QD = C::QD;
+  for (int w = tid; w < C::EPB * NF * QD; w += C::NT) {
+    const int s = w / (NF * QD), rem = w - s * NF * QD, n = rem / QD, p = rem - n * QD;
+    const int e = e0 + s;
+    B[w] = e < ne ? V(Xn[((size_t)n * ne + e) * QD + p]) : V(n == 0 ? 1.0 : 0.0);
+  }
+}
+
+template <class C, class V>
+__device__ __forceinline__ void load_own_traces_v(V *E, const double *T, int e0, int ne, int tid) {
+  constexpr int NF = C::NF, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB;
+  for (int w = tid; w < EPB * NFACE * NF * GF; w += C::NT) {
+    const int s = w / (NFACE * NF * GF), rem = w - s * NFACE * NF * GF;
+    const int f = rem / (NF * GF), ng = rem - f * NF * GF;
+    const int e = e0 + s;
+    E[(f * EPB + s) * NF * GF + ng] = e < ne ? V(T[(size_t)e * NFACE * NF * GF + rem]) : V(ng < GF ? 1.0 : 0.0);
+  }
+}
+
+// The FP32 gradient kernel's state: the slot's modal registers (or, NODAL,
+// GLL values) with the density and energy means taken out in double before
+// rounding.  Modal: the constant coefficients c0 of density and energy go to
+// Rs as means c0 phi0 (phi0 = 2^(-DIM/2), the constant orthonormal mode) and
+// are zeroed.  Nodal: each element's values at its first point are the
+// reference values subtracted.  Elements past the end read a unit density.
+template <class C>
+__device__ __forceinline__ void load_state_shifted(float *dst, double *Rs, const double *src, bool nodal, int e0,
+                                                   int ne, int tid) {
+  constexpr int NF = C::NF, LD = C::LD, QD = C::QD, EPB = C::EPB;
+  const double phi0 = C::DIM == 3 ? 0.35355339059327373 : 0.5;
+  if (nodal) {
+    for (int w = tid; w < EPB * NF * QD; w += C::NT) {
+      const int s = w / (NF * QD), rem = w - s * NF * QD, n = rem / QD, p = rem - n * QD;
+      const int e = e0 + s;
+      double x = e < ne ? src[((size_t)n * ne + e) * QD + p] : (n == 0 ? 1.0 : 0.0);
+      if (n == 0 || n == NF - 1) {
+        const double ref = e < ne ? src[((size_t)n * ne + e) * QD] : (n == 0 ? 1.0 : 0.0);
+        if (p == 0) Rs[2 * s + (n == 0 ? 0 : 1)] = ref;
+        x -= ref;
+      }
+      dst[w] = float(x);
+    }
+  } else {
+    constexpr int BLK = NF * LD;
+    for (int w = tid; w < EPB * BLK; w += C::NT) {
+      const int s = w / BLK, k = w - s * BLK, n = k / LD, m = k - n * LD;
+      const int e = e0 + s;
+      double x = e < ne ? src[(size_t)e0 * BLK + w] : (m == 0 ? 1.0 : 0.0);
+      if (m == 0 && (n == 0 || n == NF - 1)) {
+        Rs[2 * s + (n == 0 ? 0 : 1)] = x * phi0;
+        x = 0.0;
+      }
+      dst[w] = float(x);
+    }
+  }
+}
+
 // ---------------------------------------------------------------- gradients
-template <class C, int PHYS, bool NODAL>
-__global__ void __launch_bounds__(C::NT, NsCfg<C>::GRAD_MINB) ns_grad_kernel(StageArgs a) {
-  using N = NsCfg<C>;
+// V: working type (double, or float for the FP32 viscous form); inputs and
+// outputs in global memory stay double.
+template <class C, int PHYS, bool NODAL, class V = double>
+__global__ void __launch_bounds__(C::NT, NsCfg<C, V>::GRAD_MINB) ns_grad_kernel(StageArgs a) {
+  using N = NsCfg<C, V>;
   using R = typename N::Grad;
   constexpr int DIM = C::DIM, NF = C::NF, Q = C::Q, L = C::L, EPB = C::EPB, QD = C::QD, GF = C::GF;
   constexpr int NFACE = C::NFACE, NVC = N::NVC, LD = C::LD;
   extern __shared__ __align__(16) unsigned char smem_bytes[];
-  double *smem_raw = reinterpret_cast<double *>(smem_bytes);
-  double *A = smem_raw, *B = A + EPB * R::A, *E = B + EPB * R::B, *E2 = E + EPB * R::E;
-  double *Fc = E2 + EPB * R::E2, *LFc = Fc + EPB * R::Fc;
-  double *S1 = LFc + EPB * R::LFc, *S2 = S1 + EPB * R::S1;
-  double *Qc = A, *Gd = A + EPB * R::Qc;     // in the modal input, dead after the backward transform
-  GeomClass *geo = reinterpret_cast<GeomClass *>(S2 + EPB * R::S2);
+  V *smem_raw = reinterpret_cast<V *>(smem_bytes);
+  V *A = smem_raw, *B = A + EPB * R::A;
+  double *E = reinterpret_cast<double *>(B + EPB * R::B), *E2 = reinterpret_cast<double *>(B + EPB * (R::B + R::E));
+  double *Rs = reinterpret_cast<double *>(B + EPB * (R::B + R::E + R::E2));
+  V *Fc = B + EPB * (R::B + R::E + R::E2 + R::Rs), *LFc = Fc + EPB * R::Fc;
+  V *S1 = LFc + EPB * R::LFc, *S2 = S1 + EPB * R::S1;
+  V *Qc = A, *Gd = A + EPB * R::Qc;     // in the modal input, dead after the backward transform
+  GeomClass *geo = reinterpret_cast<GeomClass *>(smem_bytes + R::DATA);
   FaceLink *lnk = reinterpret_cast<FaceLink *>(geo + EPB);
   int *eid = reinterpret_cast<int *>(lnk + EPB * NFACE);
   const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
   load_geo_slots<C>(geo, lnk, eid, a, e0, tid);
-  if constexpr (NODAL) {
-    load_nodal<C>(B, a.Xn, e0, a.ne, tid);
+  if constexpr (R::F32) {
+    load_state_shifted<C>(NODAL ? B : A, Rs, NODAL ? a.Xn : a.X, NODAL, e0, a.ne, tid);
+  } else if constexpr (NODAL) {
+    load_nodal_v<C>(B, a.Xn, e0, a.ne, tid);
   } else {
-    load_modal<C>(A, a.X, e0, a.ne, tid);
+    load_modal_v<C>(A, a.X, e0, a.ne, tid);
   }
-  load_own_traces<C, double, false>(E, a.Tin, e0, a.ne, tid);
+  load_own_traces_v<C>(E, a.Tin, e0, a.ne, tid);
   __syncthreads();
   load_nbr_traces<C>(E2, a.Tin, lnk, eid, geo, a, tid);
   if constexpr (!NODAL) {
@@ -284,15 +379,37 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::GRAD_MINB) ns_grad_kernel(Sta
     // primitive component c at the GLL points
     for (int w = tid; w < EPB * QD; w += C::NT) {
       const int s = w / QD, p = w - s * QD;
-      double U[5], q[4];
+      if constexpr (R::F32) {
+        // B holds rho' = rho - rb, the momenta and E' = E - Eb; with
+        // rho = rb + rho', E/rho - Eb/rb = (E' rb - Eb rho') / (rb rho), so
+        // e - Eb/rb (a per-element constant shift, invisible to the gradient)
+        // is formed from O(Ma^2) terms
+        const V rb = V(Rs[2 * s]), Eb = V(Rs[2 * s + 1]);
+        const V rp = B[(s * NF) * QD + p], r = rb + rp;
+        if (c < DIM) {
+          Qc[w] = B[(s * NF + 1 + c) * QD + p] / r;
+        } else {
+          V k = V(0.0);
 #pragma unroll
-      for (int n = 0; n < NF; ++n) U[n] = B[(s * NF + n) * QD + p];
-      primitive<DIM>(U, q);
-      Qc[w] = q[c];
+          for (int d = 0; d < DIM; ++d) {
+            const V u = B[(s * NF + 1 + d) * QD + p] / r;
+            k = fma(u, u, k);
+          }
+          const V Ep = B[(s * NF + NF - 1) * QD + p];
+          Qc[w] = fma(V(-0.5), k, (Ep * rb - Eb * rp) / (rb * r));
+        }
+      } else {
+        V U[5], q[4];
+#pragma unroll
+        for (int n = 0; n < NF; ++n) U[n] = B[(s * NF + n) * QD + p];
+        primitive<DIM>(U, q);
+        Qc[w] = q[c];
+      }
     }
     // lift inputs ({{q_c}} - q_c) J n_d per face point, master-frame average
     for (int w = tid; w < NFACE * EPB * GF; w += C::NT) {
       const int f = w / (EPB * GF), rem = w - f * EPB * GF, s = rem / GF, g = rem - s * GF;
+      // formed in double in both forms, then rounded to the working type
       double Uo[5], Un[5], qo[4], qn[4];
 #pragma unroll
       for (int n = 0; n < NF; ++n) {
@@ -306,27 +423,27 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::GRAD_MINB) ns_grad_kernel(Sta
       const double avg = master ? 0.5 * (qo[c] + qn[c]) : 0.5 * (qn[c] + qo[c]);
       const double d = (avg - qo[c]) * gc.jr[f];
 #pragma unroll
-      for (int k = 0; k < DIM; ++k) Fc[((f * EPB + s) * DIM + k) * GF + g] = gc.onrm[f][k] * d;
+      for (int k = 0; k < DIM; ++k) Fc[((f * EPB + s) * DIM + k) * GF + g] = V(gc.onrm[f][k] * d);
     }
     __syncthreads();
     // collocation derivatives along r, s, t
     using Sh = Sh3<DIM, Q>;
-    contract<Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<L, Q>, false>(Qc, Gd, EPB, QD, DIM * QD, tid, C::NT);
-    contract<Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<L, Q>, false>(Qc, Gd + QD, EPB, QD, DIM * QD, tid, C::NT);
+    contract<Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<L, Q, V>, false>(Qc, Gd, EPB, QD, DIM * QD, tid, C::NT);
+    contract<Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<L, Q, V>, false>(Qc, Gd + QD, EPB, QD, DIM * QD, tid, C::NT);
     if constexpr (DIM == 3)
-      contract<Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<L, Q>, false>(Qc, Gd + 2 * QD, EPB, QD, DIM * QD, tid, C::NT);
+      contract<Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<L, Q, V>, false>(Qc, Gd + 2 * QD, EPB, QD, DIM * QD, tid, C::NT);
     __syncthreads();
     // chain rule (src/Hex.cpp:1994-2006): d/dx = rx d/dr + sx d/ds + tx d/dt
     for (int w = tid; w < EPB * QD; w += C::NT) {
       const int s = w / QD, p = w - s * QD;
-      double *g = Gd + s * DIM * QD + p;
+      V *g = Gd + s * DIM * QD + p;
       const double *m = geo[s].metric;
-      const double fr = g[0], fs = g[QD], ft = DIM == 3 ? g[2 * QD] : 0.0;
+      const V fr = g[0], fs = g[QD], ft = DIM == 3 ? g[2 * QD] : V(0.0);
 #pragma unroll
       for (int k = 0; k < DIM; ++k) {
-        double v = m[0 * 3 + k] * fr;
-        v = fma(m[1 * 3 + k], fs, v);
-        if (DIM == 3) v = fma(m[2 * 3 + k], ft, v);
+        V v = V(m[0 * 3 + k]) * fr;
+        v = fma(V(m[1 * 3 + k]), fs, v);
+        if (DIM == 3) v = fma(V(m[2 * 3 + k]), ft, v);
         g[k * QD] = v;
       }
     }
@@ -336,34 +453,34 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::GRAD_MINB) ns_grad_kernel(Sta
     for (int w = tid; w < EPB * DIM * LD; w += C::NT) {
       const int s = w / (DIM * LD), rem = w - s * DIM * LD;
       const int e = e0 + s;
-      if (e < a.ne) a.Ghat[((size_t)e * NVC + c) * DIM * LD + rem] = S2[w];
+      if (e < a.ne) a.Ghat[((size_t)e * NVC + c) * DIM * LD + rem] = double(S2[w]);
     }
     __syncthreads();
   }
 }
 
 // ----------------------------------------------- stresses, traces, divergence
-template <class C, int PHYS, bool NODAL>
-__global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(StageArgs a) {
-  using N = NsCfg<C>;
+template <class C, int PHYS, bool NODAL, class V = double>
+__global__ void __launch_bounds__(C::NT, NsCfg<C, V>::VISC_MINB) ns_visc_kernel(StageArgs a) {
+  using N = NsCfg<C, V>;
   using R = typename N::Visc;
   constexpr int DIM = C::DIM, NF = C::NF, Q = C::Q, L = C::L, G = C::G, EPB = C::EPB, QD = C::QD;
   constexpr int GF = C::GF, QF = C::QF, NFACE = C::NFACE, NV = N::NV, NVC = N::NVC, LD = C::LD, NGS = R::NGS;
   extern __shared__ __align__(16) unsigned char smem_bytes[];
-  double *smem_raw = reinterpret_cast<double *>(smem_bytes);
-  double *B = smem_raw, *Gg = B + EPB * R::B, *X = Gg + EPB * R::G;
-  double *S1 = X + EPB * R::X, *S2 = S1 + EPB * R::S1, *Dv = S2 + EPB * R::S2;
-  double *Gh = X, *Fg = X;                    // first loop / second loop
-  double *FF = B, *Cv = B + EPB * R::FF;      // after the stresses are formed
-  GeomClass *geo = reinterpret_cast<GeomClass *>(Dv + EPB * R::Dv);
+  V *smem_raw = reinterpret_cast<V *>(smem_bytes);
+  V *B = smem_raw, *Gg = B + EPB * R::B, *X = Gg + EPB * R::G;
+  V *S1 = X + EPB * R::X, *S2 = S1 + EPB * R::S1, *Dv = S2 + EPB * R::S2;
+  V *Gh = X, *Fg = X;                    // first loop / second loop
+  V *FF = B, *Cv = B + EPB * R::FF;      // after the stresses are formed
+  GeomClass *geo = reinterpret_cast<GeomClass *>(smem_bytes + R::DATA);
   FaceLink *lnk = reinterpret_cast<FaceLink *>(geo + EPB);
   int *eid = reinterpret_cast<int *>(lnk + EPB * NFACE);
   const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
   load_geo_slots<C>(geo, lnk, eid, a, e0, tid);
   if constexpr (NODAL) {
-    load_nodal<C>(B, a.Xn, e0, a.ne, tid);
+    load_nodal_v<C>(B, a.Xn, e0, a.ne, tid);
   } else {
-    load_modal<C>(Gg, a.X, e0, a.ne, tid);  // modal input parked in the gradient region
+    load_modal_v<C>(Gg, a.X, e0, a.ne, tid);  // modal input parked in the gradient region
     __syncthreads();
     if constexpr (N::NB1 == NF) {
       backward_batch<C, NF>(Gg, B, S1, S2, tid);
@@ -379,7 +496,7 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(Sta
     for (int w = tid; w < EPB * DIM * LD; w += C::NT) {
       const int s = w / (DIM * LD), rem = w - s * DIM * LD;
       const int e = e0 + s;
-      Gh[w] = e < a.ne ? a.Ghat[((size_t)e * NVC + c) * DIM * LD + rem] : 0.0;
+      Gh[w] = e < a.ne ? V(a.Ghat[((size_t)e * NVC + c) * DIM * LD + rem]) : V(0.0);
     }
     __syncthreads();
     backward_batch<C, DIM>(Gh, Dv, S1, S2, tid);
@@ -392,46 +509,48 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(Sta
     }
   }
   // stresses and heat flux, in place (slots gslot(n, d))
-  const double mu = a.vis, gPr = a.gamma / a.Pr;
+  const V mu = V(a.vis), gPr = V(a.gamma / a.Pr);
   for (int w = tid; w < EPB * QD; w += C::NT) {
     const int s = w / QD, p = w - s * QD;
-    double *g = Gg + s * NGS * QD + p;
-    const double *ge = Dv + s * DIM * QD + p;
-    double U[5];
+    V *g = Gg + s * NGS * QD + p;
+    const V *ge = Dv + s * DIM * QD + p;
+    V U[5];
 #pragma unroll
     for (int n = 0; n < NF; ++n) U[n] = B[(s * NF + n) * QD + p];
-    const double r = U[0];
+    const V r = U[0];
     if constexpr (DIM == 3) {
-      const double u = U[1] / r, v = U[2] / r, ww = U[3] / r;
-      const double ux = g[0 * QD], uy = g[1 * QD], uz = g[2 * QD];
-      const double vx = g[3 * QD], vy = g[4 * QD], vz = g[5 * QD];
-      const double wx = g[6 * QD], wy = g[7 * QD], wz = g[8 * QD];
-      const double ex = ge[0], ey = ge[QD], ez = ge[2 * QD];
-      double t12 = uy + vx; t12 = mu * t12;
-      double t13 = uz + wx; t13 = mu * t13;
-      double t23 = vz + wy; t23 = mu * t23;
-      double wk = 2.0 * ux - vy;
-      double t11 = 1.0 * wk - wz; t11 = (2.0 / 3.0) * t11; t11 = mu * t11;
-      wk = 2.0 * vy - ux;
-      double t22 = 1.0 * wk - wz; t22 = (2.0 / 3.0) * t22; t22 = mu * t22;
-      wk = 2.0 * wz - ux;
-      double t33 = 1.0 * wk - vy; t33 = (2.0 / 3.0) * t33; t33 = mu * t33;
-      double qx = t11 * u; qx = fma(t12, v, qx); qx = fma(t13, ww, qx);
-      double qy = t12 * u; qy = fma(t22, v, qy); qy = fma(t23, ww, qy);
-      double qz = t13 * u; qz = fma(t23, v, qz); qz = fma(t33, ww, qz);
+      const V u = U[1] / r, v = U[2] / r, ww = U[3] / r;
+      const V ux = g[0 * QD], uy = g[1 * QD], uz = g[2 * QD];
+      const V vx = g[3 * QD], vy = g[4 * QD], vz = g[5 * QD];
+      const V wx = g[6 * QD], wy = g[7 * QD], wz = g[8 * QD];
+      const V ex = ge[0], ey = ge[QD], ez = ge[2 * QD];
+      const V two = V(2.0), one = V(1.0), tt = V(2.0 / 3.0);
+      V t12 = uy + vx; t12 = mu * t12;
+      V t13 = uz + wx; t13 = mu * t13;
+      V t23 = vz + wy; t23 = mu * t23;
+      V wk = two * ux - vy;
+      V t11 = one * wk - wz; t11 = tt * t11; t11 = mu * t11;
+      wk = two * vy - ux;
+      V t22 = one * wk - wz; t22 = tt * t22; t22 = mu * t22;
+      wk = two * wz - ux;
+      V t33 = one * wk - vy; t33 = tt * t33; t33 = mu * t33;
+      V qx = t11 * u; qx = fma(t12, v, qx); qx = fma(t13, ww, qx);
+      V qy = t12 * u; qy = fma(t22, v, qy); qy = fma(t23, ww, qy);
+      V qz = t13 * u; qz = fma(t23, v, qz); qz = fma(t33, ww, qz);
       qx = fma(gPr, mu * ex, qx); qy = fma(gPr, mu * ey, qy); qz = fma(gPr, mu * ez, qz);
       g[0 * QD] = t11; g[1 * QD] = t12; g[2 * QD] = t13;
       g[3 * QD] = t22; g[4 * QD] = t23; g[5 * QD] = t33;
       g[6 * QD] = qx; g[7 * QD] = qy; g[8 * QD] = qz;
     } else {
-      const double u = U[1] / r, v = U[2] / r;
-      const double ux = g[0 * QD], uy = g[1 * QD], vx = g[2 * QD], vy = g[3 * QD];
-      const double ex = ge[0], ey = ge[QD];
-      double t12 = uy + vx; t12 = mu * t12;
-      double t11 = 2.0 * ux - vy; t11 = (2.0 / 3.0) * t11; t11 = mu * t11;
-      double t22 = 2.0 * vy - ux; t22 = (2.0 / 3.0) * t22; t22 = mu * t22;
-      double qx = t11 * u; qx = fma(t12, v, qx);
-      double qy = t12 * u; qy = fma(t22, v, qy);
+      const V u = U[1] / r, v = U[2] / r;
+      const V ux = g[0 * QD], uy = g[1 * QD], vx = g[2 * QD], vy = g[3 * QD];
+      const V ex = ge[0], ey = ge[QD];
+      const V two = V(2.0), tt = V(2.0 / 3.0);
+      V t12 = uy + vx; t12 = mu * t12;
+      V t11 = two * ux - vy; t11 = tt * t11; t11 = mu * t11;
+      V t22 = two * vy - ux; t22 = tt * t22; t22 = mu * t22;
+      V qx = t11 * u; qx = fma(t12, v, qx);
+      V qy = t12 * u; qy = fma(t22, v, qy);
       qx = fma(gPr, mu * ex, qx); qy = fma(gPr, mu * ey, qy);
       g[0 * QD] = t11; g[1 * QD] = t12; g[2 * QD] = t22;
       g[3 * QD] = qx; g[4 * QD] = qy;
@@ -443,7 +562,7 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(Sta
     for (int w = tid; w < NFACE * EPB * DIM * QF; w += C::NT) {
       const int f = w / (EPB * DIM * QF), rem = w - f * EPB * DIM * QF;
       const int s = rem / (DIM * QF), rem2 = rem - s * DIM * QF, d = rem2 / QF, x = rem2 - d * QF;
-      const double *src = Gg + (s * NGS + N::gslot(n, d)) * QD;
+      const V *src = Gg + (s * NGS + N::gslot(n, d)) * QD;
       int p;
       if constexpr (DIM == 3) {
         const int u = x / Q, v = x % Q;
@@ -468,11 +587,11 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(Sta
     __syncthreads();
     constexpr int NB = NFACE * EPB * DIM;
     if constexpr (DIM == 3) {
-      contract<Q, Q, 1, 0, Q, G, MatGL2G<L, Q>, false>(FF, S1, NB, Q * Q, G * Q, tid, C::NT);
+      contract<Q, Q, 1, 0, Q, G, MatGL2G<L, Q, V>, false>(FF, S1, NB, Q * Q, G * Q, tid, C::NT);
       __syncthreads();
-      contract<G, Q, 1, 1, Q, G, MatGL2G<L, Q>, false>(S1, Fg, NB, G * Q, G * G, tid, C::NT);
+      contract<G, Q, 1, 1, Q, G, MatGL2G<L, Q, V>, false>(S1, Fg, NB, G * Q, G * G, tid, C::NT);
     } else {
-      contract<Q, 1, 1, 0, Q, G, MatGL2G<L, Q>, false>(FF, Fg, NB, Q, G, tid, C::NT);
+      contract<Q, 1, 1, 0, Q, G, MatGL2G<L, Q, V>, false>(FF, Fg, NB, Q, G, tid, C::NT);
     }
     __syncthreads();
     // g_n . n (own normals), the viscous trace of this side
@@ -481,27 +600,27 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(Sta
       const int e = e0 + s;
       if (e >= a.ne) continue;
       const double *nr = geo[s].onrm[f];
-      double v = nr[0] * Fg[((f * EPB + s) * DIM + 0) * GF + gq];
-      v = fma(nr[1], Fg[((f * EPB + s) * DIM + 1) * GF + gq], v);
-      if (DIM == 3) v = fma(nr[2], Fg[((f * EPB + s) * DIM + 2) * GF + gq], v);
-      a.V[(((size_t)e * NFACE + f) * NV + n) * GF + gq] = v;
+      V v = V(nr[0]) * Fg[((f * EPB + s) * DIM + 0) * GF + gq];
+      v = fma(V(nr[1]), Fg[((f * EPB + s) * DIM + 1) * GF + gq], v);
+      if (DIM == 3) v = fma(V(nr[2]), Fg[((f * EPB + s) * DIM + 2) * GF + gq], v);
+      a.V[(((size_t)e * NFACE + f) * NV + n) * GF + gq] = double(v);
     }
     // collocation divergence of g_n (contravariant form) into Dv [slot][QD]
     for (int r = 0; r < DIM; ++r) {
       for (int w = tid; w < EPB * QD; w += C::NT) {
         const int s = w / QD, p = w - s * QD;
         const double *m = geo[s].metric;
-        const double *gs = Gg + s * NGS * QD + p;
-        double v = m[3 * r + 0] * gs[N::gslot(n, 0) * QD];
-        v = fma(m[3 * r + 1], gs[N::gslot(n, 1) * QD], v);
-        if (DIM == 3) v = fma(m[3 * r + 2], gs[N::gslot(n, 2) * QD], v);
+        const V *gs = Gg + s * NGS * QD + p;
+        V v = V(m[3 * r + 0]) * gs[N::gslot(n, 0) * QD];
+        v = fma(V(m[3 * r + 1]), gs[N::gslot(n, 1) * QD], v);
+        if (DIM == 3) v = fma(V(m[3 * r + 2]), gs[N::gslot(n, 2) * QD], v);
         Cv[w] = v;
       }
       __syncthreads();
       using Sh = Sh3<DIM, Q>;
-      if (r == 0) contract<Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<L, Q>, false>(Cv, Dv, EPB, QD, QD, tid, C::NT);
-      else if (r == 1) contract<Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<L, Q>, true>(Cv, Dv, EPB, QD, QD, tid, C::NT);
-      else contract<Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<L, Q>, true>(Cv, Dv, EPB, QD, QD, tid, C::NT);
+      if (r == 0) contract<Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<L, Q, V>, false>(Cv, Dv, EPB, QD, QD, tid, C::NT);
+      else if (r == 1) contract<Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<L, Q, V>, true>(Cv, Dv, EPB, QD, QD, tid, C::NT);
+      else contract<Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<L, Q, V>, true>(Cv, Dv, EPB, QD, QD, tid, C::NT);
       __syncthreads();
     }
     // projected divergence of this field
@@ -509,7 +628,7 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C>::VISC_MINB) ns_visc_kernel(Sta
     for (int w = tid; w < EPB * LD; w += C::NT) {
       const int s = w / LD, m = w - s * LD;
       const int e = e0 + s;
-      if (e < a.ne) a.Pv[((size_t)e * NV + n) * LD + m] = S2[w];
+      if (e < a.ne) a.Pv[((size_t)e * NV + n) * LD + m] = double(S2[w]);
     }
     __syncthreads();
   }

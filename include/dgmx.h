@@ -41,7 +41,11 @@ enum { DGMX_EULER2D = 1, DGMX_NS2D = 2, DGMX_EULER3D = 8, DGMX_NS3D = 9, DGMX_SH
 enum { DGMX_FLUX_LF = 0, DGMX_FLUX_ROE = 1 };
 /* Integrators are DGM's inttype values (src/TimeInt.hpp:62-85). */
 enum { DGMX_TVD3 = 3, DGMX_RK4 = 4, DGMX_LSRK14 = 14 };
-/* Arithmetic of the stage kernels. */
+/* Arithmetic of the stage kernels.  DGMX_MIXED: for Euler and shallow water
+ * (LSRK14) FP32 states, fluxes, contractions and traces about an FP64 reference
+ * state with the FP64 solution register; for Navier-Stokes the two BR1 viscous
+ * kernels in FP32 (density and energy means taken out in FP64 first) while the
+ * stage kernel, registers and traces stay FP64, with any integrator. */
 enum { DGMX_FP64 = 0, DGMX_MIXED = 1 };
 /* Boundary kinds (FP64).  DGMX_BC_SLIP_WALL: Euler and shallow-water solid
  * wall, Euler::WallBC / Euler3d::WallBC / Shallow::WallBC (src/EulerBC.hpp:43-62,

@@ -49,6 +49,7 @@ def lib():
         L.ora_nfields.argtypes = [P]
         L.ora_error.argtypes = [P]
         L.ora_set_threads.argtypes = [ctypes.c_int]
+        L.ora_lsrk14_coefficients.argtypes = [D, D]
         L.ora_set_sw_balance.argtypes = [P, ctypes.c_int]
         L.ora_set_bc.argtypes = [P, ctypes.c_int, I, D]
         L.ora_set_hold_bulk.argtypes = [P, ctypes.c_int]
@@ -193,3 +194,12 @@ class Problem:
 
 def set_threads(n: int):
     lib().ora_set_threads(int(n))
+
+
+def lsrk14_coefficients():
+    """LSRK14's 2N-storage coefficients (A, B) as the oracle steps with them
+    (src/TimeInt.cpp:1870-1917)."""
+    A, B = np.zeros(14), np.zeros(14)
+    lib().ora_lsrk14_coefficients(A.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                  B.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return A, B

@@ -1875,6 +1875,11 @@ void ora_set_hold_bulk(void *h, int on) { ((Problem *)h)->hold_bulk = on != 0; }
 long ora_ntot(void *h) { return (long)((Problem *)h)->ntot; }
 int ora_nfields(void *h) { return ((Problem *)h)->nf; }
 int ora_error(void *h) { return ((Problem *)h)->err; }
+// The LSRK14 2N-storage coefficients (A: register decay, B: update weight).
+void ora_lsrk14_coefficients(double *A, double *B) {
+  for (int k = 0; k < 14; ++k) { A[k] = kLsrkA[k]; B[k] = kLsrkB[k]; }
+}
+
 void ora_set_threads(int n) {
 #ifdef _OPENMP
   omp_set_num_threads(n);

@@ -125,6 +125,68 @@ def test_navier_stokes_br1_matches_oracle(case):
     assert rel(E.rhs(U0), F_o) > 1e-8
 
 
+NS32_CASES = [
+    # name, NS physics, its Euler counterpart, dim, n, lo, hi, p, q, inttype, dt, vis
+    ("ns3d-p7-q9-tgv", 9, 8, 3, (4, 4, 4), 0, 2 * np.pi, 7, 9, 14, 0.002, 1.0 / 1600),
+    ("ns3d-p3-tgv", 9, 8, 3, (8, 8, 8), 0, 2 * np.pi, 3, 0, 3, 0.004, 0.01),
+    ("ns2d-p4-vortex", 2, 1, 2, (6, 6), -5, 5, 4, 0, 4, 0.01, 0.02),
+]
+# FP32 viscous form: bound on its distance from the FP64 path relative to the
+# viscous part itself (the FP64 Navier-Stokes result minus the Euler result)
+TOL_VISC32 = 2e-4
+
+
+def stage_weight_rss(inttype):
+    """Root-sum-square of a scheme's effective stage weights: the factor by
+    which independent per-stage rounding errors of the right-hand side reach
+    the step.  LSRK14's 2N-storage coefficients give weights as large as
+    37 and -39 (summing to 1), so about 55; TVD3 and RK4 stay below 1."""
+    if inttype != 14:
+        return 1.0
+    A, B = oracle.lsrk14_coefficients()
+    w = [sum(B[k] * np.prod(A[j + 1:k + 1]) for k in range(j, 14)) for j in range(14)]
+    return float(np.sqrt(np.sum(np.square(w))))
+
+
+@pytest.mark.parametrize("case", NS32_CASES, ids=[c[0] for c in NS32_CASES])
+def test_navier_stokes_fp32_viscous_form(case):
+    """precision = MIXED for Navier-Stokes runs the BR1 gradient and viscous
+    kernels in FP32 (stage kernel, registers and traces FP64).  Measured
+    against the viscous contribution alone (momentum vector, energy): the
+    right-hand side (nodal path) of the FP32 form stays within TOL_VISC32 of
+    the FP64 path, and one step (modal path) within TOL_VISC32 times the
+    scheme's stage-weight factor; the FP64 path's own parity with the oracle
+    is checked on the same step.  Low-Mach Taylor-Green (E/rho ~ 180 against
+    |u|^2/2 ~ 0.5) is the case that needs the mean-shifted internal energy."""
+    import dgm_b200
+    _, phys, ephys, dim, n, lo, hi, p, q, inttype, dt, vis = case
+    m = dgm_b200.meshgen.box(dim, n, lo, hi, p, q)
+    D32 = dgm_b200.Domain(m, phys, flux="roe", inttype=inttype, vis=vis, precision=dgm_b200.MIXED)
+    D64 = dgm_b200.Domain(m, phys, flux="roe", inttype=inttype, vis=vis)
+    D0 = dgm_b200.Domain(m, ephys, flux="roe", inttype=inttype)
+    P = oracle.Problem(dgm_io.Mesh(m.dim, m.verts, m.con, m.porder, m.qorder), phys, flux="roe", vis=vis)
+    x, y, z = P.coords()
+    f = TG(x, y, z) if dim == 3 else ics.vortex_ic(x, y, [(0.0, 0.0, 1.0, 1.0, 0.5)], nf=4)
+    U0 = P.project(f)
+    F32, F64, F0 = D32.time_derivative(U0), D64.time_derivative(U0), D0.time_derivative(U0)
+    for D in (D32, D64, D0):
+        D.set_state(f)
+        D.advance(dt, 1)
+    S32, S64, S0 = D32.state(), D64.state(), D0.state()
+    P.set_state(U0)
+    assert P.advance(inttype, dt, 1) == 0
+    assert rel(S64, P.state()) < TOL_STATE
+    # density has no viscous part; the momentum components are measured as
+    # one vector (Taylor-Green's w component has none by symmetry)
+    for k in (slice(1, dim + 1), slice(dim + 1, dim + 2)):
+        rhs = np.linalg.norm(F32[k] - F64[k]) / np.linalg.norm(F64[k] - F0[k])
+        step = np.linalg.norm(S32[k] - S64[k]) / np.linalg.norm(S64[k] - S0[k])
+        assert rhs < TOL_VISC32 and step < TOL_VISC32 * stage_weight_rss(inttype), (k, rhs, step)
+    assert not np.array_equal(S32, S64)
+    for D in (D32, D64, D0):
+        D.close()
+
+
 MIXED_CASES = [
     ("euler3d-tgv", 8, 3, (4, 4, 4), 0, 2 * np.pi, 3, "laxfriedrichs", TG, 0.002, 20),
     ("euler3d-roe-p5", 8, 3, (2, 2, 2), 0, 2 * np.pi, 5, "roe", TG, 0.001, 10),
