@@ -340,6 +340,23 @@ class Domain:
         self._check(f(self.h, int(reps), _dp(rows), 64, ctypes.byref(nv), ctypes.byref(ch)))
         return rows[: nv.value].copy(), ch.value
 
+    def set_source(self, S):
+        """Time-independent source of the 2-D physics: F -= S at the GLL
+        points before the projection (FileSource / ConstSource).  S: GLL
+        values (Field layout, as set_state), nf constants (ConstSource), or
+        None to remove it.  3-D domains raise: the reference applies no
+        source there."""
+        f = lib().dgmx_set_source
+        f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        if S is None:
+            self._check(f(self.h, None))
+            return
+        S = np.asarray(S, dtype=np.float64)
+        if S.ndim == 1 and S.size == self.nf:
+            S = np.repeat(S[:, None], self.nq, axis=1)
+        S = np.ascontiguousarray(S).reshape(self.nf, self.nq)
+        self._check(f(self.h, S.ctypes.data_as(ctypes.c_void_p)))
+
     def set_bulk_hold(self, on: bool):
         """Channel::holdBulkMassFlow after every projected RHS (Navier-Stokes 3-D)."""
         f = lib().dgmx_set_bulk_hold

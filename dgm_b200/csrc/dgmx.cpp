@@ -96,6 +96,7 @@ struct dgmx_domain {
   double *U = nullptr, *Ut = nullptr, *Acc = nullptr;   // modal registers [e][n][ld]
   double *T[2] = {nullptr, nullptr};                     // traces [e][f][n][gf]
   double *Rsw = nullptr;                                 // shallow-water first RHS (modal)
+  double *Ssrc = nullptr;                                // projected source field (modal), 2-D physics
   double *Ghat = nullptr, *Vtr = nullptr, *Pv = nullptr; // Navier-Stokes BR1 work
   float *Utf = nullptr, *Tf[2] = {nullptr, nullptr};     // mixed form: FP32 register and traces
   double *uref = nullptr;                                // mixed form: reference state row (kUrefStride)
@@ -168,6 +169,7 @@ struct dgmx_domain {
     a.err = err;
     a.Ghat = Ghat; a.V = Vtr; a.Pv = Pv;
     a.uref = uref;
+    a.Ssrc = Ssrc;
     for (int t = 0; t <= kMaxBcTypes; ++t) {
       a.bckind[t] = bckind[t];
       for (int k = 0; k < 5; ++k) a.bcpar[t][k] = bcpar[t][k];
@@ -198,7 +200,7 @@ struct dgmx_domain {
     if (graph) cudaGraphExecDestroy(graph);
     graph = nullptr;
     void *ptrs[] = {U, Ut, Acc, T[0], T[1], Rsw, nod_in, nod_out, Jdev, integ, gclass, perm, err, classes, links,
-                    Ghat, Vtr, Pv, Utf, Tf[0], Tf[1], uref, R0, cbar, x_send, x_recv, x_sbuf, x_rbuf, tiles};
+                    Ghat, Vtr, Pv, Utf, Tf[0], Tf[1], uref, R0, cbar, x_send, x_recv, x_sbuf, x_rbuf, tiles, Ssrc};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (host_pinned) cudaFreeHost(host_pinned);
     if (xh_send) cudaFreeHost(xh_send);
@@ -211,7 +213,7 @@ struct dgmx_domain {
     Ghat = Vtr = Pv = nullptr;
     Utf = Tf[0] = Tf[1] = nullptr;
     uref = nullptr;
-    R0 = cbar = nullptr;
+    R0 = cbar = Ssrc = nullptr;
     x_send = x_recv = nullptr; x_sbuf = x_rbuf = nullptr; tiles = nullptr; tiles_epb = 0;
     if (ev_b) cudaEventDestroy(ev_b);
     if (ev_x) cudaEventDestroy(ev_x);
@@ -830,6 +832,40 @@ dgmx_status dgmx_partition_info(const dgmx_domain *d, int *ne_local, int *nghost
     else for (int e = 0; e < d->ne; ++e) global_of_local[e] = e;
   }
   return DGMX_OK;
+}
+
+dgmx_status dgmx_set_source(dgmx_domain *d, const double *S) {
+  if (!d) return DGMX_ERR_ARGUMENT;
+  if (d->dim == 3)
+    return d->fail(DGMX_ERR_UNSUPPORTED, "source terms are a 2-D feature: Euler3d and Navier_Stokes3d::time_derivative "
+                                         "apply none");
+  cudaSetDevice(d->prm.device);
+  if (!S) {   // clear
+    if (d->Ssrc) {
+      cudaError_t e = cudaStreamSynchronize(d->stream);
+      cudaFree(d->Ssrc);
+      d->Ssrc = nullptr;
+      if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+      if (e != cudaSuccess) return d->cuda(e, "source clear");
+    }
+    return DGMX_OK;
+  }
+  if (!d->Ssrc) {
+    cudaError_t e = dalloc(&d->Ssrc, d->nmodal());
+    if (e != cudaSuccess) { d->Ssrc = nullptr; return d->cuda(e, "alloc source"); }
+    if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  }
+  // upload the GLL values and project them once (Field layout in, register layout out)
+  const size_t n = d->nnodal();
+  const double *src = S;
+  if (!is_pinned(S)) { std::memcpy(d->host_pinned, S, sizeof(double) * n); src = d->host_pinned; }
+  cudaError_t e = cudaMemcpyAsync(d->nod_in, src, sizeof(double) * n, cudaMemcpyHostToDevice, d->stream);
+  if (e != cudaSuccess) return d->cuda(e, "source upload");
+  StageArgs a = d->base_args();
+  e = d->ops->forward(a, d->nod_in, d->Ssrc, d->stream);
+  ++d->launches;
+  if (e != cudaSuccess) return d->cuda(e, "forward kernel");
+  return d->cuda(cudaStreamSynchronize(d->stream), "set_source");
 }
 
 dgmx_status dgmx_set_bulk_hold(dgmx_domain *d, int on) {

@@ -212,6 +212,12 @@ struct StageArgs {
   // shallow-water balance (REO_SHALLOW_ENFORCE_BALANCE, src/Shallow.cpp:251-267)
   double *Rcap;           // if set, the projected RHS is stored here (modal)
   const double *Rsub;     // if set, subtracted from the projected RHS
+  // if set, a source field of the 2-D physics projected once (modal,
+  // register layout), subtracted from the projected RHS before the two
+  // above: Source::apply's F -= S at the GLL points ahead of the projection
+  // (src/Euler.cpp:282-287, src/Navier_Stokes.cpp:95-100,
+  // src/Shallow.cpp:255-260), moved past it since projection is linear
+  const double *Ssrc;
   // mixed-precision form: FP32 second register and traces; the working
   // copies are perturbations about a reference state per solve:
   // uref[10 s + n] conserved values, uref[10 s + 5 + n] its constant-mode

@@ -676,6 +676,9 @@ __device__ __forceinline__ void stage_tile(const Smem<C> &sm, const StageArgs &a
       float rr[L];
 #pragma unroll
       for (int k = 0; k < L; ++k) rr[k] = Rr[k];
+      if (a.Ssrc)
+#pragma unroll
+        for (int k = 0; k < L; ++k) rr[k] -= float(a.Ssrc[gi + k]);
       if (a.Rsub)
 #pragma unroll
         for (int k = 0; k < L; ++k) rr[k] -= float(a.Rsub[gi + k]);
@@ -703,6 +706,9 @@ __device__ __forceinline__ void stage_tile(const Smem<C> &sm, const StageArgs &a
       double rr[L];
 #pragma unroll
       for (int k = 0; k < L; ++k) rr[k] = Rr[k];
+      if (a.Ssrc)
+#pragma unroll
+        for (int k = 0; k < L; ++k) rr[k] -= a.Ssrc[gi + k];
       if (a.Rcap)   // first RHS (shallow-water balance)
 #pragma unroll
         for (int k = 0; k < L; ++k) a.Rcap[gi + k] = rr[k];
@@ -899,12 +905,13 @@ __global__ void __launch_bounds__(C::NT, C::MINB) rhs_nodal_kernel(StageArgs a) 
     }
     csync<C>();
   }
-  if (a.Rcap || a.Rsub) {
+  if (a.Ssrc || a.Rcap || a.Rsub) {
     constexpr int BLK = NF * C::LD;
     for (int w = tid; w < EPB * BLK; w += C::NT) {
       const int e = e0 + w / BLK;
       if (e >= a.ne) continue;
       const size_t gi = (size_t)e0 * BLK + w;
+      if (a.Ssrc) sm.R[w] = sm.R[w] - a.Ssrc[gi];
       if (a.Rcap) a.Rcap[gi] = sm.R[w];
       if (a.Rsub) sm.R[w] = sm.R[w] - a.Rsub[gi];
     }

@@ -163,6 +163,19 @@ const char *dgmx_group_last_error(const dgmx_group *g);
  * and energy are subtracted.  on = 0 switches it off. */
 dgmx_status dgmx_set_bulk_hold(dgmx_domain *d, int on);
 
+/* Source term of the 2-D physics, the Source database's apply (F -= S at
+ * the GLL points before the projection) for a field that does not change
+ * in time: FileSource (src/Source.hpp:150-180) with S the file's field,
+ * ConstSource (src/Source.hpp:110-148) with S constant per field.  Called
+ * from Euler::time_derivative (src/Euler.cpp:282-287),
+ * Navier_Stokes::time_derivative (src/Navier_Stokes.cpp:95-100) and
+ * Shallow::time_derivative (src/Shallow.cpp:255-260), where the
+ * shallow-water balance's first right-hand side includes it.  S: GLL values
+ * in the dgmx_set_state layout, projected once; NULL removes the source.
+ * 3-D domains refuse (DGMX_ERR_UNSUPPORTED): Euler3d and Navier_Stokes3d
+ * apply no source. */
+dgmx_status dgmx_set_source(dgmx_domain *d, const double *S);
+
 dgmx_status dgmx_destroy(dgmx_domain *d);
 
 /* nf fields, nq = total GLL points per field, nm = total modes per field. */

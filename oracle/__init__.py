@@ -50,6 +50,7 @@ def lib():
         L.ora_error.argtypes = [P]
         L.ora_set_threads.argtypes = [ctypes.c_int]
         L.ora_lsrk14_coefficients.argtypes = [D, D]
+        L.ora_set_source.argtypes = [P, ctypes.c_void_p]
         L.ora_set_sw_balance.argtypes = [P, ctypes.c_int]
         L.ora_set_bc.argtypes = [P, ctypes.c_int, I, D]
         L.ora_set_hold_bulk.argtypes = [P, ctypes.c_int]
@@ -181,6 +182,16 @@ class Problem:
 
     def set_sw_balance(self, on: bool):
         lib().ora_set_sw_balance(self.h, 1 if on else 0)
+
+    def set_source(self, S):
+        """Source field at the GLL points [nf][ntot] (2-D physics: F -= S
+        before the projection); None removes it."""
+        if S is None:
+            lib().ora_set_source(self.h, None)
+            return
+        S = np.ascontiguousarray(S, dtype=np.float64).reshape(self.nf, self.ntot)
+        self._S = S
+        lib().ora_set_source(self.h, S.ctypes.data_as(ctypes.c_void_p))
 
     def error(self) -> int:
         return lib().ora_error(self.h)

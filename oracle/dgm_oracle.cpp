@@ -671,6 +671,7 @@ struct Problem {
   int err = 0;                     // non-physical state seen (density/pressure)
   // work fields: interior [nf][ntot] and sides [nf][nstot]
   vec Us_s, Uf_s, Uv_u, Uv_s, Usrc;
+  vec S;                           // source field at the GLL points [nf][ntot] (empty: none)
   vec U, Ut, R0, R1;               // integrator registers
   // boundary sides (src/Boundary.cpp:25-75, src/Field.cpp:4426-4460): the
   // record names the element side, the BC kind and its two parameters; the
@@ -1737,6 +1738,10 @@ static void time_derivative(Problem &P, const double *Ub, double *Fb) {
   lift_all(P, Fb, 0);
   if (P.physics == NS2D) ns2d_diffusion(P, Ub, Fb);
   if (P.physics == NS3D) ns3d_diffusion(P, Ub, Fb);
+  // add_source (src/Euler.cpp:1297-1302, src/Navier_Stokes.cpp:375-381,
+  // src/Shallow.cpp:851-856): ConstSource / FileSource apply, F -= S
+  if (!P.S.empty() && P.dim == 2)
+    for (size_t i = 0; i < P.S.size(); ++i) Fb[i] = Fb[i] - P.S[i];
   project_all(P, Fb);
   if (P.physics == NS3D && P.hold_bulk) hold_bulk_mass_flow(P, Fb);
   if (P.physics == SHALLOW && P.sw_balance) {
@@ -1875,6 +1880,13 @@ void ora_set_hold_bulk(void *h, int on) { ((Problem *)h)->hold_bulk = on != 0; }
 long ora_ntot(void *h) { return (long)((Problem *)h)->ntot; }
 int ora_nfields(void *h) { return ((Problem *)h)->nf; }
 int ora_error(void *h) { return ((Problem *)h)->err; }
+// Source field S (GLL values [nf][ntot]), or none when S is null.
+void ora_set_source(void *h, const double *S) {
+  auto *P = (Problem *)h;
+  if (!S) { P->S.clear(); return; }
+  P->S.assign(S, S + (size_t)P->nf * P->ntot);
+}
+
 // The LSRK14 2N-storage coefficients (A: register decay, B: update weight).
 void ora_lsrk14_coefficients(double *A, double *B) {
   for (int k = 0; k < 14; ++k) { A[k] = kLsrkA[k]; B[k] = kLsrkB[k]; }
