@@ -24,7 +24,7 @@ _lib = None
 EULER2D, NS2D, EULER3D, NS3D, SHALLOW = 1, 2, 8, 9, 30
 TVD3, RK4, LSRK14 = 3, 4, 14
 FP64, MIXED = 0, 1
-FLUX = {"laxfriedrichs": 0, "lf": 0, "roe": 1}
+FLUX = {"laxfriedrichs": 0, "lf": 0, "roe": 1, "stegerwarming": 2, "vanleer": 3}
 STATUS = {0: "ok", 1: "argument", 2: "unsupported", 3: "cuda", 4: "non-physical", 5: "io", 6: "memory"}
 
 

@@ -562,7 +562,19 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
     g_create_error = "inttype must be 3 (TVD), 4 (RK4) or 14 (LSRK14)";
     return DGMX_ERR_UNSUPPORTED;
   }
-  if (p->flux != DGMX_FLUX_LF && p->flux != DGMX_FLUX_ROE) { g_create_error = "flux must be LF or Roe"; return DGMX_ERR_UNSUPPORTED; }
+  if (p->flux < DGMX_FLUX_LF || p->flux > DGMX_FLUX_VAN_LEER) {
+    g_create_error = "flux must be LF, Roe, Steger-Warming or van Leer";
+    return DGMX_ERR_UNSUPPORTED;
+  }
+  if ((p->flux == DGMX_FLUX_STEGER_WARMING || p->flux == DGMX_FLUX_VAN_LEER) &&
+      (phys != DGMX_EULER2D && phys != DGMX_NS2D)) {
+    g_create_error = "Steger-Warming and van Leer are 2-D Euler/Navier-Stokes fluxes (Euler3d computes Lax-Friedrichs only)";
+    return DGMX_ERR_UNSUPPORTED;
+  }
+  if ((p->flux == DGMX_FLUX_STEGER_WARMING || p->flux == DGMX_FLUX_VAN_LEER) && p->precision == DGMX_MIXED) {
+    g_create_error = "the mixed-precision form is built for the Lax-Friedrichs and Roe fluxes";
+    return DGMX_ERR_UNSUPPORTED;
+  }
   if (phys == DGMX_SHALLOW && p->flux != DGMX_FLUX_LF) { g_create_error = "shallow water supports Lax-Friedrichs only"; return DGMX_ERR_UNSUPPORTED; }
   if (p->precision != DGMX_FP64 && p->precision != DGMX_MIXED) { g_create_error = "precision must be FP64 or MIXED"; return DGMX_ERR_ARGUMENT; }
   if (p->precision == DGMX_MIXED && p->inttype != DGMX_LSRK14 && !ns_phys) {
@@ -891,7 +903,10 @@ dgmx_status dgmx_create_from_files(const char *root, const dgmx_params *params, 
     if (fc.gamma > 0) p.gamma = fc.gamma;
     if (fc.vis >= 0) p.vis = fc.vis;
     if (fc.Pr > 0) p.Pr = fc.Pr;
-    if (!fc.flux.empty()) p.flux = fc.flux == "roe" ? DGMX_FLUX_ROE : DGMX_FLUX_LF;
+    if (!fc.flux.empty())
+      p.flux = fc.flux == "roe" ? DGMX_FLUX_ROE
+               : fc.flux == "stegerwarming" ? DGMX_FLUX_STEGER_WARMING
+               : fc.flux == "vanleer" ? DGMX_FLUX_VAN_LEER : DGMX_FLUX_LF;
     dgmx_mesh m;
     m.dim = fc.dim; m.ne = fc.ne; m.verts = fc.verts.data();
     m.ncon = (int)(fc.con.size() / 4); m.con = fc.con.data();

@@ -138,6 +138,39 @@ __device__ __forceinline__ void volume_flux(const T *U, T gamma, T (*F)[5]) {
   }
 }
 
+// Flux-vector splittings of Euler::convective_flux (src/Euler.cpp:577-680)
+// for one face-frame state (rho, u normal, v tangential, H): the positive
+// part (plus) of the master state or the negative part of the slave state.
+// Steger-Warming: eigenvalues u-a, u, u+a clipped at zero.
+template <class T>
+__device__ __forceinline__ void steger_warming_split(T r, T u, T v, T H, T gamma, bool plus, T *F) {
+  const T gm1 = gamma - T(1.0);
+  const T a = sqrt(gm1 * (H - T(0.5) * (u * u + v * v)));
+  const T l0 = plus ? fmax(u - a, T(0.0)) : fmin(u - a, T(0.0));
+  const T l1 = plus ? fmax(u, T(0.0)) : fmin(u, T(0.0));
+  const T l3 = plus ? fmax(u + a, T(0.0)) : fmin(u + a, T(0.0));
+  const T c1 = T(0.5) * r / gamma, c2 = T(2.0) * gm1;
+  F[0] = c1 * (l0 + c2 * l1 + l3);
+  F[1] = c1 * ((u - a) * l0 + c2 * u * l1 + (u + a) * l3);
+  F[2] = c1 * (v * l0 + c2 * v * l1 + v * l3);
+  F[3] = c1 * ((H - u * a) * l0 + gm1 * (u * u + v * v) * l1 + (H + u * a) * l3);
+}
+// van Leer: Mach-number polynomials (the subsonic branch, as the reference
+// evaluates them at every Mach number).
+template <class T>
+__device__ __forceinline__ void van_leer_split(T r, T u, T v, T H, T gamma, bool plus, T *F) {
+  const T gm1 = gamma - T(1.0);
+  const T a = sqrt(gm1 * (H - T(0.5) * (u * u + v * v)));
+  const T M = u / a;
+  T c1, c2;
+  if (plus) { c1 = T(0.25) * r * a * (T(1.0) + M) * (T(1.0) + M); c2 = T(0.5) * gm1 * M + T(1.0); }
+  else { c1 = T(-0.25) * r * a * (T(1.0) - M) * (T(1.0) - M); c2 = T(0.5) * gm1 * M - T(1.0); }
+  F[0] = c1;
+  F[1] = plus ? c1 * T(2.0) * a * (T(1.0) / gamma) * c2 : c1 * T(2.0) * a / gamma * c2;
+  F[2] = c1 * v;
+  F[3] = c1 * (T(2.0) * a * a / (gamma * gamma - T(1.0)) * c2 * c2 + T(0.5) * v * v);
+}
+
 // Numerical flux on one face point in the frame of the master side:
 // UL = master state, UR = slave state, n = master outward normal.
 // Outputs Fh (numerical flux), FL = F(UL).n, FR = F(UR).n.
@@ -190,6 +223,21 @@ __device__ __forceinline__ bool face_flux(const T *UL, const T *UR, const T *n, 
       Fh[1] = FL[1] + G[1] * nx - G[2] * ny;
       Fh[2] = FL[2] + G[1] * ny + G[2] * nx;
       Fh[3] = FL[3] + G[3];
+    } else if (flux == DGMX_FLUX_STEGER_WARMING || flux == DGMX_FLUX_VAN_LEER) {
+      // flux-vector splitting in the face frame, F+(UL) + F-(UR), rotated back
+      T P[4], M[4];
+      if (flux == DGMX_FLUX_STEGER_WARMING) {
+        steger_warming_split<T>(rl, ul, vl, Hl, gamma, true, P);
+        steger_warming_split<T>(rr, ur, vr, Hr, gamma, false, M);
+      } else {
+        van_leer_split<T>(rl, ul, vl, Hl, gamma, true, P);
+        van_leer_split<T>(rr, ur, vr, Hr, gamma, false, M);
+      }
+      const T G0 = P[0] + M[0], G1 = P[1] + M[1], G2 = P[2] + M[2], G3 = P[3] + M[3];
+      Fh[0] = G0;
+      Fh[1] = G1 * nx - G2 * ny;
+      Fh[2] = G1 * ny + G2 * nx;
+      Fh[3] = G3;
     } else {
       const T al = sqrt(gm1 * (Hl - T(0.5) * (ul * ul + vl * vl)));
       const T ar = sqrt(gm1 * (Hr - T(0.5) * (ur * ur + vr * vr)));

@@ -37,8 +37,10 @@ typedef enum {
 
 /* Physics codes are DGM's eqntype values (src/ReoProblem.cpp:75-156). */
 enum { DGMX_EULER2D = 1, DGMX_NS2D = 2, DGMX_EULER3D = 8, DGMX_NS3D = 9, DGMX_SHALLOW = 30 };
-/* Numerical flux (src/Euler.cpp:104-113). */
-enum { DGMX_FLUX_LF = 0, DGMX_FLUX_ROE = 1 };
+/* Numerical flux (src/Euler.cpp:104-113).  Steger-Warming and van Leer:
+ * Euler and Navier-Stokes 2-D in FP64 (Euler3d computes Lax-Friedrichs
+ * only; Roe in 3-D is this library's extension). */
+enum { DGMX_FLUX_LF = 0, DGMX_FLUX_ROE = 1, DGMX_FLUX_STEGER_WARMING = 2, DGMX_FLUX_VAN_LEER = 3 };
 /* Integrators are DGM's inttype values (src/TimeInt.hpp:62-85). */
 enum { DGMX_TVD3 = 3, DGMX_RK4 = 4, DGMX_LSRK14 = 14 };
 /* Arithmetic of the stage kernels.  DGMX_MIXED: for Euler and shallow water
