@@ -286,6 +286,23 @@ class Domain:
         self._check(lib().dgmx_get_state(self.h, _dp(U)))
         return U
 
+    def set_state_async(self, U):
+        """set_state without the host wait; U: a page-locked (pinned)
+        float64 array in the Field layout, left untouched until sync()."""
+        f = lib().dgmx_set_state_async
+        f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        assert U.dtype == np.float64 and U.flags.c_contiguous and U.size == self.nf * self.nq
+        self._check(f(self.h, U.ctypes.data_as(ctypes.c_void_p)))
+
+    def state_async(self, U):
+        """get_state into a page-locked array without the host wait; U holds
+        the state once sync() returns."""
+        f = lib().dgmx_get_state_async
+        f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        assert U.dtype == np.float64 and U.flags.c_contiguous and U.size == self.nf * self.nq
+        self._check(f(self.h, U.ctypes.data_as(ctypes.c_void_p)))
+        return U
+
     def modes(self):
         """Restart-layout modal coefficients [field][element][L^d]."""
         Uh = np.zeros((self.nf, self.nm))

@@ -736,9 +736,63 @@ dgmx_status set_state_from_device_nodal(dgmx_domain *d, const double *Un_dev) {
   return d->cuda(cudaStreamSynchronize(d->stream), "set_state");
 }
 
+// set_state_from_device_nodal without a host wait: the projection, the
+// registers' reset, the mixed form's reference state (integrals and the
+// reference row on the stream) and the traces, all enqueued on d->stream.
+dgmx_status enqueue_state_from_device_nodal(dgmx_domain *d, const double *Un_dev) {
+  StageArgs a = d->base_args();
+  cudaError_t e = d->ops->forward(a, Un_dev, d->U, d->stream);
+  ++d->launches;
+  if (e != cudaSuccess) return d->cuda(e, "forward kernel");
+  if ((e = cudaMemsetAsync(d->Ut, 0, sizeof(double) * d->nmodal(), d->stream))) return d->cuda(e, "memset");
+  if ((e = cudaMemsetAsync(d->Acc, 0, sizeof(double) * d->nmodal(), d->stream))) return d->cuda(e, "memset");
+  if (d->Utf && (e = cudaMemsetAsync(d->Utf, 0, sizeof(float) * d->nmodal(), d->stream))) return d->cuda(e, "memset");
+  d->tcur = 0;
+  d->sw_captured = false;
+  if (d->mixed()) {
+    double vol = 0.0;
+    for (int k = 0; k < d->ne; ++k) vol += d->mesh.J[k];
+    vol *= std::pow(2.0, d->dim);
+    e = launch_integrals(d->nf, d->ne, d->ld, std::pow(std::sqrt(2.0), d->dim), d->U, d->Jdev, d->integ, d->stream);
+    if (e == cudaSuccess)
+      e = launch_reference_row(d->prm.physics, d->nf, d->prm.gamma, std::pow(d->tab.B[0], d->dim), vol, d->integ,
+                               d->uref, d->stream);
+    d->launches += 2;
+    if (e != cudaSuccess) return d->cuda(e, "reference state");
+  }
+  a = d->base_args();
+  e = d->mixed() ? d->ops_m->traces_modal(a, d->U, d->Tf[d->tcur], d->stream)
+                 : d->ops->traces_modal(a, d->U, d->T[d->tcur], d->stream);
+  ++d->launches;
+  return d->cuda(e, "trace kernel launch");
+}
+
 }  // namespace
 
 extern "C" {
+
+dgmx_status dgmx_set_state_async(dgmx_domain *d, const double *U) {
+  if (!d || !U) return DGMX_ERR_ARGUMENT;
+  if (d->partitioned()) return d->fail(DGMX_ERR_UNSUPPORTED, "the asynchronous state calls are not built for partitions");
+  if (!is_pinned(U)) return d->fail(DGMX_ERR_ARGUMENT, "dgmx_set_state_async needs page-locked host memory");
+  cudaSetDevice(d->prm.device);
+  cudaError_t e = cudaMemcpyAsync(d->nod_in, U, sizeof(double) * d->nnodal(), cudaMemcpyHostToDevice, d->stream);
+  if (e != cudaSuccess) return d->cuda(e, "state upload");
+  return enqueue_state_from_device_nodal(d, d->nod_in);
+}
+
+dgmx_status dgmx_get_state_async(dgmx_domain *d, double *U) {
+  if (!d || !U) return DGMX_ERR_ARGUMENT;
+  if (d->partitioned()) return d->fail(DGMX_ERR_UNSUPPORTED, "the asynchronous state calls are not built for partitions");
+  if (!is_pinned(U)) return d->fail(DGMX_ERR_ARGUMENT, "dgmx_get_state_async needs page-locked host memory");
+  cudaSetDevice(d->prm.device);
+  StageArgs a = d->base_args();
+  cudaError_t e = d->ops->backward(a, d->U, d->nod_out, d->stream);
+  ++d->launches;
+  if (e != cudaSuccess) return d->cuda(e, "backward kernel");
+  e = cudaMemcpyAsync(U, d->nod_out, sizeof(double) * d->nnodal(), cudaMemcpyDeviceToHost, d->stream);
+  return d->cuda(e, "state download");
+}
 
 dgmx_status dgmx_create(const dgmx_mesh *mesh, const dgmx_params *params, dgmx_domain **out) {
   try {

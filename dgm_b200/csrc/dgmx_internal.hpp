@@ -157,7 +157,7 @@ constexpr int kUrefStride = 24;
 
 // Fills row[5..] from row[0..nf): phi0 is the constant basis function's
 // value (the constant mode of a constant c is c / phi0).
-inline void fill_reference_row(int physics, double gamma, double phi0, double *row) {
+__host__ __device__ inline void fill_reference_row(int physics, double gamma, double phi0, double *row) {
   const bool sw = physics == DGMX_SHALLOW;
   const int dim = (physics == DGMX_EULER3D || physics == DGMX_NS3D) ? 3 : 2, nf = sw ? 3 : dim + 2;
   for (int n = 0; n < nf; ++n) row[5 + n] = row[n] / phi0;
@@ -294,6 +294,10 @@ void list_ops(std::vector<std::vector<int>> &out);
 // Field integrals from modal register mode 0: out[n] = sum_e J_e c_d Um[e][n][0].
 cudaError_t launch_integrals(int nf, int ne, int ld, double c_d, const double *Um, const double *J,
                              double *out, cudaStream_t s);
+// The mixed form's reference row from those integrals, on the stream:
+// uref[0 .. kUrefStride) = fill_reference_row(integ / vol).
+cudaError_t launch_reference_row(int physics, int nf, double gamma, double phi0, double vol, const double *integ,
+                                 double *uref, cudaStream_t s);
 
 // What an entry point in another compilation unit needs from a handle.
 struct DomainView {

@@ -66,4 +66,20 @@ cudaError_t launch_integrals(int nf, int ne, int ld, double c_d, const double *U
   return cudaGetLastError();
 }
 
+// One thread: the domain means integ / vol and the derived reference row.
+__global__ void reference_row_kernel(int physics, int nf, double gamma, double phi0, double vol,
+                                     const double *integ, double *uref) {
+  double h[kUrefStride];
+  for (int k = 0; k < kUrefStride; ++k) h[k] = 0.0;
+  for (int n = 0; n < nf; ++n) h[n] = integ[n] / vol;
+  fill_reference_row(physics, gamma, phi0, h);
+  for (int k = 0; k < kUrefStride; ++k) uref[k] = h[k];
+}
+
+cudaError_t launch_reference_row(int physics, int nf, double gamma, double phi0, double vol, const double *integ,
+                                 double *uref, cudaStream_t s) {
+  reference_row_kernel<<<1, 1, 0, s>>>(physics, nf, gamma, phi0, vol, integ, uref);
+  return cudaGetLastError();
+}
+
 }  // namespace dgmx

@@ -247,6 +247,17 @@ dgmx_status dgmx_advance(dgmx_domain *d, double dt, int nsteps);
 /* Same, but only enqueues the work on the handle's stream (no host sync,
  * no error readback); dgmx_sync collects the status. */
 dgmx_status dgmx_advance_async(dgmx_domain *d, double dt, int nsteps);
+/* dgmx_set_state / dgmx_get_state without the host wait, for pipelines that
+ * keep several handles in flight (each handle's copies and kernels run in
+ * order on its own stream, so one solve's transfers overlap another's
+ * steps).  U must be page-locked host memory (cudaHostAlloc or a pinned
+ * tensor); the caller leaves it untouched until dgmx_sync(d) returns, and
+ * reads the result of dgmx_get_state_async only after that.  The mixed
+ * form's reference state is formed on the device.  Not for partitioned
+ * handles.  No counterpart call in the reference (its state lives on the
+ * host). */
+dgmx_status dgmx_set_state_async(dgmx_domain *d, const double *U);
+dgmx_status dgmx_get_state_async(dgmx_domain *d, double *U);
 dgmx_status dgmx_sync(dgmx_domain *d);
 
 /* Conserved totals (integral of each field, FP64 device reduction). */
