@@ -625,38 +625,43 @@ def main():
     e2e_serial = world * dof * 14 * ke / te
     nbytes = 5 * D.nq * 8
 
-    # the same steps as a pipeline of two handles (the asynchronous state
+    # the same steps as a pipeline of three handles (the asynchronous state
     # calls): each step still uploads its input from pinned memory, projects
     # it, takes one LSRK14 step and reads the result back, but one handle's
-    # copies overlap the other's step (separate copy engines each way)
-    D2 = dgm_b200.Domain(mesh, dgm_b200.EULER3D, flux=WORKLOAD["flux"], inttype=dgm_b200.LSRK14,
-                         device=local, precision=dgm_b200.MIXED)
-    D2.set_variant(tiles["mixed"]["variant"])
-    pair = (D, D2)
-    s2 = torch.cuda.ExternalStream(D2.stream(), device=torch.device("cuda", local))
+    # upload and another's read-back overlap the third's step (separate copy
+    # engines each way)
+    extra = [dgm_b200.Domain(mesh, dgm_b200.EULER3D, flux=WORKLOAD["flux"], inttype=dgm_b200.LSRK14,
+                             device=local, precision=dgm_b200.MIXED) for _ in range(2)]
+    for X in extra:
+        X.set_variant(tiles["mixed"]["variant"])
+    pair = (D, *extra)
+    xs = [torch.cuda.ExternalStream(X.stream(), device=torch.device("cuda", local)) for X in extra]
     bufs = [torch.empty((5, D.nq), dtype=torch.float64, pin_memory=True).numpy() for _ in pair]
     for b in bufs:
         b[:] = Uh
 
     def pipeline(k):
         for i in range(k):
-            X, b = pair[i % 2], bufs[i % 2]
+            X, b = pair[i % len(pair)], bufs[i % len(pair)]
             X.sync()                       # its previous read-back has landed in b
             X.set_state_async(b)
             X.advance_async(dt, 1)
             X.state_async(b)
 
-    pipeline(2 * max(1, args.warmup))
+    pipeline(len(pair) * max(1, args.warmup))
     for X in pair:
         X.sync()
     barrier()
-    kp = 2 * ke
-    e0, e1, eb = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    kp = 3 * ke
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(streams["mixed"])
-    s2.wait_event(e0)
+    for sx in xs:
+        sx.wait_event(e0)
     pipeline(kp)
-    eb.record(s2)
-    streams["mixed"].wait_event(eb)
+    for sx in xs:
+        ex = torch.cuda.Event()
+        ex.record(sx)
+        streams["mixed"].wait_event(ex)
     e1.record(streams["mixed"])
     e1.synchronize()
     for X in pair:
@@ -664,7 +669,8 @@ def main():
     barrier()
     tp = max_over_ranks(e0.elapsed_time(e1) / 1e3)
     e2e = world * dof * 14 * kp / tp
-    D2.close()
+    for X in extra:
+        X.close()
 
     peak, kind = peaks()
     stage_mx, stage_64 = tmx / (14 * args.steps), t64 / (14 * args.steps)
@@ -690,8 +696,8 @@ def main():
            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                    "d2h_bytes_per_step": nbytes, "steps": kp,
                    "path": "per step: dgmx_set_state_async (pinned host -> device, projection) + dgmx_advance_async "
-                           "(1 step) + dgmx_get_state_async (device -> pinned host), mixed form, two handles "
-                           "alternating so one's copies overlap the other's step; device time from the first "
+                           "(1 step) + dgmx_get_state_async (device -> pinned host), mixed form, three handles "
+                           "in turn so uploads and read-backs overlap steps; device time from the first "
                            "upload to the last read-back",
                    "serial": {"value": e2e_serial, "steps": ke,
                               "path": "dgmx_set_state + dgmx_advance(1 step) + dgmx_get_state on one handle"}},
