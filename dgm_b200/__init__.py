@@ -374,6 +374,26 @@ class Domain:
         S = np.ascontiguousarray(S).reshape(self.nf, self.nq)
         self._check(f(self.h, S.ctypes.data_as(ctypes.c_void_p)))
 
+    def set_time(self, t: float):
+        """Domain::t (advance adds dt per step)."""
+        f = lib().dgmx_set_time
+        f.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        self._check(f(self.h, float(t)))
+
+    def time(self) -> float:
+        f = lib().dgmx_get_time
+        f.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        t = ctypes.c_double()
+        self._check(f(self.h, ctypes.byref(t)))
+        return t.value
+
+    def set_source_pulse(self, t0: float, sigma_t: float):
+        """Time factor exp(-(t - t0)^2 / (2 sigma_t^2)) on the source, the form
+        of Shallow::GaussianSource; sigma_t <= 0 removes it."""
+        f = lib().dgmx_set_source_pulse
+        f.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+        self._check(f(self.h, float(t0), float(sigma_t)))
+
     def set_bulk_hold(self, on: bool):
         """Channel::holdBulkMassFlow after every projected RHS (Navier-Stokes 3-D)."""
         f = lib().dgmx_set_bulk_hold

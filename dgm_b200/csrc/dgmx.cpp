@@ -144,6 +144,16 @@ struct dgmx_domain {
   cudaGraphExec_t graph = nullptr;
   double graph_dt = 0.0;
   int graph_tcur = -1;
+  // time (Domain::t) and the source's time factor exp(-(t - t0)^2 / (2 sigma_t^2))
+  // of Shallow::GaussianSource (src/Shallow.hpp:666-735); pulse off: factor 1
+  double t = 0.0;
+  bool pulse = false;
+  double pulse_t0 = 0.0, pulse_s2t2i = 0.0;
+  double source_factor(double tt) const {
+    if (!pulse) return 1.0;
+    const double d = tt - pulse_t0;
+    return std::exp(-(d * d * pulse_s2t2i));
+  }
   std::string errmsg;
 
   size_t nmodal() const { return (size_t)ne * nf * ld; }
@@ -170,6 +180,7 @@ struct dgmx_domain {
     a.Ghat = Ghat; a.V = Vtr; a.Pv = Pv;
     a.uref = uref;
     a.Ssrc = Ssrc;
+    a.src_scale = source_factor(t);
     for (int t = 0; t <= kMaxBcTypes; ++t) {
       a.bckind[t] = bckind[t];
       for (int k = 0; k < 5; ++k) a.bcpar[t][k] = bcpar[t][k];
@@ -266,23 +277,23 @@ dgmx_status exchange(dgmx_domain *d, double *T, int blk) {
 
 // The stages of one step: kind, whether the RHS is evaluated on Ut (else U)
 // and the two stage coefficients.
-struct StageSpec { int kind; bool on_ut; double c0, c1; };
+struct StageSpec { int kind; bool on_ut; double c0, c1, ct = 0.0; };   // ct: stage time / dt
 std::vector<StageSpec> stage_specs(int inttype, double dt) {
   std::vector<StageSpec> v;
   switch (inttype) {
     case DGMX_LSRK14:
-      for (int s = 0; s < 14; ++s) v.push_back({kLSRK, false, kLsrkA[s], kLsrkB[s]});
+      for (int s = 0; s < 14; ++s) v.push_back({kLSRK, false, kLsrkA[s], kLsrkB[s], kLsrkC[s]});
       break;
     case DGMX_TVD3:
       v.push_back({kTVD0, false, 0.0, 0.0});
-      v.push_back({kTVD1, true, kTvdA[1], kTvdB[1]});
-      v.push_back({kTVD2, true, kTvdA[2], kTvdB[2]});
+      v.push_back({kTVD1, true, kTvdA[1], kTvdB[1], 1.0});
+      v.push_back({kTVD2, true, kTvdA[2], kTvdB[2], 0.5});
       break;
     case DGMX_RK4:
       v.push_back({kRK40, false, -kRk4A[0] * dt, -kRk4B[0]});
-      v.push_back({kRK41, true, -kRk4A[1] * dt, -kRk4B[1]});
-      v.push_back({kRK41, true, -kRk4A[2] * dt, -kRk4B[2]});
-      v.push_back({kRK43, true, dt, -kRk4B[3]});
+      v.push_back({kRK41, true, -kRk4A[1] * dt, -kRk4B[1], 0.5});
+      v.push_back({kRK41, true, -kRk4A[2] * dt, -kRk4B[2], 0.5});
+      v.push_back({kRK43, true, dt, -kRk4B[3], 1.0});
       break;
     default:
       break;
@@ -297,6 +308,7 @@ StageArgs stage_args(const dgmx_domain *d, const StageSpec &sp, double dt) {
   a.U = d->U; a.Ut = d->Ut; a.A = d->Acc;
   if (d->prm.physics == DGMX_SHALLOW && d->prm.sw_balance) a.Rsub = d->Rsw;
   a.kind = sp.kind; a.X = sp.on_ut ? d->Ut : d->U; a.c0 = sp.c0; a.c1 = sp.c1;
+  a.src_scale = d->source_factor(d->t + sp.ct * dt);   // Domain::t at this stage
   a.Tin = d->T[d->tcur]; a.Tout = d->T[d->tcur ^ 1];
   if (d->mixed()) { a.Utf = d->Utf; a.Tinf = d->Tf[d->tcur]; a.Toutf = d->Tf[d->tcur ^ 1]; }
   a.R0 = d->hold ? d->R0 : nullptr;
@@ -934,6 +946,30 @@ dgmx_status dgmx_set_source(dgmx_domain *d, const double *S) {
   return d->cuda(cudaStreamSynchronize(d->stream), "set_source");
 }
 
+dgmx_status dgmx_set_time(dgmx_domain *d, double t) {
+  if (!d) return DGMX_ERR_ARGUMENT;
+  d->t = t;
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_get_time(const dgmx_domain *d, double *t) {
+  if (!d || !t) return DGMX_ERR_ARGUMENT;
+  *t = d->t;
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_set_source_pulse(dgmx_domain *d, double t0, double sigma_t) {
+  if (!d) return DGMX_ERR_ARGUMENT;
+  if (d->dim == 3) return d->fail(DGMX_ERR_UNSUPPORTED, "source terms are a 2-D feature");
+  if (sigma_t > 0.0 && d->partitioned())
+    return d->fail(DGMX_ERR_UNSUPPORTED, "the source pulse is not built for partitions");
+  d->pulse = sigma_t > 0.0;
+  d->pulse_t0 = t0;
+  d->pulse_s2t2i = d->pulse ? 1.0 / (2.0 * sigma_t * sigma_t) : 0.0;
+  if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  return DGMX_OK;
+}
+
 dgmx_status dgmx_set_bulk_hold(dgmx_domain *d, int on) {
   if (!d) return DGMX_ERR_ARGUMENT;
   if (on && !d->R0) return d->fail(DGMX_ERR_UNSUPPORTED, "the bulk-flow hold is a Navier-Stokes 3-D option");
@@ -1226,9 +1262,11 @@ dgmx_status dgmx_advance_async(dgmx_domain *d, double dt, int nsteps) {
   if (d->partitioned() && d->nccl && (st = build_tiles(d)) != DGMX_OK) return st;
   const int nst = stages_per_step(d->prm.inttype);
   const int reps = (nst & 1) ? 2 : 1;
-  if (d->xhost) {   // host-staged exchanges synchronise every stage: no graph
-    for (int s = 0; s < nsteps; ++s)
+  if (d->xhost || d->pulse) {   // host-staged exchanges synchronise every stage / per-stage source factors: no graph
+    for (int s = 0; s < nsteps; ++s) {
       if ((st = enqueue_step(d, dt)) != DGMX_OK) return st;
+      d->t += dt;
+    }
     return DGMX_OK;
   }
   if (nsteps >= reps && (!d->graph || d->graph_dt != dt || d->graph_tcur != d->tcur)) {
@@ -1256,9 +1294,12 @@ dgmx_status dgmx_advance_async(dgmx_domain *d, double dt, int nsteps) {
     cudaError_t e = cudaGraphLaunch(d->graph, d->stream);
     if (e != cudaSuccess) return d->cuda(e, "graph launch");
     d->launches += (long)nst * reps * launches_per_stage(d);
+    for (int r = 0; r < reps; ++r) d->t += dt;
   }
-  for (; s < nsteps; ++s)
+  for (; s < nsteps; ++s) {
     if ((st = enqueue_step(d, dt)) != DGMX_OK) return st;
+    d->t += dt;
+  }
   return DGMX_OK;
 }
 

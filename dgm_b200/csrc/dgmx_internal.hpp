@@ -138,6 +138,12 @@ inline constexpr double kLsrkB[14] = {0.0367762454319673, 0.3136296607553959, 0.
                            0.3326293790646110, 0.2440251405350864, 0.3718879239592277, 0.6204126221582444,
                            0.1524043173028741, 0.0760894927419266, 0.0077604214040978, 0.0024647284755382,
                            0.0780348340049386, 5.5059777270269628};
+// LSRK14 stage times as fractions of the step (src/TimeInt.cpp:1903-1917)
+inline constexpr double kLsrkC[14] = {0.0, 0.0367762454319673, 0.1249685262725025, 0.2446177702277698,
+                                      0.2476149531070420, 0.2969311120382472, 0.3978149645802642,
+                                      0.5270854589440328, 0.6981269994175695, 0.8190890835352128,
+                                      0.8527059887098624, 0.8604711817462826, 0.8627060376969976,
+                                      0.8734213127600976};
 
 // ------------------------------------------------------------ mixed form
 // Reference state of a solve (the working copies of the mixed form are
@@ -218,6 +224,8 @@ struct StageArgs {
   // (src/Euler.cpp:282-287, src/Navier_Stokes.cpp:95-100,
   // src/Shallow.cpp:255-260), moved past it since projection is linear
   const double *Ssrc;
+  // factor of Ssrc at this stage's time (1 for a source fixed in time)
+  double src_scale;
   // mixed-precision form: FP32 second register and traces; the working
   // copies are perturbations about a reference state per solve:
   // uref[10 s + n] conserved values, uref[10 s + 5 + n] its constant-mode

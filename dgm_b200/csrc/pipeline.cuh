@@ -237,7 +237,7 @@ __device__ __forceinline__ void stage_tile_pipe(const Smem<C> &sm, const StageAr
       for (int k = 0; k < L; ++k) q[k] = Rr[k];
       if (a.Ssrc)
 #pragma unroll
-        for (int k = 0; k < L; ++k) q[k] -= float(a.Ssrc[gi + k]);
+        for (int k = 0; k < L; ++k) q[k] -= float(a.src_scale * a.Ssrc[gi + k]);
       if (a.Rsub)
 #pragma unroll
         for (int k = 0; k < L; ++k) q[k] -= float(a.Rsub[gi + k]);
@@ -265,7 +265,7 @@ __device__ __forceinline__ void stage_tile_pipe(const Smem<C> &sm, const StageAr
       for (int k = 0; k < L; ++k) q[k] = Rr[k];
       if (a.Ssrc)
 #pragma unroll
-        for (int k = 0; k < L; ++k) q[k] -= a.Ssrc[gi + k];
+        for (int k = 0; k < L; ++k) q[k] -= a.src_scale * a.Ssrc[gi + k];
       if (a.Rcap)
 #pragma unroll
         for (int k = 0; k < L; ++k) a.Rcap[gi + k] = q[k];

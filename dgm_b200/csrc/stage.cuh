@@ -678,7 +678,7 @@ __device__ __forceinline__ void stage_tile(const Smem<C> &sm, const StageArgs &a
       for (int k = 0; k < L; ++k) rr[k] = Rr[k];
       if (a.Ssrc)
 #pragma unroll
-        for (int k = 0; k < L; ++k) rr[k] -= float(a.Ssrc[gi + k]);
+        for (int k = 0; k < L; ++k) rr[k] -= float(a.src_scale * a.Ssrc[gi + k]);
       if (a.Rsub)
 #pragma unroll
         for (int k = 0; k < L; ++k) rr[k] -= float(a.Rsub[gi + k]);
@@ -708,7 +708,7 @@ __device__ __forceinline__ void stage_tile(const Smem<C> &sm, const StageArgs &a
       for (int k = 0; k < L; ++k) rr[k] = Rr[k];
       if (a.Ssrc)
 #pragma unroll
-        for (int k = 0; k < L; ++k) rr[k] -= a.Ssrc[gi + k];
+        for (int k = 0; k < L; ++k) rr[k] -= a.src_scale * a.Ssrc[gi + k];
       if (a.Rcap)   // first RHS (shallow-water balance)
 #pragma unroll
         for (int k = 0; k < L; ++k) a.Rcap[gi + k] = rr[k];
@@ -911,7 +911,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) rhs_nodal_kernel(StageArgs a) 
       const int e = e0 + w / BLK;
       if (e >= a.ne) continue;
       const size_t gi = (size_t)e0 * BLK + w;
-      if (a.Ssrc) sm.R[w] = sm.R[w] - a.Ssrc[gi];
+      if (a.Ssrc) sm.R[w] = sm.R[w] - a.src_scale * a.Ssrc[gi];
       if (a.Rcap) a.Rcap[gi] = sm.R[w];
       if (a.Rsub) sm.R[w] = sm.R[w] - a.Rsub[gi];
     }

@@ -178,6 +178,19 @@ dgmx_status dgmx_set_bulk_hold(dgmx_domain *d, int on);
  * apply no source. */
 dgmx_status dgmx_set_source(dgmx_domain *d, const double *S);
 
+/* Domain::t: dgmx_advance[_async] adds dt per step (0 at creation). */
+dgmx_status dgmx_set_time(dgmx_domain *d, double t);
+dgmx_status dgmx_get_time(const dgmx_domain *d, double *t);
+
+/* A time factor on the source: S(x, t) = S(x) exp(-(t - t0)^2 / (2 sigma_t^2)),
+ * the form of Shallow::GaussianSource (src/Shallow.hpp:666-735), whose
+ * spatial part hamp exp(-(x-x0)^2/(2 sx^2) - (y-y0)^2/(2 sy^2)) on the
+ * height field is the S given to dgmx_set_source.  Each stage uses the time
+ * the reference's integrator sets for it (Domain::t = tn + c_s dt,
+ * src/TimeInt.cpp:266-302, :826-860, :1989-2013).  sigma_t <= 0 removes the
+ * factor.  While it is on, steps run without a CUDA graph. */
+dgmx_status dgmx_set_source_pulse(dgmx_domain *d, double t0, double sigma_t);
+
 dgmx_status dgmx_destroy(dgmx_domain *d);
 
 /* nf fields, nq = total GLL points per field, nm = total modes per field. */

@@ -51,6 +51,10 @@ def lib():
         L.ora_set_threads.argtypes = [ctypes.c_int]
         L.ora_lsrk14_coefficients.argtypes = [D, D]
         L.ora_set_source.argtypes = [P, ctypes.c_void_p]
+        L.ora_set_time.argtypes = [P, ctypes.c_double]
+        L.ora_get_time.argtypes = [P]
+        L.ora_get_time.restype = ctypes.c_double
+        L.ora_set_source_pulse.argtypes = [P, ctypes.c_double, ctypes.c_double]
         L.ora_set_sw_balance.argtypes = [P, ctypes.c_int]
         L.ora_set_bc.argtypes = [P, ctypes.c_int, I, D]
         L.ora_set_hold_bulk.argtypes = [P, ctypes.c_int]
@@ -182,6 +186,17 @@ class Problem:
 
     def set_sw_balance(self, on: bool):
         lib().ora_set_sw_balance(self.h, 1 if on else 0)
+
+    def set_time(self, t: float):
+        lib().ora_set_time(self.h, float(t))
+
+    def time(self) -> float:
+        return lib().ora_get_time(self.h)
+
+    def set_source_pulse(self, t0: float, sigma_t: float):
+        """Time factor exp(-(t - t0)^2 / (2 sigma_t^2)) on the source
+        (Shallow::GaussianSource); sigma_t <= 0 removes it."""
+        lib().ora_set_source_pulse(self.h, float(t0), float(sigma_t))
 
     def set_source(self, S):
         """Source field at the GLL points [nf][ntot] (2-D physics: F -= S

@@ -672,6 +672,9 @@ struct Problem {
   // work fields: interior [nf][ntot] and sides [nf][nstot]
   vec Us_s, Uf_s, Uv_u, Uv_s, Usrc;
   vec S;                           // source field at the GLL points [nf][ntot] (empty: none)
+  double t = 0.0;                  // Domain::t, set per stage by the integrators
+  bool pulse = false;              // Shallow::GaussianSource time factor on S
+  double pulse_t0 = 0.0, pulse_s2t2i = 0.0;
   vec U, Ut, R0, R1;               // integrator registers
   // boundary sides (src/Boundary.cpp:25-75, src/Field.cpp:4426-4460): the
   // record names the element side, the BC kind and its two parameters; the
@@ -1740,8 +1743,13 @@ static void time_derivative(Problem &P, const double *Ub, double *Fb) {
   if (P.physics == NS3D) ns3d_diffusion(P, Ub, Fb);
   // add_source (src/Euler.cpp:1297-1302, src/Navier_Stokes.cpp:375-381,
   // src/Shallow.cpp:851-856): ConstSource / FileSource apply, F -= S
-  if (!P.S.empty() && P.dim == 2)
-    for (size_t i = 0; i < P.S.size(); ++i) Fb[i] = Fb[i] - P.S[i];
+  if (!P.S.empty() && P.dim == 2) {
+    // GaussianSource: value = dx^2/(2sx^2) + dy^2/(2sy^2) + (t-t0)^2/(2st^2),
+    // S = hamp exp(-value) (src/Shallow.hpp:720-730), as S(x) exp(-dt^2/(2st^2))
+    const double dtp = P.t - P.pulse_t0;
+    const double g = P.pulse ? std::exp(-(dtp * dtp * P.pulse_s2t2i)) : 1.0;
+    for (size_t i = 0; i < P.S.size(); ++i) Fb[i] = Fb[i] - g * P.S[i];
+  }
   project_all(P, Fb);
   if (P.physics == NS3D && P.hold_bulk) hold_bulk_mass_flow(P, Fb);
   if (P.physics == SHALLOW && P.sw_balance) {
@@ -1759,15 +1767,18 @@ static void rk4_step(Problem &P, double dt) {
                               0.33333333333333333, 0.16666666666666667};
   const size_t M = (size_t)P.nf * P.ntot;
   double *U = P.U.data(), *Ut = P.Ut.data(), *R0 = P.R0.data(), *R1 = P.R1.data();
+  const double tn = P.t;
   time_derivative(P, U, R0);
   for (size_t i = 0; i < M; ++i) Ut[i] = (-a[0] * dt) * R0[i] + U[i];
   for (size_t i = 0; i < M; ++i) R0[i] = -b[0] * R0[i];
+  P.t = tn + 0.5 * dt;
   time_derivative(P, Ut, R1);
   for (size_t i = 0; i < M; ++i) Ut[i] = (-a[1] * dt) * R1[i] + U[i];
   for (size_t i = 0; i < M; ++i) R0[i] = -b[1] * R1[i] + R0[i];
   time_derivative(P, Ut, R1);
   for (size_t i = 0; i < M; ++i) Ut[i] = (-a[2] * dt) * R1[i] + U[i];
   for (size_t i = 0; i < M; ++i) R0[i] = -b[2] * R1[i] + R0[i];
+  P.t = tn + dt;
   time_derivative(P, Ut, R1);
   for (size_t i = 0; i < M; ++i) R0[i] = -b[3] * R1[i] + R0[i];
   for (size_t i = 0; i < M; ++i) U[i] = dt * R0[i] + U[i];
@@ -1779,14 +1790,18 @@ static void tvd3_step(Problem &P, double dt) {
   static const double b[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
   const size_t M = (size_t)P.nf * P.ntot;
   double *U = P.U.data(), *Ut = P.Ut.data(), *R0 = P.R0.data();
+  const double tn = P.t;   // stage times tn + c dt, c = 0, 1, 1/2 (src/TimeInt.cpp:740)
   time_derivative(P, U, R0);
   for (size_t i = 0; i < M; ++i) Ut[i] = -dt * R0[i] + U[i];
+  P.t = tn + 1.0 * dt;
   time_derivative(P, Ut, R0);
   for (size_t i = 0; i < M; ++i) R0[i] = -dt * R0[i] + Ut[i];
   for (size_t i = 0; i < M; ++i) { Ut[i] = b[1] * R0[i]; Ut[i] = a[1] * U[i] + Ut[i]; }
+  P.t = tn + 0.5 * dt;
   time_derivative(P, Ut, R0);
   for (size_t i = 0; i < M; ++i) R0[i] = -dt * R0[i] + Ut[i];
   for (size_t i = 0; i < M; ++i) { U[i] = a[2] * U[i]; U[i] = b[2] * R0[i] + U[i]; }
+  P.t = tn + dt;
 }
 
 // LSRK14 (src/TimeInt.cpp:1870-1917 coefficients, :1989-2013 advance)
@@ -1806,11 +1821,19 @@ static const double kLsrkB[14] = {
 static void lsrk14_step(Problem &P, double dt) {
   const size_t M = (size_t)P.nf * P.ntot;
   double *U = P.U.data(), *Ut = P.Ut.data(), *R0 = P.R0.data();
+  static const double c[14] = {0.0, 0.0367762454319673, 0.1249685262725025, 0.2446177702277698,
+                               0.2476149531070420, 0.2969311120382472, 0.3978149645802642,
+                               0.5270854589440328, 0.6981269994175695, 0.8190890835352128,
+                               0.8527059887098624, 0.8604711817462826, 0.8627060376969976,
+                               0.8734213127600976};
+  const double tn = P.t;   // t = tn + c_s dt per stage, tn + dt after (src/TimeInt.cpp:1999-2011)
   for (int s = 0; s < 14; ++s) {
+    P.t = tn + c[s] * dt;
     time_derivative(P, U, R0);
     for (size_t i = 0; i < M; ++i) { double t = kLsrkA[s] * Ut[i]; Ut[i] = -dt * R0[i] + t; }
     for (size_t i = 0; i < M; ++i) U[i] = kLsrkB[s] * Ut[i] + U[i];
   }
+  P.t = tn + dt;
 }
 
 }  // namespace ora
@@ -1885,6 +1908,15 @@ void ora_set_source(void *h, const double *S) {
   auto *P = (Problem *)h;
   if (!S) { P->S.clear(); return; }
   P->S.assign(S, S + (size_t)P->nf * P->ntot);
+}
+
+void ora_set_time(void *h, double t) { ((Problem *)h)->t = t; }
+double ora_get_time(void *h) { return ((Problem *)h)->t; }
+void ora_set_source_pulse(void *h, double t0, double sigma_t) {
+  auto *P = (Problem *)h;
+  P->pulse = sigma_t > 0.0;
+  P->pulse_t0 = t0;
+  P->pulse_s2t2i = P->pulse ? 1.0 / (2.0 * sigma_t * sigma_t) : 0.0;
 }
 
 // The LSRK14 2N-storage coefficients (A: register decay, B: update weight).

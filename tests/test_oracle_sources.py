@@ -33,3 +33,22 @@ def test_no_source_in_3d():
     F0 = P.rhs(U0)
     P.set_source(np.ones((5, x.size)))
     assert np.array_equal(P.rhs(U0), F0)
+
+
+def test_oracle_time_follows_the_integrators():
+    """Domain::t after n steps is n dt for LSRK14, TVD3 and RK4, and a source
+    pulse far from the run's times leaves the source off."""
+    P = oracle.Problem(_mesh(2, (3, 3), -2, 2, 2), oracle.SHALLOW)
+    P.set_sw_balance(False)
+    x, y, _ = P.coords()
+    U0 = P.project(ics.gaussian_bump(x, y, a=0.3, w=0.5))
+    for inttype in (14, 3, 4):
+        P.set_time(0.0)
+        P.set_state(U0)
+        assert P.advance(inttype, 0.001, 7) == 0
+        assert abs(P.time() - 0.007) < 1e-15
+    F0 = P.rhs(U0)
+    P.set_source(np.ones((3, x.size)))
+    P.set_source_pulse(100.0, 0.01)
+    P.set_time(0.0)
+    assert np.array_equal(P.rhs(U0), F0)
