@@ -280,9 +280,22 @@ class Domain:
         self._check(lib().dgmx_get_state(self.h, _dp(U)))
         return U
 
+    def _check_host_buffer(self, U):
+        """A host array the engine copies the whole state into or out of:
+        float64, C-contiguous, nf * nq values (anything else would let the
+        copy run past the array)."""
+        if not isinstance(U, np.ndarray):
+            raise ValueError("state buffer must be a numpy array")
+        if U.dtype != np.float64:
+            raise ValueError(f"state buffer must be float64, got {U.dtype}")
+        if not U.flags.c_contiguous:
+            raise ValueError("state buffer must be C-contiguous")
+        if U.size != self.nf * self.nq:
+            raise ValueError(f"state buffer holds {U.size} values, the state has {self.nf * self.nq}")
+
     def state_into(self, U):
         """get_state into a caller array (page-locked arrays are written by DMA)."""
-        assert U.dtype == np.float64 and U.flags.c_contiguous and U.size == self.nf * self.nq
+        self._check_host_buffer(U)
         self._check(lib().dgmx_get_state(self.h, _dp(U)))
         return U
 
@@ -291,7 +304,7 @@ class Domain:
         float64 array in the Field layout, left untouched until sync()."""
         f = lib().dgmx_set_state_async
         f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
-        assert U.dtype == np.float64 and U.flags.c_contiguous and U.size == self.nf * self.nq
+        self._check_host_buffer(U)
         self._check(f(self.h, U.ctypes.data_as(ctypes.c_void_p)))
 
     def state_async(self, U):
@@ -299,7 +312,7 @@ class Domain:
         the state once sync() returns."""
         f = lib().dgmx_get_state_async
         f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
-        assert U.dtype == np.float64 and U.flags.c_contiguous and U.size == self.nf * self.nq
+        self._check_host_buffer(U)
         self._check(f(self.h, U.ctypes.data_as(ctypes.c_void_p)))
         return U
 

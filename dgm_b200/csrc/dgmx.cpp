@@ -1719,7 +1719,9 @@ dgmx_status dgmx_mesh_links(const dgmx_mesh *m, int *links, int *perm_pairs) {
 // ------------------------------------------------------------------------
 // Read-only view of a handle for entry points compiled in other units.
 namespace dgmx {
-bool domain_view(dgmx_domain *d, DomainView *v) {
+bool domain_view(dgmx_domain *d, DomainView *v, bool *partitioned, std::string **errmsg) {
+  if (partitioned) *partitioned = d && d->partitioned();
+  if (errmsg) *errmsg = d ? &d->errmsg : nullptr;
   if (!d || !v || d->partitioned()) return false;
   v->ops = d->ops;
   v->stream = d->stream;

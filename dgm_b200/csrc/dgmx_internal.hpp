@@ -320,7 +320,9 @@ struct DomainView {
   std::string *errmsg;
   long *launches;
 };
-bool domain_view(dgmx_domain *d, DomainView *v);
+// False for a null handle or a partitioned one (*partitioned tells which;
+// the partitioned handle's error text is then reachable through *errmsg).
+bool domain_view(dgmx_domain *d, DomainView *v, bool *partitioned = nullptr, std::string **errmsg = nullptr);
 
 inline int nfields_of(int physics) {
   return physics == DGMX_SHALLOW ? 3 : (physics == DGMX_EULER3D || physics == DGMX_NS3D ? 5 : 4);

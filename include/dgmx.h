@@ -284,17 +284,22 @@ const char *dgmx_last_error(const dgmx_domain *d);
 long dgmx_launch_count(const dgmx_domain *d);
 
 /* Domain::time_derivative on device buffers for callers that cannot
- * allocate device memory when they need the RHS (a host callback that may
- * not call the CUDA API, a real-time loop that forbids allocation, a caller
- * whose memory belongs to an arena).  No counterpart in the reference: the
- * face-trace scratch lives in a fixed 8 MiB static device array (at most
- * 1,048,576 doubles = ne * faces * fields * side points) instead of the
- * handle's buffers; larger meshes return DGMX_ERR_ARGUMENT.  The array is
- * shared by all calls on a device and keeps the last call's contents, so
- * calls that overlap on the GPU race; the first call on a device resolves
- * the array's address and should come before any stream capture.  Enqueued
- * on the handle's stream; no cudaMalloc, cudaFree or other allocation.
- * Euler and shallow water only (Navier-Stokes returns DGMX_ERR_UNSUPPORTED). */
+ * allocate device memory when they need the RHS: a real-time loop that
+ * forbids allocation on its call path, or a caller whose device memory is
+ * owned by an arena sized once at start-up.  No counterpart in the
+ * reference: the face-trace scratch lives in a fixed 8 MiB static device
+ * array (at most 1,048,576 doubles = ne * faces * fields * side points)
+ * instead of the handle's buffers; larger meshes return DGMX_ERR_ARGUMENT.
+ * The array is shared by all calls on a device and keeps the last call's
+ * contents, so calls that overlap on the GPU race.  It is called from an
+ * ordinary host thread and does call the CUDA runtime (kernel launches; on
+ * its first use on a device cudaGetSymbolAddress, which under lazy module
+ * loading loads the module and reserves the array's 8 MiB on that device),
+ * so it is not for host functions enqueued with cudaLaunchHostFunc; make
+ * that first call at set-up time, before any stream capture.  Enqueued on
+ * the handle's stream; no cudaMalloc, cudaFree or other allocation after
+ * the first call.  Euler and shallow water on whole domains only
+ * (Navier-Stokes and partitioned handles return DGMX_ERR_UNSUPPORTED). */
 dgmx_status dgmx_time_derivative_static(dgmx_domain *d, const double *U_dev, double *F_dev);
 
 /* The handle's CUDA stream (cudaStream_t), for callers that record events or

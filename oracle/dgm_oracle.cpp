@@ -11,8 +11,10 @@
 // Citations are path:line inside the reference project (sandialabs/dgm).
 //
 // Parity status: pinned against the reference's own golden restart files
-// runs/vhex.ref, runs/nvortex.ref and runs/vquad.ref (tests/golden/, checked
-// by tests/test_oracle_golden.py).
+// runs/vhex.ref, runs/vquad.ref, runs/vortex.ref and runs/chan/chan.ref
+// (tests/golden/, checked by tests/test_oracle_golden.py and
+// tests/test_restart.py).  runs/nvortex.ref uses NodalQuad elements, which
+// this oracle does not restate, so it pins nothing here.
 // =============================================================================
 #include <cmath>
 #include <cstdint>

@@ -80,4 +80,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DGM_REFERENCE_ROOT", "")
+    if not root:
+        sys.exit("usage: make_golden.py <reference checkout root> (or set DGM_REFERENCE_ROOT)")
+    main(root)

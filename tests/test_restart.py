@@ -18,8 +18,11 @@ import oracle
 from oracle import dgm_io, ics
 from tests.cases import diff_norms
 
-REF = "/root/reference/runs/vhex.ref"
-CHAN_REF = "/root/reference/runs/chan/chan.ref"
+# The reference checkout (read-only), when one is mounted: DGM_REFERENCE_ROOT
+# names its root; the tests that read its files skip without it.
+REF_ROOT = os.environ.get("DGM_REFERENCE_ROOT", "")
+REF = os.path.join(REF_ROOT, "runs", "vhex.ref") if REF_ROOT else ""
+CHAN_REF = os.path.join(REF_ROOT, "runs", "chan", "chan.ref") if REF_ROOT else ""
 
 
 def test_reads_the_references_golden_restart():
