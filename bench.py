@@ -50,6 +50,10 @@ METRIC = "DOF-stage-updates/s mixed vs FP64 at matched L2 err; p50/p99 solve lat
 UNIT = "DOF-stage-updates/s"
 # algorithmic bytes per modal DOF and stage: read U, read Ut, write Ut, write U
 BYTES_PER_DOF_STAGE = {"fp64": 32, "mixed": 24}   # mixed: U FP64, Ut FP32
+# algorithmic flops per modal DOF and stage of the reference algorithm at
+# p=3, q=5 (volume gradients, pointwise fluxes, side interpolation and lift,
+# one face flux per unique face, projection and update: 81k per element)
+FLOPS_PER_DOF_STAGE = 253
 
 
 def parse():
@@ -61,7 +65,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n", type=int, default=WORKLOAD["n"], help="elements per direction")
     ap.add_argument("--no-forms", action="store_true", help="skip the ensemble and serving legs")
-    ap.add_argument("--l2-steps", type=int, default=100, help="steps of the mixed-vs-FP64 accuracy run")
+    ap.add_argument("--l2-steps", type=int, default=500,
+                    help="steps of the mixed-vs-FP64 accuracy run (the configuration's own 500)")
+    ap.add_argument("--oracle-steps", type=int, default=10,
+                    help="steps of the accuracy run against the FP64 oracle (rank 0, host cores)")
     ap.add_argument("--ensemble", type=int, default=1024, help="solves in the batched ensemble")
     ap.add_argument("--trace", type=int, default=200, help="requests in the serving trace")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both",
@@ -186,12 +193,14 @@ def cpu_measure(n, p, q, stages_sample, threads):
     return dof * 14 * stages_sample / t, t
 
 
-def config_dict(n, p, q, dof):
+def config_dict(n, p, q, dof, world=1):
+    """The workload, identical for both arms (the precision and the tile each
+    arm runs are reported outside `config`)."""
     return {"workload": WORKLOAD["name"] if n == WORKLOAD["n"] else f"euler3d_taylor_green_{n}^3_p{p}_roe_lsrk14",
             "mesh": f"{n}^3 Hex, periodic [0,2pi]^3", "p": p, "q": q, "physics": "Euler 3-D",
             "flux": "Roe", "integrator": "LSRK14 (14 stages/step)", "Mach": WORKLOAD["Ma"],
             "modal_dof": dof, "cfl": WORKLOAD["cfl"],
-            "precision": "mixed: FP32 states, fluxes and contractions, FP64 solution register",
+            "parallelism": f"replicas x{world}" if world > 1 else "single device",
             "l2": "inputs larger than L2 (modal U 84 MB + Ut 42 MB, traces 2x63 MB per replica in the mixed "
                   "form; 168 + 2x126 MB in FP64)"}
 
@@ -220,7 +229,8 @@ def run_reference(args):
     out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference",
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-           "data": "synthetic (Taylor-Green initial condition)", "config": config_dict(n, p, q, dof),
+           "data": "synthetic (Taylor-Green initial condition)", "config": config_dict(n, p, q, dof, args.gpus),
+           "precision": "FP64 (the oracle: CPU restatement of the reference algorithm)",
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                             "sample": f"{args.steps} LSRK14 steps of the full workload after {args.warmup} warm-up"},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -230,6 +240,92 @@ def run_reference(args):
 
 def rel_l2(a, b):
     return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
+
+
+def field_errors(S, R):
+    """Relative L2 of S against R per conserved field, for the momentum
+    vector as one field, of the z-momentum against that vector's norm, and
+    over the whole state."""
+    return {"per_field": [rel_l2(S[k], R[k]) for k in range(S.shape[0])],
+            "momentum_vector": rel_l2(S[1:4], R[1:4]),
+            "rho_w_vs_momentum_norm": float(np.linalg.norm(S[3] - R[3]) / max(np.linalg.norm(R[1:4]), 1e-300)),
+            "aggregate": rel_l2(S, R)}
+
+
+def measure_e2e(dgm_b200, D, stream, prec, mesh, local, variant, dt, args, barrier, max_over_ranks, world, dof):
+    """The metric through the public C ABI with host buffers: per step the
+    state is uploaded from pinned host memory (and projected), advanced one
+    LSRK14 step and read back.  Serial on one handle, and as a pipeline of
+    three handles (the asynchronous state calls) so one solve's upload and
+    another's read-back overlap the third's step on separate copy engines."""
+    import torch
+    Uh = torch.empty((5, D.nq), dtype=torch.float64, pin_memory=True).numpy()
+    Uh[:] = D.state()
+    for _ in range(max(1, args.warmup)):
+        D.set_state(Uh)
+        D.advance(dt, 1)
+        D.state_into(Uh)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ke = max(3, args.steps // 2)
+    e0.record(stream)
+    for _ in range(ke):
+        D.set_state(Uh)
+        D.advance(dt, 1)
+        D.state_into(Uh)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    e2e_serial = world * dof * 14 * ke / te
+    nbytes = 5 * D.nq * 8
+    extra = [dgm_b200.Domain(mesh, dgm_b200.EULER3D, flux=WORKLOAD["flux"], inttype=dgm_b200.LSRK14,
+                             device=local, precision=prec) for _ in range(2)]
+    for X in extra:
+        X.set_variant(variant)
+    pair = (D, *extra)
+    xs = [torch.cuda.ExternalStream(X.stream(), device=torch.device("cuda", local)) for X in extra]
+    bufs = [torch.empty((5, D.nq), dtype=torch.float64, pin_memory=True).numpy() for _ in pair]
+    for b in bufs:
+        b[:] = Uh
+
+    def pipeline(k):
+        for i in range(k):
+            X, b = pair[i % len(pair)], bufs[i % len(pair)]
+            X.sync()                       # its previous read-back has landed in b
+            X.set_state_async(b)
+            X.advance_async(dt, 1)
+            X.state_async(b)
+
+    pipeline(len(pair) * max(1, args.warmup))
+    for X in pair:
+        X.sync()
+    barrier()
+    kp = 3 * ke
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for sx in xs:
+        sx.wait_event(e0)
+    pipeline(kp)
+    for sx in xs:
+        ex = torch.cuda.Event()
+        ex.record(sx)
+        stream.wait_event(ex)
+    e1.record(stream)
+    e1.synchronize()
+    for X in pair:
+        X.sync()
+    barrier()
+    tp = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    for X in extra:
+        X.close()
+    return {"value": world * dof * 14 * kp / tp, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+            "d2h_bytes_per_step": nbytes, "steps": kp,
+            "path": "per step: dgmx_set_state_async (pinned host -> device, projection) + dgmx_advance_async "
+                    "(1 step) + dgmx_get_state_async (device -> pinned host), three handles in turn so uploads "
+                    "and read-backs overlap steps; device time from the first upload to the last read-back",
+            "serial": {"value": e2e_serial, "steps": ke,
+                       "path": "dgmx_set_state + dgmx_advance(1 step) + dgmx_get_state on one handle"}}
 
 
 def time_steps(D, stream, dt, steps, warmup, barrier, max_over_ranks, clk=None):
@@ -592,87 +688,49 @@ def main():
     value = world * dof * 14 * args.steps / tmx
     v64 = world * dof * 14 * args.steps / t64
 
-    # accuracy: mixed vs the FP64 path (parity-tested against the oracle) from the same state
+    # accuracy: mixed and FP64 against the FP64 oracle over the first steps
+    # (one rank), and mixed against the FP64 path (itself within 1e-12 of the
+    # oracle, tests/test_gpu_parity_at_size.py) over the configuration's own
+    # step count
+    accuracy = {}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.oracle_steps > 0:
+        import oracle
+        oracle.set_threads(os.cpu_count() or 1)
+        P = build_oracle_problem(n, p, q)
+        P.set_state(P.project(U_ic))
+        t0 = time.perf_counter()
+        P.advance(14, dt, args.oracle_steps)
+        O = P.state()
+        to = time.perf_counter() - t0
+        row = {"steps": args.oracle_steps, "t": args.oracle_steps * dt, "oracle_s": round(to, 1)}
+        for name, D in doms.items():
+            D.set_state(U_ic)
+            D.advance(dt, args.oracle_steps)
+            row[name] = field_errors(D.state(), O)
+        del P
+        accuracy["vs_fp64_oracle"] = row
     for D in doms.values():
         D.set_state(U_ic)
         D.advance(dt, args.l2_steps)
     S64, Smx = doms["fp64"].state(), doms["mixed"].state()
-    accuracy = {"steps": args.l2_steps, "t": args.l2_steps * dt, "rel_l2_mixed_vs_fp64": rel_l2(Smx, S64),
-                "rel_l2_per_field": [rel_l2(Smx[k], S64[k]) for k in range(5)],
-                "rel_l2_of_state_change_fp64": rel_l2(S64, U_ic),
-                "note": "relative L2 over all GLL values; the FP64 path matches the FP64 oracle to 1e-12"}
+    accuracy["mixed_vs_fp64"] = {"steps": args.l2_steps, "t": args.l2_steps * dt, **field_errors(Smx, S64),
+                                 "rel_l2_of_state_change_fp64": rel_l2(S64, U_ic)}
+    accuracy["note"] = ("relative L2 over all GLL values, per conserved field (rho, rho u, rho v, rho w, E); "
+                        "rho w starts at exactly zero, so its own relative figure compares round-off with a "
+                        "near-zero norm: 'momentum_vector' takes the three momenta as one field and "
+                        "'rho_w_vs_momentum_norm' measures the z-momentum error against that field's norm")
 
-    # ---- end to end through the C ABI with pinned host buffers (mixed form)
-    D = doms["mixed"]
-    Uh = torch.empty((5, D.nq), dtype=torch.float64, pin_memory=True).numpy()
-    Uh[:] = D.state()
-    for _ in range(max(1, args.warmup)):
-        D.set_state(Uh)
-        D.advance(dt, 1)
-        D.state_into(Uh)
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ke = max(3, args.steps // 2)
-    e0.record(streams["mixed"])
-    for _ in range(ke):
-        D.set_state(Uh)
-        D.advance(dt, 1)
-        D.state_into(Uh)
-    e1.record(streams["mixed"])
-    e1.synchronize()
-    barrier()
-    te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
-    e2e_serial = world * dof * 14 * ke / te
-    nbytes = 5 * D.nq * 8
-
-    # the same steps as a pipeline of three handles (the asynchronous state
-    # calls): each step still uploads its input from pinned memory, projects
-    # it, takes one LSRK14 step and reads the result back, but one handle's
-    # upload and another's read-back overlap the third's step (separate copy
-    # engines each way)
-    extra = [dgm_b200.Domain(mesh, dgm_b200.EULER3D, flux=WORKLOAD["flux"], inttype=dgm_b200.LSRK14,
-                             device=local, precision=dgm_b200.MIXED) for _ in range(2)]
-    for X in extra:
-        X.set_variant(tiles["mixed"]["variant"])
-    pair = (D, *extra)
-    xs = [torch.cuda.ExternalStream(X.stream(), device=torch.device("cuda", local)) for X in extra]
-    bufs = [torch.empty((5, D.nq), dtype=torch.float64, pin_memory=True).numpy() for _ in pair]
-    for b in bufs:
-        b[:] = Uh
-
-    def pipeline(k):
-        for i in range(k):
-            X, b = pair[i % len(pair)], bufs[i % len(pair)]
-            X.sync()                       # its previous read-back has landed in b
-            X.set_state_async(b)
-            X.advance_async(dt, 1)
-            X.state_async(b)
-
-    pipeline(len(pair) * max(1, args.warmup))
-    for X in pair:
-        X.sync()
-    barrier()
-    kp = 3 * ke
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(streams["mixed"])
-    for sx in xs:
-        sx.wait_event(e0)
-    pipeline(kp)
-    for sx in xs:
-        ex = torch.cuda.Event()
-        ex.record(sx)
-        streams["mixed"].wait_event(ex)
-    e1.record(streams["mixed"])
-    e1.synchronize()
-    for X in pair:
-        X.sync()
-    barrier()
-    tp = max_over_ranks(e0.elapsed_time(e1) / 1e3)
-    e2e = world * dof * 14 * kp / tp
-    for X in extra:
-        X.close()
+    # ---- end to end through the C ABI with pinned host buffers, both forms
+    e2e = {name: measure_e2e(dgm_b200, doms[name], streams[name], prec, mesh, local, tiles[name]["variant"], dt,
+                             args, barrier, max_over_ranks, world, dof)
+           for name, prec in forms_run}
 
     peak, kind = peaks()
+    fp64_peak = None
+    try:
+        fp64_peak = dgm_b200.fma_peak(True, local)
+    except Exception:
+        pass
     stage_mx, stage_64 = tmx / (14 * args.steps), t64 / (14 * args.steps)
 
     def roof(prec, stage_s, prof):
@@ -683,24 +741,25 @@ def main():
                 "algorithmic_bytes_per_launch": BYTES_PER_DOF_STAGE[prec] * dof,
                 "stage_us": 1e6 * stage_s}
 
+    fp64_roof = roof("fp64", stage_64, "euler3d_tgv_p3_stage_kernel.md")
+    fp64_pipe = None
+    if fp64_peak:
+        ach = FLOPS_PER_DOF_STAGE * dof / stage_64 / 1e12
+        fp64_pipe = {"bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s", "frac": ach / fp64_peak,
+                     "peak_kind": "measured live (dgmx_measure_fma_peak: FP64 FMA chains over a full grid)",
+                     "algorithmic_flops_per_dof_stage": FLOPS_PER_DOF_STAGE}
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tmx / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 solution register)",
            "data": "synthetic (Taylor-Green initial condition, no dataset)",
-           "config": config_dict(n, p, q, dof) | {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                                                  "tile": tiles["mixed"]},
+           "config": config_dict(n, p, q, dof, world),
+           "precision": "mixed: FP32 states, fluxes and contractions, FP64 solution register",
+           "tile": tiles["mixed"],
            "fp64": {"value": v64, "unit": UNIT, "ms_per_step": 1e3 * t64 / args.steps, "tile": tiles["fp64"],
-                    "roofline": roof("fp64", stage_64, "euler3d_tgv_p3_stage_kernel.md")},
+                    "roofline": fp64_roof, "roofline_fp64_pipe": fp64_pipe, "e2e": e2e["fp64"]},
            "speedup_mixed_vs_fp64": value / v64,
            "accuracy": accuracy,
-           "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes,
-                   "d2h_bytes_per_step": nbytes, "steps": kp,
-                   "path": "per step: dgmx_set_state_async (pinned host -> device, projection) + dgmx_advance_async "
-                           "(1 step) + dgmx_get_state_async (device -> pinned host), mixed form, three handles "
-                           "in turn so uploads and read-backs overlap steps; device time from the first "
-                           "upload to the last read-back",
-                   "serial": {"value": e2e_serial, "steps": ke,
-                              "path": "dgmx_set_state + dgmx_advance(1 step) + dgmx_get_state on one handle"}},
+           "e2e": e2e["mixed"],
            "gpu_launches": int(launches), "clocks": clk.summary(),
            "roofline": roof("mixed", stage_mx, "euler3d_tgv_p3_stage_mixed.md")}
     for Dx in doms.values():

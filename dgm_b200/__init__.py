@@ -88,6 +88,17 @@ def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
+def fma_peak(fp64: bool = True, device: int = 0, reps: int = 5) -> float:
+    """Measured FMA throughput of the GPU in TFLOP/s (FP64 or FP32)."""
+    f = lib().dgmx_measure_fma_peak
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    t = ctypes.c_double()
+    st = f(int(device), 1 if fp64 else 0, int(reps), ctypes.byref(t))
+    if st != 0:
+        raise DgmxError(st, "FMA peak measurement failed")
+    return t.value
+
+
 def kernel_list():
     """Compiled instantiations: rows of (physics, L, Q, elements/CTA, threads, smem bytes, min CTAs/SM)."""
     n = 4096
@@ -421,6 +432,15 @@ class Domain:
         n, w = ctypes.c_int(), ctypes.c_int()
         self._check(f(self.h, int(index), ctypes.byref(n), ctypes.byref(w)))
         return n.value, int(w.value)
+
+    def set_wait_limit(self, tries: int):
+        """Fault injection for tests: bound the prefetching stage kernel's
+        first wait per tile to `tries` (0: every wait runs out, the call
+        fails with DGMX_ERR_CUDA and the context stays usable); a negative
+        value restores the default bound."""
+        f = lib().dgmx_set_wait_limit
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        self._check(f(self.h, int(tries)))
 
     def variant_count(self) -> int:
         f = lib().dgmx_set_variant

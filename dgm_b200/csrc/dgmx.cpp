@@ -140,6 +140,8 @@ struct dgmx_domain {
   int tcur = 0;
   bool sw_captured = false;
   long launches = 0;
+  // bound of the copy pipeline's first wait per tile (dgmx_set_wait_limit)
+  int wait_tries = kWaitTries;
   // graph of one whole step
   cudaGraphExec_t graph = nullptr;
   double graph_dt = 0.0;
@@ -181,6 +183,7 @@ struct dgmx_domain {
     a.uref = uref;
     a.Ssrc = Ssrc;
     a.src_scale = source_factor(t);
+    a.wait_tries = wait_tries;
     for (int t = 0; t <= kMaxBcTypes; ++t) {
       a.bckind[t] = bckind[t];
       for (int k = 0; k < 5; ++k) a.bcpar[t][k] = bcpar[t][k];
@@ -1407,6 +1410,13 @@ dgmx_status dgmx_autotune(dgmx_domain *d, int reps, double *rows, int cap, int *
   if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
   if (nvariants) *nvariants = (int)vs->size();
   if (chosen) *chosen = best;
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_set_wait_limit(dgmx_domain *d, int tries) {
+  if (!d) return DGMX_ERR_ARGUMENT;
+  d->wait_tries = tries < 0 ? kWaitTries : tries;
+  if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
   return DGMX_OK;
 }
 

@@ -250,7 +250,11 @@ struct StageArgs {
   // if set, the constant-mode coefficient of every field's final projected
   // RHS, [e][field] (bulk-flow hold)
   double *R0;
+  // tries of the copy pipeline's wait for a tile's inputs before it gives
+  // up (bit 1 of err[0]); kWaitTries unless a test lowers it
+  int wait_tries;
 };
+constexpr int kWaitTries = 1 << 20;
 
 // Bulk-flow hold (hold.cu): cbar[n] = sum_e J_e R0[e][n] / sum_e J_e for the
 // held fields (density, x-momentum, energy), then the stage kind's linear

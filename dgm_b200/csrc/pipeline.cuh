@@ -77,8 +77,8 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
 }
 
 // Bounded wait (each try suspends for at most a few microseconds).
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
-  for (int it = 0; it < (1 << 20); ++it)
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, int tries = kWaitTries) {
+  for (int it = 0; it < tries; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -337,10 +337,11 @@ __global__ void __launch_bounds__(C::NT, C::MINB) stage_pipe_kernel(StageArgs a)
     if (e0 < 0) break;
     const int b = i & 1;
     unsigned char *buf = bufs + b * P::BUF_B;
-    const bool ok = mbar_wait(&bar[b], (unsigned)((i >> 1) & 1));
+    const bool ok = mbar_wait(&bar[b], (unsigned)((i >> 1) & 1), a.wait_tries);
     if (__syncthreads_or(!ok)) {
       if (tid == 0) atomicOr(a.err, 2);
-      // let copies still in flight land before the CTA leaves
+      // let copies still in flight land before the CTA leaves (with the
+      // full bound, whatever bound the first wait had)
       mbar_wait(&bar[b], (unsigned)((i >> 1) & 1));
       return;
     }

@@ -402,6 +402,7 @@ StageArgs arena_args(const dgmx_pool *P, const Arena &a) {
   s.ne = a.cap; s.gamma = P->prm.gamma; s.flux = P->prm.flux; s.err = a.err;
   s.uref = a.mixed ? a.uref : nullptr;
   s.esolve = a.esolve;
+  s.wait_tries = kWaitTries;
   return s;
 }
 

@@ -283,6 +283,22 @@ const char *dgmx_last_error(const dgmx_domain *d);
 /* Number of kernel launches the handle has issued since creation. */
 long dgmx_launch_count(const dgmx_domain *d);
 
+/* Measured fused multiply-add throughput of this GPU in TFLOP/s (fp64 = 1:
+ * FP64, 0: FP32), best of `reps` timed launches of independent FMA chains
+ * over a full grid; the denominator of the FP64/FP32 pipe fractions the
+ * benchmark reports.  Allocates 16 bytes for the duration of the call.  No
+ * counterpart in the reference. */
+dgmx_status dgmx_measure_fma_peak(int device, int fp64, int reps, double *tflops);
+
+/* Fault-injection hook for tests of failure detection (no counterpart in
+ * the reference).  Bounds the number of tries of the prefetching stage
+ * kernel's first wait for a tile's inputs; a wait that runs out sets bit 1
+ * of the handle's device error word, the CTA waits (with the normal bound)
+ * for its copies in flight and leaves, and the call returns DGMX_ERR_CUDA
+ * with the context still usable.  0 makes every such wait run out at once;
+ * a negative value restores the default (2^20 tries). */
+dgmx_status dgmx_set_wait_limit(dgmx_domain *d, int tries);
+
 /* Domain::time_derivative on device buffers for callers that cannot
  * allocate device memory when they need the RHS: a real-time loop that
  * forbids allocation on its call path, or a caller whose device memory is
