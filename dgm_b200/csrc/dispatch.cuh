@@ -4,6 +4,7 @@
 
 #include "ns.cuh"
 #include "pipeline.cuh"
+#include "stage2.cuh"
 
 namespace dgmx {
 
@@ -37,6 +38,29 @@ static cudaError_t upload_tables_lq(const Tables1D &t) {
     for (size_t k = 0; k < (size_t)Q * (Q - 1); ++k) gw[end_ * Q * (Q - 1) + k] = t.g2gl[k] / t.w[end_ ? Q - 1 : 0];
   if ((e = put(cBw<T, L, Q>, bw, (size_t)L * Q)) != cudaSuccess) return e;
   return put(cG2GLw<T, L, Q>, gw, (size_t)2 * Q * (Q - 1));
+}
+
+// Tables of the second-form stage kernel (only its compilation unit
+// instantiates them: constant memory is 64 KB per module): the weighted
+// derivative E = B W D and the lift-projection BwG = B W G2GL (L rows each).
+template <int L, int Q, class T>
+static cudaError_t upload_tables2_lq(const Tables1D &t) {
+  std::vector<T> e2((size_t)L * Q), bwg((size_t)L * (Q - 1));
+  for (int a = 0; a < L; ++a) {
+    for (int j = 0; j < Q; ++j) {
+      double acc = 0.0;
+      for (int i = 0; i < Q; ++i) acc += t.B[(size_t)a * Q + i] * t.w[i] * t.D[(size_t)i * Q + j];
+      e2[(size_t)a * Q + j] = T(acc);
+    }
+    for (int g = 0; g < Q - 1; ++g) {
+      double acc = 0.0;
+      for (int i = 0; i < Q; ++i) acc += t.B[(size_t)a * Q + i] * t.w[i] * t.g2gl[(size_t)i * (Q - 1) + g];
+      bwg[(size_t)a * (Q - 1) + g] = T(acc);
+    }
+  }
+  cudaError_t e = cudaMemcpyToSymbol(cE2<T, L, Q>, e2.data(), sizeof(T) * e2.size());
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyToSymbol(cBwG<T, L, Q>, bwg.data(), sizeof(T) * bwg.size());
 }
 
 template <int PHYS, int L, int Q, int EPB, int MINB, bool MIXED = false>
@@ -246,6 +270,69 @@ struct PLaunch {
     return o;
   }
 };
+
+// The second-form stage kernel (stage2.cuh) for LSRK and right-hand-side
+// stages; other stage kinds, and every other kernel of the handle, come from
+// the plain tile of the same (L, Q).
+template <int PHYS, int L, int Q, int EPB, int NT, int MINB, bool MIXED = false>
+struct Launch2 {
+  using Base = Launch<PHYS, L, Q, default_epb(3, Q), 0, MIXED>;
+  using C = Cfg2<PHYS, L, Q, EPB, NT, MINB, MIXED>;
+  static cudaError_t init(const Tables1D &t) {
+    cudaError_t e = Base::init(t);
+    if (e != cudaSuccess) return e;
+    if ((e = upload_tables2_lq<L, Q, typename C::R>(t)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(stage2_kernel<C, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+  }
+  static int blocks_per_sm() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage2_kernel<C, PHYS>, NT, C::SMEM) != cudaSuccess) {
+      cudaGetLastError();
+      return 1;
+    }
+    return n > 0 ? n : 1;
+  }
+  static cudaError_t stage_grid(const StageArgs &a, int g, cudaStream_t s) {
+    if (a.kind != kLSRK && a.kind != kRHS) return Base::stage_grid(a, g, s);
+    stage2_kernel<C, PHYS><<<g, NT, C::SMEM, s>>>(a);
+    return cudaGetLastError();
+  }
+  static cudaError_t stage(const StageArgs &a, cudaStream_t s) {
+    if (a.kind != kLSRK && a.kind != kRHS) return Base::stage(a, s);
+    stage2_kernel<C, PHYS><<<(unsigned)((a.ne + EPB - 1) / EPB), NT, C::SMEM, s>>>(a);
+    return cudaGetLastError();
+  }
+  static KernelOps ops() {
+    KernelOps o = Base::ops();
+    o.epb = EPB; o.nt = NT; o.minb = MINB; o.smem = C::SMEM;
+    o.init = init; o.stage = stage; o.stage_grid = stage_grid; o.blocks_per_sm = blocks_per_sm;
+    o.warp = 3;
+    return o;
+  }
+};
+
+template <int PHYS, int P, int Q, int EPB, int NT, int MINB, bool MIXED>
+void reg2_variant() {
+  using C = Cfg2<PHYS, P + 1, Q, EPB, NT, MINB, MIXED>;
+  if constexpr (C::SMEM <= 227 * 1024 && (MINB == 0 || (65536 / (NT * MINB) >= 40 &&
+                                                        (int)((228 * 1024) / (C::SMEM + 1024)) >= MINB)))
+    register_ops(PHYS + (MIXED ? kMixedKey : 0), P + 1, Q, Launch2<PHYS, P + 1, Q, EPB, NT, MINB, MIXED>::ops());
+}
+
+// Second-form variants of a 3-D Euler (p, q): one element per CTA at two
+// thread counts, uncapped and with the register cap of the shared-memory
+// occupancy.
+template <int PHYS, int P, int Q, bool MIXED = false>
+void reg2() {
+  constexpr int NTA = ((P + 1) * (P + 1) * 5 + 31) / 32 * 32;   // one thread per modal row
+  constexpr int NTB = NTA + 32;
+  using CA = Cfg2<PHYS, P + 1, Q, 1, NTA, 0, MIXED>;
+  constexpr int BA = (int)((228 * 1024) / (CA::SMEM + 1024)) > 16 ? 16 : (int)((228 * 1024) / (CA::SMEM + 1024));
+  reg2_variant<PHYS, P, Q, 1, NTA, 0, MIXED>();
+  reg2_variant<PHYS, P, Q, 1, NTB, 0, MIXED>();
+  if constexpr (BA >= 2) reg2_variant<PHYS, P, Q, 1, NTA, BA, MIXED>();
+  if constexpr (BA >= 2) reg2_variant<PHYS, P, Q, 1, NTB, BA, MIXED>();
+}
 
 template <int PHYS, int P, int Q, int EPB, int MINB, bool MIXED>
 void reg_pipe() {

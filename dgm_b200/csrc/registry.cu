@@ -25,7 +25,12 @@ void register_ops(int physics, int L, int Q, const KernelOps &ops) {
 const KernelOps *find_ops(int physics, int L, int Q) {
   std::lock_guard<std::mutex> lk(table_mutex());
   auto it = table().find(std::make_tuple(physics, L, Q));
-  return it == table().end() || it->second.empty() ? nullptr : &it->second.front();
+  if (it == table().end() || it->second.empty()) return nullptr;
+  // the default is the first plain CTA tile (it handles every stage kind and
+  // boundary sides), whatever order the compilation units registered in
+  for (const KernelOps &o : it->second)
+    if (o.warp == 0) return &o;
+  return &it->second.front();
 }
 
 const std::vector<KernelOps> *find_variants(int physics, int L, int Q) {

@@ -1,0 +1,698 @@
+// Fused DG stage kernel, second form (3-D hexahedra, sm_100a), FP64 and the
+// mixed FP32 form.
+//
+// Same arithmetic contract as stage_tile (stage.cuh): one launch evaluates
+// Domain::time_derivative on the modal register, applies the LSRK stage
+// update (or stores the right-hand side) and writes the next stage's face
+// traces.  What differs is how the element's operators are ordered, so that
+// every 1-D contraction reads and writes shared memory once and the number
+// of passes (and barriers) per element is small:
+//
+//  * the projected volume term of the reference, forward(sum_r D_r G_r) with
+//    G_r the contravariant flux (src/Euler3d.cpp:506-566 differentiated by
+//    src/Hex.cpp:2030-2071 and projected by src/Hex.cpp:703-812), is one
+//    sum-factorised operator: along its own axis r the weighted derivative
+//    E = B W D (L x Q), along the other two the weighted basis P = B W, and
+//    the three directions share passes:
+//        R = P_k P_j (E_i G_0) + P_k E_j (P_i G_1) + E_k P_j (P_i G_2);
+//    the i-axis pass runs in registers right after the pointwise fluxes
+//    (one thread per (j, k) column and direction r);
+//  * the lift of a face (G2GL interpolation, 1/w_end and the projection,
+//    src/Hex.cpp:1768-1952) is the 2-D projection BwG x BwG of the face
+//    term times the end value of the normal-axis basis, BwG = B W G2GL, and
+//    is added to the projected right-hand side in the last pass;
+//  * the update writes each modal row from registers and the next traces
+//    (modal -> face Gauss points, src/Hex.cpp:933-947) start from the same
+//    registers (end reduction along the contiguous axis).
+// Every (L, Q) works; the element's shared-memory regions are laid out by
+// lifetime (offsets below) with odd pitches on the rows that a warp reads
+// along, so pencils fall on distinct banks.
+//
+// Scope: Euler 3-D, no boundary sides, LSRK and right-hand-side stages (the
+// other stage kinds run the plain kernel of the same (L, Q)).
+#pragma once
+
+#include "stage.cuh"
+
+namespace dgmx {
+
+// Tables of the second form (constant memory, per working type and (L, Q)).
+template <class T, int L, int Q> __constant__ T cE2[L * Q];          // E[a][j] = sum_i B[a][i] w_i D[i][j]
+template <class T, int L, int Q> __constant__ T cBwG[L * (Q - 1)];   // BwG[a][g] = sum_i B[a][i] w_i G2GL[i][g]
+
+template <int PHYS, int L_, int Q_, int EPB_, int NT_, int MINB_, bool MIXED_>
+struct Cfg2 {
+  static constexpr bool MIXED = MIXED_;
+  static constexpr int PHYSICS = PHYS;
+  using R = std::conditional_t<MIXED_, float, double>;
+  static constexpr int NF = phys_nf(PHYS), L = L_, Q = Q_, G = Q_ - 1, EPB = EPB_, NT = NT_;
+  static constexpr int MINB = MINB_ > 0 ? MINB_ : 1, MINB_REQ = MINB_;
+  static constexpr int NFACE = 6, GF = G * G, LD = L * L * L, QD = Q * Q * Q;
+  // odd pitches for rows of an even length
+  static constexpr int PL = L % 2 == 0 ? L + 1 : L;   // modal rows (and face-plane rows of L)
+  static constexpr int PG = G % 2 == 0 ? G + 1 : G;   // face-trace rows of G
+  // region sizes (values of R)
+  static constexpr int S_UA = NF * L * L * PL;          // modal block, padded rows
+  static constexpr int S_TR = NFACE * NF * G * PG;      // own traces / face terms, padded rows
+  static constexpr int S_TN = NFACE * NF * GF;          // neighbour traces (neighbour's order)
+  static constexpr int S_Z1 = NFACE * NF * G * PL;      // lift pass 1: [f][n][g][b'] padded
+  static constexpr int S_XL = NFACE * NF * L * PL;      // lifted-projected face terms [f][n][a'][b'] padded
+  static constexpr int S_T1 = NF * L * L * Q;           // [n][a][b][k]
+  static constexpr int S_T2 = NF * L * Q * Q;           // [n][a][j][k]
+  static constexpr int S_UN = NF * Q * Q * Q;           // nodal values [n][i][j][k]
+  static constexpr int S_X1 = NF * L * Q * Q;           // one of X0, X1, X2: [n][a][j][k]
+  static constexpr int S_X = 3 * S_X1 + 2;              // (+1 between arrays: they start on different banks)
+  static constexpr int S_Y1 = NF * L * L * Q;           // Y0 or Y2: [n][a][b][k]
+  static constexpr int S_Y = 2 * S_Y1 + 1;
+  static constexpr int S_UB = NF * L * L * PL;          // updated modal block, padded rows
+  static constexpr int S_FP = NFACE * NF * L * L;       // end-reduced face planes [f][n][a'][b']
+  static constexpr int S_W1 = NFACE * NF * G * PL;      // trace pass 1 [f][n][g][b'] padded
+  // lifetimes (phases): UA 0-3, TR 0-2a, TN 0-1, Z1 2a-2b, XL 2b-8, T1 3-4,
+  // T2 4-5, UN 5-6, X 6-7, Y 7-8, UB 8-9, FP 8-10a, W1 10a-10b.
+  // Region A (from 0): UA | TR | TN (phases 0-2), then UN (5-6), then Y (7-8)
+  static constexpr int O_UA = 0, O_TR = O_UA + S_UA, O_TN = O_TR + S_TR;
+  static constexpr int O_Z1 = O_TN;                     // TN is dead after the face fluxes
+  static constexpr int O_T1 = O_TR;                     // TR is dead after lift pass 1
+  static constexpr int O_UN = 0;                        // UA, T1 dead by phase 5 (T2 lives elsewhere)
+  static constexpr int O_Y = 0;                         // UN dead after phase 6
+  static constexpr int A_END = cmax(cmax(O_TN + cmax(S_TN, S_Z1), O_T1 + S_T1), cmax(O_UN + S_UN, O_Y + S_Y));
+  // Region B: X (6-7); T2 (4-5) inside it; UB, FP, W1 (8-10) inside it
+  static constexpr int O_X = A_END;
+  static constexpr int O_T2 = O_X + S_X - S_T2;         // the tail of X: phase 5 reads it before X is written
+  static constexpr int O_UB = O_X, O_FP = O_UB + S_UB, O_W1 = O_FP + S_FP;
+  static constexpr int B_END = cmax(O_X + S_X, O_W1 + S_W1);
+  static_assert(O_T2 >= A_END, "T2 must not overlap region A");
+  static_assert(O_T1 + S_T1 <= O_Z1, "T1 (phase 3) must not overlap Z1 (read in phase 2b, the same interval)");
+  // XL after both (alive from phase 2 to phase 8)
+  static constexpr int O_XL = B_END;
+  static constexpr int SZ_SLOT = O_XL + S_XL;
+  static constexpr size_t DATA = ((size_t)EPB * SZ_SLOT * sizeof(R) + 15) / 16 * 16;
+  static constexpr size_t SMEM = DATA + (size_t)EPB * (NFACE * sizeof(FaceLink) + 16 + (MIXED_ ? sizeof(RefState<R>) : 0));
+};
+
+template <class C>
+struct Smem2 {
+  using T = typename C::R;
+  T *base;
+  FaceLink *lnk;
+  int *eid, *cls;
+  RefState<T> *ref;
+  __device__ Smem2(unsigned char *raw) {
+    base = reinterpret_cast<T *>(raw);
+    lnk = reinterpret_cast<FaceLink *>(raw + C::DATA);
+    eid = reinterpret_cast<int *>(lnk + C::EPB * C::NFACE);
+    cls = eid + C::EPB;
+    ref = reinterpret_cast<RefState<T> *>(reinterpret_cast<unsigned char *>(eid) + 16 * C::EPB);
+  }
+  __device__ T *slot(int s) const { return base + (size_t)s * C::SZ_SLOT; }
+};
+
+// ---- phase 0: inputs -------------------------------------------------------
+template <class C>
+__device__ __forceinline__ void s2_load(const Smem2<C> &sm, const StageArgs &a, int e0, int tid) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, L = C::L, G = C::G, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB, PL = C::PL,
+                PG = C::PG;
+  // links and class
+  for (int w = tid; w < EPB * NFACE; w += C::NT) {
+    const int s = w / NFACE, f = w - s * NFACE, e = e0 + s;
+    const FaceLink lk = e < a.ne ? a.links[(size_t)e * NFACE + f] : FaceLink{0, 0, 0, -1};
+    sm.lnk[w] = lk;
+    if (f == 0) {
+      const int gc = e < a.ne ? a.gclass[e] : -1;
+      sm.cls[s] = gc >= 0 ? gc : 0;
+      sm.eid[s] = gc >= 0 ? e : -1;
+      if constexpr (C::MIXED)
+        sm.ref[s] = *reinterpret_cast<const RefState<float> *>(a.uref + kUrefStride * solve_of(a, gc >= 0 ? e : -1) + 10);
+    }
+  }
+  // modal register rows (perturbation about the reference in the mixed form)
+  constexpr int RPS = NF * L * L;
+  for (int r = tid; r < EPB * RPS; r += C::NT) {
+    const int s = r / RPS, rr = r - s * RPS, e = e0 + s;
+    double v[L];
+    if (e < a.ne) {
+      ld_row<L>(a.X + ((size_t)e * RPS + rr) * L, v);
+      if constexpr (C::MIXED)
+        if (rr % (L * L) == 0) v[0] -= a.uref[kUrefStride * solve_of(a, e) + 5 + rr / (L * L)];
+    } else {
+#pragma unroll
+      for (int k = 0; k < L; ++k) v[k] = (!C::MIXED && k == 0 && rr % (L * L) == 0) ? 1.0 : 0.0;
+    }
+    T *dst = sm.slot(s) + C::O_UA + rr * PL;
+#pragma unroll
+    for (int k = 0; k < L; ++k) dst[k] = T(v[k]);
+  }
+  // own traces, rows of G into padded rows
+  const T *Tin = trace_in<C>(a);
+  constexpr int TPS = NFACE * NF * G;
+  for (int r = tid; r < EPB * TPS; r += C::NT) {
+    const int s = r / TPS, rr = r - s * TPS, e = e0 + s;
+    T v[G];
+    if (e < a.ne) {
+      ld_row<G>(Tin + (size_t)e * NFACE * NF * GF + rr * G, v);
+    } else {
+#pragma unroll
+      for (int k = 0; k < G; ++k) v[k] = T((!C::MIXED && (rr / G) % NF == 0) ? 1.0 : 0.0);
+    }
+    T *dst = sm.slot(s) + C::O_TR + rr * PG;
+#pragma unroll
+    for (int k = 0; k < G; ++k) dst[k] = v[k];
+  }
+  // neighbour face blocks (their own point order), rows of G
+  for (int r = tid; r < EPB * TPS; r += C::NT) {
+    const int s = r / TPS, rr = r - s * TPS, f = rr / (NF * G), q = rr - f * NF * G, e = e0 + s;
+    T v[G];
+    if (e < a.ne) {
+      const FaceLink lk = a.links[(size_t)e * NFACE + f];
+      ld_row<G>(Tin + ((size_t)lk.elem * NFACE + lk.face) * NF * GF + q * G, v);
+    } else {
+#pragma unroll
+      for (int k = 0; k < G; ++k) v[k] = T((!C::MIXED && q / G == 0) ? 1.0 : 0.0);
+    }
+    T *dst = sm.slot(s) + C::O_TN + rr * G;
+#pragma unroll
+    for (int k = 0; k < G; ++k) dst[k] = v[k];
+  }
+}
+
+// ---- phase 1: numerical flux at every face point -----------------------------
+// E = (F^ - F(U_own)).n J_side/J_el in the layout of the own traces, as
+// face_fluxes (stage.cuh) computes it.
+template <class C, int PHYS>
+__device__ __forceinline__ void s2_face_flux(const Smem2<C> &sm, const StageArgs &a, int tid) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, G = C::G, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB, PG = C::PG;
+  for (int w = tid; w < EPB * NFACE * GF; w += C::NT) {
+    const int s = w / (NFACE * GF), rem = w - s * NFACE * GF, f = rem / GF, g = rem - f * GF;
+    const int e = sm.eid[s];
+    if (e < 0) continue;
+    const FaceLink lk = sm.lnk[s * NFACE + f];
+    const GeomClass *gc = a.classes + sm.cls[s];
+    const int gn = __ldg(a.perm + lk.perm + g);
+    T *eo = sm.slot(s) + C::O_TR + (f * NF) * G * PG + (g / G) * PG + g % G;
+    const T *tn = sm.slot(s) + C::O_TN + (f * NF) * GF + gn;
+    T Uo[5], Un[5], Fh[5], FL[5], FR[5];
+#pragma unroll
+    for (int n = 0; n < NF; ++n) { Uo[n] = eo[n * G * PG]; Un[n] = tn[n * GF]; }
+    const T nm[3] = {T(__ldg(&gc->nrm[f][0])), T(__ldg(&gc->nrm[f][1])), T(__ldg(&gc->nrm[f][2]))};
+    const int mbits = __ldg(&gc->master);
+    const bool master = (mbits >> f) & 1;
+    const T jr = T(__ldg(&gc->jr[f]));
+    const double *fr = gc->fr[f];
+    bool ok;
+    if constexpr (C::MIXED) {
+      if (master) ok = face_flux_pert<PHYS, T>(sm.ref[s], Uo, Un, nm, T(a.gamma), a.flux, Fh, FR, fr);
+      else ok = face_flux_pert<PHYS, T>(sm.ref[s], Un, Uo, nm, T(a.gamma), a.flux, Fh, FR, fr);
+#pragma unroll
+      for (int n = 0; n < NF; ++n) eo[n * G * PG] = master ? Fh[n] * jr : (FR[n] - Fh[n]) * jr;
+    } else {
+      if (master) ok = face_flux<PHYS, T>(Uo, Un, nm, T(a.gamma), a.flux, Fh, FL, FR, fr);
+      else ok = face_flux<PHYS, T>(Un, Uo, nm, T(a.gamma), a.flux, Fh, FL, FR, fr);
+#pragma unroll
+      for (int n = 0; n < NF; ++n) eo[n * G * PG] = master ? (Fh[n] - FL[n]) * jr : (FR[n] - Fh[n]) * jr;
+    }
+    if (!ok) {
+      atomicOr(a.err, 1);
+      atomicMin(a.err + 1, e);
+    }
+  }
+}
+
+// ---- phase 2: lift and projection of the face terms --------------------------
+// pass a: Z1[f][n][g][b'] = sum_h BwG[b'][h] E[f][n][g][h]
+template <class C>
+__device__ __forceinline__ void s2_lift_a(const Smem2<C> &sm, int tid) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, L = C::L, Q = C::Q, G = C::G, NFACE = C::NFACE, EPB = C::EPB, PG = C::PG, PL = C::PL;
+  constexpr int N = NFACE * NF * G;
+  for (int w = tid; w < EPB * N; w += C::NT) {
+    const int s = w / N, r = w - s * N;   // r = (f*NF + n)*G + g
+    const T *src = sm.slot(s) + C::O_TR + r * PG;
+    T v[G];
+#pragma unroll
+    for (int h = 0; h < G; ++h) v[h] = src[h];
+    T *dst = sm.slot(s) + C::O_Z1 + r * PL;
+#pragma unroll
+    for (int b = 0; b < L; ++b) {
+      T acc = T(0);
+#pragma unroll
+      for (int h = 0; h < G; ++h) acc = fma(cBwG<T, L, Q>[b * G + h], v[h], acc);
+      dst[b] = acc;
+    }
+  }
+}
+// pass b: XL[f][n][a'][b'] = sum_g BwG[a'][g] Z1[f][n][g][b']
+template <class C>
+__device__ __forceinline__ void s2_lift_b(const Smem2<C> &sm, int tid) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, L = C::L, Q = C::Q, G = C::G, NFACE = C::NFACE, EPB = C::EPB, PL = C::PL;
+  constexpr int N = NFACE * NF * L;
+  for (int w = tid; w < EPB * N; w += C::NT) {
+    const int s = w / N, r = w - s * N, fn = r / L, b = r - fn * L;
+    const T *src = sm.slot(s) + C::O_Z1 + fn * G * PL + b;
+    T v[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) v[g] = src[g * PL];
+    T *dst = sm.slot(s) + C::O_XL + fn * L * PL + b;
+#pragma unroll
+    for (int a = 0; a < L; ++a) {
+      T acc = T(0);
+#pragma unroll
+      for (int g = 0; g < G; ++g) acc = fma(cBwG<T, L, Q>[a * G + g], v[g], acc);
+      dst[a * PL] = acc;
+    }
+  }
+}
+
+// ---- phases 3-5: modal -> GLL values ----------------------------------------
+template <class C>
+__device__ __forceinline__ void s2_backward_k(const Smem2<C> &sm, int tid) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, L = C::L, Q = C::Q, EPB = C::EPB, PL = C::PL;
+  constexpr int N = NF * L * L;
+  for (int w = tid; w < EPB * N; w += C::NT) {
+    const int s = w / N, r = w - s * N;   // r = (n*L + a)*L + b
+    const T *src = sm.slot(s) + C::O_UA + r * PL;
+    T v[L];
+#pragma unroll
+    for (int c = 0; c < L; ++c) v[c] = src[c];
+    T *dst = sm.slot(s) + C::O_T1 + r * Q;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+      T acc = T(0);
+#pragma unroll
+      for (int c = 0; c < L; ++c) acc = fma(cB<T, L, Q>[c * Q + k], v[c], acc);
+      dst[k] = acc;
+    }
+  }
+}
+template <class C>
+__device__ __forceinline__ void s2_backward_j(const Smem2<C> &sm, int tid) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, L = C::L, Q = C::Q, EPB = C::EPB;
+  constexpr int N = NF * L * Q;
+  for (int w = tid; w < EPB * N; w += C::NT) {
+    const int s = w / N, r = w - s * N, na = r / Q, k = r - na * Q;   // na = n*L + a
+    const T *src = sm.slot(s) + C::O_T1 + na * L * Q + k;
+    T v[L];
+#pragma unroll
+    for (int b = 0; b < L; ++b) v[b] = src[b * Q];
+    T *dst = sm.slot(s) + C::O_T2 + na * Q * Q + k;
+#pragma unroll
+    for (int j = 0; j < Q; ++j) {
+      T acc = T(0);
+#pragma unroll
+      for (int b = 0; b < L; ++b) acc = fma(cB<T, L, Q>[b * Q + j], v[b], acc);
+      dst[j * Q] = acc;
+    }
+  }
+}
+template <class C>
+__device__ __forceinline__ void s2_backward_i(const Smem2<C> &sm, int tid) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, L = C::L, Q = C::Q, EPB = C::EPB;
+  constexpr int N = NF * Q * Q;
+  for (int w = tid; w < EPB * N; w += C::NT) {
+    const int s = w / N, r = w - s * N, n = r / (Q * Q), jk = r - n * Q * Q;
+    const T *src = sm.slot(s) + C::O_T2 + n * L * Q * Q + jk;
+    T v[L];
+#pragma unroll
+    for (int a = 0; a < L; ++a) v[a] = src[a * Q * Q];
+    T *dst = sm.slot(s) + C::O_UN + n * Q * Q * Q + jk;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      T acc = T(0);
+#pragma unroll
+      for (int a = 0; a < L; ++a) acc = fma(cB<T, L, Q>[a * Q + i], v[a], acc);
+      dst[i * Q * Q] = acc;
+    }
+  }
+}
+
+// ---- phase 6: contravariant fluxes and the i-axis pass ----------------------
+// Column (j, k), direction r: G_r = sum_d metric[r][d] F_d(U) at the Q points
+// of the column, then X_r[n][a] = sum_i C_r[a][i] G_r[n][i] with C_0 = E (the
+// derivative along i) and C_1 = C_2 = B W.  With the contravariant velocity
+// V_r = metric[r] . u:  G_r[rho] = rho V_r, G_r[m_d] = m_d V_r + p metric[r][d],
+// G_r[E] = (E + p) V_r.  The mixed form evaluates F(Ub + u') - F(Ub)
+// (volume_flux_pert, kernels.cuh) the same way.
+template <class C, int PHYS>
+__device__ __forceinline__ void s2_volume(const Smem2<C> &sm, const StageArgs &a, int tid) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, L = C::L, Q = C::Q, EPB = C::EPB;
+  constexpr int N = 3 * Q * Q;
+  const T gm1 = T(a.gamma) - T(1.0);
+  for (int w = tid; w < EPB * N; w += C::NT) {
+    const int s = w / N, rem = w - s * N, r = rem / (Q * Q), jk = rem - r * Q * Q;
+    const GeomClass *gc = a.classes + sm.cls[s];
+    const T m0 = T(__ldg(&gc->metric[3 * r + 0])), m1 = T(__ldg(&gc->metric[3 * r + 1])),
+            m2 = T(__ldg(&gc->metric[3 * r + 2]));
+    const T *un = sm.slot(s) + C::O_UN + jk;
+    T acc[5][L];
+#pragma unroll
+    for (int n = 0; n < NF; ++n)
+#pragma unroll
+      for (int b = 0; b < L; ++b) acc[n][b] = T(0);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      T U[5], Gr[5];
+#pragma unroll
+      for (int n = 0; n < NF; ++n) U[n] = un[(n * Q + i) * Q * Q];
+      if constexpr (C::MIXED) {
+        const RefState<T> &b = sm.ref[s];
+        const T rho = b.r + U[0], ir = p_rcp(rho);
+        const T mx = b.m[0] + U[1], my = b.m[1] + U[2], mz = b.m[2] + U[3];
+        const T upx = (U[1] - b.u[0] * U[0]) * ir, upy = (U[2] - b.u[1] * U[0]) * ir, upz = (U[3] - b.u[2] * U[0]) * ir;
+        T sdot = T(0);
+        sdot = fma(U[1], b.u[0], sdot); sdot = fma(mx, upx, sdot);
+        sdot = fma(U[2], b.u[1], sdot); sdot = fma(my, upy, sdot);
+        sdot = fma(U[3], b.u[2], sdot); sdot = fma(mz, upz, sdot);
+        const T pp = gm1 * fma(T(-0.5), sdot, U[4]);
+        const T Hp = U[4] + pp, H = b.H + Hp;
+        const T Vb = m0 * b.u[0] + m1 * b.u[1] + m2 * b.u[2];       // reference contravariant velocity
+        const T Vp = m0 * upx + m1 * upy + m2 * upz;                 // its perturbation
+        Gr[0] = m0 * U[1] + m1 * U[2] + m2 * U[3];
+        Gr[1] = fma(U[1], Vb, fma(mx, Vp, pp * m0));
+        Gr[2] = fma(U[2], Vb, fma(my, Vp, pp * m1));
+        Gr[3] = fma(U[3], Vb, fma(mz, Vp, pp * m2));
+        Gr[4] = fma(Hp, Vb, H * Vp);
+      } else {
+        const T ir = T(1.0) / U[0];
+        const T u = U[1] * ir, v = U[2] * ir, ww = U[3] * ir;
+        T p = u * U[1];
+        p = fma(v, U[2], p);
+        p = fma(ww, U[3], p);
+        p = T(-0.5) * gm1 * p;
+        p = fma(gm1, U[4], p);
+        const T V = fma(m2, ww, fma(m1, v, m0 * u));
+        Gr[0] = U[0] * V;
+        Gr[1] = fma(U[1], V, p * m0);
+        Gr[2] = fma(U[2], V, p * m1);
+        Gr[3] = fma(U[3], V, p * m2);
+        Gr[4] = (U[4] + p) * V;
+      }
+      if (r == 0) {
+#pragma unroll
+        for (int n = 0; n < NF; ++n)
+#pragma unroll
+          for (int b = 0; b < L; ++b) acc[n][b] = fma(cE2<T, L, Q>[b * Q + i], Gr[n], acc[n][b]);
+      } else {
+#pragma unroll
+        for (int n = 0; n < NF; ++n)
+#pragma unroll
+          for (int b = 0; b < L; ++b) acc[n][b] = fma(cBw<T, L, Q>[b * Q + i], Gr[n], acc[n][b]);
+      }
+    }
+    T *dst = sm.slot(s) + C::O_X + r * (C::S_X1 + 1) + jk;
+#pragma unroll
+    for (int n = 0; n < NF; ++n)
+#pragma unroll
+      for (int b = 0; b < L; ++b) dst[(n * L + b) * Q * Q] = acc[n][b];
+  }
+}
+
+// ---- phase 7: j-axis pass -------------------------------------------------------
+// Y0 = P_j X0 + E_j X1, Y2 = P_j X2   ([n][a][b][k])
+template <class C>
+__device__ __forceinline__ void s2_pass_j(const Smem2<C> &sm, int tid) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, L = C::L, Q = C::Q, EPB = C::EPB;
+  constexpr int N = NF * L * Q;
+  for (int w = tid; w < EPB * N; w += C::NT) {
+    const int s = w / N, r = w - s * N, na = r / Q, k = r - na * Q;
+    const T *x = sm.slot(s) + C::O_X + na * Q * Q + k;
+    T x0[Q], x1[Q], x2[Q];
+#pragma unroll
+    for (int j = 0; j < Q; ++j) {
+      x0[j] = x[j * Q];
+      x1[j] = x[(C::S_X1 + 1) + j * Q];
+      x2[j] = x[2 * (C::S_X1 + 1) + j * Q];
+    }
+    T *y = sm.slot(s) + C::O_Y + na * L * Q + k;
+#pragma unroll
+    for (int b = 0; b < L; ++b) {
+      T y0 = T(0), y2 = T(0);
+#pragma unroll
+      for (int j = 0; j < Q; ++j) {
+        y0 = fma(cBw<T, L, Q>[b * Q + j], x0[j], y0);
+        y0 = fma(cE2<T, L, Q>[b * Q + j], x1[j], y0);
+        y2 = fma(cBw<T, L, Q>[b * Q + j], x2[j], y2);
+      }
+      y[b * Q] = y0;
+      y[(C::S_Y1 + 1) + b * Q] = y2;
+    }
+  }
+}
+
+// ---- phase 8: k-axis pass, face terms, update, next modal block ------------
+template <class C, int PHYS>
+__device__ __forceinline__ void s2_update(const Smem2<C> &sm, const StageArgs &a, int tid) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, L = C::L, Q = C::Q, EPB = C::EPB, PL = C::PL;
+  constexpr int N = NF * L * L;
+  for (int w = tid; w < EPB * N; w += C::NT) {
+    const int s = w / N, r = w - s * N, n = r / (L * L), ab = r - n * L * L, aa = ab / L, bb = ab - aa * L;
+    const int e = sm.eid[s];
+    T *sl = sm.slot(s);
+    // R[c] = sum_k P[c][k] Y0[k] + E[c][k] Y2[k]
+    const T *y = sl + C::O_Y + r * Q;
+    T y0[Q], y2[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) { y0[k] = y[k]; y2[k] = y[(C::S_Y1 + 1) + k]; }
+    // face terms: k faces (0: k=0, 5: k=Q-1) plane (a, b); j faces (1: j=0,
+    // 3: j=Q-1) plane (a, c); i faces (4: i=0, 2: i=Q-1) plane (b, c)
+    const T *xl = sl + C::O_XL;
+    constexpr int FB = NF * L * PL;   // one face's block
+    const T xk0 = xl[0 * FB + (n * L + aa) * PL + bb], xk1 = xl[5 * FB + (n * L + aa) * PL + bb];
+    const T *xj0 = xl + 1 * FB + (n * L + aa) * PL, *xj1 = xl + 3 * FB + (n * L + aa) * PL;
+    const T *xi0 = xl + 4 * FB + (n * L + bb) * PL, *xi1 = xl + 2 * FB + (n * L + bb) * PL;
+    const T eb0 = cEnd<T, L, Q>[bb], eb1 = cEnd<T, L, Q>[L + bb];
+    const T ea0 = cEnd<T, L, Q>[aa], ea1 = cEnd<T, L, Q>[L + aa];
+    T R[L];
+#pragma unroll
+    for (int c = 0; c < L; ++c) {
+      T acc = T(0);
+#pragma unroll
+      for (int k = 0; k < Q; ++k) {
+        acc = fma(cBw<T, L, Q>[c * Q + k], y0[k], acc);
+        acc = fma(cE2<T, L, Q>[c * Q + k], y2[k], acc);
+      }
+      acc = fma(cEnd<T, L, Q>[c], xk0, acc);
+      acc = fma(cEnd<T, L, Q>[L + c], xk1, acc);
+      acc = fma(eb0, xj0[c], acc);
+      acc = fma(eb1, xj1[c], acc);
+      acc = fma(ea0, xi0[c], acc);
+      acc = fma(ea1, xi1[c], acc);
+      R[c] = acc;
+    }
+    // The state the right-hand side was evaluated on (X; X = U for LSRK)
+    // is read back from global memory: its shared copy is dead by now.
+    T *ub = sl + C::O_UB + r * PL;
+    if (e < 0) {
+#pragma unroll
+      for (int c = 0; c < L; ++c) ub[c] = T(0);
+    } else {
+      const size_t gi = ((size_t)e * N + r) * L;
+      const double dt = a.dts ? a.dts[solve_of(a, e)] : a.dt;
+      double x[L];
+      ld_row<L>(a.X + gi, x);
+      if constexpr (C::MIXED) {
+        const double ref0 = ab == 0 ? a.uref[kUrefStride * solve_of(a, e) + 5 + n] : 0.0;
+        float q[L];
+#pragma unroll
+        for (int c = 0; c < L; ++c) q[c] = R[c];
+        if (a.Ssrc)
+#pragma unroll
+          for (int c = 0; c < L; ++c) q[c] -= float(a.src_scale * a.Ssrc[gi + c]);
+        if (a.Rsub)
+#pragma unroll
+          for (int c = 0; c < L; ++c) q[c] -= float(a.Rsub[gi + c]);
+        if (a.kind == kRHS) {
+#pragma unroll
+          for (int c = 0; c < L; ++c) { a.A[gi + c] = q[c]; ub[c] = float(c == 0 ? x[c] - ref0 : x[c]); }
+        } else {
+          float ut[L];
+          double u[L];
+          ld_row<L>(a.Utf + gi, ut);
+          const float c0 = float(a.c0), mdt = -float(dt);
+#pragma unroll
+          for (int c = 0; c < L; ++c) {
+            ut[c] = fmaf(mdt, q[c], c0 * ut[c]);
+            u[c] = fma(a.c1, double(ut[c]), x[c]);
+          }
+          st_row<L>(a.Utf + gi, ut);
+          st_row<L>(a.U + gi, u);
+#pragma unroll
+          for (int c = 0; c < L; ++c) ub[c] = float(c == 0 ? u[c] - ref0 : u[c]);
+        }
+      } else {
+        double q[L];
+#pragma unroll
+        for (int c = 0; c < L; ++c) q[c] = R[c];
+        if (a.Ssrc)
+#pragma unroll
+          for (int c = 0; c < L; ++c) q[c] -= a.src_scale * a.Ssrc[gi + c];
+        if (a.Rcap)
+#pragma unroll
+          for (int c = 0; c < L; ++c) a.Rcap[gi + c] = q[c];
+        if (a.Rsub)
+#pragma unroll
+          for (int c = 0; c < L; ++c) q[c] -= a.Rsub[gi + c];
+        if (a.kind == kRHS) {
+#pragma unroll
+          for (int c = 0; c < L; ++c) { a.A[gi + c] = q[c]; ub[c] = x[c]; }
+        } else {
+          double ut[L], u[L];
+          ld_row<L>(a.Ut + gi, ut);
+#pragma unroll
+          for (int c = 0; c < L; ++c) {
+            ut[c] = fma(-dt, q[c], a.c0 * ut[c]);
+            u[c] = fma(a.c1, ut[c], x[c]);
+            ub[c] = u[c];
+          }
+          st_row<L>(a.Ut + gi, ut);
+          st_row<L>(a.U + gi, u);
+        }
+      }
+    }
+    // end values along c of the next modal block: faces 0 (k=0) and 5 (k=Q-1)
+    T f0 = T(0), f5 = T(0);
+#pragma unroll
+    for (int c = 0; c < L; ++c) {
+      const T xv = ub[c];
+      f0 = fma(cEnd<T, L, Q>[c], xv, f0);
+      f5 = fma(cEnd<T, L, Q>[L + c], xv, f5);
+    }
+    T *fp = sl + C::O_FP;
+    constexpr int PB = NF * L * L;   // one face plane block
+    fp[0 * PB + r] = f0;
+    fp[5 * PB + r] = f5;
+  }
+}
+
+// ---- phase 9: end values along b (faces 1, 3) and a (faces 4, 2) ------------
+template <class C>
+__device__ __forceinline__ void s2_ends_ab(const Smem2<C> &sm, int tid) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, L = C::L, Q = C::Q, EPB = C::EPB, PL = C::PL;
+  constexpr int N = NF * L * L, PB = NF * L * L;
+  for (int w = tid; w < EPB * 2 * N; w += C::NT) {
+    const int s = w / (2 * N), rem = w - s * 2 * N, ax = rem / N, r = rem - ax * N;
+    const int n = r / (L * L), xy = r - n * L * L, x = xy / L, y = xy - x * L;
+    const T *ub = sm.slot(s) + C::O_UB + n * L * L * PL;
+    T lo = T(0), hi = T(0);
+    T *fp = sm.slot(s) + C::O_FP;
+    if (ax == 0) {   // along b at (a = x, c = y): faces 1 (j=0) and 3 (j=Q-1), plane (a, c)
+#pragma unroll
+      for (int b = 0; b < L; ++b) {
+        const T v = ub[(x * L + b) * PL + y];
+        lo = fma(cEnd<T, L, Q>[b], v, lo);
+        hi = fma(cEnd<T, L, Q>[L + b], v, hi);
+      }
+      fp[1 * PB + r] = lo;
+      fp[3 * PB + r] = hi;
+    } else {         // along a at (b = x, c = y): faces 4 (i=0) and 2 (i=Q-1), plane (b, c)
+#pragma unroll
+      for (int aa = 0; aa < L; ++aa) {
+        const T v = ub[(aa * L + x) * PL + y];
+        lo = fma(cEnd<T, L, Q>[aa], v, lo);
+        hi = fma(cEnd<T, L, Q>[L + aa], v, hi);
+      }
+      fp[4 * PB + r] = lo;
+      fp[2 * PB + r] = hi;
+    }
+  }
+}
+
+// ---- phase 10: face planes -> Gauss points, stored as the next traces -------
+// pass a: W1[f][n][g][b'] = sum_a' Bg[a'][g] FP[f][n][a'][b']
+template <class C>
+__device__ __forceinline__ void s2_traces_a(const Smem2<C> &sm, int tid) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, L = C::L, Q = C::Q, G = C::G, NFACE = C::NFACE, EPB = C::EPB, PL = C::PL;
+  constexpr int N = NFACE * NF * L;
+  for (int w = tid; w < EPB * N; w += C::NT) {
+    const int s = w / N, r = w - s * N, fn = r / L, b = r - fn * L;
+    const T *src = sm.slot(s) + C::O_FP + fn * L * L + b;
+    T v[L];
+#pragma unroll
+    for (int aa = 0; aa < L; ++aa) v[aa] = src[aa * L];
+    T *dst = sm.slot(s) + C::O_W1 + fn * G * PL + b;
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      T acc = T(0);
+#pragma unroll
+      for (int aa = 0; aa < L; ++aa) acc = fma(cBg<T, L, Q>[aa * G + g], v[aa], acc);
+      dst[g * PL] = acc;
+    }
+  }
+}
+// pass b: trace[f][n][g][h] = sum_b' Bg[b'][h] W1[f][n][g][b'], a row of G
+// per thread straight to global memory
+template <class C, class TT>
+__device__ __forceinline__ void s2_traces_b(const Smem2<C> &sm, TT *Tout, int e0, int ne, int tid) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, L = C::L, Q = C::Q, G = C::G, NFACE = C::NFACE, EPB = C::EPB, PL = C::PL, GF = C::GF;
+  constexpr int N = NFACE * NF * G;
+  for (int w = tid; w < EPB * N; w += C::NT) {
+    const int s = w / N, r = w - s * N, e = e0 + s;   // r = (f*NF + n)*G + g
+    if (e >= ne) continue;
+    const T *src = sm.slot(s) + C::O_W1 + r * PL;
+    T v[L];
+#pragma unroll
+    for (int b = 0; b < L; ++b) v[b] = src[b];
+    TT out[G];
+#pragma unroll
+    for (int h = 0; h < G; ++h) {
+      T acc = T(0);
+#pragma unroll
+      for (int b = 0; b < L; ++b) acc = fma(cBg<T, L, Q>[b * G + h], v[b], acc);
+      out[h] = TT(acc);
+    }
+    st_row<G>(Tout + (size_t)e * NFACE * NF * GF + r * G, out);
+  }
+}
+
+template <class C, int PHYS>
+__device__ __forceinline__ void stage2_tile(const Smem2<C> &sm, const StageArgs &a, int e0, int tid) {
+  s2_load<C>(sm, a, e0, tid);
+  __syncthreads();
+  s2_face_flux<C, PHYS>(sm, a, tid);
+  __syncthreads();
+  s2_lift_a<C>(sm, tid);
+  __syncthreads();
+  s2_lift_b<C>(sm, tid);
+  s2_backward_k<C>(sm, tid);
+  __syncthreads();
+  s2_backward_j<C>(sm, tid);
+  __syncthreads();
+  s2_backward_i<C>(sm, tid);
+  __syncthreads();
+  s2_volume<C, PHYS>(sm, a, tid);
+  __syncthreads();
+  s2_pass_j<C>(sm, tid);
+  __syncthreads();
+  s2_update<C, PHYS>(sm, a, tid);
+  __syncthreads();
+  s2_ends_ab<C>(sm, tid);
+  __syncthreads();
+  s2_traces_a<C>(sm, tid);
+  __syncthreads();
+  s2_traces_b<C>(sm, trace_out<C>(a), e0, a.ne, tid);
+}
+
+// One tile (EPB elements) per CTA, or with a tile list a persistent loop over
+// the listed tiles (element pools).
+template <class C, int PHYS>
+__global__ void __launch_bounds__(C::NT, C::MINB) stage2_kernel(StageArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem2<C> sm(smem_raw);
+  const int ntile = a.tiles ? *a.ntiles : (int)gridDim.x;
+  for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
+    if (t != (int)blockIdx.x) __syncthreads();
+    stage2_tile<C, PHYS>(sm, a, (a.tiles ? a.tiles[t] : t) * C::EPB, threadIdx.x);
+  }
+}
+
+}  // namespace dgmx

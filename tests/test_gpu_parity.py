@@ -242,6 +242,12 @@ VARIANT_CASES = [
     # physics, dim, n, lo, hi, p, flux, inttype, ic, dt, steps, precision
     ("euler3d-roe-p3", 8, 3, (3, 2, 3), 0, 2 * np.pi, 3, "roe", 14, TG, 0.002, 2, 0),
     ("euler3d-lf-p4-tvd", 8, 3, (2, 2, 2), 0, 2 * np.pi, 4, "laxfriedrichs", 3, TG, 0.001, 2, 0),
+    ("euler3d-lf-p4-lsrk-ragged", 8, 3, (2, 3, 2), 0, 2 * np.pi, 4, "laxfriedrichs", 14, TG, 0.001, 2, 0),
+    ("euler3d-roe-p2-lsrk", 8, 3, (3, 3, 2), 0, 2 * np.pi, 2, "roe", 14, TG, 0.002, 2, 0),
+    ("euler3d-lf-p5-lsrk-rotated", 8, 3, (2, 2, 2), 0, 2 * np.pi, 5, "laxfriedrichs", 14, TG, 0.001, 2, 0, True),
+    ("euler3d-roe-p3-rotated", 8, 3, (3, 2, 3), 0, 2 * np.pi, 3, "roe", 14, TG, 0.002, 2, 0, True),
+    ("euler3d-roe-p3-mixed-rotated", 8, 3, (3, 2, 3), 0, 2 * np.pi, 3, "roe", 14, TG, 0.002, 2, 1, True),
+    ("euler3d-lf-p5-mixed", 8, 3, (2, 2, 2), 0, 2 * np.pi, 5, "laxfriedrichs", 14, TG, 0.001, 2, 1),
     ("euler2d-roe-p3-rk4", 1, 2, (4, 3), -5, 5, 3, "roe", 4, IV, 0.01, 3, 0),
     ("shallow-p2", 30, 2, (4, 4), -2, 2, 2, "laxfriedrichs", 14, GB, 0.001, 3, 0),
     ("ns3d-p3", 9, 3, (2, 2, 2), 0, 2 * np.pi, 3, "laxfriedrichs", 14, TG, 0.002, 2, 0),
@@ -256,8 +262,10 @@ def test_every_tile_variant_matches_oracle(case):
     caps, and the prefetching persistent kernel where the block sizes allow
     it -- gives the oracle's answer (FP64: 1e-12; mixed form: 1e-6)."""
     import dgm_b200
-    _, phys, dim, n, lo, hi, p, flux, inttype, ic, dt, steps, prec = case
-    m = dgm_b200.meshgen.box(dim, n, lo, hi, p)
+    _, phys, dim, n, lo, hi, p, flux, inttype, ic, dt, steps, prec = case[:13]
+    rotated = len(case) > 13 and case[13]
+    from tests.cases import rotated_box
+    m = rotated_box(dim, n, lo, hi, p, 0, seed=3) if rotated else dgm_b200.meshgen.box(dim, n, lo, hi, p)
     vis = 0.05 if phys == oracle.NS3D else 0.0
     P = oracle.Problem(dgm_io.Mesh(m.dim, m.verts, m.con, m.porder, m.qorder), phys, flux=flux, vis=vis)
     if phys == oracle.SHALLOW:
@@ -280,6 +288,8 @@ def test_every_tile_variant_matches_oracle(case):
         assert err < (1e-6 if prec else TOL_STATE), (k, kind, err)
     if phys == oracle.EULER3D and p == 3:
         assert 2 in kinds       # the prefetching kernel is built for this case
+    if phys == oracle.EULER3D and 2 <= p <= 5:
+        assert 3 in kinds       # the second-form stage kernel is built for this case
 
 
 def test_shallow_balance_keeps_state_steady():
