@@ -9,6 +9,12 @@ struct RegEuler3D {
 #define R(P) reg<DGMX_EULER3D, P, P + 1>(); reg<DGMX_EULER3D, P, P + 2>();
     R(2) R(3) R(4) R(5) R(6) R(7)
 #undef R
+    // second-form stage kernels at q = p+2, after the plain tiles (every
+    // template instantiation of a tile lives in one compilation unit: its
+    // launchers and its constant tables must come from the same module)
+#define R2(P) reg2<DGMX_EULER3D, P, P + 2>();
+    R2(2) R2(3) R2(4) R2(5)
+#undef R2
   }
 } reg_euler3d;
 }  // namespace

@@ -10,6 +10,9 @@ struct RegMixed {
 #define R3(P) reg<DGMX_EULER3D, P, P + 2, true>();
     R3(1) R3(2) R3(3) R3(4) R3(5) R3(6) R3(7)
 #undef R3
+#define R3B(P) reg2<DGMX_EULER3D, P, P + 2, true>();
+    R3B(2) R3B(3) R3B(4) R3B(5)
+#undef R3B
 #define R2(P) reg<DGMX_EULER2D, P, P + 1, true>(); reg<DGMX_EULER2D, P, P + 2, true>(); \
               reg<DGMX_SHALLOW, P, P + 1, true>(); reg<DGMX_SHALLOW, P, P + 2, true>();
     R2(1) R2(2) R2(3) R2(4) R2(5) R2(6) R2(7) R2(8)

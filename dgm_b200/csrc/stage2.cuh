@@ -107,6 +107,16 @@ struct Smem2 {
   __device__ T *slot(int s) const { return base + (size_t)s * C::SZ_SLOT; }
 };
 
+// End value B[m][end] of basis function m for a thread-varying m, by selects
+// over compile-time constant-bank operands (no divergent constant loads).
+template <class T, int L, int Q>
+__device__ __forceinline__ T end_value(int end, int m) {
+  T v = cEnd<T, L, Q>[end * L];
+#pragma unroll
+  for (int k = 1; k < L; ++k) v = (m == k) ? cEnd<T, L, Q>[end * L + k] : v;
+  return v;
+}
+
 // ---- phase 0: inputs -------------------------------------------------------
 template <class C>
 __device__ __forceinline__ void s2_load(const Smem2<C> &sm, const StageArgs &a, int e0, int tid) {
@@ -177,8 +187,82 @@ __device__ __forceinline__ void s2_load(const Smem2<C> &sm, const StageArgs &a, 
 }
 
 // ---- phase 1: numerical flux at every face point -----------------------------
+// The 3-D Euler flux of face_flux (kernels.cuh) written without the face
+// frame: for an orthonormal frame (n, s, t) the rotation and its inverse
+// cancel, so F(U).n = (m.n, m (u.n) + p n, (E + p) u.n), and the Roe
+// dissipation's two tangential waves become one tangential vector
+//   a_sh = (dm - (dm.n) n) - (u~ - (u~.n) n) drho,
+// with G_n, G_0 and G_E as in the frame and G_t = u~_t G_0 + min(u~.n, 0) a_sh.
+// Lax-Friedrichs (src/Euler3d.cpp:601-816) uses max(|u.n| + c) over both
+// sides, which is the reference's max(|u.n - c|, |u.n|, |u.n + c|).  Same
+// algebra as the frame form; only the rounding differs.
+template <class T>
+__device__ __forceinline__ bool face_flux_vec3(const T *UL, const T *UR, const T *n, T gamma, int flux, T *Fh,
+                                               T *FL, T *FR) {
+  const T gm1 = gamma - T(1.0);
+  const T n0 = n[0], n1 = n[1], n2 = n[2];
+  const T rl = UL[0], irl = T(1.0) / rl;
+  const T uxl = UL[1] * irl, uyl = UL[2] * irl, uzl = UL[3] * irl;
+  const T unl = fma(uzl, n2, fma(uyl, n1, uxl * n0));
+  const T pl = gm1 * fma(T(-0.5), fma(UL[3], uzl, fma(UL[2], uyl, UL[1] * uxl)), UL[4]);
+  const T rr = UR[0], irr = T(1.0) / rr;
+  const T uxr = UR[1] * irr, uyr = UR[2] * irr, uzr = UR[3] * irr;
+  const T unr = fma(uzr, n2, fma(uyr, n1, uxr * n0));
+  const T pr = gm1 * fma(T(-0.5), fma(UR[3], uzr, fma(UR[2], uyr, UR[1] * uxr)), UR[4]);
+  const bool ok = rl >= T(kAeps) && pl >= T(kAeps) && rr >= T(kAeps) && pr >= T(kAeps);
+  FL[0] = rl * unl;
+  FL[1] = fma(UL[1], unl, pl * n0);
+  FL[2] = fma(UL[2], unl, pl * n1);
+  FL[3] = fma(UL[3], unl, pl * n2);
+  FL[4] = (UL[4] + pl) * unl;
+  FR[0] = rr * unr;
+  FR[1] = fma(UR[1], unr, pr * n0);
+  FR[2] = fma(UR[2], unr, pr * n1);
+  FR[3] = fma(UR[3], unr, pr * n2);
+  FR[4] = (UR[4] + pr) * unr;
+  const T Hl = (UL[4] + pl) * irl, Hr = (UR[4] + pr) * irr;
+  if (flux == DGMX_FLUX_ROE) {
+    const T R = sqrt(rr * irl), iRp1 = T(1.0) / (T(1.0) + R);
+    const T ux = fma(R, uxr, uxl) * iRp1, uy = fma(R, uyr, uyl) * iRp1, uz = fma(R, uzr, uzl) * iRp1;
+    const T H = fma(R, Hr, Hl) * iRp1;
+    const T q2 = fma(uz, uz, fma(uy, uy, ux * ux));
+    const T a2 = gm1 * fma(T(-0.5), q2, H);
+    const T ainv = rsqrt(a2), a = a2 * ainv;
+    const T un = fma(uz, n2, fma(uy, n1, ux * n0));
+    const T dr = rr - rl, dmx = UR[1] - UL[1], dmy = UR[2] - UL[2], dmz = UR[3] - UL[3], dE = UR[4] - UL[4];
+    const T dmn = fma(dmz, n2, fma(dmy, n1, dmx * n0));
+    const T utx = fma(-un, n0, ux), uty = fma(-un, n1, uy), utz = fma(-un, n2, uz);
+    const T shx = fma(-utx, dr, fma(-dmn, n0, dmx)), shy = fma(-uty, dr, fma(-dmn, n1, dmy)),
+            shz = fma(-utz, dr, fma(-dmn, n2, dmz));
+    const T shu = fma(shz, utz, fma(shy, uty, shx * utx));
+    const T a1 = gm1 * ainv * ainv * (fma(dr, fma(-un, un, H), un * dmn) - (dE - shu));
+    const T a0 = T(0.5) * ainv * (fma(dr, un + a, -dmn) - a * a1);
+    const T a4 = dr - (a0 + a1);
+    const T l0 = fmin(un - a, T(0.0)), l1 = fmin(un, T(0.0)), l4 = fmin(un + a, T(0.0));
+    const T w0 = l0 * a0, w1 = l1 * a1, w4 = l4 * a4;
+    const T G0 = w0 + w1 + w4;
+    const T Gn = fma(un + a, w4, fma(un, w1, (un - a) * w0));
+    const T GE = fma(fma(un, a, H), w4, fma(T(0.5) * q2, w1, fma(fma(-un, a, H), w0, l1 * shu)));
+    Fh[0] = FL[0] + G0;
+    Fh[1] = FL[1] + fma(Gn, n0, fma(G0, utx, l1 * shx));
+    Fh[2] = FL[2] + fma(Gn, n1, fma(G0, uty, l1 * shy));
+    Fh[3] = FL[3] + fma(Gn, n2, fma(G0, utz, l1 * shz));
+    Fh[4] = FL[4] + GE;
+  } else {
+    const T cl = sqrt(gm1 * fma(T(-0.5), fma(uzl, uzl, fma(uyl, uyl, uxl * uxl)), Hl));
+    const T cr = sqrt(gm1 * fma(T(-0.5), fma(uzr, uzr, fma(uyr, uyr, uxr * uxr)), Hr));
+    const T lmax = fmax(fabs(unl) + cl, fabs(unr) + cr);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) Fh[k] = T(0.5) * (FL[k] + FR[k] + lmax * (UL[k] - UR[k]));
+  }
+  return ok;
+}
+
 // E = (F^ - F(U_own)).n J_side/J_el in the layout of the own traces, as
-// face_fluxes (stage.cuh) computes it.
+// face_fluxes (stage.cuh) computes it.  Both sides of a face evaluate the
+// flux with the master's state first; the states are selected before one
+// flux evaluation so that a warp holding master and slave points runs it
+// once.
 template <class C, int PHYS>
 __device__ __forceinline__ void s2_face_flux(const Smem2<C> &sm, const StageArgs &a, int tid) {
   using T = typename C::R;
@@ -192,25 +276,26 @@ __device__ __forceinline__ void s2_face_flux(const Smem2<C> &sm, const StageArgs
     const int gn = __ldg(a.perm + lk.perm + g);
     T *eo = sm.slot(s) + C::O_TR + (f * NF) * G * PG + (g / G) * PG + g % G;
     const T *tn = sm.slot(s) + C::O_TN + (f * NF) * GF + gn;
-    T Uo[5], Un[5], Fh[5], FL[5], FR[5];
-#pragma unroll
-    for (int n = 0; n < NF; ++n) { Uo[n] = eo[n * G * PG]; Un[n] = tn[n * GF]; }
-    const T nm[3] = {T(__ldg(&gc->nrm[f][0])), T(__ldg(&gc->nrm[f][1])), T(__ldg(&gc->nrm[f][2]))};
     const int mbits = __ldg(&gc->master);
     const bool master = (mbits >> f) & 1;
+    T UL[5], UR[5], Fh[5], FL[5], FR[5];
+#pragma unroll
+    for (int k = 0; k < NF; ++k) {
+      const T uo = eo[k * G * PG], un = tn[k * GF];
+      UL[k] = master ? uo : un;
+      UR[k] = master ? un : uo;
+    }
+    const T nm[3] = {T(__ldg(&gc->nrm[f][0])), T(__ldg(&gc->nrm[f][1])), T(__ldg(&gc->nrm[f][2]))};
     const T jr = T(__ldg(&gc->jr[f]));
-    const double *fr = gc->fr[f];
     bool ok;
     if constexpr (C::MIXED) {
-      if (master) ok = face_flux_pert<PHYS, T>(sm.ref[s], Uo, Un, nm, T(a.gamma), a.flux, Fh, FR, fr);
-      else ok = face_flux_pert<PHYS, T>(sm.ref[s], Un, Uo, nm, T(a.gamma), a.flux, Fh, FR, fr);
+      ok = face_flux_pert<PHYS, T>(sm.ref[s], UL, UR, nm, T(a.gamma), a.flux, Fh, FR, gc->fr[f]);
 #pragma unroll
-      for (int n = 0; n < NF; ++n) eo[n * G * PG] = master ? Fh[n] * jr : (FR[n] - Fh[n]) * jr;
+      for (int k = 0; k < NF; ++k) eo[k * G * PG] = (master ? Fh[k] : FR[k] - Fh[k]) * jr;
     } else {
-      if (master) ok = face_flux<PHYS, T>(Uo, Un, nm, T(a.gamma), a.flux, Fh, FL, FR, fr);
-      else ok = face_flux<PHYS, T>(Un, Uo, nm, T(a.gamma), a.flux, Fh, FL, FR, fr);
+      ok = face_flux_vec3<T>(UL, UR, nm, T(a.gamma), a.flux, Fh, FL, FR);
 #pragma unroll
-      for (int n = 0; n < NF; ++n) eo[n * G * PG] = master ? (Fh[n] - FL[n]) * jr : (FR[n] - Fh[n]) * jr;
+      for (int k = 0; k < NF; ++k) eo[k * G * PG] = (master ? Fh[k] - FL[k] : FR[k] - Fh[k]) * jr;
     }
     if (!ok) {
       atomicOr(a.err, 1);
@@ -341,10 +426,12 @@ template <class C, int PHYS>
 __device__ __forceinline__ void s2_volume(const Smem2<C> &sm, const StageArgs &a, int tid) {
   using T = typename C::R;
   constexpr int NF = C::NF, L = C::L, Q = C::Q, EPB = C::EPB;
-  constexpr int N = 3 * Q * Q;
+  // the columns of one direction fill whole warps, so r is warp-uniform
+  constexpr int RS = (Q * Q + 31) / 32 * 32, N = 3 * RS;
   const T gm1 = T(a.gamma) - T(1.0);
   for (int w = tid; w < EPB * N; w += C::NT) {
-    const int s = w / N, rem = w - s * N, r = rem / (Q * Q), jk = rem - r * Q * Q;
+    const int s = w / N, rem = w - s * N, r = rem / RS, jk = rem - r * RS;
+    if (jk >= Q * Q) continue;
     const GeomClass *gc = a.classes + sm.cls[s];
     const T m0 = T(__ldg(&gc->metric[3 * r + 0])), m1 = T(__ldg(&gc->metric[3 * r + 1])),
             m2 = T(__ldg(&gc->metric[3 * r + 2]));
@@ -467,8 +554,8 @@ __device__ __forceinline__ void s2_update(const Smem2<C> &sm, const StageArgs &a
     const T xk0 = xl[0 * FB + (n * L + aa) * PL + bb], xk1 = xl[5 * FB + (n * L + aa) * PL + bb];
     const T *xj0 = xl + 1 * FB + (n * L + aa) * PL, *xj1 = xl + 3 * FB + (n * L + aa) * PL;
     const T *xi0 = xl + 4 * FB + (n * L + bb) * PL, *xi1 = xl + 2 * FB + (n * L + bb) * PL;
-    const T eb0 = cEnd<T, L, Q>[bb], eb1 = cEnd<T, L, Q>[L + bb];
-    const T ea0 = cEnd<T, L, Q>[aa], ea1 = cEnd<T, L, Q>[L + aa];
+    const T eb0 = end_value<T, L, Q>(0, bb), eb1 = end_value<T, L, Q>(1, bb);
+    const T ea0 = end_value<T, L, Q>(0, aa), ea1 = end_value<T, L, Q>(1, aa);
     T R[L];
 #pragma unroll
     for (int c = 0; c < L; ++c) {
