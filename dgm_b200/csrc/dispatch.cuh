@@ -320,18 +320,19 @@ void reg2_variant() {
 }
 
 // Second-form variants of a 3-D Euler (p, q): one element per CTA at two
-// thread counts, uncapped and with the register cap of the shared-memory
-// occupancy.
+// thread counts, uncapped and with register caps near 96 and 80 registers
+// per thread (the CTAs per SM such caps allow).
 template <int PHYS, int P, int Q, bool MIXED = false>
 void reg2() {
   constexpr int NTA = ((P + 1) * (P + 1) * 5 + 31) / 32 * 32;   // one thread per modal row
   constexpr int NTB = NTA + 32;
-  using CA = Cfg2<PHYS, P + 1, Q, 1, NTA, 0, MIXED>;
-  constexpr int BA = (int)((228 * 1024) / (CA::SMEM + 1024)) > 16 ? 16 : (int)((228 * 1024) / (CA::SMEM + 1024));
   reg2_variant<PHYS, P, Q, 1, NTA, 0, MIXED>();
   reg2_variant<PHYS, P, Q, 1, NTB, 0, MIXED>();
-  if constexpr (BA >= 2) reg2_variant<PHYS, P, Q, 1, NTA, BA, MIXED>();
-  if constexpr (BA >= 2) reg2_variant<PHYS, P, Q, 1, NTB, BA, MIXED>();
+  if constexpr (65536 / (NTB * 96) >= 2) reg2_variant<PHYS, P, Q, 1, NTB, 65536 / (NTB * 96), MIXED>();
+  if constexpr (65536 / (NTA * 96) >= 2) reg2_variant<PHYS, P, Q, 1, NTA, 65536 / (NTA * 96), MIXED>();
+  if constexpr (65536 / (NTB * 80) >= 2 && 65536 / (NTB * 80) != 65536 / (NTB * 96))
+    reg2_variant<PHYS, P, Q, 1, NTB, 65536 / (NTB * 80), MIXED>();
+  if constexpr (MIXED && 65536 / (NTB * 64) >= 2) reg2_variant<PHYS, P, Q, 1, NTB, 65536 / (NTB * 64), MIXED>();
 }
 
 template <int PHYS, int P, int Q, int EPB, int MINB, bool MIXED>

@@ -23,10 +23,16 @@
 //    is added to the projected right-hand side in the last pass;
 //  * the update writes each modal row from registers and the next traces
 //    (modal -> face Gauss points, src/Hex.cpp:933-947) start from the same
-//    registers (end reduction along the contiguous axis).
+//    registers (end reduction along the contiguous axis);
+//  * what only one thread consumes is read from global memory by that
+//    thread (the face traces by the face-point threads, the modal rows by
+//    the first backward pass), so shared memory carries only the
+//    intermediates that change hands -- its bandwidth, not the FP64 pipe,
+//    bounded the first version of this kernel;
+//  * independent passes share a barrier interval (nine per element).
 // Every (L, Q) works; the element's shared-memory regions are laid out by
-// lifetime (offsets below) with odd pitches on the rows that a warp reads
-// along, so pencils fall on distinct banks.
+// barrier interval (offsets below) with odd pitches on the rows that a warp
+// reads along, so pencils fall on distinct banks.
 //
 // Scope: Euler 3-D, no boundary sides, LSRK and right-hand-side stages (the
 // other stage kinds run the plain kernel of the same (L, Q)).
@@ -50,12 +56,9 @@ struct Cfg2 {
   static constexpr int NFACE = 6, GF = G * G, LD = L * L * L, QD = Q * Q * Q;
   // odd pitches for rows of an even length
   static constexpr int PL = L % 2 == 0 ? L + 1 : L;   // modal rows (and face-plane rows of L)
-  static constexpr int PG = G % 2 == 0 ? G + 1 : G;   // face-trace rows of G
+  static constexpr int PE = GF % 2 == 0 ? GF + 1 : GF;   // one (face, field) block of face terms
   // region sizes (values of R)
-  static constexpr int S_UA = NF * L * L * PL;          // modal block, padded rows
-  static constexpr int S_TR = NFACE * NF * G * PG;      // own traces / face terms, padded rows
-  static constexpr int S_TN = NFACE * NF * GF;          // neighbour traces (neighbour's order)
-  static constexpr int S_Z1 = NFACE * NF * G * PL;      // lift pass 1: [f][n][g][b'] padded
+  static constexpr int S_EF = NFACE * NF * PE;          // face terms [f][n][g h], padded blocks
   static constexpr int S_XL = NFACE * NF * L * PL;      // lifted-projected face terms [f][n][a'][b'] padded
   static constexpr int S_T1 = NF * L * L * Q;           // [n][a][b][k]
   static constexpr int S_T2 = NF * L * Q * Q;           // [n][a][j][k]
@@ -67,24 +70,19 @@ struct Cfg2 {
   static constexpr int S_UB = NF * L * L * PL;          // updated modal block, padded rows
   static constexpr int S_FP = NFACE * NF * L * L;       // end-reduced face planes [f][n][a'][b']
   static constexpr int S_W1 = NFACE * NF * G * PL;      // trace pass 1 [f][n][g][b'] padded
-  // lifetimes (phases): UA 0-3, TR 0-2a, TN 0-1, Z1 2a-2b, XL 2b-8, T1 3-4,
-  // T2 4-5, UN 5-6, X 6-7, Y 7-8, UB 8-9, FP 8-10a, W1 10a-10b.
-  // Region A (from 0): UA | TR | TN (phases 0-2), then UN (5-6), then Y (7-8)
-  static constexpr int O_UA = 0, O_TR = O_UA + S_UA, O_TN = O_TR + S_TR;
-  static constexpr int O_Z1 = O_TN;                     // TN is dead after the face fluxes
-  static constexpr int O_T1 = O_TR;                     // TR is dead after lift pass 1
-  static constexpr int O_UN = 0;                        // UA, T1 dead by phase 5 (T2 lives elsewhere)
-  static constexpr int O_Y = 0;                         // UN dead after phase 6
-  static constexpr int A_END = cmax(cmax(O_TN + cmax(S_TN, S_Z1), O_T1 + S_T1), cmax(O_UN + S_UN, O_Y + S_Y));
-  // Region B: X (6-7); T2 (4-5) inside it; UB, FP, W1 (8-10) inside it
-  static constexpr int O_X = A_END;
-  static constexpr int O_T2 = O_X + S_X - S_T2;         // the tail of X: phase 5 reads it before X is written
-  static constexpr int O_UB = O_X, O_FP = O_UB + S_UB, O_W1 = O_FP + S_FP;
-  static constexpr int B_END = cmax(O_X + S_X, O_W1 + S_W1);
-  static_assert(O_T2 >= A_END, "T2 must not overlap region A");
-  static_assert(O_T1 + S_T1 <= O_Z1, "T1 (phase 3) must not overlap Z1 (read in phase 2b, the same interval)");
-  // XL after both (alive from phase 2 to phase 8)
-  static constexpr int O_XL = B_END;
+  // Barrier intervals: 1 face fluxes -> EF, backward k-pass -> T1;
+  // 2 lift EF -> XL, j-pass T1 -> T2; 3 i-pass T2 -> UN; 4 volume UN -> X;
+  // 5 j-pass X -> Y; 6 k-pass, lift, update Y, XL -> UB, FP; 7 ends UB -> FP;
+  // 8 traces FP -> W1; 9 traces W1 -> global.  A region written in one
+  // interval may share memory only with regions that no thread touches in
+  // that interval.
+  static constexpr int O_EF = 0, O_T1 = O_EF + S_EF, O_T2 = O_T1 + S_T1;   // intervals 1-2
+  static constexpr int O_UN = 0;                                           // 3-4 (T2 is above it)
+  static constexpr int O_Y = 0;                                            // 5-6
+  static constexpr int O_X = cmax(S_UN, S_Y);                              // 4-5
+  static constexpr int O_UB = O_X, O_FP = O_UB + S_UB, O_W1 = O_FP + S_FP;  // 6-9 (X is dead)
+  static constexpr int O_XL = cmax(cmax(O_T2 + S_T2, O_X + S_X), O_W1 + S_W1);   // 2-6
+  static_assert(O_T2 >= S_UN, "T2 (read in interval 3) must not overlap UN (written in interval 3)");
   static constexpr int SZ_SLOT = O_XL + S_XL;
   static constexpr size_t DATA = ((size_t)EPB * SZ_SLOT * sizeof(R) + 15) / 16 * 16;
   static constexpr size_t SMEM = DATA + (size_t)EPB * (NFACE * sizeof(FaceLink) + 16 + (MIXED_ ? sizeof(RefState<R>) : 0));
@@ -117,13 +115,11 @@ __device__ __forceinline__ T end_value(int end, int m) {
   return v;
 }
 
-// ---- phase 0: inputs -------------------------------------------------------
+
+// ---- the tile's links, class and (mixed form) reference state ----------------
 template <class C>
 __device__ __forceinline__ void s2_load(const Smem2<C> &sm, const StageArgs &a, int e0, int tid) {
-  using T = typename C::R;
-  constexpr int NF = C::NF, L = C::L, G = C::G, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB, PL = C::PL,
-                PG = C::PG;
-  // links and class
+  constexpr int NFACE = C::NFACE, EPB = C::EPB;
   for (int w = tid; w < EPB * NFACE; w += C::NT) {
     const int s = w / NFACE, f = w - s * NFACE, e = e0 + s;
     const FaceLink lk = e < a.ne ? a.links[(size_t)e * NFACE + f] : FaceLink{0, 0, 0, -1};
@@ -136,57 +132,9 @@ __device__ __forceinline__ void s2_load(const Smem2<C> &sm, const StageArgs &a, 
         sm.ref[s] = *reinterpret_cast<const RefState<float> *>(a.uref + kUrefStride * solve_of(a, gc >= 0 ? e : -1) + 10);
     }
   }
-  // modal register rows (perturbation about the reference in the mixed form)
-  constexpr int RPS = NF * L * L;
-  for (int r = tid; r < EPB * RPS; r += C::NT) {
-    const int s = r / RPS, rr = r - s * RPS, e = e0 + s;
-    double v[L];
-    if (e < a.ne) {
-      ld_row<L>(a.X + ((size_t)e * RPS + rr) * L, v);
-      if constexpr (C::MIXED)
-        if (rr % (L * L) == 0) v[0] -= a.uref[kUrefStride * solve_of(a, e) + 5 + rr / (L * L)];
-    } else {
-#pragma unroll
-      for (int k = 0; k < L; ++k) v[k] = (!C::MIXED && k == 0 && rr % (L * L) == 0) ? 1.0 : 0.0;
-    }
-    T *dst = sm.slot(s) + C::O_UA + rr * PL;
-#pragma unroll
-    for (int k = 0; k < L; ++k) dst[k] = T(v[k]);
-  }
-  // own traces, rows of G into padded rows
-  const T *Tin = trace_in<C>(a);
-  constexpr int TPS = NFACE * NF * G;
-  for (int r = tid; r < EPB * TPS; r += C::NT) {
-    const int s = r / TPS, rr = r - s * TPS, e = e0 + s;
-    T v[G];
-    if (e < a.ne) {
-      ld_row<G>(Tin + (size_t)e * NFACE * NF * GF + rr * G, v);
-    } else {
-#pragma unroll
-      for (int k = 0; k < G; ++k) v[k] = T((!C::MIXED && (rr / G) % NF == 0) ? 1.0 : 0.0);
-    }
-    T *dst = sm.slot(s) + C::O_TR + rr * PG;
-#pragma unroll
-    for (int k = 0; k < G; ++k) dst[k] = v[k];
-  }
-  // neighbour face blocks (their own point order), rows of G
-  for (int r = tid; r < EPB * TPS; r += C::NT) {
-    const int s = r / TPS, rr = r - s * TPS, f = rr / (NF * G), q = rr - f * NF * G, e = e0 + s;
-    T v[G];
-    if (e < a.ne) {
-      const FaceLink lk = a.links[(size_t)e * NFACE + f];
-      ld_row<G>(Tin + ((size_t)lk.elem * NFACE + lk.face) * NF * GF + q * G, v);
-    } else {
-#pragma unroll
-      for (int k = 0; k < G; ++k) v[k] = T((!C::MIXED && q / G == 0) ? 1.0 : 0.0);
-    }
-    T *dst = sm.slot(s) + C::O_TN + rr * G;
-#pragma unroll
-    for (int k = 0; k < G; ++k) dst[k] = v[k];
-  }
 }
 
-// ---- phase 1: numerical flux at every face point -----------------------------
+// ---- interval 1a: numerical flux at every face point --------------------------
 // The 3-D Euler flux of face_flux (kernels.cuh) written without the face
 // frame: for an orthonormal frame (n, s, t) the rotation and its inverse
 // cancel, so F(U).n = (m.n, m (u.n) + p n, (E + p) u.n), and the Roe
@@ -258,141 +206,153 @@ __device__ __forceinline__ bool face_flux_vec3(const T *UL, const T *UR, const T
   return ok;
 }
 
-// E = (F^ - F(U_own)).n J_side/J_el in the layout of the own traces, as
-// face_fluxes (stage.cuh) computes it.  Both sides of a face evaluate the
-// flux with the master's state first; the states are selected before one
-// flux evaluation so that a warp holding master and slave points runs it
-// once.
+
+// E = (F^ - F(U_own)).n J_side/J_el at face point g of face f, as
+// face_fluxes (stage.cuh) computes it, from the own and neighbour traces in
+// global memory (a warp's points are two faces' contiguous rows).  Both sides
+// of a face evaluate the flux with the master's state first; the states are
+// selected before one flux evaluation so that a warp holding master and
+// slave points runs it once.
 template <class C, int PHYS>
-__device__ __forceinline__ void s2_face_flux(const Smem2<C> &sm, const StageArgs &a, int tid) {
+__device__ __forceinline__ void s2_face_point(const Smem2<C> &sm, const StageArgs &a, int e0, int w) {
   using T = typename C::R;
-  constexpr int NF = C::NF, G = C::G, GF = C::GF, NFACE = C::NFACE, EPB = C::EPB, PG = C::PG;
-  for (int w = tid; w < EPB * NFACE * GF; w += C::NT) {
-    const int s = w / (NFACE * GF), rem = w - s * NFACE * GF, f = rem / GF, g = rem - f * GF;
-    const int e = sm.eid[s];
-    if (e < 0) continue;
-    const FaceLink lk = sm.lnk[s * NFACE + f];
-    const GeomClass *gc = a.classes + sm.cls[s];
-    const int gn = __ldg(a.perm + lk.perm + g);
-    T *eo = sm.slot(s) + C::O_TR + (f * NF) * G * PG + (g / G) * PG + g % G;
-    const T *tn = sm.slot(s) + C::O_TN + (f * NF) * GF + gn;
-    const int mbits = __ldg(&gc->master);
-    const bool master = (mbits >> f) & 1;
-    T UL[5], UR[5], Fh[5], FL[5], FR[5];
+  constexpr int NF = C::NF, GF = C::GF, NFACE = C::NFACE, PE = C::PE;
+  const int s = w / (NFACE * GF), rem = w - s * NFACE * GF, f = rem / GF, g = rem - f * GF;
+  const int e = sm.eid[s];
+  if (e < 0) return;
+  const FaceLink lk = sm.lnk[s * NFACE + f];
+  const GeomClass *gc = a.classes + sm.cls[s];
+  const T *Tin = trace_in<C>(a);
+  const int gn = __ldg(a.perm + lk.perm + g);
+  const T *to = Tin + ((size_t)e * NFACE + f) * NF * GF + g;
+  const T *tn = Tin + ((size_t)lk.elem * NFACE + lk.face) * NF * GF + gn;
+  const int mbits = __ldg(&gc->master);
+  const bool master = (mbits >> f) & 1;
+  T UL[5], UR[5], Fh[5], FL[5], FR[5];
 #pragma unroll
-    for (int k = 0; k < NF; ++k) {
-      const T uo = eo[k * G * PG], un = tn[k * GF];
-      UL[k] = master ? uo : un;
-      UR[k] = master ? un : uo;
+  for (int k = 0; k < NF; ++k) {
+    const T uo = to[k * GF], un = tn[k * GF];
+    UL[k] = master ? uo : un;
+    UR[k] = master ? un : uo;
+  }
+  const T nm[3] = {T(__ldg(&gc->nrm[f][0])), T(__ldg(&gc->nrm[f][1])), T(__ldg(&gc->nrm[f][2]))};
+  const T jr = T(__ldg(&gc->jr[f]));
+  T *eo = sm.slot(s) + C::O_EF + f * NF * PE + g;
+  bool ok;
+  if constexpr (C::MIXED) {
+    ok = face_flux_pert<PHYS, T>(sm.ref[s], UL, UR, nm, T(a.gamma), a.flux, Fh, FR, gc->fr[f]);
+#pragma unroll
+    for (int k = 0; k < NF; ++k) eo[k * PE] = (master ? Fh[k] : FR[k] - Fh[k]) * jr;
+  } else {
+    ok = face_flux_vec3<T>(UL, UR, nm, T(a.gamma), a.flux, Fh, FL, FR);
+#pragma unroll
+    for (int k = 0; k < NF; ++k) eo[k * PE] = (master ? Fh[k] - FL[k] : FR[k] - Fh[k]) * jr;
+  }
+  if (!ok) {
+    atomicOr(a.err, 1);
+    atomicMin(a.err + 1, e);
+  }
+}
+
+// ---- interval 1b: backward k-pass from the modal rows in global memory ----
+// T1[n][a][b][k] = sum_c B[c][k] u[n][a][b][c]; the mixed form takes the
+// solve's reference state out of the constant mode in FP64 first.  Elements
+// past the end get the constant state (their results are discarded).
+template <class C>
+__device__ __forceinline__ void s2_backward_k_row(const Smem2<C> &sm, const StageArgs &a, int e0, int w) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, L = C::L, Q = C::Q, RPS = NF * L * L;
+  const int s = w / RPS, r = w - s * RPS, e = e0 + s;   // r = (n*L + a)*L + b
+  double v[L];
+  if (e < a.ne) {
+    ld_row<L>(a.X + ((size_t)e * RPS + r) * L, v);
+    if constexpr (C::MIXED)
+      if (r % (L * L) == 0) v[0] -= a.uref[kUrefStride * solve_of(a, e) + 5 + r / (L * L)];
+  } else {
+#pragma unroll
+    for (int k = 0; k < L; ++k) v[k] = (!C::MIXED && k == 0 && r % (L * L) == 0) ? 1.0 : 0.0;
+  }
+  T *dst = sm.slot(s) + C::O_T1 + r * Q;
+#pragma unroll
+  for (int k = 0; k < Q; ++k) {
+    T acc = T(0);
+#pragma unroll
+    for (int c = 0; c < L; ++c) acc = fma(cB<T, L, Q>[c * Q + k], T(v[c]), acc);
+    dst[k] = acc;
+  }
+}
+
+template <class C, int PHYS>
+__device__ __forceinline__ void s2_interval1(const Smem2<C> &sm, const StageArgs &a, int e0, int tid) {
+  constexpr int N1 = C::EPB * C::NFACE * C::GF, N2 = C::EPB * C::NF * C::L * C::L;
+  for (int w = tid; w < N1 + N2; w += C::NT) {
+    if (w < N1) s2_face_point<C, PHYS>(sm, a, e0, w);
+    else s2_backward_k_row<C>(sm, a, e0, w - N1);
+  }
+}
+
+// ---- interval 2a: lift and projection of one face's terms of one field ------
+// XL[a'][b'] = sum_g BwG[a'][g] sum_h BwG[b'][h] E[g][h]; one column b' at a
+// time keeps the registers to the 16 face terms and 8 partial sums.
+template <class C>
+__device__ __forceinline__ void s2_lift(const Smem2<C> &sm, int w) {
+  using T = typename C::R;
+  constexpr int NF = C::NF, L = C::L, Q = C::Q, G = C::G, GF = C::GF, NFACE = C::NFACE, PE = C::PE, PL = C::PL;
+  const int s = w / (NFACE * NF), fn = w - s * NFACE * NF;
+  const T *src = sm.slot(s) + C::O_EF + fn * PE;
+  T E[GF];
+#pragma unroll
+  for (int q = 0; q < GF; ++q) E[q] = src[q];
+  T *dst = sm.slot(s) + C::O_XL + fn * L * PL;
+#pragma unroll
+  for (int b = 0; b < L; ++b) {
+    T z[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      T acc = T(0);
+#pragma unroll
+      for (int h = 0; h < G; ++h) acc = fma(cBwG<T, L, Q>[b * G + h], E[g * G + h], acc);
+      z[g] = acc;
     }
-    const T nm[3] = {T(__ldg(&gc->nrm[f][0])), T(__ldg(&gc->nrm[f][1])), T(__ldg(&gc->nrm[f][2]))};
-    const T jr = T(__ldg(&gc->jr[f]));
-    bool ok;
-    if constexpr (C::MIXED) {
-      ok = face_flux_pert<PHYS, T>(sm.ref[s], UL, UR, nm, T(a.gamma), a.flux, Fh, FR, gc->fr[f]);
 #pragma unroll
-      for (int k = 0; k < NF; ++k) eo[k * G * PG] = (master ? Fh[k] : FR[k] - Fh[k]) * jr;
-    } else {
-      ok = face_flux_vec3<T>(UL, UR, nm, T(a.gamma), a.flux, Fh, FL, FR);
+    for (int aa = 0; aa < L; ++aa) {
+      T acc = T(0);
 #pragma unroll
-      for (int k = 0; k < NF; ++k) eo[k * G * PG] = (master ? Fh[k] - FL[k] : FR[k] - Fh[k]) * jr;
-    }
-    if (!ok) {
-      atomicOr(a.err, 1);
-      atomicMin(a.err + 1, e);
+      for (int g = 0; g < G; ++g) acc = fma(cBwG<T, L, Q>[aa * G + g], z[g], acc);
+      dst[aa * PL + b] = acc;
     }
   }
 }
 
-// ---- phase 2: lift and projection of the face terms --------------------------
-// pass a: Z1[f][n][g][b'] = sum_h BwG[b'][h] E[f][n][g][h]
+// ---- interval 2b-3: modal -> GLL values (j and i passes) ---------------------
 template <class C>
-__device__ __forceinline__ void s2_lift_a(const Smem2<C> &sm, int tid) {
+__device__ __forceinline__ void s2_backward_j_pencil(const Smem2<C> &sm, int w) {
   using T = typename C::R;
-  constexpr int NF = C::NF, L = C::L, Q = C::Q, G = C::G, NFACE = C::NFACE, EPB = C::EPB, PG = C::PG, PL = C::PL;
-  constexpr int N = NFACE * NF * G;
-  for (int w = tid; w < EPB * N; w += C::NT) {
-    const int s = w / N, r = w - s * N;   // r = (f*NF + n)*G + g
-    const T *src = sm.slot(s) + C::O_TR + r * PG;
-    T v[G];
+  constexpr int NF = C::NF, L = C::L, Q = C::Q, N = NF * L * Q;
+  const int s = w / N, r = w - s * N, na = r / Q, k = r - na * Q;   // na = n*L + a
+  const T *src = sm.slot(s) + C::O_T1 + na * L * Q + k;
+  T v[L];
 #pragma unroll
-    for (int h = 0; h < G; ++h) v[h] = src[h];
-    T *dst = sm.slot(s) + C::O_Z1 + r * PL;
+  for (int b = 0; b < L; ++b) v[b] = src[b * Q];
+  T *dst = sm.slot(s) + C::O_T2 + na * Q * Q + k;
 #pragma unroll
-    for (int b = 0; b < L; ++b) {
-      T acc = T(0);
+  for (int j = 0; j < Q; ++j) {
+    T acc = T(0);
 #pragma unroll
-      for (int h = 0; h < G; ++h) acc = fma(cBwG<T, L, Q>[b * G + h], v[h], acc);
-      dst[b] = acc;
-    }
-  }
-}
-// pass b: XL[f][n][a'][b'] = sum_g BwG[a'][g] Z1[f][n][g][b']
-template <class C>
-__device__ __forceinline__ void s2_lift_b(const Smem2<C> &sm, int tid) {
-  using T = typename C::R;
-  constexpr int NF = C::NF, L = C::L, Q = C::Q, G = C::G, NFACE = C::NFACE, EPB = C::EPB, PL = C::PL;
-  constexpr int N = NFACE * NF * L;
-  for (int w = tid; w < EPB * N; w += C::NT) {
-    const int s = w / N, r = w - s * N, fn = r / L, b = r - fn * L;
-    const T *src = sm.slot(s) + C::O_Z1 + fn * G * PL + b;
-    T v[G];
-#pragma unroll
-    for (int g = 0; g < G; ++g) v[g] = src[g * PL];
-    T *dst = sm.slot(s) + C::O_XL + fn * L * PL + b;
-#pragma unroll
-    for (int a = 0; a < L; ++a) {
-      T acc = T(0);
-#pragma unroll
-      for (int g = 0; g < G; ++g) acc = fma(cBwG<T, L, Q>[a * G + g], v[g], acc);
-      dst[a * PL] = acc;
-    }
+    for (int b = 0; b < L; ++b) acc = fma(cB<T, L, Q>[b * Q + j], v[b], acc);
+    dst[j * Q] = acc;
   }
 }
 
-// ---- phases 3-5: modal -> GLL values ----------------------------------------
 template <class C>
-__device__ __forceinline__ void s2_backward_k(const Smem2<C> &sm, int tid) {
-  using T = typename C::R;
-  constexpr int NF = C::NF, L = C::L, Q = C::Q, EPB = C::EPB, PL = C::PL;
-  constexpr int N = NF * L * L;
-  for (int w = tid; w < EPB * N; w += C::NT) {
-    const int s = w / N, r = w - s * N;   // r = (n*L + a)*L + b
-    const T *src = sm.slot(s) + C::O_UA + r * PL;
-    T v[L];
-#pragma unroll
-    for (int c = 0; c < L; ++c) v[c] = src[c];
-    T *dst = sm.slot(s) + C::O_T1 + r * Q;
-#pragma unroll
-    for (int k = 0; k < Q; ++k) {
-      T acc = T(0);
-#pragma unroll
-      for (int c = 0; c < L; ++c) acc = fma(cB<T, L, Q>[c * Q + k], v[c], acc);
-      dst[k] = acc;
-    }
+__device__ __forceinline__ void s2_interval2(const Smem2<C> &sm, int tid) {
+  constexpr int N1 = C::EPB * C::NFACE * C::NF, N2 = C::EPB * C::NF * C::L * C::Q;
+  for (int w = tid; w < N1 + N2; w += C::NT) {
+    if (w < N2) s2_backward_j_pencil<C>(sm, w);
+    else s2_lift<C>(sm, w - N2);
   }
 }
-template <class C>
-__device__ __forceinline__ void s2_backward_j(const Smem2<C> &sm, int tid) {
-  using T = typename C::R;
-  constexpr int NF = C::NF, L = C::L, Q = C::Q, EPB = C::EPB;
-  constexpr int N = NF * L * Q;
-  for (int w = tid; w < EPB * N; w += C::NT) {
-    const int s = w / N, r = w - s * N, na = r / Q, k = r - na * Q;   // na = n*L + a
-    const T *src = sm.slot(s) + C::O_T1 + na * L * Q + k;
-    T v[L];
-#pragma unroll
-    for (int b = 0; b < L; ++b) v[b] = src[b * Q];
-    T *dst = sm.slot(s) + C::O_T2 + na * Q * Q + k;
-#pragma unroll
-    for (int j = 0; j < Q; ++j) {
-      T acc = T(0);
-#pragma unroll
-      for (int b = 0; b < L; ++b) acc = fma(cB<T, L, Q>[b * Q + j], v[b], acc);
-      dst[j * Q] = acc;
-    }
-  }
-}
+
 template <class C>
 __device__ __forceinline__ void s2_backward_i(const Smem2<C> &sm, int tid) {
   using T = typename C::R;
@@ -415,91 +375,121 @@ __device__ __forceinline__ void s2_backward_i(const Smem2<C> &sm, int tid) {
   }
 }
 
-// ---- phase 6: contravariant fluxes and the i-axis pass ----------------------
-// Column (j, k), direction r: G_r = sum_d metric[r][d] F_d(U) at the Q points
-// of the column, then X_r[n][a] = sum_i C_r[a][i] G_r[n][i] with C_0 = E (the
-// derivative along i) and C_1 = C_2 = B W.  With the contravariant velocity
-// V_r = metric[r] . u:  G_r[rho] = rho V_r, G_r[m_d] = m_d V_r + p metric[r][d],
-// G_r[E] = (E + p) V_r.  The mixed form evaluates F(Ub + u') - F(Ub)
-// (volume_flux_pert, kernels.cuh) the same way.
-template <class C, int PHYS>
-__device__ __forceinline__ void s2_volume(const Smem2<C> &sm, const StageArgs &a, int tid) {
+// ---- interval 4: contravariant fluxes and the i-axis pass --------------------
+// Column (j, k), directions [R0, R0 + NR): G_r = sum_d metric[r][d] F_d(U)
+// at the Q points of the column, then X_r[n][a] = sum_i C_r[a][i] G_r[n][i]
+// with C_0 = E (the derivative along i) and C_1 = C_2 = B W.  With the
+// contravariant velocity V_r = metric[r] . u:  G_r[rho] = rho V_r,
+// G_r[m_d] = m_d V_r + p metric[r][d], G_r[E] = (E + p) V_r.  The mixed form
+// evaluates F(Ub + u') - F(Ub) (as volume_flux_pert, kernels.cuh) the same
+// way.  FP64 runs one direction per thread (20 accumulators; the columns of
+// a direction fill whole warps), the FP32 form all three (60).
+template <class C, int NR, int R0>
+__device__ __forceinline__ void s2_volume_column(const Smem2<C> &sm, const StageArgs &a, int s, int jk) {
   using T = typename C::R;
-  constexpr int NF = C::NF, L = C::L, Q = C::Q, EPB = C::EPB;
-  // the columns of one direction fill whole warps, so r is warp-uniform
-  constexpr int RS = (Q * Q + 31) / 32 * 32, N = 3 * RS;
+  constexpr int NF = C::NF, L = C::L, Q = C::Q;
   const T gm1 = T(a.gamma) - T(1.0);
-  for (int w = tid; w < EPB * N; w += C::NT) {
-    const int s = w / N, rem = w - s * N, r = rem / RS, jk = rem - r * RS;
-    if (jk >= Q * Q) continue;
-    const GeomClass *gc = a.classes + sm.cls[s];
-    const T m0 = T(__ldg(&gc->metric[3 * r + 0])), m1 = T(__ldg(&gc->metric[3 * r + 1])),
-            m2 = T(__ldg(&gc->metric[3 * r + 2]));
-    const T *un = sm.slot(s) + C::O_UN + jk;
-    T acc[5][L];
+  const GeomClass *gc = a.classes + sm.cls[s];
+  T met[NR][3];
+#pragma unroll
+  for (int r = 0; r < NR; ++r)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) met[r][d] = T(__ldg(&gc->metric[3 * (R0 + r) + d]));
+  const T *un = sm.slot(s) + C::O_UN + jk;
+  T acc[NR][5][L];
+#pragma unroll
+  for (int r = 0; r < NR; ++r)
 #pragma unroll
     for (int n = 0; n < NF; ++n)
 #pragma unroll
-      for (int b = 0; b < L; ++b) acc[n][b] = T(0);
+      for (int b = 0; b < L; ++b) acc[r][n][b] = T(0);
 #pragma unroll
-    for (int i = 0; i < Q; ++i) {
-      T U[5], Gr[5];
+  for (int i = 0; i < Q; ++i) {
+    T U[5];
 #pragma unroll
-      for (int n = 0; n < NF; ++n) U[n] = un[(n * Q + i) * Q * Q];
-      if constexpr (C::MIXED) {
-        const RefState<T> &b = sm.ref[s];
-        const T rho = b.r + U[0], ir = p_rcp(rho);
-        const T mx = b.m[0] + U[1], my = b.m[1] + U[2], mz = b.m[2] + U[3];
-        const T upx = (U[1] - b.u[0] * U[0]) * ir, upy = (U[2] - b.u[1] * U[0]) * ir, upz = (U[3] - b.u[2] * U[0]) * ir;
-        T sdot = T(0);
-        sdot = fma(U[1], b.u[0], sdot); sdot = fma(mx, upx, sdot);
-        sdot = fma(U[2], b.u[1], sdot); sdot = fma(my, upy, sdot);
-        sdot = fma(U[3], b.u[2], sdot); sdot = fma(mz, upz, sdot);
-        const T pp = gm1 * fma(T(-0.5), sdot, U[4]);
-        const T Hp = U[4] + pp, H = b.H + Hp;
+    for (int n = 0; n < NF; ++n) U[n] = un[(n * Q + i) * Q * Q];
+    if constexpr (C::MIXED) {
+      const RefState<T> &b = sm.ref[s];
+      const T rho = b.r + U[0], ir = p_rcp(rho);
+      const T mx = b.m[0] + U[1], my = b.m[1] + U[2], mz = b.m[2] + U[3];
+      const T upx = (U[1] - b.u[0] * U[0]) * ir, upy = (U[2] - b.u[1] * U[0]) * ir, upz = (U[3] - b.u[2] * U[0]) * ir;
+      T sdot = T(0);
+      sdot = fma(U[1], b.u[0], sdot); sdot = fma(mx, upx, sdot);
+      sdot = fma(U[2], b.u[1], sdot); sdot = fma(my, upy, sdot);
+      sdot = fma(U[3], b.u[2], sdot); sdot = fma(mz, upz, sdot);
+      const T pp = gm1 * fma(T(-0.5), sdot, U[4]);
+      const T Hp = U[4] + pp, H = b.H + Hp;
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        const T m0 = met[r][0], m1 = met[r][1], m2 = met[r][2];
         const T Vb = m0 * b.u[0] + m1 * b.u[1] + m2 * b.u[2];       // reference contravariant velocity
         const T Vp = m0 * upx + m1 * upy + m2 * upz;                 // its perturbation
+        T Gr[5];
         Gr[0] = m0 * U[1] + m1 * U[2] + m2 * U[3];
         Gr[1] = fma(U[1], Vb, fma(mx, Vp, pp * m0));
         Gr[2] = fma(U[2], Vb, fma(my, Vp, pp * m1));
         Gr[3] = fma(U[3], Vb, fma(mz, Vp, pp * m2));
         Gr[4] = fma(Hp, Vb, H * Vp);
-      } else {
-        const T ir = T(1.0) / U[0];
-        const T u = U[1] * ir, v = U[2] * ir, ww = U[3] * ir;
-        T p = u * U[1];
-        p = fma(v, U[2], p);
-        p = fma(ww, U[3], p);
-        p = T(-0.5) * gm1 * p;
-        p = fma(gm1, U[4], p);
+#pragma unroll
+        for (int n = 0; n < NF; ++n)
+#pragma unroll
+          for (int bb = 0; bb < L; ++bb)
+            acc[r][n][bb] = fma(R0 + r == 0 ? cE2<T, L, Q>[bb * Q + i] : cBw<T, L, Q>[bb * Q + i], Gr[n], acc[r][n][bb]);
+      }
+    } else {
+      const T ir = T(1.0) / U[0];
+      const T u = U[1] * ir, v = U[2] * ir, ww = U[3] * ir;
+      T p = u * U[1];
+      p = fma(v, U[2], p);
+      p = fma(ww, U[3], p);
+      p = T(-0.5) * gm1 * p;
+      p = fma(gm1, U[4], p);
+      const T Ep = U[4] + p;
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        const T m0 = met[r][0], m1 = met[r][1], m2 = met[r][2];
         const T V = fma(m2, ww, fma(m1, v, m0 * u));
+        T Gr[5];
         Gr[0] = U[0] * V;
         Gr[1] = fma(U[1], V, p * m0);
         Gr[2] = fma(U[2], V, p * m1);
         Gr[3] = fma(U[3], V, p * m2);
-        Gr[4] = (U[4] + p) * V;
-      }
-      if (r == 0) {
+        Gr[4] = Ep * V;
 #pragma unroll
         for (int n = 0; n < NF; ++n)
 #pragma unroll
-          for (int b = 0; b < L; ++b) acc[n][b] = fma(cE2<T, L, Q>[b * Q + i], Gr[n], acc[n][b]);
-      } else {
-#pragma unroll
-        for (int n = 0; n < NF; ++n)
-#pragma unroll
-          for (int b = 0; b < L; ++b) acc[n][b] = fma(cBw<T, L, Q>[b * Q + i], Gr[n], acc[n][b]);
+          for (int bb = 0; bb < L; ++bb)
+            acc[r][n][bb] = fma(R0 + r == 0 ? cE2<T, L, Q>[bb * Q + i] : cBw<T, L, Q>[bb * Q + i], Gr[n], acc[r][n][bb]);
       }
     }
-    T *dst = sm.slot(s) + C::O_X + r * (C::S_X1 + 1) + jk;
+  }
+  T *dst = sm.slot(s) + C::O_X + jk;
+#pragma unroll
+  for (int r = 0; r < NR; ++r)
 #pragma unroll
     for (int n = 0; n < NF; ++n)
 #pragma unroll
-      for (int b = 0; b < L; ++b) dst[(n * L + b) * Q * Q] = acc[n][b];
+      for (int b = 0; b < L; ++b) dst[(R0 + r) * (C::S_X1 + 1) + (n * L + b) * Q * Q] = acc[r][n][b];
+}
+
+template <class C, int PHYS>
+__device__ __forceinline__ void s2_volume(const Smem2<C> &sm, const StageArgs &a, int tid) {
+  constexpr int Q = C::Q, EPB = C::EPB;
+  // FP64: the columns of one direction fill whole warps (warp-uniform r)
+  constexpr int NDIR = C::MIXED ? 1 : 3, RS = (Q * Q + 31) / 32 * 32, N = NDIR * RS;
+  for (int w = tid; w < EPB * N; w += C::NT) {
+    const int s = w / N, rem = w - s * N, r = rem / RS, jk = rem - r * RS;
+    if (jk >= Q * Q) continue;
+    // the direction is a template argument, so the coefficients stay
+    // constant-bank operands of the FMAs
+    if constexpr (C::MIXED) s2_volume_column<C, 3, 0>(sm, a, s, jk);
+    else if (r == 0) s2_volume_column<C, 1, 0>(sm, a, s, jk);
+    else if (r == 1) s2_volume_column<C, 1, 1>(sm, a, s, jk);
+    else s2_volume_column<C, 1, 2>(sm, a, s, jk);
   }
 }
 
-// ---- phase 7: j-axis pass -------------------------------------------------------
+// ---- interval 5: j-axis pass --------------------------------------------------
 // Y0 = P_j X0 + E_j X1, Y2 = P_j X2   ([n][a][b][k])
 template <class C>
 __device__ __forceinline__ void s2_pass_j(const Smem2<C> &sm, int tid) {
@@ -532,7 +522,7 @@ __device__ __forceinline__ void s2_pass_j(const Smem2<C> &sm, int tid) {
   }
 }
 
-// ---- phase 8: k-axis pass, face terms, update, next modal block ------------
+// ---- interval 6: k-axis pass, face terms, update, next modal block ---------
 template <class C, int PHYS>
 __device__ __forceinline__ void s2_update(const Smem2<C> &sm, const StageArgs &a, int tid) {
   using T = typename C::R;
@@ -658,7 +648,7 @@ __device__ __forceinline__ void s2_update(const Smem2<C> &sm, const StageArgs &a
   }
 }
 
-// ---- phase 9: end values along b (faces 1, 3) and a (faces 4, 2) ------------
+// ---- interval 7: end values along b (faces 1, 3) and a (faces 4, 2) ---------
 template <class C>
 __device__ __forceinline__ void s2_ends_ab(const Smem2<C> &sm, int tid) {
   using T = typename C::R;
@@ -692,7 +682,7 @@ __device__ __forceinline__ void s2_ends_ab(const Smem2<C> &sm, int tid) {
   }
 }
 
-// ---- phase 10: face planes -> Gauss points, stored as the next traces -------
+// ---- intervals 8-9: face planes -> Gauss points, stored as the next traces --
 // pass a: W1[f][n][g][b'] = sum_a' Bg[a'][g] FP[f][n][a'][b']
 template <class C>
 __device__ __forceinline__ void s2_traces_a(const Smem2<C> &sm, int tid) {
@@ -745,14 +735,9 @@ template <class C, int PHYS>
 __device__ __forceinline__ void stage2_tile(const Smem2<C> &sm, const StageArgs &a, int e0, int tid) {
   s2_load<C>(sm, a, e0, tid);
   __syncthreads();
-  s2_face_flux<C, PHYS>(sm, a, tid);
+  s2_interval1<C, PHYS>(sm, a, e0, tid);
   __syncthreads();
-  s2_lift_a<C>(sm, tid);
-  __syncthreads();
-  s2_lift_b<C>(sm, tid);
-  s2_backward_k<C>(sm, tid);
-  __syncthreads();
-  s2_backward_j<C>(sm, tid);
+  s2_interval2<C>(sm, tid);
   __syncthreads();
   s2_backward_i<C>(sm, tid);
   __syncthreads();
