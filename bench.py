@@ -662,7 +662,8 @@ def main():
         if args.precision != "both" and args.variant >= 0:
             pick = args.variant
         _, kind = D.set_variant(pick)
-        tiles[name] = {"variant": pick, "kernel": "stage_pipe_kernel" if kind == 2 else "stage_kernel",
+        tiles[name] = {"variant": pick,
+                       "kernel": {2: "stage_pipe_kernel", 3: "stage2_kernel"}.get(kind, "stage_kernel"),
                        "elements_per_cta": int(rows[pick][0]), "min_ctas_per_sm": int(rows[pick][1]),
                        "threads_per_cta": int(rows[pick][2]), "candidates_us": [round(float(r[3]), 1) for r in rows]}
         doms[name] = D

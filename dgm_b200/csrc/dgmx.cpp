@@ -1404,6 +1404,9 @@ dgmx_status dgmx_autotune(dgmx_domain *d, int reps, double *rows, int cap, int *
   cudaEventDestroy(e1);
   cudaFree(scratch);
   if (st != DGMX_OK) return st;
+  // the timing launches evaluate whatever state the handle holds (possibly
+  // none yet): what they flagged says nothing about the caller's next call
+  if ((st = reset_error_word(d)) != DGMX_OK) return st;
   const KernelOps &chosen_ops = (*vs)[best];
   if ((e = chosen_ops.init(d->tab)) != cudaSuccess) return d->cuda(e, "variant init");
   if (d->mixed()) d->ops_m = &chosen_ops; else d->ops = &chosen_ops;

@@ -244,6 +244,8 @@ VARIANT_CASES = [
     ("euler3d-lf-p4-tvd", 8, 3, (2, 2, 2), 0, 2 * np.pi, 4, "laxfriedrichs", 3, TG, 0.001, 2, 0),
     ("euler3d-lf-p4-lsrk-ragged", 8, 3, (2, 3, 2), 0, 2 * np.pi, 4, "laxfriedrichs", 14, TG, 0.001, 2, 0),
     ("euler3d-roe-p2-lsrk", 8, 3, (3, 3, 2), 0, 2 * np.pi, 2, "roe", 14, TG, 0.002, 2, 0),
+    ("euler3d-lf-p3-lsrk-rotated", 8, 3, (3, 2, 3), 0, 2 * np.pi, 3, "laxfriedrichs", 14, TG, 0.002, 2, 0, True),
+    ("euler3d-lf-p3-mixed", 8, 3, (3, 2, 3), 0, 2 * np.pi, 3, "laxfriedrichs", 14, TG, 0.002, 2, 1),
     ("euler3d-lf-p5-lsrk-rotated", 8, 3, (2, 2, 2), 0, 2 * np.pi, 5, "laxfriedrichs", 14, TG, 0.001, 2, 0, True),
     ("euler3d-roe-p3-rotated", 8, 3, (3, 2, 3), 0, 2 * np.pi, 3, "roe", 14, TG, 0.002, 2, 0, True),
     ("euler3d-roe-p3-mixed-rotated", 8, 3, (3, 2, 3), 0, 2 * np.pi, 3, "roe", 14, TG, 0.002, 2, 1, True),

@@ -89,10 +89,11 @@ def _tgv32(flux, steps):
     assert int(m.qorder[0]) == 5
     P = oracle.Problem(dgm_io.Mesh(3, m.verts, m.con, m.porder, m.qorder), oracle.EULER3D, flux=flux)
     D = dgm_b200.Domain(m, dgm_b200.EULER3D, flux=flux, inttype=dgm_b200.LSRK14)
-    D.autotune(reps=3)     # the tile the benchmark would run
     x, y, z = P.coords()
     f = ics.taylor_green(x, y, z, Ma=0.1)
     dt = cfl_dt(f, 2 * math.pi / n, p, 3)
+    D.set_state(f)
+    D.autotune(reps=3)     # the tile the benchmark would run
     P.set_state(P.project(f))
     D.set_state(f)
     assert P.advance(14, dt, steps) == 0
