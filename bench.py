@@ -540,30 +540,37 @@ def forms(dgm_b200, args):
     specs = serving.ensemble_requests(args.ensemble, seed=0)
     ens = {}
     for name, prec in (("fp64", dgm_b200.FP64), ("mixed", dgm_b200.MIXED)):
-        pool = dgm_b200.Pool(prec)
-        dof = 0
-        t0 = time.perf_counter()
-        for spec in specs:
-            r = serving.build(spec)
-            pool.add(r.mesh, r.physics, r.U0, r.dt, r.t_end)
-            dof += r.dof
-        setup = time.perf_counter() - t0
-        pool.step(3)
-        l0 = pool.launch_count()
-        k = 5
-        t0 = time.perf_counter()
-        pool.step(k)            # returns after the GPU has finished
-        t = time.perf_counter() - t0
-        ens[name] = {"value": dof * 14 * k / t, "unit": UNIT, "ms_per_step": 1e3 * t / k,
-                     "device_bytes": pool.stats()[0], "launches_per_step": (pool.launch_count() - l0) // k,
-                     "admission_s": round(setup, 2)}
-        pool.close()
+        for path in ("fused", "per_arena"):
+            pool = dgm_b200.Pool(prec, fused=path == "fused")
+            dof = 0
+            t0 = time.perf_counter()
+            for spec in specs:
+                r = serving.build(spec)
+                pool.add(r.mesh, r.physics, r.U0, r.dt, r.t_end)
+                dof += r.dof
+            setup = time.perf_counter() - t0
+            pool.step(3)
+            l0 = pool.launch_count()
+            k = 5
+            t0 = time.perf_counter()
+            pool.step(k)            # returns after the GPU has finished
+            t = time.perf_counter() - t0
+            row = {"value": dof * 14 * k / t, "unit": UNIT, "ms_per_step": 1e3 * t / k,
+                   "device_bytes": pool.stats()[0], "launches_per_step": (pool.launch_count() - l0) // k,
+                   "admission_s": round(setup, 2)}
+            pool.close()
+            if path == "fused":
+                ens[name] = row
+            else:
+                ens[name]["per_arena"] = row
     ens["speedup_mixed_vs_fp64"] = ens["mixed"]["value"] / ens["fp64"]["value"]
     ens["config"] = {"solves": args.ensemble, "modal_dof": dof, "physics": "Euler 2-D isentropic vortex, LF",
                      "mesh": "N x N periodic Quad on [-5,5]^2, N ~ U{8..64}", "p": "U{2..7}, q = p+2",
                      "beta": "U[1,5]", "centre": "U[-2,2]^2", "seed": 0,
-                     "launch": "one persistent stage launch per (order) arena per stage, one CUDA graph per "
-                               "arena step, arenas on concurrent streams; tiles autotuned per (physics, p)",
+                     "launch": "one persistent launch per LSRK stage for every order together (the fused "
+                               "multi-order stage kernel over (arena, tile) work items), one CUDA graph per step; "
+                               "'per_arena': one persistent launch per (order) arena per stage, arenas on concurrent "
+                               "streams, tiles autotuned per (physics, p)",
                      "timing": f"{k} steps after 3, host clock around synchronous pool steps"}
     res["ensemble"] = ens
 

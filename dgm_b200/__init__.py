@@ -701,13 +701,19 @@ class Pool:
     """
 
     def __init__(self, precision: int = FP64, flux: str = "laxfriedrichs", gamma: float = 1.4,
-                 budget_bytes: int = 0, autotune: bool = True, device: int = 0):
+                 budget_bytes: int = 0, autotune: bool = True, device: int = 0, fused: bool = True):
+        """fused: the 2-D arenas share one stage launch across orders
+        (dgmx_pool_set_fused); False gives every arena its own launches."""
         p = _PoolParams(precision, FLUX[flux.lower()], device, 1 if autotune else 0, gamma, int(budget_bytes))
         h = ctypes.c_void_p()
         st = _pool_lib().dgmx_pool_create(ctypes.byref(p), ctypes.byref(h))
         if st != 0:
             raise DgmxError(st, "pool creation failed")
         self.h = h
+        if not fused:
+            f = _pool_lib().dgmx_pool_set_fused
+            f.argtypes = [ctypes.c_void_p, ctypes.c_int]
+            self._check(f(self.h, 0))
         self.nf, self.nq = {}, {}
 
     def close(self):

@@ -311,6 +311,24 @@ cudaError_t launch_integrals(int nf, int ne, int ld, double c_d, const double *U
 cudaError_t launch_reference_row(int physics, int nf, double gamma, double phi0, double vol, const double *integ,
                                  double *uref, cudaStream_t s);
 
+// The pools' multi-order stage kernel (fused.cuh): one launch per LSRK stage
+// over (arena, tile) work items of every 2-D arena.
+struct FusedOps {
+  cudaError_t (*init)();                 // tables and attributes, current device
+  int (*blocks_per_sm)();
+  cudaError_t (*launch)(const StageArgs *args, int narena, const int *bodies, const int2 *items,
+                        const int *nitems, int stage, int grid, cudaStream_t s);
+  int (*epb)(int body);                  // elements per tile of a body
+};
+const FusedOps &fused_ops_fp64();
+const FusedOps &fused_ops_mixed();
+// Body of (physics, L, Q) in the fused kernel: Euler 2-D 0..6 and shallow
+// water 7..13 for p = 1..7 at q = p + 2; -1 when it has none.
+inline int fused_body(int physics, int L, int Q) {
+  if ((physics != DGMX_EULER2D && physics != DGMX_SHALLOW) || Q != L + 1 || L < 2 || L > 8) return -1;
+  return (physics == DGMX_SHALLOW ? 7 : 0) + (L - 2);
+}
+
 // What an entry point in another compilation unit needs from a handle.
 struct DomainView {
   const KernelOps *ops;

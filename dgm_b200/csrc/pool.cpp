@@ -11,6 +11,13 @@
 // carries its own step (dts[solve]) and, in the mixed form, its own
 // reference state (uref[solve]).
 //
+// The 2-D arenas (Euler 2-D and shallow water, p = 1..7, q = p + 2) are
+// advanced together by default: one persistent launch of the fused
+// multi-order stage kernel (fused.cuh) per LSRK stage walks a device-side
+// list of (arena, tile) work items, so a step of any mix of orders is 14
+// launches, replayed from one CUDA graph.  Other arenas (3-D Euler, other q)
+// keep their own per-arena launches.
+//
 // Per solve the arithmetic is exactly dgmx_advance's with inttype 14
 // (src/TimeInt.cpp:1989-2013); the last step is shortened to end on t_end.
 #include <algorithm>
@@ -126,6 +133,7 @@ struct PoolSolve {
 struct Arena {
   int phys = 0, L = 0, Q = 0, dim = 0, nf = 0, nfaces = 0, gf = 0, ld = 0, qd = 0;
   bool mixed = false;
+  int body = -1;                      // fused multi-order kernel body, -1: own launches
   Tables1D tab;
   const KernelOps *fops = nullptr;   // FP64 tile: projections
   const KernelOps *sops = nullptr;   // stage tile (FP64 or mixed)
@@ -177,6 +185,18 @@ struct dgmx_pool {
   size_t scratch_n = 0;
   long launches = 0;
   std::string errmsg;
+  // fused multi-order stage kernel for the 2-D arenas
+  bool fused_on = true, fused_ready = false, args_dirty = true, items_dirty = true;
+  const FusedOps *fops = nullptr;
+  cudaStream_t fstream = nullptr;
+  cudaEvent_t fuploaded = nullptr;
+  StageArgs *args_dev = nullptr, *args_pin = nullptr;   // [14][arenas]
+  int args_cap = 0;                                     // arenas the table holds
+  int *bodies_dev = nullptr, *bodies_pin = nullptr;
+  int2 *items_dev = nullptr, *items_pin = nullptr;      // (arena, tile)
+  int *nitems_dev = nullptr, *nitems_pin = nullptr;
+  int items_cap = 0, fgrid = 1;
+  cudaGraphExec_t fgraph = nullptr;
 
   dgmx_status fail(dgmx_status s, const std::string &m) { errmsg = m; return s; }
   dgmx_status cuda(cudaError_t e, const char *what) {
@@ -292,6 +312,29 @@ dgmx_status grow(dgmx_pool *P, Arena &a, int new_cap) {
   a.grid = std::max(1, std::min(new_cap / a.epb, P->nsm * a.sops->blocks_per_sm()));
   if (a.graph) { cudaGraphExecDestroy(a.graph); a.graph = nullptr; }
   a.tiles_dirty = true;
+  P->args_dirty = true;   // the fused kernel's stage arguments hold these pointers
+  return DGMX_OK;
+}
+
+// The fused kernel's stream finishes its work before a caller touches an
+// arena's buffers from the arena stream.
+cudaError_t fused_quiesce(dgmx_pool *P) {
+  return P->fstream ? cudaStreamSynchronize(P->fstream) : cudaSuccess;
+}
+
+// First use of the fused multi-order kernel: its tables and attributes, its
+// stream and the counters of its work list.
+dgmx_status fused_setup(dgmx_pool *P) {
+  if (P->fused_ready) return DGMX_OK;
+  P->fops = P->prm.precision == DGMX_MIXED ? &fused_ops_mixed() : &fused_ops_fp64();
+  cudaError_t e = P->fops->init();
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&P->fstream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->fuploaded, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = dalloc(&P->nitems_dev, (size_t)1);
+  if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void **>(&P->nitems_pin), sizeof(int), cudaHostAllocDefault);
+  if (e != cudaSuccess) return P->cuda(e, "fused kernel setup");
+  P->fgrid = std::max(1, P->nsm * P->fops->blocks_per_sm());
+  P->fused_ready = true;
   return DGMX_OK;
 }
 
@@ -314,9 +357,19 @@ dgmx_status get_arena(dgmx_pool *P, int phys, int L, int Q, Arena **out) {
   const size_t fixed = sizeof(GeomClass) * kClassCap + sizeof(int) * kPermCap +
                        sizeof(double) * (kUrefStride + 1) * kSlotCap + 8;
   if (!P->fits(fixed)) return P->fail(DGMX_ERR_MEMORY, "pool budget exceeded");
-  const int v = P->prm.autotune ? tuned_variant(phys, mixed, L, Q, P->prm.gamma, P->prm.flux, P->prm.device) : -1;
-  a->sops = (v >= 0 && v < (int)vs->size()) ? &(*vs)[v] : &(*vs)[0];
-  a->epb = a->sops->epb;
+  a->body = P->fused_on ? fused_body(phys, L, Q) : -1;
+  if (a->body >= 0) {
+    // the fused kernel's body of this (physics, p, q) steps the arena; the
+    // plain default tile supplies its trace and projection kernels
+    dgmx_status st = fused_setup(P);
+    if (st != DGMX_OK) return st;
+    a->sops = &(*vs)[0];
+    a->epb = P->fops->epb(a->body);
+  } else {
+    const int v = P->prm.autotune ? tuned_variant(phys, mixed, L, Q, P->prm.gamma, P->prm.flux, P->prm.device) : -1;
+    a->sops = (v >= 0 && v < (int)vs->size()) ? &(*vs)[v] : &(*vs)[0];
+    a->epb = a->sops->epb;
+  }
   a->tab = make_tables(L, Q, Q - 1);
   cudaError_t e = a->fops->init(a->tab);
   if (e == cudaSuccess) e = a->sops->init(a->tab);
@@ -558,7 +611,8 @@ dgmx_status add_impl(dgmx_pool *P, const dgmx_mesh *m, int phys, const double *U
     fill_reference_row(phys, P->prm.gamma, std::pow(a.tab.B[0], a.dim), ref);
   }
   // uploads (the arena stream is idle between steps)
-  cudaError_t e = cudaStreamSynchronize(a.stream);
+  cudaError_t e = fused_quiesce(P);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(a.stream);
   auto up = [&](void *dst, const void *src, size_t bytes) {
     if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, a.stream);
   };
@@ -604,6 +658,7 @@ dgmx_status add_impl(dgmx_pool *P, const dgmx_mesh *m, int phys, const double *U
   P->solves[sv.id] = sv;
   a.live.push_back(sv.id);
   a.tiles_dirty = true;
+  if (a.body >= 0) P->items_dirty = true;
   *id = sv.id;
   return DGMX_OK;
 }
@@ -611,25 +666,143 @@ dgmx_status add_impl(dgmx_pool *P, const dgmx_mesh *m, int phys, const double *U
 // The step a live solve takes next (shortened to land on t_end).
 double next_dt(const PoolSolve &s) { return std::min(s.dt, s.t_end - s.t); }
 
+// Work list and stage arguments of the fused kernel, uploaded on its stream
+// when the fused arenas' membership or buffers changed.
+dgmx_status fused_upload(dgmx_pool *P) {
+  cudaError_t e = cudaSuccess;
+  const int narena = (int)P->arenas.size();
+  if (P->items_dirty) {
+    cudaEventSynchronize(P->fuploaded);
+    // arenas of higher order (more work per tile) first, so the short tiles
+    // fill the end of each stage
+    std::vector<int> order;
+    for (int ai = 0; ai < narena; ++ai) if (P->arenas[ai]->body >= 0) order.push_back(ai);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+      return (size_t)P->arenas[x]->nf * P->arenas[x]->qd * P->arenas[x]->epb >
+             (size_t)P->arenas[y]->nf * P->arenas[y]->qd * P->arenas[y]->epb;
+    });
+    std::vector<int2> items;
+    for (int ai : order) {
+      const Arena &a = *P->arenas[ai];
+      for (int id : a.live) {
+        const PoolSolve &sv = P->solves[id];
+        for (int t = sv.e0 / a.epb; t < (sv.e0 + sv.nalloc) / a.epb; ++t) items.push_back(make_int2(ai, t));
+      }
+    }
+    if ((int)items.size() > P->items_cap) {
+      const int cap = std::max<int>((int)items.size(), 2 * P->items_cap);
+      if (P->items_dev) cudaFree(P->items_dev);
+      if (P->items_pin) cudaFreeHost(P->items_pin);
+      P->items_dev = nullptr; P->items_pin = nullptr; P->items_cap = 0;
+      e = dalloc(&P->items_dev, (size_t)cap);
+      if (e == cudaSuccess)
+        e = cudaHostAlloc(reinterpret_cast<void **>(&P->items_pin), sizeof(int2) * cap, cudaHostAllocDefault);
+      if (e != cudaSuccess) return P->cuda(e, "fused work list");
+      P->items_cap = cap;
+      if (P->fgraph) { cudaGraphExecDestroy(P->fgraph); P->fgraph = nullptr; }
+    }
+    std::copy(items.begin(), items.end(), P->items_pin);
+    *P->nitems_pin = (int)items.size();
+    if (!items.empty())
+      e = cudaMemcpyAsync(P->items_dev, P->items_pin, sizeof(int2) * items.size(), cudaMemcpyHostToDevice, P->fstream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(P->nitems_dev, P->nitems_pin, sizeof(int), cudaMemcpyHostToDevice, P->fstream);
+    if (e != cudaSuccess) return P->cuda(e, "fused work list");
+    P->items_dirty = false;
+  }
+  if (P->args_dirty) {
+    cudaEventSynchronize(P->fuploaded);
+    if (narena > P->args_cap) {
+      const int cap = std::max(narena, 2 * P->args_cap);
+      void *old[] = {P->args_dev, P->bodies_dev};
+      for (void *q : old) if (q) cudaFree(q);
+      if (P->args_pin) cudaFreeHost(P->args_pin);
+      if (P->bodies_pin) cudaFreeHost(P->bodies_pin);
+      P->args_dev = nullptr; P->bodies_dev = nullptr; P->args_pin = nullptr; P->bodies_pin = nullptr; P->args_cap = 0;
+      e = dalloc(&P->args_dev, (size_t)14 * cap);
+      if (e == cudaSuccess) e = dalloc(&P->bodies_dev, (size_t)cap);
+      if (e == cudaSuccess)
+        e = cudaHostAlloc(reinterpret_cast<void **>(&P->args_pin), sizeof(StageArgs) * 14 * cap, cudaHostAllocDefault);
+      if (e == cudaSuccess)
+        e = cudaHostAlloc(reinterpret_cast<void **>(&P->bodies_pin), sizeof(int) * cap, cudaHostAllocDefault);
+      if (e != cudaSuccess) return P->cuda(e, "fused stage arguments");
+      P->args_cap = cap;
+      if (P->fgraph) { cudaGraphExecDestroy(P->fgraph); P->fgraph = nullptr; }
+    }
+    std::memset(P->args_pin, 0, sizeof(StageArgs) * 14 * P->args_cap);
+    for (int ai = 0; ai < P->args_cap; ++ai) P->bodies_pin[ai] = -1;
+    for (int ai = 0; ai < narena; ++ai) {
+      const Arena &a = *P->arenas[ai];
+      if (a.body < 0) continue;
+      P->bodies_pin[ai] = a.body;
+      StageArgs g = arena_args(P, a);
+      g.kind = kLSRK; g.X = a.U; g.U = a.U; g.Ut = a.Ut; g.Utf = a.Utf; g.dts = a.dts;
+      for (int k = 0; k < 14; ++k) {
+        const int tc = (a.tcur + k) & 1;
+        g.c0 = kLsrkA[k]; g.c1 = kLsrkB[k];
+        g.Tin = a.T[tc]; g.Tout = a.T[tc ^ 1]; g.Tinf = a.Tf[tc]; g.Toutf = a.Tf[tc ^ 1];
+        P->args_pin[(size_t)k * P->args_cap + ai] = g;
+      }
+    }
+    e = cudaMemcpyAsync(P->args_dev, P->args_pin, sizeof(StageArgs) * 14 * P->args_cap, cudaMemcpyHostToDevice,
+                        P->fstream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(P->bodies_dev, P->bodies_pin, sizeof(int) * P->args_cap, cudaMemcpyHostToDevice, P->fstream);
+    if (e != cudaSuccess) return P->cuda(e, "fused stage arguments");
+    P->args_dirty = false;
+  }
+  return DGMX_OK;
+}
+
+// One LSRK14 step of every fused arena: 14 launches of the fused kernel.
+dgmx_status fused_capture(dgmx_pool *P) {
+  if (P->fgraph) { cudaGraphExecDestroy(P->fgraph); P->fgraph = nullptr; }
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(P->fstream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return P->cuda(e, "graph capture");
+  for (int k = 0; k < 14 && e == cudaSuccess; ++k)
+    e = P->fops->launch(P->args_dev, P->args_cap, P->bodies_dev, P->items_dev, P->nitems_dev, k, P->fgrid, P->fstream);
+  const cudaError_t e2 = cudaStreamEndCapture(P->fstream, &g);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&P->fgraph, g, 0);
+  if (g) cudaGraphDestroy(g);
+  return P->cuda(e, "graph capture");
+}
+
 dgmx_status step_impl(dgmx_pool *P, int nsteps) {
   for (int k = 0; k < nsteps; ++k) {
-    bool any = false;
+    bool any = false, fused_any = false;
     for (auto &ap : P->arenas) {
       Arena &a = *ap;
+      const bool fz = a.body >= 0;
+      // a fused arena whose membership changed (solves finished, joined or
+      // left, possibly all of them) changes the fused kernel's work list
+      if (fz && a.tiles_dirty) { P->items_dirty = true; a.tiles_dirty = false; }
       if (a.live.empty()) continue;
       any = true;
+      cudaEvent_t up_ev = fz ? P->fuploaded : a.uploaded;
       // per-solve steps, and the tile list when membership changed; the
       // pinned staging is rewritten only after its last copy has run
       for (int id : a.live) {
         const PoolSolve &s = P->solves[id];
         const double h = next_dt(s);
         if (a.dts_pin[s.slot] != h) {
-          if (!a.dts_dirty) cudaEventSynchronize(a.uploaded);
+          if (!a.dts_dirty) cudaEventSynchronize(up_ev);
           a.dts_dirty = true;
           a.dts_pin[s.slot] = h;
         }
       }
       cudaError_t e = cudaSuccess;
+      if (fz) {
+        // stepped below by the fused kernel, from its own work list
+        if (a.dts_dirty) {
+          e = cudaMemcpyAsync(a.dts, a.dts_pin, sizeof(double) * a.next_slot, cudaMemcpyHostToDevice, P->fstream);
+          a.dts_dirty = false;
+        }
+        if (e != cudaSuccess) return P->cuda(e, "pool upload");
+        fused_any = true;
+        continue;
+      }
       if (a.tiles_dirty) {
         cudaEventSynchronize(a.uploaded);
         std::vector<int> tl;
@@ -656,6 +829,15 @@ dgmx_status step_impl(dgmx_pool *P, int nsteps) {
       if ((e = cudaGraphLaunch(a.graph, a.stream)) != cudaSuccess) return P->cuda(e, "graph launch");
       P->launches += 14;
     }
+    if (fused_any) {
+      dgmx_status st = fused_upload(P);
+      if (st != DGMX_OK) return st;
+      cudaError_t e = cudaEventRecord(P->fuploaded, P->fstream);
+      if (e != cudaSuccess) return P->cuda(e, "pool upload");
+      if (!P->fgraph && (st = fused_capture(P)) != DGMX_OK) return st;
+      if ((e = cudaGraphLaunch(P->fgraph, P->fstream)) != cudaSuccess) return P->cuda(e, "graph launch");
+      P->launches += 14;
+    }
     if (!any) break;
     // host time keeping; solves that reach t_end leave the tile list
     for (auto &ap : P->arenas) {
@@ -679,6 +861,10 @@ dgmx_status step_impl(dgmx_pool *P, int nsteps) {
     }
   }
   dgmx_status st = DGMX_OK;
+  if (P->fstream) {
+    const cudaError_t e = cudaStreamSynchronize(P->fstream);
+    if (e != cudaSuccess) return P->cuda(e, "pool step");
+  }
   for (size_t i = 0; i < P->arenas.size(); ++i) {
     cudaError_t e = cudaStreamSynchronize(P->arenas[i]->stream);
     if (e != cudaSuccess) return P->cuda(e, "pool step");
@@ -714,8 +900,16 @@ dgmx_status dgmx_pool_create(const dgmx_pool_params *params, dgmx_pool **out) {
 dgmx_status dgmx_pool_destroy(dgmx_pool *p) {
   if (!p) return DGMX_ERR_ARGUMENT;
   cudaSetDevice(p->prm.device);
+  if (p->fstream) cudaStreamSynchronize(p->fstream);
   for (auto &a : p->arenas) free_arena(*a);
   if (p->scratch) cudaFree(p->scratch);
+  if (p->fgraph) cudaGraphExecDestroy(p->fgraph);
+  void *dev[] = {p->args_dev, p->bodies_dev, p->items_dev, p->nitems_dev};
+  for (void *q : dev) if (q) cudaFree(q);
+  void *pin[] = {p->args_pin, p->bodies_pin, p->items_pin, p->nitems_pin};
+  for (void *q : pin) if (q) cudaFreeHost(q);
+  if (p->fuploaded) cudaEventDestroy(p->fuploaded);
+  if (p->fstream) cudaStreamDestroy(p->fstream);
   delete p;
   return DGMX_OK;
 }
@@ -779,7 +973,8 @@ dgmx_status dgmx_pool_get_state(dgmx_pool *p, int id, double *U) {
   if (st != DGMX_OK) return st;
   StageArgs g = arena_args(p, a);
   g.ne = s.ne; g.gclass = a.gclass + s.e0; g.esolve = a.esolve + s.e0;
-  cudaError_t e = cudaStreamSynchronize(a.stream);
+  cudaError_t e = fused_quiesce(p);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(a.stream);
   if (e == cudaSuccess) e = a.fops->backward(g, a.U + (size_t)s.e0 * a.nf * a.ld, p->scratch, a.stream);
   ++p->launches;
   if (e == cudaSuccess) e = cudaMemcpyAsync(U, p->scratch, sizeof(double) * nodal, cudaMemcpyDeviceToHost, a.stream);
@@ -804,14 +999,15 @@ dgmx_status dgmx_pool_remove(dgmx_pool *p, int id) {
   cudaSetDevice(p->prm.device);
   const PoolSolve s = it->second;
   Arena &a = *p->arenas[s.arena];
-  cudaError_t e = cudaStreamSynchronize(a.stream);
+  cudaError_t e = fused_quiesce(p);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(a.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(a.gclass + s.e0, 0xff, sizeof(int) * (size_t)s.nalloc, a.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(a.stream);
   if (e != cudaSuccess) return p->cuda(e, "remove");
   give_range(a, s.e0, s.nalloc);
   a.free_slots.push_back(s.slot);
   auto lv = std::find(a.live.begin(), a.live.end(), id);
-  if (lv != a.live.end()) { a.live.erase(lv); a.tiles_dirty = true; }
+  if (lv != a.live.end()) { a.live.erase(lv); a.tiles_dirty = true; if (a.body >= 0) p->items_dirty = true; }
   p->solves.erase(it);
   return DGMX_OK;
 }
@@ -834,6 +1030,13 @@ dgmx_status dgmx_pool_stats(dgmx_pool *p, size_t *bytes, int *resident, int *act
 }
 
 long dgmx_pool_launch_count(const dgmx_pool *p) { return p ? p->launches : 0; }
+
+dgmx_status dgmx_pool_set_fused(dgmx_pool *p, int on) {
+  if (!p) return DGMX_ERR_ARGUMENT;
+  if (!p->arenas.empty()) return p->fail(DGMX_ERR_ARGUMENT, "the stepping path is chosen before the first solve");
+  p->fused_on = on != 0;
+  return DGMX_OK;
+}
 
 const char *dgmx_pool_last_error(const dgmx_pool *p) { return p ? p->errmsg.c_str() : "null pool"; }
 

@@ -37,7 +37,9 @@ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 // One kernel tile: PHYS physics, L modes and Q GLL points per direction,
 // EPB elements per CTA, MINB CTAs per SM requested from the register
 // allocator (__launch_bounds__ minimum blocks; 0 = no request).
-template <int PHYS, int L_, int Q_, int EPB_, int MINB_ = 0, bool MIXED_ = false>
+// NT_ (nonzero) fixes the CTA's thread count, for kernels that run several
+// tiles' bodies under one launch shape.
+template <int PHYS, int L_, int Q_, int EPB_, int MINB_ = 0, bool MIXED_ = false, int NT_ = 0>
 struct Cfg {
   // working precision: FP64, or FP32 for the mixed form (the solution
   // register U stays FP64 in global memory)
@@ -52,7 +54,7 @@ struct Cfg {
   static constexpr int NFACE = 2 * DIM;
   static constexpr int LD = Pow<L, DIM>::v, QD = Pow<Q, DIM>::v;
   static constexpr int GF = Pow<G, DIM - 1>::v, QF = Pow<Q, DIM - 1>::v, LF = Pow<L, DIM - 1>::v;
-  static constexpr int NT = cmax(64, ((EPB * QD + 31) / 32) * 32 > 1024 ? 1024 : ((EPB * QD + 31) / 32) * 32);
+  static constexpr int NT = NT_ > 0 ? NT_ : cmax(64, ((EPB * QD + 31) / 32) * 32 > 1024 ? 1024 : ((EPB * QD + 31) / 32) * 32);
   // per-slot region sizes (doubles)
   // Rows of an even number of values are stored at an odd pitch in shared
   // memory, so the pencils a warp reads (one per lane, K apart) fall on

@@ -11,9 +11,13 @@
  * dgmx_advance (dgmx.h) with inttype 14.
  *
  * Solves of equal (physics, p, q) share one set of device arrays (an
- * "arena"); an RK stage is one persistent kernel launch per arena that
- * walks a device-side tile list, so solves join and leave between steps
- * without re-capturing the per-step CUDA graph.  Solves never interact:
+ * "arena").  The 2-D arenas (Euler 2-D and shallow water, p = 1..7,
+ * q = p + 2) are stepped together: an RK stage is ONE persistent kernel
+ * launch that walks a device-side list of (arena, tile) work items and runs
+ * each with the stage body of its order, so a step of any mix of orders is
+ * 14 launches replayed from one CUDA graph; other arenas launch their own
+ * persistent stage kernel over their tile list.  Solves join and leave
+ * between steps without re-capturing the graphs.  Solves never interact:
  * each result is the same alone and in any mix.
  *
  * Layouts are those of dgmx.h: initial values and states are GLL values in
@@ -81,7 +85,14 @@ dgmx_status dgmx_pool_remove(dgmx_pool *p, int id);
  * degrees of freedom (fields x elements x (p+1)^d) of the unfinished ones. */
 dgmx_status dgmx_pool_stats(dgmx_pool *p, size_t *bytes, int *resident, int *active, long long *dof_active);
 
-/* Stage-kernel launches issued so far (14 per arena per step). */
+/* The stepping path of the 2-D arenas: 1 (default) one fused launch per
+ * stage across orders, 0 one launch per arena per stage.  Only before the
+ * first solve or prepare (DGMX_ERR_ARGUMENT afterwards).  No counterpart in
+ * the reference. */
+dgmx_status dgmx_pool_set_fused(dgmx_pool *p, int on);
+
+/* Stage-kernel launches issued so far (14 per step for the fused 2-D arenas
+ * together, plus 14 per other arena). */
 long dgmx_pool_launch_count(const dgmx_pool *p);
 
 const char *dgmx_pool_last_error(const dgmx_pool *p);

@@ -164,3 +164,53 @@ def test_nonphysical_state_names_its_solve():
     with pytest.raises(dgm_b200.NonPhysicalState, match=f"solve {bad}"):
         pool.step(1)
     assert pool.info(good)[1] == 1
+
+
+def _order_mix():
+    """Euler 2-D vortices at p = 2..7 and shallow-water bumps at p = 2, 3
+    (q = p + 2), one solve each, of uneven sizes."""
+    cases = []
+    for k, p in enumerate(range(2, 8)):
+        n = (3 + k % 3, 4 + k % 2)
+        cases.append((f"vortex-p{p}", 1, 2, n, -5, 5, p, IV if k % 2 else IV2, 0.004, 0.02))
+    cases.append(("bump-p2", 30, 2, (5, 4), -2, 2, 2, GB, 0.001, 0.004))
+    cases.append(("bump-p3", 30, 2, (3, 6), -2, 2, 3, GB, 0.001, 0.004))
+    return cases
+
+
+def test_fused_multi_order_launch_is_one_per_stage():
+    """The 2-D arenas of every order step together: 14 launches per step
+    (one per LSRK stage) whatever the mix of orders and physics; the same
+    pool stepped per arena issues 14 per arena."""
+    import dgm_b200
+    cases = _order_mix()
+    counts = {}
+    for fused in (True, False):
+        pool = dgm_b200.Pool(dgm_b200.FP64, fused=fused)
+        for c in cases:
+            m, _, f = mesh_ic(c)
+            pool.add(m, c[1], f, c[8], c[9])
+        pool.step(1)
+        l0 = pool.launch_count()
+        pool.step(2)
+        counts[fused] = (pool.launch_count() - l0) // 2
+        pool.close()
+    arenas = len({(c[1], c[6]) for c in cases})
+    assert counts[True] == 14, counts
+    assert counts[False] == 14 * arenas, counts
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "mixed"])
+def test_fused_and_per_arena_paths_agree(precision):
+    """One fused launch per stage across orders gives each solve the result
+    of its own arena's launches (the same stage body per element)."""
+    import dgm_b200
+    cases = _order_mix()
+    states = {}
+    for fused in (True, False):
+        pool = dgm_b200.Pool(precision, fused=fused)
+        ids = run_pool(pool, cases)
+        states[fused] = {name: pool.state(sid) for name, sid in ids.items()}
+        pool.close()
+    for name in states[True]:
+        assert rel(states[True][name], states[False][name]) <= (1e-14 if precision == 0 else 1e-6), name
