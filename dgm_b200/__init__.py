@@ -759,6 +759,18 @@ class Pool:
     def step(self, nsteps: int = 1):
         self._check(_pool_lib().dgmx_pool_step(self.h, int(nsteps)))
 
+    def step_async(self, nsteps: int = 1):
+        """Enqueue nsteps steps and return; admission may overlap them.
+        Call sync() before finished(), state() or remove()."""
+        f = _pool_lib().dgmx_pool_step_async
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        self._check(f(self.h, int(nsteps)))
+
+    def sync(self):
+        f = _pool_lib().dgmx_pool_sync
+        f.argtypes = [ctypes.c_void_p]
+        self._check(f(self.h))
+
     def finished(self):
         buf = (ctypes.c_int * 4096)()
         out, n = [], ctypes.c_int()

@@ -197,6 +197,7 @@ struct dgmx_pool {
   int *nitems_dev = nullptr, *nitems_pin = nullptr;
   int items_cap = 0, fgrid = 1;
   cudaGraphExec_t fgraph = nullptr;
+  bool unsynced = false;              // steps enqueued since the last sync
 
   dgmx_status fail(dgmx_status s, const std::string &m) { errmsg = m; return s; }
   dgmx_status cuda(cudaError_t e, const char *what) {
@@ -263,6 +264,11 @@ cudaError_t alloc_elems(const Arena &a, int cap, ElemArrays &x) {
 dgmx_status grow(dgmx_pool *P, Arena &a, int new_cap) {
   const size_t more = (size_t)(new_cap - a.cap) * a.elem_bytes();
   if (!P->fits(more)) return P->fail(DGMX_ERR_MEMORY, "pool budget exceeded");
+  // the arrays are copied and freed: no step may be reading them
+  if (P->fstream) {
+    const cudaError_t q = cudaStreamSynchronize(P->fstream);
+    if (q != cudaSuccess) return P->cuda(q, "arena growth");
+  }
   ElemArrays x;
   cudaError_t e = alloc_elems(a, new_cap, x);
   if (e != cudaSuccess) return P->cuda(e, "arena allocation");
@@ -610,9 +616,11 @@ dgmx_status add_impl(dgmx_pool *P, const dgmx_mesh *m, int phys, const double *U
     }
     fill_reference_row(phys, P->prm.gamma, std::pow(a.tab.B[0], a.dim), ref);
   }
-  // uploads (the arena stream is idle between steps)
-  cudaError_t e = fused_quiesce(P);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(a.stream);
+  // uploads on the arena stream.  A fused step in flight does not touch the
+  // slots, classes, permutations and solve rows written here (none of them
+  // is on its work list yet), so admission overlaps it; a per-arena step in
+  // flight finishes first (it runs on this stream).
+  cudaError_t e = cudaStreamSynchronize(a.stream);
   auto up = [&](void *dst, const void *src, size_t bytes) {
     if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, a.stream);
   };
@@ -769,7 +777,25 @@ dgmx_status fused_capture(dgmx_pool *P) {
   return P->cuda(e, "graph capture");
 }
 
-dgmx_status step_impl(dgmx_pool *P, int nsteps) {
+// Waits for every enqueued step and reads the arenas' error words.
+dgmx_status sync_impl(dgmx_pool *P) {
+  dgmx_status st = DGMX_OK;
+  if (P->fstream) {
+    const cudaError_t e = cudaStreamSynchronize(P->fstream);
+    if (e != cudaSuccess) return P->cuda(e, "pool step");
+  }
+  for (size_t i = 0; i < P->arenas.size(); ++i) {
+    cudaError_t e = cudaStreamSynchronize(P->arenas[i]->stream);
+    if (e != cudaSuccess) return P->cuda(e, "pool step");
+    const dgmx_status s2 = check_arena_error(P, (int)i);
+    if (s2 != DGMX_OK && st == DGMX_OK) st = s2;
+  }
+  P->unsynced = false;
+  return st;
+}
+
+dgmx_status step_impl(dgmx_pool *P, int nsteps, bool sync) {
+  P->unsynced = true;
   for (int k = 0; k < nsteps; ++k) {
     bool any = false, fused_any = false;
     for (auto &ap : P->arenas) {
@@ -860,18 +886,7 @@ dgmx_status step_impl(dgmx_pool *P, int nsteps) {
       a.live.swap(keep);
     }
   }
-  dgmx_status st = DGMX_OK;
-  if (P->fstream) {
-    const cudaError_t e = cudaStreamSynchronize(P->fstream);
-    if (e != cudaSuccess) return P->cuda(e, "pool step");
-  }
-  for (size_t i = 0; i < P->arenas.size(); ++i) {
-    cudaError_t e = cudaStreamSynchronize(P->arenas[i]->stream);
-    if (e != cudaSuccess) return P->cuda(e, "pool step");
-    const dgmx_status s2 = check_arena_error(P, (int)i);
-    if (s2 != DGMX_OK && st == DGMX_OK) st = s2;
-  }
-  return st;
+  return sync ? sync_impl(P) : DGMX_OK;
 }
 
 }  // namespace
@@ -946,14 +961,31 @@ dgmx_status dgmx_pool_step(dgmx_pool *p, int nsteps) {
   if (!p || nsteps < 0) return DGMX_ERR_ARGUMENT;
   try {
     cudaSetDevice(p->prm.device);
-    return step_impl(p, nsteps);
+    return step_impl(p, nsteps, true);
   } catch (...) {
     return p->fail(DGMX_ERR_MEMORY, "host allocation failed");
   }
 }
 
+dgmx_status dgmx_pool_step_async(dgmx_pool *p, int nsteps) {
+  if (!p || nsteps < 0) return DGMX_ERR_ARGUMENT;
+  try {
+    cudaSetDevice(p->prm.device);
+    return step_impl(p, nsteps, false);
+  } catch (...) {
+    return p->fail(DGMX_ERR_MEMORY, "host allocation failed");
+  }
+}
+
+dgmx_status dgmx_pool_sync(dgmx_pool *p) {
+  if (!p) return DGMX_ERR_ARGUMENT;
+  cudaSetDevice(p->prm.device);
+  return sync_impl(p);
+}
+
 dgmx_status dgmx_pool_finished(dgmx_pool *p, int *ids, int cap, int *n) {
   if (!p || !n || (cap > 0 && !ids)) return DGMX_ERR_ARGUMENT;
+  if (p->unsynced) return p->fail(DGMX_ERR_ARGUMENT, "steps are still in flight: call dgmx_pool_sync first");
   const int k = std::max(0, std::min(cap, (int)p->finished_queue.size()));
   for (int i = 0; i < k; ++i) ids[i] = p->finished_queue[i];
   p->finished_queue.erase(p->finished_queue.begin(), p->finished_queue.begin() + k);

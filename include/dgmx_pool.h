@@ -71,7 +71,18 @@ dgmx_status dgmx_pool_add(dgmx_pool *p, const dgmx_mesh *mesh, int physics, cons
  * dgmx_pool_last_error; the other solves' steps are complete. */
 dgmx_status dgmx_pool_step(dgmx_pool *p, int nsteps);
 
-/* Ids of solves that reached their end time since the previous call. */
+/* dgmx_pool_step without the wait: the steps are enqueued (one CUDA graph
+ * per step) and the call returns, so the caller can admit new solves while
+ * they run (admission into the fused 2-D arenas does not wait for a step in
+ * flight unless an arena has to grow).  dgmx_pool_sync waits for them and
+ * reports what dgmx_pool_step would have.  dgmx_pool_finished, get_state
+ * and remove need the steps synced.  No counterpart in the reference. */
+dgmx_status dgmx_pool_step_async(dgmx_pool *p, int nsteps);
+dgmx_status dgmx_pool_sync(dgmx_pool *p);
+
+/* Ids of solves that reached their end time since the previous call
+ * (DGMX_ERR_ARGUMENT while steps enqueued by dgmx_pool_step_async are not
+ * synced). */
 dgmx_status dgmx_pool_finished(dgmx_pool *p, int *ids, int cap, int *n);
 
 /* Current GLL values of a solve (Field layout), its time and step count. */

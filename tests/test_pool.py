@@ -214,3 +214,34 @@ def test_fused_and_per_arena_paths_agree(precision):
         pool.close()
     for name in states[True]:
         assert rel(states[True][name], states[False][name]) <= (1e-14 if precision == 0 else 1e-6), name
+
+
+def test_async_steps_overlap_admission_with_the_same_results():
+    """Steps enqueued without a wait (dgmx_pool_step_async) while new solves
+    are admitted give each solve the result of the synchronous sequence;
+    finished() asks for the sync first."""
+    import dgm_b200
+    first, second = SOLVES[0], SOLVES[2]
+    res = {}
+    for mode in ("sync", "async"):
+        pool = dgm_b200.Pool(dgm_b200.FP64)
+        m0, _, f0 = mesh_ic(first)
+        a = pool.add(m0, first[1], f0, first[8], first[9])
+        m1, _, f1 = mesh_ic(second)
+        if mode == "sync":
+            pool.step(1)
+            b = pool.add(m1, second[1], f1, second[8], second[9])
+        else:
+            pool.step_async(1)
+            b = pool.add(m1, second[1], f1, second[8], second[9])   # while the step runs
+            with pytest.raises(dgm_b200.DgmxError):
+                pool.finished()
+            pool.sync()
+        for _ in range(20):
+            pool.step(1)
+            if pool.stats()[2] == 0:
+                break
+        res[mode] = (pool.state(a), pool.state(b))
+        pool.close()
+    assert np.array_equal(res["sync"][0], res["async"][0])
+    assert np.array_equal(res["sync"][1], res["async"][1])
