@@ -485,6 +485,20 @@ def other_configs(dgm_b200, args, only=None):
             "rel_l2_vs_fp64_per_field": [rel_l2(a, b) for a, b in zip(D.state(), U64)],
             "kinetic_energy_rel_diff_vs_fp64": abs(ke32[-1] - ke[-1]) / ke[-1],
             "kinetic_energy_max_rel_diff_vs_fp64": max(abs(a - b) / b for a, b in zip(ke32, ke))}
+        # the same with the viscous kernels' 1-D contractions as 3xTF32
+        # tensor-core products
+        D.set_tensor_contractions(True)
+        D.set_state(U0)
+        D.advance(dt, 3)
+        D.set_state(U0)
+        ttc, ketc = timed_steps(D)
+        res["ns3d_tgv_3xtf32_viscous"] = {
+            "workload": "ns3d_taylor_green_24^3_p7_q9_re1600_pr0.71_roe_lsrk14", "steps_timed": k3,
+            "value": dof * 14 * k3 / ttc, "unit": UNIT, "ms_per_step": 1e3 * ttc / k3,
+            "rel_l2_vs_fp64_per_field": [rel_l2(a, b) for a, b in zip(D.state(), U64)],
+            "kinetic_energy_rel_diff_vs_fp64": abs(ketc[-1] - ke[-1]) / ke[-1],
+            "note": "FP32 viscous kernels with their contractions on the tensor cores (mma.sync m16n8k8 TF32, "
+                    "3 products per contraction: small x big + big x small + big x big)"}
         D.close()
     if only in (None, "channel"):
         # the reference's channel regression case (runs/chan: NS 3-D, 512 hexes, p=3,

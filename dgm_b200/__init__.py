@@ -433,6 +433,13 @@ class Domain:
         self._check(f(self.h, int(index), ctypes.byref(n), ctypes.byref(w)))
         return n.value, int(w.value)
 
+    def set_tensor_contractions(self, on: bool):
+        """Navier-Stokes 3-D, p >= 5, FP32 viscous form: 3xTF32 tensor-core
+        contractions in the viscous kernels (dgmx_set_tensor_contractions)."""
+        f = lib().dgmx_set_tensor_contractions
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        self._check(f(self.h, 1 if on else 0))
+
     def set_wait_limit(self, tries: int):
         """Fault injection for tests: bound the prefetching stage kernel's
         first wait per tile to `tries` (0: every wait runs out, the call

@@ -115,6 +115,7 @@ struct dgmx_domain {
   // Navier-Stokes with precision = DGMX_MIXED: the BR1 viscous kernels run in
   // FP32 (from the uncapped tile vops); stage, registers and traces stay FP64
   bool visc32 = false;
+  bool visc_tc = false;     // the FP32 viscous kernels' contractions on the tensor cores (3xTF32)
   const KernelOps *vops = nullptr;
   // element partition: ghost slots in the trace buffers and the halo
   // exchange lists (plan.nranks == 1: the whole mesh, no exchange)
@@ -202,9 +203,11 @@ struct dgmx_domain {
   }
   bool ns() const { return prm.physics == DGMX_NS2D || prm.physics == DGMX_NS3D; }
   cudaError_t ns_grad(const StageArgs &a, bool nodal, cudaStream_t s) const {
+    if (visc32 && visc_tc) return vops->ns_grad32tc(a, nodal, s);
     return visc32 ? vops->ns_grad32(a, nodal, s) : ops->ns_grad(a, nodal, s);
   }
   cudaError_t ns_visc(const StageArgs &a, bool nodal, cudaStream_t s) const {
+    if (visc32 && visc_tc) return vops->ns_visc32tc(a, nodal, s);
     return visc32 ? vops->ns_visc32(a, nodal, s) : ops->ns_visc(a, nodal, s);
   }
   bool mixed() const { return prm.precision == DGMX_MIXED; }
@@ -1413,6 +1416,16 @@ dgmx_status dgmx_autotune(dgmx_domain *d, int reps, double *rows, int cap, int *
   if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
   if (nvariants) *nvariants = (int)vs->size();
   if (chosen) *chosen = best;
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_set_tensor_contractions(dgmx_domain *d, int on) {
+  if (!d) return DGMX_ERR_ARGUMENT;
+  if (on && (!d->visc32 || !d->vops || !d->vops->ns_grad32tc))
+    return d->fail(DGMX_ERR_UNSUPPORTED, "tensor-core contractions run in the FP32 viscous form (precision "
+                                         "DGMX_MIXED) of Navier-Stokes 3-D at p >= 5");
+  d->visc_tc = on != 0;
+  if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
   return DGMX_OK;
 }
 

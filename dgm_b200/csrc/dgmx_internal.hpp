@@ -297,6 +297,10 @@ struct KernelOps {
   // uncapped tile of each (physics, L, Q, EPB)
   cudaError_t (*ns_grad32)(const StageArgs &a, bool nodal, cudaStream_t s) = nullptr;
   cudaError_t (*ns_visc32)(const StageArgs &a, bool nodal, cudaStream_t s) = nullptr;
+  // the FP32 viscous kernels with 3xTF32 tensor-core contractions (3-D,
+  // p >= 5)
+  cudaError_t (*ns_grad32tc)(const StageArgs &a, bool nodal, cudaStream_t s) = nullptr;
+  cudaError_t (*ns_visc32tc)(const StageArgs &a, bool nodal, cudaStream_t s) = nullptr;
 };
 void register_ops(int physics, int L, int Q, const KernelOps &ops);
 const KernelOps *find_ops(int physics, int L, int Q);            // default variant

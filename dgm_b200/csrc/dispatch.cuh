@@ -66,6 +66,9 @@ static cudaError_t upload_tables2_lq(const Tables1D &t) {
 template <int PHYS, int L, int Q, int EPB, int MINB, bool MIXED = false>
 struct Launch {
   using C = Cfg<PHYS, L, Q, EPB, MINB, MIXED>;
+  // 3xTF32 tensor-core contractions in the FP32 viscous kernels: 3-D
+  // Navier-Stokes at p >= 5 (1-D operators of at least 7 x 7)
+  static constexpr bool kTensorViscous = PHYS == DGMX_NS3D && L >= 6;
   static dim3 grid(int ne) { return dim3((unsigned)((ne + EPB - 1) / EPB)); }
   static cudaError_t init(const Tables1D &t) {
     cudaError_t e = upload_tables_lq<L, Q, typename C::R>(t);
@@ -97,6 +100,12 @@ struct Launch {
       if ((e = cudaFuncSetAttribute(ns_grad_kernel<C, PHYS, true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
       if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
       if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+      if constexpr (kTensorViscous) {
+        if ((e = cudaFuncSetAttribute(ns_grad_kernel<C, PHYS, false, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
+        if ((e = cudaFuncSetAttribute(ns_grad_kernel<C, PHYS, true, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
+        if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, false, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+        if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, true, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+      }
     }
     return cudaSuccess;
   }
@@ -115,6 +124,26 @@ struct Launch {
       using N = NsCfg<C, float>;
       if (nodal) ns_visc_kernel<C, PHYS, true, float><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
       else ns_visc_kernel<C, PHYS, false, float><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
+  }
+  static cudaError_t ns_grad32tc(const StageArgs &a, bool nodal, cudaStream_t s) {
+    if constexpr (is_ns(PHYS) && !MIXED && MINB == 0 && kTensorViscous) {
+      using N = NsCfg<C, float>;
+      if (nodal) ns_grad_kernel<C, PHYS, true, float, true><<<grid(a.ne), C::NT, N::Grad::SMEM, s>>>(a);
+      else ns_grad_kernel<C, PHYS, false, float, true><<<grid(a.ne), C::NT, N::Grad::SMEM, s>>>(a);
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
+  }
+  static cudaError_t ns_visc32tc(const StageArgs &a, bool nodal, cudaStream_t s) {
+    if constexpr (is_ns(PHYS) && !MIXED && MINB == 0 && kTensorViscous) {
+      using N = NsCfg<C, float>;
+      if (nodal) ns_visc_kernel<C, PHYS, true, float, true><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
+      else ns_visc_kernel<C, PHYS, false, float, true><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;
@@ -200,6 +229,9 @@ struct Launch {
     o.rhs_nodal = rhs_nodal; o.forward = forward; o.backward = backward;
     if constexpr (is_ns(PHYS) && !MIXED) { o.ns_grad = ns_grad; o.ns_visc = ns_visc; }
     if constexpr (is_ns(PHYS) && !MIXED && MINB == 0) { o.ns_grad32 = ns_grad32; o.ns_visc32 = ns_visc32; }
+    if constexpr (is_ns(PHYS) && !MIXED && MINB == 0 && kTensorViscous) {
+      o.ns_grad32tc = ns_grad32tc; o.ns_visc32tc = ns_visc32tc;
+    }
     return o;
   }
 };

@@ -88,6 +88,107 @@ __device__ __forceinline__ void contract(const T *__restrict__ in, T *__restrict
   }
 }
 
+// ------------------------------------------------- tensor-core contraction
+// The same contraction as `contract` (FP32 data) on the tensor cores:
+// rows = pencils of all batches, one 16-pencil tile per warp at a time,
+// out[16 x N] = in[16 x K] M[K x N] as mma.sync m16n8k8 TF32 products with
+// FP32 accumulation, K and N padded to multiples of 8 with zeros.  Each
+// operand is split into a TF32 part and the TF32 rounding of its remainder
+// (3xTF32: a b ~ a_s b_b + a_b b_s + a_b b_b, the small products first), so
+// the products keep about FP32 accuracy.  Fragment layouts of m16n8k8.tf32
+// (g = lane / 4, c = lane % 4): A (row g | g + 8, col c | c + 4), B (row c |
+// c + 4, col g), D (row g | g + 8, col 2c, 2c + 1).
+__device__ __forceinline__ unsigned tf32_rna(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void tf32_split(float x, unsigned &big, unsigned &small) {
+  big = tf32_rna(x);
+  small = tf32_rna(x - __uint_as_float(big));
+}
+__device__ __forceinline__ void mma_tf32_16x8x8(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+template <int I0, int I1, int I2, int AX, int K, int N, class M, bool ACC, int IS0 = -1, int IS1 = -1,
+          int OS0 = -1, int OS1 = -1>
+__device__ __forceinline__ void contract_tc(const float *__restrict__ in, float *__restrict__ out, int nbatch,
+                                            int sin, int sout, int tid, int nthr) {
+  constexpr int O1 = AX == 1 ? N : I1, O2 = AX == 2 ? N : I2;
+  constexpr int P0 = AX == 0 ? I1 : I0;
+  constexpr int P1 = AX == 2 ? I1 : I2;
+  constexpr int NP = P0 * P1;
+  constexpr int is1 = IS1 >= 0 ? IS1 : I2, is0 = IS0 >= 0 ? IS0 : I1 * is1;
+  constexpr int os1 = OS1 >= 0 ? OS1 : O2, os0 = OS0 >= 0 ? OS0 : O1 * os1;
+  constexpr int isA = AX == 0 ? is0 : (AX == 1 ? is1 : 1);
+  constexpr int osA = AX == 0 ? os0 : (AX == 1 ? os1 : 1);
+  constexpr int KS = (K + 7) / 8, NS = (N + 7) / 8;
+  const int lane = tid & 31, g = lane >> 2, c = lane & 3;
+  // the operator's fragments, split once per call
+  unsigned bb[KS][NS][2], bs[KS][NS][2];
+#pragma unroll
+  for (int ks = 0; ks < KS; ++ks)
+#pragma unroll
+    for (int ns = 0; ns < NS; ++ns)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int k = ks * 8 + c + 4 * h, n = ns * 8 + g;
+        const float v = (k < K && n < N) ? M::get(k, n) : 0.0f;
+        tf32_split(v, bb[ks][ns][h], bs[ks][ns][h]);
+      }
+  const int rows = nbatch * NP;
+  for (int t0 = (tid >> 5) * 16; t0 < rows; t0 += (nthr >> 5) * 16) {
+    int io[2], oo[2];
+    size_t ib[2], ob[2];
+    bool ok[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int w = t0 + g + 8 * h;
+      ok[h] = w < rows;
+      const int b = ok[h] ? w / NP : 0, p = ok[h] ? w - b * NP : 0;
+      const int pa = p / P1, pb = p - pa * P1;
+      if (AX == 0) { io[h] = pa * is1 + pb; oo[h] = pa * os1 + pb; }
+      else if (AX == 1) { io[h] = pa * is0 + pb; oo[h] = pa * os0 + pb; }
+      else { io[h] = pa * is0 + pb * is1; oo[h] = pa * os0 + pb * os1; }
+      ib[h] = (size_t)b * sin; ob[h] = (size_t)b * sout;
+    }
+    float acc[NS][4];
+#pragma unroll
+    for (int ns = 0; ns < NS; ++ns)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[ns][q] = 0.0f;
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks) {
+      unsigned ab[4], as[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int h = q & 1, k = ks * 8 + c + 4 * (q >> 1);
+        const float v = (ok[h] && k < K) ? in[ib[h] + io[h] + k * isA] : 0.0f;
+        tf32_split(v, ab[q], as[q]);
+      }
+#pragma unroll
+      for (int ns = 0; ns < NS; ++ns) {
+        mma_tf32_16x8x8(acc[ns], as, bb[ks][ns][0], bb[ks][ns][1]);
+        mma_tf32_16x8x8(acc[ns], ab, bs[ks][ns][0], bs[ks][ns][1]);
+        mma_tf32_16x8x8(acc[ns], ab, bb[ks][ns][0], bb[ks][ns][1]);
+      }
+    }
+#pragma unroll
+    for (int ns = 0; ns < NS; ++ns)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int h = q >> 1, n = ns * 8 + 2 * c + (q & 1);
+        if (!ok[h] || n >= N) continue;
+        float *dst = out + ob[h] + oo[h] + n * osA;
+        if (ACC) *dst += acc[ns][q]; else *dst = acc[ns][q];
+      }
+  }
+}
+
 // ------------------------------------------------------------------ physics
 // Positivity threshold aepsM = eps^(2/3) (src/Constants.hpp:43).
 __device__ constexpr double kAeps = 4.8148248609680896e-11;

@@ -23,6 +23,18 @@ namespace dgmx {
 
 constexpr bool is_ns(int p) { return p == DGMX_NS2D || p == DGMX_NS3D; }
 
+// A contraction of the viscous kernels: with TC, FP32 data and an operator
+// of at least 5 x 5, on the tensor cores (contract_tc, 3xTF32); otherwise
+// on the CUDA cores (contract).
+template <bool TC, int I0, int I1, int I2, int AX, int K, int N, class M, bool ACC, class T, int IS0 = -1,
+          int IS1 = -1, int OS0 = -1, int OS1 = -1>
+__device__ __forceinline__ void vcontract(const T *in, T *out, int nbatch, int sin, int sout, int tid, int nthr) {
+  if constexpr (TC && std::is_same<T, float>::value && K >= 5 && N >= 5)
+    contract_tc<I0, I1, I2, AX, K, N, M, ACC, IS0, IS1, OS0, OS1>(in, out, nbatch, sin, sout, tid, nthr);
+  else
+    contract<I0, I1, I2, AX, K, N, M, ACC, T, IS0, IS1, OS0, OS1>(in, out, nbatch, sin, sout, tid, nthr);
+}
+
 // Bytes of a viscous kernel's value regions, rounded up to 8: the geometry
 // slots that follow hold doubles, and an odd number of float values would
 // leave them on a 4-byte boundary (a no-op for double values).
@@ -165,16 +177,16 @@ __device__ __forceinline__ void load_nbr_traces(V *E2, const double *T, const Fa
 
 // G2GL of NB face-major arrays [f][slot][b][GF] and accumulation with the
 // inverse end weights into dst [slot][b][QD] (faces in increasing order).
-template <class C, int NB, class V>
+template <class C, int NB, class V, bool TC = false>
 __device__ __forceinline__ void lift_batch(const V *Fg, V *LFc, V *S, V *dst, int tid) {
   constexpr int DIM = C::DIM, L = C::L, Q = C::Q, G = C::G, EPB = C::EPB, QD = C::QD, QF = C::QF;
   constexpr int NBT = C::NFACE * EPB * NB;
   if constexpr (DIM == 3) {
-    contract<G, G, 1, 0, G, Q, MatG2GL<L, Q, V>, false>(Fg, S, NBT, G * G, Q * G, tid, C::NT);
+    vcontract<TC, G, G, 1, 0, G, Q, MatG2GL<L, Q, V>, false>(Fg, S, NBT, G * G, Q * G, tid, C::NT);
     __syncthreads();
-    contract<Q, G, 1, 1, G, Q, MatG2GL<L, Q, V>, false>(S, LFc, NBT, Q * G, Q * Q, tid, C::NT);
+    vcontract<TC, Q, G, 1, 1, G, Q, MatG2GL<L, Q, V>, false>(S, LFc, NBT, Q * G, Q * Q, tid, C::NT);
   } else {
-    contract<G, 1, 1, 0, G, Q, MatG2GL<L, Q, V>, false>(Fg, LFc, NBT, G, Q, tid, C::NT);
+    vcontract<TC, G, 1, 1, 0, G, Q, MatG2GL<L, Q, V>, false>(Fg, LFc, NBT, G, Q, tid, C::NT);
   }
   __syncthreads();
   const V w0 = V(1.0) / cW<V, L, Q>[0], w1 = V(1.0) / cW<V, L, Q>[Q - 1];
@@ -205,7 +217,7 @@ __device__ __forceinline__ void lift_batch(const V *Fg, V *LFc, V *S, V *dst, in
 
 // w-weighted projection of NB arrays [slot][b][QD] (weighted in place) to
 // modal dst [slot][b][LD].
-template <class C, int NB, class V>
+template <class C, int NB, class V, bool TC = false>
 __device__ __forceinline__ void forward_batch(V *src, V *dst, V *S1, V *S2, int tid) {
   constexpr int DIM = C::DIM, L = C::L, Q = C::Q, QD = C::QD, LD = C::LD, NBT = C::EPB * NB;
   for (int w = tid; w < NBT * QD; w += C::NT) {
@@ -217,33 +229,33 @@ __device__ __forceinline__ void forward_batch(V *src, V *dst, V *S1, V *S2, int 
   }
   __syncthreads();
   if constexpr (DIM == 3) {
-    contract<Q, Q, Q, 0, Q, L, MatBt<L, Q, V>, false>(src, S1, NBT, QD, L * Q * Q, tid, C::NT);
+    vcontract<TC, Q, Q, Q, 0, Q, L, MatBt<L, Q, V>, false>(src, S1, NBT, QD, L * Q * Q, tid, C::NT);
     __syncthreads();
-    contract<L, Q, Q, 1, Q, L, MatBt<L, Q, V>, false>(S1, S2, NBT, L * Q * Q, L * L * Q, tid, C::NT);
+    vcontract<TC, L, Q, Q, 1, Q, L, MatBt<L, Q, V>, false>(S1, S2, NBT, L * Q * Q, L * L * Q, tid, C::NT);
     __syncthreads();
-    contract<L, L, Q, 2, Q, L, MatBt<L, Q, V>, false>(S2, dst, NBT, L * L * Q, LD, tid, C::NT);
+    vcontract<TC, L, L, Q, 2, Q, L, MatBt<L, Q, V>, false>(S2, dst, NBT, L * L * Q, LD, tid, C::NT);
   } else {
-    contract<Q, Q, 1, 0, Q, L, MatBt<L, Q, V>, false>(src, S1, NBT, QD, L * Q, tid, C::NT);
+    vcontract<TC, Q, Q, 1, 0, Q, L, MatBt<L, Q, V>, false>(src, S1, NBT, QD, L * Q, tid, C::NT);
     __syncthreads();
-    contract<L, Q, 1, 1, Q, L, MatBt<L, Q, V>, false>(S1, dst, NBT, L * Q, LD, tid, C::NT);
+    vcontract<TC, L, Q, 1, 1, Q, L, MatBt<L, Q, V>, false>(S1, dst, NBT, L * Q, LD, tid, C::NT);
   }
   __syncthreads();
 }
 
 // modal [slot][b][LD] -> GLL [slot][b][QD]
-template <class C, int NB, class V>
+template <class C, int NB, class V, bool TC = false>
 __device__ __forceinline__ void backward_batch(const V *src, V *dst, V *S1, V *S2, int tid) {
   constexpr int L = C::L, Q = C::Q, NBT = C::EPB * NB;
   if constexpr (C::DIM == 3) {
-    contract<L, L, L, 0, L, Q, MatB<L, Q, V>, false>(src, S1, NBT, C::LD, Q * L * L, tid, C::NT);
+    vcontract<TC, L, L, L, 0, L, Q, MatB<L, Q, V>, false>(src, S1, NBT, C::LD, Q * L * L, tid, C::NT);
     __syncthreads();
-    contract<Q, L, L, 1, L, Q, MatB<L, Q, V>, false>(S1, S2, NBT, Q * L * L, Q * Q * L, tid, C::NT);
+    vcontract<TC, Q, L, L, 1, L, Q, MatB<L, Q, V>, false>(S1, S2, NBT, Q * L * L, Q * Q * L, tid, C::NT);
     __syncthreads();
-    contract<Q, Q, L, 2, L, Q, MatB<L, Q, V>, false>(S2, dst, NBT, Q * Q * L, C::QD, tid, C::NT);
+    vcontract<TC, Q, Q, L, 2, L, Q, MatB<L, Q, V>, false>(S2, dst, NBT, Q * Q * L, C::QD, tid, C::NT);
   } else {
-    contract<L, L, 1, 0, L, Q, MatB<L, Q, V>, false>(src, S1, NBT, C::LD, Q * L, tid, C::NT);
+    vcontract<TC, L, L, 1, 0, L, Q, MatB<L, Q, V>, false>(src, S1, NBT, C::LD, Q * L, tid, C::NT);
     __syncthreads();
-    contract<Q, L, 1, 1, L, Q, MatB<L, Q, V>, false>(S1, dst, NBT, Q * L, C::QD, tid, C::NT);
+    vcontract<TC, Q, L, 1, 1, L, Q, MatB<L, Q, V>, false>(S1, dst, NBT, Q * L, C::QD, tid, C::NT);
   }
   __syncthreads();
 }
@@ -336,7 +348,7 @@ __device__ __forceinline__ void load_state_shifted(float *dst, double *Rs, const
 // ---------------------------------------------------------------- gradients
 // V: working type (double, or float for the FP32 viscous form); inputs and
 // outputs in global memory stay double.
-template <class C, int PHYS, bool NODAL, class V = double>
+template <class C, int PHYS, bool NODAL, class V = double, bool TC = false>
 __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::GRAD_MINB) ns_grad_kernel(StageArgs a) {
   using N = NsCfg<C, V>;
   using R = typename N::Grad;
@@ -368,10 +380,10 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::GRAD_MINB) ns_grad_kernel(
   if constexpr (!NODAL) {
     __syncthreads();
     if constexpr (N::NB1 == NF) {
-      backward_batch<C, NF>(A, B, S1, S2, tid);
+      backward_batch<C, NF, V, TC>(A, B, S1, S2, tid);
     } else {   // one slot: fields [0, NB1) then [NB1, NF)
-      backward_batch<C, N::NB1>(A, B, S1, S2, tid);
-      backward_batch<C, NF - N::NB1>(A + N::NB1 * LD, B + N::NB1 * QD, S1, S2, tid);
+      backward_batch<C, N::NB1, V, TC>(A, B, S1, S2, tid);
+      backward_batch<C, NF - N::NB1, V, TC>(A + N::NB1 * LD, B + N::NB1 * QD, S1, S2, tid);
     }
   }
   __syncthreads();
@@ -428,10 +440,10 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::GRAD_MINB) ns_grad_kernel(
     __syncthreads();
     // collocation derivatives along r, s, t
     using Sh = Sh3<DIM, Q>;
-    contract<Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<L, Q, V>, false>(Qc, Gd, EPB, QD, DIM * QD, tid, C::NT);
-    contract<Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<L, Q, V>, false>(Qc, Gd + QD, EPB, QD, DIM * QD, tid, C::NT);
+    vcontract<TC, Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<L, Q, V>, false>(Qc, Gd, EPB, QD, DIM * QD, tid, C::NT);
+    vcontract<TC, Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<L, Q, V>, false>(Qc, Gd + QD, EPB, QD, DIM * QD, tid, C::NT);
     if constexpr (DIM == 3)
-      contract<Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<L, Q, V>, false>(Qc, Gd + 2 * QD, EPB, QD, DIM * QD, tid, C::NT);
+      vcontract<TC, Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<L, Q, V>, false>(Qc, Gd + 2 * QD, EPB, QD, DIM * QD, tid, C::NT);
     __syncthreads();
     // chain rule (src/Hex.cpp:1994-2006): d/dx = rx d/dr + sx d/ds + tx d/dt
     for (int w = tid; w < EPB * QD; w += C::NT) {
@@ -448,8 +460,8 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::GRAD_MINB) ns_grad_kernel(
       }
     }
     __syncthreads();
-    lift_batch<C, DIM>(Fc, LFc, S1, Gd, tid);
-    forward_batch<C, DIM>(Gd, S2, S1, LFc, tid);
+    lift_batch<C, DIM, V, TC>(Fc, LFc, S1, Gd, tid);
+    forward_batch<C, DIM, V, TC>(Gd, S2, S1, LFc, tid);
     for (int w = tid; w < EPB * DIM * LD; w += C::NT) {
       const int s = w / (DIM * LD), rem = w - s * DIM * LD;
       const int e = e0 + s;
@@ -460,7 +472,7 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::GRAD_MINB) ns_grad_kernel(
 }
 
 // ----------------------------------------------- stresses, traces, divergence
-template <class C, int PHYS, bool NODAL, class V = double>
+template <class C, int PHYS, bool NODAL, class V = double, bool TC = false>
 __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::VISC_MINB) ns_visc_kernel(StageArgs a) {
   using N = NsCfg<C, V>;
   using R = typename N::Visc;
@@ -483,10 +495,10 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::VISC_MINB) ns_visc_kernel(
     load_modal_v<C>(Gg, a.X, e0, a.ne, tid);  // modal input parked in the gradient region
     __syncthreads();
     if constexpr (N::NB1 == NF) {
-      backward_batch<C, NF>(Gg, B, S1, S2, tid);
+      backward_batch<C, NF, V, TC>(Gg, B, S1, S2, tid);
     } else {   // one slot: fields [0, NB1) then [NB1, NF)
-      backward_batch<C, N::NB1>(Gg, B, S1, S2, tid);
-      backward_batch<C, NF - N::NB1>(Gg + N::NB1 * LD, B + N::NB1 * QD, S1, S2, tid);
+      backward_batch<C, N::NB1, V, TC>(Gg, B, S1, S2, tid);
+      backward_batch<C, NF - N::NB1, V, TC>(Gg + N::NB1 * LD, B + N::NB1 * QD, S1, S2, tid);
     }
   }
   __syncthreads();
@@ -499,7 +511,7 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::VISC_MINB) ns_visc_kernel(
       Gh[w] = e < a.ne ? V(a.Ghat[((size_t)e * NVC + c) * DIM * LD + rem]) : V(0.0);
     }
     __syncthreads();
-    backward_batch<C, DIM>(Gh, Dv, S1, S2, tid);
+    backward_batch<C, DIM, V, TC>(Gh, Dv, S1, S2, tid);
     if (c < DIM) {
       for (int w = tid; w < EPB * DIM * QD; w += C::NT) {
         const int s = w / (DIM * QD), rem = w - s * DIM * QD;
@@ -587,11 +599,11 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::VISC_MINB) ns_visc_kernel(
     __syncthreads();
     constexpr int NB = NFACE * EPB * DIM;
     if constexpr (DIM == 3) {
-      contract<Q, Q, 1, 0, Q, G, MatGL2G<L, Q, V>, false>(FF, S1, NB, Q * Q, G * Q, tid, C::NT);
+      vcontract<TC, Q, Q, 1, 0, Q, G, MatGL2G<L, Q, V>, false>(FF, S1, NB, Q * Q, G * Q, tid, C::NT);
       __syncthreads();
-      contract<G, Q, 1, 1, Q, G, MatGL2G<L, Q, V>, false>(S1, Fg, NB, G * Q, G * G, tid, C::NT);
+      vcontract<TC, G, Q, 1, 1, Q, G, MatGL2G<L, Q, V>, false>(S1, Fg, NB, G * Q, G * G, tid, C::NT);
     } else {
-      contract<Q, 1, 1, 0, Q, G, MatGL2G<L, Q, V>, false>(FF, Fg, NB, Q, G, tid, C::NT);
+      vcontract<TC, Q, 1, 1, 0, Q, G, MatGL2G<L, Q, V>, false>(FF, Fg, NB, Q, G, tid, C::NT);
     }
     __syncthreads();
     // g_n . n (own normals), the viscous trace of this side
@@ -618,13 +630,13 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::VISC_MINB) ns_visc_kernel(
       }
       __syncthreads();
       using Sh = Sh3<DIM, Q>;
-      if (r == 0) contract<Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<L, Q, V>, false>(Cv, Dv, EPB, QD, QD, tid, C::NT);
-      else if (r == 1) contract<Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<L, Q, V>, true>(Cv, Dv, EPB, QD, QD, tid, C::NT);
-      else contract<Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<L, Q, V>, true>(Cv, Dv, EPB, QD, QD, tid, C::NT);
+      if (r == 0) vcontract<TC, Sh::a, Sh::b, Sh::c, 0, Q, Q, MatD<L, Q, V>, false>(Cv, Dv, EPB, QD, QD, tid, C::NT);
+      else if (r == 1) vcontract<TC, Sh::a, Sh::b, Sh::c, 1, Q, Q, MatD<L, Q, V>, true>(Cv, Dv, EPB, QD, QD, tid, C::NT);
+      else vcontract<TC, Sh::a, Sh::b, Sh::c, 2, Q, Q, MatD<L, Q, V>, true>(Cv, Dv, EPB, QD, QD, tid, C::NT);
       __syncthreads();
     }
     // projected divergence of this field
-    forward_batch<C, 1>(Dv, S2, S1, FF, tid);
+    forward_batch<C, 1, V, TC>(Dv, S2, S1, FF, tid);
     for (int w = tid; w < EPB * LD; w += C::NT) {
       const int s = w / LD, m = w - s * LD;
       const int e = e0 + s;

@@ -290,6 +290,14 @@ long dgmx_launch_count(const dgmx_domain *d);
  * counterpart in the reference. */
 dgmx_status dgmx_measure_fma_peak(int device, int fp64, int reps, double *tflops);
 
+/* The FP32 viscous form of Navier-Stokes 3-D at p >= 5 (precision
+ * DGMX_MIXED): on = 1 runs the 1-D contractions of its two viscous kernels
+ * on the tensor cores as 3xTF32 products (each operand split into a TF32
+ * part and the TF32 rounding of its remainder, three mma.sync products
+ * summed in FP32), on = 0 on the CUDA cores (the default).  No counterpart
+ * in the reference, which contracts in FP64 (src/Hex.cpp:2030-2071). */
+dgmx_status dgmx_set_tensor_contractions(dgmx_domain *d, int on);
+
 /* Fault-injection hook for tests of failure detection (no counterpart in
  * the reference).  Bounds the number of tries of the prefetching stage
  * kernel's first wait for a tile's inputs; a wait that runs out sets bit 1

@@ -148,8 +148,12 @@ def stage_weight_rss(inttype):
     return float(np.sqrt(np.sum(np.square(w))))
 
 
-@pytest.mark.parametrize("case", NS32_CASES, ids=[c[0] for c in NS32_CASES])
-def test_navier_stokes_fp32_viscous_form(case):
+NS32_RUNS = [(c, False) for c in NS32_CASES] + [(NS32_CASES[0], True)]
+
+
+@pytest.mark.parametrize("case,tensor", NS32_RUNS,
+                         ids=[c[0] + ("-3xtf32" if t else "") for c, t in NS32_RUNS])
+def test_navier_stokes_fp32_viscous_form(case, tensor):
     """precision = MIXED for Navier-Stokes runs the BR1 gradient and viscous
     kernels in FP32 (stage kernel, registers and traces FP64).  Measured
     against the viscous contribution alone (momentum vector, energy): the
@@ -157,11 +161,15 @@ def test_navier_stokes_fp32_viscous_form(case):
     the FP64 path, and one step (modal path) within TOL_VISC32 times the
     scheme's stage-weight factor; the FP64 path's own parity with the oracle
     is checked on the same step.  Low-Mach Taylor-Green (E/rho ~ 180 against
-    |u|^2/2 ~ 0.5) is the case that needs the mean-shifted internal energy."""
+    |u|^2/2 ~ 0.5) is the case that needs the mean-shifted internal energy.
+    `tensor`: the viscous kernels' contractions as 3xTF32 tensor-core
+    products (p >= 5), held to the same bars."""
     import dgm_b200
     _, phys, ephys, dim, n, lo, hi, p, q, inttype, dt, vis = case
     m = dgm_b200.meshgen.box(dim, n, lo, hi, p, q)
     D32 = dgm_b200.Domain(m, phys, flux="roe", inttype=inttype, vis=vis, precision=dgm_b200.MIXED)
+    if tensor:
+        D32.set_tensor_contractions(True)
     D64 = dgm_b200.Domain(m, phys, flux="roe", inttype=inttype, vis=vis)
     D0 = dgm_b200.Domain(m, ephys, flux="roe", inttype=inttype)
     P = oracle.Problem(dgm_io.Mesh(m.dim, m.verts, m.con, m.porder, m.qorder), phys, flux="roe", vis=vis)
