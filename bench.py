@@ -75,8 +75,9 @@ def parse():
                     help="time one form only (profiling runs); the default line needs both")
     ap.add_argument("--ns-steps", type=int, default=10,
                     help="steps of the Navier-Stokes Taylor-Green leg (1000 for the full history)")
-    ap.add_argument("--only", choices=["vortex2d", "ns3d_tgv", "channel"], default=None,
-                    help="run one of the other configurations alone and print its JSON (profiling)")
+    ap.add_argument("--only", choices=["vortex2d", "ns3d_tgv", "channel", "ensemble"], default=None,
+                    help="run one of the other configurations (or the batched ensemble) alone and print its "
+                         "JSON (profiling)")
     ap.add_argument("--variant", type=int, default=-1,
                     help="single-form runs: use this tile variant instead of the autotuner's pick")
     return ap.parse_args()
@@ -547,8 +548,9 @@ def other_configs(dgm_b200, args, only=None):
     return res
 
 
-def forms(dgm_b200, args):
-    """The batched ensemble and the serving trace on this GPU (pool path)."""
+def forms(dgm_b200, args, serve=True):
+    """The batched ensemble and (serve) the serving trace on this GPU (pool
+    path)."""
     from dgm_b200 import serving
     res = {}
     specs = serving.ensemble_requests(args.ensemble, seed=0)
@@ -587,6 +589,8 @@ def forms(dgm_b200, args):
                                "streams, tiles autotuned per (physics, p)",
                      "timing": f"{k} steps after 3, host clock around synchronous pool steps"}
     res["ensemble"] = ens
+    if not serve:
+        return res
 
     trace = serving.poisson_trace(args.trace, rate=200.0, seed=1)
     reqs = [serving.build(s) for s in trace]
@@ -654,7 +658,9 @@ def main():
     torch.cuda.set_device(local)
     if args.only:
         if rank == 0:
-            print(json.dumps(other_configs(dgm_b200, args, args.only)), flush=True)
+            res = forms(dgm_b200, args, serve=False) if args.only == "ensemble" else \
+                other_configs(dgm_b200, args, args.only)
+            print(json.dumps(res), flush=True)
         return 0
     dist = None
     if world > 1:
