@@ -351,20 +351,37 @@ void reg2_variant() {
     register_ops(PHYS + (MIXED ? kMixedKey : 0), P + 1, Q, Launch2<PHYS, P + 1, Q, EPB, NT, MINB, MIXED>::ops());
 }
 
+// CTAs per SM of NT threads that a cap of R registers per thread allows: a
+// warp's registers come from one of the SM's four 16K-register scheduler
+// partitions, so ceil(warps / 4) warps of 32 x R registers share 16K;
+// clipped to what the tile's shared memory allows.
+template <class C>
+constexpr int blocks_for_regs(int nt, int r) {
+  const int per_part = 16384 / (32 * r), warps = (nt + 31) / 32;
+  const int by_regs = per_part * 4 / warps;
+  const int by_smem = (int)((228 * 1024) / (C::SMEM + 1024));
+  return by_regs < by_smem ? by_regs : by_smem;
+}
+
 // Second-form variants of a 3-D Euler (p, q): one element per CTA at two
-// thread counts, uncapped and with register caps near 96 and 80 registers
-// per thread (the CTAs per SM such caps allow).
+// thread counts, uncapped and with the CTAs per SM that caps of 96 and 80
+// (and for the FP32 form 64) registers per thread allow.
 template <int PHYS, int P, int Q, bool MIXED = false>
 void reg2() {
   constexpr int NTA = ((P + 1) * (P + 1) * 5 + 31) / 32 * 32;   // one thread per modal row
   constexpr int NTB = NTA + 32;
+  using CA = Cfg2<PHYS, P + 1, Q, 1, NTA, 0, MIXED>;
+  using CB = Cfg2<PHYS, P + 1, Q, 1, NTB, 0, MIXED>;
+  constexpr int A96 = blocks_for_regs<CA>(NTA, 96), A80 = blocks_for_regs<CA>(NTA, 80);
+  constexpr int B96 = blocks_for_regs<CB>(NTB, 96), B80 = blocks_for_regs<CB>(NTB, 80);
+  constexpr int B64 = blocks_for_regs<CB>(NTB, 64);
   reg2_variant<PHYS, P, Q, 1, NTA, 0, MIXED>();
   reg2_variant<PHYS, P, Q, 1, NTB, 0, MIXED>();
-  if constexpr (65536 / (NTB * 96) >= 2) reg2_variant<PHYS, P, Q, 1, NTB, 65536 / (NTB * 96), MIXED>();
-  if constexpr (65536 / (NTA * 96) >= 2) reg2_variant<PHYS, P, Q, 1, NTA, 65536 / (NTA * 96), MIXED>();
-  if constexpr (65536 / (NTB * 80) >= 2 && 65536 / (NTB * 80) != 65536 / (NTB * 96))
-    reg2_variant<PHYS, P, Q, 1, NTB, 65536 / (NTB * 80), MIXED>();
-  if constexpr (MIXED && 65536 / (NTB * 64) >= 2) reg2_variant<PHYS, P, Q, 1, NTB, 65536 / (NTB * 64), MIXED>();
+  if constexpr (B96 >= 2) reg2_variant<PHYS, P, Q, 1, NTB, B96, MIXED>();
+  if constexpr (A96 >= 2) reg2_variant<PHYS, P, Q, 1, NTA, A96, MIXED>();
+  if constexpr (B80 >= 2 && B80 != B96) reg2_variant<PHYS, P, Q, 1, NTB, B80, MIXED>();
+  if constexpr (A80 >= 2 && A80 != A96) reg2_variant<PHYS, P, Q, 1, NTA, A80, MIXED>();
+  if constexpr (MIXED && B64 >= 2 && B64 != B80) reg2_variant<PHYS, P, Q, 1, NTB, B64, MIXED>();
 }
 
 template <int PHYS, int P, int Q, int EPB, int MINB, bool MIXED>

@@ -57,18 +57,27 @@ struct Cfg2 {
   // odd pitches for rows of an even length
   static constexpr int PL = L % 2 == 0 ? L + 1 : L;   // modal rows (and face-plane rows of L)
   static constexpr int PE = GF % 2 == 0 ? GF + 1 : GF;   // one (face, field) block of face terms
+  // block pitches chosen for the passes that read or write across blocks:
+  // XLS (one (face, field) block of lifted terms, odd: the lift writes one
+  // value per block), FPS (one face plane, = L (mod 16) for L = 4: the
+  // trace pass reads column b' of a block, L per block), XS (one X row of
+  // Q x Q, = Q (mod 32): the j-pass reads Q consecutive k per row)
+  static constexpr int XLS = (L * PL) % 2 == 0 ? L * PL + 1 : L * PL;
+  static constexpr int FPS = L * PL;
+  static constexpr int XS = Q * Q + ((Q - Q * Q) % 32 + 32) % 32 <= Q * Q + Q * Q / 2
+                                ? Q * Q + ((Q - Q * Q) % 32 + 32) % 32 : Q * Q;
   // region sizes (values of R)
   static constexpr int S_EF = NFACE * NF * PE;          // face terms [f][n][g h], padded blocks
-  static constexpr int S_XL = NFACE * NF * L * PL;      // lifted-projected face terms [f][n][a'][b'] padded
+  static constexpr int S_XL = NFACE * NF * XLS;         // lifted-projected face terms [f][n][a'][b'] padded
   static constexpr int S_T1 = NF * L * L * Q;           // [n][a][b][k]
   static constexpr int S_T2 = NF * L * Q * Q;           // [n][a][j][k]
   static constexpr int S_UN = NF * Q * Q * Q;           // nodal values [n][i][j][k]
-  static constexpr int S_X1 = NF * L * Q * Q;           // one of X0, X1, X2: [n][a][j][k]
+  static constexpr int S_X1 = NF * L * XS;              // one of X0, X1, X2: [n][a][j][k], rows of XS
   static constexpr int S_X = 3 * S_X1 + 2;              // (+1 between arrays: they start on different banks)
   static constexpr int S_Y1 = NF * L * L * Q;           // Y0 or Y2: [n][a][b][k]
   static constexpr int S_Y = 2 * S_Y1 + 1;
   static constexpr int S_UB = NF * L * L * PL;          // updated modal block, padded rows
-  static constexpr int S_FP = NFACE * NF * L * L;       // end-reduced face planes [f][n][a'][b']
+  static constexpr int S_FP = NFACE * NF * FPS;         // end-reduced face planes [f][n][a'][b'], blocks of FPS
   static constexpr int S_W1 = NFACE * NF * G * PL;      // trace pass 1 [f][n][g][b'] padded
   // Barrier intervals: 1 face fluxes -> EF, backward k-pass -> T1;
   // 2 lift EF -> XL, j-pass T1 -> T2; 3 i-pass T2 -> UN; 4 volume UN -> X;
@@ -144,9 +153,13 @@ __device__ __forceinline__ void s2_load(const Smem2<C> &sm, const StageArgs &a, 
 // Lax-Friedrichs (src/Euler3d.cpp:601-816) uses max(|u.n| + c) over both
 // sides, which is the reference's max(|u.n - c|, |u.n|, |u.n + c|).  Same
 // algebra as the frame form; only the rounding differs.
+// What a side needs is the jump F^ - F(U_own).n: the master side (UL) gets
+// the flux's dissipation part G = F^ - F(UL).n, the slave side (UR)
+// D - G with D = F(UR).n - F(UL).n, so F^ itself is never formed (and the
+// two sides' fluxes, F(UL).n + G, agree as before).
 template <class T>
-__device__ __forceinline__ bool face_flux_vec3(const T *UL, const T *UR, const T *n, T gamma, int flux, T *Fh,
-                                               T *FL, T *FR) {
+__device__ __forceinline__ bool face_jump_vec3(const T *UL, const T *UR, const T *n, T gamma, int flux, bool master,
+                                               T *out) {
   const T gm1 = gamma - T(1.0);
   const T n0 = n[0], n1 = n[1], n2 = n[2];
   const T rl = UL[0], irl = T(1.0) / rl;
@@ -158,17 +171,16 @@ __device__ __forceinline__ bool face_flux_vec3(const T *UL, const T *UR, const T
   const T unr = fma(uzr, n2, fma(uyr, n1, uxr * n0));
   const T pr = gm1 * fma(T(-0.5), fma(UR[3], uzr, fma(UR[2], uyr, UR[1] * uxr)), UR[4]);
   const bool ok = rl >= T(kAeps) && pl >= T(kAeps) && rr >= T(kAeps) && pr >= T(kAeps);
-  FL[0] = rl * unl;
-  FL[1] = fma(UL[1], unl, pl * n0);
-  FL[2] = fma(UL[2], unl, pl * n1);
-  FL[3] = fma(UL[3], unl, pl * n2);
-  FL[4] = (UL[4] + pl) * unl;
-  FR[0] = rr * unr;
-  FR[1] = fma(UR[1], unr, pr * n0);
-  FR[2] = fma(UR[2], unr, pr * n1);
-  FR[3] = fma(UR[3], unr, pr * n2);
-  FR[4] = (UR[4] + pr) * unr;
+  // D = F(UR).n - F(UL).n, needed by the slave side only
+  const T dp = pr - pl;
+  T D[5];
+  D[0] = fma(rr, unr, -rl * unl);
+  D[1] = fma(UR[1], unr, fma(-UL[1], unl, dp * n0));
+  D[2] = fma(UR[2], unr, fma(-UL[2], unl, dp * n1));
+  D[3] = fma(UR[3], unr, fma(-UL[3], unl, dp * n2));
+  D[4] = fma(UR[4] + pr, unr, -(UL[4] + pl) * unl);
   const T Hl = (UL[4] + pl) * irl, Hr = (UR[4] + pr) * irr;
+  T Gv[5];   // F^ - F(UL).n
   if (flux == DGMX_FLUX_ROE) {
     const T R = sqrt(rr * irl), iRp1 = T(1.0) / (T(1.0) + R);
     const T ux = fma(R, uxr, uxl) * iRp1, uy = fma(R, uyr, uyl) * iRp1, uz = fma(R, uzr, uzl) * iRp1;
@@ -190,19 +202,20 @@ __device__ __forceinline__ bool face_flux_vec3(const T *UL, const T *UR, const T
     const T w0 = l0 * a0, w1 = l1 * a1, w4 = l4 * a4;
     const T G0 = w0 + w1 + w4;
     const T Gn = fma(un + a, w4, fma(un, w1, (un - a) * w0));
-    const T GE = fma(fma(un, a, H), w4, fma(T(0.5) * q2, w1, fma(fma(-un, a, H), w0, l1 * shu)));
-    Fh[0] = FL[0] + G0;
-    Fh[1] = FL[1] + fma(Gn, n0, fma(G0, utx, l1 * shx));
-    Fh[2] = FL[2] + fma(Gn, n1, fma(G0, uty, l1 * shy));
-    Fh[3] = FL[3] + fma(Gn, n2, fma(G0, utz, l1 * shz));
-    Fh[4] = FL[4] + GE;
+    Gv[0] = G0;
+    Gv[1] = fma(Gn, n0, fma(G0, utx, l1 * shx));
+    Gv[2] = fma(Gn, n1, fma(G0, uty, l1 * shy));
+    Gv[3] = fma(Gn, n2, fma(G0, utz, l1 * shz));
+    Gv[4] = fma(fma(un, a, H), w4, fma(T(0.5) * q2, w1, fma(fma(-un, a, H), w0, l1 * shu)));
   } else {
     const T cl = sqrt(gm1 * fma(T(-0.5), fma(uzl, uzl, fma(uyl, uyl, uxl * uxl)), Hl));
     const T cr = sqrt(gm1 * fma(T(-0.5), fma(uzr, uzr, fma(uyr, uyr, uxr * uxr)), Hr));
-    const T lmax = fmax(fabs(unl) + cl, fabs(unr) + cr);
+    const T hl = T(0.5) * fmax(fabs(unl) + cl, fabs(unr) + cr);
 #pragma unroll
-    for (int k = 0; k < 5; ++k) Fh[k] = T(0.5) * (FL[k] + FR[k] + lmax * (UL[k] - UR[k]));
+    for (int k = 0; k < 5; ++k) Gv[k] = fma(T(0.5), D[k], hl * (UL[k] - UR[k]));
   }
+#pragma unroll
+  for (int k = 0; k < 5; ++k) out[k] = master ? Gv[k] : D[k] - Gv[k];
   return ok;
 }
 
@@ -228,7 +241,7 @@ __device__ __forceinline__ void s2_face_point(const Smem2<C> &sm, const StageArg
   const T *tn = Tin + ((size_t)lk.elem * NFACE + lk.face) * NF * GF + gn;
   const int mbits = __ldg(&gc->master);
   const bool master = (mbits >> f) & 1;
-  T UL[5], UR[5], Fh[5], FL[5], FR[5];
+  T UL[5], UR[5], Fh[5], FR[5];
 #pragma unroll
   for (int k = 0; k < NF; ++k) {
     const T uo = to[k * GF], un = tn[k * GF];
@@ -244,9 +257,9 @@ __device__ __forceinline__ void s2_face_point(const Smem2<C> &sm, const StageArg
 #pragma unroll
     for (int k = 0; k < NF; ++k) eo[k * PE] = (master ? Fh[k] : FR[k] - Fh[k]) * jr;
   } else {
-    ok = face_flux_vec3<T>(UL, UR, nm, T(a.gamma), a.flux, Fh, FL, FR);
+    ok = face_jump_vec3<T>(UL, UR, nm, T(a.gamma), a.flux, master, Fh);
 #pragma unroll
-    for (int k = 0; k < NF; ++k) eo[k * PE] = (master ? Fh[k] - FL[k] : FR[k] - Fh[k]) * jr;
+    for (int k = 0; k < NF; ++k) eo[k * PE] = Fh[k] * jr;
   }
   if (!ok) {
     atomicOr(a.err, 1);
@@ -285,10 +298,9 @@ __device__ __forceinline__ void s2_backward_k_row(const Smem2<C> &sm, const Stag
 template <class C, int PHYS>
 __device__ __forceinline__ void s2_interval1(const Smem2<C> &sm, const StageArgs &a, int e0, int tid) {
   constexpr int N1 = C::EPB * C::NFACE * C::GF, N2 = C::EPB * C::NF * C::L * C::L;
-  for (int w = tid; w < N1 + N2; w += C::NT) {
-    if (w < N1) s2_face_point<C, PHYS>(sm, a, e0, w);
-    else s2_backward_k_row<C>(sm, a, e0, w - N1);
-  }
+  // two loops: one body holding both tasks keeps both tasks' state live
+  for (int w = tid; w < N1; w += C::NT) s2_face_point<C, PHYS>(sm, a, e0, w);
+  for (int w = tid; w < N2; w += C::NT) s2_backward_k_row<C>(sm, a, e0, w);
 }
 
 // ---- interval 2a: lift and projection of one face's terms of one field ------
@@ -303,7 +315,7 @@ __device__ __forceinline__ void s2_lift(const Smem2<C> &sm, int w) {
   T E[GF];
 #pragma unroll
   for (int q = 0; q < GF; ++q) E[q] = src[q];
-  T *dst = sm.slot(s) + C::O_XL + fn * L * PL;
+  T *dst = sm.slot(s) + C::O_XL + fn * C::XLS;
 #pragma unroll
   for (int b = 0; b < L; ++b) {
     T z[G];
@@ -347,10 +359,8 @@ __device__ __forceinline__ void s2_backward_j_pencil(const Smem2<C> &sm, int w) 
 template <class C>
 __device__ __forceinline__ void s2_interval2(const Smem2<C> &sm, int tid) {
   constexpr int N1 = C::EPB * C::NFACE * C::NF, N2 = C::EPB * C::NF * C::L * C::Q;
-  for (int w = tid; w < N1 + N2; w += C::NT) {
-    if (w < N2) s2_backward_j_pencil<C>(sm, w);
-    else s2_lift<C>(sm, w - N2);
-  }
+  for (int w = tid; w < N2; w += C::NT) s2_backward_j_pencil<C>(sm, w);
+  for (int w = tid; w < N1; w += C::NT) s2_lift<C>(sm, w);
 }
 
 template <class C>
@@ -469,7 +479,7 @@ __device__ __forceinline__ void s2_volume_column(const Smem2<C> &sm, const Stage
 #pragma unroll
     for (int n = 0; n < NF; ++n)
 #pragma unroll
-      for (int b = 0; b < L; ++b) dst[(R0 + r) * (C::S_X1 + 1) + (n * L + b) * Q * Q] = acc[r][n][b];
+      for (int b = 0; b < L; ++b) dst[(R0 + r) * (C::S_X1 + 1) + (n * L + b) * C::XS] = acc[r][n][b];
 }
 
 template <class C, int PHYS>
@@ -498,7 +508,7 @@ __device__ __forceinline__ void s2_pass_j(const Smem2<C> &sm, int tid) {
   constexpr int N = NF * L * Q;
   for (int w = tid; w < EPB * N; w += C::NT) {
     const int s = w / N, r = w - s * N, na = r / Q, k = r - na * Q;
-    const T *x = sm.slot(s) + C::O_X + na * Q * Q + k;
+    const T *x = sm.slot(s) + C::O_X + na * C::XS + k;
     T x0[Q], x1[Q], x2[Q];
 #pragma unroll
     for (int j = 0; j < Q; ++j) {
@@ -540,10 +550,10 @@ __device__ __forceinline__ void s2_update(const Smem2<C> &sm, const StageArgs &a
     // face terms: k faces (0: k=0, 5: k=Q-1) plane (a, b); j faces (1: j=0,
     // 3: j=Q-1) plane (a, c); i faces (4: i=0, 2: i=Q-1) plane (b, c)
     const T *xl = sl + C::O_XL;
-    constexpr int FB = NF * L * PL;   // one face's block
-    const T xk0 = xl[0 * FB + (n * L + aa) * PL + bb], xk1 = xl[5 * FB + (n * L + aa) * PL + bb];
-    const T *xj0 = xl + 1 * FB + (n * L + aa) * PL, *xj1 = xl + 3 * FB + (n * L + aa) * PL;
-    const T *xi0 = xl + 4 * FB + (n * L + bb) * PL, *xi1 = xl + 2 * FB + (n * L + bb) * PL;
+    constexpr int FB = NF * C::XLS;   // one face's block
+    const T xk0 = xl[0 * FB + n * C::XLS + aa * PL + bb], xk1 = xl[5 * FB + n * C::XLS + aa * PL + bb];
+    const T *xj0 = xl + 1 * FB + n * C::XLS + aa * PL, *xj1 = xl + 3 * FB + n * C::XLS + aa * PL;
+    const T *xi0 = xl + 4 * FB + n * C::XLS + bb * PL, *xi1 = xl + 2 * FB + n * C::XLS + bb * PL;
     const T eb0 = end_value<T, L, Q>(0, bb), eb1 = end_value<T, L, Q>(1, bb);
     const T ea0 = end_value<T, L, Q>(0, aa), ea1 = end_value<T, L, Q>(1, aa);
     T R[L];
@@ -641,10 +651,10 @@ __device__ __forceinline__ void s2_update(const Smem2<C> &sm, const StageArgs &a
       f0 = fma(cEnd<T, L, Q>[c], xv, f0);
       f5 = fma(cEnd<T, L, Q>[L + c], xv, f5);
     }
-    T *fp = sl + C::O_FP;
-    constexpr int PB = NF * L * L;   // one face plane block
-    fp[0 * PB + r] = f0;
-    fp[5 * PB + r] = f5;
+    T *fp = sl + C::O_FP + n * C::FPS + ab;
+    constexpr int PB = NF * C::FPS;   // one face's planes
+    fp[0 * PB] = f0;
+    fp[5 * PB] = f5;
   }
 }
 
@@ -653,13 +663,13 @@ template <class C>
 __device__ __forceinline__ void s2_ends_ab(const Smem2<C> &sm, int tid) {
   using T = typename C::R;
   constexpr int NF = C::NF, L = C::L, Q = C::Q, EPB = C::EPB, PL = C::PL;
-  constexpr int N = NF * L * L, PB = NF * L * L;
+  constexpr int N = NF * L * L, PB = NF * C::FPS;
   for (int w = tid; w < EPB * 2 * N; w += C::NT) {
     const int s = w / (2 * N), rem = w - s * 2 * N, ax = rem / N, r = rem - ax * N;
     const int n = r / (L * L), xy = r - n * L * L, x = xy / L, y = xy - x * L;
     const T *ub = sm.slot(s) + C::O_UB + n * L * L * PL;
     T lo = T(0), hi = T(0);
-    T *fp = sm.slot(s) + C::O_FP;
+    T *fp = sm.slot(s) + C::O_FP + n * C::FPS + xy;
     if (ax == 0) {   // along b at (a = x, c = y): faces 1 (j=0) and 3 (j=Q-1), plane (a, c)
 #pragma unroll
       for (int b = 0; b < L; ++b) {
@@ -667,8 +677,8 @@ __device__ __forceinline__ void s2_ends_ab(const Smem2<C> &sm, int tid) {
         lo = fma(cEnd<T, L, Q>[b], v, lo);
         hi = fma(cEnd<T, L, Q>[L + b], v, hi);
       }
-      fp[1 * PB + r] = lo;
-      fp[3 * PB + r] = hi;
+      fp[1 * PB] = lo;
+      fp[3 * PB] = hi;
     } else {         // along a at (b = x, c = y): faces 4 (i=0) and 2 (i=Q-1), plane (b, c)
 #pragma unroll
       for (int aa = 0; aa < L; ++aa) {
@@ -676,8 +686,8 @@ __device__ __forceinline__ void s2_ends_ab(const Smem2<C> &sm, int tid) {
         lo = fma(cEnd<T, L, Q>[aa], v, lo);
         hi = fma(cEnd<T, L, Q>[L + aa], v, hi);
       }
-      fp[4 * PB + r] = lo;
-      fp[2 * PB + r] = hi;
+      fp[4 * PB] = lo;
+      fp[2 * PB] = hi;
     }
   }
 }
@@ -691,7 +701,7 @@ __device__ __forceinline__ void s2_traces_a(const Smem2<C> &sm, int tid) {
   constexpr int N = NFACE * NF * L;
   for (int w = tid; w < EPB * N; w += C::NT) {
     const int s = w / N, r = w - s * N, fn = r / L, b = r - fn * L;
-    const T *src = sm.slot(s) + C::O_FP + fn * L * L + b;
+    const T *src = sm.slot(s) + C::O_FP + fn * C::FPS + b;
     T v[L];
 #pragma unroll
     for (int aa = 0; aa < L; ++aa) v[aa] = src[aa * L];
