@@ -63,12 +63,31 @@ static cudaError_t upload_tables2_lq(const Tables1D &t) {
   return cudaMemcpyToSymbol(cBwG<T, L, Q>, bwg.data(), sizeof(T) * bwg.size());
 }
 
+// Whether two CTAs of the FP32 viscous kernels' tile CV fit one SM's shared
+// memory (Navier-Stokes only: other physics have no viscous kernels).
+template <bool NS, class CV>
+struct ViscPairFits {
+  static constexpr bool value = false;
+};
+template <class CV>
+struct ViscPairFits<true, CV> {
+  static constexpr bool value = 2 * (NsCfg<CV, float>::Grad::SMEM + 1024) <= 228 * 1024 &&
+                                2 * (NsCfg<CV, float>::Visc::SMEM + 1024) <= 228 * 1024;
+};
+
 template <int PHYS, int L, int Q, int EPB, int MINB, bool MIXED = false>
 struct Launch {
   using C = Cfg<PHYS, L, Q, EPB, MINB, MIXED>;
   // 3xTF32 tensor-core contractions in the FP32 viscous kernels: 3-D
   // Navier-Stokes at p >= 5 (1-D operators of at least 7 x 7)
   static constexpr bool kTensorViscous = PHYS == DGMX_NS3D && L >= 6;
+  // The FP32 viscous kernels' tile.  Above 512 quadrature points one thread
+  // per point (and its registers) leaves one CTA per SM, whose barriers then
+  // idle the SM; 384 threads (two points each) and two CTAs per SM let one
+  // CTA's barrier waits overlap the other's work, where both fit.
+  using CV2 = Cfg<PHYS, L, Q, EPB, 2, MIXED, 384>;
+  static constexpr bool kViscPair = C::QD > 512 && EPB == 1 && ViscPairFits<is_ns(PHYS) && !MIXED, CV2>::value;
+  using CV = std::conditional_t<kViscPair, CV2, C>;
   static dim3 grid(int ne) { return dim3((unsigned)((ne + EPB - 1) / EPB)); }
   static cudaError_t init(const Tables1D &t) {
     cudaError_t e = upload_tables_lq<L, Q, typename C::R>(t);
@@ -93,27 +112,27 @@ struct Launch {
     if constexpr (is_ns(PHYS) && !MIXED && MINB == 0) {
       // the FP32 viscous kernels (one set per (physics, L, Q, EPB): the
       // uncapped tile carries them) and their FP32 tables
-      using N = NsCfg<C, float>;
+      using N = NsCfg<CV, float>;
       if ((e = upload_tables_lq<L, Q, float>(t)) != cudaSuccess) return e;
       const int sg = (int)N::Grad::SMEM, sv = (int)N::Visc::SMEM;
-      if ((e = cudaFuncSetAttribute(ns_grad_kernel<C, PHYS, false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
-      if ((e = cudaFuncSetAttribute(ns_grad_kernel<C, PHYS, true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
-      if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
-      if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+      if ((e = cudaFuncSetAttribute(ns_grad_kernel<CV, PHYS, false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
+      if ((e = cudaFuncSetAttribute(ns_grad_kernel<CV, PHYS, true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
+      if ((e = cudaFuncSetAttribute(ns_visc_kernel<CV, PHYS, false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+      if ((e = cudaFuncSetAttribute(ns_visc_kernel<CV, PHYS, true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
       if constexpr (kTensorViscous) {
-        if ((e = cudaFuncSetAttribute(ns_grad_kernel<C, PHYS, false, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
-        if ((e = cudaFuncSetAttribute(ns_grad_kernel<C, PHYS, true, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
-        if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, false, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
-        if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, true, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+        if ((e = cudaFuncSetAttribute(ns_grad_kernel<CV, PHYS, false, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
+        if ((e = cudaFuncSetAttribute(ns_grad_kernel<CV, PHYS, true, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
+        if ((e = cudaFuncSetAttribute(ns_visc_kernel<CV, PHYS, false, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+        if ((e = cudaFuncSetAttribute(ns_visc_kernel<CV, PHYS, true, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
       }
     }
     return cudaSuccess;
   }
   static cudaError_t ns_grad32(const StageArgs &a, bool nodal, cudaStream_t s) {
     if constexpr (is_ns(PHYS) && !MIXED && MINB == 0) {
-      using N = NsCfg<C, float>;
-      if (nodal) ns_grad_kernel<C, PHYS, true, float><<<grid(a.ne), C::NT, N::Grad::SMEM, s>>>(a);
-      else ns_grad_kernel<C, PHYS, false, float><<<grid(a.ne), C::NT, N::Grad::SMEM, s>>>(a);
+      using N = NsCfg<CV, float>;
+      if (nodal) ns_grad_kernel<CV, PHYS, true, float><<<grid(a.ne), CV::NT, N::Grad::SMEM, s>>>(a);
+      else ns_grad_kernel<CV, PHYS, false, float><<<grid(a.ne), CV::NT, N::Grad::SMEM, s>>>(a);
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;
@@ -121,9 +140,9 @@ struct Launch {
   }
   static cudaError_t ns_visc32(const StageArgs &a, bool nodal, cudaStream_t s) {
     if constexpr (is_ns(PHYS) && !MIXED && MINB == 0) {
-      using N = NsCfg<C, float>;
-      if (nodal) ns_visc_kernel<C, PHYS, true, float><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
-      else ns_visc_kernel<C, PHYS, false, float><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
+      using N = NsCfg<CV, float>;
+      if (nodal) ns_visc_kernel<CV, PHYS, true, float><<<grid(a.ne), CV::NT, N::Visc::SMEM, s>>>(a);
+      else ns_visc_kernel<CV, PHYS, false, float><<<grid(a.ne), CV::NT, N::Visc::SMEM, s>>>(a);
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;
@@ -131,9 +150,9 @@ struct Launch {
   }
   static cudaError_t ns_grad32tc(const StageArgs &a, bool nodal, cudaStream_t s) {
     if constexpr (is_ns(PHYS) && !MIXED && MINB == 0 && kTensorViscous) {
-      using N = NsCfg<C, float>;
-      if (nodal) ns_grad_kernel<C, PHYS, true, float, true><<<grid(a.ne), C::NT, N::Grad::SMEM, s>>>(a);
-      else ns_grad_kernel<C, PHYS, false, float, true><<<grid(a.ne), C::NT, N::Grad::SMEM, s>>>(a);
+      using N = NsCfg<CV, float>;
+      if (nodal) ns_grad_kernel<CV, PHYS, true, float, true><<<grid(a.ne), CV::NT, N::Grad::SMEM, s>>>(a);
+      else ns_grad_kernel<CV, PHYS, false, float, true><<<grid(a.ne), CV::NT, N::Grad::SMEM, s>>>(a);
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;
@@ -141,9 +160,9 @@ struct Launch {
   }
   static cudaError_t ns_visc32tc(const StageArgs &a, bool nodal, cudaStream_t s) {
     if constexpr (is_ns(PHYS) && !MIXED && MINB == 0 && kTensorViscous) {
-      using N = NsCfg<C, float>;
-      if (nodal) ns_visc_kernel<C, PHYS, true, float, true><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
-      else ns_visc_kernel<C, PHYS, false, float, true><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
+      using N = NsCfg<CV, float>;
+      if (nodal) ns_visc_kernel<CV, PHYS, true, float, true><<<grid(a.ne), CV::NT, N::Visc::SMEM, s>>>(a);
+      else ns_visc_kernel<CV, PHYS, false, float, true><<<grid(a.ne), CV::NT, N::Visc::SMEM, s>>>(a);
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;
