@@ -60,21 +60,21 @@ struct Cfg2 {
   // block pitches chosen for the passes that read or write across blocks:
   // XLS (one (face, field) block of lifted terms, odd: the lift writes one
   // value per block), FPS (one face plane, = L (mod 16) for L = 4: the
-  // trace pass reads column b' of a block, L per block), XS (one X row of
-  // Q x Q, = Q (mod 32): the j-pass reads Q consecutive k per row)
+  // trace pass reads column b' of a block, L per block), XJ (one j-plane of
+  // X and T2, [n a][k], = Q (mod 16): a pass over (j, k) columns writes or
+  // reads Q consecutive k per j)
   static constexpr int XLS = (L * PL) % 2 == 0 ? L * PL + 1 : L * PL;
   static constexpr int FPS = L * PL;
-  static constexpr int XS = Q * Q + ((Q - Q * Q) % 32 + 32) % 32 <= Q * Q + Q * Q / 2
-                                ? Q * Q + ((Q - Q * Q) % 32 + 32) % 32 : Q * Q;
+  static constexpr int XJ = NF * L * Q + ((Q - NF * L * Q) % 16 + 16) % 16;
   // region sizes (values of R)
   static constexpr int S_EF = NFACE * NF * PE;          // face terms [f][n][g h], padded blocks
   static constexpr int S_XL = NFACE * NF * XLS;         // lifted-projected face terms [f][n][a'][b'] padded
-  static constexpr int S_T1 = NF * L * L * Q;           // [n][a][b][k]
-  static constexpr int S_T2 = NF * L * Q * Q;           // [n][a][j][k]
+  static constexpr int S_T1 = NF * L * L * Q;           // [b][n a][k]
+  static constexpr int S_T2 = Q * XJ;                   // [j][n a][k], planes of XJ
   static constexpr int S_UN = NF * Q * Q * Q;           // nodal values [n][i][j][k]
-  static constexpr int S_X1 = NF * L * XS;              // one of X0, X1, X2: [n][a][j][k], rows of XS
+  static constexpr int S_X1 = Q * XJ;                   // one of X0, X1, X2: [j][n a][k], planes of XJ
   static constexpr int S_X = 3 * S_X1 + 2;              // (+1 between arrays: they start on different banks)
-  static constexpr int S_Y1 = NF * L * L * Q;           // Y0 or Y2: [n][a][b][k]
+  static constexpr int S_Y1 = NF * L * L * Q;           // Y0 or Y2: [b][n a][k]
   static constexpr int S_Y = 2 * S_Y1 + 1;
   static constexpr int S_UB = NF * L * L * PL;          // updated modal block, padded rows
   static constexpr int S_FP = NFACE * NF * FPS;         // end-reduced face planes [f][n][a'][b'], blocks of FPS
@@ -268,7 +268,7 @@ __device__ __forceinline__ void s2_face_point(const Smem2<C> &sm, const StageArg
 }
 
 // ---- interval 1b: backward k-pass from the modal rows in global memory ----
-// T1[n][a][b][k] = sum_c B[c][k] u[n][a][b][c]; the mixed form takes the
+// T1[b][n a][k] = sum_c B[c][k] u[n][a][b][c]; the mixed form takes the
 // solve's reference state out of the constant mode in FP64 first.  Elements
 // past the end get the constant state (their results are discarded).
 template <class C>
@@ -285,7 +285,9 @@ __device__ __forceinline__ void s2_backward_k_row(const Smem2<C> &sm, const Stag
 #pragma unroll
     for (int k = 0; k < L; ++k) v[k] = (!C::MIXED && k == 0 && r % (L * L) == 0) ? 1.0 : 0.0;
   }
-  T *dst = sm.slot(s) + C::O_T1 + r * Q;
+  // planes of NF L Q = 4 (mod 16) values at p = 3: this pass's (n a, b) rows
+  // and the j pass's contiguous reads both fall on distinct banks
+  T *dst = sm.slot(s) + C::O_T1 + (r % L) * (NF * L * Q) + (r / L) * Q;
 #pragma unroll
   for (int k = 0; k < Q; ++k) {
     T acc = T(0);
@@ -341,18 +343,18 @@ template <class C>
 __device__ __forceinline__ void s2_backward_j_pencil(const Smem2<C> &sm, int w) {
   using T = typename C::R;
   constexpr int NF = C::NF, L = C::L, Q = C::Q, N = NF * L * Q;
-  const int s = w / N, r = w - s * N, na = r / Q, k = r - na * Q;   // na = n*L + a
-  const T *src = sm.slot(s) + C::O_T1 + na * L * Q + k;
+  const int s = w / N, r = w - s * N;   // r = (n*L + a)*Q + k
+  const T *src = sm.slot(s) + C::O_T1 + r;
   T v[L];
 #pragma unroll
-  for (int b = 0; b < L; ++b) v[b] = src[b * Q];
-  T *dst = sm.slot(s) + C::O_T2 + na * Q * Q + k;
+  for (int b = 0; b < L; ++b) v[b] = src[b * N];
+  T *dst = sm.slot(s) + C::O_T2 + r;
 #pragma unroll
   for (int j = 0; j < Q; ++j) {
     T acc = T(0);
 #pragma unroll
     for (int b = 0; b < L; ++b) acc = fma(cB<T, L, Q>[b * Q + j], v[b], acc);
-    dst[j * Q] = acc;
+    dst[j * C::XJ] = acc;
   }
 }
 
@@ -369,11 +371,11 @@ __device__ __forceinline__ void s2_backward_i(const Smem2<C> &sm, int tid) {
   constexpr int NF = C::NF, L = C::L, Q = C::Q, EPB = C::EPB;
   constexpr int N = NF * Q * Q;
   for (int w = tid; w < EPB * N; w += C::NT) {
-    const int s = w / N, r = w - s * N, n = r / (Q * Q), jk = r - n * Q * Q;
-    const T *src = sm.slot(s) + C::O_T2 + n * L * Q * Q + jk;
+    const int s = w / N, r = w - s * N, n = r / (Q * Q), jk = r - n * Q * Q, j = jk / Q, k = jk - j * Q;
+    const T *src = sm.slot(s) + C::O_T2 + j * C::XJ + n * L * Q + k;
     T v[L];
 #pragma unroll
-    for (int a = 0; a < L; ++a) v[a] = src[a * Q * Q];
+    for (int a = 0; a < L; ++a) v[a] = src[a * Q];
     T *dst = sm.slot(s) + C::O_UN + n * Q * Q * Q + jk;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
@@ -473,13 +475,14 @@ __device__ __forceinline__ void s2_volume_column(const Smem2<C> &sm, const Stage
       }
     }
   }
-  T *dst = sm.slot(s) + C::O_X + jk;
+  const int j = jk / Q, k = jk - j * Q;
+  T *dst = sm.slot(s) + C::O_X + j * C::XJ + k;
 #pragma unroll
   for (int r = 0; r < NR; ++r)
 #pragma unroll
     for (int n = 0; n < NF; ++n)
 #pragma unroll
-      for (int b = 0; b < L; ++b) dst[(R0 + r) * (C::S_X1 + 1) + (n * L + b) * C::XS] = acc[r][n][b];
+      for (int b = 0; b < L; ++b) dst[(R0 + r) * (C::S_X1 + 1) + (n * L + b) * Q] = acc[r][n][b];
 }
 
 template <class C, int PHYS>
@@ -500,23 +503,25 @@ __device__ __forceinline__ void s2_volume(const Smem2<C> &sm, const StageArgs &a
 }
 
 // ---- interval 5: j-axis pass --------------------------------------------------
-// Y0 = P_j X0 + E_j X1, Y2 = P_j X2   ([n][a][b][k])
+// Y0 = P_j X0 + E_j X1, Y2 = P_j X2   ([b][n a][k]: planes of NF L Q = 4 (mod
+// 16) values at p = 3, so both this pass's writes and the update's reads of
+// (n a, b) rows fall on distinct banks)
 template <class C>
 __device__ __forceinline__ void s2_pass_j(const Smem2<C> &sm, int tid) {
   using T = typename C::R;
   constexpr int NF = C::NF, L = C::L, Q = C::Q, EPB = C::EPB;
   constexpr int N = NF * L * Q;
   for (int w = tid; w < EPB * N; w += C::NT) {
-    const int s = w / N, r = w - s * N, na = r / Q, k = r - na * Q;
-    const T *x = sm.slot(s) + C::O_X + na * C::XS + k;
+    const int s = w / N, r = w - s * N;   // r = (n*L + a)*Q + k
+    const T *x = sm.slot(s) + C::O_X + r;   // a warp reads contiguous values
     T x0[Q], x1[Q], x2[Q];
 #pragma unroll
     for (int j = 0; j < Q; ++j) {
-      x0[j] = x[j * Q];
-      x1[j] = x[(C::S_X1 + 1) + j * Q];
-      x2[j] = x[2 * (C::S_X1 + 1) + j * Q];
+      x0[j] = x[j * C::XJ];
+      x1[j] = x[(C::S_X1 + 1) + j * C::XJ];
+      x2[j] = x[2 * (C::S_X1 + 1) + j * C::XJ];
     }
-    T *y = sm.slot(s) + C::O_Y + na * L * Q + k;
+    T *y = sm.slot(s) + C::O_Y + r;
 #pragma unroll
     for (int b = 0; b < L; ++b) {
       T y0 = T(0), y2 = T(0);
@@ -526,8 +531,8 @@ __device__ __forceinline__ void s2_pass_j(const Smem2<C> &sm, int tid) {
         y0 = fma(cE2<T, L, Q>[b * Q + j], x1[j], y0);
         y2 = fma(cBw<T, L, Q>[b * Q + j], x2[j], y2);
       }
-      y[b * Q] = y0;
-      y[(C::S_Y1 + 1) + b * Q] = y2;
+      y[b * N] = y0;
+      y[(C::S_Y1 + 1) + b * N] = y2;
     }
   }
 }
@@ -543,7 +548,7 @@ __device__ __forceinline__ void s2_update(const Smem2<C> &sm, const StageArgs &a
     const int e = sm.eid[s];
     T *sl = sm.slot(s);
     // R[c] = sum_k P[c][k] Y0[k] + E[c][k] Y2[k]
-    const T *y = sl + C::O_Y + r * Q;
+    const T *y = sl + C::O_Y + bb * (NF * L * Q) + (n * L + aa) * Q;
     T y0[Q], y2[Q];
 #pragma unroll
     for (int k = 0; k < Q; ++k) { y0[k] = y[k]; y2[k] = y[(C::S_Y1 + 1) + k]; }
