@@ -746,6 +746,39 @@ __device__ __forceinline__ void s2_traces_b(const Smem2<C> &sm, TT *Tout, int e0
   }
 }
 
+// L2 prefetch hints (no data is moved into the SM, nothing waits): the
+// second register of tile `tile` (read by its update, six intervals later),
+// and the face traces, modal rows and second register of tile `next` (-1:
+// none).  Only addresses of elements that exist are named.
+__device__ __forceinline__ void prefetch_l2_lines(const void *base, int bytes, int line) {
+  if (line * 128 < bytes) asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const char *>(base) + line * 128));
+}
+
+template <class C>
+__device__ __forceinline__ void s2_prefetch(const StageArgs &a, int tile, int next, int tid) {
+  using T = typename C::R;
+  constexpr int TB = C::NFACE * C::NF * C::GF * (int)sizeof(T), XB = C::NF * C::LD * (int)sizeof(double);
+  constexpr int UB = C::NF * C::LD * (int)sizeof(T);
+  constexpr int LT = (TB + 127) / 128, LX = (XB + 127) / 128, LU = (UB + 127) / 128;
+  const bool lsrk = a.kind == kLSRK;
+  const T *ut = nullptr;
+  if (lsrk) {
+    if constexpr (C::MIXED) ut = a.Utf; else ut = a.Ut;
+  }
+  for (int w = tid; w < C::EPB * (LT + LX + 2 * LU); w += C::NT) {
+    const int s = w / (LT + LX + 2 * LU), l = w - s * (LT + LX + 2 * LU);
+    const int e = tile * C::EPB + s, en = next * C::EPB + s;
+    if (l < LU) {
+      if (lsrk && e < a.ne) prefetch_l2_lines(ut + (size_t)e * C::NF * C::LD, UB, l);
+    } else if (next >= 0 && en < a.ne) {
+      const int m = l - LU;
+      if (m < LT) prefetch_l2_lines(trace_in<C>(a) + (size_t)en * C::NFACE * C::NF * C::GF, TB, m);
+      else if (m < LT + LX) prefetch_l2_lines(a.X + (size_t)en * C::NF * C::LD, XB, m - LT);
+      else if (lsrk) prefetch_l2_lines(ut + (size_t)en * C::NF * C::LD, UB, m - LT - LX);
+    }
+  }
+}
+
 template <class C, int PHYS>
 __device__ __forceinline__ void stage2_tile(const Smem2<C> &sm, const StageArgs &a, int e0, int tid) {
   s2_load<C>(sm, a, e0, tid);
@@ -776,9 +809,22 @@ __global__ void __launch_bounds__(C::NT, C::MINB) stage2_kernel(StageArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem2<C> sm(smem_raw);
   const int ntile = a.tiles ? *a.ntiles : (int)gridDim.x;
+  // One tile per CTA: the CTAs resident at once are about (SMs x CTAs per SM)
+  // and start in block order, so the tile that many blocks ahead starts
+  // about when this one ends.  Persistent over a tile list: this CTA's next
+  // tile.  Its inputs are asked into L2 now, and this tile's second
+  // register, which only the update reads, too.
+  unsigned nsm;
+  asm("mov.u32 %0, %%nsmid;" : "=r"(nsm));
+  const int ahead = (int)nsm * (C::MINB_REQ > 8 ? C::MINB_REQ : 8);
   for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
     if (t != (int)blockIdx.x) __syncthreads();
-    stage2_tile<C, PHYS>(sm, a, (a.tiles ? a.tiles[t] : t) * C::EPB, threadIdx.x);
+    const int tile = a.tiles ? a.tiles[t] : t;
+    const int next = a.tiles ? (t + (int)gridDim.x < ntile ? a.tiles[t + gridDim.x] : -1) : t + ahead;
+    // FP64 only: measured on 32^3, p = 3, the hints take an LSRK stage from
+    // 292 to 279 us in FP64 and from 233 to 238 us in the FP32 form
+    if constexpr (!C::MIXED) s2_prefetch<C>(a, tile, next, threadIdx.x);
+    stage2_tile<C, PHYS>(sm, a, tile * C::EPB, threadIdx.x);
   }
 }
 
