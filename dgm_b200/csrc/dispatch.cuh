@@ -325,10 +325,10 @@ struct PLaunch {
 // The second-form stage kernel (stage2.cuh) for LSRK and right-hand-side
 // stages; other stage kinds, and every other kernel of the handle, come from
 // the plain tile of the same (L, Q).
-template <int PHYS, int L, int Q, int EPB, int NT, int MINB, bool MIXED = false>
+template <int PHYS, int L, int Q, int EPB, int NT, int MINB, bool MIXED = false, int VD = 0>
 struct Launch2 {
   using Base = Launch<PHYS, L, Q, default_epb(3, Q), 0, MIXED>;
-  using C = Cfg2<PHYS, L, Q, EPB, NT, MINB, MIXED>;
+  using C = Cfg2<PHYS, L, Q, EPB, NT, MINB, MIXED, VD>;
   static cudaError_t init(const Tables1D &t) {
     cudaError_t e = Base::init(t);
     if (e != cudaSuccess) return e;
@@ -362,12 +362,12 @@ struct Launch2 {
   }
 };
 
-template <int PHYS, int P, int Q, int EPB, int NT, int MINB, bool MIXED>
+template <int PHYS, int P, int Q, int EPB, int NT, int MINB, bool MIXED, int VD = 0>
 void reg2_variant() {
-  using C = Cfg2<PHYS, P + 1, Q, EPB, NT, MINB, MIXED>;
+  using C = Cfg2<PHYS, P + 1, Q, EPB, NT, MINB, MIXED, VD>;
   if constexpr (C::SMEM <= 227 * 1024 && (MINB == 0 || (65536 / (NT * MINB) >= 40 &&
                                                         (int)((228 * 1024) / (C::SMEM + 1024)) >= MINB)))
-    register_ops(PHYS + (MIXED ? kMixedKey : 0), P + 1, Q, Launch2<PHYS, P + 1, Q, EPB, NT, MINB, MIXED>::ops());
+    register_ops(PHYS + (MIXED ? kMixedKey : 0), P + 1, Q, Launch2<PHYS, P + 1, Q, EPB, NT, MINB, MIXED, VD>::ops());
 }
 
 // CTAs per SM of NT threads that a cap of R registers per thread allows: a
@@ -393,7 +393,7 @@ void reg2() {
   using CB = Cfg2<PHYS, P + 1, Q, 1, NTB, 0, MIXED>;
   constexpr int A96 = blocks_for_regs<CA>(NTA, 96), A80 = blocks_for_regs<CA>(NTA, 80);
   constexpr int B96 = blocks_for_regs<CB>(NTB, 96), B80 = blocks_for_regs<CB>(NTB, 80);
-  constexpr int B64 = blocks_for_regs<CB>(NTB, 64);
+  constexpr int B64 = blocks_for_regs<CB>(NTB, 64), A64 = blocks_for_regs<CA>(NTA, 64);
   reg2_variant<PHYS, P, Q, 1, NTA, 0, MIXED>();
   reg2_variant<PHYS, P, Q, 1, NTB, 0, MIXED>();
   if constexpr (B96 >= 2) reg2_variant<PHYS, P, Q, 1, NTB, B96, MIXED>();
@@ -401,6 +401,10 @@ void reg2() {
   if constexpr (B80 >= 2 && B80 != B96) reg2_variant<PHYS, P, Q, 1, NTB, B80, MIXED>();
   if constexpr (A80 >= 2 && A80 != A96) reg2_variant<PHYS, P, Q, 1, NTA, A80, MIXED>();
   if constexpr (MIXED && B64 >= 2 && B64 != B80) reg2_variant<PHYS, P, Q, 1, NTB, B64, MIXED>();
+  // FP32 with the volume's three directions spread over three warps
+  if constexpr (MIXED && A80 >= 2) reg2_variant<PHYS, P, Q, 1, NTA, A80, MIXED, 1>();
+  if constexpr (MIXED && B80 >= 2) reg2_variant<PHYS, P, Q, 1, NTB, B80, MIXED, 1>();
+  if constexpr (MIXED && A64 >= 2 && A64 != A80) reg2_variant<PHYS, P, Q, 1, NTA, A64, MIXED, 1>();
 }
 
 template <int PHYS, int P, int Q, int EPB, int MINB, bool MIXED>

@@ -46,9 +46,14 @@ namespace dgmx {
 template <class T, int L, int Q> __constant__ T cE2[L * Q];          // E[a][j] = sum_i B[a][i] w_i D[i][j]
 template <class T, int L, int Q> __constant__ T cBwG[L * (Q - 1)];   // BwG[a][g] = sum_i B[a][i] w_i G2GL[i][g]
 
-template <int PHYS, int L_, int Q_, int EPB_, int NT_, int MINB_, bool MIXED_>
+template <int PHYS, int L_, int Q_, int EPB_, int NT_, int MINB_, bool MIXED_, int VDIRS_ = 0>
 struct Cfg2 {
   static constexpr bool MIXED = MIXED_;
+  // directions of the volume pass per thread: 1 spreads a column's three
+  // directions over three warps, 3 keeps them in one thread (default: FP64
+  // 1, FP32 3)
+  static constexpr int VDIRS = VDIRS_ > 0 ? VDIRS_ : (MIXED_ ? 3 : 1);
+  static_assert(VDIRS == 1 || VDIRS == 3, "the volume pass takes one or all three directions per thread");
   static constexpr int PHYSICS = PHYS;
   using R = std::conditional_t<MIXED_, float, double>;
   static constexpr int NF = phys_nf(PHYS), L = L_, Q = Q_, G = Q_ - 1, EPB = EPB_, NT = NT_;
@@ -394,8 +399,8 @@ __device__ __forceinline__ void s2_backward_i(const Smem2<C> &sm, int tid) {
 // contravariant velocity V_r = metric[r] . u:  G_r[rho] = rho V_r,
 // G_r[m_d] = m_d V_r + p metric[r][d], G_r[E] = (E + p) V_r.  The mixed form
 // evaluates F(Ub + u') - F(Ub) (as volume_flux_pert, kernels.cuh) the same
-// way.  FP64 runs one direction per thread (20 accumulators; the columns of
-// a direction fill whole warps), the FP32 form all three (60).
+// way.  One direction per thread (20 accumulators; the columns of a direction
+// fill whole warps) or all three (60); Cfg2::VDIRS chooses.
 template <class C, int NR, int R0>
 __device__ __forceinline__ void s2_volume_column(const Smem2<C> &sm, const StageArgs &a, int s, int jk) {
   using T = typename C::R;
@@ -488,14 +493,15 @@ __device__ __forceinline__ void s2_volume_column(const Smem2<C> &sm, const Stage
 template <class C, int PHYS>
 __device__ __forceinline__ void s2_volume(const Smem2<C> &sm, const StageArgs &a, int tid) {
   constexpr int Q = C::Q, EPB = C::EPB;
-  // FP64: the columns of one direction fill whole warps (warp-uniform r)
-  constexpr int NDIR = C::MIXED ? 1 : 3, RS = (Q * Q + 31) / 32 * 32, N = NDIR * RS;
+  // one direction per thread: the columns of one direction fill whole warps
+  // (warp-uniform r)
+  constexpr int NDIR = 3 / C::VDIRS, RS = (Q * Q + 31) / 32 * 32, N = NDIR * RS;
   for (int w = tid; w < EPB * N; w += C::NT) {
     const int s = w / N, rem = w - s * N, r = rem / RS, jk = rem - r * RS;
     if (jk >= Q * Q) continue;
     // the direction is a template argument, so the coefficients stay
     // constant-bank operands of the FMAs
-    if constexpr (C::MIXED) s2_volume_column<C, 3, 0>(sm, a, s, jk);
+    if constexpr (C::VDIRS == 3) s2_volume_column<C, 3, 0>(sm, a, s, jk);
     else if (r == 0) s2_volume_column<C, 1, 0>(sm, a, s, jk);
     else if (r == 1) s2_volume_column<C, 1, 1>(sm, a, s, jk);
     else s2_volume_column<C, 1, 2>(sm, a, s, jk);
