@@ -405,7 +405,9 @@ void reg2() {
   if constexpr (MIXED && A80 >= 2) reg2_variant<PHYS, P, Q, 1, NTA, A80, MIXED, 1>();
   if constexpr (MIXED && B80 >= 2) reg2_variant<PHYS, P, Q, 1, NTB, B80, MIXED, 1>();
   if constexpr (MIXED && A64 >= 2 && A64 != A80) reg2_variant<PHYS, P, Q, 1, NTA, A64, MIXED, 1>();
-}
+  constexpr int A56 = blocks_for_regs<CA>(NTA, 56);
+  if constexpr (MIXED && B64 >= 2 && B64 != B80) reg2_variant<PHYS, P, Q, 1, NTB, B64, MIXED, 1>();
+  if constexpr (MIXED && A56 >= 2 && A56 != A64) reg2_variant<PHYS, P, Q, 1, NTA, A56, MIXED, 1>();}
 
 template <int PHYS, int P, int Q, int EPB, int MINB, bool MIXED>
 void reg_pipe() {
