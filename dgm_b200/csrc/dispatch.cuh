@@ -384,7 +384,9 @@ constexpr int blocks_for_regs(int nt, int r) {
 
 // Second-form variants of a 3-D Euler (p, q): one element per CTA at two
 // thread counts, uncapped and with the CTAs per SM that caps of 96 and 80
-// (and for the FP32 form 64) registers per thread allow.
+// (and for the FP32 form 64) registers per thread allow; for the FP32 form
+// also the volume pass with one direction per thread (fewer registers) at
+// caps of 80, 64 and 56.  Appended variants keep the earlier indices.
 template <int PHYS, int P, int Q, bool MIXED = false>
 void reg2() {
   constexpr int NTA = ((P + 1) * (P + 1) * 5 + 31) / 32 * 32;   // one thread per modal row
@@ -407,7 +409,8 @@ void reg2() {
   if constexpr (MIXED && A64 >= 2 && A64 != A80) reg2_variant<PHYS, P, Q, 1, NTA, A64, MIXED, 1>();
   constexpr int A56 = blocks_for_regs<CA>(NTA, 56);
   if constexpr (MIXED && B64 >= 2 && B64 != B80) reg2_variant<PHYS, P, Q, 1, NTB, B64, MIXED, 1>();
-  if constexpr (MIXED && A56 >= 2 && A56 != A64) reg2_variant<PHYS, P, Q, 1, NTA, A56, MIXED, 1>();}
+  if constexpr (MIXED && A56 >= 2 && A56 != A64) reg2_variant<PHYS, P, Q, 1, NTA, A56, MIXED, 1>();
+}
 
 template <int PHYS, int P, int Q, int EPB, int MINB, bool MIXED>
 void reg_pipe() {
