@@ -410,6 +410,10 @@ void reg2() {
   constexpr int A56 = blocks_for_regs<CA>(NTA, 56);
   if constexpr (MIXED && B64 >= 2 && B64 != B80) reg2_variant<PHYS, P, Q, 1, NTB, B64, MIXED, 1>();
   if constexpr (MIXED && A56 >= 2 && A56 != A64) reg2_variant<PHYS, P, Q, 1, NTA, A56, MIXED, 1>();
+  // FP64 at 72 registers: one more CTA per SM for a few dozen bytes of spills
+  constexpr int A72 = blocks_for_regs<CA>(NTA, 72), B72 = blocks_for_regs<CB>(NTB, 72);
+  if constexpr (!MIXED && A72 >= 2 && A72 != A80) reg2_variant<PHYS, P, Q, 1, NTA, A72, MIXED>();
+  if constexpr (!MIXED && B72 >= 2 && B72 != B80) reg2_variant<PHYS, P, Q, 1, NTB, B72, MIXED>();
 }
 
 template <int PHYS, int P, int Q, int EPB, int MINB, bool MIXED>
