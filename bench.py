@@ -12,16 +12,25 @@ initial state.  A "step" is one LSRK14 step (14 fused stage launches).
   value  device-resident throughput of the mixed form (FP32 working
          precision, FP64 solution register): modal DOF x 14 stages x K /
          time (CUDA events on the engine's stream, max over ranks); the
-         plain FP64 path is measured the same way under "fp64", and
-         "accuracy" gives the mixed form's relative L2 distance from the
-         FP64 path after a fixed number of steps
-  e2e    the same metric through the public C ABI with host buffers: every
-         step uploads the state from pinned host memory (dgmx_set_state),
-         advances one step (dgmx_advance) and reads the state back
-         (dgmx_get_state)
+         plain FP64 path is measured the same way under "fp64"
+  accuracy  per conserved field, the mixed and FP64 paths against the FP64
+         oracle after 10 steps (rank 0, host cores), and the mixed path
+         against the GPU FP64 path after the configuration's 500 steps
+  e2e    the same metric through the public C ABI with host buffers, for
+         both forms: every step uploads the state from pinned host memory
+         (dgmx_set_state_async), advances one step (dgmx_advance_async) and
+         reads the state back (dgmx_get_state_async), three handles in turn
+  roofline  algorithmic bytes per stage launch over its CUDA-event time
+         against the measured HBM bandwidth (and, for FP64, algorithmic
+         flops against the FP64 FMA rate measured live), with the DRAM
+         bytes of one ncu capture from profiles/
   forms  (one GPU) the batched ensemble of 1024 independent 2-D vortex
          solves and a Poisson-arrival serving trace, both through the
          element pool (include/dgmx_pool.h), FP64 and mixed
+  other_configs  (rank 0) the 2-D vortex (16^2, p=4) against the oracle,
+         the Navier-Stokes Taylor-Green (24^3, p=7, q=9) in FP64, with the
+         FP32 viscous kernels and with their 3xTF32 contractions, and the
+         reference's channel regression case against its golden restart
 Ranks (torchrun, N > 1) run independent replicas of the workload (weak
 scaling, no collective in the data path; NCCL only for the barrier and the
 max-over-ranks time).  --impl reference times the CPU restatement of the
