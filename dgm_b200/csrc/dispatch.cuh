@@ -75,6 +75,16 @@ struct ViscPairFits<true, CV> {
                                 2 * (NsCfg<CV, float>::Visc::SMEM + 1024) <= 228 * 1024;
 };
 
+// Whether two CTAs of the FP64 gradient kernel's tile CG fit one SM.
+template <bool NS, class CG>
+struct GradPairFits {
+  static constexpr bool value = false;
+};
+template <class CG>
+struct GradPairFits<true, CG> {
+  static constexpr bool value = 2 * (NsCfg<CG, double>::Grad::SMEM + 1024) <= 228 * 1024;
+};
+
 template <int PHYS, int L, int Q, int EPB, int MINB, bool MIXED = false>
 struct Launch {
   using C = Cfg<PHYS, L, Q, EPB, MINB, MIXED>;
@@ -88,6 +98,12 @@ struct Launch {
   using CV2 = Cfg<PHYS, L, Q, EPB, 2, MIXED, 384>;
   static constexpr bool kViscPair = C::QD > 512 && EPB == 1 && ViscPairFits<is_ns(PHYS) && !MIXED, CV2>::value;
   using CV = std::conditional_t<kViscPair, CV2, C>;
+  // The FP64 gradient kernel's tile, the same way: 384 threads and two CTAs
+  // per SM, where its shared memory without the staged traces (read from
+  // global memory instead, NsCfg::Grad::TRG) fits twice.
+  using CG2 = Cfg<PHYS, L, Q, EPB, 2, MIXED, 384>;
+  static constexpr bool kGradPair = C::QD > 512 && EPB == 1 && GradPairFits<is_ns(PHYS) && !MIXED, CG2>::value;
+  using CG = std::conditional_t<kGradPair, CG2, C>;
   static dim3 grid(int ne) { return dim3((unsigned)((ne + EPB - 1) / EPB)); }
   static cudaError_t init(const Tables1D &t) {
     cudaError_t e = upload_tables_lq<L, Q, typename C::R>(t);
@@ -103,9 +119,9 @@ struct Launch {
     }
     if constexpr (is_ns(PHYS) && !MIXED) {
       using N = NsCfg<C>;
-      const int sg = (int)N::Grad::SMEM, sv = (int)N::Visc::SMEM;
-      if ((e = cudaFuncSetAttribute(ns_grad_kernel<C, PHYS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
-      if ((e = cudaFuncSetAttribute(ns_grad_kernel<C, PHYS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
+      const int sg = (int)NsCfg<CG>::Grad::SMEM, sv = (int)N::Visc::SMEM;
+      if ((e = cudaFuncSetAttribute(ns_grad_kernel<CG, PHYS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
+      if ((e = cudaFuncSetAttribute(ns_grad_kernel<CG, PHYS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
       if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
       if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
     }
@@ -170,9 +186,9 @@ struct Launch {
   }
   static cudaError_t ns_grad(const StageArgs &a, bool nodal, cudaStream_t s) {
     if constexpr (is_ns(PHYS) && !MIXED) {
-      using N = NsCfg<C>;
-      if (nodal) ns_grad_kernel<C, PHYS, true><<<grid(a.ne), C::NT, N::Grad::SMEM, s>>>(a);
-      else ns_grad_kernel<C, PHYS, false><<<grid(a.ne), C::NT, N::Grad::SMEM, s>>>(a);
+      using N = NsCfg<CG>;
+      if (nodal) ns_grad_kernel<CG, PHYS, true><<<grid(a.ne), CG::NT, N::Grad::SMEM, s>>>(a);
+      else ns_grad_kernel<CG, PHYS, false><<<grid(a.ne), CG::NT, N::Grad::SMEM, s>>>(a);
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;

@@ -72,7 +72,11 @@ struct NsCfg {
     static constexpr int pad(int n) { return (n + DW - 1) / DW * DW; }
     static constexpr int Qc = QD, Gd = DIM * QD;
     static constexpr int A = pad(cmax(NF * LD, Qc + Gd)), B = pad(NF * QD);
-    static constexpr int E = NFACE * NF * GF * DW, E2 = NFACE * NF * GF * DW, Rs = F32 ? 2 * DW : 0;
+    // TRG: the FP64 tile with fewer threads than points (two CTAs per SM)
+    // reads the own and neighbour traces from global memory in each
+    // component's lift-input pass instead of staging them in E and E2
+    static constexpr bool TRG = !F32 && NT < QD;
+    static constexpr int E = TRG ? 0 : NFACE * NF * GF * DW, E2 = E, Rs = F32 ? 2 * DW : 0;
     static constexpr int Fc = NFACE * DIM * GF, LFc = cmax(NFACE * DIM * QF, DIM * F2);
     static constexpr int S1 = cmax(cmax(NB1 * P1, DIM == 3 ? NFACE * DIM * Q * G : 0), DIM * F1);
     static constexpr int S2 = cmax(cmax(NB1 * P2, DIM * F2), DIM * LD);
@@ -374,9 +378,9 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::GRAD_MINB) ns_grad_kernel(
   } else {
     load_modal_v<C>(A, a.X, e0, a.ne, tid);
   }
-  load_own_traces_v<C>(E, a.Tin, e0, a.ne, tid);
+  if constexpr (!R::TRG) load_own_traces_v<C>(E, a.Tin, e0, a.ne, tid);
   __syncthreads();
-  load_nbr_traces<C>(E2, a.Tin, lnk, eid, geo, a, tid);
+  if constexpr (!R::TRG) load_nbr_traces<C>(E2, a.Tin, lnk, eid, geo, a, tid);
   if constexpr (!NODAL) {
     __syncthreads();
     if constexpr (N::NB1 == NF) {
@@ -423,10 +427,32 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::GRAD_MINB) ns_grad_kernel(
       const int f = w / (EPB * GF), rem = w - f * EPB * GF, s = rem / GF, g = rem - s * GF;
       // formed in double in both forms, then rounded to the working type
       double Uo[5], Un[5], qo[4], qn[4];
+      if constexpr (R::TRG) {
+        // the values load_own_traces_v and load_nbr_traces would have staged
+        const int e = eid[s];
+        if (e >= 0) {
+          const double *to = a.Tin + ((size_t)e * NFACE + f) * NF * GF + g;
+          const FaceLink lk = lnk[s * NFACE + f];
+          const double *t = a.Tin + ((size_t)(lk.elem * NFACE + lk.face) * NF) * GF + a.perm[lk.perm + g];
 #pragma unroll
-      for (int n = 0; n < NF; ++n) {
-        Uo[n] = E[((f * EPB + s) * NF + n) * GF + g];
-        Un[n] = E2[((f * EPB + s) * NF + n) * GF + g];
+          for (int n = 0; n < NF; ++n) { Uo[n] = to[n * GF]; Un[n] = t[n * GF]; }
+          const int bt = (geo[s].bc >> (4 * f)) & 15;
+          if (bt) {
+            double Ut[5];
+#pragma unroll
+            for (int n = 0; n < NF; ++n) Ut[n] = Un[n];
+            ghost_state<C::DIM, NF>(a.bckind[bt], a.bcpar[bt], Ut, geo[s].onrm[f], true, Un);
+          }
+        } else {
+#pragma unroll
+          for (int n = 0; n < NF; ++n) Uo[n] = Un[n] = n == 0 ? 1.0 : 0.0;
+        }
+      } else {
+#pragma unroll
+        for (int n = 0; n < NF; ++n) {
+          Uo[n] = E[((f * EPB + s) * NF + n) * GF + g];
+          Un[n] = E2[((f * EPB + s) * NF + n) * GF + g];
+        }
       }
       primitive<DIM>(Uo, qo);
       primitive<DIM>(Un, qn);

@@ -58,6 +58,10 @@ CASES = [
      (1.0, 178.575), True),
     ("ns3d-isothermal-hold-rk4-p2", 9, (2, 3, 4), 2, "laxfriedrichs", 4, 0.001, 2, 0.01, BC_ISOTHERMAL_WALL,
      (1.05, 178.575), True),
+    # p = 7, q = 9: the FP64 gradient kernel's two-CTA tile, which reads the
+    # wall sides' ghost traces from global memory
+    ("ns3d-isothermal-tvd3-p7", 9, (2, 2, 2), 7, "laxfriedrichs", 3, 0.0002, 1, 0.02, BC_ISOTHERMAL_WALL,
+     (1.0, 178.575), False),
 ]
 
 
