@@ -85,6 +85,16 @@ struct GradPairFits<true, CG> {
   static constexpr bool value = 2 * (NsCfg<CG, double>::Grad::SMEM + 1024) <= 228 * 1024;
 };
 
+// Whether two CTAs of the lean FP64 viscous tile CW fit one SM.
+template <bool NS, class CW>
+struct ViscLeanFits {
+  static constexpr bool value = false;
+};
+template <class CW>
+struct ViscLeanFits<true, CW> {
+  static constexpr bool value = NsCfg<CW, double>::Visc::LEAN && 2 * (NsCfg<CW, double>::Visc::SMEM + 1024) <= 228 * 1024;
+};
+
 template <int PHYS, int L, int Q, int EPB, int MINB, bool MIXED = false>
 struct Launch {
   using C = Cfg<PHYS, L, Q, EPB, MINB, MIXED>;
@@ -104,6 +114,10 @@ struct Launch {
   using CG2 = Cfg<PHYS, L, Q, EPB, 2, MIXED, 384>;
   static constexpr bool kGradPair = C::QD > 512 && EPB == 1 && GradPairFits<is_ns(PHYS) && !MIXED, CG2>::value;
   using CG = std::conditional_t<kGradPair, CG2, C>;
+  // and the FP64 viscous kernel's, with its lean layout (NsCfg::Visc::LEAN)
+  using CW2 = Cfg<PHYS, L, Q, EPB, 2, MIXED, 384>;
+  static constexpr bool kViscLean = C::QD > 512 && EPB == 1 && ViscLeanFits<is_ns(PHYS) && !MIXED, CW2>::value;
+  using CW = std::conditional_t<kViscLean, CW2, C>;
   static dim3 grid(int ne) { return dim3((unsigned)((ne + EPB - 1) / EPB)); }
   static cudaError_t init(const Tables1D &t) {
     cudaError_t e = upload_tables_lq<L, Q, typename C::R>(t);
@@ -118,12 +132,11 @@ struct Launch {
       if ((e = cudaFuncSetAttribute(backward_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
     }
     if constexpr (is_ns(PHYS) && !MIXED) {
-      using N = NsCfg<C>;
-      const int sg = (int)NsCfg<CG>::Grad::SMEM, sv = (int)N::Visc::SMEM;
+      const int sg = (int)NsCfg<CG>::Grad::SMEM, sv = (int)NsCfg<CW>::Visc::SMEM;
       if ((e = cudaFuncSetAttribute(ns_grad_kernel<CG, PHYS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
       if ((e = cudaFuncSetAttribute(ns_grad_kernel<CG, PHYS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sg))) return e;
-      if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
-      if ((e = cudaFuncSetAttribute(ns_visc_kernel<C, PHYS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+      if ((e = cudaFuncSetAttribute(ns_visc_kernel<CW, PHYS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
+      if ((e = cudaFuncSetAttribute(ns_visc_kernel<CW, PHYS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv))) return e;
     }
     if constexpr (is_ns(PHYS) && !MIXED && MINB == 0) {
       // the FP32 viscous kernels (one set per (physics, L, Q, EPB): the
@@ -196,9 +209,9 @@ struct Launch {
   }
   static cudaError_t ns_visc(const StageArgs &a, bool nodal, cudaStream_t s) {
     if constexpr (is_ns(PHYS) && !MIXED) {
-      using N = NsCfg<C>;
-      if (nodal) ns_visc_kernel<C, PHYS, true><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
-      else ns_visc_kernel<C, PHYS, false><<<grid(a.ne), C::NT, N::Visc::SMEM, s>>>(a);
+      using N = NsCfg<CW>;
+      if (nodal) ns_visc_kernel<CW, PHYS, true><<<grid(a.ne), CW::NT, N::Visc::SMEM, s>>>(a);
+      else ns_visc_kernel<CW, PHYS, false><<<grid(a.ne), CW::NT, N::Visc::SMEM, s>>>(a);
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;

@@ -93,14 +93,22 @@ struct NsCfg {
   // modal gradient components Gh in the first loop and the face-point
   // values Fg in the second.
   struct Visc {
+    // LEAN: the FP64 tile with fewer threads than points (two CTAs per SM).
+    // It keeps only the density and momenta of the state (the stresses need
+    // the velocity alone), transforms one field or gradient component at a
+    // time, writes the velocity gradient straight into its stress slots,
+    // forms the stresses before the energy gradient is brought into the
+    // heat-flux slots, and keeps the divergence behind the face values in B.
+    static constexpr bool LEAN = std::is_same<V, double>::value && NT < QD && EPB == 1;
     static constexpr int NGS = DIM == 3 ? 9 : 5;
     static constexpr int FF = cmax(NFACE * DIM * QF, F2), Cv = QD;
-    static constexpr int B = cmax(NF * QD, FF + Cv);
+    static constexpr int B = LEAN ? cmax((DIM + 1) * QD, FF + Cv + QD) : cmax(NF * QD, FF + Cv);
     static constexpr int G = cmax(NGS * QD, NF * LD);
     static constexpr int X = cmax(DIM * LD, NFACE * DIM * GF);
-    static constexpr int S1 = cmax(cmax(NB1 * P1, DIM * P1), cmax(DIM == 3 ? NFACE * DIM * C::G * Q : 0, F1));
-    static constexpr int S2 = cmax(cmax(NB1 * P2, DIM * P2), LD);
-    static constexpr int Dv = DIM * QD;
+    static constexpr int S1 = LEAN ? cmax(P1, cmax(DIM == 3 ? NFACE * DIM * C::G * Q : 0, F1))
+                                   : cmax(cmax(NB1 * P1, DIM * P1), cmax(DIM == 3 ? NFACE * DIM * C::G * Q : 0, F1));
+    static constexpr int S2 = LEAN ? cmax(cmax(P2, LD), F2) : cmax(cmax(NB1 * P2, DIM * P2), LD);
+    static constexpr int Dv = LEAN ? 0 : DIM * QD;
     static constexpr int SLOT = B + G + X + S1 + S2 + Dv;
     static constexpr size_t DATA = ns_data_bytes<V>(EPB * SLOT);
     static constexpr size_t SMEM = DATA + (size_t)EPB * (sizeof(GeomClass) + NFACE * 16 + 16);
@@ -498,6 +506,113 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::GRAD_MINB) ns_grad_kernel(
 }
 
 // ----------------------------------------------- stresses, traces, divergence
+// The viscous stress (src/Navier_Stokes3d.cpp:305-344) from the velocity
+// gradient at one point, g[k * stride] = (ux, uy, [uz,] vx, vy, [vz, wx, wy,
+// wz]); t = (t11, t12, t13, t22, t23, t33) in 3-D, (t11, t12, t22) in 2-D.
+template <int DIM, class V>
+__device__ __forceinline__ void viscous_stress(const V *g, int stride, V mu, V *t) {
+  if constexpr (DIM == 3) {
+    const V ux = g[0 * stride], uy = g[1 * stride], uz = g[2 * stride];
+    const V vx = g[3 * stride], vy = g[4 * stride], vz = g[5 * stride];
+    const V wx = g[6 * stride], wy = g[7 * stride], wz = g[8 * stride];
+    const V two = V(2.0), one = V(1.0), tt = V(2.0 / 3.0);
+    V t12 = uy + vx; t12 = mu * t12;
+    V t13 = uz + wx; t13 = mu * t13;
+    V t23 = vz + wy; t23 = mu * t23;
+    V wk = two * ux - vy;
+    V t11 = one * wk - wz; t11 = tt * t11; t11 = mu * t11;
+    wk = two * vy - ux;
+    V t22 = one * wk - wz; t22 = tt * t22; t22 = mu * t22;
+    wk = two * wz - ux;
+    V t33 = one * wk - vy; t33 = tt * t33; t33 = mu * t33;
+    t[0] = t11; t[1] = t12; t[2] = t13; t[3] = t22; t[4] = t23; t[5] = t33;
+  } else {
+    const V ux = g[0 * stride], uy = g[1 * stride], vx = g[2 * stride], vy = g[3 * stride];
+    const V two = V(2.0), tt = V(2.0 / 3.0);
+    V t12 = uy + vx; t12 = mu * t12;
+    V t11 = two * ux - vy; t11 = tt * t11; t11 = mu * t11;
+    V t22 = two * vy - ux; t22 = tt * t22; t22 = mu * t22;
+    t[0] = t11; t[1] = t12; t[2] = t22;
+  }
+}
+
+// The energy flux tau . u + (gamma mu / Pr) grad e at one point.
+template <int DIM, class V>
+__device__ __forceinline__ void heat_flux(const V *t, V u, V v, V w, V ex, V ey, V ez, V mu, V gPr, V *q) {
+  if constexpr (DIM == 3) {
+    V qx = t[0] * u; qx = fma(t[1], v, qx); qx = fma(t[2], w, qx);
+    V qy = t[1] * u; qy = fma(t[3], v, qy); qy = fma(t[4], w, qy);
+    V qz = t[2] * u; qz = fma(t[4], v, qz); qz = fma(t[5], w, qz);
+    q[0] = fma(gPr, mu * ex, qx); q[1] = fma(gPr, mu * ey, qy); q[2] = fma(gPr, mu * ez, qz);
+  } else {
+    V qx = t[0] * u; qx = fma(t[1], v, qx);
+    V qy = t[1] * u; qy = fma(t[2], v, qy);
+    q[0] = fma(gPr, mu * ex, qx); q[1] = fma(gPr, mu * ey, qy);
+  }
+}
+
+// The viscous kernel's first part for the lean FP64 tile (NsCfg::Visc::LEAN,
+// one element per CTA): the density and momenta at the GLL points into B,
+// the velocity gradient into the stress slots of Gg one component at a time
+// (Gh = X holds one component's modal gradient), the stresses in place, the
+// energy gradient into the heat-flux slots, then the heat flux in place.
+// The arithmetic of every value is that of the staged path.
+template <class C, bool NODAL, class V, bool TC>
+__device__ __forceinline__ void ns_visc_lean_front(const StageArgs &a, V *B, V *Gg, V *X, V *S1, V *S2, int e0,
+                                                   int tid) {
+  using N = NsCfg<C, V>;
+  constexpr int DIM = C::DIM, NF = C::NF, QD = C::QD, LD = C::LD, NVC = N::NVC, NGS = N::Visc::NGS;
+  constexpr int NT6 = DIM == 3 ? 6 : 3;
+  static_assert(C::EPB == 1, "the lean viscous tile holds one element");
+  const int e = e0 < a.ne ? e0 : -1;
+  // state: density and momenta (the stresses need the velocity only)
+  if constexpr (NODAL) {
+    for (int w = tid; w < (DIM + 1) * QD; w += C::NT) {
+      const int n = w / QD, p = w - n * QD;
+      B[w] = e >= 0 ? V(a.Xn[((size_t)n * a.ne + e) * QD + p]) : V(n == 0 ? 1.0 : 0.0);
+    }
+  } else {
+    for (int w = tid; w < NF * LD; w += C::NT)
+      Gg[w] = e >= 0 ? V(a.X[(size_t)e0 * NF * LD + w]) : V(w % LD == 0 ? 1.0 : 0.0);
+    __syncthreads();
+    for (int n = 0; n <= DIM; ++n) backward_batch<C, 1, V, TC>(Gg + n * LD, B + n * QD, S1, S2, tid);
+  }
+  __syncthreads();
+  // velocity gradient: component c, direction d into slot c*DIM + d
+  for (int c = 0; c < DIM; ++c) {
+    for (int w = tid; w < DIM * LD; w += C::NT)
+      X[w] = e >= 0 ? V(a.Ghat[((size_t)e * NVC + c) * DIM * LD + w]) : V(0.0);
+    __syncthreads();
+    for (int d = 0; d < DIM; ++d) backward_batch<C, 1, V, TC>(X + d * LD, Gg + (c * DIM + d) * QD, S1, S2, tid);
+  }
+  const V mu = V(a.vis), gPr = V(a.gamma / a.Pr);
+  for (int p = tid; p < QD; p += C::NT) {
+    V t[6];
+    viscous_stress<DIM, V>(Gg + p, QD, mu, t);
+#pragma unroll
+    for (int k = 0; k < NT6; ++k) Gg[k * QD + p] = t[k];
+  }
+  __syncthreads();
+  // energy gradient into the heat-flux slots (the velocity gradient's last
+  // components, dead once the stresses are formed)
+  for (int w = tid; w < DIM * LD; w += C::NT)
+    X[w] = e >= 0 ? V(a.Ghat[((size_t)e * NVC + DIM) * DIM * LD + w]) : V(0.0);
+  __syncthreads();
+  for (int d = 0; d < DIM; ++d) backward_batch<C, 1, V, TC>(X + d * LD, Gg + (NT6 + d) * QD, S1, S2, tid);
+  for (int p = tid; p < QD; p += C::NT) {
+    V t[6], q[3];
+#pragma unroll
+    for (int k = 0; k < NT6; ++k) t[k] = Gg[k * QD + p];
+    const V r = B[p];
+    const V u = B[QD + p] / r, v = B[2 * QD + p] / r, w = DIM == 3 ? B[3 * QD + p] / r : V(0.0);
+    const V *ge = Gg + NT6 * QD + p;
+    heat_flux<DIM, V>(t, u, v, w, ge[0], ge[QD], DIM == 3 ? ge[2 * QD] : V(0.0), mu, gPr, q);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) Gg[(NT6 + d) * QD + p] = q[d];
+  }
+  static_assert(NGS == NT6 + DIM, "stress and heat-flux slots");
+}
+
 template <class C, int PHYS, bool NODAL, class V = double, bool TC = false>
 __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::VISC_MINB) ns_visc_kernel(StageArgs a) {
   using N = NsCfg<C, V>;
@@ -510,12 +625,15 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::VISC_MINB) ns_visc_kernel(
   V *S1 = X + EPB * R::X, *S2 = S1 + EPB * R::S1, *Dv = S2 + EPB * R::S2;
   V *Gh = X, *Fg = X;                    // first loop / second loop
   V *FF = B, *Cv = B + EPB * R::FF;      // after the stresses are formed
+  if constexpr (R::LEAN) Dv = Cv + EPB * R::Cv;   // the divergence behind the face values
   GeomClass *geo = reinterpret_cast<GeomClass *>(smem_bytes + R::DATA);
   FaceLink *lnk = reinterpret_cast<FaceLink *>(geo + EPB);
   int *eid = reinterpret_cast<int *>(lnk + EPB * NFACE);
   const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
   load_geo_slots<C>(geo, lnk, eid, a, e0, tid);
-  if constexpr (NODAL) {
+  if constexpr (R::LEAN) {
+    ns_visc_lean_front<C, NODAL, V, TC>(a, B, Gg, X, S1, S2, e0, tid);
+  } else if constexpr (NODAL) {
     load_nodal_v<C>(B, a.Xn, e0, a.ne, tid);
   } else {
     load_modal_v<C>(Gg, a.X, e0, a.ne, tid);  // modal input parked in the gradient region
@@ -527,6 +645,7 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::VISC_MINB) ns_visc_kernel(
       backward_batch<C, NF - N::NB1, V, TC>(Gg + N::NB1 * LD, B + N::NB1 * QD, S1, S2, tid);
     }
   }
+  if constexpr (!R::LEAN) {
   __syncthreads();
   // projected gradients at the GLL points: velocity components into Gg
   // (component c, direction d at slot c*DIM+d), the energy gradient into Dv
@@ -556,44 +675,22 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::VISC_MINB) ns_visc_kernel(
 #pragma unroll
     for (int n = 0; n < NF; ++n) U[n] = B[(s * NF + n) * QD + p];
     const V r = U[0];
+    V t[6], q[3];
+    viscous_stress<DIM, V>(g, QD, mu, t);
     if constexpr (DIM == 3) {
       const V u = U[1] / r, v = U[2] / r, ww = U[3] / r;
-      const V ux = g[0 * QD], uy = g[1 * QD], uz = g[2 * QD];
-      const V vx = g[3 * QD], vy = g[4 * QD], vz = g[5 * QD];
-      const V wx = g[6 * QD], wy = g[7 * QD], wz = g[8 * QD];
-      const V ex = ge[0], ey = ge[QD], ez = ge[2 * QD];
-      const V two = V(2.0), one = V(1.0), tt = V(2.0 / 3.0);
-      V t12 = uy + vx; t12 = mu * t12;
-      V t13 = uz + wx; t13 = mu * t13;
-      V t23 = vz + wy; t23 = mu * t23;
-      V wk = two * ux - vy;
-      V t11 = one * wk - wz; t11 = tt * t11; t11 = mu * t11;
-      wk = two * vy - ux;
-      V t22 = one * wk - wz; t22 = tt * t22; t22 = mu * t22;
-      wk = two * wz - ux;
-      V t33 = one * wk - vy; t33 = tt * t33; t33 = mu * t33;
-      V qx = t11 * u; qx = fma(t12, v, qx); qx = fma(t13, ww, qx);
-      V qy = t12 * u; qy = fma(t22, v, qy); qy = fma(t23, ww, qy);
-      V qz = t13 * u; qz = fma(t23, v, qz); qz = fma(t33, ww, qz);
-      qx = fma(gPr, mu * ex, qx); qy = fma(gPr, mu * ey, qy); qz = fma(gPr, mu * ez, qz);
-      g[0 * QD] = t11; g[1 * QD] = t12; g[2 * QD] = t13;
-      g[3 * QD] = t22; g[4 * QD] = t23; g[5 * QD] = t33;
-      g[6 * QD] = qx; g[7 * QD] = qy; g[8 * QD] = qz;
+      heat_flux<DIM, V>(t, u, v, ww, ge[0], ge[QD], ge[2 * QD], mu, gPr, q);
     } else {
       const V u = U[1] / r, v = U[2] / r;
-      const V ux = g[0 * QD], uy = g[1 * QD], vx = g[2 * QD], vy = g[3 * QD];
-      const V ex = ge[0], ey = ge[QD];
-      const V two = V(2.0), tt = V(2.0 / 3.0);
-      V t12 = uy + vx; t12 = mu * t12;
-      V t11 = two * ux - vy; t11 = tt * t11; t11 = mu * t11;
-      V t22 = two * vy - ux; t22 = tt * t22; t22 = mu * t22;
-      V qx = t11 * u; qx = fma(t12, v, qx);
-      V qy = t12 * u; qy = fma(t22, v, qy);
-      qx = fma(gPr, mu * ex, qx); qy = fma(gPr, mu * ey, qy);
-      g[0 * QD] = t11; g[1 * QD] = t12; g[2 * QD] = t22;
-      g[3 * QD] = qx; g[4 * QD] = qy;
+      heat_flux<DIM, V>(t, u, v, V(0.0), ge[0], ge[QD], V(0.0), mu, gPr, q);
     }
+    constexpr int NT6 = DIM == 3 ? 6 : 3;
+#pragma unroll
+    for (int k = 0; k < NT6; ++k) g[k * QD] = t[k];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) g[(NT6 + d) * QD] = q[d];
   }
+  } // !LEAN
   __syncthreads();
   for (int n = 0; n < NV; ++n) {
     // face GLL values of g_n (DIM components), face-major [f][slot][d][QF]
