@@ -63,16 +63,16 @@ static cudaError_t upload_tables2_lq(const Tables1D &t) {
   return cudaMemcpyToSymbol(cBwG<T, L, Q>, bwg.data(), sizeof(T) * bwg.size());
 }
 
-// Whether two CTAs of the FP32 viscous kernels' tile CV fit one SM's shared
-// memory (Navier-Stokes only: other physics have no viscous kernels).
+// Whether CV::MINB CTAs of the FP32 viscous kernels' tile CV fit one SM's
+// shared memory (Navier-Stokes only: other physics have no viscous kernels).
 template <bool NS, class CV>
 struct ViscPairFits {
   static constexpr bool value = false;
 };
 template <class CV>
 struct ViscPairFits<true, CV> {
-  static constexpr bool value = 2 * (NsCfg<CV, float>::Grad::SMEM + 1024) <= 228 * 1024 &&
-                                2 * (NsCfg<CV, float>::Visc::SMEM + 1024) <= 228 * 1024;
+  static constexpr bool value = CV::MINB * (NsCfg<CV, float>::Grad::SMEM + 1024) <= 228 * 1024 &&
+                                CV::MINB * (NsCfg<CV, float>::Visc::SMEM + 1024) <= 228 * 1024;
 };
 
 // Whether two CTAs of the FP64 gradient kernel's tile CG fit one SM.
@@ -103,9 +103,10 @@ struct Launch {
   static constexpr bool kTensorViscous = PHYS == DGMX_NS3D && L >= 6;
   // The FP32 viscous kernels' tile.  Above 512 quadrature points one thread
   // per point (and its registers) leaves one CTA per SM, whose barriers then
-  // idle the SM; 384 threads (two points each) and two CTAs per SM let one
-  // CTA's barrier waits overlap the other's work, where both fit.
-  using CV2 = Cfg<PHYS, L, Q, EPB, 2, MIXED, 384>;
+  // idle the SM; 384 threads (two points each) and three CTAs per SM (the
+  // traces read from global memory and the lean viscous layout, NsCfg::Grad::
+  // TRG and NsCfg::Visc::LEAN) let CTAs' barrier waits overlap the others' work.
+  using CV2 = Cfg<PHYS, L, Q, EPB, 3, MIXED, 384>;
   static constexpr bool kViscPair = C::QD > 512 && EPB == 1 && ViscPairFits<is_ns(PHYS) && !MIXED, CV2>::value;
   using CV = std::conditional_t<kViscPair, CV2, C>;
   // The FP64 gradient kernel's tile, the same way: 384 threads and two CTAs

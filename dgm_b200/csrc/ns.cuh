@@ -72,10 +72,10 @@ struct NsCfg {
     static constexpr int pad(int n) { return (n + DW - 1) / DW * DW; }
     static constexpr int Qc = QD, Gd = DIM * QD;
     static constexpr int A = pad(cmax(NF * LD, Qc + Gd)), B = pad(NF * QD);
-    // TRG: the FP64 tile with fewer threads than points (two CTAs per SM)
+    // TRG: a tile with fewer threads than points (several CTAs per SM)
     // reads the own and neighbour traces from global memory in each
     // component's lift-input pass instead of staging them in E and E2
-    static constexpr bool TRG = !F32 && NT < QD;
+    static constexpr bool TRG = NT < QD;
     static constexpr int E = TRG ? 0 : NFACE * NF * GF * DW, E2 = E, Rs = F32 ? 2 * DW : 0;
     static constexpr int Fc = NFACE * DIM * GF, LFc = cmax(NFACE * DIM * QF, DIM * F2);
     static constexpr int S1 = cmax(cmax(NB1 * P1, DIM == 3 ? NFACE * DIM * Q * G : 0), DIM * F1);
@@ -93,13 +93,13 @@ struct NsCfg {
   // modal gradient components Gh in the first loop and the face-point
   // values Fg in the second.
   struct Visc {
-    // LEAN: the FP64 tile with fewer threads than points (two CTAs per SM).
+    // LEAN: a tile with fewer threads than points (several CTAs per SM).
     // It keeps only the density and momenta of the state (the stresses need
     // the velocity alone), transforms one field or gradient component at a
     // time, writes the velocity gradient straight into its stress slots,
     // forms the stresses before the energy gradient is brought into the
     // heat-flux slots, and keeps the divergence behind the face values in B.
-    static constexpr bool LEAN = std::is_same<V, double>::value && NT < QD && EPB == 1;
+    static constexpr bool LEAN = NT < QD && EPB == 1;
     static constexpr int NGS = DIM == 3 ? 9 : 5;
     static constexpr int FF = cmax(NFACE * DIM * QF, F2), Cv = QD;
     static constexpr int B = LEAN ? cmax((DIM + 1) * QD, FF + Cv + QD) : cmax(NF * QD, FF + Cv);
@@ -551,7 +551,7 @@ __device__ __forceinline__ void heat_flux(const V *t, V u, V v, V w, V ex, V ey,
   }
 }
 
-// The viscous kernel's first part for the lean FP64 tile (NsCfg::Visc::LEAN,
+// The viscous kernel's first part for the lean tile (NsCfg::Visc::LEAN,
 // one element per CTA): the density and momenta at the GLL points into B,
 // the velocity gradient into the stress slots of Gg one component at a time
 // (Gh = X holds one component's modal gradient), the stresses in place, the
