@@ -111,14 +111,14 @@ struct Launch {
   using CV2 = Cfg<PHYS, L, Q, EPB, 4, MIXED, 256>;
   static constexpr bool kViscPair = C::QD > 512 && EPB == 1 && ViscPairFits<is_ns(PHYS) && !MIXED, CV2>::value;
   using CV = std::conditional_t<kViscPair, CV2, C>;
-  // The FP64 gradient kernel's tile, the same way: 384 threads and two CTAs
-  // per SM, where its shared memory without the staged traces (read from
-  // global memory instead, NsCfg::Grad::TRG) fits twice.
-  using CG2 = Cfg<PHYS, L, Q, EPB, 2, MIXED, 384>;
+  // The FP64 gradient kernel's tile, the same way: 512 threads and two CTAs
+  // per SM (64 registers), where its shared memory without the staged traces
+  // (read from global memory instead, NsCfg::Grad::TRG) fits twice.
+  using CG2 = Cfg<PHYS, L, Q, EPB, 2, MIXED, 512>;
   static constexpr bool kGradPair = C::QD > 512 && EPB == 1 && GradPairFits<is_ns(PHYS) && !MIXED, CG2>::value;
   using CG = std::conditional_t<kGradPair, CG2, C>;
   // and the FP64 viscous kernel's, with its lean layout (NsCfg::Visc::LEAN)
-  using CW2 = Cfg<PHYS, L, Q, EPB, 2, MIXED, 384>;
+  using CW2 = Cfg<PHYS, L, Q, EPB, 2, MIXED, 512>;
   static constexpr bool kViscLean = C::QD > 512 && EPB == 1 && ViscLeanFits<is_ns(PHYS) && !MIXED, CW2>::value;
   using CW = std::conditional_t<kViscLean, CW2, C>;
   static dim3 grid(int ne) { return dim3((unsigned)((ne + EPB - 1) / EPB)); }
