@@ -157,13 +157,15 @@ class Domain:
     @classmethod
     def partition(cls, mesh, physics: int, part, nranks: int, rank: int, flux: str = "laxfriedrichs",
                   inttype: int = LSRK14, gamma: float = 1.4, vis: float = 0.0, Pr: float = 0.72,
-                  sw_balance: bool = True, device: int = 0):
+                  sw_balance: bool = True, device: int = 0, precision: int = FP64):
         """The rank's part of an element partition (part[e] = owning rank);
         its arrays cover its own elements in increasing global order.  Call
-        set_exchange_nccl on every rank before stepping."""
+        set_exchange_nccl (or set_exchange_host) on every rank before
+        setting the state: with precision=MIXED, set_state gathers every
+        rank's element integrals for the common reference state."""
         m, keep = _mesh_struct(mesh)
         part = np.ascontiguousarray(part, dtype=np.int32)
-        p = _Params(physics, FLUX[flux.lower()], inttype, 0, 1 if sw_balance else 0, device, gamma, vis, Pr)
+        p = _Params(physics, FLUX[flux.lower()], inttype, precision, 1 if sw_balance else 0, device, gamma, vis, Pr)
         h = ctypes.c_void_p()
         f = lib().dgmx_create_partition
         f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
@@ -642,12 +644,12 @@ class Group:
     are global (Field layout over all elements)."""
 
     def __init__(self, mesh, physics: int, part, flux: str = "laxfriedrichs", inttype: int = LSRK14,
-                 gamma: float = 1.4, vis: float = 0.0, Pr: float = 0.72, device: int = 0):
+                 gamma: float = 1.4, vis: float = 0.0, Pr: float = 0.72, device: int = 0, precision: int = FP64):
         m, self._keep = _mesh_struct(mesh)
         part = np.ascontiguousarray(part, dtype=np.int32)
         self._keep.append(part)
         self.nparts = int(part.max()) + 1
-        p = _Params(physics, FLUX[flux.lower()], inttype, 0, 0, device, gamma, vis, Pr)
+        p = _Params(physics, FLUX[flux.lower()], inttype, precision, 0, device, gamma, vis, Pr)
         L = lib()
         L.dgmx_group_create.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
                                         ctypes.c_void_p]

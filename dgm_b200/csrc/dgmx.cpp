@@ -120,6 +120,7 @@ struct dgmx_domain {
   // element partition: ghost slots in the trace buffers and the halo
   // exchange lists (plan.nranks == 1: the whole mesh, no exchange)
   PartitionPlan plan;
+  int ne_global = 0, max_ne = 0;                         // whole mesh; most elements of one rank
   int nslot = 0;                                         // ne + ghost slots
   int *x_send = nullptr, *x_recv = nullptr;              // concatenated block lists (device)
   std::vector<int> x_cnt, x_off;                         // per peer block counts and offsets
@@ -242,15 +243,43 @@ struct dgmx_domain {
 
 namespace {
 
-// Halo exchange of one trace buffer (blk doubles per face block) between the
-// ranks of a partitioned domain over NCCL: pack, grouped send/receive with
-// every peer, unpack into the ghost slots.  A no-op when the domain is not
-// partitioned or belongs to an in-process group (the group exchanges).
-dgmx_status exchange(dgmx_domain *d, double *T, int blk) {
+// One buffer the halo exchange moves: FP64 blocks of blk values, or the
+// mixed form's FP32 trace blocks, packed at an even stride so that a block
+// is wire() whole doubles in the send and receive buffers.
+struct Halo {
+  double *T = nullptr;
+  float *Tf = nullptr;
+  int blk = 0;
+  int wire() const { return Tf ? (blk + 1) / 2 : blk; }   // doubles per block in x_sbuf / x_rbuf
+  cudaError_t pack(const dgmx_domain *d, cudaStream_t s) const {
+    return Tf ? launch_pack(Tf, d->x_send, d->x_total, blk, 2 * wire(), reinterpret_cast<float *>(d->x_sbuf), s)
+              : launch_pack(T, d->x_send, d->x_total, blk, d->x_sbuf, s);
+  }
+  cudaError_t unpack(const dgmx_domain *d, cudaStream_t s) const {
+    return Tf ? launch_unpack(reinterpret_cast<const float *>(d->x_rbuf), d->x_recv, d->x_total, blk, 2 * wire(), Tf, s)
+              : launch_unpack(d->x_rbuf, d->x_recv, d->x_total, blk, T, s);
+  }
+};
+Halo fp64_halo(double *T, int blk) { Halo h; h.T = T; h.blk = blk; return h; }
+// the stage traces of slot k (FP32 in the mixed form)
+Halo trace_halo(const dgmx_domain *d, int k) {
+  Halo h;
+  if (d->mixed()) h.Tf = d->Tf[k]; else h.T = d->T[k];
+  h.blk = d->nf * d->gf;
+  return h;
+}
+Halo visc_halo(const dgmx_domain *d) { return fp64_halo(d->Vtr, (d->nf - 1) * d->gf); }
+
+// Halo exchange of one buffer between the ranks of a partitioned domain
+// over NCCL (or the caller's host transport): pack, grouped send/receive
+// with every peer, unpack into the ghost slots.  A no-op when the domain is
+// not partitioned or belongs to an in-process group (the group exchanges).
+dgmx_status exchange(dgmx_domain *d, const Halo &h) {
   if (!d->partitioned() || d->in_group) return DGMX_OK;
   if (!d->nccl && !d->xhost)
     return d->fail(DGMX_ERR_ARGUMENT, "partitioned domain without an exchange (dgmx_set_exchange_nccl)");
-  cudaError_t e = launch_pack(T, d->x_send, d->x_total, blk, d->x_sbuf, d->stream);
+  const int blk = h.wire();
+  cudaError_t e = h.pack(d, d->stream);
   if (e != cudaSuccess) return d->cuda(e, "halo pack");
   if (d->xhost) {
     // host-staged: blocks to the host, the caller's transport, back, unpack
@@ -261,7 +290,7 @@ dgmx_status exchange(dgmx_domain *d, double *T, int blk) {
     if (d->xhost(d->xhost_ctx, d->xh_send, d->xh_recv, d->x_cnt.data(), d->x_off.data(), blk, d->plan.nranks) != 0)
       return d->fail(DGMX_ERR_CUDA, "host halo transport reported a failure");
     if (n) e = cudaMemcpyAsync(d->x_rbuf, d->xh_recv, sizeof(double) * n, cudaMemcpyHostToDevice, d->stream);
-    if (e == cudaSuccess) e = launch_unpack(d->x_rbuf, d->x_recv, d->x_total, blk, T, d->stream);
+    if (e == cudaSuccess) e = h.unpack(d, d->stream);
     d->launches += 2;
     return d->cuda(e, "halo unpack");
   }
@@ -276,7 +305,7 @@ dgmx_status exchange(dgmx_domain *d, double *T, int blk) {
   const ncclResult_t r2 = nc.GroupEnd();
   if (r == ncclSuccess) r = r2;
   if (r != ncclSuccess) return d->fail(DGMX_ERR_CUDA, std::string("halo exchange: ") + nc.GetErrorString(r));
-  e = launch_unpack(d->x_rbuf, d->x_recv, d->x_total, blk, T, d->stream);
+  e = h.unpack(d, d->stream);
   d->launches += 2;
   return d->cuda(e, "halo unpack");
 }
@@ -370,9 +399,9 @@ dgmx_status stage_overlapped(dgmx_domain *d, const StageArgs &a) {
   if (e == cudaSuccess) e = cudaEventRecord(d->ev_b, d->stream);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(d->xstream, d->ev_b, 0);
   if (e != cudaSuccess) return d->cuda(e, "boundary tiles");
-  const int blk = d->nf * d->gf;
-  double *T = d->T[d->tcur ^ 1];
-  e = launch_pack(T, d->x_send, d->x_total, blk, d->x_sbuf, d->xstream);
+  const Halo h = trace_halo(d, d->tcur ^ 1);
+  const int blk = h.wire();
+  e = h.pack(d, d->xstream);
   if (e != cudaSuccess) return d->cuda(e, "halo pack");
   const NcclApi &nc = nccl_api();
   ncclResult_t r = nc.GroupStart();
@@ -385,7 +414,7 @@ dgmx_status stage_overlapped(dgmx_domain *d, const StageArgs &a) {
   const ncclResult_t r2 = nc.GroupEnd();
   if (r == ncclSuccess) r = r2;
   if (r != ncclSuccess) return d->fail(DGMX_ERR_CUDA, std::string("halo exchange: ") + nc.GetErrorString(r));
-  e = launch_unpack(d->x_rbuf, d->x_recv, d->x_total, blk, T, d->xstream);
+  e = h.unpack(d, d->xstream);
   if (e == cudaSuccess) e = cudaEventRecord(d->ev_x, d->xstream);
   if (e == cudaSuccess) e = stage_tiles(d, a, 1, d->stream);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(d->stream, d->ev_x, 0);
@@ -404,7 +433,7 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
       if ((e = d->ns_grad(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous gradient kernel");
       if ((e = d->ns_visc(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
       d->launches += 2;
-      dgmx_status xs = exchange(d, d->Vtr, (d->nf - 1) * d->gf);
+      dgmx_status xs = exchange(d, visc_halo(d));
       if (xs != DGMX_OK) return xs;
     }
     if (d->partitioned() && d->nccl && !d->xhost && d->xstream) {
@@ -418,7 +447,7 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
     ++d->launches;
     if (d->hold && (e = d->hold_after(a, d->T[d->tcur ^ 1], nullptr)) != cudaSuccess)
       return d->cuda(e, "bulk-flow hold");
-    dgmx_status xs = exchange(d, d->T[d->tcur ^ 1], d->nf * d->gf);
+    dgmx_status xs = exchange(d, trace_halo(d, d->tcur ^ 1));
     if (xs != DGMX_OK) return xs;
     d->tcur ^= 1;
   }
@@ -431,32 +460,155 @@ int launches_per_stage(const dgmx_domain *d) {
   return (d->ns() ? 3 : 1) + (d->hold ? 2 : 0) + halo;
 }
 
-// Mixed form: the reference state the FP32 working copies are perturbations
-// about is the domain mean of U (any constant gives the same scheme; the
-// mean keeps the perturbations small); one row, see fill_reference_row.
-dgmx_status update_reference(dgmx_domain *d) {
-  const double c = std::pow(std::sqrt(2.0), d->dim);
-  cudaError_t e = launch_integrals(d->nf, d->ne, d->ld, c, d->U, d->Jdev, d->integ, d->stream);
-  ++d->launches;
-  double tot[5] = {0, 0, 0, 0, 0};
-  if (e == cudaSuccess) e = cudaMemcpyAsync(tot, d->integ, sizeof(double) * d->nf, cudaMemcpyDeviceToHost, d->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
-  if (e != cudaSuccess) return d->cuda(e, "reference state");
-  double vol = 0.0;
-  for (int k = 0; k < d->ne; ++k) vol += d->mesh.J[k];
-  vol *= std::pow(2.0, d->dim);
+// Host repeat of launch_reference_integrals' summation order over the
+// products rows[e][n] of ne elements in global element order: lane
+// l = e mod kRefLanes in increasing e, lanes pairwise with halving strides,
+// then times c_d.  Bit-identical to the kernel (every product and sum
+// rounded on its own there, IEEE double here).
+void reference_sum(const double *rows, int ne, int nf, double c_d, double *out) {
+  std::vector<double> red(kRefLanes);
+  for (int n = 0; n < nf; ++n) {
+    for (int l = 0; l < kRefLanes; ++l) {
+      double acc = 0.0;
+      for (int e = l; e < ne; e += kRefLanes) acc += rows[(size_t)e * nf + n];
+      red[l] = acc;
+    }
+    for (int s = kRefLanes / 2; s > 0; s >>= 1)
+      for (int l = 0; l < s; ++l) red[l] += red[l + s];
+    out[n] = c_d * red[0];
+  }
+}
+
+// The mixed form's reference row from the field integrals tot[0 .. nf) and
+// the sum of the element Jacobians, uploaded to d->uref.
+dgmx_status upload_reference(dgmx_domain *d, const double *tot, double jsum) {
+  const double vol = jsum * std::pow(2.0, d->dim);
   const double phi0 = std::pow(d->tab.B[0], d->dim);   // constant mode's value
   double h[kUrefStride] = {};
   for (int n = 0; n < d->nf; ++n) h[n] = tot[n] / vol;
   fill_reference_row(d->prm.physics, d->prm.gamma, phi0, h);
-  e = cudaMemcpyAsync(d->uref, h, sizeof(h), cudaMemcpyHostToDevice, d->stream);
+  cudaError_t e = cudaMemcpyAsync(d->uref, h, sizeof(h), cudaMemcpyHostToDevice, d->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
   return d->cuda(e, "reference state upload");
 }
 
-// traces of U into T[tcur]
+// This domain's per-element integrands J_e * Um[e][n][0] ([e][n], local
+// order) on the host; d->nod_out (nf * ne * qd doubles) is the scratch.
+dgmx_status element_integrands(dgmx_domain *d, std::vector<double> &rows) {
+  rows.assign((size_t)d->ne * d->nf, 0.0);
+  cudaError_t e = launch_element_integrands(d->nf, d->ne, d->ld, d->U, d->Jdev, d->nod_out, d->stream);
+  ++d->launches;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(rows.data(), d->nod_out, sizeof(double) * rows.size(), cudaMemcpyDeviceToHost, d->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+  return d->cuda(e, "element integrands");
+}
+
+// Every rank's cap blocks of blk doubles to every rank through the
+// domain's transport (NCCL sends between device buffers, or the caller's
+// host function): all[q * cap * blk ...] = rank q's blocks.  Collective.
+dgmx_status allgather_blocks(dgmx_domain *d, const std::vector<double> &mine, int cap, int blk,
+                             std::vector<double> &all) {
+  const int nr = d->plan.nranks, me = d->plan.rank;
+  const size_t per = (size_t)cap * blk;
+  all.assign((size_t)nr * per, 0.0);
+  std::copy(mine.begin(), mine.begin() + per, all.begin() + (size_t)me * per);
+  if (d->xhost) {
+    // the halo's conventions: peers in rank order, none to this rank itself
+    std::vector<double> snd((size_t)(nr - 1) * per), rcv((size_t)(nr - 1) * per);
+    std::vector<int> cnt(nr, cap), off(nr);
+    for (int q = 0; q < nr; ++q) {
+      off[q] = (q < me ? q : (q > me ? q - 1 : 0)) * cap;
+      if (q == me) cnt[q] = 0;
+      else std::copy(mine.begin(), mine.begin() + per, snd.begin() + (size_t)off[q] * blk);
+    }
+    if (d->xhost(d->xhost_ctx, snd.data(), rcv.data(), cnt.data(), off.data(), blk, nr) != 0)
+      return d->fail(DGMX_ERR_CUDA, "host transport reported a failure (reference state)");
+    for (int q = 0; q < nr; ++q)
+      if (q != me) std::copy(rcv.begin() + (size_t)off[q] * blk, rcv.begin() + (size_t)off[q] * blk + per,
+                             all.begin() + (size_t)q * per);
+    return DGMX_OK;
+  }
+  if (!d->nccl) return d->fail(DGMX_ERR_ARGUMENT, "partitioned domain without an exchange (dgmx_set_exchange_nccl)");
+  double *sb = nullptr, *rb = nullptr;
+  cudaError_t e = dalloc(&sb, per);
+  if (e == cudaSuccess) e = dalloc(&rb, (size_t)nr * per);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sb, mine.data(), sizeof(double) * per, cudaMemcpyHostToDevice, d->stream);
+  ncclResult_t r = ncclSuccess;
+  if (e == cudaSuccess) {
+    const NcclApi &nc = nccl_api();
+    r = nc.GroupStart();
+    for (int q = 0; q < nr && r == ncclSuccess; ++q) {
+      if (q == me) continue;
+      r = nc.Send(sb, per, ncclFloat64, q, d->nccl, d->stream);
+      if (r == ncclSuccess) r = nc.Recv(rb + (size_t)q * per, per, ncclFloat64, q, d->nccl, d->stream);
+    }
+    const ncclResult_t r2 = nc.GroupEnd();
+    if (r == ncclSuccess) r = r2;
+    if (r == ncclSuccess) {
+      for (int q = 0; q < nr && e == cudaSuccess; ++q)
+        if (q != me)
+          e = cudaMemcpyAsync(all.data() + (size_t)q * per, rb + (size_t)q * per, sizeof(double) * per,
+                              cudaMemcpyDeviceToHost, d->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+    }
+  }
+  if (sb) cudaFree(sb);
+  if (rb) cudaFree(rb);
+  if (r != ncclSuccess) return d->fail(DGMX_ERR_CUDA, std::string("reference state gather: ") + nccl_api().GetErrorString(r));
+  return d->cuda(e, "reference state gather");
+}
+
+// Mixed form: the reference state the FP32 working copies are perturbations
+// about is the domain mean of U (any constant gives the same scheme; the
+// mean keeps the perturbations small); one row, see fill_reference_row.
+// Its integrals follow one fixed summation order over the whole mesh
+// (launch_reference_integrals), so a partitioned domain (its ranks gather
+// every element's integrands) gets the row of the unpartitioned one, on
+// every rank.
+dgmx_status update_reference(dgmx_domain *d) {
+  const double c = std::pow(std::sqrt(2.0), d->dim);
+  double tot[5] = {0, 0, 0, 0, 0};
+  double jsum = 0.0;
+  if (!d->partitioned()) {
+    cudaError_t e = launch_reference_integrals(d->nf, d->ne, d->ld, c, d->U, d->Jdev, d->integ, d->stream);
+    ++d->launches;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(tot, d->integ, sizeof(double) * d->nf, cudaMemcpyDeviceToHost, d->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+    if (e != cudaSuccess) return d->cuda(e, "reference state");
+    for (int k = 0; k < d->ne; ++k) jsum += d->mesh.J[k];
+    return upload_reference(d, tot, jsum);
+  }
+  // ranks: blocks (global id, J, integrands) padded to max_ne per rank
+  std::vector<double> rows, all;
+  dgmx_status st = element_integrands(d, rows);
+  if (st != DGMX_OK) return st;
+  const int nf = d->nf, blk = nf + 2;
+  std::vector<double> mine((size_t)d->max_ne * blk, -1.0);
+  for (int e = 0; e < d->ne; ++e) {
+    double *b = &mine[(size_t)e * blk];
+    b[0] = d->plan.global_of_local[e];
+    b[1] = d->mesh.J[e];
+    for (int n = 0; n < nf; ++n) b[2 + n] = rows[(size_t)e * nf + n];
+  }
+  if ((st = allgather_blocks(d, mine, d->max_ne, blk, all)) != DGMX_OK) return st;
+  std::vector<double> R((size_t)d->ne_global * nf, 0.0), J(d->ne_global, 0.0);
+  for (size_t i = 0; i < all.size() / blk; ++i) {
+    const double *b = &all[i * blk];
+    const long g = (long)b[0];
+    if (g < 0 || g >= d->ne_global) continue;   // padding
+    J[g] = b[1];
+    for (int n = 0; n < nf; ++n) R[(size_t)g * nf + n] = b[2 + n];
+  }
+  reference_sum(R.data(), d->ne_global, nf, c, tot);
+  for (int k = 0; k < d->ne_global; ++k) jsum += J[k];
+  return upload_reference(d, tot, jsum);
+}
+
+// traces of U into T[tcur] (Tf[tcur] in the mixed form)
 dgmx_status refresh_traces(dgmx_domain *d) {
   if (d->mixed()) {
+    if (d->in_group) return DGMX_OK;   // the group sets its parts' reference state and traces
     const dgmx_status st = update_reference(d);
     if (st != DGMX_OK) return st;
   }
@@ -465,7 +617,7 @@ dgmx_status refresh_traces(dgmx_domain *d) {
                              : d->ops->traces_modal(a, d->U, d->T[d->tcur], d->stream);
   ++d->launches;
   if (e != cudaSuccess) return d->cuda(e, "trace kernel launch");
-  return exchange(d, d->T[d->tcur], d->nf * d->gf);
+  return exchange(d, trace_halo(d, d->tcur));
 }
 
 // Shallow-water balance: the first RHS ever evaluated is subtracted from all
@@ -480,7 +632,7 @@ dgmx_status capture_sw_source(dgmx_domain *d) {
   d->tcur ^= 1;
   d->sw_captured = true;
   if (e != cudaSuccess) return d->cuda(e, "shallow-water source capture");
-  return exchange(d, d->T[d->tcur], d->nf * d->gf);
+  return exchange(d, trace_halo(d, d->tcur));
 }
 
 dgmx_status check_error_word(dgmx_domain *d) {
@@ -647,8 +799,8 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
     return DGMX_ERR_ARGUMENT;
   }
   if (pspec && pspec->nranks > 1) {
-    if (d->mixed() || d->hold) {
-      g_create_error = "partitioned domains are FP64 without the bulk-flow hold";
+    if (d->hold) {
+      g_create_error = "the bulk-flow hold is not built for partitions";
       return DGMX_ERR_UNSUPPORTED;
     }
     if (pspec->group && phys == DGMX_SHALLOW && p->sw_balance) {
@@ -660,6 +812,10 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
       g_create_error = err;
       return DGMX_ERR_ARGUMENT;
     }
+    d->ne_global = d->mesh.ne;
+    std::vector<int> per(pspec->nranks, 0);
+    for (int e = 0; e < d->ne_global; ++e) ++per[pspec->part[e]];
+    d->max_ne = *std::max_element(per.begin(), per.end());
     d->mesh = std::move(local);
     d->ne = d->plan.ne_local;
     d->in_group = pspec->group;
@@ -771,7 +927,8 @@ dgmx_status enqueue_state_from_device_nodal(dgmx_domain *d, const double *Un_dev
     double vol = 0.0;
     for (int k = 0; k < d->ne; ++k) vol += d->mesh.J[k];
     vol *= std::pow(2.0, d->dim);
-    e = launch_integrals(d->nf, d->ne, d->ld, std::pow(std::sqrt(2.0), d->dim), d->U, d->Jdev, d->integ, d->stream);
+    e = launch_reference_integrals(d->nf, d->ne, d->ld, std::pow(std::sqrt(2.0), d->dim), d->U, d->Jdev, d->integ,
+                                   d->stream);
     if (e == cudaSuccess)
       e = launch_reference_row(d->prm.physics, d->nf, d->prm.gamma, std::pow(d->tab.B[0], d->dim), vol, d->integ,
                                d->uref, d->stream);
@@ -1209,7 +1366,7 @@ dgmx_status dgmx_time_derivative_device(dgmx_domain *d, const double *U_dev, dou
   cudaError_t e = d->ops->traces_nodal(a, d->stream);
   ++d->launches;
   if (e != cudaSuccess) return d->cuda(e, "nodal trace kernel");
-  dgmx_status xs = exchange(d, d->T[d->tcur ^ 1], d->nf * d->gf);
+  dgmx_status xs = exchange(d, fp64_halo(d->T[d->tcur ^ 1], d->nf * d->gf));
   if (xs != DGMX_OK) return xs;
   a.Tin = d->T[d->tcur ^ 1];
   if (d->prm.physics == DGMX_SHALLOW && d->prm.sw_balance) {
@@ -1220,7 +1377,7 @@ dgmx_status dgmx_time_derivative_device(dgmx_domain *d, const double *U_dev, dou
     if ((e = d->ns_grad(a, true, d->stream)) != cudaSuccess) return d->cuda(e, "viscous gradient kernel");
     if ((e = d->ns_visc(a, true, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
     d->launches += 2;
-    if ((xs = exchange(d, d->Vtr, (d->nf - 1) * d->gf)) != DGMX_OK) return xs;
+    if ((xs = exchange(d, visc_halo(d))) != DGMX_OK) return xs;
   }
   a.R0 = d->hold ? d->R0 : nullptr;
   e = d->ops->rhs_nodal(a, d->stream);
@@ -1489,14 +1646,14 @@ struct dgmx_group {
 
 namespace {
 
-// which = 0: T[tcur], 1: T[tcur ^ 1], 2: viscous traces; on stream s
+// which = 0: stage traces T[tcur], 1: T[tcur ^ 1] (Tf in the mixed form),
+// 2: viscous traces; on stream s
 dgmx_status group_exchange(dgmx_group *g, int which, cudaStream_t s) {
-  auto buf = [&](dgmx_domain *d) { return which == 2 ? d->Vtr : d->T[which == 0 ? d->tcur : d->tcur ^ 1]; };
-  dgmx_domain *d0 = g->parts[0];
-  const int blk = which == 2 ? (d0->nf - 1) * d0->gf : d0->nf * d0->gf;
+  auto halo = [&](dgmx_domain *d) { return which == 2 ? visc_halo(d) : trace_halo(d, which == 0 ? d->tcur : d->tcur ^ 1); };
+  const int blk = halo(g->parts[0]).wire();   // doubles per block in the send and receive buffers
   cudaError_t e = cudaSuccess;
   for (dgmx_domain *d : g->parts) {
-    if (e == cudaSuccess) e = launch_pack(buf(d), d->x_send, d->x_total, blk, d->x_sbuf, s);
+    if (e == cudaSuccess) e = halo(d).pack(d, s);
     ++d->launches;
   }
   const int n = (int)g->parts.size();
@@ -1508,10 +1665,41 @@ dgmx_status group_exchange(dgmx_group *g, int which, cudaStream_t s) {
                           sizeof(double) * blk * dr->x_cnt[q], cudaMemcpyDeviceToDevice, s);
     }
   for (dgmx_domain *d : g->parts) {
-    if (e == cudaSuccess) e = launch_unpack(d->x_rbuf, d->x_recv, d->x_total, blk, buf(d), s);
+    if (e == cudaSuccess) e = halo(d).unpack(d, s);
     ++d->launches;
   }
   if (e != cudaSuccess) { g->errmsg = std::string("group halo exchange: ") + cudaGetErrorString(e); return DGMX_ERR_CUDA; }
+  return DGMX_OK;
+}
+
+// Mixed form: one reference row for every part, the unpartitioned
+// domain's (the integrands of all parts in global element order, summed as
+// launch_reference_integrals does), then each part's FP32 traces.
+dgmx_status group_reference(dgmx_group *g) {
+  dgmx_domain *d0 = g->parts[0];
+  const int nf = d0->nf, ne = g->ne;
+  std::vector<double> R((size_t)ne * nf, 0.0), J(ne, 0.0), rows;
+  for (dgmx_domain *d : g->parts) {
+    dgmx_status st = element_integrands(d, rows);
+    if (st != DGMX_OK) { g->errmsg = d->errmsg; return st; }
+    for (int e = 0; e < d->ne; ++e) {
+      const int gid = d->plan.global_of_local[e];
+      J[gid] = d->mesh.J[e];
+      for (int n = 0; n < nf; ++n) R[(size_t)gid * nf + n] = rows[(size_t)e * nf + n];
+    }
+  }
+  double tot[5] = {0, 0, 0, 0, 0}, jsum = 0.0;
+  reference_sum(R.data(), ne, nf, std::pow(std::sqrt(2.0), d0->dim), tot);
+  for (int k = 0; k < ne; ++k) jsum += J[k];
+  for (dgmx_domain *d : g->parts) {
+    dgmx_status st = upload_reference(d, tot, jsum);
+    if (st != DGMX_OK) { g->errmsg = d->errmsg; return st; }
+    const StageArgs a = d->base_args();
+    cudaError_t e = d->ops_m->traces_modal(a, d->U, d->Tf[d->tcur], d->stream);
+    ++d->launches;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+    if (e != cudaSuccess) { g->errmsg = std::string("group traces: ") + cudaGetErrorString(e); return DGMX_ERR_CUDA; }
+  }
   return DGMX_OK;
 }
 
@@ -1575,7 +1763,9 @@ dgmx_status dgmx_group_set_state(dgmx_group *g, const double *U) {
     if (st != DGMX_OK) return group_fail(g, d, st);
   }
   cudaSetDevice(d0->prm.device);
-  dgmx_status st = group_exchange(g, 0, g->stream());
+  dgmx_status st = d0->mixed() ? group_reference(g) : DGMX_OK;
+  if (st != DGMX_OK) return st;
+  st = group_exchange(g, 0, g->stream());
   if (st != DGMX_OK) return st;
   return cudaStreamSynchronize(g->stream()) == cudaSuccess ? DGMX_OK : DGMX_ERR_CUDA;
 }

@@ -108,9 +108,12 @@ struct PartitionPlan {
 };
 bool partition_mesh(const HostMesh &g, const int *part, int nranks, int rank, HostMesh &local, PartitionPlan &plan,
                     std::string &err);
-// Pack / unpack of blk-double blocks by index (exchange.cu).
+// Pack / unpack of blk-value blocks by index (exchange.cu); the FP32 forms
+// place block i at buf + i * bs.
 cudaError_t launch_pack(const double *T, const int *idx, int n, int blk, double *buf, cudaStream_t s);
 cudaError_t launch_unpack(const double *buf, const int *idx, int n, int blk, double *T, cudaStream_t s);
+cudaError_t launch_pack(const float *T, const int *idx, int n, int blk, int bs, float *buf, cudaStream_t s);
+cudaError_t launch_unpack(const float *buf, const int *idx, int n, int blk, int bs, float *T, cudaStream_t s);
 
 // DGM input files (.inp/.msh/.con/.ord)
 struct FileCase {
@@ -310,6 +313,17 @@ void list_ops(std::vector<std::vector<int>> &out);
 // Field integrals from modal register mode 0: out[n] = sum_e J_e c_d Um[e][n][0].
 cudaError_t launch_integrals(int nf, int ne, int ld, double c_d, const double *Um, const double *J,
                              double *out, cudaStream_t s);
+// The mixed form's reference integrals in a fixed order a host can repeat:
+// field n's products J_e * Um[e][n][0], each rounded on its own, summed by
+// lane l = e mod kRefLanes in increasing e, then lanes pairwise (halving
+// strides), then times c_d.  Partitions gather the products
+// (launch_element_integrands, [e][n]) and sum them in that order on the
+// host (reference_sum), so every partition of a mesh gets the same row.
+constexpr int kRefLanes = 256;
+cudaError_t launch_reference_integrals(int nf, int ne, int ld, double c_d, const double *Um, const double *J,
+                                       double *out, cudaStream_t s);
+cudaError_t launch_element_integrands(int nf, int ne, int ld, const double *Um, const double *J, double *out,
+                                      cudaStream_t s);
 // The mixed form's reference row from those integrals, on the stream:
 // uref[0 .. kUrefStride) = fill_reference_row(integ / vol).
 cudaError_t launch_reference_row(int physics, int nf, double gamma, double phi0, double vol, const double *integ,

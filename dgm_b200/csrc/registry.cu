@@ -71,6 +71,48 @@ cudaError_t launch_integrals(int nf, int ne, int ld, double c_d, const double *U
   return cudaGetLastError();
 }
 
+// The mixed form's reference integrals (order in dgmx_internal.hpp): one
+// block of kRefLanes threads per field; products and sums rounded on
+// their own so that no contraction changes the order's result.
+__global__ void reference_integrals_kernel(int nf, int ne, int ld, double c_d, const double *Um, const double *J,
+                                           double *out) {
+  __shared__ double red[kRefLanes];
+  const int n = blockIdx.x, l = threadIdx.x;
+  double acc = 0.0;
+  for (int e = l; e < ne; e += kRefLanes) acc = __dadd_rn(acc, __dmul_rn(J[e], Um[((size_t)e * nf + n) * ld]));
+  red[l] = acc;
+  __syncthreads();
+  for (int s = kRefLanes / 2; s > 0; s >>= 1) {
+    if (l < s) red[l] = __dadd_rn(red[l], red[l + s]);
+    __syncthreads();
+  }
+  if (l == 0) out[n] = __dmul_rn(c_d, red[0]);
+}
+
+cudaError_t launch_reference_integrals(int nf, int ne, int ld, double c_d, const double *Um, const double *J,
+                                       double *out, cudaStream_t s) {
+  reference_integrals_kernel<<<nf, kRefLanes, 0, s>>>(nf, ne, ld, c_d, Um, J, out);
+  return cudaGetLastError();
+}
+
+// out[e][n] = J_e * Um[e][n][0], rounded as reference_integrals_kernel does.
+__global__ void element_integrands_kernel(int nf, int ne, int ld, const double *Um, const double *J, double *out) {
+  const long long total = (long long)ne * nf;
+  for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < total;
+       w += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(w / nf);
+    out[w] = __dmul_rn(J[e], Um[(size_t)w * ld]);
+  }
+}
+
+cudaError_t launch_element_integrands(int nf, int ne, int ld, const double *Um, const double *J, double *out,
+                                      cudaStream_t s) {
+  if (ne <= 0) return cudaSuccess;
+  const long long b = ((long long)ne * nf + 255) / 256;
+  element_integrands_kernel<<<(int)(b < 4 * 148 ? b : 4 * 148), 256, 0, s>>>(nf, ne, ld, Um, J, out);
+  return cudaGetLastError();
+}
+
 // One thread: the domain means integ / vol and the derived reference row.
 __global__ void reference_row_kernel(int physics, int nf, double gamma, double phi0, double vol,
                                      const double *integ, double *uref) {

@@ -121,7 +121,9 @@ dgmx_status dgmx_create_with_boundaries(const dgmx_mesh *mesh, const dgmx_params
  * increasing global order: its Field-layout arrays are over those elements);
  * faces whose neighbour lives on another rank read ghost slots that a halo
  * exchange fills after every stage (and after the viscous flux kernel for
- * Navier-Stokes).  FP64 only, no bulk-flow hold. */
+ * Navier-Stokes).  FP64 or DGMX_MIXED (FP32 trace blocks on the wire; the
+ * reference state is the unpartitioned domain's, from every rank's element
+ * integrals, so setting the state is collective); no bulk-flow hold. */
 dgmx_status dgmx_create_partition(const dgmx_mesh *mesh, const dgmx_params *params, const int *part, int nranks,
                                   int rank, dgmx_domain **out);
 /* NCCL transport for the multi-rank exchange: rank 0 makes the id, every

@@ -56,6 +56,57 @@ def test_group_equals_single_domain(case):
     G.close()
 
 
+MIXED_CASES = [
+    # name, physics, dim, n, lo, hi, p, flux, dt, steps, nparts, kind
+    ("euler3d-roe-p3-2-slabs", 8, 3, (4, 4, 4), 0.0, 2 * np.pi, 3, "roe", 0.002, 3, 2, "slabs"),
+    ("euler3d-lf-p2-3-random", 8, 3, (3, 3, 2), 0.0, 2 * np.pi, 2, "laxfriedrichs", 0.002, 3, 3, "random"),
+    ("euler2d-lf-p4-3-slabs", 1, 2, (5, 4), -5.0, 5.0, 4, "laxfriedrichs", 0.005, 3, 3, "slabs"),
+    ("shallow-lf-p3-2-random", 30, 2, (4, 4), -2.0, 2.0, 3, "laxfriedrichs", 0.001, 3, 2, "random"),
+]
+
+
+def _ic_mixed(phys, x, y, z):
+    if phys == 30:
+        return ics.gaussian_bump(x, y, a=0.3, w=0.5)
+    return _ic(phys, x, y, z)
+
+
+@pytest.mark.parametrize("case", MIXED_CASES, ids=[c[0] for c in MIXED_CASES])
+def test_mixed_group_equals_mixed_single_domain(case):
+    """The mixed form (FP32 traces, FP64 register, LSRK14) on an element
+    partition: every part takes the unpartitioned domain's reference state
+    (the integrals summed over the whole mesh in one fixed order), the FP32
+    trace blocks cross in the halo, and the state equals the unpartitioned
+    mixed domain's bit for bit; it stays within 1e-6 of the FP64 oracle."""
+    import dgm_b200
+    _, phys, dim, n, lo, hi, p, flux, dt, steps, nparts, kind = case
+    m = dgm_b200.meshgen.box(dim, n, lo, hi, p)
+    ne = m.verts.shape[0]
+    part = ((np.arange(ne) * nparts) // ne if kind == "slabs"
+            else np.random.default_rng(7).permutation(np.arange(ne) % nparts))
+    D = dgm_b200.Domain(m, phys, flux=flux, inttype=dgm_b200.LSRK14, precision=dgm_b200.MIXED, sw_balance=False)
+    G = dgm_b200.Group(m, phys, part, flux=flux, inttype=dgm_b200.LSRK14, precision=dgm_b200.MIXED)
+    x, y, z = D.coordinates()
+    f = _ic_mixed(phys, x, y, z)
+    D.set_state(f)
+    G.set_state(f)
+    assert np.array_equal(G.state(), D.state())
+    D.advance(dt, steps)
+    G.advance(dt, steps)
+    S = D.state()
+    assert np.array_equal(G.state(), S)
+    P = oracle.Problem(dgm_io.Mesh(m.dim, m.verts, m.con, m.porder, m.qorder), phys, flux=flux)
+    if phys == oracle.SHALLOW:
+        P.set_sw_balance(False)
+    U0 = P.project(f)
+    P.set_state(U0)
+    P.advance(14, dt, steps)
+    O = P.state()
+    err = float(np.sqrt(((S - O) ** 2).sum() / (O ** 2).sum()))
+    assert 1e-13 < err < 1e-6, err
+    G.close()
+
+
 def test_partition_handles_and_nccl_id():
     """A rank's handle covers its own elements; the NCCL id is made through
     the lazily loaded NCCL library; stepping without an exchange is refused."""
@@ -83,11 +134,11 @@ def _rank_run(rank, nranks, port, case, result):
     _os.environ["MASTER_ADDR"] = "127.0.0.1"
     _os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=nranks, timeout=datetime.timedelta(seconds=60))
-    phys, n, p, flux, inttype, dt, steps, vis = case
+    phys, n, p, flux, inttype, dt, steps, vis, prec = case
     m = dgm_b200.meshgen.box(3, n, 0.0, 2 * np.pi, p)
     ne = m.verts.shape[0]
     part = (np.arange(ne) * nranks) // ne
-    D = dgm_b200.Domain.partition(m, phys, part, nranks, rank, flux=flux, inttype=inttype, vis=vis)
+    D = dgm_b200.Domain.partition(m, phys, part, nranks, rank, flux=flux, inttype=inttype, vis=vis, precision=prec)
     D.set_exchange_host()
     nl, ng, gids = D.partition_info()
     x, y, z = D.coordinates()
@@ -98,12 +149,15 @@ def _rank_run(rank, nranks, port, case, result):
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("case", [(8, (3, 2, 4), 3, "roe", 14, 0.002, 2, 0.0),
-                                  (9, (2, 2, 3), 2, "laxfriedrichs", 3, 0.002, 2, 0.02)],
-                         ids=["euler3d-lsrk14", "ns3d-tvd3"])
+@pytest.mark.parametrize("case", [(8, (3, 2, 4), 3, "roe", 14, 0.002, 2, 0.0, 0),
+                                  (9, (2, 2, 3), 2, "laxfriedrichs", 3, 0.002, 2, 0.02, 0),
+                                  (8, (3, 2, 4), 3, "roe", 14, 0.002, 2, 0.0, 1)],
+                         ids=["euler3d-lsrk14", "ns3d-tvd3", "euler3d-lsrk14-mixed"])
 def test_two_process_ranks_equal_single_domain(case):
     """Two processes, each one rank of a partitioned domain, exchanging halos
-    through the host: the gathered state equals the unpartitioned run."""
+    through the host: the gathered state equals the unpartitioned run (the
+    mixed form's ranks gather the reference state's element integrals
+    through the same transport)."""
     import socket
     import torch.multiprocessing as mp
     import dgm_b200
@@ -121,9 +175,9 @@ def test_two_process_ranks_equal_single_domain(case):
         if pr.is_alive():
             pr.kill()
         assert pr.exitcode == 0
-    phys, n, p, flux, inttype, dt, steps, vis = case
+    phys, n, p, flux, inttype, dt, steps, vis, prec = case
     m = dgm_b200.meshgen.box(3, n, 0.0, 2 * np.pi, p)
-    D = dgm_b200.Domain(m, phys, flux=flux, inttype=inttype, vis=vis)
+    D = dgm_b200.Domain(m, phys, flux=flux, inttype=inttype, vis=vis, precision=prec)
     x, y, z = D.coordinates()
     D.set_state(ics.taylor_green(x, y, z, Ma=0.1))
     D.advance(dt, steps)
