@@ -31,10 +31,13 @@ initial state.  A "step" is one LSRK14 step (14 fused stage launches).
          the Navier-Stokes Taylor-Green (24^3, p=7, q=9) in FP64, with the
          FP32 viscous kernels and with their 3xTF32 contractions, and the
          reference's channel regression case against its golden restart
-Ranks (torchrun, N > 1) run independent replicas of the workload (weak
-scaling, no collective in the data path; NCCL only for the barrier and the
-max-over-ranks time).  --impl reference times the CPU restatement of the
-reference algorithm (the oracle) on the host cores instead.
+Ranks (torchrun, N > 1) run the workload as an element partition, one
+z-slab of n^3 elements per GPU on a box that grows with N (weak scaling),
+with the face-trace halo after every stage over NCCL, overlapped with the
+interior tiles (run_partitioned); --layout replicas runs independent copies
+instead, and --transport host stages the halo through the host over gloo.
+--impl reference times the CPU restatement of the reference algorithm (the
+oracle) on the host cores instead.
 """
 from __future__ import annotations
 
@@ -89,6 +92,12 @@ def parse():
                          "JSON (profiling)")
     ap.add_argument("--variant", type=int, default=-1,
                     help="single-form runs: use this tile variant instead of the autotuner's pick")
+    ap.add_argument("--layout", choices=["partition", "replicas"], default="partition",
+                    help="N > 1: one element partition per GPU with a halo exchange (weak scaling: the box "
+                         "grows by n^3 elements per GPU), or independent replicas")
+    ap.add_argument("--transport", choices=["nccl", "host"], default="nccl",
+                    help="partitioned halo over NCCL (device buffers, overlapped), or staged through the host "
+                         "over a gloo process group (ranks may then share one GPU)")
     return ap.parse_args()
 
 
@@ -203,16 +212,25 @@ def cpu_measure(n, p, q, stages_sample, threads):
     return dof * 14 * stages_sample / t, t
 
 
-def config_dict(n, p, q, dof, world=1):
+def config_dict(n, p, q, dof, world=1, layout="partition", transport="nccl"):
     """The workload, identical for both arms (the precision and the tile each
-    arm runs are reported outside `config`)."""
-    return {"workload": WORKLOAD["name"] if n == WORKLOAD["n"] else f"euler3d_taylor_green_{n}^3_p{p}_roe_lsrk14",
-            "mesh": f"{n}^3 Hex, periodic [0,2pi]^3", "p": p, "q": q, "physics": "Euler 3-D",
-            "flux": "Roe", "integrator": "LSRK14 (14 stages/step)", "Mach": WORKLOAD["Ma"],
-            "modal_dof": dof, "cfl": WORKLOAD["cfl"],
-            "parallelism": f"replicas x{world}" if world > 1 else "single device",
-            "l2": "inputs larger than L2 (modal U 84 MB + Ut 42 MB, traces 2x63 MB per replica in the mixed "
-                  "form; 168 + 2x126 MB in FP64)"}
+    arm runs are reported outside `config`).  dof: modal DOF per GPU."""
+    c = {"workload": WORKLOAD["name"] if n == WORKLOAD["n"] else f"euler3d_taylor_green_{n}^3_p{p}_roe_lsrk14",
+         "mesh": f"{n}^3 Hex, periodic [0,2pi]^3", "p": p, "q": q, "physics": "Euler 3-D",
+         "flux": "Roe", "integrator": "LSRK14 (14 stages/step)", "Mach": WORKLOAD["Ma"],
+         "modal_dof": dof, "cfl": WORKLOAD["cfl"], "parallelism": "single device",
+         "l2": "inputs larger than L2 (modal U 84 MB + Ut 42 MB, traces 2x63 MB per GPU in the mixed "
+               "form; 168 + 2x126 MB in FP64)"}
+    if world > 1 and layout == "partition":
+        c["mesh"] = f"{n}x{n}x{n * world} Hex, periodic [0,2pi]^2 x [0,{2 * world}pi]"
+        c["modal_dof"] = dof * world
+        c["parallelism"] = (f"element partition: {world} z-slabs of {n}^3 elements, one per GPU; halo exchange of "
+                            f"the face traces after every stage over "
+                            + ("NCCL, overlapped with the interior tiles" if transport == "nccl"
+                               else "the host (process group point-to-point)"))
+    elif world > 1:
+        c["parallelism"] = f"replicas x{world} (independent copies, no halo)"
+    return c
 
 
 def run_reference(args):
@@ -239,7 +257,8 @@ def run_reference(args):
     out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference",
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-           "data": "synthetic (Taylor-Green initial condition)", "config": config_dict(n, p, q, dof, args.gpus),
+           "data": "synthetic (Taylor-Green initial condition)",
+           "config": config_dict(n, p, q, dof, args.gpus, args.layout, args.transport),
            "precision": "FP64 (the oracle: CPU restatement of the reference algorithm)",
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                             "sample": f"{args.steps} LSRK14 steps of the full workload after {args.warmup} warm-up"},
@@ -655,6 +674,137 @@ def forms(dgm_b200, args, serve=True):
     return res
 
 
+def run_partitioned(args, torch, dgm_b200, dist, rank, world, local):
+    """N > 1: the workload as an element partition, one rank per GPU (weak
+    scaling).  The Taylor-Green box grows along z to n x n x nN elements over
+    [0,2pi]^2 x [0,2pi N] (the initial condition is 2pi-periodic, so every
+    rank's slab of n^3 elements holds the single-GPU problem), rank r owns the
+    z-slab r, and after every stage the face traces on the slab faces cross to
+    the neighbouring ranks: over NCCL from device buffers while the interior
+    tiles run (dgmx_set_exchange_nccl, the overlapped stage), or with
+    --transport host through pinned host memory and the process group.  Both
+    forms (FP64 and mixed) are timed on the device (CUDA events on the
+    engine's stream, max over ranks); e2e uploads every rank's state from
+    pinned host memory, advances one step and reads it back.  The partitioned
+    state equals the unpartitioned one bit for bit (tests/test_gpu_partition.py),
+    so the accuracy figures are those of the single-GPU line."""
+    n, p, q = args.n, WORKLOAD["p"], WORKLOAD["q"]
+    host = args.transport == "host"
+    L = 2 * math.pi
+    mesh = dgm_b200.meshgen.box(3, (n, n, n * world), 0.0, (L, L, L * world), p, q)
+    part = (np.arange(n ** 3 * world) // n ** 3).astype(np.int32)   # element e = i + n (j + n k): z-slabs
+    dof = 5 * n ** 3 * (p + 1) ** 3                                  # per rank
+
+    def barrier():
+        dist.barrier()
+        torch.cuda.synchronize()
+
+    def reduce(v, op):
+        t = torch.tensor([v], dtype=torch.float64, device="cpu" if host else "cuda")
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max_over_ranks(v):
+        return reduce(v, dist.ReduceOp.MAX)
+
+    nid = None
+    if not host:
+        obj = [dgm_b200.nccl_unique_id() if rank == 0 else None]
+        dist.broadcast_object_list(obj, src=0)
+        nid = obj[0]
+    doms, tiles = {}, {}
+    U_ic = dt = None
+    for name, prec in (("fp64", dgm_b200.FP64), ("mixed", dgm_b200.MIXED)):
+        D = dgm_b200.Domain.partition(mesh, dgm_b200.EULER3D, part, world, rank, flux=WORKLOAD["flux"],
+                                      inttype=dgm_b200.LSRK14, device=local, precision=prec)
+        if host:
+            D.set_exchange_host()
+        else:
+            D.set_exchange_nccl(nid)
+        if U_ic is None:
+            x, y, z = D.coordinates()
+            U_ic = taylor_green(x, y, z, WORKLOAD["Ma"], WORKLOAD["gamma"])
+            dt = -reduce(-cfl_dt(U_ic, L / n, p, WORKLOAD["gamma"], WORKLOAD["cfl"]), dist.ReduceOp.MAX)
+        D.set_state(U_ic)
+        rows, pick = D.autotune(reps=10)
+        pick = int(-reduce(-pick, dist.ReduceOp.MAX))   # one tile for every rank (rank-order independent)
+        _, kind = D.set_variant(pick)
+        D.set_state(U_ic)
+        tiles[name] = {"variant": pick,
+                       "kernel": {2: "stage_pipe_kernel", 3: "stage2_kernel"}.get(kind, "stage_kernel"),
+                       "elements_per_cta": int(rows[pick][0]), "min_ctas_per_sm": int(rows[pick][1]),
+                       "threads_per_cta": int(rows[pick][2])}
+        doms[name] = D
+    streams = {k: torch.cuda.ExternalStream(D.stream(), device=torch.device("cuda", local)) for k, D in doms.items()}
+    clk = ClockSampler(local)
+    t64, _ = time_steps(doms["fp64"], streams["fp64"], dt, args.steps, args.warmup, barrier, max_over_ranks)
+    tmx, launches = time_steps(doms["mixed"], streams["mixed"], dt, args.steps, args.warmup, barrier,
+                               max_over_ranks, clk)
+    value = world * dof * 14 * args.steps / tmx
+    v64 = world * dof * 14 * args.steps / t64
+
+    def e2e(D, stream):
+        Uh = torch.empty((5, D.nq), dtype=torch.float64, pin_memory=True).numpy()
+        Uh[:] = U_ic
+        for _ in range(max(1, args.warmup)):
+            D.set_state(Uh)
+            D.advance(dt, 1)
+            D.state_into(Uh)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k = max(3, args.steps // 2)
+        e0.record(stream)
+        for _ in range(k):
+            D.set_state(Uh)
+            D.advance(dt, 1)
+            D.state_into(Uh)
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+        nbytes = world * 5 * D.nq * 8
+        return {"value": world * dof * 14 * k / t, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": nbytes, "steps": k,
+                "path": "per step on every rank: dgmx_set_state (pinned host -> device, projection, reference "
+                        "state and traces with their halo) + dgmx_advance (1 step) + dgmx_get_state (device -> "
+                        "pinned host); bytes summed over the ranks"}
+
+    e2e_res = {name: e2e(D, streams[name]) for name, D in doms.items()}
+    peak, pkind = peaks()
+    stage_mx, stage_64 = tmx / (14 * args.steps), t64 / (14 * args.steps)
+
+    def roof(prec, stage_s, prof):
+        a = BYTES_PER_DOF_STAGE[prec] * dof / stage_s / 1e9
+        return {"bound": "hbm", "achieved": a, "peak": peak, "unit": "GB/s", "frac": a / peak,
+                "peak_kind": pkind, "traffic": profile_traffic(prof),
+                "kernel": f"{tiles[prec]['kernel']}<Euler3D, L=4, Q=5, {prec}> (boundary and interior tiles of "
+                          f"one rank, per GPU; the stage time includes the halo)",
+                "algorithmic_bytes_per_launch": BYTES_PER_DOF_STAGE[prec] * dof, "stage_us": 1e6 * stage_s}
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tmx / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 solution register)",
+           "data": "synthetic (Taylor-Green initial condition, no dataset)",
+           "config": config_dict(n, p, q, dof, world, "partition", args.transport),
+           "precision": "mixed: FP32 states, fluxes and contractions, FP64 solution register",
+           "tile": tiles["mixed"],
+           "fp64": {"value": v64, "unit": UNIT, "ms_per_step": 1e3 * t64 / args.steps, "tile": tiles["fp64"],
+                    "roofline": roof("fp64", stage_64, "euler3d_tgv_p3_stage_kernel.md"), "e2e": e2e_res["fp64"]},
+           "speedup_mixed_vs_fp64": value / v64,
+           "accuracy": {"note": "the partitioned state equals the unpartitioned one bit for bit in both forms "
+                                "(tests/test_gpu_partition.py); the per-field errors are the single-GPU line's"},
+           "e2e": e2e_res["mixed"],
+           "gpu_launches": int(launches), "clocks": clk.summary(),
+           "roofline": roof("mixed", stage_mx, "euler3d_tgv_p3_stage_mixed.md")}
+    for D in doms.values():
+        D.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -664,6 +814,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.layout == "partition" and args.transport == "host":
+        local %= max(1, torch.cuda.device_count())   # host-staged ranks may share a GPU (no kernel waits on a peer)
     torch.cuda.set_device(local)
     if args.only:
         if rank == 0:
@@ -672,11 +824,17 @@ def main():
             print(json.dumps(res), flush=True)
         return 0
     dist = None
+    host_pg = world > 1 and args.layout == "partition" and args.transport == "host"
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        if host_pg:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+        else:
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+    if world > 1 and args.layout == "partition":
+        return run_partitioned(args, torch, dgm_b200, dist, rank, world, local)
     n, p, q = args.n, WORKLOAD["p"], WORKLOAD["q"]
     mesh = dgm_b200.meshgen.box(3, (n, n, n), 0.0, 2 * math.pi, p, q)
     dof = 5 * n ** 3 * (p + 1) ** 3
@@ -801,7 +959,7 @@ def main():
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tmx / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 solution register)",
            "data": "synthetic (Taylor-Green initial condition, no dataset)",
-           "config": config_dict(n, p, q, dof, world),
+           "config": config_dict(n, p, q, dof, world, "replicas"),
            "precision": "mixed: FP32 states, fluxes and contractions, FP64 solution register",
            "tile": tiles["mixed"],
            "fp64": {"value": v64, "unit": UNIT, "ms_per_step": 1e3 * t64 / args.steps, "tile": tiles["fp64"],

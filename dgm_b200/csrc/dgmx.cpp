@@ -456,8 +456,10 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
 
 int stages_per_step(int inttype) { return inttype == DGMX_LSRK14 ? 14 : (inttype == DGMX_TVD3 ? 3 : 4); }
 int launches_per_stage(const dgmx_domain *d) {
-  const int halo = d->partitioned() && !d->in_group ? (d->ns() ? 4 : 2) : 0;   // pack + unpack per exchange
-  return (d->ns() ? 3 : 1) + (d->hold ? 2 : 0) + halo;
+  const bool rank = d->partitioned() && !d->in_group;
+  const int halo = rank ? (d->ns() ? 4 : 2) : 0;   // pack + unpack per exchange
+  const int split = rank && d->nccl && !d->xhost && d->xstream ? 1 : 0;   // boundary and interior tiles
+  return (d->ns() ? 3 : 1) + split + (d->hold ? 2 : 0) + halo;
 }
 
 // Host repeat of launch_reference_integrals' summation order over the
