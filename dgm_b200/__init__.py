@@ -111,6 +111,16 @@ def kernel_list():
 BC_SLIP_WALL, BC_ISOTHERMAL_WALL, BC_STATE, BC_SUBSONIC_OUTFLOW, BC_SUPERSONIC_OUTFLOW = 1, 2, 3, 4, 5
 
 
+def _bc_arrays(boundaries):
+    """(count, sides [n][3] int32, parameters [n][5]) of boundary records
+    (element, side, kind, up to five parameters); count 0 for None."""
+    recs = list(boundaries) if boundaries is not None else []
+    r = np.zeros((max(len(recs), 1), 8))
+    for i, rec in enumerate(recs):
+        r[i, :len(rec)] = rec
+    return (len(recs), np.ascontiguousarray(r[:, :3].astype(np.int32)), np.ascontiguousarray(r[:, 3:8]))
+
+
 class Domain:
     """One DGM Domain on one GPU (Field layout [field][element][Q^d])."""
 
@@ -157,26 +167,32 @@ class Domain:
     @classmethod
     def partition(cls, mesh, physics: int, part, nranks: int, rank: int, flux: str = "laxfriedrichs",
                   inttype: int = LSRK14, gamma: float = 1.4, vis: float = 0.0, Pr: float = 0.72,
-                  sw_balance: bool = True, device: int = 0, precision: int = FP64):
+                  sw_balance: bool = True, device: int = 0, precision: int = FP64, boundaries=None,
+                  bulk_hold: bool = False):
         """The rank's part of an element partition (part[e] = owning rank);
         its arrays cover its own elements in increasing global order.  Call
         set_exchange_nccl (or set_exchange_host) on every rank before
         setting the state: with precision=MIXED, set_state gathers every
-        rank's element integrals for the common reference state."""
+        rank's element integrals for the common reference state.
+        boundaries: the records of the constructor, global element ids;
+        bulk_hold: the channel's hold with its means over the whole mesh."""
         m, keep = _mesh_struct(mesh)
         part = np.ascontiguousarray(part, dtype=np.int32)
         p = _Params(physics, FLUX[flux.lower()], inttype, precision, 1 if sw_balance else 0, device, gamma, vis, Pr)
         h = ctypes.c_void_p()
-        f = lib().dgmx_create_partition
+        nbc, sides, par = _bc_arrays(boundaries)
+        f = lib().dgmx_create_partition_with_boundaries
         f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
-                      ctypes.c_void_p]
+                      ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
         st = f(ctypes.byref(m), ctypes.byref(p), part.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), int(nranks),
-               int(rank), ctypes.byref(h))
+               int(rank), nbc, sides.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(par), ctypes.byref(h))
         if st != 0:
             raise DgmxError(st, lib().dgmx_last_error(None).decode())
         self = cls.__new__(cls)
-        self._keep = keep + [part]
+        self._keep = keep + [part, sides, par]
         self._init(h, mesh.dim)
+        if bulk_hold:
+            self.set_bulk_hold(True)
         return self
 
     def set_exchange_nccl(self, nccl_id: bytes):
@@ -644,15 +660,20 @@ class Group:
     are global (Field layout over all elements)."""
 
     def __init__(self, mesh, physics: int, part, flux: str = "laxfriedrichs", inttype: int = LSRK14,
-                 gamma: float = 1.4, vis: float = 0.0, Pr: float = 0.72, device: int = 0, precision: int = FP64):
+                 gamma: float = 1.4, vis: float = 0.0, Pr: float = 0.72, device: int = 0, precision: int = FP64,
+                 boundaries=None, bulk_hold: bool = False):
         m, self._keep = _mesh_struct(mesh)
         part = np.ascontiguousarray(part, dtype=np.int32)
         self._keep.append(part)
         self.nparts = int(part.max()) + 1
         p = _Params(physics, FLUX[flux.lower()], inttype, precision, 0, device, gamma, vis, Pr)
         L = lib()
-        L.dgmx_group_create.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
-                                        ctypes.c_void_p]
+        nbc, sides, par = _bc_arrays(boundaries)
+        self._keep += [sides, par]
+        L.dgmx_group_create_with_boundaries.argtypes = [
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+            ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+        L.dgmx_group_set_bulk_hold.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.dgmx_group_last_error.restype = ctypes.c_char_p
         L.dgmx_group_last_error.argtypes = [ctypes.c_void_p]
         for n in ("dgmx_group_set_state", "dgmx_group_get_state"):
@@ -660,11 +681,14 @@ class Group:
         L.dgmx_group_advance.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.dgmx_group_destroy.argtypes = [ctypes.c_void_p]
         h = ctypes.c_void_p()
-        st = L.dgmx_group_create(ctypes.byref(m), ctypes.byref(p), part.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                                 self.nparts, ctypes.byref(h))
+        st = L.dgmx_group_create_with_boundaries(
+            ctypes.byref(m), ctypes.byref(p), part.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), self.nparts, nbc,
+            sides.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(par), ctypes.byref(h))
         if st != 0:
             raise DgmxError(st, L.dgmx_group_last_error(None).decode())
         self.h = h
+        if bulk_hold:
+            self._check(L.dgmx_group_set_bulk_hold(self.h, 1))
         self.nf = 3 if physics == SHALLOW else (5 if physics in (EULER3D, NS3D) else 4)
         q = int(mesh.qorder[0]) or int(mesh.porder[0]) + 2
         self.nq = int(mesh.verts.shape[0]) * q ** int(mesh.dim)

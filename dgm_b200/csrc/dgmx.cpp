@@ -121,6 +121,11 @@ struct dgmx_domain {
   // exchange lists (plan.nranks == 1: the whole mesh, no exchange)
   PartitionPlan plan;
   int ne_global = 0, max_ne = 0;                         // whole mesh; most elements of one rank
+  // bulk-flow hold on a partition: every rank's constant coefficients in
+  // the whole mesh's order, so cbar is the unpartitioned domain's
+  double *R0g = nullptr, *Jg = nullptr;                  // [ne_global][nf], [ne_global]
+  double *hold_rows = nullptr;                           // [nranks][max_ne][nf] as received
+  int *gid_all = nullptr;                                // [nranks][max_ne] global ids (-1: padding)
   int nslot = 0;                                         // ne + ghost slots
   int *x_send = nullptr, *x_recv = nullptr;              // concatenated block lists (device)
   std::vector<int> x_cnt, x_off;                         // per peer block counts and offsets
@@ -192,15 +197,31 @@ struct dgmx_domain {
     }
     return a;
   }
-  // bulk-flow hold after a stage of kind a.kind (hold.cu); Fn: nodal RHS
-  cudaError_t hold_after(const StageArgs &a, double *Tout, double *Fn) {
+  // bulk-flow hold after a stage of kind a.kind (hold.cu) over this
+  // handle's elements; Fn: nodal RHS
+  HoldArgs hold_args(const StageArgs &a, double *Tout, double *Fn) const {
     HoldArgs h;
     h.ne = ne; h.nf = nf; h.ld = ld; h.gf = gf; h.qd = qd; h.nfaces = nfaces;
     h.R0 = R0; h.J = Jdev; h.cbar = cbar;
     h.kind = a.kind; h.c0 = a.c0; h.c1 = a.c1; h.dt = a.dt;
     h.U = a.U; h.Ut = a.Ut; h.A = a.A; h.Tout = Tout; h.Fn = Fn;
+    return h;
+  }
+  cudaError_t hold_after(const StageArgs &a, double *Tout, double *Fn) {
     launches += 2;
-    return launch_hold(h, stream);
+    return launch_hold(hold_args(a, Tout, Fn), stream);
+  }
+  // the same with the means taken over the whole mesh: R0g / Jg in global
+  // element order (filled by the caller), cbar then applied here
+  cudaError_t hold_after_global(const StageArgs &a, double *Tout, double *Fn, double *cb) {
+    HoldArgs g = hold_args(a, Tout, Fn);
+    g.ne = ne_global; g.R0 = R0g; g.J = Jg; g.cbar = cb;
+    cudaError_t e = launch_hold_reduce(g, stream);
+    HoldArgs h = hold_args(a, Tout, Fn);
+    h.cbar = cb;
+    if (e == cudaSuccess) e = launch_hold_apply(h, stream);
+    launches += 2;
+    return e;
   }
   bool ns() const { return prm.physics == DGMX_NS2D || prm.physics == DGMX_NS3D; }
   cudaError_t ns_grad(const StageArgs &a, bool nodal, cudaStream_t s) const {
@@ -218,7 +239,8 @@ struct dgmx_domain {
     if (graph) cudaGraphExecDestroy(graph);
     graph = nullptr;
     void *ptrs[] = {U, Ut, Acc, T[0], T[1], Rsw, nod_in, nod_out, Jdev, integ, gclass, perm, err, classes, links,
-                    Ghat, Vtr, Pv, Utf, Tf[0], Tf[1], uref, R0, cbar, x_send, x_recv, x_sbuf, x_rbuf, tiles, Ssrc};
+                    Ghat, Vtr, Pv, Utf, Tf[0], Tf[1], uref, R0, cbar, x_send, x_recv, x_sbuf, x_rbuf, tiles, Ssrc,
+                    R0g, Jg, hold_rows, gid_all};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (host_pinned) cudaFreeHost(host_pinned);
     if (xh_send) cudaFreeHost(xh_send);
@@ -232,6 +254,7 @@ struct dgmx_domain {
     Utf = Tf[0] = Tf[1] = nullptr;
     uref = nullptr;
     R0 = cbar = Ssrc = nullptr;
+    R0g = Jg = hold_rows = nullptr; gid_all = nullptr;
     x_send = x_recv = nullptr; x_sbuf = x_rbuf = nullptr; tiles = nullptr; tiles_epb = 0;
     if (ev_b) cudaEventDestroy(ev_b);
     if (ev_x) cudaEventDestroy(ev_x);
@@ -308,6 +331,50 @@ dgmx_status exchange(dgmx_domain *d, const Halo &h) {
   e = h.unpack(d, d->stream);
   d->launches += 2;
   return d->cuda(e, "halo unpack");
+}
+
+dgmx_status allgather_blocks(dgmx_domain *d, const std::vector<double> &mine, int cap, int blk,
+                             std::vector<double> &all);
+
+// Bulk-flow hold on a rank of a partition: this rank's constant
+// coefficients go to every peer (NCCL sends on the stream, or the host
+// transport), all ranks' rows are scattered into the whole mesh's order
+// (R0g), and the means over R0g / Jg, the unpartitioned domain's cbar, are
+// applied to this rank's elements.  Elsewhere: the handle's own hold.
+dgmx_status hold_stage(dgmx_domain *d, const StageArgs &a, double *Tout, double *Fn) {
+  if (!d->partitioned() || d->in_group) return d->cuda(d->hold_after(a, Tout, Fn), "bulk-flow hold");
+  const int nr = d->plan.nranks, me = d->plan.rank, nf = d->nf;
+  const size_t per = (size_t)d->max_ne * nf;
+  double *mine = d->hold_rows + (size_t)me * per;
+  cudaError_t e = cudaMemcpyAsync(mine, d->R0, sizeof(double) * d->ne * nf, cudaMemcpyDeviceToDevice, d->stream);
+  if (e != cudaSuccess) return d->cuda(e, "bulk-flow hold rows");
+  if (d->xhost) {
+    std::vector<double> h(per, 0.0), all;
+    e = cudaMemcpyAsync(h.data(), mine, sizeof(double) * d->ne * nf, cudaMemcpyDeviceToHost, d->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+    if (e != cudaSuccess) return d->cuda(e, "bulk-flow hold rows");
+    const dgmx_status st = allgather_blocks(d, h, d->max_ne, nf, all);
+    if (st != DGMX_OK) return st;
+    e = cudaMemcpyAsync(d->hold_rows, all.data(), sizeof(double) * all.size(), cudaMemcpyHostToDevice, d->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+    if (e != cudaSuccess) return d->cuda(e, "bulk-flow hold rows");
+  } else {
+    if (!d->nccl) return d->fail(DGMX_ERR_ARGUMENT, "partitioned domain without an exchange (dgmx_set_exchange_nccl)");
+    const NcclApi &nc = nccl_api();
+    ncclResult_t r = nc.GroupStart();
+    for (int q = 0; q < nr && r == ncclSuccess; ++q) {
+      if (q == me) continue;
+      r = nc.Send(mine, per, ncclFloat64, q, d->nccl, d->stream);
+      if (r == ncclSuccess) r = nc.Recv(d->hold_rows + (size_t)q * per, per, ncclFloat64, q, d->nccl, d->stream);
+    }
+    const ncclResult_t r2 = nc.GroupEnd();
+    if (r == ncclSuccess) r = r2;
+    if (r != ncclSuccess) return d->fail(DGMX_ERR_CUDA, std::string("bulk-flow hold rows: ") + nc.GetErrorString(r));
+  }
+  e = launch_scatter_rows(d->hold_rows, d->gid_all, nr * d->max_ne, nf, d->R0g, d->stream);
+  ++d->launches;
+  if (e == cudaSuccess) e = d->hold_after_global(a, Tout, Fn, d->cbar);
+  return d->cuda(e, "bulk-flow hold");
 }
 
 // The stages of one step: kind, whether the RHS is evaluated on Ut (else U)
@@ -436,7 +503,7 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
       dgmx_status xs = exchange(d, visc_halo(d));
       if (xs != DGMX_OK) return xs;
     }
-    if (d->partitioned() && d->nccl && !d->xhost && d->xstream) {
+    if (d->partitioned() && d->nccl && !d->xhost && d->xstream && !d->hold) {   // the hold needs all tiles first
       const dgmx_status xs = stage_overlapped(d, a);
       if (xs != DGMX_OK) return xs;
       d->tcur ^= 1;
@@ -445,8 +512,10 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
     e = d->stage_ops()->stage(a, d->stream);
     if (e != cudaSuccess) return d->cuda(e, "stage kernel launch");
     ++d->launches;
-    if (d->hold && (e = d->hold_after(a, d->T[d->tcur ^ 1], nullptr)) != cudaSuccess)
-      return d->cuda(e, "bulk-flow hold");
+    if (d->hold) {
+      const dgmx_status hs = hold_stage(d, a, d->T[d->tcur ^ 1], nullptr);
+      if (hs != DGMX_OK) return hs;
+    }
     dgmx_status xs = exchange(d, trace_halo(d, d->tcur ^ 1));
     if (xs != DGMX_OK) return xs;
     d->tcur ^= 1;
@@ -458,8 +527,9 @@ int stages_per_step(int inttype) { return inttype == DGMX_LSRK14 ? 14 : (inttype
 int launches_per_stage(const dgmx_domain *d) {
   const bool rank = d->partitioned() && !d->in_group;
   const int halo = rank ? (d->ns() ? 4 : 2) : 0;   // pack + unpack per exchange
-  const int split = rank && d->nccl && !d->xhost && d->xstream ? 1 : 0;   // boundary and interior tiles
-  return (d->ns() ? 3 : 1) + split + (d->hold ? 2 : 0) + halo;
+  const int split = rank && d->nccl && !d->xhost && d->xstream && !d->hold ? 1 : 0;   // boundary and interior tiles
+  const int hold = d->hold ? (rank ? 3 : 2) : 0;   // (scatter,) reduce, apply
+  return (d->ns() ? 3 : 1) + split + hold + halo;
 }
 
 // Host repeat of launch_reference_integrals' summation order over the
@@ -800,11 +870,9 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
     g_create_error = err;
     return DGMX_ERR_ARGUMENT;
   }
+  std::vector<double> Jglob;   // partitions of Navier-Stokes 3-D: the whole mesh's Jacobians and
+  std::vector<int> gid_host;   // every rank's global ids, for the bulk-flow hold
   if (pspec && pspec->nranks > 1) {
-    if (d->hold) {
-      g_create_error = "the bulk-flow hold is not built for partitions";
-      return DGMX_ERR_UNSUPPORTED;
-    }
     if (pspec->group && phys == DGMX_SHALLOW && p->sw_balance) {
       g_create_error = "in-process partitions of shallow water need sw_balance = 0";
       return DGMX_ERR_UNSUPPORTED;
@@ -818,6 +886,15 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
     std::vector<int> per(pspec->nranks, 0);
     for (int e = 0; e < d->ne_global; ++e) ++per[pspec->part[e]];
     d->max_ne = *std::max_element(per.begin(), per.end());
+    if (phys == DGMX_NS3D) {
+      Jglob = d->mesh.J;
+      gid_host.assign((size_t)pspec->nranks * d->max_ne, -1);
+      std::vector<int> fill(pspec->nranks, 0);
+      for (int e = 0; e < d->ne_global; ++e) {
+        const int q = pspec->part[e];
+        gid_host[(size_t)q * d->max_ne + fill[q]++] = e;
+      }
+    }
     d->mesh = std::move(local);
     d->ne = d->plan.ne_local;
     d->in_group = pspec->group;
@@ -853,7 +930,15 @@ dgmx_status create_impl(const dgmx_mesh *m, const dgmx_params *p, dgmx_domain **
                           chk(dalloc(&d->Vtr, (size_t)d->nslot * d->nfaces * (d->nf - 1) * d->gf), "alloc viscous traces") &&
                           chk(dalloc(&d->Pv, (size_t)d->ne * (d->nf - 1) * d->ld), "alloc viscous divergence"))) &&
             (!d->ns() || d->dim != 3 || (chk(dalloc(&d->R0, (size_t)d->ne * d->nf), "alloc hold coefficients") &&
-                                          chk(dalloc(&d->cbar, (size_t)d->nf), "alloc hold means")));
+                                          chk(dalloc(&d->cbar, (size_t)d->nf), "alloc hold means"))) &&
+            (gid_host.empty() ||
+             (chk(dalloc(&d->R0g, (size_t)d->ne_global * d->nf), "alloc hold coefficients (whole mesh)") &&
+              chk(dalloc(&d->Jg, (size_t)d->ne_global), "alloc Jacobians (whole mesh)") &&
+              chk(dalloc(&d->hold_rows, gid_host.size() * d->nf), "alloc hold rows") &&
+              chk(dalloc(&d->gid_all, gid_host.size()), "alloc global ids") &&
+              chk(cudaMemcpy(d->Jg, Jglob.data(), sizeof(double) * Jglob.size(), cudaMemcpyHostToDevice), "upload") &&
+              chk(cudaMemcpy(d->gid_all, gid_host.data(), sizeof(int) * gid_host.size(), cudaMemcpyHostToDevice),
+                  "upload")));
   if (ok) {
     ok = chk(cudaMemcpy(d->gclass, d->mesh.gclass.data(), sizeof(int) * d->ne, cudaMemcpyHostToDevice), "upload") &&
          chk(cudaMemcpy(d->classes, d->mesh.classes.data(), sizeof(GeomClass) * d->mesh.classes.size(),
@@ -980,24 +1065,35 @@ dgmx_status dgmx_create(const dgmx_mesh *mesh, const dgmx_params *params, dgmx_d
   }
 }
 
+}  // extern "C"
+
+namespace {
+// (element, side, kind) records with five parameters each into a BoundarySpec
+dgmx_status parse_boundaries(int nbc, const int *bc_sides, const double *bc_params, BoundarySpec &b) {
+  if (nbc < 0 || (nbc > 0 && (!bc_sides || !bc_params))) { g_create_error = "null argument"; return DGMX_ERR_ARGUMENT; }
+  for (int i = 0; i < nbc; ++i) {
+    const int k = bc_sides[3 * i + 2];
+    if (k < DGMX_BC_SLIP_WALL || k > DGMX_BC_SUPERSONIC_OUTFLOW) {
+      g_create_error = "unknown boundary kind " + std::to_string(k);
+      return DGMX_ERR_ARGUMENT;
+    }
+    const int t = b.type_of(k, bc_params + 5 * i);
+    if (!t) { g_create_error = "more than 15 distinct boundary types"; return DGMX_ERR_UNSUPPORTED; }
+    b.sides.push_back(BoundarySide{bc_sides[3 * i], bc_sides[3 * i + 1], t});
+  }
+  return DGMX_OK;
+}
+}  // namespace
+
+extern "C" {
+
 dgmx_status dgmx_create_with_boundaries(const dgmx_mesh *mesh, const dgmx_params *params, int nbc,
                                         const int *bc_sides, const double *bc_params, dgmx_domain **out) {
-  if (!mesh || !params || !out || nbc < 0 || (nbc > 0 && (!bc_sides || !bc_params))) {
-    g_create_error = "null argument";
-    return DGMX_ERR_ARGUMENT;
-  }
+  if (!mesh || !params || !out) { g_create_error = "null argument"; return DGMX_ERR_ARGUMENT; }
   try {
     BoundarySpec b;
-    for (int i = 0; i < nbc; ++i) {
-      const int k = bc_sides[3 * i + 2];
-      if (k < DGMX_BC_SLIP_WALL || k > DGMX_BC_SUPERSONIC_OUTFLOW) {
-        g_create_error = "unknown boundary kind " + std::to_string(k);
-        return DGMX_ERR_ARGUMENT;
-      }
-      const int t = b.type_of(k, bc_params + 5 * i);
-      if (!t) { g_create_error = "more than 15 distinct boundary types"; return DGMX_ERR_UNSUPPORTED; }
-      b.sides.push_back(BoundarySide{bc_sides[3 * i], bc_sides[3 * i + 1], t});
-    }
+    const dgmx_status st = parse_boundaries(nbc, bc_sides, bc_params, b);
+    if (st != DGMX_OK) return st;
     return create_impl(mesh, params, out, &b);
   } catch (const std::exception &ex) {
     g_create_error = ex.what();
@@ -1007,11 +1103,20 @@ dgmx_status dgmx_create_with_boundaries(const dgmx_mesh *mesh, const dgmx_params
 
 dgmx_status dgmx_create_partition(const dgmx_mesh *mesh, const dgmx_params *params, const int *part, int nranks,
                                   int rank, dgmx_domain **out) {
+  return dgmx_create_partition_with_boundaries(mesh, params, part, nranks, rank, 0, nullptr, nullptr, out);
+}
+
+dgmx_status dgmx_create_partition_with_boundaries(const dgmx_mesh *mesh, const dgmx_params *params, const int *part,
+                                                  int nranks, int rank, int nbc, const int *bc_sides,
+                                                  const double *bc_params, dgmx_domain **out) {
   if (!mesh || !params || !part || !out || nranks < 1) { g_create_error = "null argument"; return DGMX_ERR_ARGUMENT; }
   try {
+    BoundarySpec b;
+    const dgmx_status st = parse_boundaries(nbc, bc_sides, bc_params, b);
+    if (st != DGMX_OK) return st;
     PartitionSpec ps;
     ps.part = part; ps.nranks = nranks; ps.rank = rank;
-    return create_impl(mesh, params, out, nullptr, &ps);
+    return create_impl(mesh, params, out, nbc > 0 ? &b : nullptr, &ps);
   } catch (const std::exception &ex) {
     g_create_error = ex.what();
     return DGMX_ERR_ARGUMENT;
@@ -1138,7 +1243,7 @@ dgmx_status dgmx_set_source_pulse(dgmx_domain *d, double t0, double sigma_t) {
 dgmx_status dgmx_set_bulk_hold(dgmx_domain *d, int on) {
   if (!d) return DGMX_ERR_ARGUMENT;
   if (on && !d->R0) return d->fail(DGMX_ERR_UNSUPPORTED, "the bulk-flow hold is a Navier-Stokes 3-D option");
-  if (on && d->partitioned()) return d->fail(DGMX_ERR_UNSUPPORTED, "the bulk-flow hold is not built for partitions");
+  if (on && d->partitioned() && !d->R0g) return d->fail(DGMX_ERR_UNSUPPORTED, "partition without the whole-mesh hold buffers");
   if (d->hold != (on != 0)) {
     d->hold = on != 0;
     if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
@@ -1387,7 +1492,7 @@ dgmx_status dgmx_time_derivative_device(dgmx_domain *d, const double *U_dev, dou
   if (e != cudaSuccess) return d->cuda(e, "nodal rhs kernel");
   if (d->hold) {
     a.kind = kRHS; a.A = nullptr;
-    if ((e = d->hold_after(a, nullptr, F_dev)) != cudaSuccess) return d->cuda(e, "bulk-flow hold");
+    if ((xs = hold_stage(d, a, nullptr, F_dev)) != DGMX_OK) return xs;
   }
   // the traces of the current modal register live in T[tcur]; T[tcur^1]
   // was used as scratch and is rewritten by the next stage.
@@ -1716,6 +1821,12 @@ extern "C" {
 
 dgmx_status dgmx_group_create(const dgmx_mesh *mesh, const dgmx_params *params, const int *part, int nparts,
                               dgmx_group **out) {
+  return dgmx_group_create_with_boundaries(mesh, params, part, nparts, 0, nullptr, nullptr, out);
+}
+
+dgmx_status dgmx_group_create_with_boundaries(const dgmx_mesh *mesh, const dgmx_params *params, const int *part,
+                                              int nparts, int nbc, const int *bc_sides, const double *bc_params,
+                                              dgmx_group **out) {
   if (!mesh || !params || !part || !out || nparts < 2) { g_create_error = "group: null argument or nparts < 2"; return DGMX_ERR_ARGUMENT; }
   *out = nullptr;
   auto g = std::make_unique<dgmx_group>();
@@ -1727,7 +1838,9 @@ dgmx_status dgmx_group_create(const dgmx_mesh *mesh, const dgmx_params *params, 
     dgmx_domain *d = nullptr;
     dgmx_status st;
     try {
-      st = create_impl(mesh, params, &d, nullptr, &ps);
+      BoundarySpec b;
+      st = parse_boundaries(nbc, bc_sides, bc_params, b);
+      if (st == DGMX_OK) st = create_impl(mesh, params, &d, nbc > 0 ? &b : nullptr, &ps);
     } catch (const std::exception &ex) {
       g_create_error = ex.what();
       st = DGMX_ERR_ARGUMENT;
@@ -1736,6 +1849,15 @@ dgmx_status dgmx_group_create(const dgmx_mesh *mesh, const dgmx_params *params, 
     g->parts.push_back(d);
   }
   *out = g.release();
+  return DGMX_OK;
+}
+
+dgmx_status dgmx_group_set_bulk_hold(dgmx_group *g, int on) {
+  if (!g) return DGMX_ERR_ARGUMENT;
+  for (dgmx_domain *d : g->parts) {
+    const dgmx_status st = dgmx_set_bulk_hold(d, on);
+    if (st != DGMX_OK) return group_fail(g, d, st);
+  }
   return DGMX_OK;
 }
 
@@ -1817,6 +1939,36 @@ dgmx_status dgmx_group_advance(dgmx_group *g, double dt, int nsteps) {
           d->launches += 2;
         }
         if (e == cudaSuccess && (st = group_exchange(g, 2, s)) != DGMX_OK) return st;
+      }
+      if (d0->hold) {
+        // bulk-flow hold: every part's tiles, the parts' constant
+        // coefficients into the whole mesh's order, the unpartitioned
+        // domain's means (part 0's buffers), applied to every part, then
+        // the exchange of the held traces
+        for (dgmx_domain *d : g->parts) {
+          const StageArgs a = stage_args(d, sp, dt);
+          if (e == cudaSuccess) e = stage_tiles(d, a, 0, s);
+          if (e == cudaSuccess) e = stage_tiles(d, a, 1, s);
+          if (e == cudaSuccess)
+            e = launch_scatter_rows(d->R0, d->gid_all + (size_t)d->plan.rank * d->max_ne, d->ne, d->nf, d0->R0g, s);
+          d->launches += 3;
+        }
+        if (e == cudaSuccess) {
+          HoldArgs h = d0->hold_args(stage_args(d0, sp, dt), nullptr, nullptr);
+          h.ne = d0->ne_global; h.R0 = d0->R0g; h.J = d0->Jg;
+          e = launch_hold_reduce(h, s);
+          ++d0->launches;
+        }
+        for (dgmx_domain *d : g->parts) {
+          HoldArgs h = d->hold_args(stage_args(d, sp, dt), d->T[d->tcur ^ 1], nullptr);
+          h.cbar = d0->cbar;
+          if (e == cudaSuccess) e = launch_hold_apply(h, s);
+          ++d->launches;
+        }
+        if (e == cudaSuccess && (st = group_exchange(g, 1, s)) != DGMX_OK) return st;
+        for (dgmx_domain *d : g->parts) d->tcur ^= 1;
+        if (e != cudaSuccess) break;
+        continue;
       }
       // boundary tiles of every part, then their exchange on the side
       // stream while the interior tiles run

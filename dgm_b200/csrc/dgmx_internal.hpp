@@ -271,7 +271,14 @@ struct HoldArgs {
   double c0, c1, dt;
   double *U, *Ut, *A, *Tout, *Fn;
 };
-cudaError_t launch_hold(const HoldArgs &h, cudaStream_t s);
+cudaError_t launch_hold(const HoldArgs &h, cudaStream_t s);   // reduce, then apply
+// The two halves: cbar from R0 / J over h.ne elements (one block, fixed
+// order), and its application to the registers and traces of h.ne elements.
+cudaError_t launch_hold_reduce(const HoldArgs &h, cudaStream_t s);
+cudaError_t launch_hold_apply(const HoldArgs &h, cudaStream_t s);
+// dst[gid[i]][0 .. nf) = src[i][0 .. nf) for the n rows with gid[i] >= 0
+// (element partitions: a part's constant coefficients into the whole mesh's).
+cudaError_t launch_scatter_rows(const double *src, const int *gid, int n, int nf, double *dst, cudaStream_t s);
 
 // Registry key offset of the mixed-precision (FP32 working precision) tiles.
 constexpr int kMixedKey = 1000;

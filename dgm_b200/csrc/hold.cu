@@ -99,13 +99,38 @@ __global__ void __launch_bounds__(kHoldThreads) hold_apply_kernel(HoldArgs h) {
   }
 }
 
+__global__ void scatter_rows_kernel(const double *__restrict__ src, const int *__restrict__ gid, int n, int nf,
+                                    double *__restrict__ dst) {
+  const long long total = (long long)n * nf;
+  for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < total;
+       w += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(w / nf), k = (int)(w - (long long)i * nf);
+    const int g = gid[i];
+    if (g >= 0) dst[(size_t)g * nf + k] = src[w];
+  }
+}
+
 }  // namespace
 
-cudaError_t launch_hold(const HoldArgs &h, cudaStream_t s) {
+cudaError_t launch_hold_reduce(const HoldArgs &h, cudaStream_t s) {
   hold_reduce_kernel<<<1, kHoldThreads, 0, s>>>(h);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hold_apply(const HoldArgs &h, cudaStream_t s) {
   hold_apply_kernel<<<4 * 148, kHoldThreads, 0, s>>>(h);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hold(const HoldArgs &h, cudaStream_t s) {
+  cudaError_t e = launch_hold_reduce(h, s);
+  return e == cudaSuccess ? launch_hold_apply(h, s) : e;
+}
+
+cudaError_t launch_scatter_rows(const double *src, const int *gid, int n, int nf, double *dst, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const long long b = ((long long)n * nf + 255) / 256;
+  scatter_rows_kernel<<<(int)(b < 4 * 148 ? b : 4 * 148), 256, 0, s>>>(src, gid, n, nf, dst);
   return cudaGetLastError();
 }
 

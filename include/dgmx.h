@@ -123,9 +123,17 @@ dgmx_status dgmx_create_with_boundaries(const dgmx_mesh *mesh, const dgmx_params
  * exchange fills after every stage (and after the viscous flux kernel for
  * Navier-Stokes).  FP64 or DGMX_MIXED (FP32 trace blocks on the wire; the
  * reference state is the unpartitioned domain's, from every rank's element
- * integrals, so setting the state is collective); no bulk-flow hold. */
+ * integrals, so setting the state is collective).  Boundary sides as in
+ * dgmx_create_with_boundaries (global element ids; each rank keeps its own).
+ * The bulk-flow hold (dgmx_set_bulk_hold, Navier-Stokes 3-D) takes its means
+ * over the whole mesh: after every stage each rank sends its elements'
+ * constant coefficients to every peer, and the stage then runs without the
+ * boundary / interior overlap. */
 dgmx_status dgmx_create_partition(const dgmx_mesh *mesh, const dgmx_params *params, const int *part, int nranks,
                                   int rank, dgmx_domain **out);
+dgmx_status dgmx_create_partition_with_boundaries(const dgmx_mesh *mesh, const dgmx_params *params, const int *part,
+                                                  int nranks, int rank, int nbc, const int *bc_sides,
+                                                  const double *bc_params, dgmx_domain **out);
 /* NCCL transport for the multi-rank exchange: rank 0 makes the id, every
  * rank passes the same id (collective over the ranks). */
 #define DGMX_NCCL_ID_BYTES 128
@@ -154,6 +162,11 @@ dgmx_status dgmx_partition_plan(const dgmx_mesh *mesh, const int *part, int nran
 typedef struct dgmx_group dgmx_group;
 dgmx_status dgmx_group_create(const dgmx_mesh *mesh, const dgmx_params *params, const int *part, int nparts,
                               dgmx_group **out);
+dgmx_status dgmx_group_create_with_boundaries(const dgmx_mesh *mesh, const dgmx_params *params, const int *part,
+                                              int nparts, int nbc, const int *bc_sides, const double *bc_params,
+                                              dgmx_group **out);
+/* the bulk-flow hold on every part, means over the whole mesh */
+dgmx_status dgmx_group_set_bulk_hold(dgmx_group *g, int on);
 dgmx_status dgmx_group_destroy(dgmx_group *g);
 dgmx_domain *dgmx_group_part(dgmx_group *g, int r);
 dgmx_status dgmx_group_set_state(dgmx_group *g, const double *U);

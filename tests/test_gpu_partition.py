@@ -7,6 +7,7 @@ import pytest
 
 import oracle
 from oracle import dgm_io, ics
+from tests.cases import BC_ISOTHERMAL_WALL
 
 pytestmark = pytest.mark.gpu
 
@@ -134,30 +135,80 @@ def _rank_run(rank, nranks, port, case, result):
     _os.environ["MASTER_ADDR"] = "127.0.0.1"
     _os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=nranks, timeout=datetime.timedelta(seconds=60))
-    phys, n, p, flux, inttype, dt, steps, vis, prec = case
-    m = dgm_b200.meshgen.box(3, n, 0.0, 2 * np.pi, p)
+    phys, n, p, flux, inttype, dt, steps, vis, prec, hold = case
+    m, rec, ic = _case_mesh(n, p, hold)
     ne = m.verts.shape[0]
     part = (np.arange(ne) * nranks) // ne
-    D = dgm_b200.Domain.partition(m, phys, part, nranks, rank, flux=flux, inttype=inttype, vis=vis, precision=prec)
+    D = dgm_b200.Domain.partition(m, phys, part, nranks, rank, flux=flux, inttype=inttype, vis=vis, precision=prec,
+                                  boundaries=rec, bulk_hold=hold)
     D.set_exchange_host()
     nl, ng, gids = D.partition_info()
     x, y, z = D.coordinates()
-    D.set_state(ics.taylor_green(x, y, z, Ma=0.1))
+    D.set_state(ic(x, y, z))
     D.advance(dt, steps)
     result[rank] = (gids.copy(), D.state())
     dist.barrier()
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("case", [(8, (3, 2, 4), 3, "roe", 14, 0.002, 2, 0.0, 0),
-                                  (9, (2, 2, 3), 2, "laxfriedrichs", 3, 0.002, 2, 0.02, 0),
-                                  (8, (3, 2, 4), 3, "roe", 14, 0.002, 2, 0.0, 1)],
-                         ids=["euler3d-lsrk14", "ns3d-tvd3", "euler3d-lsrk14-mixed"])
+def _case_mesh(n, p, walls):
+    """Periodic box [0,2pi]^3 with the Taylor-Green state, or the channel:
+    [0,2pi]^2 x [0,2] with isothermal walls at z = 0 and z = 2 and the
+    wall-bounded shear flow."""
+    import dgm_b200
+    from tests.test_gpu_boundaries import channel_ic, wall_records
+    if not walls:
+        return dgm_b200.meshgen.box(3, n, 0.0, 2 * np.pi, p), None, lambda x, y, z: ics.taylor_green(x, y, z, Ma=0.1)
+    m = dgm_b200.meshgen.box(3, n, (0.0, 0.0, 0.0), (2 * np.pi, 2 * np.pi, 2.0), p)
+    return m, wall_records(n, BC_ISOTHERMAL_WALL, 1.0, 178.575), channel_ic
+
+
+HOLD_CASES = [
+    # name, n, p, flux, inttype, dt, steps, vis, nparts, kind, hold
+    ("ns3d-walls-hold-lsrk14-2-slabs", (3, 2, 4), 3, "laxfriedrichs", 14, 0.001, 2, 0.02, 2, "slabs", True),
+    ("ns3d-walls-hold-rk4-3-random", (2, 3, 4), 2, "laxfriedrichs", 4, 0.001, 2, 0.01, 3, "random", True),
+    ("ns3d-walls-tvd3-2-random", (2, 2, 3), 3, "laxfriedrichs", 3, 0.001, 3, 0.02, 2, "random", False),
+]
+
+
+@pytest.mark.parametrize("case", HOLD_CASES, ids=[c[0] for c in HOLD_CASES])
+def test_group_walls_and_hold_equal_single_domain(case):
+    """Boundary sides and the channel's bulk-flow hold on an element
+    partition: each part keeps its own wall sides, and the hold's means are
+    taken over the whole mesh in global element order (every part's constant
+    coefficients gathered after each stage), so the state equals the
+    unpartitioned domain's bit for bit."""
+    import dgm_b200
+    _, n, p, flux, inttype, dt, steps, vis, nparts, kind, hold = case
+    m, rec, ic = _case_mesh(n, p, True)
+    ne = m.verts.shape[0]
+    part = ((np.arange(ne) * nparts) // ne if kind == "slabs"
+            else np.random.default_rng(11).permutation(np.arange(ne) % nparts))
+    D = dgm_b200.Domain(m, 9, flux=flux, inttype=inttype, vis=vis, boundaries=rec, bulk_hold=hold)
+    G = dgm_b200.Group(m, 9, part, flux=flux, inttype=inttype, vis=vis, boundaries=rec, bulk_hold=hold)
+    x, y, z = D.coordinates()
+    f = ic(x, y, z)
+    D.set_state(f)
+    G.set_state(f)
+    D.advance(dt, steps)
+    G.advance(dt, steps)
+    S = D.state()
+    assert np.array_equal(G.state(), S)
+    assert not np.array_equal(S, f)
+    G.close()
+
+
+@pytest.mark.parametrize("case", [(8, (3, 2, 4), 3, "roe", 14, 0.002, 2, 0.0, 0, False),
+                                  (9, (2, 2, 3), 2, "laxfriedrichs", 3, 0.002, 2, 0.02, 0, False),
+                                  (8, (3, 2, 4), 3, "roe", 14, 0.002, 2, 0.0, 1, False),
+                                  (9, (3, 2, 4), 3, "laxfriedrichs", 14, 0.001, 2, 0.02, 0, True)],
+                         ids=["euler3d-lsrk14", "ns3d-tvd3", "euler3d-lsrk14-mixed", "ns3d-walls-hold-lsrk14"])
 def test_two_process_ranks_equal_single_domain(case):
     """Two processes, each one rank of a partitioned domain, exchanging halos
     through the host: the gathered state equals the unpartitioned run (the
-    mixed form's ranks gather the reference state's element integrals
-    through the same transport)."""
+    mixed form's ranks gather the reference state's element integrals, and
+    the bulk-flow hold's ranks every stage's constant coefficients, through
+    the same transport)."""
     import socket
     import torch.multiprocessing as mp
     import dgm_b200
@@ -175,11 +226,12 @@ def test_two_process_ranks_equal_single_domain(case):
         if pr.is_alive():
             pr.kill()
         assert pr.exitcode == 0
-    phys, n, p, flux, inttype, dt, steps, vis, prec = case
-    m = dgm_b200.meshgen.box(3, n, 0.0, 2 * np.pi, p)
-    D = dgm_b200.Domain(m, phys, flux=flux, inttype=inttype, vis=vis, precision=prec)
+    phys, n, p, flux, inttype, dt, steps, vis, prec, hold = case
+    m, rec, ic = _case_mesh(n, p, hold)
+    D = dgm_b200.Domain(m, phys, flux=flux, inttype=inttype, vis=vis, precision=prec, boundaries=rec,
+                        bulk_hold=hold)
     x, y, z = D.coordinates()
-    D.set_state(ics.taylor_green(x, y, z, Ma=0.1))
+    D.set_state(ic(x, y, z))
     D.advance(dt, steps)
     S = D.state()
     qd = (p + 2) ** 3
