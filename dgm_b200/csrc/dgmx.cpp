@@ -144,6 +144,8 @@ struct dgmx_domain {
   cudaEvent_t ev_b = nullptr, ev_x = nullptr;
   int *tiles = nullptr;                                  // [boundary tiles | interior tiles], then the two counts
   int tiles_epb = 0, ntiles_b = 0, ntiles_i = 0;
+  int *vtiles = nullptr;                                 // the same split at the viscous kernel's tile size
+  int vtiles_epb = 0, nvt_b = 0, nvt_i = 0;
   int tcur = 0;
   bool sw_captured = false;
   long launches = 0;
@@ -232,6 +234,15 @@ struct dgmx_domain {
     if (visc32 && visc_tc) return vops->ns_visc32tc(a, nodal, s);
     return visc32 ? vops->ns_visc32(a, nodal, s) : ops->ns_visc(a, nodal, s);
   }
+  int visc_epb() const { return (visc32 ? vops : ops)->epb; }
+  // the viscous flux kernel over tile list which (0 boundary, 1 interior);
+  // no launch for an empty list
+  cudaError_t ns_visc_tiles(StageArgs a, int which, cudaStream_t s) const {
+    a.nvtiles = which == 0 ? nvt_b : nvt_i;
+    if (!a.nvtiles) return cudaSuccess;
+    a.vtiles = vtiles + (which == 0 ? 0 : nvt_b);
+    return ns_visc(a, false, s);
+  }
   bool mixed() const { return prm.precision == DGMX_MIXED; }
   const KernelOps *stage_ops() const { return mixed() ? ops_m : ops; }
 
@@ -240,7 +251,7 @@ struct dgmx_domain {
     graph = nullptr;
     void *ptrs[] = {U, Ut, Acc, T[0], T[1], Rsw, nod_in, nod_out, Jdev, integ, gclass, perm, err, classes, links,
                     Ghat, Vtr, Pv, Utf, Tf[0], Tf[1], uref, R0, cbar, x_send, x_recv, x_sbuf, x_rbuf, tiles, Ssrc,
-                    R0g, Jg, hold_rows, gid_all};
+                    R0g, Jg, hold_rows, gid_all, vtiles};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (host_pinned) cudaFreeHost(host_pinned);
     if (xh_send) cudaFreeHost(xh_send);
@@ -256,6 +267,7 @@ struct dgmx_domain {
     R0 = cbar = Ssrc = nullptr;
     R0g = Jg = hold_rows = nullptr; gid_all = nullptr;
     x_send = x_recv = nullptr; x_sbuf = x_rbuf = nullptr; tiles = nullptr; tiles_epb = 0;
+    vtiles = nullptr; vtiles_epb = 0;
     if (ev_b) cudaEventDestroy(ev_b);
     if (ev_x) cudaEventDestroy(ev_x);
     if (xstream) cudaStreamDestroy(xstream);
@@ -445,6 +457,31 @@ dgmx_status build_tiles(dgmx_domain *d) {
   return DGMX_OK;
 }
 
+// The boundary / interior split of build_tiles at the viscous flux
+// kernel's tile size (Navier-Stokes), for its launch over a list.
+dgmx_status build_vtiles(dgmx_domain *d) {
+  if (!d->ns()) return DGMX_OK;
+  const int epb = d->visc_epb();
+  if (d->vtiles && d->vtiles_epb == epb) return DGMX_OK;
+  const int nt = (d->ne + epb - 1) / epb, nf = d->nfaces;
+  std::vector<int> b, in;
+  for (int t = 0; t < nt; ++t) {
+    bool bnd = false;
+    for (int e = t * epb; e < std::min(d->ne, (t + 1) * epb) && !bnd; ++e)
+      for (int f = 0; f < nf; ++f)
+        if (d->mesh.links[(size_t)e * nf + f].elem >= d->ne) { bnd = true; break; }
+    (bnd ? b : in).push_back(t);
+  }
+  b.insert(b.end(), in.begin(), in.end());
+  if (d->vtiles) { cudaFree(d->vtiles); d->vtiles = nullptr; }
+  cudaError_t e = dalloc(&d->vtiles, b.size());
+  if (e == cudaSuccess) e = cudaMemcpy(d->vtiles, b.data(), sizeof(int) * b.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return d->cuda(e, "viscous tile lists");
+  d->vtiles_epb = epb; d->nvt_b = (int)(b.size() - in.size()); d->nvt_i = (int)in.size();
+  if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  return DGMX_OK;
+}
+
 // The stage kernel over one of the two tile lists (0 boundary, 1 interior).
 cudaError_t stage_tiles(const dgmx_domain *d, StageArgs a, int which, cudaStream_t s) {
   const int n = which == 0 ? d->ntiles_b : d->ntiles_i;
@@ -459,6 +496,29 @@ cudaError_t stage_tiles(const dgmx_domain *d, StageArgs a, int which, cudaStream
   return o->stage_grid(a, n < cap ? n : cap, s);
 }
 
+// The NCCL halo exchange of one buffer enqueued on stream s (pack, grouped
+// send / receive with every peer, unpack), without a host wait.
+dgmx_status exchange_on(dgmx_domain *d, const Halo &h, cudaStream_t s) {
+  const int blk = h.wire();
+  cudaError_t e = h.pack(d, s);
+  if (e != cudaSuccess) return d->cuda(e, "halo pack");
+  const NcclApi &nc = nccl_api();
+  ncclResult_t r = nc.GroupStart();
+  for (int q = 0; q < d->plan.nranks && r == ncclSuccess; ++q) {
+    if (!d->x_cnt[q]) continue;
+    const size_t off = (size_t)d->x_off[q] * blk, n = (size_t)d->x_cnt[q] * blk;
+    r = nc.Send(d->x_sbuf + off, n, ncclFloat64, q, d->nccl, s);
+    if (r == ncclSuccess) r = nc.Recv(d->x_rbuf + off, n, ncclFloat64, q, d->nccl, s);
+  }
+  const ncclResult_t r2 = nc.GroupEnd();
+  if (r == ncclSuccess) r = r2;
+  if (r != ncclSuccess) return d->fail(DGMX_ERR_CUDA, std::string("halo exchange: ") + nc.GetErrorString(r));
+  d->launches += 2;
+  return d->cuda(h.unpack(d, s), "halo unpack");
+}
+
+bool overlaps(const dgmx_domain *d) { return d->partitioned() && d->nccl && !d->xhost && d->xstream; }
+
 // One stage of an NCCL rank with the exchange overlapped: boundary tiles,
 // then the exchange on xstream while the interior tiles run on stream.
 dgmx_status stage_overlapped(dgmx_domain *d, const StageArgs &a) {
@@ -466,27 +526,30 @@ dgmx_status stage_overlapped(dgmx_domain *d, const StageArgs &a) {
   if (e == cudaSuccess) e = cudaEventRecord(d->ev_b, d->stream);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(d->xstream, d->ev_b, 0);
   if (e != cudaSuccess) return d->cuda(e, "boundary tiles");
-  const Halo h = trace_halo(d, d->tcur ^ 1);
-  const int blk = h.wire();
-  e = h.pack(d, d->xstream);
-  if (e != cudaSuccess) return d->cuda(e, "halo pack");
-  const NcclApi &nc = nccl_api();
-  ncclResult_t r = nc.GroupStart();
-  for (int q = 0; q < d->plan.nranks && r == ncclSuccess; ++q) {
-    if (!d->x_cnt[q]) continue;
-    const size_t off = (size_t)d->x_off[q] * blk, n = (size_t)d->x_cnt[q] * blk;
-    r = nc.Send(d->x_sbuf + off, n, ncclFloat64, q, d->nccl, d->xstream);
-    if (r == ncclSuccess) r = nc.Recv(d->x_rbuf + off, n, ncclFloat64, q, d->nccl, d->xstream);
-  }
-  const ncclResult_t r2 = nc.GroupEnd();
-  if (r == ncclSuccess) r = r2;
-  if (r != ncclSuccess) return d->fail(DGMX_ERR_CUDA, std::string("halo exchange: ") + nc.GetErrorString(r));
-  e = h.unpack(d, d->xstream);
-  if (e == cudaSuccess) e = cudaEventRecord(d->ev_x, d->xstream);
+  const dgmx_status xs = exchange_on(d, trace_halo(d, d->tcur ^ 1), d->xstream);
+  if (xs != DGMX_OK) return xs;
+  e = cudaEventRecord(d->ev_x, d->xstream);
   if (e == cudaSuccess) e = stage_tiles(d, a, 1, d->stream);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(d->stream, d->ev_x, 0);
-  d->launches += 4;
+  d->launches += 2;
   return d->cuda(e, "overlapped stage");
+}
+
+// Navier-Stokes viscous flux of an NCCL rank with its trace exchange
+// overlapped: boundary tiles, then the exchange of their viscous traces on
+// xstream while the interior tiles run on stream.
+dgmx_status visc_overlapped(dgmx_domain *d, const StageArgs &a) {
+  cudaError_t e = d->ns_visc_tiles(a, 0, d->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(d->ev_b, d->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(d->xstream, d->ev_b, 0);
+  if (e != cudaSuccess) return d->cuda(e, "viscous boundary tiles");
+  const dgmx_status xs = exchange_on(d, visc_halo(d), d->xstream);
+  if (xs != DGMX_OK) return xs;
+  e = cudaEventRecord(d->ev_x, d->xstream);
+  if (e == cudaSuccess) e = d->ns_visc_tiles(a, 1, d->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(d->stream, d->ev_x, 0);
+  d->launches += 2;
+  return d->cuda(e, "overlapped viscous flux");
 }
 
 // enqueue the stages of one time step on d->stream
@@ -498,12 +561,18 @@ dgmx_status enqueue_step(dgmx_domain *d, double dt) {
     cudaError_t e;
     if (d->ns()) {
       if ((e = d->ns_grad(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous gradient kernel");
-      if ((e = d->ns_visc(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
-      d->launches += 2;
-      dgmx_status xs = exchange(d, visc_halo(d));
-      if (xs != DGMX_OK) return xs;
+      ++d->launches;
+      if (overlaps(d)) {
+        const dgmx_status xs = visc_overlapped(d, a);
+        if (xs != DGMX_OK) return xs;
+      } else {
+        if ((e = d->ns_visc(a, false, d->stream)) != cudaSuccess) return d->cuda(e, "viscous flux kernel");
+        ++d->launches;
+        const dgmx_status xs = exchange(d, visc_halo(d));
+        if (xs != DGMX_OK) return xs;
+      }
     }
-    if (d->partitioned() && d->nccl && !d->xhost && d->xstream && !d->hold) {   // the hold needs all tiles first
+    if (overlaps(d) && !d->hold) {   // the hold needs all tiles first
       const dgmx_status xs = stage_overlapped(d, a);
       if (xs != DGMX_OK) return xs;
       d->tcur ^= 1;
@@ -527,7 +596,9 @@ int stages_per_step(int inttype) { return inttype == DGMX_LSRK14 ? 14 : (inttype
 int launches_per_stage(const dgmx_domain *d) {
   const bool rank = d->partitioned() && !d->in_group;
   const int halo = rank ? (d->ns() ? 4 : 2) : 0;   // pack + unpack per exchange
-  const int split = rank && d->nccl && !d->xhost && d->xstream && !d->hold ? 1 : 0;   // boundary and interior tiles
+  // boundary and interior tiles: the stage kernel (not with the hold) and
+  // the viscous flux kernel
+  const int split = (overlaps(d) && !d->hold ? 1 : 0) + (overlaps(d) && d->ns() ? 1 : 0);
   const int hold = d->hold ? (rank ? 3 : 2) : 0;   // (scatter,) reduce, apply
   return (d->ns() ? 3 : 1) + split + hold + halo;
 }
@@ -1529,7 +1600,7 @@ dgmx_status dgmx_advance_async(dgmx_domain *d, double dt, int nsteps) {
   // The trace buffers swap once per stage, so a graph holds two steps when a
   // step has an odd stage count (TVD3) and the buffer parity repeats.  The
   // graph is rebuilt when dt or the starting parity changes.
-  if (d->partitioned() && d->nccl && (st = build_tiles(d)) != DGMX_OK) return st;
+  if (overlaps(d) && ((st = build_tiles(d)) != DGMX_OK || (st = build_vtiles(d)) != DGMX_OK)) return st;
   const int nst = stages_per_step(d->prm.inttype);
   const int reps = (nst & 1) ? 2 : 1;
   if (d->xhost || d->pulse) {   // host-staged exchanges synchronise every stage / per-stage source factors: no graph
@@ -1919,7 +1990,7 @@ dgmx_status dgmx_group_advance(dgmx_group *g, double dt, int nsteps) {
   for (dgmx_domain *d : g->parts) {
     if (d->prm.physics == DGMX_SHALLOW && d->prm.sw_balance) { g->errmsg = "shallow-water balance is off in groups"; return DGMX_ERR_UNSUPPORTED; }
     if (reset_error_word(d) != DGMX_OK || cudaStreamSynchronize(d->stream) != cudaSuccess) return group_fail(g, d, DGMX_ERR_CUDA);
-    if (build_tiles(d) != DGMX_OK) return group_fail(g, d, DGMX_ERR_CUDA);
+    if (build_tiles(d) != DGMX_OK || build_vtiles(d) != DGMX_OK) return group_fail(g, d, DGMX_ERR_CUDA);
   }
   if (!g->xs) {
     cudaError_t ce = cudaStreamCreateWithFlags(&g->xs, cudaStreamNonBlocking);
@@ -1932,13 +2003,25 @@ dgmx_status dgmx_group_advance(dgmx_group *g, double dt, int nsteps) {
   for (int step = 0; step < nsteps && st == DGMX_OK; ++step)
     for (const StageSpec &sp : specs) {
       if (d0->ns()) {
+        // gradients, the viscous flux of the boundary tiles, then the
+        // exchange of their viscous traces on the side stream while the
+        // interior tiles' viscous flux runs
         for (dgmx_domain *d : g->parts) {
           const StageArgs a = stage_args(d, sp, dt);
           if (e == cudaSuccess) e = d->ns_grad(a, false, s);
-          if (e == cudaSuccess) e = d->ns_visc(a, false, s);
+          if (e == cudaSuccess) e = d->ns_visc_tiles(a, 0, s);
           d->launches += 2;
         }
-        if (e == cudaSuccess && (st = group_exchange(g, 2, s)) != DGMX_OK) return st;
+        if (e == cudaSuccess) e = cudaEventRecord(g->ev_b, s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(g->xs, g->ev_b, 0);
+        if (e == cudaSuccess && (st = group_exchange(g, 2, g->xs)) != DGMX_OK) return st;
+        if (e == cudaSuccess) e = cudaEventRecord(g->ev_x, g->xs);
+        for (dgmx_domain *d : g->parts) {
+          const StageArgs a = stage_args(d, sp, dt);
+          if (e == cudaSuccess) e = d->ns_visc_tiles(a, 1, s);
+          ++d->launches;
+        }
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, g->ev_x, 0);
       }
       if (d0->hold) {
         // bulk-flow hold: every part's tiles, the parts' constant

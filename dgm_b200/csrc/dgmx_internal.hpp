@@ -243,6 +243,10 @@ struct StageArgs {
   const int *tiles;
   const int *ntiles;
   const double *dts;
+  // the viscous flux kernel over a tile list: CTA b takes tile vtiles[b]
+  // (null: tile b), one CTA per listed tile (nvtiles)
+  const int *vtiles;
+  int nvtiles;
   // Navier-Stokes BR1 (src/Navier_Stokes3d.cpp:182-391)
   double *Ghat;           // projected primitive gradients, modal [e][comp][dir][L^d]
   double *V;              // viscous normal-flux traces [e][face][field-1][gf]

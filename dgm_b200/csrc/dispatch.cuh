@@ -122,6 +122,7 @@ struct Launch {
   static constexpr bool kViscLean = C::QD > 512 && EPB == 1 && ViscLeanFits<is_ns(PHYS) && !MIXED, CW2>::value;
   using CW = std::conditional_t<kViscLean, CW2, C>;
   static dim3 grid(int ne) { return dim3((unsigned)((ne + EPB - 1) / EPB)); }
+  static dim3 vgrid(const StageArgs &a) { return a.vtiles ? dim3((unsigned)a.nvtiles) : grid(a.ne); }
   static cudaError_t init(const Tables1D &t) {
     cudaError_t e = upload_tables_lq<L, Q, typename C::R>(t);
     if (e != cudaSuccess) return e;
@@ -173,8 +174,8 @@ struct Launch {
   static cudaError_t ns_visc32(const StageArgs &a, bool nodal, cudaStream_t s) {
     if constexpr (is_ns(PHYS) && !MIXED && MINB == 0) {
       using N = NsCfg<CV, float>;
-      if (nodal) ns_visc_kernel<CV, PHYS, true, float><<<grid(a.ne), CV::NT, N::Visc::SMEM, s>>>(a);
-      else ns_visc_kernel<CV, PHYS, false, float><<<grid(a.ne), CV::NT, N::Visc::SMEM, s>>>(a);
+      if (nodal) ns_visc_kernel<CV, PHYS, true, float><<<vgrid(a), CV::NT, N::Visc::SMEM, s>>>(a);
+      else ns_visc_kernel<CV, PHYS, false, float><<<vgrid(a), CV::NT, N::Visc::SMEM, s>>>(a);
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;
@@ -193,8 +194,8 @@ struct Launch {
   static cudaError_t ns_visc32tc(const StageArgs &a, bool nodal, cudaStream_t s) {
     if constexpr (is_ns(PHYS) && !MIXED && MINB == 0 && kTensorViscous) {
       using N = NsCfg<CV, float>;
-      if (nodal) ns_visc_kernel<CV, PHYS, true, float, true><<<grid(a.ne), CV::NT, N::Visc::SMEM, s>>>(a);
-      else ns_visc_kernel<CV, PHYS, false, float, true><<<grid(a.ne), CV::NT, N::Visc::SMEM, s>>>(a);
+      if (nodal) ns_visc_kernel<CV, PHYS, true, float, true><<<vgrid(a), CV::NT, N::Visc::SMEM, s>>>(a);
+      else ns_visc_kernel<CV, PHYS, false, float, true><<<vgrid(a), CV::NT, N::Visc::SMEM, s>>>(a);
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;
@@ -213,8 +214,8 @@ struct Launch {
   static cudaError_t ns_visc(const StageArgs &a, bool nodal, cudaStream_t s) {
     if constexpr (is_ns(PHYS) && !MIXED) {
       using N = NsCfg<CW>;
-      if (nodal) ns_visc_kernel<CW, PHYS, true><<<grid(a.ne), CW::NT, N::Visc::SMEM, s>>>(a);
-      else ns_visc_kernel<CW, PHYS, false><<<grid(a.ne), CW::NT, N::Visc::SMEM, s>>>(a);
+      if (nodal) ns_visc_kernel<CW, PHYS, true><<<vgrid(a), CW::NT, N::Visc::SMEM, s>>>(a);
+      else ns_visc_kernel<CW, PHYS, false><<<vgrid(a), CW::NT, N::Visc::SMEM, s>>>(a);
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;

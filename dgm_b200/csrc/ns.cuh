@@ -629,7 +629,7 @@ __global__ void __launch_bounds__(C::NT, NsCfg<C, V>::VISC_MINB) ns_visc_kernel(
   GeomClass *geo = reinterpret_cast<GeomClass *>(smem_bytes + R::DATA);
   FaceLink *lnk = reinterpret_cast<FaceLink *>(geo + EPB);
   int *eid = reinterpret_cast<int *>(lnk + EPB * NFACE);
-  const int tid = threadIdx.x, e0 = blockIdx.x * EPB;
+  const int tid = threadIdx.x, e0 = (a.vtiles ? a.vtiles[blockIdx.x] : (int)blockIdx.x) * EPB;
   load_geo_slots<C>(geo, lnk, eid, a, e0, tid);
   if constexpr (R::LEAN) {
     ns_visc_lean_front<C, NODAL, V, TC>(a, B, Gg, X, S1, S2, e0, tid);
