@@ -707,11 +707,6 @@ def run_partitioned(args, torch, dgm_b200, dist, rank, world, local):
     def max_over_ranks(v):
         return reduce(v, dist.ReduceOp.MAX)
 
-    nid = None
-    if not host:
-        obj = [dgm_b200.nccl_unique_id() if rank == 0 else None]
-        dist.broadcast_object_list(obj, src=0)
-        nid = obj[0]
     doms, tiles = {}, {}
     U_ic = dt = None
     for name, prec in (("fp64", dgm_b200.FP64), ("mixed", dgm_b200.MIXED)):
@@ -719,8 +714,10 @@ def run_partitioned(args, torch, dgm_b200, dist, rank, world, local):
                                       inttype=dgm_b200.LSRK14, device=local, precision=prec)
         if host:
             D.set_exchange_host()
-        else:
-            D.set_exchange_nccl(nid)
+        else:   # one NCCL communicator per handle, each from its own id
+            obj = [dgm_b200.nccl_unique_id() if rank == 0 else None]
+            dist.broadcast_object_list(obj, src=0)
+            D.set_exchange_nccl(obj[0])
         if U_ic is None:
             x, y, z = D.coordinates()
             U_ic = taylor_green(x, y, z, WORKLOAD["Ma"], WORKLOAD["gamma"])

@@ -1603,7 +1603,10 @@ dgmx_status dgmx_advance_async(dgmx_domain *d, double dt, int nsteps) {
   if (overlaps(d) && ((st = build_tiles(d)) != DGMX_OK || (st = build_vtiles(d)) != DGMX_OK)) return st;
   const int nst = stages_per_step(d->prm.inttype);
   const int reps = (nst & 1) ? 2 : 1;
-  if (d->xhost || d->pulse) {   // host-staged exchanges synchronise every stage / per-stage source factors: no graph
+  // no graph: host-staged exchanges synchronise every stage, a source pulse
+  // changes its factor every stage, and NCCL ranks enqueue their sends and
+  // receives directly (a step is a few dozen launches, well under its time)
+  if (d->xhost || d->pulse || d->nccl) {
     for (int s = 0; s < nsteps; ++s) {
       if ((st = enqueue_step(d, dt)) != DGMX_OK) return st;
       d->t += dt;

@@ -135,7 +135,9 @@ dgmx_status dgmx_create_partition_with_boundaries(const dgmx_mesh *mesh, const d
                                                   int nranks, int rank, int nbc, const int *bc_sides,
                                                   const double *bc_params, dgmx_domain **out);
 /* NCCL transport for the multi-rank exchange: rank 0 makes the id, every
- * rank passes the same id (collective over the ranks). */
+ * rank passes the same id (collective over the ranks).  One id per
+ * communicator: each partitioned handle needs a fresh id.  Steps of such a
+ * handle are enqueued directly, not replayed from a CUDA graph. */
 #define DGMX_NCCL_ID_BYTES 128
 dgmx_status dgmx_nccl_unique_id(unsigned char *id);
 dgmx_status dgmx_set_exchange_nccl(dgmx_domain *d, const unsigned char *id);
