@@ -134,3 +134,27 @@ def test_connectivity_matches_oracle(which):
                 le, ls, q = pairs[(e, f, g)]
                 assert (le, ls) == (links[e, f, 0], links[e, f, 1])
                 assert perm[e, f, g] == q
+
+
+@pytest.mark.parametrize("world,layout,transport", [(1, "partition", "nccl"), (4, "partition", "nccl"),
+                                                    (2, "partition", "host"), (8, "replicas", "nccl")])
+def test_bench_arms_describe_the_same_workload(world, layout, transport):
+    """Both arms of bench.py build their `config` with one function from the
+    same arguments: at N > 1 the partitioned box grows with N (weak scaling)
+    and the modal DOF counted are the whole job's."""
+    import argparse
+    import bench
+    n, p, q = 32, 3, 5
+    dof = 5 * n ** 3 * (p + 1) ** 3
+    c = bench.config_dict(n, p, q, dof, world, layout, transport)
+    assert c["workload"] == "euler3d_taylor_green_32^3_p3_roe_lsrk14"
+    if world == 1:
+        assert c["parallelism"] == "single device" and c["modal_dof"] == dof
+    elif layout == "partition":
+        assert c["modal_dof"] == dof * world
+        assert c["mesh"].startswith(f"32x32x{32 * world} Hex")
+        assert ("NCCL" in c["parallelism"]) == (transport == "nccl")
+    else:
+        assert c["modal_dof"] == dof and c["parallelism"].startswith("replicas")
+    ns = argparse.Namespace(layout=layout, transport=transport)
+    assert bench.config_dict(n, p, q, dof, world, ns.layout, ns.transport) == c
