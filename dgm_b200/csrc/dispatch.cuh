@@ -95,9 +95,9 @@ struct ViscLeanFits<true, CW> {
   static constexpr bool value = NsCfg<CW, double>::Visc::LEAN && 2 * (NsCfg<CW, double>::Visc::SMEM + 1024) <= 228 * 1024;
 };
 
-template <int PHYS, int L, int Q, int EPB, int MINB, bool MIXED = false>
+template <int PHYS, int L, int Q, int EPB, int MINB, bool MIXED = false, int NT_ = 0>
 struct Launch {
-  using C = Cfg<PHYS, L, Q, EPB, MINB, MIXED>;
+  using C = Cfg<PHYS, L, Q, EPB, MINB, MIXED, NT_>;
   // 3xTF32 tensor-core contractions in the FP32 viscous kernels: 3-D
   // Navier-Stokes at p >= 5 (1-D operators of at least 7 x 7)
   static constexpr bool kTensorViscous = PHYS == DGMX_NS3D && L >= 6;
@@ -476,11 +476,11 @@ constexpr bool ns_fits() {
 
 // Register variant (EPB, MINB) when it is distinct and sensible: the
 // register cap 64K/(NT*MINB) stays >= 48 and the tile fits shared memory.
-template <int PHYS, int P, int Q, int EPB, int MINB, bool MIXED>
+template <int PHYS, int P, int Q, int EPB, int MINB, bool MIXED, int NT = 0>
 void reg_variant() {
-  using C = Cfg<PHYS, P + 1, Q, EPB, MINB, MIXED>;
+  using C = Cfg<PHYS, P + 1, Q, EPB, MINB, MIXED, NT>;
   if constexpr (ns_fits<PHYS, C>() && (MINB == 0 || (65536 / (C::NT * MINB) >= 48 && smem_blocks<C>() >= MINB))) {
-    register_ops(PHYS + (MIXED ? kMixedKey : 0), P + 1, Q, Launch<PHYS, P + 1, Q, EPB, MINB, MIXED>::ops());
+    register_ops(PHYS + (MIXED ? kMixedKey : 0), P + 1, Q, Launch<PHYS, P + 1, Q, EPB, MINB, MIXED, NT>::ops());
   }
 }
 
