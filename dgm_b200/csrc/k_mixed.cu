@@ -8,8 +8,12 @@ namespace {
 struct RegMixed {
   RegMixed() {
 #define R3(P) reg<DGMX_EULER3D, P, P + 2, true>();
-    R3(1) R3(2) R3(3) R3(4) R3(5) R3(6) R3(7)
+    R3(1) R3(2) R3(3) R3(4) R3(5) R3(6)
 #undef R3
+    // p = 7: 512 threads instead of one per point (736 threads at 80
+    // registers spill 132 bytes); registered first, the default
+    reg_variant<DGMX_EULER3D, 7, 9, 1, 0, true, 512>();
+    reg<DGMX_EULER3D, 7, 9, true>();
 #define R3B(P) reg2<DGMX_EULER3D, P, P + 2, true>();
     R3B(2) R3B(3) R3B(4) R3B(5)
 #undef R3B
